@@ -1,0 +1,184 @@
+/*
+ * suli_gpu.h — C-ABI of libsuli_gpu.so, the B200 (sm_100a) implementation of the
+ * per-time-step hot path of SuLi-IC (lacia-udesc/SuLi-OpenMP, directory SuLi-IC/).
+ *
+ * The reference exposes its hot path as argument-less Fortran subroutines that read and
+ * write module arrays (SuLi-IC/0_modules.f90:87-201).  This header replaces each of them
+ * with one extern "C" entry point that acts on a solver context whose fields live in HBM:
+ *
+ *   reference subroutine (file:line)                  entry point here
+ *   ------------------------------------------------  ---------------------------------
+ *   level_set()            14_level_set.f90:221-285    suli_level_set
+ *   heaviside()            14_level_set.f90:612-707    suli_heaviside
+ *   mod_ls1()              14_level_set.f90:709-805    suli_mod_ls1
+ *   level_set_ini() tail   14_level_set.f90:205-217    suli_level_set_ini
+ *   visco()                5_viscosidade.f90:12-219    suli_visco
+ *   convdiff()+classico()  6_convdiff.f90:14-189,
+ *                          7_advectivo.f90:3-290       suli_convdiff
+ *   tempo()                11_diversos.f90:10-230      suli_tempo
+ *   contorno(nlock)        3_contorno.f90:10-492       suli_contorno
+ *   graddin()              9_grad.f90:10-278           suli_graddin
+ *   posdin()               10_pos.f90:1-96             suli_posdin
+ *   est(div)               4_plot.f90:500-525          suli_est
+ *   time loop body         1_principal.f90:64-108      suli_step
+ *   dt = a_dt(tt)          1_principal.f90:78          suli_set_dt
+ *   iniciais() RK table    2_iniciais.f90:85-104       suli_iniciais
+ *
+ * Conventions
+ *  - Every function returns an int status: 0 = OK, > 0 = warning (e.g. the Poisson
+ *    solve hit its iteration cap, which the reference only prints, 9_grad.f90:178),
+ *    < 0 = error.  suli_last_error() gives a message for the last failing call.
+ *  - Host arrays passed to suli_upload/suli_download use the reference's Fortran layout:
+ *    column-major, i fastest, with the extents of the module arrays (halos included);
+ *    suli_field_extent() returns them.  A Fortran caller passes c_loc(u) directly.
+ *  - One context = one CUDA stream; a context must be used from one host thread at a time.
+ *  - Nothing here falls back to the CPU: a missing device or kernel is an error.
+ */
+#ifndef SULI_GPU_H
+#define SULI_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define SULI_OK                 0
+#define SULI_WARN_CG_MAXIT      1   /* Poisson solve stopped at cg_maxit (9_grad.f90:175-178) */
+#define SULI_ERR_ARG           -1   /* bad argument / unsupported parameter combination      */
+#define SULI_ERR_CUDA          -2   /* a CUDA call failed                                     */
+#define SULI_ERR_NAN           -3   /* NaN/Inf met in a reduction                             */
+#define SULI_ERR_UNSUPPORTED   -4   /* option of the reference not built here                 */
+#define SULI_ERR_NOMEM         -5
+#define SULI_ERR_NODEVICE      -6
+#define SULI_ERR_SIZE          -7   /* size beyond a stated maximum                           */
+
+/* ---- run-time parameters (the reference's compile-time parameters, 0_modules.f90) ---- */
+typedef struct suli_params {
+    int    nx, ny, nz;              /* cells (disc, 0_modules.f90:15)                          */
+    double dx, dy, dz;              /* cell sizes (0_modules.f90:7)                            */
+    double dt;                      /* base time step (0_modules.f90:9)                        */
+    int    ccx0, ccxf;              /* x walls: 0 periodic 1 free-slip 2 no-slip 3 prescribed 4 outflow(xf) (0_modules.f90:53-54) */
+    int    ccy0, ccyf;              /* y walls: 0 periodic 1 free-slip 2 no-slip 3 prescribed  (0_modules.f90:58-59) */
+    int    ccz0, cczf;              /* z walls: 1 free-slip 2 no-slip 3 prescribed; 0 periodic is an extension (both ends) */
+    int    t_tempo;                 /* 0 Euler, 1 RK2, 2 RK3, 3 AB2 (0_modules.f90:24)         */
+    int    der;                     /* advection scheme: 1 upwind (0_modules.f90:26)           */
+    int    adv_type;                /* advective form: 1 classic (0_modules.f90:27)            */
+    int    m_turb;                  /* 0 none, 1 Smagorinsky (0_modules.f90:31)                */
+    int    obst_t;                  /* obstacles: only 0 is supported (0_modules.f90:29)       */
+    int    t_hs;                    /* Heaviside type: only 0 (0_modules.f90:199)              */
+    double csmag;                   /* Smagorinsky constant (0_modules.f90:181)                */
+    double gx, gz;                  /* gravity components, gz acts downward (0_modules.f90:143) */
+    double chezy;                   /* wall-friction Chezy coefficient (0_modules.f90:141)     */
+    double rho_f1, mi_f1;           /* fluid where ls < 0 (air)   (14_level_set.f90:26-27)     */
+    double rho_f2, mi_f2;           /* fluid where ls > 0 (water) (14_level_set.f90:28-29)     */
+    double sigma;                   /* surface tension (14_level_set.f90:30)                   */
+    double alpha1;                  /* Heaviside half-width in cells (14_level_set.f90:25)     */
+    double dt1;                     /* reinitialisation pseudo time step, 0.1*max(dx,dy,dz) (0_modules.f90:198) */
+    int    reinit_maxit;            /* 3 (14_level_set.f90:397)                                */
+    double vol_tol;                 /* volume-correction trigger, 0.1 (14_level_set.f90:257)   */
+    /* Poisson solve (9_grad.f90:175): cg_stop 0 = the reference's test sum(r~^2) > cg_tol/(nx*ny*nz),
+       checked on the residual at the start of the iteration (cg_tol = 1e-4 reproduces it);
+       cg_stop 1 = relative test ||r~||_2 <= cg_tol * ||b~||_2 on the current residual. */
+    int    cg_stop;
+    double cg_tol;
+    int    cg_maxit;                /* 10000 in the reference                                  */
+    int    precision;               /* 0 = plain FP64; 1 = FP32 stencils + FP32 inner CG with FP64 refinement */
+    int    refine_maxit;            /* outer FP64 refinement sweeps for precision 1            */
+    double inner_tol;               /* relative tolerance of each FP32 inner solve             */
+    int    reserved[8];
+} suli_params;
+
+/* ---- field identifiers (module arrays of 0_modules.f90) ------------------------------ */
+enum suli_field {
+    SULI_F_U = 0, SULI_F_V, SULI_F_W,                 /* velpre u,v,w   (0_modules.f90:92-94)  */
+    SULI_F_PRD1, SULI_F_PRD0, SULI_F_PRD,             /* velpre (0_modules.f90:121)          */
+    SULI_F_RHO, SULI_F_LS_NU,                         /* velpre (0_modules.f90:122)          */
+    SULI_F_FU, SULI_F_U0, SULI_F_FU0, SULI_F_FU1,     /* vartempo (0_modules.f90:131)        */
+    SULI_F_FV, SULI_F_V0, SULI_F_FV0, SULI_F_FV1,     /* vartempo (0_modules.f90:132)        */
+    SULI_F_FW, SULI_F_W0, SULI_F_FW0, SULI_F_FW1,     /* vartempo (0_modules.f90:133)        */
+    SULI_F_NUT, SULI_F_XNUT, SULI_F_YNUT, SULI_F_ZNUT,/* smag (0_modules.f90:182-185)        */
+    SULI_F_LS, SULI_F_MOD_LS, SULI_F_KURV, SULI_F_HS, /* ls_param (0_modules.f90:193)        */
+    SULI_F_DDLSDX, SULI_F_DDLSDY, SULI_F_DDLSDZ,
+    SULI_F_HSX, SULI_F_HSY, SULI_F_HSZ,
+    SULI_F_UB, SULI_F_VB, SULI_F_WB,                  /* obst (0_modules.f90:71-73)          */
+    SULI_F_TF_U, SULI_F_TF_V, SULI_F_TF_W,            /* mms_m source terms (0_modules.f90:215-217) */
+    /* prescribed-boundary planes (velpre, 0_modules.f90:96-118) */
+    SULI_F_BXX0, SULI_F_BXX1, SULI_F_BXY0, SULI_F_BXZ0,
+    SULI_F_BXXF, SULI_F_BXXF1, SULI_F_BXYF, SULI_F_BXZF,
+    SULI_F_BYX0, SULI_F_BYY0, SULI_F_BYY1, SULI_F_BYZ0,
+    SULI_F_BYXF, SULI_F_BYYF, SULI_F_BYYF1, SULI_F_BYZF,
+    SULI_F_BZX0, SULI_F_BZY0, SULI_F_BZZ0, SULI_F_BZZ1,
+    SULI_F_BZXF, SULI_F_BZYF, SULI_F_BZZF, SULI_F_BZZF1,
+    SULI_F_COUNT
+};
+
+/* ---- scalar identifiers --------------------------------------------------------------- */
+enum suli_scalar {
+    SULI_S_DT = 0,      /* the global dt, mutated per RK stage (1_principal.f90:78) */
+    SULI_S_VOL_INI,     /* ls_param vol_ini (14_level_set.f90:208-215) */
+    SULI_S_VOL_INS,     /* ls_param vol_ins (14_level_set.f90:246-253) */
+    SULI_S_DT1,         /* ls_param dt1 */
+    SULI_S_T,           /* disc t */
+    SULI_S_NTT,         /* number of RK stages (2_iniciais.f90:85-104) */
+    SULI_S_A_DT1, SULI_S_A_DT2, SULI_S_A_DT3,
+    SULI_S_COUNT
+};
+
+/* Inclusive Fortran index ranges of a field (planes have lo[2] = hi[2] = 0). */
+int suli_field_extent(const suli_params* p, int field, int lo[3], int hi[3]);
+/* The reference's compiled defaults, 0_modules.f90 and 14_level_set.f90:25-31. */
+int suli_params_default(suli_params* p);
+/* sizeof(suli_params) and sizeof(suli_step_stats) as compiled, for binding checks
+   (no counterpart in the reference, which has no foreign-language boundary). */
+int suli_abi_sizes(int* params_bytes, int* stats_bytes);
+
+/* ---- context ---------------------------------------------------------------------------- */
+typedef struct suli_ctx suli_ctx;
+
+/* Allocates every field in HBM of `device` and zeroes it.  Replaces the static module
+   arrays of 0_modules.f90 (the reference's 30M-cell guard, 1_principal.f90:31-34, is lifted). */
+int suli_create(const suli_params* p, int device, suli_ctx** out);
+int suli_destroy(suli_ctx* c);
+const char* suli_last_error(const suli_ctx* c);
+int suli_synchronize(suli_ctx* c);
+
+/* Fortran-layout host copies (c_loc of the module array).  Synchronous. */
+int suli_upload(suli_ctx* c, int field, const double* host);
+int suli_download(suli_ctx* c, int field, double* host);
+int suli_set_scalar(suli_ctx* c, int scalar, double v);
+int suli_get_scalar(suli_ctx* c, int scalar, double* v);
+
+/* iniciais() without the presets: u = u_init, v = w = 0, prd = 0, ub = 0, RK table
+   (2_iniciais.f90:36-46, 85-104).  The level-set preset is written by the caller. */
+int suli_iniciais(suli_ctx* c, double u_init);
+/* heaviside(); vol_ini = sum(hs) dV; mod_ls1() (14_level_set.f90:205-217). */
+int suli_level_set_ini(suli_ctx* c);
+
+/* Hot-path subroutines. */
+int suli_level_set(suli_ctx* c, double* vol_ins);          /* 14_level_set.f90:221-285 */
+int suli_heaviside(suli_ctx* c);                           /* 14_level_set.f90:612-707 */
+int suli_mod_ls1(suli_ctx* c);                             /* 14_level_set.f90:709-805 */
+int suli_visco(suli_ctx* c);                               /* 5_viscosidade.f90:12-219 */
+int suli_convdiff(suli_ctx* c);                            /* 6_convdiff.f90:14-189    */
+int suli_tempo(suli_ctx* c, int tt, int it);               /* 11_diversos.f90:10-230   */
+int suli_contorno(suli_ctx* c, int nlock);                 /* 3_contorno.f90:10-492    */
+int suli_graddin(suli_ctx* c, int* iters, double* resid); /* 9_grad.f90:10-278; resid = ||r~||/||b~|| */
+int suli_posdin(suli_ctx* c);                              /* 10_pos.f90:1-96          */
+int suli_est(suli_ctx* c, double* max_div);                /* 4_plot.f90:500-525 (FP64) */
+int suli_set_dt(suli_ctx* c, double dt);                   /* dt = a_dt(tt), 1_principal.f90:78 */
+
+typedef struct suli_step_stats {
+    int    cg_iters[3];     /* Poisson iterations of each RK stage (inner FP32 iterations for precision 1) */
+    double cg_resid[3];     /* final relative FP64 residual of each stage */
+    double vol_ins;
+    double max_div;         /* max |div u| after the step (FP64) */
+    int    status;
+} suli_step_stats;
+
+/* One time step it (1_principal.f90:64-108 without MMS/plot/restart), plus est(). */
+int suli_step(suli_ctx* c, int it, suli_step_stats* st);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SULI_GPU_H */

@@ -1,0 +1,119 @@
+// ctx.cuh — the solver context: device field arena, scalars, scratch, and the kernel
+// launchers shared by the host API (suli_gpu.cu) and the kernel translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include "../../include/suli_gpu.h"
+#include "geom.cuh"
+
+namespace suli {
+
+// Device-resident state of the Poisson solve (graddin, 9_grad.f90:10-278).  Written by the
+// last block of each reduction kernel; read by the next kernel and, at poll points, by the
+// host through a pinned mirror.
+struct CGState {
+    double rr;        // r~.r~ of the current residual
+    double rr_start;  // r~.r~ at the start of the current iteration (alfamupr)
+    double alpha;
+    double beta;
+    double bb;        // b~.b~ (scaled right-hand side)
+    double thr;       // stopping threshold on r~.r~
+    double pq;        // last p.q
+    int iters;
+    int done;
+    int maxit;
+    int mode;         // suli_params.cg_stop
+    int status;       // 0 ok, SULI_WARN_CG_MAXIT, SULI_ERR_NAN
+    int pad;
+};
+
+// Boundary planes of prescribed walls (velpre, 0_modules.f90:96-118), Fortran layout.
+struct Planes {
+    const double *bxx0, *bxx1, *bxy0, *bxz0, *bxxf, *bxxf1, *bxyf, *bxzf;
+    const double *byx0, *byy0, *byy1, *byz0, *byxf, *byyf, *byyf1, *byzf;
+    const double *bzx0, *bzy0, *bzz0, *bzz1, *bzxf, *bzyf, *bzzf, *bzzf1;
+};
+
+// Deterministic reduction scratch: one slot of per-block partials plus a block counter.
+struct RedSlot {
+    double* partial;       // [max_blocks * 2]
+    unsigned int* counter;
+    double* out;           // [2] results
+};
+
+constexpr int kMaxRedBlocks = 1 << 16;
+
+}  // namespace suli
+
+struct suli_ctx {
+    suli_params P;
+    suli::Geo g;
+    suli::BC bc;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    // one arena for all 3-D fields
+    double* arena = nullptr;
+    size_t arena_elems = 0;
+    double* f[SULI_F_COUNT] = {nullptr};   // 3-D fields in the shared box; planes separate
+    size_t plane_elems[SULI_F_COUNT] = {0};
+    // work arrays (same box)
+    double *ls1 = nullptr, *ls2 = nullptr, *funcs = nullptr;
+    double *nrmx = nullptr, *nrmy = nullptr, *nrmz = nullptr;
+    double *cg_d = nullptr, *cg_e = nullptr, *cg_r = nullptr, *cg_b = nullptr;
+    double *cg_pa = nullptr, *cg_pb = nullptr, *cg_q = nullptr;
+    double *cg_ax = nullptr, *cg_ay = nullptr, *cg_az = nullptr;
+    // reductions
+    double* red_partial = nullptr;
+    unsigned int* red_counter = nullptr;
+    double* red_out = nullptr;
+    suli::CGState* cg = nullptr;        // device
+    suli::CGState* cg_host = nullptr;   // pinned mirror
+    double* host_scalars = nullptr;     // pinned, small
+    // scalars of disc / ls_param
+    double dt = 0, t = 0, dt1 = 0, vol_ini = 0, vol_ins = 0;
+    int ntt = 1;
+    double a_dt[3] = {0, 0, 0};
+    bool tf_active = false;             // tf_u/v/w uploaded non-zero
+    int last_reinit_iters = 0;
+    int last_volfix_iters = 0;
+    int cg_batch = 16;
+    // cached CUDA graphs of CG iteration batches (parity 0: p_old = pa)
+    cudaGraphExec_t cg_graph = nullptr;
+    bool use_graphs = true;
+    suli::Planes planes() const;
+};
+
+inline suli::Planes suli_ctx::planes() const {
+    suli::Planes pl;
+    pl.bxx0 = f[SULI_F_BXX0]; pl.bxx1 = f[SULI_F_BXX1]; pl.bxy0 = f[SULI_F_BXY0]; pl.bxz0 = f[SULI_F_BXZ0];
+    pl.bxxf = f[SULI_F_BXXF]; pl.bxxf1 = f[SULI_F_BXXF1]; pl.bxyf = f[SULI_F_BXYF]; pl.bxzf = f[SULI_F_BXZF];
+    pl.byx0 = f[SULI_F_BYX0]; pl.byy0 = f[SULI_F_BYY0]; pl.byy1 = f[SULI_F_BYY1]; pl.byz0 = f[SULI_F_BYZ0];
+    pl.byxf = f[SULI_F_BYXF]; pl.byyf = f[SULI_F_BYYF]; pl.byyf1 = f[SULI_F_BYYF1]; pl.byzf = f[SULI_F_BYZF];
+    pl.bzx0 = f[SULI_F_BZX0]; pl.bzy0 = f[SULI_F_BZY0]; pl.bzz0 = f[SULI_F_BZZ0]; pl.bzz1 = f[SULI_F_BZZ1];
+    pl.bzxf = f[SULI_F_BZXF]; pl.bzyf = f[SULI_F_BZYF]; pl.bzzf = f[SULI_F_BZZF]; pl.bzzf1 = f[SULI_F_BZZF1];
+    return pl;
+}
+
+namespace suli {
+// ---- kernel launchers (k_fp64.cu) ----
+void launch_lsprops(suli_ctx* c, const double* ls, bool do_mod, bool do_hs, bool do_vol);
+void launch_curv(suli_ctx* c);
+void launch_ls_advect(suli_ctx* c, const double* cur, const double* phi0, double* out,
+                      double a, double b, double gd);
+void launch_reinit_funcs(suli_ctx* c);
+void launch_reinit_stage(suli_ctx* c, const double* cur, const double* phi0, double* out,
+                         double a, double b, double gd);
+void launch_reinit_err(suli_ctx* c, const double* after, const double* before, double band);
+void launch_volfix(suli_ctx* c, double fac);
+void launch_visco(suli_ctx* c);
+void launch_convdiff(suli_ctx* c);
+void launch_tempo(suli_ctx* c, int tt, int it);
+void launch_contorno(suli_ctx* c, int nlock);
+void launch_cg_setup(suli_ctx* c);
+void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new);
+void launch_cg_final(suli_ctx* c);
+void launch_posdin(suli_ctx* c);
+void launch_est(suli_ctx* c);
+void launch_fill(suli_ctx* c, double* a, double v);
+}  // namespace suli

@@ -1,0 +1,1166 @@
+// k_fp64.cu — FP64 kernels of the SuLi-IC hot path for sm_100a.
+//
+// Compiled with -fmad=false: every expression below keeps the reference's order of
+// operations, so results match a contraction-free CPU evaluation bit for bit except where a
+// transcendental (sin/cos in heaviside) or a reduction order differs.  Reductions are
+// deterministic: fixed warp-shuffle trees per block and a fixed-order sum of the block
+// partials done by the last block to finish (no floating-point atomics).
+#include <cuda_runtime.h>
+#include <cmath>
+#include "ctx.cuh"
+#include "weno.cuh"
+
+namespace suli {
+
+#define FIDX(a, i, j, k) (a)[G.idx((i), (j), (k))]
+
+// ------------------------------------------------------------------------------------
+// reductions
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ int flat_tid() {
+    return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+}
+__device__ __forceinline__ int flat_bid() {
+    return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+}
+
+// Sum over the block; the result is valid in thread 0.  Fixed reduction tree.
+__device__ double block_sum(double v) {
+    __shared__ double sh[32];
+    const int tid = flat_tid();
+    const int nt = blockDim.x * blockDim.y * blockDim.z;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((tid & 31) == 0) sh[tid >> 5] = v;
+    __syncthreads();
+    const int nw = (nt + 31) >> 5;
+    v = (tid < nw) ? sh[tid] : 0.0;
+    if (tid < 32) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+__device__ double block_max(double v) {
+    __shared__ double sh[32];
+    const int tid = flat_tid();
+    const int nt = blockDim.x * blockDim.y * blockDim.z;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if ((tid & 31) == 0) sh[tid >> 5] = v;
+    __syncthreads();
+    const int nw = (nt + 31) >> 5;
+    v = (tid < nw) ? sh[tid] : 0.0;
+    if (tid < 32) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+// Two block partials per block; the last block to arrive sums all partials in block order
+// and returns true (totals valid in thread 0 of that block).  `is_max` selects max.
+__device__ bool reduce2_last(double a, double b, double* partial, unsigned int* counter,
+                             double& ta, double& tb, bool is_max = false) {
+    __shared__ bool last;
+    const int tid = flat_tid();
+    const int nt = blockDim.x * blockDim.y * blockDim.z;
+    const int bid = flat_bid();
+    const int nb = gridDim.x * gridDim.y * gridDim.z;
+    a = is_max ? block_max(a) : block_sum(a);
+    b = is_max ? block_max(b) : block_sum(b);
+    if (tid == 0) {
+        partial[2 * bid] = a;
+        partial[2 * bid + 1] = b;
+        __threadfence();
+        const unsigned int t = atomicAdd(counter, 1u);
+        last = (t == (unsigned int)(nb - 1));
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double sa = 0.0, sb = 0.0;
+    for (int q = tid; q < nb; q += nt) {
+        const double pa = __ldcg(&partial[2 * q]), pb = __ldcg(&partial[2 * q + 1]);
+        if (is_max) { sa = fmax(sa, pa); sb = fmax(sb, pb); }
+        else { sa += pa; sb += pb; }
+    }
+    sa = is_max ? block_max(sa) : block_sum(sa);
+    sb = is_max ? block_max(sb) : block_sum(sb);
+    if (tid == 0) { ta = sa; tb = sb; *counter = 0u; }
+    return true;
+}
+
+// ------------------------------------------------------------------------------------
+// small helpers of 8_derivadas.f90
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+// Fortran MAX(x,0.) / MIN(x,0.)
+__device__ __forceinline__ double pmax(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double pmin(double a, double b) { return a < b ? a : b; }
+
+struct Thread3 {
+    int i, j, k;
+};
+__device__ __forceinline__ Thread3 tid3(int i0, int j0, int k0) {
+    Thread3 t;
+    t.i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+    t.j = j0 + blockIdx.y * blockDim.y + threadIdx.y;
+    t.k = k0 + blockIdx.z * blockDim.z + threadIdx.z;
+    return t;
+}
+static inline dim3 grid3(int ni, int nj, int nk, dim3 b) {
+    return dim3((ni + b.x - 1) / b.x, (nj + b.y - 1) / b.y, (nk + b.z - 1) / b.z);
+}
+static const dim3 kBlk(32, 8, 1);
+
+struct Weno3 {
+    double dpx, dnx, dpy, dny, dpz, dnz;
+};
+// der_weno at one cell (14_level_set.f90:343-384) of a cell field f.
+__device__ __forceinline__ Weno3 der_weno_at(const Geo& G, const double* __restrict__ f, int i, int j,
+                                             int k, int ihx, int ihy, int ihz, double dx, double dy,
+                                             double dz) {
+    Weno3 W;
+    double P[7];
+    pencil7<double>([&](int q) { return FIDX(f, q, j, k); }, i, G.nx, ihx, P);
+    weno_pair<double>(P, dx, W.dpx, W.dnx);
+    pencil7<double>([&](int q) { return FIDX(f, i, q, k); }, j, G.ny, ihy, P);
+    weno_pair<double>(P, dy, W.dpy, W.dny);
+    pencil7<double>([&](int q) { return FIDX(f, i, j, q); }, k, G.nz, ihz, P);
+    weno_pair<double>(P, dz, W.dpz, W.dnz);
+    return W;
+}
+__device__ __forceinline__ double larger(double a, double b) { return (fabs(a) > fabs(b)) ? a : b; }
+
+struct LsConst {
+    int ihx, ihy, ihz, ihn;
+    double dx, dy, dz, dx1;
+    double ad;          // alpha1*dx1
+    double pi;
+    double rho1, rho2, mi1, mi2;
+};
+
+// ------------------------------------------------------------------------------------
+// level set: mod_ls1 part A + heaviside + volume (14_level_set.f90:612-722, 743-759)
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_lsprops(Geo G, LsConst L, const double* __restrict__ ls,
+                                                 double* mod_ls, double* nrmx, double* nrmy, double* nrmz,
+                                                 double* hs, double* hsx, double* hsy, double* hsz, double* rho,
+                                                 double* ls_nu, int do_mod, int do_hs, int do_vol,
+                                                 double* partial, unsigned int* counter, double* out) {
+    const Thread3 t = tid3(1, 1, 1);
+    const bool in = (t.i <= G.nx && t.j <= G.ny && t.k <= G.nz);
+    double vol = 0.0;
+    if (in) {
+        const long long c = G.idx(t.i, t.j, t.k);
+        const Weno3 W = der_weno_at(G, ls, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
+        const double a = larger(W.dpx, W.dnx), b = larger(W.dpy, W.dny), cc = larger(W.dpz, W.dnz);
+        if (do_mod) {
+            const double m = sqrt(a * a + b * b + cc * cc);
+            mod_ls[c] = m;
+            if (m == 0) { nrmx[c] = 0.; nrmy[c] = 0.; nrmz[c] = 0.; }
+            else { nrmx[c] = a / m; nrmy[c] = b / m; nrmz[c] = cc / m; }
+        }
+        if (do_hs) {
+            const double l = ls[c];
+            double h;
+            if (l < -L.ad) {
+                h = 0.; hsx[c] = 0.; hsy[c] = 0.; hsz[c] = 0.;
+            } else if (l > L.ad) {
+                h = 1.; hsx[c] = 0.; hsy[c] = 0.; hsz[c] = 0.;
+            } else {
+                h = 0.5 * (1. + l / L.ad + 1. / L.pi * sin(L.pi * l / L.ad));
+                const double cs = cos(L.pi * l / L.ad);
+                hsx[c] = 0.5 * a * (1. + cs) / L.ad;
+                hsy[c] = 0.5 * b * (1. + cs) / L.ad;
+                hsz[c] = 0.5 * cc * (1. + cs) / L.ad;
+            }
+            hs[c] = h;
+            rho[c] = L.rho1 * (1. - h) + L.rho2 * h;
+            ls_nu[c] = L.mi1 * (1. - h) + L.mi2 * h;
+            if (do_vol) vol = (1. - (1. - h)) * L.dx * L.dy * L.dz;
+        }
+    }
+    if (do_vol) {
+        double ta, tb;
+        if (reduce2_last(vol, 0.0, partial, counter, ta, tb) && flat_tid() == 0) out[0] = ta;
+    }
+}
+
+// mod_ls1 part B: curvature from the WENO derivatives of the normal (14_level_set.f90:761-803)
+__global__ void __launch_bounds__(256) k_curv(Geo G, LsConst L, const double* __restrict__ nx_,
+                                              const double* __restrict__ ny_, const double* __restrict__ nz_,
+                                              double* ddx, double* ddy, double* ddz, double* kurv) {
+    const Thread3 t = tid3(1, 1, 1);
+    if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
+    double P[7], dp, dn;
+    pencil7<double>([&](int q) { return FIDX(nx_, q, t.j, t.k); }, t.i, G.nx, L.ihn, P);
+    weno_pair<double>(P, L.dx, dp, dn);
+    const double ax = (fabs(dn) > fabs(dp)) ? dn : dp;
+    pencil7<double>([&](int q) { return FIDX(ny_, t.i, q, t.k); }, t.j, G.ny, L.ihn, P);
+    weno_pair<double>(P, L.dy, dp, dn);
+    const double ay = (fabs(dn) > fabs(dp)) ? dn : dp;
+    pencil7<double>([&](int q) { return FIDX(nz_, t.i, t.j, q); }, t.k, G.nz, L.ihn, P);
+    weno_pair<double>(P, L.dz, dp, dn);
+    const double az = (fabs(dn) > fabs(dp)) ? dn : dp;
+    const long long c = G.idx(t.i, t.j, t.k);
+    ddx[c] = ax; ddy[c] = ay; ddz[c] = az;
+    kurv[c] = ax + ay + az;
+}
+
+// conv_weno + intt_ls: one TVD-RK3 stage of level-set transport (14_level_set.f90:287-341)
+__global__ void __launch_bounds__(256) k_ls_advect(Geo G, LsConst L, const double* __restrict__ cur,
+                                                   const double* phi0, double* out,
+                                                   const double* __restrict__ u, const double* __restrict__ v,
+                                                   const double* __restrict__ w, double a, double b, double gd) {
+    const Thread3 t = tid3(1, 1, 1);
+    if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
+    const int i = t.i, j = t.j, k = t.k;
+    const Weno3 W = der_weno_at(G, cur, i, j, k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
+    const double ua = (FIDX(u, i, j, k) + FIDX(u, i + 1, j, k)) * 0.5;
+    const double va = (FIDX(v, i, j, k) + FIDX(v, i, j + 1, k)) * 0.5;
+    const double wa = (FIDX(w, i, j, k) + FIDX(w, i, j, k + 1)) * 0.5;
+    const double apos = pmax(ua, 0.), aneg = pmin(ua, 0.);
+    const double bpos = pmax(va, 0.), bneg = pmin(va, 0.);
+    const double cpos = pmax(wa, 0.), cneg = pmin(wa, 0.);
+    const double sy7 = -(apos * W.dnx + aneg * W.dpx + bpos * W.dny + bneg * W.dpy + cpos * W.dnz + cneg * W.dpz);
+    const long long c = G.idx(i, j, k);
+    const double p0 = phi0[c];
+    const double gxv = cur[c];
+    out[c] = a * p0 + b * gxv + gd * sy7;
+}
+
+// reinic_weno selection (14_level_set.f90:406-431)
+__device__ __forceinline__ double reinit_mod(double l, const Weno3& W) {
+    const double cst = 0.00000001;
+    double a, b, c;
+    if (l > 0.) {
+        a = pmax(pmax(W.dnx, cst), -pmin(W.dpx, cst));
+        b = pmax(pmax(W.dny, cst), -pmin(W.dpy, cst));
+        c = pmax(pmax(W.dnz, cst), -pmin(W.dpz, cst));
+    } else {
+        a = pmax(pmax(W.dpx, cst), -pmin(W.dnx, cst));
+        b = pmax(pmax(W.dpy, cst), -pmin(W.dny, cst));
+        c = pmax(pmax(W.dpz, cst), -pmin(W.dnz, cst));
+    }
+    return sqrt(a * a + b * b + c * c);
+}
+
+__global__ void __launch_bounds__(256) k_reinit_funcs(Geo G, LsConst L, const double* __restrict__ ls,
+                                                      double* funcs) {
+    const Thread3 t = tid3(1, 1, 1);
+    if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
+    const Weno3 W = der_weno_at(G, ls, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
+    const long long c = G.idx(t.i, t.j, t.k);
+    const double l = ls[c];
+    const double m = reinit_mod(l, W);
+    funcs[c] = l / sqrt(l * l + m * m * L.dx1 * L.dx1);
+}
+
+__global__ void __launch_bounds__(256) k_reinit_stage(Geo G, LsConst L, const double* __restrict__ cur,
+                                                      const double* phi0, double* out,
+                                                      const double* __restrict__ funcs, double a, double b,
+                                                      double gd) {
+    const Thread3 t = tid3(1, 1, 1);
+    if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
+    const Weno3 W = der_weno_at(G, cur, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
+    const long long c = G.idx(t.i, t.j, t.k);
+    const double l = cur[c];
+    const double m = reinit_mod(l, W);
+    const double sy7 = funcs[c] * (1. - m);
+    const double p0 = phi0[c];
+    out[c] = a * p0 + b * l + gd * sy7;
+}
+
+// signed band error of the reinitialisation (14_level_set.f90:492-503): sum and count
+__global__ void __launch_bounds__(256) k_reinit_err(Geo G, const double* __restrict__ after,
+                                                    const double* __restrict__ before, double band,
+                                                    double* partial, unsigned int* counter, double* out) {
+    const Thread3 t = tid3(1, 1, 1);
+    double s = 0.0, n = 0.0;
+    if (t.i <= G.nx && t.j <= G.ny && t.k <= G.nz) {
+        const long long c = G.idx(t.i, t.j, t.k);
+        const double l = after[c];
+        if (fabs(l) <= band) { s = l - before[c]; n = 1.0; }
+    }
+    double ta, tb;
+    if (reduce2_last(s, n, partial, counter, ta, tb) && flat_tid() == 0) { out[0] = ta; out[1] = tb; }
+}
+
+// volume correction step (14_level_set.f90:259-265)
+__global__ void k_volfix(Geo G, double* ls, const double* __restrict__ mod_ls, double dt1fac, double vol_ini) {
+    const Thread3 t = tid3(1, 1, 1);
+    if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
+    const long long c = G.idx(t.i, t.j, t.k);
+    ls[c] = ls[c] - dt1fac * mod_ls[c] / vol_ini;
+}
+
+// ------------------------------------------------------------------------------------
+// visco (5_viscosidade.f90:12-219), m_turb 0 / 1
+// ------------------------------------------------------------------------------------
+struct ViscConst {
+    double dx, dy, dz, cdel, csmag;   // cdel = (dx*dy*dz)**(2/3) computed on the host
+};
+__global__ void __launch_bounds__(256) k_nut(Geo G, ViscConst V, const double* __restrict__ u,
+                                             const double* __restrict__ v, const double* __restrict__ w,
+                                             const double* __restrict__ rho, double* nut) {
+    const Thread3 t = tid3(1, 1, 1);
+    if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
+    const int i = t.i, j = t.j, k = t.k;
+    const double tdx = 2. * V.dx, tdy = 2. * V.dy, tdz = 2. * V.dz;
+    // derivax/y/z of the staggered fields, then interp?_fc to the cell centre
+    const double dudx = ((FIDX(u, i + 1, j, k) - FIDX(u, i - 1, j, k)) / tdx + (FIDX(u, i + 2, j, k) - FIDX(u, i, j, k)) / tdx) * 0.5;
+    const double dudy = ((FIDX(u, i, j + 1, k) - FIDX(u, i, j - 1, k)) / tdy + (FIDX(u, i + 1, j + 1, k) - FIDX(u, i + 1, j - 1, k)) / tdy) * 0.5;
+    const double dudz = ((FIDX(u, i, j, k + 1) - FIDX(u, i, j, k - 1)) / tdz + (FIDX(u, i + 1, j, k + 1) - FIDX(u, i + 1, j, k - 1)) / tdz) * 0.5;
+    const double dvdx = ((FIDX(v, i + 1, j, k) - FIDX(v, i - 1, j, k)) / tdx + (FIDX(v, i + 1, j + 1, k) - FIDX(v, i - 1, j + 1, k)) / tdx) * 0.5;
+    const double dvdy = ((FIDX(v, i, j + 1, k) - FIDX(v, i, j - 1, k)) / tdy + (FIDX(v, i, j + 2, k) - FIDX(v, i, j, k)) / tdy) * 0.5;
+    const double dvdz = ((FIDX(v, i, j, k + 1) - FIDX(v, i, j, k - 1)) / tdz + (FIDX(v, i, j + 1, k + 1) - FIDX(v, i, j + 1, k - 1)) / tdz) * 0.5;
+    const double dwdx = ((FIDX(w, i + 1, j, k) - FIDX(w, i - 1, j, k)) / tdx + (FIDX(w, i + 1, j, k + 1) - FIDX(w, i - 1, j, k + 1)) / tdx) * 0.5;
+    const double dwdy = ((FIDX(w, i, j + 1, k) - FIDX(w, i, j - 1, k)) / tdy + (FIDX(w, i, j + 1, k + 1) - FIDX(w, i, j - 1, k + 1)) / tdy) * 0.5;
+    const double dwdz = ((FIDX(w, i, j, k + 1) - FIDX(w, i, j, k - 1)) / tdz + (FIDX(w, i, j, k + 2) - FIDX(w, i, j, k)) / tdz) * 0.5;
+    const double p1 = dudx + 0.5 * (dudy + dvdx + dudz + dwdx);
+    const double p2 = dvdy + 0.5 * (dvdx + dudy + dvdz + dwdy);
+    const double p3 = dwdz + 0.5 * (dwdy + dvdz + dudz + dwdx);
+    const long long c = G.idx(i, j, k);
+    nut[c] = V.cdel * V.csmag * V.csmag * sqrt(2. * (p1 + p2 + p3) * (p1 + p2 + p3)) * rho[c];
+}
+
+// xnut/ynut/znut = face(ls_nu) + face(nut) with the end-face copy of interp?_cf
+__global__ void __launch_bounds__(256) k_facenu(Geo G, int m_turb, const double* __restrict__ ls_nu,
+                                                const double* __restrict__ nut, double* xnut, double* ynut,
+                                                double* znut) {
+    const Thread3 t = tid3(1, 1, 1);
+    const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
+    if (i > nx + 1 || j > ny + 1 || k > nz + 1) return;
+    if (j <= ny && k <= nz) {
+        const int ic = clampi(i, 2, nx);
+        const double lx = (FIDX(ls_nu, ic, j, k) + FIDX(ls_nu, ic - 1, j, k)) * 0.5;
+        const double xa = m_turb ? (FIDX(nut, ic, j, k) + FIDX(nut, ic - 1, j, k)) * 0.5 : 0.;
+        FIDX(xnut, i, j, k) = lx + xa;
+    }
+    if (i <= nx && k <= nz) {
+        const int jc = clampi(j, 2, ny);
+        const double ly = (FIDX(ls_nu, i, jc, k) + FIDX(ls_nu, i, jc - 1, k)) * 0.5;
+        const double ya = m_turb ? (FIDX(nut, i, jc, k) + FIDX(nut, i, jc - 1, k)) * 0.5 : 0.;
+        FIDX(ynut, i, j, k) = ly + ya;
+    }
+    if (i <= nx && j <= ny) {
+        const int kc = clampi(k, 2, nz);
+        const double lz = (FIDX(ls_nu, i, j, kc) + FIDX(ls_nu, i, j, kc - 1)) * 0.5;
+        const double za = m_turb ? (FIDX(nut, i, j, kc) + FIDX(nut, i, j, kc - 1)) * 0.5 : 0.;
+        FIDX(znut, i, j, k) = lz + za;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// convdiff + classico (6_convdiff.f90:14-189, 7_advectivo.f90:33-113)
+// ------------------------------------------------------------------------------------
+struct CDConst {
+    double dx, dy, dz, gx, gz, sigma, cz;   // cz = gz/(chezy*chezy)
+    int tf;                                  // tf_u/v/w are non-zero
+    int cap_z2, cap_y2, cap_yn;              // planes where ub/vb/wb are captured (3_contorno.f90:247-264)
+};
+struct CDFields {
+    const double *u, *v, *w, *rho, *hsx, *hsy, *hsz, *kurv, *nut, *xnut, *ynut, *znut, *ub, *vb, *wb;
+    const double *tfu, *tfv, *tfw;
+    double *Fu, *Fv, *Fw;
+};
+
+__device__ __forceinline__ bool on_cap(const CDConst& C, int j, int k, int ny) {
+    return (C.cap_z2 && k == 2) || (C.cap_y2 && j == 2) || (C.cap_yn && j == ny);
+}
+
+__global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) {
+    const Thread3 t = tid3(1, 1, 1);
+    const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
+    if (i > nx + 1 || j > ny + 1 || k > nz + 1) return;
+    const double dx = C.dx, dy = C.dy, dz = C.dz;
+    const double* __restrict__ u = F.u;
+    const double* __restrict__ v = F.v;
+    const double* __restrict__ w = F.w;
+    // ---- Fu on u-faces (i = 1..nx+1, j = 1..ny, k = 1..nz)
+    if (j <= ny && k <= nz) {
+        const double uc = FIDX(u, i, j, k);
+        const double bma4 = (FIDX(v, i, j, k) + FIDX(v, i - 1, j, k) + FIDX(v, i, j + 1, k) + FIDX(v, i - 1, j + 1, k)) * 0.25;
+        const double dma4 = (FIDX(w, i, j, k) + FIDX(w, i - 1, j, k) + FIDX(w, i, j, k + 1) + FIDX(w, i - 1, j, k + 1)) * 0.25;
+        double a1 = pmax(uc, 0.), a2 = pmin(uc, 0.);
+        const double dudx = a1 * (uc - FIDX(u, i - 1, j, k)) / dx + a2 * (FIDX(u, i + 1, j, k) - uc) / dx;
+        a1 = pmax(bma4, 0.); a2 = pmin(bma4, 0.);
+        const double dudy = a1 * (uc - FIDX(u, i, j - 1, k)) / dy + a2 * (FIDX(u, i, j + 1, k) - uc) / dy;
+        a1 = pmax(dma4, 0.); a2 = pmin(dma4, 0.);
+        const double dudz = a1 * (uc - FIDX(u, i, j, k - 1)) / dz + a2 * (FIDX(u, i, j, k + 1) - uc) / dz;
+        const double uint_ = dudx + dudy + dudz;
+        const int ic = clampi(i, 2, nx);
+        const double rhox = (FIDX(F.rho, ic, j, k) + FIDX(F.rho, ic - 1, j, k)) * 0.5;
+        const double tx1 = FIDX(F.hsx, ic, j, k) * FIDX(F.kurv, ic, j, k) / FIDX(F.rho, ic, j, k);
+        const double tx0 = FIDX(F.hsx, ic - 1, j, k) * FIDX(F.kurv, ic - 1, j, k) / FIDX(F.rho, ic - 1, j, k);
+        const double dhsdx = (tx1 + tx0) * 0.5;
+        const double ama_i = FIDX(F.nut, clampi(i, 1, nx), j, k) / dx;
+        const double ama_m = FIDX(F.nut, clampi(i - 1, 1, nx), j, k) / dx;
+        const int jp = clampi(j + 1, 2, ny), jm = clampi(j, 2, ny);
+        const double bma_p = ((FIDX(F.xnut, i, jp, k) + FIDX(F.xnut, i, jp - 1, k)) * 0.5) / dy;
+        const double bma_m = ((FIDX(F.xnut, i, jm, k) + FIDX(F.xnut, i, jm - 1, k)) * 0.5) / dy;
+        const int kp = clampi(k + 1, 2, nz), km = clampi(k, 2, nz);
+        const double dma_p = ((FIDX(F.xnut, i, j, kp) + FIDX(F.xnut, i, j, kp - 1)) * 0.5) / dz;
+        const double dma_m = ((FIDX(F.xnut, i, j, km) + FIDX(F.xnut, i, j, km - 1)) * 0.5) / dz;
+        const double Gv = (ama_i * 2. * (FIDX(u, i + 1, j, k) - uc) - ama_m * 2. * (uc - FIDX(u, i - 1, j, k))) / dx +
+                          bma_p * ((FIDX(u, i, j + 1, k) - uc) / dy + (FIDX(v, i, j + 1, k) - FIDX(v, i - 1, j + 1, k)) / dx) -
+                          bma_m * ((uc - FIDX(u, i, j - 1, k)) / dy + (FIDX(v, i, j, k) - FIDX(v, i - 1, j, k)) / dx) +
+                          dma_p * ((FIDX(u, i, j, k + 1) - uc) / dz + (FIDX(w, i, j, k + 1) - FIDX(w, i - 1, j, k + 1)) / dx) -
+                          dma_m * ((uc - FIDX(u, i, j, k - 1)) / dz + (FIDX(w, i, j, k) - FIDX(w, i - 1, j, k)) / dx);
+        double r = -uint_ + Gv / rhox + C.gx - C.sigma * dhsdx;
+        if (C.tf) r = r + FIDX(F.tfu, i, j, k);
+        if (on_cap(C, j, k, ny)) { const double b = FIDX(F.ub, i, j, k); r = r - C.cz * sqrt(b * b) * uc; }
+        FIDX(F.Fu, i, j, k) = r;
+    }
+    // ---- Fv on v-faces (i = 1..nx, j = 1..ny+1, k = 1..nz)
+    if (i <= nx && k <= nz) {
+        const double vc = FIDX(v, i, j, k);
+        const double amb4 = (FIDX(u, i, j, k) + FIDX(u, i + 1, j, k) + FIDX(u, i, j - 1, k) + FIDX(u, i + 1, j - 1, k)) * 0.25;
+        const double dmb4 = (FIDX(w, i, j, k) + FIDX(w, i, j - 1, k) + FIDX(w, i, j, k + 1) + FIDX(w, i, j - 1, k + 1)) * 0.25;
+        double a1 = pmax(amb4, 0.), a2 = pmin(amb4, 0.);
+        const double dvdx = a1 * (vc - FIDX(v, i - 1, j, k)) / dx + a2 * (FIDX(v, i + 1, j, k) - vc) / dx;
+        a1 = pmax(vc, 0.); a2 = pmin(vc, 0.);
+        const double dvdy = a1 * (vc - FIDX(v, i, j - 1, k)) / dy + a2 * (FIDX(v, i, j + 1, k) - vc) / dy;
+        a1 = pmax(dmb4, 0.); a2 = pmin(dmb4, 0.);
+        const double dvdz = a1 * (vc - FIDX(v, i, j, k - 1)) / dz + a2 * (FIDX(v, i, j, k + 1) - vc) / dz;
+        const double vint = dvdx + dvdy + dvdz;
+        const int jc = clampi(j, 2, ny);
+        const double rhoy = (FIDX(F.rho, i, jc, k) + FIDX(F.rho, i, jc - 1, k)) * 0.5;
+        const double ty1 = FIDX(F.hsy, i, jc, k) * FIDX(F.kurv, i, jc, k) / FIDX(F.rho, i, jc, k);
+        const double ty0 = FIDX(F.hsy, i, jc - 1, k) * FIDX(F.kurv, i, jc - 1, k) / FIDX(F.rho, i, jc - 1, k);
+        const double dhsdy = (ty1 + ty0) * 0.5;
+        const int ip = clampi(i + 1, 2, nx), im = clampi(i, 2, nx);
+        const double amb_p = ((FIDX(F.ynut, ip, j, k) + FIDX(F.ynut, ip - 1, j, k)) * 0.5) / dx;
+        const double amb_m = ((FIDX(F.ynut, im, j, k) + FIDX(F.ynut, im - 1, j, k)) * 0.5) / dx;
+        const double bmb_j = FIDX(F.nut, i, clampi(j, 1, ny), k) / dy;
+        const double bmb_m = FIDX(F.nut, i, clampi(j - 1, 1, ny), k) / dy;
+        const int kp = clampi(k + 1, 2, nz), km = clampi(k, 2, nz);
+        const double dmb_p = ((FIDX(F.ynut, i, j, kp) + FIDX(F.ynut, i, j, kp - 1)) * 0.5) / dz;
+        const double dmb_m = ((FIDX(F.ynut, i, j, km) + FIDX(F.ynut, i, j, km - 1)) * 0.5) / dz;
+        const double Gv = amb_p * ((FIDX(v, i + 1, j, k) - vc) / dx + (FIDX(u, i + 1, j, k) - FIDX(u, i + 1, j - 1, k)) / dy) -
+                          amb_m * ((vc - FIDX(v, i - 1, j, k)) / dx + (FIDX(u, i, j, k) - FIDX(u, i, j - 1, k)) / dy) +
+                          (bmb_j * 2. * (FIDX(v, i, j + 1, k) - vc) - bmb_m * 2. * (vc - FIDX(v, i, j - 1, k))) / dy +
+                          dmb_p * ((FIDX(v, i, j, k + 1) - vc) / dz + (FIDX(w, i, j, k + 1) - FIDX(w, i, j - 1, k + 1)) / dy) -
+                          dmb_m * ((vc - FIDX(v, i, j, k - 1)) / dz + (FIDX(w, i, j, k) - FIDX(w, i, j - 1, k)) / dy);
+        double r = -vint + Gv / rhoy - C.sigma * dhsdy;
+        if (C.tf) r = r + FIDX(F.tfv, i, j, k);
+        if (on_cap(C, j, k, ny)) { const double b = FIDX(F.vb, i, j, k); r = r - C.cz * sqrt(b * b) * vc; }
+        FIDX(F.Fv, i, j, k) = r;
+    }
+    // ---- Fw on w-faces (i = 1..nx, j = 1..ny, k = 1..nz+1)
+    if (i <= nx && j <= ny) {
+        const double wc = FIDX(w, i, j, k);
+        const double amd4 = (FIDX(u, i, j, k) + FIDX(u, i + 1, j, k) + FIDX(u, i, j, k - 1) + FIDX(u, i + 1, j, k - 1)) * 0.25;
+        const double bmd4 = (FIDX(v, i, j, k) + FIDX(v, i, j + 1, k) + FIDX(v, i, j, k - 1) + FIDX(v, i, j + 1, k - 1)) * 0.25;
+        double a1 = pmax(amd4, 0.), a2 = pmin(amd4, 0.);
+        const double dwdx = a1 * (wc - FIDX(w, i - 1, j, k)) / dx + a2 * (FIDX(w, i + 1, j, k) - wc) / dx;
+        a1 = pmax(bmd4, 0.); a2 = pmin(bmd4, 0.);
+        const double dwdy = a1 * (wc - FIDX(w, i, j - 1, k)) / dy + a2 * (FIDX(w, i, j + 1, k) - wc) / dy;
+        a1 = pmax(wc, 0.); a2 = pmin(wc, 0.);
+        const double dwdz = a1 * (wc - FIDX(w, i, j, k - 1)) / dz + a2 * (FIDX(w, i, j, k + 1) - wc) / dz;
+        const double wint = dwdx + dwdy + dwdz;
+        const int kc = clampi(k, 2, nz);
+        const double rhoz = (FIDX(F.rho, i, j, kc) + FIDX(F.rho, i, j, kc - 1)) * 0.5;
+        const double tz1 = FIDX(F.hsz, i, j, kc) * FIDX(F.kurv, i, j, kc) / FIDX(F.rho, i, j, kc);
+        const double tz0 = FIDX(F.hsz, i, j, kc - 1) * FIDX(F.kurv, i, j, kc - 1) / FIDX(F.rho, i, j, kc - 1);
+        const double dhsdz = (tz1 + tz0) * 0.5;
+        const int ip = clampi(i + 1, 2, nx), im = clampi(i, 2, nx);
+        const double amd_p = ((FIDX(F.znut, ip, j, k) + FIDX(F.znut, ip - 1, j, k)) * 0.5) / dx;
+        const double amd_m = ((FIDX(F.znut, im, j, k) + FIDX(F.znut, im - 1, j, k)) * 0.5) / dx;
+        const int jp = clampi(j + 1, 2, ny), jm = clampi(j, 2, ny);
+        const double bmd_p = ((FIDX(F.znut, i, jp, k) + FIDX(F.znut, i, jp - 1, k)) * 0.5) / dy;
+        const double bmd_m = ((FIDX(F.znut, i, jm, k) + FIDX(F.znut, i, jm - 1, k)) * 0.5) / dy;
+        const double dmd_k = FIDX(F.nut, i, j, clampi(k, 1, nz)) / dz;
+        const double dmd_m = FIDX(F.nut, i, j, clampi(k - 1, 1, nz)) / dz;
+        const double Gv = amd_p * ((FIDX(w, i + 1, j, k) - wc) / dx + (FIDX(u, i + 1, j, k) - FIDX(u, i + 1, j, k - 1)) / dz) -
+                          amd_m * ((wc - FIDX(w, i - 1, j, k)) / dx + (FIDX(u, i, j, k) - FIDX(u, i, j, k - 1)) / dz) +
+                          bmd_p * ((FIDX(w, i, j + 1, k) - wc) / dy + (FIDX(v, i, j + 1, k) - FIDX(v, i, j + 1, k - 1)) / dz) -
+                          bmd_m * ((wc - FIDX(w, i, j - 1, k)) / dy + (FIDX(v, i, j, k) - FIDX(v, i, j, k - 1)) / dz) +
+                          (dmd_k * 2. * (FIDX(w, i, j, k + 1) - wc) - dmd_m * 2. * (wc - FIDX(w, i, j, k - 1))) / dz;
+        double r = -wint + Gv / rhoz - C.gz - C.sigma * dhsdz;
+        if (C.tf) r = r + FIDX(F.tfw, i, j, k);
+        if (on_cap(C, j, k, ny)) { const double b = FIDX(F.wb, i, j, k); r = r - C.cz * sqrt(b * b) * wc; }
+        FIDX(F.Fw, i, j, k) = r;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// tempo (11_diversos.f90:10-230)
+// ------------------------------------------------------------------------------------
+struct TempoArgs {
+    double* a[3]; const double* F[3]; double* a0[3]; double* f0[3]; double* f1[3];
+    int tm, tt, it;
+    double dt;
+};
+__global__ void __launch_bounds__(256) k_tempo(Geo G, TempoArgs T) {
+    const Thread3 t = tid3(1, 1, 1);
+    const int i = t.i, j = t.j, k = t.k;
+    if (i > G.nx + 1 || j > G.ny + 1 || k > G.nz + 1) return;
+    const bool valid[3] = {j <= G.ny && k <= G.nz, i <= G.nx && k <= G.nz, i <= G.nx && j <= G.ny};
+    const long long c = G.idx(i, j, k);
+    const double dt = T.dt;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        if (!valid[m]) continue;
+        double* A = T.a[m];
+        const double Fv = T.F[m][c];
+        if (T.tm == 0 || (T.tm == 3 && T.it == 1)) {
+            A[c] = A[c] + dt * Fv;
+            if (T.tm == 3) T.f0[m][c] = Fv;
+        } else if (T.tm == 1) {
+            if (T.tt == 1) { const double aux1 = dt; T.a0[m][c] = A[c]; A[c] = A[c] + aux1 * Fv; }
+            else if (T.tt == 2) { const double aux1 = dt; A[c] = T.a0[m][c] + aux1 * Fv; }
+        } else if (T.tm == 2) {
+            if (T.tt == 1) {
+                const double aux1 = dt;
+                T.a0[m][c] = A[c]; T.f0[m][c] = Fv; A[c] = A[c] + aux1 * Fv;
+            } else if (T.tt == 2) {
+                const double aux1 = 2. * dt;
+                T.f1[m][c] = Fv; A[c] = T.a0[m][c] - dt * T.f0[m][c] + aux1 * Fv;
+            } else if (T.tt == 3) {
+                const double aux1 = dt / 6.;
+                A[c] = T.a0[m][c] + aux1 * (T.f0[m][c] + 4. * T.f1[m][c] + Fv);
+            }
+        } else if (T.tm == 3) {
+            A[c] = A[c] + dt * 0.5 * (3 * Fv - T.f0[m][c]);
+            T.f0[m][c] = Fv;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// contorno (3_contorno.f90:10-492), phases in the reference's order.  prd_corr returns
+// zeros (:899-919), so its "+ dpd?" terms vanish.  ccz0 = cczf = 0 is the periodic-z
+// extension mirroring the periodic-x rows.
+// ------------------------------------------------------------------------------------
+struct BCArgs {
+    double *u, *v, *w, *ub, *vb, *wb, *prd1;
+    Planes pl;
+    int nlock;
+};
+// pressure ghosts: composition of the x, y, z copies (:37-54) = value at the mapped index
+__global__ void k_prd_ghosts(Geo G, BC bc, double* prd1) {
+    const Thread3 t = tid3(0, 0, 0);
+    const int i = t.i, j = t.j, k = t.k;
+    if (i > G.nx + 1 || j > G.ny + 1 || k > G.nz + 1) return;
+    const bool gh = (i < 1 || i > G.nx || j < 1 || j > G.ny || k < 1 || k > G.nz);
+    if (!gh) return;
+    const int mi = map_any(i, G.nx, bc.perx), mj = map_any(j, G.ny, bc.pery), mk = map_any(k, G.nz, bc.perz);
+    FIDX(prd1, i, j, k) = FIDX(prd1, mi, mj, mk);
+}
+
+// y walls (:58-114), thread per (i,k)
+__global__ void k_bc_y(Geo G, BC bc, BCArgs A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = G.nx, ny = G.ny, nz = G.nz, ny1 = ny + 1;
+    const bool per = (bc.y0 == 0 && bc.yf == 0);
+    const int lu = nx + 3, lv = nx + 2;   // leading dims of byx*, byy*/byz* planes
+    // u: i in 0..nx+2, k in 0..nz+1
+    if (i <= nx + 2 && k <= nz + 1) {
+        double* u = A.u;
+        if (per) FIDX(u, i, 0, k) = FIDX(u, i, ny, k);
+        if (bc.y0 == 1) FIDX(u, i, 0, k) = FIDX(u, i, 1, k);
+        if (bc.y0 == 2) FIDX(u, i, 0, k) = -FIDX(u, i, 1, k);
+        if (bc.y0 == 3) FIDX(u, i, 0, k) = A.pl.byx0[i + lu * k];
+        if (per) FIDX(u, i, ny + 1, k) = FIDX(u, i, 1, k);
+        if (bc.yf == 1) FIDX(u, i, ny + 1, k) = FIDX(u, i, ny, k);
+        if (bc.yf == 2) FIDX(u, i, ny + 1, k) = -FIDX(u, i, ny, k);
+        if (bc.yf == 3) FIDX(u, i, ny + 1, k) = A.pl.byxf[i + lu * k];
+    }
+    // v: i in 0..nx+1, k in 0..nz+1
+    if (i <= nx + 1 && k <= nz + 1) {
+        double* v = A.v;
+        if (per) { FIDX(v, i, 0, k) = FIDX(v, i, ny1 - 1, k); FIDX(v, i, 1, k) = FIDX(v, i, ny1, k); }
+        if (bc.y0 == 1) FIDX(v, i, 0, k) = -FIDX(v, i, 2, k);
+        if (bc.y0 == 2) FIDX(v, i, 0, k) = FIDX(v, i, 2, k);
+        if (bc.y0 == 3) FIDX(v, i, 0, k) = A.pl.byy0[i + lv * k];
+        if (per) FIDX(v, i, ny1 + 1, k) = FIDX(v, i, 2, k);
+        if (bc.yf == 1) FIDX(v, i, ny1 + 1, k) = -FIDX(v, i, ny1 - 1, k);
+        if (bc.yf == 2) FIDX(v, i, ny1 + 1, k) = FIDX(v, i, ny1 - 1, k);
+        if (bc.yf == 3) FIDX(v, i, ny1 + 1, k) = A.pl.byyf1[i + lv * k];
+    }
+    // w: i in 0..nx+1, k in 0..nz+2
+    if (i <= nx + 1 && k <= nz + 2) {
+        double* w = A.w;
+        if (per) FIDX(w, i, 0, k) = FIDX(w, i, ny, k);
+        if (bc.y0 == 1) FIDX(w, i, 0, k) = FIDX(w, i, 1, k);
+        if (bc.y0 == 2) FIDX(w, i, 0, k) = -FIDX(w, i, 1, k);
+        if (bc.y0 == 3) FIDX(w, i, 0, k) = A.pl.byz0[i + lv * k];
+        if (per) FIDX(w, i, ny + 1, k) = FIDX(w, i, 1, k);
+        if (bc.yf == 1) FIDX(w, i, ny + 1, k) = FIDX(w, i, ny, k);
+        if (bc.yf == 2) FIDX(w, i, ny + 1, k) = -FIDX(w, i, ny, k);
+        if (bc.yf == 3) FIDX(w, i, ny + 1, k) = A.pl.byzf[i + lv * k];
+    }
+}
+
+// x walls (:116-197), thread per (j,k)
+__global__ void k_bc_x(Geo G, BC bc, BCArgs A) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = G.nx, ny = G.ny, nz = G.nz, nx1 = nx + 1;
+    const bool per = (bc.x0 == 0 && bc.xf == 0);
+    const int ly = ny + 2, lyv = ny + 3;   // leading dims of bxx*/bxz* and bxy* planes
+    if (j <= ny + 1 && k <= nz + 1) {   // u
+        double* u = A.u;
+        if (per) FIDX(u, 0, j, k) = FIDX(u, nx1 - 1, j, k);
+        if (bc.x0 == 1) FIDX(u, 0, j, k) = -FIDX(u, 2, j, k);
+        if (bc.x0 == 2) FIDX(u, 0, j, k) = FIDX(u, 2, j, k);
+        if (bc.x0 == 3) FIDX(u, 0, j, k) = A.pl.bxx0[j + ly * k];
+        if (per) FIDX(u, nx1 + 1, j, k) = FIDX(u, 2, j, k);
+        if (bc.xf == 1) FIDX(u, nx1 + 1, j, k) = -FIDX(u, nx1 - 1, j, k);
+        if (bc.xf == 2) FIDX(u, nx1 + 1, j, k) = FIDX(u, nx1 - 1, j, k);
+        if (bc.xf == 3) FIDX(u, nx1 + 1, j, k) = A.pl.bxxf1[j + ly * k];
+        if (bc.xf == 4) FIDX(u, nx1 + 1, j, k) = FIDX(u, nx1, j, k);
+    }
+    if (j <= ny + 2 && k <= nz + 1) {   // v
+        double* v = A.v;
+        if (per) FIDX(v, 0, j, k) = FIDX(v, nx, j, k);
+        if (bc.x0 == 1) FIDX(v, 0, j, k) = FIDX(v, 1, j, k);
+        if (bc.x0 == 2) FIDX(v, 0, j, k) = -FIDX(v, 1, j, k);
+        if (bc.x0 == 3 || bc.x0 == 4) FIDX(v, 0, j, k) = A.pl.bxy0[j + lyv * k];
+        if (per) FIDX(v, nx + 1, j, k) = FIDX(v, 1, j, k);
+        if (bc.xf == 1) FIDX(v, nx + 1, j, k) = FIDX(v, nx, j, k);
+        if (bc.xf == 2) FIDX(v, nx + 1, j, k) = -FIDX(v, nx, j, k);
+        if (bc.xf == 3) FIDX(v, nx + 1, j, k) = A.pl.bxyf[j + lyv * k];
+        if (bc.xf == 4) FIDX(v, nx + 1, j, k) = FIDX(v, nx, j, k);
+    }
+    if (j <= ny + 1 && k <= nz + 2) {   // w
+        double* w = A.w;
+        if (per) FIDX(w, 0, j, k) = FIDX(w, nx, j, k);
+        if (bc.x0 == 1) FIDX(w, 0, j, k) = FIDX(w, 1, j, k);
+        if (bc.x0 == 2) FIDX(w, 0, j, k) = -FIDX(w, 1, j, k);
+        if (bc.x0 == 3) FIDX(w, 0, j, k) = A.pl.bxz0[j + ly * k];
+        if (bc.x0 == 4) FIDX(w, 0, j, k) = FIDX(w, 1, j, k);
+        if (per) FIDX(w, nx + 1, j, k) = FIDX(w, 1, j, k);
+        if (bc.xf == 1) FIDX(w, nx + 1, j, k) = FIDX(w, nx, j, k);
+        if (bc.xf == 2) FIDX(w, nx + 1, j, k) = -FIDX(w, nx, j, k);
+        if (bc.xf == 3) FIDX(w, nx + 1, j, k) = A.pl.bxzf[j + ly * k];
+        if (bc.xf == 4) FIDX(w, nx + 1, j, k) = FIDX(w, nx, j, k);
+    }
+}
+
+// z walls (:199-241) and the wall-friction capture (:247-264), thread per (i,j)
+__global__ void k_bc_z(Geo G, BC bc, BCArgs A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = G.nx, ny = G.ny, nz = G.nz, nz1 = nz + 1;
+    const bool per = (bc.z0 == 0 && bc.zf == 0);
+    const int lu = nx + 3, lv = nx + 2;
+    if (i <= nx + 2 && j <= ny + 1) {   // u
+        double* u = A.u;
+        if (per) FIDX(u, i, j, 0) = FIDX(u, i, j, nz);
+        if (bc.z0 == 1) FIDX(u, i, j, 0) = FIDX(u, i, j, 1);
+        if (bc.z0 == 2) FIDX(u, i, j, 0) = -FIDX(u, i, j, 1);
+        if (bc.z0 == 3) FIDX(u, i, j, 0) = A.pl.bzx0[i + lu * j];
+        if (per) FIDX(u, i, j, nz + 1) = FIDX(u, i, j, 1);
+        if (bc.zf == 1) FIDX(u, i, j, nz + 1) = FIDX(u, i, j, nz);
+        if (bc.zf == 2) FIDX(u, i, j, nz + 1) = -FIDX(u, i, j, nz);
+        if (bc.zf == 3) FIDX(u, i, j, nz + 1) = A.pl.bzxf[i + lu * j];
+    }
+    if (i <= nx + 1 && j <= ny + 2) {   // v
+        double* v = A.v;
+        if (per) FIDX(v, i, j, 0) = FIDX(v, i, j, nz);
+        if (bc.z0 == 1) FIDX(v, i, j, 0) = FIDX(v, i, j, 1);
+        if (bc.z0 == 2) FIDX(v, i, j, 0) = -FIDX(v, i, j, 1);
+        if (bc.z0 == 3) FIDX(v, i, j, 0) = A.pl.bzy0[i + lv * j];
+        if (per) FIDX(v, i, j, nz + 1) = FIDX(v, i, j, 1);
+        if (bc.zf == 1) FIDX(v, i, j, nz + 1) = FIDX(v, i, j, nz);
+        if (bc.zf == 2) FIDX(v, i, j, nz + 1) = -FIDX(v, i, j, nz);
+        if (bc.zf == 3) FIDX(v, i, j, nz + 1) = A.pl.bzyf[i + lv * j];
+    }
+    if (i <= nx + 1 && j <= ny + 1) {   // w
+        double* w = A.w;
+        if (per) FIDX(w, i, j, 0) = FIDX(w, i, j, nz1 - 1);
+        if (bc.z0 == 1) FIDX(w, i, j, 0) = -FIDX(w, i, j, 2);
+        if (bc.z0 == 2) FIDX(w, i, j, 0) = FIDX(w, i, j, 2);
+        if (bc.z0 == 3) FIDX(w, i, j, 0) = A.pl.bzz0[i + lv * j];
+        if (per) FIDX(w, i, j, nz1 + 1) = FIDX(w, i, j, 2);
+        if (bc.zf == 1) FIDX(w, i, j, nz1 + 1) = -FIDX(w, i, j, nz1 - 1);
+        if (bc.zf == 2) FIDX(w, i, j, nz1 + 1) = FIDX(w, i, j, nz1 - 1);
+        if (bc.zf == 3) FIDX(w, i, j, nz1 + 1) = A.pl.bzzf1[i + lv * j];
+    }
+    // capture: each thread copies within its own (i,j) column, after its own z writes
+    if (bc.z0 == 2) {
+        if (i <= nx + 2 && j <= ny + 1) FIDX(A.ub, i, j, 2) = FIDX(A.u, i, j, 2);
+        if (i <= nx + 1 && j <= ny + 2) FIDX(A.vb, i, j, 2) = FIDX(A.v, i, j, 2);
+        if (i <= nx + 1 && j <= ny + 1) FIDX(A.wb, i, j, 2) = FIDX(A.w, i, j, 2);
+    }
+    if (bc.y0 == 2 && j == 2) {
+        if (i <= nx + 2) for (int k = 0; k <= nz + 1; ++k) FIDX(A.ub, i, 2, k) = FIDX(A.u, i, 2, k);
+        if (i <= nx + 1) for (int k = 0; k <= nz + 1; ++k) FIDX(A.vb, i, 2, k) = FIDX(A.v, i, 2, k);
+        if (i <= nx + 1) for (int k = 0; k <= nz + 2; ++k) FIDX(A.wb, i, 2, k) = FIDX(A.w, i, 2, k);
+    }
+    if (bc.yf == 2 && j == ny) {
+        if (i <= nx + 2) for (int k = 0; k <= nz + 1; ++k) FIDX(A.ub, i, ny, k) = FIDX(A.u, i, ny, k);
+        if (i <= nx + 1) for (int k = 0; k <= nz + 1; ++k) FIDX(A.vb, i, ny, k) = FIDX(A.v, i, ny, k);
+        if (i <= nx + 1) for (int k = 0; k <= nz + 2; ++k) FIDX(A.wb, i, ny, k) = FIDX(A.w, i, ny, k);
+    }
+}
+
+// nlock = 2: boundary-normal velocities, y then x then z (:297-441)
+__global__ void k_bc_ny(Geo G, BC bc, BCArgs A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = G.nx, ny = G.ny, nz = G.nz, ny1 = ny + 1, lv = nx + 2;
+    if (i > nx + 1 || k > nz + 1) return;
+    double* v = A.v;
+    const bool per = (bc.y0 == 0 && bc.yf == 0);
+    if (per) FIDX(v, i, 1, k) = FIDX(v, i, ny1, k);
+    if (bc.y0 == 1 || bc.y0 == 2) FIDX(v, i, 1, k) = 0.;
+    if (bc.y0 == 3) FIDX(v, i, 1, k) = A.pl.byy1[i + lv * k];
+    if (per) FIDX(v, i, ny1, k) = FIDX(v, i, 1, k);
+    if (bc.yf == 1 || bc.yf == 2) FIDX(v, i, ny1, k) = 0.;
+    if (bc.yf == 3) FIDX(v, i, ny1, k) = A.pl.byyf[i + lv * k];
+}
+__global__ void k_bc_nx(Geo G, BC bc, BCArgs A) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = G.nx, ny = G.ny, nz = G.nz, nx1 = nx + 1, ly = ny + 2;
+    const bool per = (bc.x0 == 0 && bc.xf == 0);
+    if (j <= ny + 1 && k <= nz + 1) {
+        double* u = A.u;
+        if (per) FIDX(u, 1, j, k) = FIDX(u, nx1, j, k);
+        if (bc.x0 == 1 || bc.x0 == 2) FIDX(u, 1, j, k) = 0.;
+        if (bc.x0 == 3) FIDX(u, 1, j, k) = A.pl.bxx1[j + ly * k];
+        if (per) FIDX(u, nx1, j, k) = FIDX(u, 1, j, k);
+        if (bc.xf == 1) FIDX(u, nx1, j, k) = 0.;
+        if (bc.xf == 2) { FIDX(u, nx1, j, k) = 0.; FIDX(u, nx1 + 1, j, k) = FIDX(u, nx1 - 1, j, k); }
+        if (bc.xf == 3) FIDX(u, nx1, j, k) = A.pl.bxxf[j + ly * k];
+        if (bc.xf == 4) FIDX(u, nx1, j, k) = FIDX(u, nx1 - 1, j, k);
+    }
+    if (bc.xf == 2) {
+        if (j <= ny + 2 && k <= nz + 1) FIDX(A.v, nx + 1, j, k) = -FIDX(A.v, nx, j, k);
+        if (j <= ny + 1 && k <= nz + 2) FIDX(A.w, nx + 1, j, k) = -FIDX(A.w, nx, j, k);
+    }
+}
+__global__ void k_bc_nz(Geo G, BC bc, BCArgs A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = G.nx, ny = G.ny, nz = G.nz, nz1 = nz + 1, lv = nx + 2;
+    if (i > nx + 1 || j > ny + 1) return;
+    double* w = A.w;
+    const bool per = (bc.z0 == 0 && bc.zf == 0);
+    if (per) FIDX(w, i, j, 1) = FIDX(w, i, j, nz1);
+    if (bc.z0 == 1 || bc.z0 == 2) FIDX(w, i, j, 1) = 0.;
+    if (bc.z0 == 3) FIDX(w, i, j, 1) = A.pl.bzz1[i + lv * j];
+    if (per) FIDX(w, i, j, nz1) = FIDX(w, i, j, 1);
+    if (bc.zf == 1 || bc.zf == 2) FIDX(w, i, j, nz1) = 0.;
+    if (bc.zf == 3) FIDX(w, i, j, nz1) = A.pl.bzzf[i + lv * j];
+}
+
+// ------------------------------------------------------------------------------------
+// graddin (9_grad.f90:10-278)
+// ------------------------------------------------------------------------------------
+struct CGConst {
+    double cx, cy, cz;     // dt/(dx*dx) ...
+    double dx, dy, dz;
+    double tol;            // cg_tol
+    double ncell;          // nx*ny*nz
+    int mode, maxit;
+};
+__device__ __forceinline__ double face_s_x(const Geo& G, const double* rho, double cx, int f, int j, int k) {
+    const int fc = clampi(f, 2, G.nx);
+    return cx / ((FIDX(rho, fc, j, k) + FIDX(rho, fc - 1, j, k)) * 0.5);
+}
+__device__ __forceinline__ double face_s_y(const Geo& G, const double* rho, double cy, int i, int f, int k) {
+    const int fc = clampi(f, 2, G.ny);
+    return cy / ((FIDX(rho, i, fc, k) + FIDX(rho, i, fc - 1, k)) * 0.5);
+}
+__device__ __forceinline__ double face_s_z(const Geo& G, const double* rho, double cz, int i, int j, int f) {
+    const int fc = clampi(f, 2, G.nz);
+    return cz / ((FIDX(rho, i, j, fc) + FIDX(rho, i, j, fc - 1)) * 0.5);
+}
+
+// diagonal d, scaled unknown e = prd1*sqrt(d), scaled right-hand side b = q/sqrt(d) (:46-87, :118-124)
+__global__ void __launch_bounds__(256) k_cg_diag(Geo G, CGConst K, const double* __restrict__ rho,
+                                                 const double* __restrict__ u, const double* __restrict__ v,
+                                                 const double* __restrict__ w, const double* __restrict__ prd1,
+                                                 double* d, double* e, double* b) {
+    const Thread3 t = tid3(1, 1, 1);
+    const int i = t.i, j = t.j, k = t.k;
+    if (i > G.nx || j > G.ny || k > G.nz) return;
+    const double dv = face_s_x(G, rho, K.cx, i + 1, j, k) + face_s_x(G, rho, K.cx, i, j, k) +
+                      face_s_y(G, rho, K.cy, i, j + 1, k) + face_s_y(G, rho, K.cy, i, j, k) +
+                      face_s_z(G, rho, K.cz, i, j, k + 1) + face_s_z(G, rho, K.cz, i, j, k);
+    const double q = (FIDX(u, i, j, k) - FIDX(u, i + 1, j, k)) / K.dx + (FIDX(v, i, j, k) - FIDX(v, i, j + 1, k)) / K.dy +
+                     (FIDX(w, i, j, k) - FIDX(w, i, j, k + 1)) / K.dz;
+    const long long c = G.idx(i, j, k);
+    const double sd = sqrt(dv);
+    d[c] = dv;
+    e[c] = prd1[c] * sd;
+    b[c] = q / sd;
+}
+
+// scaled face coefficients and the first residual (:126-151); reduction of r.r and b.b
+__global__ void __launch_bounds__(256) k_cg_coef(Geo G, BC bc, CGConst K, const double* __restrict__ rho,
+                                                 const double* __restrict__ d, const double* __restrict__ e,
+                                                 const double* __restrict__ b, const double* __restrict__ prd1,
+                                                 double* ax, double* ay, double* az, double* r, CGState* st,
+                                                 double* partial, unsigned int* counter) {
+    const Thread3 t = tid3(1, 1, 1);
+    const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
+    double rr = 0.0, bbv = 0.0;
+    if (i <= nx && j <= ny && k <= nz) {
+        const long long c = G.idx(i, j, k);
+        const double dc = d[c];
+        auto dd = [&](int ii, int jj, int kk) {
+            return FIDX(d, map_any(ii, nx, bc.perx), map_any(jj, ny, bc.pery), map_any(kk, nz, bc.perz));
+        };
+        // e at a neighbour: interior value, or the halo value prd1(ghost)*sqrt(d(ghost))
+        auto ee = [&](int ii, int jj, int kk) {
+            if (ii < 1 || ii > nx || jj < 1 || jj > ny || kk < 1 || kk > nz) return FIDX(prd1, ii, jj, kk) * sqrt(dd(ii, jj, kk));
+            return FIDX(e, ii, jj, kk);
+        };
+        const double app = face_s_x(G, rho, K.cx, i + 1, j, k) / sqrt(dc * dd(i + 1, j, k));
+        const double anp = face_s_x(G, rho, K.cx, i, j, k) / sqrt(dc * dd(i - 1, j, k));
+        const double bpp = face_s_y(G, rho, K.cy, i, j + 1, k) / sqrt(dc * dd(i, j + 1, k));
+        const double bnp = face_s_y(G, rho, K.cy, i, j, k) / sqrt(dc * dd(i, j - 1, k));
+        const double cpp = face_s_z(G, rho, K.cz, i, j, k + 1) / sqrt(dc * dd(i, j, k + 1));
+        const double cnp = face_s_z(G, rho, K.cz, i, j, k) / sqrt(dc * dd(i, j, k - 1));
+        ax[c] = anp; ay[c] = bnp; az[c] = cnp;
+        if (i == nx) FIDX(ax, nx + 1, j, k) = app;
+        if (j == ny) FIDX(ay, i, ny + 1, k) = bpp;
+        if (k == nz) FIDX(az, i, j, nz + 1) = cpp;
+        const double bv = b[c];
+        const double rv = e[c] - app * ee(i + 1, j, k) - anp * ee(i - 1, j, k) - bpp * ee(i, j + 1, k) -
+                          bnp * ee(i, j - 1, k) - cpp * ee(i, j, k + 1) - cnp * ee(i, j, k - 1) - bv;
+        r[c] = rv;
+        rr = rv * rv;
+        bbv = bv * bv;
+    }
+    double trr, tbb;
+    if (reduce2_last(rr, bbv, partial, counter, trr, tbb) && flat_tid() == 0) {
+        st->rr = trr;
+        st->rr_start = trr;
+        st->bb = tbb;
+        st->thr = (K.mode == 0) ? K.tol / K.ncell : K.tol * K.tol * tbb;
+        st->alpha = 0.; st->beta = 0.; st->pq = 0.;
+        st->iters = 0;
+        st->maxit = K.maxit;
+        st->mode = K.mode;
+        st->status = 0;
+        const bool go = (fabs(trr) > st->thr) && (K.maxit > 0);
+        st->done = go ? 0 : 1;
+        if (!isfinite(trr)) { st->status = SULI_ERR_NAN; st->done = 1; }
+    }
+}
+
+// CG kernel A: p = r + beta*p_old (also at the neighbours), q = A~p, reduction of p.q (:192-205)
+constexpr int kTX = 32, kTY = 8, kKC = 8;
+__global__ void __launch_bounds__(kTX * kTY) k_cg_spmv(Geo G, BC bc, const double* __restrict__ r,
+                                                       const double* __restrict__ p_old, double* p_new, double* q,
+                                                       const double* __restrict__ ax, const double* __restrict__ ay,
+                                                       const double* __restrict__ az, CGState* st, double* partial,
+                                                       unsigned int* counter) {
+    if (st->done) return;
+    __shared__ double s[kTY + 2][kTX + 2];
+    const double beta = st->beta;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i = blockIdx.x * kTX + tx + 1, j = blockIdx.y * kTY + ty + 1;
+    const int k0 = blockIdx.z * kKC + 1;
+    const int k1 = min(k0 + kKC - 1, nz);
+    const bool in = (i <= nx && j <= ny);
+    auto pn = [&](int ii, int jj, int kk) {
+        const long long c = G.idx(map_any(ii, nx, bc.perx), map_any(jj, ny, bc.pery), map_any(kk, nz, bc.perz));
+        return r[c] + beta * p_old[c];
+    };
+    double pkm1 = 0., pk = 0., azk = 0.;
+    if (in) { pkm1 = pn(i, j, k0 - 1); pk = pn(i, j, k0); azk = FIDX(az, i, j, k0); }
+    double dot = 0.;
+    for (int k = k0; k <= k1; ++k) {
+        double pkp1 = 0., azkp1 = 0.;
+        if (in) {
+            pkp1 = pn(i, j, k + 1);
+            azkp1 = FIDX(az, i, j, k + 1);
+            s[ty + 1][tx + 1] = pk;
+            if (tx == 0) s[ty + 1][0] = pn(i - 1, j, k);
+            if (tx == kTX - 1 || i == nx) s[ty + 1][tx + 2] = pn(i + 1, j, k);
+            if (ty == 0) s[0][tx + 1] = pn(i, j - 1, k);
+            if (ty == kTY - 1 || j == ny) s[ty + 2][tx + 1] = pn(i, j + 1, k);
+        }
+        __syncthreads();
+        if (in) {
+            const long long c = G.idx(i, j, k);
+            const double qv = pk - s[ty + 1][tx + 2] * FIDX(ax, i + 1, j, k) - s[ty + 1][tx] * ax[c] -
+                              s[ty + 2][tx + 1] * FIDX(ay, i, j + 1, k) - s[ty][tx + 1] * ay[c] - pkp1 * azkp1 -
+                              pkm1 * azk;
+            q[c] = qv;
+            p_new[c] = pk;
+            dot += pk * qv;
+        }
+        __syncthreads();
+        pkm1 = pk; pk = pkp1; azk = azkp1;
+    }
+    double tpq, tdum;
+    if (reduce2_last(dot, 0.0, partial, counter, tpq, tdum) && flat_tid() == 0) {
+        st->rr_start = st->rr;
+        st->pq = tpq;
+        st->alpha = st->rr / tpq;
+        if (!isfinite(st->alpha)) { st->status = SULI_ERR_NAN; st->done = 1; }
+    }
+}
+
+// CG kernel B: e -= alpha p, r -= alpha q, reduction of r.r, beta and the stopping test (:210-221, :175)
+__global__ void __launch_bounds__(kTX * kTY) k_cg_update(Geo G, double* e, double* r, const double* __restrict__ p,
+                                                         const double* __restrict__ q, CGState* st, double* partial,
+                                                         unsigned int* counter) {
+    if (st->done) return;
+    const double alpha = st->alpha;
+    const int i = blockIdx.x * kTX + threadIdx.x + 1, j = blockIdx.y * kTY + threadIdx.y + 1;
+    const int k0 = blockIdx.z * kKC + 1;
+    const int k1 = min(k0 + kKC - 1, G.nz);
+    double rr = 0.;
+    if (i <= G.nx && j <= G.ny) {
+        for (int k = k0; k <= k1; ++k) {
+            const long long c = G.idx(i, j, k);
+            e[c] = e[c] - alpha * p[c];
+            const double rv = r[c] - alpha * q[c];
+            r[c] = rv;
+            rr += rv * rv;
+        }
+    }
+    double trr, tdum;
+    if (reduce2_last(rr, 0.0, partial, counter, trr, tdum) && flat_tid() == 0) {
+        const double rr_old = st->rr;
+        st->rr = trr;
+        st->beta = trr / rr_old;
+        st->iters = st->iters + 1;
+        bool go;
+        if (st->mode == 0) go = fabs(st->rr_start) > st->thr;
+        else go = trr > st->thr;
+        if (st->iters >= st->maxit) { go = false; st->status = SULI_WARN_CG_MAXIT; }
+        if (!isfinite(trr)) { go = false; st->status = SULI_ERR_NAN; }
+        st->done = go ? 0 : 1;
+    }
+}
+
+// de-normalisation over the halo box (:268-274)
+__global__ void k_cg_final(Geo G, BC bc, const double* __restrict__ d, const double* __restrict__ e,
+                           double* prd1, const CGState* st) {
+    const Thread3 t = tid3(0, 0, 0);
+    const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
+    if (i > nx + 1 || j > ny + 1 || k > nz + 1) return;
+    const int mi = map_any(i, nx, bc.perx), mj = map_any(j, ny, bc.pery), mk = map_any(k, nz, bc.perz);
+    const bool gh = (mi != i || mj != j || mk != k);
+    const double sd = sqrt(FIDX(d, mi, mj, mk));
+    if (!gh) {
+        FIDX(prd1, i, j, k) = FIDX(e, i, j, k) / sd;
+    } else if (st->iters == 0) {
+        FIDX(prd1, i, j, k) = (FIDX(prd1, i, j, k) * sd) / sd;
+    } else {
+        FIDX(prd1, i, j, k) = FIDX(e, mi, mj, mk) / sd;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// posdin (10_pos.f90:1-96) and est (4_plot.f90:500-525)
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_posdin(Geo G, double aux1, double aux2, double aux3,
+                                                const double* __restrict__ rho, const double* __restrict__ prd1,
+                                                double* u, double* v, double* w) {
+    const Thread3 t = tid3(1, 1, 1);
+    const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
+    if (i > nx + 1 || j > ny + 1 || k > nz + 1) return;
+    if (j <= ny && k <= nz) {
+        const int ic = clampi(i, 2, nx);
+        const double rhox = (FIDX(rho, ic, j, k) + FIDX(rho, ic - 1, j, k)) * 0.5;
+        FIDX(u, i, j, k) = FIDX(u, i, j, k) - aux1 * (FIDX(prd1, i, j, k) - FIDX(prd1, i - 1, j, k)) / rhox;
+    }
+    if (i <= nx && k <= nz) {
+        const int jc = clampi(j, 2, ny);
+        const double rhoy = (FIDX(rho, i, jc, k) + FIDX(rho, i, jc - 1, k)) * 0.5;
+        FIDX(v, i, j, k) = FIDX(v, i, j, k) - aux2 * (FIDX(prd1, i, j, k) - FIDX(prd1, i, j - 1, k)) / rhoy;
+    }
+    if (i <= nx && j <= ny) {
+        const int kc = clampi(k, 2, nz);
+        const double rhoz = (FIDX(rho, i, j, kc) + FIDX(rho, i, j, kc - 1)) * 0.5;
+        FIDX(w, i, j, k) = FIDX(w, i, j, k) - aux3 * (FIDX(prd1, i, j, k) - FIDX(prd1, i, j, k - 1)) / rhoz;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_est(Geo G, double dx, double dy, double dz, const double* __restrict__ u,
+                                             const double* __restrict__ v, const double* __restrict__ w,
+                                             double* partial, unsigned int* counter, double* out) {
+    const Thread3 t = tid3(1, 1, 1);
+    double m = 0.;
+    if (t.i <= G.nx && t.j <= G.ny && t.k <= G.nz) {
+        const int i = t.i, j = t.j, k = t.k;
+        const double dv = (FIDX(u, i + 1, j, k) - FIDX(u, i, j, k)) / dx + (FIDX(v, i, j + 1, k) - FIDX(v, i, j, k)) / dy +
+                          (FIDX(w, i, j, k + 1) - FIDX(w, i, j, k)) / dz;
+        m = fabs(dv);
+        if (isnan(dv)) m = INFINITY;
+    }
+    double ta, tb;
+    if (reduce2_last(m, 0.0, partial, counter, ta, tb, true) && flat_tid() == 0) out[0] = ta;
+}
+
+__global__ void k_fill(double* a, long long n, double v) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) a[q] = v;
+}
+
+// ------------------------------------------------------------------------------------
+// launchers
+// ------------------------------------------------------------------------------------
+static LsConst ls_const(const suli_ctx* c) {
+    LsConst L;
+    L.ihx = (c->P.ccx0 == 0) ? 0 : 2;
+    L.ihy = (c->P.ccy0 == 0) ? 0 : 2;
+    L.ihz = (c->P.ccz0 == 0) ? 0 : 1;
+    L.ihn = L.ihz;   // der_weno leaves ihs at its z value (14_level_set.f90:377, 717)
+    L.dx = c->P.dx; L.dy = c->P.dy; L.dz = c->P.dz;
+    L.dx1 = fmax(L.dx, fmax(L.dy, L.dz));
+    L.ad = c->P.alpha1 * L.dx1;
+    L.pi = acos(-1.0);
+    L.rho1 = c->P.rho_f1; L.rho2 = c->P.rho_f2; L.mi1 = c->P.mi_f1; L.mi2 = c->P.mi_f2;
+    return L;
+}
+static dim3 cells_grid(const Geo& g) { return grid3(g.nx, g.ny, g.nz, kBlk); }
+static dim3 faces_grid(const Geo& g) { return grid3(g.nx + 1, g.ny + 1, g.nz + 1, kBlk); }
+
+void launch_lsprops(suli_ctx* c, const double* ls, bool do_mod, bool do_hs, bool do_vol) {
+    const Geo& G = c->g;
+    k_lsprops<<<cells_grid(G), kBlk, 0, c->stream>>>(
+        G, ls_const(c), ls, c->f[SULI_F_MOD_LS], c->nrmx, c->nrmy, c->nrmz, c->f[SULI_F_HS], c->f[SULI_F_HSX],
+        c->f[SULI_F_HSY], c->f[SULI_F_HSZ], c->f[SULI_F_RHO], c->f[SULI_F_LS_NU], do_mod, do_hs, do_vol,
+        c->red_partial, c->red_counter, c->red_out);
+}
+void launch_curv(suli_ctx* c) {
+    const Geo& G = c->g;
+    k_curv<<<cells_grid(G), kBlk, 0, c->stream>>>(G, ls_const(c), c->nrmx, c->nrmy, c->nrmz, c->f[SULI_F_DDLSDX],
+                                                   c->f[SULI_F_DDLSDY], c->f[SULI_F_DDLSDZ], c->f[SULI_F_KURV]);
+}
+void launch_ls_advect(suli_ctx* c, const double* cur, const double* phi0, double* out, double a, double b, double gd) {
+    const Geo& G = c->g;
+    k_ls_advect<<<cells_grid(G), kBlk, 0, c->stream>>>(G, ls_const(c), cur, phi0, out, c->f[SULI_F_U], c->f[SULI_F_V],
+                                                        c->f[SULI_F_W], a, b, gd);
+}
+void launch_reinit_funcs(suli_ctx* c) {
+    const Geo& G = c->g;
+    k_reinit_funcs<<<cells_grid(G), kBlk, 0, c->stream>>>(G, ls_const(c), c->f[SULI_F_LS], c->funcs);
+}
+void launch_reinit_stage(suli_ctx* c, const double* cur, const double* phi0, double* out, double a, double b, double gd) {
+    const Geo& G = c->g;
+    k_reinit_stage<<<cells_grid(G), kBlk, 0, c->stream>>>(G, ls_const(c), cur, phi0, out, c->funcs, a, b, gd);
+}
+void launch_reinit_err(suli_ctx* c, const double* after, const double* before, double band) {
+    const Geo& G = c->g;
+    k_reinit_err<<<cells_grid(G), kBlk, 0, c->stream>>>(G, after, before, band, c->red_partial, c->red_counter,
+                                                         c->red_out);
+}
+void launch_volfix(suli_ctx* c, double dt1fac) {
+    const Geo& G = c->g;
+    k_volfix<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->f[SULI_F_LS], c->f[SULI_F_MOD_LS], dt1fac, c->vol_ini);
+}
+void launch_visco(suli_ctx* c) {
+    const Geo& G = c->g;
+    if (c->P.m_turb == 1) {
+        ViscConst V;
+        V.dx = c->P.dx; V.dy = c->P.dy; V.dz = c->P.dz; V.csmag = c->P.csmag;
+        V.cdel = pow(c->P.dx * c->P.dy * c->P.dz, 2. / 3.);
+        k_nut<<<cells_grid(G), kBlk, 0, c->stream>>>(G, V, c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W],
+                                                      c->f[SULI_F_RHO], c->f[SULI_F_NUT]);
+    }
+    k_facenu<<<faces_grid(G), kBlk, 0, c->stream>>>(G, c->P.m_turb, c->f[SULI_F_LS_NU], c->f[SULI_F_NUT],
+                                                     c->f[SULI_F_XNUT], c->f[SULI_F_YNUT], c->f[SULI_F_ZNUT]);
+}
+void launch_convdiff(suli_ctx* c) {
+    const Geo& G = c->g;
+    CDConst C;
+    C.dx = c->P.dx; C.dy = c->P.dy; C.dz = c->P.dz; C.gx = c->P.gx; C.gz = c->P.gz; C.sigma = c->P.sigma;
+    C.cz = c->P.gz / (c->P.chezy * c->P.chezy);
+    C.tf = c->tf_active ? 1 : 0;
+    C.cap_z2 = (c->P.ccz0 == 2); C.cap_y2 = (c->P.ccy0 == 2); C.cap_yn = (c->P.ccyf == 2);
+    CDFields F;
+    F.u = c->f[SULI_F_U]; F.v = c->f[SULI_F_V]; F.w = c->f[SULI_F_W]; F.rho = c->f[SULI_F_RHO];
+    F.hsx = c->f[SULI_F_HSX]; F.hsy = c->f[SULI_F_HSY]; F.hsz = c->f[SULI_F_HSZ]; F.kurv = c->f[SULI_F_KURV];
+    F.nut = c->f[SULI_F_NUT]; F.xnut = c->f[SULI_F_XNUT]; F.ynut = c->f[SULI_F_YNUT]; F.znut = c->f[SULI_F_ZNUT];
+    F.ub = c->f[SULI_F_UB]; F.vb = c->f[SULI_F_VB]; F.wb = c->f[SULI_F_WB];
+    F.tfu = c->f[SULI_F_TF_U]; F.tfv = c->f[SULI_F_TF_V]; F.tfw = c->f[SULI_F_TF_W];
+    F.Fu = c->f[SULI_F_FU]; F.Fv = c->f[SULI_F_FV]; F.Fw = c->f[SULI_F_FW];
+    cudaMemcpyAsync(c->f[SULI_F_PRD0], c->f[SULI_F_PRD1], G.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+    k_convdiff<<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F);
+}
+void launch_tempo(suli_ctx* c, int tt, int it) {
+    const Geo& G = c->g;
+    TempoArgs T;
+    T.a[0] = c->f[SULI_F_U]; T.a[1] = c->f[SULI_F_V]; T.a[2] = c->f[SULI_F_W];
+    T.F[0] = c->f[SULI_F_FU]; T.F[1] = c->f[SULI_F_FV]; T.F[2] = c->f[SULI_F_FW];
+    T.a0[0] = c->f[SULI_F_U0]; T.a0[1] = c->f[SULI_F_V0]; T.a0[2] = c->f[SULI_F_W0];
+    T.f0[0] = c->f[SULI_F_FU0]; T.f0[1] = c->f[SULI_F_FV0]; T.f0[2] = c->f[SULI_F_FW0];
+    T.f1[0] = c->f[SULI_F_FU1]; T.f1[1] = c->f[SULI_F_FV1]; T.f1[2] = c->f[SULI_F_FW1];
+    T.tm = c->P.t_tempo; T.tt = tt; T.it = it; T.dt = c->dt;
+    k_tempo<<<faces_grid(G), kBlk, 0, c->stream>>>(G, T);
+}
+void launch_contorno(suli_ctx* c, int nlock) {
+    const Geo& G = c->g;
+    if (nlock != 1 && nlock != 2) return;   // nlock 3 acts only with obstacles
+    BCArgs A;
+    A.u = c->f[SULI_F_U]; A.v = c->f[SULI_F_V]; A.w = c->f[SULI_F_W];
+    A.ub = c->f[SULI_F_UB]; A.vb = c->f[SULI_F_VB]; A.wb = c->f[SULI_F_WB];
+    A.prd1 = c->f[SULI_F_PRD1];
+    A.pl = c->planes();
+    A.nlock = nlock;
+    const dim3 b2(32, 8);
+    k_prd_ghosts<<<grid3(G.nx + 2, G.ny + 2, G.nz + 2, kBlk), kBlk, 0, c->stream>>>(G, c->bc, A.prd1);
+    k_bc_y<<<grid3(G.nx + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
+    k_bc_x<<<grid3(G.ny + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
+    k_bc_z<<<grid3(G.nx + 3, G.ny + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
+    if (nlock == 2) {
+        k_bc_ny<<<grid3(G.nx + 2, G.nz + 2, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
+        k_bc_nx<<<grid3(G.ny + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
+        k_bc_nz<<<grid3(G.nx + 2, G.ny + 2, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
+    }
+}
+static CGConst cg_const(const suli_ctx* c) {
+    CGConst K;
+    K.cx = c->dt / (c->P.dx * c->P.dx);
+    K.cy = c->dt / (c->P.dy * c->P.dy);
+    K.cz = c->dt / (c->P.dz * c->P.dz);
+    K.dx = c->P.dx; K.dy = c->P.dy; K.dz = c->P.dz;
+    K.tol = c->P.cg_tol;
+    K.ncell = (double)(c->P.nx * c->P.ny * c->P.nz);
+    K.mode = c->P.cg_stop;
+    K.maxit = c->P.cg_maxit;
+    return K;
+}
+void launch_cg_setup(suli_ctx* c) {
+    const Geo& G = c->g;
+    const CGConst K = cg_const(c);
+    k_cg_diag<<<cells_grid(G), kBlk, 0, c->stream>>>(G, K, c->f[SULI_F_RHO], c->f[SULI_F_U], c->f[SULI_F_V],
+                                                      c->f[SULI_F_W], c->f[SULI_F_PRD1], c->cg_d, c->cg_e, c->cg_b);
+    k_cg_coef<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->bc, K, c->f[SULI_F_RHO], c->cg_d, c->cg_e, c->cg_b,
+                                                      c->f[SULI_F_PRD1], c->cg_ax, c->cg_ay, c->cg_az, c->cg_r, c->cg,
+                                                      c->red_partial, c->red_counter);
+}
+void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new) {
+    const Geo& G = c->g;
+    const dim3 b(kTX, kTY, 1);
+    const dim3 gr((G.nx + kTX - 1) / kTX, (G.ny + kTY - 1) / kTY, (G.nz + kKC - 1) / kKC);
+    k_cg_spmv<<<gr, b, 0, c->stream>>>(G, c->bc, c->cg_r, p_old, p_new, c->cg_q, c->cg_ax, c->cg_ay, c->cg_az, c->cg,
+                                       c->red_partial, c->red_counter);
+    k_cg_update<<<gr, b, 0, c->stream>>>(G, c->cg_e, c->cg_r, p_new, c->cg_q, c->cg, c->red_partial, c->red_counter);
+}
+void launch_cg_final(suli_ctx* c) {
+    const Geo& G = c->g;
+    k_cg_final<<<grid3(G.nx + 2, G.ny + 2, G.nz + 2, kBlk), kBlk, 0, c->stream>>>(G, c->bc, c->cg_d, c->cg_e,
+                                                                                   c->f[SULI_F_PRD1], c->cg);
+}
+void launch_posdin(suli_ctx* c) {
+    const Geo& G = c->g;
+    const double aux1 = c->dt / c->P.dx, aux2 = c->dt / c->P.dy, aux3 = c->dt / c->P.dz;
+    k_posdin<<<faces_grid(G), kBlk, 0, c->stream>>>(G, aux1, aux2, aux3, c->f[SULI_F_RHO], c->f[SULI_F_PRD1],
+                                                     c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W]);
+    cudaMemcpyAsync(c->f[SULI_F_PRD], c->f[SULI_F_PRD1], G.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+}
+void launch_est(suli_ctx* c) {
+    const Geo& G = c->g;
+    k_est<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->P.dx, c->P.dy, c->P.dz, c->f[SULI_F_U], c->f[SULI_F_V],
+                                                  c->f[SULI_F_W], c->red_partial, c->red_counter, c->red_out);
+}
+void launch_fill(suli_ctx* c, double* a, double v) {
+    const long long n = (long long)c->g.n;
+    k_fill<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(a, n, v);
+}
+
+}  // namespace suli

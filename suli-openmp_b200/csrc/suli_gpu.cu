@@ -1,0 +1,596 @@
+// suli_gpu.cu — host side of the C-ABI declared in include/suli_gpu.h.
+//
+// Owns the solver context (field arena in HBM, stream, reduction scratch) and sequences the
+// kernels of k_fp64.cu in the order of the reference's subroutines.  Data-dependent control
+// flow of the reference (the reinitialisation error loop, the volume-correction loop and the
+// Poisson stopping test) is decided from device-resident scalars; the host reads them back
+// only where the reference branches on them.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "ctx.cuh"
+
+using namespace suli;
+
+namespace {
+
+int fail(suli_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CUDA_TRY(c, expr)                                                                       \
+    do {                                                                                        \
+        cudaError_t e_ = (expr);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return fail((c), SULI_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CHECK_LAUNCH(c)                                                                          \
+    do {                                                                                         \
+        cudaError_t e_ = cudaGetLastError();                                                     \
+        if (e_ != cudaSuccess) return fail((c), SULI_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+bool is_plane(int f) { return f >= SULI_F_BXX0 && f < SULI_F_COUNT; }
+
+// Fortran extents of each module array (0_modules.f90).
+int extent(const suli_params* p, int f, int lo[3], int hi[3]) {
+    const int nx = p->nx, ny = p->ny, nz = p->nz;
+    auto set = [&](int a, int b, int c, int d, int e, int g) {
+        lo[0] = a; hi[0] = b; lo[1] = c; hi[1] = d; lo[2] = e; hi[2] = g;
+        return 0;
+    };
+    switch (f) {
+    case SULI_F_U: case SULI_F_UB: return set(0, nx + 2, 0, ny + 1, 0, nz + 1);
+    case SULI_F_V: case SULI_F_VB: return set(0, nx + 1, 0, ny + 2, 0, nz + 1);
+    case SULI_F_W: case SULI_F_WB: return set(0, nx + 1, 0, ny + 1, 0, nz + 2);
+    case SULI_F_PRD1: case SULI_F_PRD0: case SULI_F_PRD: return set(0, nx + 1, 0, ny + 1, 0, nz + 1);
+    case SULI_F_RHO: case SULI_F_LS_NU: case SULI_F_NUT: case SULI_F_LS: case SULI_F_MOD_LS: case SULI_F_KURV:
+    case SULI_F_HS: case SULI_F_DDLSDX: case SULI_F_DDLSDY: case SULI_F_DDLSDZ: case SULI_F_HSX: case SULI_F_HSY:
+    case SULI_F_HSZ:
+        return set(1, nx, 1, ny, 1, nz);
+    case SULI_F_FU: case SULI_F_U0: case SULI_F_FU0: case SULI_F_FU1: case SULI_F_XNUT: case SULI_F_TF_U:
+        return set(1, nx + 1, 1, ny, 1, nz);
+    case SULI_F_FV: case SULI_F_V0: case SULI_F_FV0: case SULI_F_FV1: case SULI_F_YNUT: case SULI_F_TF_V:
+        return set(1, nx, 1, ny + 1, 1, nz);
+    case SULI_F_FW: case SULI_F_W0: case SULI_F_FW0: case SULI_F_FW1: case SULI_F_ZNUT: case SULI_F_TF_W:
+        return set(1, nx, 1, ny, 1, nz + 1);
+    case SULI_F_BXX0: case SULI_F_BXX1: case SULI_F_BXXF: case SULI_F_BXXF1: return set(0, ny + 1, 0, nz + 1, 0, 0);
+    case SULI_F_BXY0: case SULI_F_BXYF: return set(0, ny + 2, 0, nz + 1, 0, 0);
+    case SULI_F_BXZ0: case SULI_F_BXZF: return set(0, ny + 1, 0, nz + 2, 0, 0);
+    case SULI_F_BYX0: case SULI_F_BYXF: return set(0, nx + 2, 0, nz + 1, 0, 0);
+    case SULI_F_BYY0: case SULI_F_BYY1: case SULI_F_BYYF: case SULI_F_BYYF1: return set(0, nx + 1, 0, nz + 1, 0, 0);
+    case SULI_F_BYZ0: case SULI_F_BYZF: return set(0, nx + 1, 0, nz + 2, 0, 0);
+    case SULI_F_BZX0: case SULI_F_BZXF: return set(0, nx + 2, 0, ny + 1, 0, 0);
+    case SULI_F_BZY0: case SULI_F_BZYF: return set(0, nx + 1, 0, ny + 2, 0, 0);
+    case SULI_F_BZZ0: case SULI_F_BZZ1: case SULI_F_BZZF: case SULI_F_BZZF1: return set(0, nx + 1, 0, ny + 1, 0, 0);
+    default: return SULI_ERR_ARG;
+    }
+}
+
+// Scatter a dense Fortran-layout block into the padded box and back.
+__global__ void k_scatter(Geo G, const double* __restrict__ src, double* dst, int l0, int l1, int l2, int n0, int n1,
+                          int n2) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long tot = (long long)n0 * n1 * n2;
+    if (q >= tot) return;
+    const int a = (int)(q % n0);
+    const int b = (int)((q / n0) % n1);
+    const int cc = (int)(q / ((long long)n0 * n1));
+    dst[G.idx(l0 + a, l1 + b, l2 + cc)] = src[q];
+}
+__global__ void k_gather(Geo G, const double* __restrict__ src, double* dst, int l0, int l1, int l2, int n0, int n1,
+                         int n2) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long tot = (long long)n0 * n1 * n2;
+    if (q >= tot) return;
+    const int a = (int)(q % n0);
+    const int b = (int)((q / n0) % n1);
+    const int cc = (int)(q / ((long long)n0 * n1));
+    dst[q] = src[G.idx(l0 + a, l1 + b, l2 + cc)];
+}
+
+int sync_read(suli_ctx* c, const void* dev, void* host, size_t bytes) {
+    CUDA_TRY(c, cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SULI_OK;
+}
+
+int validate(const suli_params* p, std::string& why) {
+    if (p->nx < 4 || p->ny < 4 || p->nz < 4) { why = "nx, ny, nz must be >= 4 (WENO stencil)"; return SULI_ERR_ARG; }
+    if (!(p->dx > 0 && p->dy > 0 && p->dz > 0)) { why = "dx, dy, dz must be positive"; return SULI_ERR_ARG; }
+    if ((p->ccx0 == 0) != (p->ccxf == 0)) { why = "periodic x needs ccx0 = ccxf = 0 (0_modules.f90:56)"; return SULI_ERR_ARG; }
+    if ((p->ccy0 == 0) != (p->ccyf == 0)) { why = "periodic y needs ccy0 = ccyf = 0"; return SULI_ERR_ARG; }
+    if ((p->ccz0 == 0) != (p->cczf == 0)) { why = "periodic z needs ccz0 = cczf = 0"; return SULI_ERR_ARG; }
+    if (p->ccx0 < 0 || p->ccx0 > 4 || p->ccxf < 0 || p->ccxf > 4) { why = "ccx0/ccxf out of range"; return SULI_ERR_ARG; }
+    if (p->ccy0 < 0 || p->ccy0 > 3 || p->ccyf < 0 || p->ccyf > 3) { why = "ccy0/ccyf out of range"; return SULI_ERR_ARG; }
+    if (p->ccz0 < 0 || p->ccz0 > 3 || p->cczf < 0 || p->cczf > 3) { why = "ccz0/cczf out of range"; return SULI_ERR_ARG; }
+    if (p->obst_t != 0) { why = "obstacles (obst_t != 0) are not built"; return SULI_ERR_UNSUPPORTED; }
+    if (p->t_hs != 0) { why = "t_hs != 0 is not built"; return SULI_ERR_UNSUPPORTED; }
+    if (p->der != 1 || p->adv_type != 1) { why = "only der = 1, adv_type = 1 (classic upwind advection) are built"; return SULI_ERR_UNSUPPORTED; }
+    if (p->m_turb != 0 && p->m_turb != 1) { why = "only m_turb 0 and 1 are built"; return SULI_ERR_UNSUPPORTED; }
+    if (p->t_tempo < 0 || p->t_tempo > 3) { why = "t_tempo out of range"; return SULI_ERR_ARG; }
+    if (p->precision != 0) { why = "precision 1 (mixed) is not built in this library version"; return SULI_ERR_UNSUPPORTED; }
+    if (p->cg_stop != 0 && p->cg_stop != 1) { why = "cg_stop must be 0 or 1"; return SULI_ERR_ARG; }
+    if (p->cg_maxit < 0) { why = "cg_maxit must be >= 0"; return SULI_ERR_ARG; }
+    if (p->reinit_maxit < 1) { why = "reinit_maxit must be >= 1"; return SULI_ERR_ARG; }
+    return SULI_OK;
+}
+
+}  // namespace
+
+
+extern "C" {
+
+int suli_field_extent(const suli_params* p, int field, int lo[3], int hi[3]) {
+    if (!p || !lo || !hi) return SULI_ERR_ARG;
+    return extent(p, field, lo, hi);
+}
+
+int suli_abi_sizes(int* params_bytes, int* stats_bytes) {
+    if (params_bytes) *params_bytes = (int)sizeof(suli_params);
+    if (stats_bytes) *stats_bytes = (int)sizeof(suli_step_stats);
+    return SULI_OK;
+}
+
+int suli_params_default(suli_params* p) {
+    if (!p) return SULI_ERR_ARG;
+    std::memset(p, 0, sizeof(*p));
+    p->dx = p->dy = p->dz = 0.02;
+    p->nx = (int)(.5 / p->dx); p->ny = (int)(1. / p->dy); p->nz = (int)(0.9 / p->dz);
+    p->dt = 0.001;
+    p->ccx0 = p->ccxf = 0; p->ccy0 = p->ccyf = 2; p->ccz0 = 2; p->cczf = 1;
+    p->t_tempo = 1; p->der = 1; p->adv_type = 1; p->m_turb = 0; p->obst_t = 0; p->t_hs = 0;
+    p->csmag = 0.13;
+    const double decliv = 0.0002;
+    p->gx = 9.80665 * std::sin(std::atan(decliv));
+    p->gz = 9.80665 * std::cos(std::atan(decliv));
+    p->chezy = 44.5;
+    p->rho_f1 = 1.204; p->mi_f1 = 0.000018253; p->rho_f2 = 998.0; p->mi_f2 = 0.00100798;
+    p->sigma = 0.0728; p->alpha1 = 1.5;
+    p->dt1 = 0.1 * std::fmax(p->dx, std::fmax(p->dy, p->dz));
+    p->reinit_maxit = 3; p->vol_tol = 0.1;
+    p->cg_stop = 0; p->cg_tol = 0.0001; p->cg_maxit = 10000;
+    p->precision = 0; p->refine_maxit = 20; p->inner_tol = 1e-3;
+    return SULI_OK;
+}
+
+int suli_create(const suli_params* p, int device, suli_ctx** out) {
+    if (!p || !out) return SULI_ERR_ARG;
+    *out = nullptr;
+    std::string why;
+    const int v = validate(p, why);
+    if (v != SULI_OK) { std::fprintf(stderr, "suli_create: %s\n", why.c_str()); return v; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) {
+        cudaGetLastError();
+        std::fprintf(stderr, "suli_create: no CUDA device %d (there is no CPU fallback)\n", device);
+        return SULI_ERR_NODEVICE;
+    }
+    suli_ctx* c = new suli_ctx();
+    c->P = *p;
+    c->device = device;
+    c->g = make_geo(p->nx, p->ny, p->nz);
+    c->bc.x0 = p->ccx0; c->bc.xf = p->ccxf; c->bc.y0 = p->ccy0; c->bc.yf = p->ccyf; c->bc.z0 = p->ccz0; c->bc.zf = p->cczf;
+    c->bc.perx = (p->ccx0 == 0); c->bc.pery = (p->ccy0 == 0); c->bc.perz = (p->ccz0 == 0);
+    auto bail = [&](cudaError_t e, const char* what) {
+        std::fprintf(stderr, "suli_create: %s: %s\n", what, cudaGetErrorString(e));
+        suli_destroy(c);
+        return (e == cudaErrorMemoryAllocation) ? SULI_ERR_NOMEM : SULI_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return bail(e, "cudaSetDevice");
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+    // arena: 40 module fields + 16 work arrays, all in the shared padded box
+    const int n3d = SULI_F_BXX0;
+    const int nwork = 16;
+    const size_t per = (size_t)c->g.n;
+    c->arena_elems = per * (size_t)(n3d + nwork);
+    if ((e = cudaMalloc(&c->arena, c->arena_elems * sizeof(double))) != cudaSuccess) return bail(e, "arena");
+    if ((e = cudaMemsetAsync(c->arena, 0, c->arena_elems * sizeof(double), c->stream)) != cudaSuccess) return bail(e, "memset");
+    for (int f = 0; f < n3d; ++f) c->f[f] = c->arena + per * f;
+    double* wk = c->arena + per * n3d;
+    double** work[16] = {&c->ls1, &c->ls2, &c->funcs, &c->nrmx, &c->nrmy, &c->nrmz, &c->cg_d, &c->cg_e,
+                         &c->cg_r, &c->cg_b, &c->cg_pa, &c->cg_pb, &c->cg_q, &c->cg_ax, &c->cg_ay, &c->cg_az};
+    for (int q = 0; q < nwork; ++q) *work[q] = wk + per * q;
+    for (int f = SULI_F_BXX0; f < SULI_F_COUNT; ++f) {
+        int lo[3], hi[3];
+        extent(p, f, lo, hi);
+        const size_t n = (size_t)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1);
+        c->plane_elems[f] = n;
+        if ((e = cudaMalloc(&c->f[f], n * sizeof(double))) != cudaSuccess) return bail(e, "plane");
+        if ((e = cudaMemsetAsync(c->f[f], 0, n * sizeof(double), c->stream)) != cudaSuccess) return bail(e, "memset");
+    }
+    const long long nb = (long long)((p->nx + 1 + 31) / 32) * ((p->ny + 1 + 7) / 8) * (p->nz + 1) + 64;
+    if ((e = cudaMalloc(&c->red_partial, (size_t)nb * 2 * sizeof(double))) != cudaSuccess) return bail(e, "partial");
+    if ((e = cudaMalloc(&c->red_counter, 64 * sizeof(unsigned int))) != cudaSuccess) return bail(e, "counter");
+    if ((e = cudaMemsetAsync(c->red_counter, 0, 64 * sizeof(unsigned int), c->stream)) != cudaSuccess) return bail(e, "memset");
+    if ((e = cudaMalloc(&c->red_out, 16 * sizeof(double))) != cudaSuccess) return bail(e, "red_out");
+    if ((e = cudaMalloc(&c->cg, sizeof(CGState))) != cudaSuccess) return bail(e, "cg state");
+    if ((e = cudaMemsetAsync(c->cg, 0, sizeof(CGState), c->stream)) != cudaSuccess) return bail(e, "memset");
+    if ((e = cudaMallocHost(&c->cg_host, 2 * sizeof(CGState))) != cudaSuccess) return bail(e, "pinned");
+    if ((e = cudaMallocHost(&c->host_scalars, 16 * sizeof(double))) != cudaSuccess) return bail(e, "pinned");
+    if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bail(e, "sync");
+    c->dt = p->dt;
+    c->dt1 = p->dt1;
+    c->ntt = 1;
+    c->a_dt[0] = c->a_dt[1] = c->a_dt[2] = p->dt;
+    *out = c;
+    return SULI_OK;
+}
+
+int suli_destroy(suli_ctx* c) {
+    if (!c) return SULI_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->cg_graph) cudaGraphExecDestroy(c->cg_graph);
+    cudaFree(c->arena);
+    for (int f = SULI_F_BXX0; f < SULI_F_COUNT; ++f) cudaFree(c->f[f]);
+    cudaFree(c->red_partial);
+    cudaFree(c->red_counter);
+    cudaFree(c->red_out);
+    cudaFree(c->cg);
+    if (c->cg_host) cudaFreeHost(c->cg_host);
+    if (c->host_scalars) cudaFreeHost(c->host_scalars);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return SULI_OK;
+}
+
+const char* suli_last_error(const suli_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int suli_synchronize(suli_ctx* c) {
+    if (!c) return SULI_ERR_ARG;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SULI_OK;
+}
+
+int suli_upload(suli_ctx* c, int field, const double* host) {
+    if (!c || !host || field < 0 || field >= SULI_F_COUNT) return fail(c, SULI_ERR_ARG, "upload: bad field");
+    cudaSetDevice(c->device);
+    int lo[3], hi[3];
+    extent(&c->P, field, lo, hi);
+    const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
+    const size_t n = (size_t)n0 * n1 * n2;
+    if (is_plane(field)) {
+        CUDA_TRY(c, cudaMemcpyAsync(c->f[field], host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        return SULI_OK;
+    }
+    if (field == SULI_F_TF_U || field == SULI_F_TF_V || field == SULI_F_TF_W) {
+        for (size_t q = 0; q < n; ++q)
+            if (host[q] != 0.0) { c->tf_active = true; break; }
+    }
+    // stage through the CG q buffer (same size class as any field, free between calls)
+    double* stage = c->cg_q;
+    CUDA_TRY(c, cudaMemcpyAsync(stage, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    k_scatter<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->g, stage, c->f[field], lo[0], lo[1], lo[2], n0, n1, n2);
+    CHECK_LAUNCH(c);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SULI_OK;
+}
+
+int suli_download(suli_ctx* c, int field, double* host) {
+    if (!c || !host || field < 0 || field >= SULI_F_COUNT) return fail(c, SULI_ERR_ARG, "download: bad field");
+    cudaSetDevice(c->device);
+    int lo[3], hi[3];
+    extent(&c->P, field, lo, hi);
+    const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
+    const size_t n = (size_t)n0 * n1 * n2;
+    if (is_plane(field)) {
+        CUDA_TRY(c, cudaMemcpyAsync(host, c->f[field], n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        return SULI_OK;
+    }
+    double* stage = c->cg_q;
+    k_gather<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->g, c->f[field], stage, lo[0], lo[1], lo[2], n0, n1, n2);
+    CHECK_LAUNCH(c);
+    CUDA_TRY(c, cudaMemcpyAsync(host, stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SULI_OK;
+}
+
+int suli_set_scalar(suli_ctx* c, int id, double v) {
+    if (!c) return SULI_ERR_ARG;
+    switch (id) {
+    case SULI_S_DT: c->dt = v; return SULI_OK;
+    case SULI_S_VOL_INI: c->vol_ini = v; return SULI_OK;
+    case SULI_S_VOL_INS: c->vol_ins = v; return SULI_OK;
+    case SULI_S_DT1: c->dt1 = v; return SULI_OK;
+    case SULI_S_T: c->t = v; return SULI_OK;
+    case SULI_S_NTT: if (v < 1 || v > 3) return fail(c, SULI_ERR_ARG, "ntt must be 1..3"); c->ntt = (int)v; return SULI_OK;
+    case SULI_S_A_DT1: c->a_dt[0] = v; return SULI_OK;
+    case SULI_S_A_DT2: c->a_dt[1] = v; return SULI_OK;
+    case SULI_S_A_DT3: c->a_dt[2] = v; return SULI_OK;
+    default: return fail(c, SULI_ERR_ARG, "set_scalar: bad id");
+    }
+}
+
+int suli_get_scalar(suli_ctx* c, int id, double* v) {
+    if (!c || !v) return SULI_ERR_ARG;
+    switch (id) {
+    case SULI_S_DT: *v = c->dt; return SULI_OK;
+    case SULI_S_VOL_INI: *v = c->vol_ini; return SULI_OK;
+    case SULI_S_VOL_INS: *v = c->vol_ins; return SULI_OK;
+    case SULI_S_DT1: *v = c->dt1; return SULI_OK;
+    case SULI_S_T: *v = c->t; return SULI_OK;
+    case SULI_S_NTT: *v = c->ntt; return SULI_OK;
+    case SULI_S_A_DT1: *v = c->a_dt[0]; return SULI_OK;
+    case SULI_S_A_DT2: *v = c->a_dt[1]; return SULI_OK;
+    case SULI_S_A_DT3: *v = c->a_dt[2]; return SULI_OK;
+    default: return fail(c, SULI_ERR_ARG, "get_scalar: bad id");
+    }
+}
+
+int suli_set_dt(suli_ctx* c, double dt) {
+    if (!c) return SULI_ERR_ARG;
+    c->dt = dt;
+    return SULI_OK;
+}
+
+// iniciais (2_iniciais.f90:36-46 and 85-104), without obstacle/wave/level-set presets
+int suli_iniciais(suli_ctx* c, double u_init) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    c->t = 0.;
+    launch_fill(c, c->f[SULI_F_U], u_init);
+    launch_fill(c, c->f[SULI_F_V], 0.);
+    launch_fill(c, c->f[SULI_F_W], 0.);
+    launch_fill(c, c->f[SULI_F_PRD0], 0.);
+    launch_fill(c, c->f[SULI_F_PRD1], 0.);
+    launch_fill(c, c->f[SULI_F_UB], 0.);
+    launch_fill(c, c->f[SULI_F_VB], 0.);
+    launch_fill(c, c->f[SULI_F_WB], 0.);
+    CHECK_LAUNCH(c);
+    std::vector<double> bx(c->plane_elems[SULI_F_BXX0], u_init);
+    CUDA_TRY(c, cudaMemcpyAsync(c->f[SULI_F_BXX0], bx.data(), bx.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->f[SULI_F_BXX1], bx.data(), bx.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const int tm = c->P.t_tempo;
+    const double dt = c->P.dt;
+    c->dt = dt;
+    if (tm == 0 || tm == 3) { c->ntt = 1; c->a_dt[0] = c->a_dt[1] = c->a_dt[2] = 1.0 * dt; }
+    else if (tm == 1) { c->ntt = 2; c->a_dt[0] = 0.5 * dt; c->a_dt[1] = 1.0 * dt; c->a_dt[2] = 1.0 * dt; }
+    else { c->ntt = 3; c->a_dt[0] = 0.5 * dt; c->a_dt[1] = 1.0 * dt; c->a_dt[2] = 1.0 * dt; }
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SULI_OK;
+}
+
+int suli_heaviside(suli_ctx* c) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    launch_lsprops(c, c->f[SULI_F_LS], false, true, false);
+    CHECK_LAUNCH(c);
+    return SULI_OK;
+}
+
+int suli_mod_ls1(suli_ctx* c) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    launch_lsprops(c, c->f[SULI_F_LS], true, false, false);
+    launch_curv(c);
+    CHECK_LAUNCH(c);
+    return SULI_OK;
+}
+
+int suli_level_set_ini(suli_ctx* c) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    launch_lsprops(c, c->f[SULI_F_LS], true, true, true);
+    launch_curv(c);
+    CHECK_LAUNCH(c);
+    int r = sync_read(c, c->red_out, c->host_scalars, sizeof(double));
+    if (r != SULI_OK) return r;
+    c->vol_ini = c->host_scalars[0];
+    return SULI_OK;
+}
+
+// level_set (14_level_set.f90:221-285)
+int suli_level_set(suli_ctx* c, double* vol_ins) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    const double adtl[3] = {1., 3. / 4., 1. / 3.}, bdtl[3] = {0., 1. / 4., 2. / 3.}, gdtl[3] = {1., 1. / 4., 2. / 3.};
+    double* L0 = c->f[SULI_F_LS];
+    double* L1 = c->ls1;
+    double* L2 = c->ls2;
+    // transport: three TVD-RK3 stages with dt1 := dt (:231-239)
+    const double dta = c->dt;
+    launch_ls_advect(c, L0, L0, L1, adtl[0], bdtl[0], gdtl[0] * dta);
+    launch_ls_advect(c, L1, L0, L2, adtl[1], bdtl[1], gdtl[1] * dta);
+    launch_ls_advect(c, L2, L0, L0, adtl[2], bdtl[2], gdtl[2] * dta);
+    CHECK_LAUNCH(c);
+    // reinitialisation (reinic_weno, :386-509)
+    const double dt1 = c->dt1;
+    const double dx1 = std::fmax(c->P.dx, std::fmax(c->P.dy, c->P.dz));
+    launch_reinit_funcs(c);
+    int il = 0;
+    double error = 999.;
+    while (error > dt1 * dx1 * dx1) {
+        il = il + 1;
+        launch_reinit_stage(c, L0, L0, L1, adtl[0], bdtl[0], gdtl[0] * dt1);
+        launch_reinit_stage(c, L1, L0, L2, adtl[1], bdtl[1], gdtl[1] * dt1);
+        launch_reinit_stage(c, L2, L0, L0, adtl[2], bdtl[2], gdtl[2] * dt1);
+        CHECK_LAUNCH(c);
+        if (il == c->P.reinit_maxit) {
+            error = 0.;
+        } else {
+            launch_reinit_err(c, L0, L2, 2. * c->P.alpha1 * dx1);
+            CHECK_LAUNCH(c);
+            int r = sync_read(c, c->red_out, c->host_scalars, 2 * sizeof(double));
+            if (r != SULI_OK) return r;
+            error = c->host_scalars[0] / c->host_scalars[1];   // nr = 0 gives NaN and ends the loop
+        }
+    }
+    c->last_reinit_iters = il;
+    // mod_ls1 + heaviside + volume (:243-253)
+    launch_lsprops(c, L0, true, true, true);
+    launch_curv(c);
+    CHECK_LAUNCH(c);
+    int r = sync_read(c, c->red_out, c->host_scalars, sizeof(double));
+    if (r != SULI_OK) return r;
+    c->vol_ins = c->host_scalars[0];
+    // volume correction (:257-278); the trailing mod_ls1/heaviside pair (:280-282) recomputes
+    // identical values from an unchanged ls and is skipped.
+    int passes = 0;
+    while (std::fabs(c->vol_ins - c->vol_ini) / c->vol_ins > c->P.vol_tol && passes < 1000) {
+        launch_volfix(c, dt1 * (c->vol_ins - c->vol_ini));
+        launch_lsprops(c, L0, true, true, true);
+        launch_curv(c);
+        CHECK_LAUNCH(c);
+        r = sync_read(c, c->red_out, c->host_scalars, sizeof(double));
+        if (r != SULI_OK) return r;
+        c->vol_ins = c->host_scalars[0];
+        ++passes;
+    }
+    c->last_volfix_iters = passes;
+    if (vol_ins) *vol_ins = c->vol_ins;
+    return SULI_OK;
+}
+
+int suli_visco(suli_ctx* c) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    launch_visco(c);
+    CHECK_LAUNCH(c);
+    return SULI_OK;
+}
+
+int suli_convdiff(suli_ctx* c) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    launch_convdiff(c);
+    CHECK_LAUNCH(c);
+    return SULI_OK;
+}
+
+int suli_tempo(suli_ctx* c, int tt, int it) {
+    if (!c) return SULI_ERR_ARG;
+    if (tt < 1 || tt > 3) return fail(c, SULI_ERR_ARG, "tempo: tt must be 1..3");
+    cudaSetDevice(c->device);
+    launch_tempo(c, tt, it);
+    CHECK_LAUNCH(c);
+    return SULI_OK;
+}
+
+int suli_contorno(suli_ctx* c, int nlock) {
+    if (!c) return SULI_ERR_ARG;
+    if (nlock < 1 || nlock > 3) return fail(c, SULI_ERR_ARG, "contorno: nlock must be 1..3");
+    cudaSetDevice(c->device);
+    launch_contorno(c, nlock);
+    CHECK_LAUNCH(c);
+    return SULI_OK;
+}
+
+// graddin (9_grad.f90:10-278)
+int suli_graddin(suli_ctx* c, int* iters, double* resid) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    launch_cg_setup(c);
+    CHECK_LAUNCH(c);
+    // iteration 1 uses p_old = r with beta = 0 (erroppr = erropr, :172)
+    launch_cg_iter(c, c->cg_r, c->cg_pa);
+    CHECK_LAUNCH(c);
+    long long issued = 1;
+    int parity = 0;   // next p_old: 0 -> pa, 1 -> pb
+    const long long cap = (long long)c->P.cg_maxit + 2;
+    int slot = 0;
+    cudaEvent_t ev[2];
+    cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    bool pending[2] = {false, false};
+    bool finished = false;
+    while (!finished) {
+        // enqueue one batch; kernels after convergence return at once
+        for (int b = 0; b < c->cg_batch && issued < cap; ++b, ++issued) {
+            if (parity == 0) launch_cg_iter(c, c->cg_pa, c->cg_pb);
+            else launch_cg_iter(c, c->cg_pb, c->cg_pa);
+            parity ^= 1;
+        }
+        CHECK_LAUNCH(c);
+        cudaMemcpyAsync(&c->cg_host[slot], c->cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream);
+        cudaEventRecord(ev[slot], c->stream);
+        pending[slot] = true;
+        const int prev = slot ^ 1;
+        if (pending[prev]) {
+            cudaEventSynchronize(ev[prev]);
+            pending[prev] = false;
+            if (c->cg_host[prev].done) finished = true;
+        }
+        if (issued >= cap) {
+            cudaEventSynchronize(ev[slot]);
+            pending[slot] = false;
+            finished = true;
+        }
+        slot = prev;
+    }
+    for (int s = 0; s < 2; ++s) {
+        if (pending[s]) cudaEventSynchronize(ev[s]);
+        cudaEventDestroy(ev[s]);
+    }
+    launch_cg_final(c);
+    CHECK_LAUNCH(c);
+    int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
+    if (r != SULI_OK) return r;
+    const CGState& s = c->cg_host[0];
+    if (iters) *iters = s.iters;
+    if (resid) *resid = (s.bb > 0.) ? std::sqrt(s.rr / s.bb) : 0.;
+    if (s.status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the Poisson solve");
+    return s.status;
+}
+
+int suli_posdin(suli_ctx* c) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    launch_posdin(c);
+    CHECK_LAUNCH(c);
+    return SULI_OK;
+}
+
+int suli_est(suli_ctx* c, double* max_div) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    launch_est(c);
+    CHECK_LAUNCH(c);
+    int r = sync_read(c, c->red_out, c->host_scalars, sizeof(double));
+    if (r != SULI_OK) return r;
+    if (max_div) *max_div = c->host_scalars[0];
+    return SULI_OK;
+}
+
+// one time step (1_principal.f90:64-108, without MMS/plot/restart), then est()
+int suli_step(suli_ctx* c, int it, suli_step_stats* st) {
+    if (!c) return SULI_ERR_ARG;
+    int status = SULI_OK;
+    c->t = it * c->dt;
+    int r = suli_level_set(c, nullptr);
+    if (r < 0) return r;
+    for (int tt = 1; tt <= c->ntt; ++tt) {
+        c->dt = c->a_dt[tt - 1];
+        if ((r = suli_visco(c)) < 0) return r;
+        if ((r = suli_convdiff(c)) < 0) return r;
+        if ((r = suli_tempo(c, tt, it)) < 0) return r;
+        if ((r = suli_contorno(c, 2)) < 0) return r;
+        int n = 0;
+        double res = 0.;
+        r = suli_graddin(c, &n, &res);
+        if (r < 0) return r;
+        if (r > 0) status = r;
+        if (st) { st->cg_iters[tt - 1] = n; st->cg_resid[tt - 1] = res; }
+        if ((r = suli_posdin(c)) < 0) return r;
+        if ((r = suli_contorno(c, 1)) < 0) return r;
+    }
+    double md = 0.;
+    if ((r = suli_est(c, &md)) < 0) return r;
+    if (st) {
+        for (int tt = c->ntt; tt < 3; ++tt) { st->cg_iters[tt] = 0; st->cg_resid[tt] = 0.; }
+        st->vol_ins = c->vol_ins;
+        st->max_div = md;
+        st->status = status;
+    }
+    return status;
+}
+
+}  // extern "C"

@@ -1,0 +1,165 @@
+"""Host-side mirror of the reference's subroutine surface over libsuli_gpu.so.
+
+`Solver` keeps the names and call order of SuLi-IC (1_principal.f90:36-108): a driver
+written against the Fortran program reads the same here —
+
+    s = Solver(params)
+    s.iniciais(u_init); s.upload("ls", ls0); s.level_set_ini()
+    s.contorno(1); s.contorno(3)
+    for it in range(1, ts + 1):
+        s.level_set(); s.contorno(3)
+        for tt in range(1, s.ntt + 1):
+            s.set_dt(s.a_dt[tt - 1])
+            s.visco(); s.convdiff(); s.tempo(tt, it); s.contorno(2)
+            s.graddin(); s.posdin(); s.contorno(1)
+
+or simply `s.step(it)`.  Every call goes through the C-ABI (include/suli_gpu.h); the fields
+stay on the GPU and only the arrays a caller asks for are copied.  A missing library or
+device raises; nothing falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import FIELD, SCALAR, SuliParams, SuliStepStats
+
+
+class SuliError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class Solver:
+    """One solver context (one CUDA stream, all fields resident in HBM)."""
+
+    def __init__(self, params: SuliParams, device: int = 0, lib_path=None):
+        self.lib = _abi.load_library(lib_path)
+        self.params = params.copy()
+        h = C.c_void_p()
+        rc = self.lib.suli_create(C.byref(self.params), int(device), C.byref(h))
+        if rc != 0:
+            raise SuliError(rc, "suli_create failed (see stderr)")
+        self._h = h
+        self.last_status = 0
+
+    # ---------------------------------------------------------------- plumbing
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.suli_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int, what: str) -> int:
+        if rc < 0:
+            msg = self.lib.suli_last_error(self._h)
+            raise SuliError(rc, f"{what}: {msg.decode() if msg else ''}")
+        self.last_status = rc
+        return rc
+
+    def shape(self, name: str):
+        return _abi.field_shape(self.params, name)
+
+    def upload(self, name: str, arr) -> None:
+        a = np.asfortranarray(arr, dtype=np.float64)
+        if a.shape != self.shape(name):
+            a = np.asfortranarray(np.broadcast_to(a, self.shape(name)), dtype=np.float64)
+        ptr = a.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(self.lib.suli_upload(self._h, FIELD[name], ptr), f"upload {name}")
+
+    def download(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape(name), dtype=np.float64, order="F")
+        ptr = out.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(self.lib.suli_download(self._h, FIELD[name], ptr), f"download {name}")
+        return out
+
+    def set_scalar(self, name: str, v: float) -> None:
+        self._check(self.lib.suli_set_scalar(self._h, SCALAR[name], float(v)), f"set {name}")
+
+    def get_scalar(self, name: str) -> float:
+        v = C.c_double()
+        self._check(self.lib.suli_get_scalar(self._h, SCALAR[name], C.byref(v)), f"get {name}")
+        return v.value
+
+    @property
+    def ntt(self) -> int:
+        return int(self.get_scalar("ntt"))
+
+    @property
+    def a_dt(self):
+        return [self.get_scalar("a_dt1"), self.get_scalar("a_dt2"), self.get_scalar("a_dt3")]
+
+    def synchronize(self) -> None:
+        self._check(self.lib.suli_synchronize(self._h), "synchronize")
+
+    # ---------------------------------------------------------------- reference surface
+    def iniciais(self, u_init: float = 0.0) -> None:
+        self._check(self.lib.suli_iniciais(self._h, float(u_init)), "iniciais")
+
+    def level_set_ini(self) -> None:
+        self._check(self.lib.suli_level_set_ini(self._h), "level_set_ini")
+
+    def level_set(self) -> float:
+        v = C.c_double()
+        self._check(self.lib.suli_level_set(self._h, C.byref(v)), "level_set")
+        return v.value
+
+    def heaviside(self) -> None:
+        self._check(self.lib.suli_heaviside(self._h), "heaviside")
+
+    def mod_ls1(self) -> None:
+        self._check(self.lib.suli_mod_ls1(self._h), "mod_ls1")
+
+    def visco(self) -> None:
+        self._check(self.lib.suli_visco(self._h), "visco")
+
+    def convdiff(self) -> None:
+        self._check(self.lib.suli_convdiff(self._h), "convdiff")
+
+    def tempo(self, tt: int, it: int) -> None:
+        self._check(self.lib.suli_tempo(self._h, int(tt), int(it)), "tempo")
+
+    def contorno(self, nlock: int) -> None:
+        self._check(self.lib.suli_contorno(self._h, int(nlock)), "contorno")
+
+    def graddin(self):
+        n = C.c_int()
+        r = C.c_double()
+        self._check(self.lib.suli_graddin(self._h, C.byref(n), C.byref(r)), "graddin")
+        return n.value, r.value
+
+    def posdin(self) -> None:
+        self._check(self.lib.suli_posdin(self._h), "posdin")
+
+    def est(self) -> float:
+        v = C.c_double()
+        self._check(self.lib.suli_est(self._h, C.byref(v)), "est")
+        return v.value
+
+    def set_dt(self, dt: float) -> None:
+        self._check(self.lib.suli_set_dt(self._h, float(dt)), "set_dt")
+
+    def step(self, it: int) -> dict:
+        st = SuliStepStats()
+        self._check(self.lib.suli_step(self._h, int(it), C.byref(st)), "step")
+        return {
+            "cg_iters": list(st.cg_iters),
+            "cg_resid": list(st.cg_resid),
+            "vol_ins": st.vol_ins,
+            "max_div": st.max_div,
+            "status": st.status,
+        }

@@ -1,0 +1,283 @@
+"""GPU parity: every hot-path subroutine of libsuli_gpu.so, called through the C-ABI,
+against the CPU oracle on the same seeded inputs.
+
+Tolerances (FP64 plain path, kernels compiled without FMA contraction):
+  * stencil kernels (visco, convdiff, tempo, contorno, posdin, WENO level-set kernels):
+    max|gpu - cpu| <= 1e-13 * max|cpu| per field; most are bit-identical, the sin/cos of the
+    smoothed Heaviside differ by ulps;
+  * Poisson solve (reductions in a different order, so the CG trajectory differs by rounding):
+    iteration count within 3, projected velocity within 1e-9 and mean-free pressure within
+    1e-8 relative, at a relative residual of 1e-12;
+  * whole steps: <= 1e-10 relative per field after 10 steps (the bar stated for the plain
+    FP64 path).
+"""
+import numpy as np
+import pytest
+
+from helpers import OUT_FIELDS, STATE_FIELDS, load_state, rel_err, seeded_state, small_params
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-13
+BCS = [
+    (2, 2, 2, 2, 2, 1),   # closed tank, free-slip lid (benchmark cases)
+    (0, 0, 2, 2, 2, 1),   # the reference default: periodic x
+    (1, 1, 0, 0, 1, 2),   # free-slip x, periodic y, no-slip lid
+    (2, 4, 1, 1, 2, 1),   # outflow at x = xf
+    (0, 0, 0, 0, 0, 0),   # periodic in all three directions (z periodic is an extension)
+]
+
+
+def layered_ls(p):
+    """A level set varying only in z (the reference's default case, tipo = 1); all water
+    when z is periodic too."""
+    if p.ccz0 == 0:
+        return np.ones((p.nx, p.ny, p.nz))
+    z = (np.arange(1, p.nz + 1) - 0.5) * p.dz
+    return np.broadcast_to(0.5 * p.nz * p.dz - z, (p.nx, p.ny, p.nz)).copy()
+
+
+def pair(pkg, orc, p, seed=0, derived=True, layered=False):
+    g = pkg.Solver(p)
+    o = orc.Oracle(p)
+    st = seeded_state(p, seed)
+    if layered:
+        st["ls"] = layered_ls(p)
+    load_state(o, st)
+    if derived:
+        o.heaviside()
+        o.mod_ls1()
+        o.visco()
+        o.contorno(1)
+        for f in STATE_FIELDS:
+            st[f] = o.download(f)
+    load_state(g, st)
+    return g, o
+
+
+def compare(g, o, fields, tol=TOL, what=""):
+    bad = []
+    for f in fields:
+        e = rel_err(g.download(f), o.download(f))
+        if not e <= tol:
+            bad.append((f, e))
+    assert not bad, f"{what}: fields over tolerance {tol}: {bad}"
+
+
+@pytest.mark.parametrize("bc", BCS)
+def test_heaviside_mod_ls1(pkg, orc, bc):
+    p = small_params(nx=13, ny=11, nz=9, bc=bc)
+    g, o = pair(pkg, orc, p, seed=1, derived=False)
+    for m in (g, o):
+        m.heaviside()
+        m.mod_ls1()
+    compare(g, o, OUT_FIELDS["heaviside"] + OUT_FIELDS["mod_ls1"], what="heaviside/mod_ls1")
+
+
+@pytest.mark.parametrize("m_turb", [0, 1])
+@pytest.mark.parametrize("bc", BCS[:3])
+def test_visco(pkg, orc, bc, m_turb):
+    p = small_params(nx=13, ny=11, nz=9, bc=bc, m_turb=m_turb)
+    g, o = pair(pkg, orc, p, seed=2)
+    for m in (g, o):
+        m.visco()
+    compare(g, o, OUT_FIELDS["visco"], what="visco")
+
+
+@pytest.mark.parametrize("bc", BCS)
+def test_convdiff(pkg, orc, bc):
+    p = small_params(nx=13, ny=11, nz=9, bc=bc)
+    g, o = pair(pkg, orc, p, seed=3)
+    for m in (g, o):
+        m.convdiff()
+    compare(g, o, OUT_FIELDS["convdiff"], what="convdiff")
+
+
+def test_convdiff_with_forcing(pkg, orc):
+    """Manufactured-solution source terms tf_u/v/w (6_convdiff.f90:156,168,183)."""
+    p = small_params(nx=10, ny=9, nz=8)
+    g, o = pair(pkg, orc, p, seed=4)
+    rng = np.random.default_rng(9)
+    for f in ("tf_u", "tf_v", "tf_w"):
+        a = rng.standard_normal(g.shape(f))
+        g.upload(f, a)
+        o.upload(f, a)
+    for m in (g, o):
+        m.convdiff()
+    compare(g, o, OUT_FIELDS["convdiff"], what="convdiff+tf")
+
+
+@pytest.mark.parametrize("t_tempo", [0, 1, 2, 3])
+def test_tempo(pkg, orc, t_tempo):
+    p = small_params(nx=9, ny=8, nz=7, t_tempo=t_tempo)
+    g, o = pair(pkg, orc, p, seed=5)
+    rng = np.random.default_rng(11)
+    for m in (g, o):
+        m.iniciais(0.1)
+    for it in (1, 2):
+        for tt in range(1, {0: 1, 1: 2, 2: 3, 3: 1}[t_tempo] + 1):
+            for f in ("Fu", "Fv", "Fw"):
+                a = rng.standard_normal(g.shape(f))
+                g.upload(f, a)
+                o.upload(f, a)
+            dt = [0.5e-3, 1e-3, 1e-3][tt - 1]
+            for m in (g, o):
+                m.set_dt(dt)
+                m.tempo(tt, it)
+            compare(g, o, OUT_FIELDS["tempo"], tol=0.0, what=f"tempo t_tempo={t_tempo} tt={tt} it={it}")
+
+
+@pytest.mark.parametrize("nlock", [1, 2])
+@pytest.mark.parametrize("bc", BCS + [(3, 3, 3, 3, 3, 3)])
+def test_contorno(pkg, orc, bc, nlock):
+    p = small_params(nx=9, ny=8, nz=7, bc=bc)
+    g, o = pair(pkg, orc, p, seed=6, derived=False)
+    rng = np.random.default_rng(13)
+    if 3 in bc:
+        for f in pkg.FIELD_NAMES[pkg.FIELD["bxx0"]:]:
+            a = rng.standard_normal(g.shape(f))
+            g.upload(f, a)
+            o.upload(f, a)
+    for m in (g, o):
+        m.contorno(nlock)
+    compare(g, o, OUT_FIELDS["contorno"], tol=0.0, what=f"contorno({nlock}) bc={bc}")
+
+
+@pytest.mark.parametrize("bc", BCS[:3])
+def test_posdin_est(pkg, orc, bc):
+    p = small_params(nx=12, ny=10, nz=9, bc=bc)
+    g, o = pair(pkg, orc, p, seed=7)
+    for m in (g, o):
+        m.set_dt(1.3e-3)
+        m.posdin()
+    compare(g, o, OUT_FIELDS["posdin"], what="posdin")
+    assert g.est() == pytest.approx(o.est(), rel=1e-14)
+
+
+@pytest.mark.parametrize("bc", BCS)
+def test_graddin_tight(pkg, orc, bc):
+    """Periodic cases use a density uniform along the periodic axes: with density varying
+    across a periodic boundary the end-face copy of interpx_cf (8_derivadas.f90:318-323)
+    makes the scaled operator non-symmetric and the reference's CG diverges (pinned by
+    test_graddin_periodic_quirk)."""
+    p = small_params(nx=14, ny=12, nz=10, bc=bc)
+    p.cg_stop, p.cg_tol, p.cg_maxit = 1, 1e-12, 20000
+    g, o = pair(pkg, orc, p, seed=8, layered=(0 in bc))
+    res = {}
+    for name, m in (("g", g), ("o", o)):
+        m.set_dt(1e-3)
+        m.contorno(2)
+        res[name] = m.graddin()
+        m.posdin()
+        m.contorno(1)
+    (ng, rg), (no, ro) = res["g"], res["o"]
+    assert abs(ng - no) <= 3, (ng, no)
+    assert rg <= 1e-12 and ro <= 1e-12
+    for f in ("u", "v", "w"):
+        assert rel_err(g.download(f), o.download(f)) <= 1e-9, f
+    pg, po = g.download("prd1"), o.download("prd1")
+    pg, po = pg - pg[1:-1, 1:-1, 1:-1].mean(), po - po[1:-1, 1:-1, 1:-1].mean()
+    assert rel_err(pg, po) <= 1e-8
+    assert g.est() <= 1e-8 * max(1.0, abs(o.est()) * 1e8)
+
+
+def test_graddin_periodic_quirk(pkg, orc):
+    """Density varying across the periodic x boundary: both sides follow the same (diverging)
+    CG trajectory of the reference for the first iterations."""
+    p = small_params(nx=14, ny=12, nz=10, bc=(0, 0, 2, 2, 2, 1))
+    p.cg_stop, p.cg_tol, p.cg_maxit = 1, 1e-12, 12
+    g, o = pair(pkg, orc, p, seed=8)
+    for m in (g, o):
+        m.set_dt(1e-3)
+        m.contorno(2)
+        assert m.graddin()[0] == 12
+    assert rel_err(g.download("prd1"), o.download("prd1")) <= 1e-9
+
+
+def test_graddin_reference_stop(pkg, orc):
+    """The reference's own stopping test: sum(r~^2) > 1e-4/(nx ny nz), checked on the residual
+    at the start of each iteration (9_grad.f90:175)."""
+    p = small_params(nx=14, ny=12, nz=10)
+    p.cg_stop, p.cg_tol, p.cg_maxit = 0, 1e-4, 10000
+    g, o = pair(pkg, orc, p, seed=9)
+    res = {}
+    for name, m in (("g", g), ("o", o)):
+        m.set_dt(1e-3)
+        m.contorno(2)
+        res[name] = m.graddin()
+    assert abs(res["g"][0] - res["o"][0]) <= 1
+    if res["g"][0] == res["o"][0]:
+        assert rel_err(g.download("prd1"), o.download("prd1")) <= 1e-8
+
+
+def test_graddin_zero_iterations_keeps_pressure(pkg, orc):
+    """A divergence-free field with cg_maxit = 0: prd1 is re-normalised, nothing else."""
+    p = small_params(nx=10, ny=9, nz=8)
+    p.cg_maxit = 0
+    g, o = pair(pkg, orc, p, seed=10)
+    for m in (g, o):
+        m.set_dt(1e-3)
+        m.contorno(2)
+        m.graddin()
+    compare(g, o, ["prd1"], tol=0.0, what="graddin 0 iterations")
+
+
+@pytest.mark.parametrize("bc", BCS[:3])
+def test_level_set(pkg, orc, bc):
+    p = small_params(nx=16, ny=12, nz=14, bc=bc)
+    g, o = pair(pkg, orc, p, seed=11)
+    for m in (g, o):
+        m.set_scalar("vol_ini", 0.0)
+    o.level_set_ini()
+    g.level_set_ini()
+    assert g.get_scalar("vol_ini") == pytest.approx(o.get_scalar("vol_ini"), rel=1e-14)
+    for m in (g, o):
+        m.set_dt(2e-3)
+        m.level_set()
+    compare(g, o, OUT_FIELDS["level_set"], tol=1e-12, what="level_set")
+    assert g.get_scalar("vol_ins") == pytest.approx(o.get_scalar("vol_ins"), rel=1e-13)
+
+
+def test_step_parity_dam_break(pkg, orc):
+    """Ten whole steps of a small dam break: every state field within 1e-10 relative."""
+    p, init = pkg.cases.dam_break(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-12)
+    g = pkg.Solver(p)
+    o = orc.Oracle(p)
+    init(g)
+    init(o)
+    for it in range(1, 11):
+        sg, so = g.step(it), o.step(it)
+        assert sg["status"] == 0 and so["status"] == 0
+        assert max(abs(a - b) for a, b in zip(sg["cg_iters"], so["cg_iters"])) <= 3
+    worst = {}
+    for f in ("u", "v", "w", "ls", "rho", "hs", "kurv", "nut"):
+        worst[f] = rel_err(g.download(f), o.download(f))
+    pg, po = g.download("prd1"), o.download("prd1")
+    worst["prd1(mean-free)"] = rel_err(pg - pg.mean(), po - po.mean())
+    assert max(worst.values()) <= 1e-10, worst
+    assert sg["max_div"] <= 1e-8
+
+
+def test_nan_is_reported_not_faulted(pkg, orc):
+    """A NaN in the velocity makes the Poisson reductions return SULI_ERR_NAN."""
+    p = small_params(nx=8, ny=8, nz=8)
+    g, _ = pair(pkg, orc, p, seed=12)
+    u = g.download("u")
+    u[3, 3, 3] = np.nan
+    g.upload("u", u)
+    g.set_dt(1e-3)
+    with pytest.raises(pkg.SuliError) as ei:
+        g.graddin()
+    assert ei.value.code == pkg._abi.ERR_NAN
+    # the context stays usable
+    g.upload("u", np.zeros(g.shape("u")))
+    g.graddin()
+
+
+def test_cg_maxit_warning(pkg, orc):
+    p = small_params(nx=10, ny=9, nz=8)
+    p.cg_stop, p.cg_tol, p.cg_maxit = 1, 1e-14, 5
+    g, _ = pair(pkg, orc, p, seed=13)
+    g.set_dt(1e-3)
+    n, _ = g.graddin()
+    assert n == 5 and g.last_status == pkg._abi.WARN_CG_MAXIT
