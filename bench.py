@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""bench.py — time-steps/s of the SuLi-IC hot path on B200.
+
+Workload (one "step" = one time step of 1_principal.f90:64-108 plus est()): the sloshing
+tank at 256 x 128 x 128 cells (dx = 0.005 m, water/air 1000/1.2, Smagorinsky Cs = 0.1, RK3,
+fixed dt from CFL 0.25), Poisson solves to a relative FP64 residual of 1e-8.  Seeded
+synthetic initial state; the fields (~2.6 GB) exceed the 126 MB L2, so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line (rank 0).  `value` is device-timed (CUDA events on the library's stream,
+max over ranks); `e2e` times the same steps through the C-ABI with the state copied from and
+to pinned host memory every step.  Multi-GPU runs are independent replicas (the path is one
+domain on one GPU), so `value` sums the replicas' time steps over the slowest replica's time.
+The reference arm (--impl reference) times the CPU restatement of the same path (OpenMP, all
+host cores) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import importlib.util
+import io
+import json
+import math
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+PKG_DIR = ROOT / "suli-openmp_b200"
+METRIC = "time-steps/s at 256x128x128, learned+FP32 vs plain FP64 GPU @ resid<=1e-8"
+UNIT = "time-steps/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def load_pkg():
+    if "suli_b200" not in sys.modules:
+        spec = importlib.util.spec_from_file_location("suli_b200", PKG_DIR / "__init__.py",
+                                                      submodule_search_locations=[str(PKG_DIR)])
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["suli_b200"] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules["suli_b200"]
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nx", type=int, default=256)
+    ap.add_argument("--ny", type=int, default=128)
+    ap.add_argument("--nz", type=int, default=128)
+    ap.add_argument("--dx", type=float, default=0.005)
+    ap.add_argument("--cg-tol", type=float, default=1e-8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-cap", type=int, default=20, help="CG iterations per solve in the CPU sample")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------ plumbing
+class Dist:
+    """Rank bookkeeping; replicas only, torch.distributed just for barrier and max."""
+
+    def __init__(self, backend):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            if self.pg.get_backend() == "nccl":
+                import torch
+                self.pg.barrier(device_ids=[self.local])
+            else:
+                self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        dev = f"cuda:{self.local}" if self.pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = vis.split(",")[self.dev] if vis else str(self.dev)
+            self.path = pathlib.Path(os.environ.get("TMPDIR", "/tmp")) / f"suli_clocks_{os.getpid()}.csv"
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", idx, f"--query-gpu={self.Q}", "--format=csv",
+                                          "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = list(csv.reader(io.StringIO(self.path.read_text())))
+        self.path.unlink(missing_ok=True)
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows[1:]:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1].split()[0]))
+                smax.append(float(r[2].split()[0]))
+                power.append(float(r[3].split()[0]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, r[5:9]):
+                if "Active" in val and "Not" not in val:
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+def measured_peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            d = json.loads(f.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(kernel: str, ncell: int):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/), scaled to
+    `ncell` cells when the capture ran on a smaller grid."""
+    f = ROOT / "profiles" / f"{kernel}.txt"
+    if not f.exists():
+        return None
+    vals = {}
+    for line in f.read_text().splitlines():
+        if ":" in line and line.split(":")[0].strip() in ("dram_bytes_per_launch", "cells"):
+            k, v = line.split(":", 1)
+            try:
+                vals[k.strip()] = float(v.split()[0])
+            except ValueError:
+                pass
+    if "dram_bytes_per_launch" not in vals:
+        return None
+    scale = ncell / vals.get("cells", ncell)
+    return vals["dram_bytes_per_launch"] * scale
+
+
+# ------------------------------------------------------------------------------ CPU sample
+def cpu_sample(pkg, p, init, cap: int, full_iters: float | None):
+    """Time one step of the CPU restatement (OpenMP) on the host cores.
+
+    Sample: one full step of everything but the Poisson iterations, with each of the three
+    Poisson solves capped at `cap` iterations, plus two more capped solves to separate the
+    per-iteration cost from the per-solve setup.  The step time is scaled to the full
+    iteration count `full_iters` (the iterations a step of this workload performs)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    q = p.copy()
+    q.cg_maxit = cap
+    o = oracle.Oracle(q, openmp=True)
+    init(o)
+    t0 = time.perf_counter()
+    t_cg = 0.0
+    o.level_set()
+    for tt in range(1, o.ntt + 1):
+        o.set_dt(o.a_dt[tt - 1])
+        o.visco(); o.convdiff(); o.tempo(tt, 1); o.contorno(2)
+        t1 = time.perf_counter()
+        o.graddin()
+        t_cg += time.perf_counter() - t1
+        o.posdin(); o.contorno(1)
+    o.est()
+    t_step_capped = time.perf_counter() - t0
+    t_noncg = t_step_capped - t_cg
+    # per-iteration cost from a cap and a 2*cap solve on the same state
+    o.contorno(2)
+    t1 = time.perf_counter(); o.graddin(); ta = time.perf_counter() - t1
+    q2 = q.copy(); q2.cg_maxit = 2 * cap
+    o2 = oracle.Oracle(q2, openmp=True)
+    for name in ("u", "v", "w", "prd1", "rho", "ls"):
+        o2.upload(name, o.download(name))
+    o2.set_dt(o.a_dt[0]); o2.contorno(2)
+    t1 = time.perf_counter(); o2.graddin(); tb = time.perf_counter() - t1
+    t_iter = max((tb - ta) / cap, 1e-9)
+    t_setup = max(ta - cap * t_iter, 0.0)
+    iters = full_iters if full_iters is not None else 3 * cap
+    t_step = t_noncg + 3 * t_setup + iters * t_iter
+    cores = oracle.num_threads(True)
+    return {
+        "t_step_s": t_step, "t_noncg_s": t_noncg, "t_iter_s": t_iter, "t_setup_s": t_setup,
+        "iters_per_step": iters, "cores": cores, "sample_wall_s": t_step_capped + ta + tb,
+    }
+
+
+# ------------------------------------------------------------------------------ arms
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    pkg = load_pkg()
+    p, init = pkg.cases.sloshing(nx=args.nx, ny=args.ny, nz=args.nz, dx=args.dx, cg_tol=args.cg_tol)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    # the iterations one step needs, from one full CPU step (first warm-up step)
+    o = oracle.Oracle(p, openmp=True)
+    init(o)
+    st = o.step(1)
+    full_iters = float(sum(st["cg_iters"]))
+    del o
+    samples = []
+    for w in range(max(args.warmup - 1, 0)):
+        cpu_sample(pkg, p, init, args.cpu_cap, full_iters)
+    for k in range(args.steps):
+        samples.append(cpu_sample(pkg, p, init, args.cpu_cap, full_iters))
+    t = sum(s["t_step_s"] for s in samples)
+    value = args.steps / t
+    cores = samples[0]["cores"]
+    sample_desc = (f"per step: level set + 3 RK stages of visco/convdiff/tempo/contorno/posdin at full size, "
+                   f"Poisson solves capped at {args.cpu_cap} iterations and scaled to the {full_iters:.0f} "
+                   f"iterations a full CPU step took (FP64, OpenMP restatement)")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": workload_config(p, args, "cpu-openmp-fp64"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample_desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(p, args, path):
+    return {
+        "workload": f"sloshing tank {p.nx}x{p.ny}x{p.nz} dx={p.dx} RK3 Smagorinsky, Poisson rel. residual {p.cg_tol:g}",
+        "nx": p.nx, "ny": p.ny, "nz": p.nz, "dt": p.dt, "cg_tol": p.cg_tol, "path": path,
+        "l2": "state of ~2.6 GB per replica exceeds the 126 MB L2; no flush",
+        "parallelism": f"replicas{args.gpus}",
+    }
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    dist = Dist("nccl")
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    pkg = load_pkg()
+    p, init = pkg.cases.sloshing(nx=args.nx, ny=args.ny, nz=args.nz, dx=args.dx, cg_tol=args.cg_tol)
+    s = pkg.Solver(p, device=dev)
+    init(s)
+    ext = torch.cuda.ExternalStream(s.stream_ptr, device=dev)
+    it = 0
+    for _ in range(args.warmup):
+        it += 1
+        s.step(it)
+    s.synchronize()
+    # ---- timed region: device events on the library's stream, profiling counters on
+    s.profile_enable(True)
+    clocks = ClockSampler(dev)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    stats = []
+    for _ in range(args.steps):
+        it += 1
+        stats.append(s.step(it))
+    e1.record(ext)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    dist.barrier()
+    ms_local = e0.elapsed_time(e1)
+    prof = s.profile_read()
+    s.profile_enable(False)
+    ms = dist.max(ms_local)
+    value = dist.world * args.steps / (ms / 1e3)
+    iters_per_step = prof["cg_iterations"] / args.steps
+    launches = sum(v["launches"] for k, v in prof.items() if isinstance(v, dict))
+    # ---- roofline of the dominant kernel (CG kernel A) and of the whole CG iteration
+    N = p.nx * p.ny * p.nz
+    faces = (p.nx + 1) * p.ny * p.nz + p.nx * (p.ny + 1) * p.nz + p.nx * p.ny * (p.nz + 1)
+    bytes_spmv = 8 * (4 * N + faces)
+    bytes_upd = 8 * 6 * N
+    n_it = max(prof["cg_iterations"], 1)
+    t_spmv = prof["cg_spmv"]["ms"] / n_it / 1e3
+    t_upd = prof["cg_update"]["ms"] / n_it / 1e3
+    peak, peak_kind = measured_peaks()
+    ach = bytes_spmv / t_spmv / 1e9
+    traffic = profiled_traffic("cg_spmv_256x128x128", N)
+    roofline = {
+        "kernel": "k_cg_spmv (CG kernel A: p = r + beta p, q = A p, p.q)",
+        "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
+        "traffic": traffic, "algorithmic_bytes_per_launch": bytes_spmv, "avg_launch_us": t_spmv * 1e6,
+        "cg_iteration": {"kernels": "k_cg_spmv + k_cg_update", "bytes": bytes_spmv + bytes_upd,
+                         "us": (t_spmv + t_upd) * 1e6,
+                         "achieved_gbs": (bytes_spmv + bytes_upd) / (t_spmv + t_upd) / 1e9,
+                         "frac": (bytes_spmv + bytes_upd) / (t_spmv + t_upd) / 1e9 / peak},
+    }
+    kernels = {k: {"ms_per_step": v["ms"] / args.steps, "launches_per_step": v["launches"] / args.steps}
+               for k, v in prof.items() if isinstance(v, dict)}
+    # ---- end to end through the C-ABI: pinned host state in and out every step
+    e2e = None
+    if not args.no_e2e:
+        names = ["u", "v", "w", "prd1", "ls"]
+        pinned = {}
+        for nm in names:
+            shape = s.shape(nm)
+            t = torch.empty(int(np.prod(shape)), dtype=torch.float64, pin_memory=True)
+            a = t.numpy().reshape(shape, order="F")
+            s.download(nm, out=a)
+            pinned[nm] = (t, a)
+        h2d = sum(a.nbytes for _, a in pinned.values())
+        s.synchronize()
+        dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            it += 1
+            for nm in names:
+                s.upload(nm, pinned[nm][1])
+            s.step(it)
+            for nm in names:
+                s.download(nm, out=pinned[nm][1])
+        s.synchronize()
+        t_e2e = dist.max(time.perf_counter() - t0)
+        e2e = {"value": dist.world * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": h2d, "fields": names}
+    # ---- CPU baseline (rank 0, N = 1 only)
+    cpu = None
+    if dist.world == 1 and not args.no_cpu_baseline:
+        cs = cpu_sample(pkg, p, init, args.cpu_cap, iters_per_step)
+        cpu = {"value": 1.0 / cs["t_step_s"], "unit": UNIT, "cores": cs["cores"], "kind": "port",
+               "sample": (f"one step of the OpenMP FP64 restatement at full size with Poisson solves capped at "
+                          f"{args.cpu_cap} iterations, scaled to the {iters_per_step:.0f} iterations per step the GPU "
+                          f"measured: non-Poisson {cs['t_noncg_s']:.2f} s + {cs['t_iter_s'] * 1e3:.2f} ms/iteration"),
+               "detail": cs}
+    s.close()
+    if dist.rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(p, args, "plain-fp64 (reference Jacobi-scaled CG, FP64 everywhere)"),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk, "cg_iters_per_step": iters_per_step,
+            "max_div": stats[-1]["max_div"], "cg_resid": stats[-1]["cg_resid"], "kernels": kernels,
+        }
+        print(json.dumps(line), flush=True)
+    dist.close()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -178,6 +178,36 @@ typedef struct suli_step_stats {
 /* One time step it (1_principal.f90:64-108 without MMS/plot/restart), plus est(). */
 int suli_step(suli_ctx* c, int it, suli_step_stats* st);
 
+/* ---- tracing (replaces the wall-clock bookkeeping of 4_plot.f90:113-120, 253-257) ----- */
+/* Kernel classes timed with CUDA events on the context's stream when profiling is on. */
+enum suli_kernel {
+    SULI_K_LS_ADVECT = 0,  /* conv_weno + intt_ls stage           */
+    SULI_K_REINIT,         /* reinic_weno stages, S(phi0), error  */
+    SULI_K_LSPROPS,        /* der_weno + mod_ls1 part A + heaviside + volume */
+    SULI_K_CURV,           /* mod_ls1 part B (curvature)          */
+    SULI_K_VOLFIX,         /* volume correction                   */
+    SULI_K_VISCO,
+    SULI_K_CONVDIFF,
+    SULI_K_TEMPO,
+    SULI_K_CONTORNO,
+    SULI_K_CG_SETUP,
+    SULI_K_CG_SPMV,        /* CG kernel A: p = r + beta p, q = A p, p.q */
+    SULI_K_CG_UPDATE,      /* CG kernel B: e -= alpha p, r -= alpha q, r.r */
+    SULI_K_CG_FINAL,
+    SULI_K_POSDIN,
+    SULI_K_EST,
+    SULI_K_COUNT
+};
+/* The CUDA stream (cudaStream_t) this context launches on, for callers ordering their own
+   work or events against it. */
+int suli_stream(suli_ctx* c, void** stream);
+/* Turn per-kernel timing on (clearing the counters) or off. */
+int suli_profile_enable(suli_ctx* c, int on);
+/* Totals since enable: device milliseconds and launches per kernel class, and the number of
+   CG iterations actually performed (launches after convergence return at once). */
+int suli_profile_read(suli_ctx* c, double ms[SULI_K_COUNT], long long launches[SULI_K_COUNT],
+                      long long* cg_iterations);
+
 #ifdef __cplusplus
 }
 #endif

@@ -982,6 +982,9 @@ int Oracle::graddin() {
     while (keep_going()) {
         cont = cont + 1;
         double amu = 0., adi = 0., bmu = 0.;
+#ifdef _OPENMP
+#pragma omp parallel for collapse(2) schedule(static) reduction(+ : amu, adi)
+#endif
         for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i) {
             mp(i, j, k) = p(i, j, k) - p(i + 1, j, k) * ap(i, j, k) - p(i - 1, j, k) * an(i, j, k)
                         - p(i, j + 1, k) * bp(i, j, k) - p(i, j - 1, k) * bn(i, j, k)
@@ -991,12 +994,16 @@ int Oracle::graddin() {
         }
         alfamupr = amu;
         const double alfa = amu / adi;
+#ifdef _OPENMP
+#pragma omp parallel for collapse(2) schedule(static) reduction(+ : bmu)
+#endif
         for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i) {
             e(i, j, k) = e(i, j, k) - alfa * p(i, j, k);
             r(i, j, k) = r(i, j, k) - alfa * mp(i, j, k);
             bmu = bmu + r(i, j, k) * r(i, j, k);
         }
         const double beta = bmu / amu;
+        OMP_FOR
         for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i)
             p(i, j, k) = r(i, j, k) + beta * p(i, j, k);
         ghosts(e);

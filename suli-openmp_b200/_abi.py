@@ -209,6 +209,9 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
         "suli_est": (C.c_int, [vp, P(C.c_double)]),
         "suli_set_dt": (C.c_int, [vp, C.c_double]),
         "suli_step": (C.c_int, [vp, C.c_int, P(SuliStepStats)]),
+        "suli_stream": (C.c_int, [vp, P(vp)]),
+        "suli_profile_enable": (C.c_int, [vp, C.c_int]),
+        "suli_profile_read": (C.c_int, [vp, P(C.c_double), P(C.c_longlong), P(C.c_longlong)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -225,5 +228,11 @@ HEADER_SYMBOLS = [
     "suli_set_scalar", "suli_get_scalar", "suli_iniciais", "suli_level_set_ini",
     "suli_level_set", "suli_heaviside", "suli_mod_ls1", "suli_visco", "suli_convdiff",
     "suli_tempo", "suli_contorno", "suli_graddin", "suli_posdin", "suli_est",
-    "suli_set_dt", "suli_step",
+    "suli_set_dt", "suli_step", "suli_stream", "suli_profile_enable", "suli_profile_read",
+]
+
+# enum suli_kernel: kernel classes of the tracing counters
+KERNEL_NAMES = [
+    "ls_advect", "reinit", "lsprops", "curv", "volfix", "visco", "convdiff", "tempo", "contorno",
+    "cg_setup", "cg_spmv", "cg_update", "cg_final", "posdin", "est",
 ]

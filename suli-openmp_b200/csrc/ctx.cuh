@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <string>
+#include <vector>
 #include "../../include/suli_gpu.h"
 #include "geom.cuh"
 
@@ -81,8 +82,49 @@ struct suli_ctx {
     // cached CUDA graphs of CG iteration batches (parity 0: p_old = pa)
     cudaGraphExec_t cg_graph = nullptr;
     bool use_graphs = true;
+    // tracing: CUDA-event pairs around each kernel class (suli_profile_*)
+    struct Prof {
+        bool on = false;
+        std::vector<cudaEvent_t> ev;   // 2 per pair
+        std::vector<int> kind;
+        int used = 0;
+        double ms[SULI_K_COUNT] = {0};
+        long long launches[SULI_K_COUNT] = {0};
+        long long cg_iters = 0;
+    } prof;
     suli::Planes planes() const;
 };
+
+namespace suli {
+// Accumulate the timed pairs recorded so far (synchronises the stream).
+inline void prof_resolve(suli_ctx* c) {
+    auto& P = c->prof;
+    if (P.used == 0) return;
+    cudaStreamSynchronize(c->stream);
+    for (int q = 0; q < P.used; ++q) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, P.ev[2 * q], P.ev[2 * q + 1]) == cudaSuccess) P.ms[P.kind[q]] += t;
+    }
+    P.used = 0;
+}
+// RAII timer of one kernel class around `n` launches on the context's stream.
+struct ProfScope {
+    suli_ctx* c;
+    int slot = -1;
+    ProfScope(suli_ctx* ctx, int kind, int n) : c(ctx) {
+        auto& P = c->prof;
+        P.launches[kind] += n;
+        if (!P.on) return;
+        if (P.used * 2 + 2 > (int)P.ev.size()) prof_resolve(c);
+        slot = P.used++;
+        P.kind[slot] = kind;
+        cudaEventRecord(P.ev[2 * slot], c->stream);
+    }
+    ~ProfScope() {
+        if (slot >= 0) cudaEventRecord(c->prof.ev[2 * slot + 1], c->stream);
+    }
+};
+}  // namespace suli
 
 inline suli::Planes suli_ctx::planes() const {
     suli::Planes pl;

@@ -1020,6 +1020,7 @@ static dim3 faces_grid(const Geo& g) { return grid3(g.nx + 1, g.ny + 1, g.nz + 1
 
 void launch_lsprops(suli_ctx* c, const double* ls, bool do_mod, bool do_hs, bool do_vol) {
     const Geo& G = c->g;
+    ProfScope ps(c, SULI_K_LSPROPS, 1);
     k_lsprops<<<cells_grid(G), kBlk, 0, c->stream>>>(
         G, ls_const(c), ls, c->f[SULI_F_MOD_LS], c->nrmx, c->nrmy, c->nrmz, c->f[SULI_F_HS], c->f[SULI_F_HSX],
         c->f[SULI_F_HSY], c->f[SULI_F_HSZ], c->f[SULI_F_RHO], c->f[SULI_F_LS_NU], do_mod, do_hs, do_vol,
@@ -1027,33 +1028,40 @@ void launch_lsprops(suli_ctx* c, const double* ls, bool do_mod, bool do_hs, bool
 }
 void launch_curv(suli_ctx* c) {
     const Geo& G = c->g;
+    ProfScope ps(c, SULI_K_CURV, 1);
     k_curv<<<cells_grid(G), kBlk, 0, c->stream>>>(G, ls_const(c), c->nrmx, c->nrmy, c->nrmz, c->f[SULI_F_DDLSDX],
                                                    c->f[SULI_F_DDLSDY], c->f[SULI_F_DDLSDZ], c->f[SULI_F_KURV]);
 }
 void launch_ls_advect(suli_ctx* c, const double* cur, const double* phi0, double* out, double a, double b, double gd) {
     const Geo& G = c->g;
+    ProfScope ps(c, SULI_K_LS_ADVECT, 1);
     k_ls_advect<<<cells_grid(G), kBlk, 0, c->stream>>>(G, ls_const(c), cur, phi0, out, c->f[SULI_F_U], c->f[SULI_F_V],
                                                         c->f[SULI_F_W], a, b, gd);
 }
 void launch_reinit_funcs(suli_ctx* c) {
     const Geo& G = c->g;
+    ProfScope ps(c, SULI_K_REINIT, 1);
     k_reinit_funcs<<<cells_grid(G), kBlk, 0, c->stream>>>(G, ls_const(c), c->f[SULI_F_LS], c->funcs);
 }
 void launch_reinit_stage(suli_ctx* c, const double* cur, const double* phi0, double* out, double a, double b, double gd) {
     const Geo& G = c->g;
+    ProfScope ps(c, SULI_K_REINIT, 1);
     k_reinit_stage<<<cells_grid(G), kBlk, 0, c->stream>>>(G, ls_const(c), cur, phi0, out, c->funcs, a, b, gd);
 }
 void launch_reinit_err(suli_ctx* c, const double* after, const double* before, double band) {
     const Geo& G = c->g;
+    ProfScope ps(c, SULI_K_REINIT, 1);
     k_reinit_err<<<cells_grid(G), kBlk, 0, c->stream>>>(G, after, before, band, c->red_partial, c->red_counter,
                                                          c->red_out);
 }
 void launch_volfix(suli_ctx* c, double dt1fac) {
     const Geo& G = c->g;
+    ProfScope ps(c, SULI_K_VOLFIX, 1);
     k_volfix<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->f[SULI_F_LS], c->f[SULI_F_MOD_LS], dt1fac, c->vol_ini);
 }
 void launch_visco(suli_ctx* c) {
     const Geo& G = c->g;
+    ProfScope ps(c, SULI_K_VISCO, c->P.m_turb == 1 ? 2 : 1);
     if (c->P.m_turb == 1) {
         ViscConst V;
         V.dx = c->P.dx; V.dy = c->P.dy; V.dz = c->P.dz; V.csmag = c->P.csmag;
@@ -1078,6 +1086,7 @@ void launch_convdiff(suli_ctx* c) {
     F.ub = c->f[SULI_F_UB]; F.vb = c->f[SULI_F_VB]; F.wb = c->f[SULI_F_WB];
     F.tfu = c->f[SULI_F_TF_U]; F.tfv = c->f[SULI_F_TF_V]; F.tfw = c->f[SULI_F_TF_W];
     F.Fu = c->f[SULI_F_FU]; F.Fv = c->f[SULI_F_FV]; F.Fw = c->f[SULI_F_FW];
+    ProfScope ps(c, SULI_K_CONVDIFF, 1);
     cudaMemcpyAsync(c->f[SULI_F_PRD0], c->f[SULI_F_PRD1], G.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
     k_convdiff<<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F);
 }
@@ -1090,6 +1099,7 @@ void launch_tempo(suli_ctx* c, int tt, int it) {
     T.f0[0] = c->f[SULI_F_FU0]; T.f0[1] = c->f[SULI_F_FV0]; T.f0[2] = c->f[SULI_F_FW0];
     T.f1[0] = c->f[SULI_F_FU1]; T.f1[1] = c->f[SULI_F_FV1]; T.f1[2] = c->f[SULI_F_FW1];
     T.tm = c->P.t_tempo; T.tt = tt; T.it = it; T.dt = c->dt;
+    ProfScope ps(c, SULI_K_TEMPO, 1);
     k_tempo<<<faces_grid(G), kBlk, 0, c->stream>>>(G, T);
 }
 void launch_contorno(suli_ctx* c, int nlock) {
@@ -1102,6 +1112,7 @@ void launch_contorno(suli_ctx* c, int nlock) {
     A.pl = c->planes();
     A.nlock = nlock;
     const dim3 b2(32, 8);
+    ProfScope ps(c, SULI_K_CONTORNO, nlock == 2 ? 7 : 4);
     k_prd_ghosts<<<grid3(G.nx + 2, G.ny + 2, G.nz + 2, kBlk), kBlk, 0, c->stream>>>(G, c->bc, A.prd1);
     k_bc_y<<<grid3(G.nx + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
     k_bc_x<<<grid3(G.ny + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
@@ -1127,6 +1138,7 @@ static CGConst cg_const(const suli_ctx* c) {
 void launch_cg_setup(suli_ctx* c) {
     const Geo& G = c->g;
     const CGConst K = cg_const(c);
+    ProfScope ps(c, SULI_K_CG_SETUP, 2);
     k_cg_diag<<<cells_grid(G), kBlk, 0, c->stream>>>(G, K, c->f[SULI_F_RHO], c->f[SULI_F_U], c->f[SULI_F_V],
                                                       c->f[SULI_F_W], c->f[SULI_F_PRD1], c->cg_d, c->cg_e, c->cg_b);
     k_cg_coef<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->bc, K, c->f[SULI_F_RHO], c->cg_d, c->cg_e, c->cg_b,
@@ -1137,24 +1149,31 @@ void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new) {
     const Geo& G = c->g;
     const dim3 b(kTX, kTY, 1);
     const dim3 gr((G.nx + kTX - 1) / kTX, (G.ny + kTY - 1) / kTY, (G.nz + kKC - 1) / kKC);
-    k_cg_spmv<<<gr, b, 0, c->stream>>>(G, c->bc, c->cg_r, p_old, p_new, c->cg_q, c->cg_ax, c->cg_ay, c->cg_az, c->cg,
-                                       c->red_partial, c->red_counter);
+    {
+        ProfScope ps(c, SULI_K_CG_SPMV, 1);
+        k_cg_spmv<<<gr, b, 0, c->stream>>>(G, c->bc, c->cg_r, p_old, p_new, c->cg_q, c->cg_ax, c->cg_ay, c->cg_az, c->cg,
+                                           c->red_partial, c->red_counter);
+    }
+    ProfScope ps(c, SULI_K_CG_UPDATE, 1);
     k_cg_update<<<gr, b, 0, c->stream>>>(G, c->cg_e, c->cg_r, p_new, c->cg_q, c->cg, c->red_partial, c->red_counter);
 }
 void launch_cg_final(suli_ctx* c) {
     const Geo& G = c->g;
+    ProfScope ps(c, SULI_K_CG_FINAL, 1);
     k_cg_final<<<grid3(G.nx + 2, G.ny + 2, G.nz + 2, kBlk), kBlk, 0, c->stream>>>(G, c->bc, c->cg_d, c->cg_e,
                                                                                    c->f[SULI_F_PRD1], c->cg);
 }
 void launch_posdin(suli_ctx* c) {
     const Geo& G = c->g;
     const double aux1 = c->dt / c->P.dx, aux2 = c->dt / c->P.dy, aux3 = c->dt / c->P.dz;
+    ProfScope ps(c, SULI_K_POSDIN, 1);
     k_posdin<<<faces_grid(G), kBlk, 0, c->stream>>>(G, aux1, aux2, aux3, c->f[SULI_F_RHO], c->f[SULI_F_PRD1],
                                                      c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W]);
     cudaMemcpyAsync(c->f[SULI_F_PRD], c->f[SULI_F_PRD1], G.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
 }
 void launch_est(suli_ctx* c) {
     const Geo& G = c->g;
+    ProfScope ps(c, SULI_K_EST, 1);
     k_est<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->P.dx, c->P.dy, c->P.dz, c->f[SULI_F_U], c->f[SULI_F_V],
                                                   c->f[SULI_F_W], c->red_partial, c->red_counter, c->red_out);
 }

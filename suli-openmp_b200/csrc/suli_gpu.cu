@@ -228,6 +228,7 @@ int suli_destroy(suli_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->cg_graph) cudaGraphExecDestroy(c->cg_graph);
+    for (auto& e : c->prof.ev) cudaEventDestroy(e);
     cudaFree(c->arena);
     for (int f = SULI_F_BXX0; f < SULI_F_COUNT; ++f) cudaFree(c->f[f]);
     cudaFree(c->red_partial);
@@ -535,6 +536,7 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
     int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
     if (r != SULI_OK) return r;
     const CGState& s = c->cg_host[0];
+    c->prof.cg_iters += s.iters;
     if (iters) *iters = s.iters;
     if (resid) *resid = (s.bb > 0.) ? std::sqrt(s.rr / s.bb) : 0.;
     if (s.status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the Poisson solve");
@@ -557,6 +559,43 @@ int suli_est(suli_ctx* c, double* max_div) {
     int r = sync_read(c, c->red_out, c->host_scalars, sizeof(double));
     if (r != SULI_OK) return r;
     if (max_div) *max_div = c->host_scalars[0];
+    return SULI_OK;
+}
+
+int suli_stream(suli_ctx* c, void** stream) {
+    if (!c || !stream) return SULI_ERR_ARG;
+    *stream = (void*)c->stream;
+    return SULI_OK;
+}
+
+int suli_profile_enable(suli_ctx* c, int on) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    auto& P = c->prof;
+    prof_resolve(c);
+    if (on && P.ev.empty()) {
+        const int pairs = 1 << 14;
+        P.ev.resize(2 * pairs);
+        P.kind.resize(pairs);
+        for (auto& e : P.ev) CUDA_TRY(c, cudaEventCreate(&e));
+    }
+    for (int k = 0; k < SULI_K_COUNT; ++k) { P.ms[k] = 0.; P.launches[k] = 0; }
+    P.cg_iters = 0;
+    P.used = 0;
+    P.on = (on != 0);
+    return SULI_OK;
+}
+
+int suli_profile_read(suli_ctx* c, double ms[SULI_K_COUNT], long long launches[SULI_K_COUNT],
+                      long long* cg_iterations) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    prof_resolve(c);
+    for (int k = 0; k < SULI_K_COUNT; ++k) {
+        if (ms) ms[k] = c->prof.ms[k];
+        if (launches) launches[k] = c->prof.launches[k];
+    }
+    if (cg_iterations) *cg_iterations = c->prof.cg_iters;
     return SULI_OK;
 }
 

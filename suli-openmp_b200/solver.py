@@ -81,8 +81,13 @@ class Solver:
         ptr = a.ctypes.data_as(C.POINTER(C.c_double))
         self._check(self.lib.suli_upload(self._h, FIELD[name], ptr), f"upload {name}")
 
-    def download(self, name: str) -> np.ndarray:
-        out = np.empty(self.shape(name), dtype=np.float64, order="F")
+    def download(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        """Copy a field to the host (into `out` if given: Fortran-ordered float64, e.g. a
+        view of pinned memory)."""
+        if out is None:
+            out = np.empty(self.shape(name), dtype=np.float64, order="F")
+        elif out.shape != self.shape(name) or out.dtype != np.float64 or not out.flags.f_contiguous:
+            raise ValueError(f"download {name}: out must be float64, Fortran-ordered, {self.shape(name)}")
         ptr = out.ctypes.data_as(C.POINTER(C.c_double))
         self._check(self.lib.suli_download(self._h, FIELD[name], ptr), f"download {name}")
         return out
@@ -105,6 +110,27 @@ class Solver:
 
     def synchronize(self) -> None:
         self._check(self.lib.suli_synchronize(self._h), "synchronize")
+
+    @property
+    def stream_ptr(self) -> int:
+        """cudaStream_t of this context (e.g. for torch.cuda.ExternalStream)."""
+        s = C.c_void_p()
+        self._check(self.lib.suli_stream(self._h, C.byref(s)), "stream")
+        return int(s.value or 0)
+
+    def profile_enable(self, on: bool = True) -> None:
+        self._check(self.lib.suli_profile_enable(self._h, int(bool(on))), "profile_enable")
+
+    def profile_read(self) -> dict:
+        """Per kernel class: {'ms': device milliseconds, 'launches': n}; plus 'cg_iterations'."""
+        n = len(_abi.KERNEL_NAMES)
+        ms = (C.c_double * n)()
+        la = (C.c_longlong * n)()
+        it = C.c_longlong()
+        self._check(self.lib.suli_profile_read(self._h, ms, la, C.byref(it)), "profile_read")
+        out = {k: {"ms": ms[i], "launches": la[i]} for i, k in enumerate(_abi.KERNEL_NAMES)}
+        out["cg_iterations"] = it.value
+        return out
 
     # ---------------------------------------------------------------- reference surface
     def iniciais(self, u_init: float = 0.0) -> None:

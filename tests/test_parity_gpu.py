@@ -154,12 +154,14 @@ def test_posdin_est(pkg, orc, bc):
     assert g.est() == pytest.approx(o.est(), rel=1e-14)
 
 
-@pytest.mark.parametrize("bc", BCS)
+@pytest.mark.parametrize("bc", [b for b in BCS if 4 not in b])
 def test_graddin_tight(pkg, orc, bc):
     """Periodic cases use a density uniform along the periodic axes: with density varying
     across a periodic boundary the end-face copy of interpx_cf (8_derivadas.f90:318-323)
     makes the scaled operator non-symmetric and the reference's CG diverges (pinned by
-    test_graddin_periodic_quirk)."""
+    test_graddin_periodic_quirk).  The outflow wall (ccxf = 4) leaves the pure-Neumann
+    pressure problem with an inconsistent right-hand side, so a 1e-12 target lies in the
+    rounding-noise regime; it is covered by the reference stopping test below."""
     p = small_params(nx=14, ny=12, nz=10, bc=bc)
     p.cg_stop, p.cg_tol, p.cg_maxit = 1, 1e-12, 20000
     g, o = pair(pkg, orc, p, seed=8, layered=(0 in bc))
@@ -194,12 +196,13 @@ def test_graddin_periodic_quirk(pkg, orc):
     assert rel_err(g.download("prd1"), o.download("prd1")) <= 1e-9
 
 
-def test_graddin_reference_stop(pkg, orc):
+@pytest.mark.parametrize("bc", BCS)
+def test_graddin_reference_stop(pkg, orc, bc):
     """The reference's own stopping test: sum(r~^2) > 1e-4/(nx ny nz), checked on the residual
     at the start of each iteration (9_grad.f90:175)."""
-    p = small_params(nx=14, ny=12, nz=10)
+    p = small_params(nx=14, ny=12, nz=10, bc=bc)
     p.cg_stop, p.cg_tol, p.cg_maxit = 0, 1e-4, 10000
-    g, o = pair(pkg, orc, p, seed=9)
+    g, o = pair(pkg, orc, p, seed=9, layered=(0 in bc))
     res = {}
     for name, m in (("g", g), ("o", o)):
         m.set_dt(1e-3)
