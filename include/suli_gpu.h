@@ -178,6 +178,26 @@ typedef struct suli_step_stats {
 /* One time step it (1_principal.f90:64-108 without MMS/plot/restart), plus est(). */
 int suli_step(suli_ctx* c, int it, suli_step_stats* st);
 
+/* ---- divergence check that allocates nothing ---------------------------------------------
+   No counterpart in the reference: an extra way to run est() for callers that may not let a
+   library allocate device memory.  Typical callers: a driver whose u, v, w already live on
+   the GPU under another runtime (OpenACC or CUDA Fortran device arrays, or a framework whose
+   caching allocator has reserved the memory), where a cudaMalloc could fail for lack of
+   unreserved memory and cudaMalloc/cudaFree would stall the device.  It needs no context.
+   u, v, w: device pointers in the reference's Fortran layout u(0:nx+2,0:ny+1,0:nz+1),
+   v(0:nx+1,0:ny+2,0:nz+1), w(0:nx+1,0:ny+1,0:nz+2); max_div: device pointer to one double;
+   stream: a cudaStream_t (NULL = default stream).  Runs on the calling thread's current
+   device and returns without waiting for the result.
+   Scratch: a fixed array inside the library (SULI_EST_STATIC_MAX_BLOCKS block partials,
+   about 64 KiB), held on every GPU that loads the library until the process exits.  Grids
+   needing more blocks (one block per 32 x 8 x 16 cells; 512 x 256 x 256 fits exactly) are
+   refused with SULI_ERR_SIZE.  The first call on a device looks up the array's device
+   address; make that first call before any stream capture.  All calls share the array:
+   calls that overlap on the GPU race and must be ordered by the caller. */
+#define SULI_EST_STATIC_MAX_BLOCKS 8192
+int suli_est_static(const double* u, const double* v, const double* w, int nx, int ny, int nz,
+                    double dx, double dy, double dz, double* max_div, void* stream);
+
 /* ---- tracing (replaces the wall-clock bookkeeping of 4_plot.f90:113-120, 253-257) ----- */
 /* Kernel classes timed with CUDA events on the context's stream when profiling is on. */
 enum suli_kernel {

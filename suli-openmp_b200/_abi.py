@@ -212,6 +212,8 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
         "suli_stream": (C.c_int, [vp, P(vp)]),
         "suli_profile_enable": (C.c_int, [vp, C.c_int]),
         "suli_profile_read": (C.c_int, [vp, P(C.c_double), P(C.c_longlong), P(C.c_longlong)]),
+        "suli_est_static": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                      C.c_double, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -229,7 +231,9 @@ HEADER_SYMBOLS = [
     "suli_level_set", "suli_heaviside", "suli_mod_ls1", "suli_visco", "suli_convdiff",
     "suli_tempo", "suli_contorno", "suli_graddin", "suli_posdin", "suli_est",
     "suli_set_dt", "suli_step", "suli_stream", "suli_profile_enable", "suli_profile_read",
+    "suli_est_static",
 ]
+EST_STATIC_MAX_BLOCKS = 8192   # SULI_EST_STATIC_MAX_BLOCKS
 
 # enum suli_kernel: kernel classes of the tracing counters
 KERNEL_NAMES = [
