@@ -844,52 +844,52 @@ __global__ void __launch_bounds__(256) k_cg_coef(Geo G, BC bc, CGConst K, const 
     }
 }
 
-// CG kernel A: p = r + beta*p_old (also at the neighbours), q = A~p, reduction of p.q (:192-205)
-constexpr int kTX = 32, kTY = 8, kKC = 8;
+// CG kernel A: p = r + beta*p_old (also at the neighbours), q = A~p, reduction of p.q (:192-205).
+// One thread owns a column of kCGZA cells: the z neighbours of its cells are shared in
+// registers and every global load of the column is independent (issued back to back), which
+// is what keeps enough bytes in flight; x/y neighbours come through L1.  32-bit offsets.
+constexpr int kTX = 32, kTY = 8, kCGZA = 4, kCGZB = 8;
 __global__ void __launch_bounds__(kTX * kTY) k_cg_spmv(Geo G, BC bc, const double* __restrict__ r,
-                                                       const double* __restrict__ p_old, double* p_new, double* q,
-                                                       const double* __restrict__ ax, const double* __restrict__ ay,
-                                                       const double* __restrict__ az, CGState* st, double* partial,
-                                                       unsigned int* counter) {
+                                                       const double* __restrict__ p_old, double* __restrict__ p_new,
+                                                       double* __restrict__ q, const double* __restrict__ ax,
+                                                       const double* __restrict__ ay, const double* __restrict__ az,
+                                                       CGState* st, double* partial, unsigned int* counter) {
     if (st->done) return;
-    __shared__ double s[kTY + 2][kTX + 2];
     const double beta = st->beta;
-    const int nx = G.nx, ny = G.ny, nz = G.nz;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int i = blockIdx.x * kTX + tx + 1, j = blockIdx.y * kTY + ty + 1;
-    const int k0 = blockIdx.z * kKC + 1;
-    const int k1 = min(k0 + kKC - 1, nz);
-    const bool in = (i <= nx && j <= ny);
-    auto pn = [&](int ii, int jj, int kk) {
-        const long long c = G.idx(map_any(ii, nx, bc.perx), map_any(jj, ny, bc.pery), map_any(kk, nz, bc.perz));
-        return r[c] + beta * p_old[c];
-    };
-    double pkm1 = 0., pk = 0., azk = 0.;
-    if (in) { pkm1 = pn(i, j, k0 - 1); pk = pn(i, j, k0); azk = FIDX(az, i, j, k0); }
+    const int nx = G.nx, ny = G.ny, nz = G.nz, px = G.px, pxy = (int)G.pxy;
+    const int i = blockIdx.x * kTX + threadIdx.x + 1, j = blockIdx.y * kTY + threadIdx.y + 1;
+    const int k0 = blockIdx.z * kCGZA + 1;
     double dot = 0.;
-    for (int k = k0; k <= k1; ++k) {
-        double pkp1 = 0., azkp1 = 0.;
-        if (in) {
-            pkp1 = pn(i, j, k + 1);
-            azkp1 = FIDX(az, i, j, k + 1);
-            s[ty + 1][tx + 1] = pk;
-            if (tx == 0) s[ty + 1][0] = pn(i - 1, j, k);
-            if (tx == kTX - 1 || i == nx) s[ty + 1][tx + 2] = pn(i + 1, j, k);
-            if (ty == 0) s[0][tx + 1] = pn(i, j - 1, k);
-            if (ty == kTY - 1 || j == ny) s[ty + 2][tx + 1] = pn(i, j + 1, k);
+    if (i <= nx && j <= ny) {
+        // neighbour offsets with the ghost maps of 9_grad.f90:99-116 (periodic wrap or Neumann copy)
+        const int oxm = (i > 1) ? -1 : (bc.perx ? nx - 1 : 0);
+        const int oxp = (i < nx) ? 1 : (bc.perx ? -(nx - 1) : 0);
+        const int oym = (j > 1) ? -px : (bc.pery ? (ny - 1) * px : 0);
+        const int oyp = (j < ny) ? px : (bc.pery ? -(ny - 1) * px : 0);
+        const int c0 = kBase + (i - 1) + px * j;
+        double col[kCGZA + 2];   // p at k0-1 .. k0+kCGZA
+#pragma unroll
+        for (int m = 0; m < kCGZA + 2; ++m) {
+            const int k = map_any(k0 - 1 + m, nz, bc.perz);
+            const int c = c0 + pxy * k;
+            col[m] = r[c] + beta * p_old[c];
         }
-        __syncthreads();
-        if (in) {
-            const long long c = G.idx(i, j, k);
-            const double qv = pk - s[ty + 1][tx + 2] * FIDX(ax, i + 1, j, k) - s[ty + 1][tx] * ax[c] -
-                              s[ty + 2][tx + 1] * FIDX(ay, i, j + 1, k) - s[ty][tx + 1] * ay[c] - pkp1 * azkp1 -
-                              pkm1 * azk;
+#pragma unroll
+        for (int m = 0; m < kCGZA; ++m) {
+            const int k = k0 + m;
+            if (k > nz) break;
+            const int c = c0 + pxy * k;
+            const double pxp = r[c + oxp] + beta * p_old[c + oxp];
+            const double pxm = r[c + oxm] + beta * p_old[c + oxm];
+            const double pyp = r[c + oyp] + beta * p_old[c + oyp];
+            const double pym = r[c + oym] + beta * p_old[c + oym];
+            const double pc = col[m + 1];
+            const double qv = pc - pxp * ax[c + 1] - pxm * ax[c] - pyp * ay[c + px] - pym * ay[c] -
+                              col[m + 2] * az[c + pxy] - col[m] * az[c];
             q[c] = qv;
-            p_new[c] = pk;
-            dot += pk * qv;
+            p_new[c] = pc;
+            dot += pc * qv;
         }
-        __syncthreads();
-        pkm1 = pk; pk = pkp1; azk = azkp1;
     }
     double tpq, tdum;
     if (reduce2_last(dot, 0.0, partial, counter, tpq, tdum) && flat_tid() == 0) {
@@ -901,22 +901,24 @@ __global__ void __launch_bounds__(kTX * kTY) k_cg_spmv(Geo G, BC bc, const doubl
 }
 
 // CG kernel B: e -= alpha p, r -= alpha q, reduction of r.r, beta and the stopping test (:210-221, :175)
-__global__ void __launch_bounds__(kTX * kTY) k_cg_update(Geo G, double* e, double* r, const double* __restrict__ p,
-                                                         const double* __restrict__ q, CGState* st, double* partial,
-                                                         unsigned int* counter) {
+__global__ void __launch_bounds__(kTX * kTY) k_cg_update(Geo G, double* __restrict__ e, double* __restrict__ r,
+                                                         const double* __restrict__ p, const double* __restrict__ q,
+                                                         CGState* st, double* partial, unsigned int* counter) {
     if (st->done) return;
     const double alpha = st->alpha;
     const int i = blockIdx.x * kTX + threadIdx.x + 1, j = blockIdx.y * kTY + threadIdx.y + 1;
-    const int k0 = blockIdx.z * kKC + 1;
-    const int k1 = min(k0 + kKC - 1, G.nz);
+    const int k0 = blockIdx.z * kCGZB + 1;
+    const int pxy = (int)G.pxy;
     double rr = 0.;
     if (i <= G.nx && j <= G.ny) {
+        const int c0 = kBase + (i - 1) + G.px * j;
+        const int k1 = min(k0 + kCGZB - 1, G.nz);
         for (int k = k0; k <= k1; ++k) {
-            const long long c = G.idx(i, j, k);
+            const int c = c0 + pxy * k;
             e[c] = e[c] - alpha * p[c];
-            const double rv = r[c] - alpha * q[c];
-            r[c] = rv;
-            rr += rv * rv;
+            const double rn = r[c] - alpha * q[c];
+            r[c] = rn;
+            rr += rn * rn;
         }
     }
     double trr, tdum;
@@ -1148,14 +1150,15 @@ void launch_cg_setup(suli_ctx* c) {
 void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new) {
     const Geo& G = c->g;
     const dim3 b(kTX, kTY, 1);
-    const dim3 gr((G.nx + kTX - 1) / kTX, (G.ny + kTY - 1) / kTY, (G.nz + kKC - 1) / kKC);
+    const dim3 ga((G.nx + kTX - 1) / kTX, (G.ny + kTY - 1) / kTY, (G.nz + kCGZA - 1) / kCGZA);
+    const dim3 gb((G.nx + kTX - 1) / kTX, (G.ny + kTY - 1) / kTY, (G.nz + kCGZB - 1) / kCGZB);
     {
         ProfScope ps(c, SULI_K_CG_SPMV, 1);
-        k_cg_spmv<<<gr, b, 0, c->stream>>>(G, c->bc, c->cg_r, p_old, p_new, c->cg_q, c->cg_ax, c->cg_ay, c->cg_az, c->cg,
+        k_cg_spmv<<<ga, b, 0, c->stream>>>(G, c->bc, c->cg_r, p_old, p_new, c->cg_q, c->cg_ax, c->cg_ay, c->cg_az, c->cg,
                                            c->red_partial, c->red_counter);
     }
     ProfScope ps(c, SULI_K_CG_UPDATE, 1);
-    k_cg_update<<<gr, b, 0, c->stream>>>(G, c->cg_e, c->cg_r, p_new, c->cg_q, c->cg, c->red_partial, c->red_counter);
+    k_cg_update<<<gb, b, 0, c->stream>>>(G, c->cg_e, c->cg_r, p_new, c->cg_q, c->cg, c->red_partial, c->red_counter);
 }
 void launch_cg_final(suli_ctx* c) {
     const Geo& G = c->g;

@@ -202,12 +202,23 @@ def test_graddin_reference_stop(pkg, orc, bc):
     at the start of each iteration (9_grad.f90:175)."""
     p = small_params(nx=14, ny=12, nz=10, bc=bc)
     p.cg_stop, p.cg_tol, p.cg_maxit = 0, 1e-4, 10000
+    if 4 in bc:
+        # outflow (ccxf = 4): the Neumann pressure problem gets a right-hand side with a
+        # null-space component, the residual stagnates and where it stops is rounding noise;
+        # compare a fixed 30-iteration trajectory instead
+        p.cg_tol, p.cg_maxit = 1e-30, 30
     g, o = pair(pkg, orc, p, seed=9, layered=(0 in bc))
     res = {}
     for name, m in (("g", g), ("o", o)):
         m.set_dt(1e-3)
         m.contorno(2)
         res[name] = m.graddin()
+        m.posdin()
+    if 4 in bc:
+        assert res["g"][0] == res["o"][0] == 30
+        for f in ("u", "v", "w", "prd1"):
+            assert rel_err(g.download(f), o.download(f)) <= 1e-9, f
+        return
     assert abs(res["g"][0] - res["o"][0]) <= 1
     if res["g"][0] == res["o"][0]:
         assert rel_err(g.download("prd1"), o.download("prd1")) <= 1e-8
