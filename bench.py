@@ -58,6 +58,7 @@ def parse_args():
     ap.add_argument("--nz", type=int, default=128)
     ap.add_argument("--dx", type=float, default=0.005)
     ap.add_argument("--cg-tol", type=float, default=1e-8)
+    ap.add_argument("--inner-tol", type=float, default=1e-3, help="relative tolerance of each FP32 inner solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-cap", type=int, default=20, help="CG iterations per solve in the CPU sample")
@@ -285,24 +286,18 @@ def workload_config(p, args, path):
     }
 
 
-def run_ours(args):
-    import numpy as np
+def time_path(args, dist, pkg, p, init, dev, it0=0):
+    """Warm up, then time K steps of one solver path with CUDA events on its own stream."""
     import torch
 
-    dist = Dist("nccl")
-    dev = dist.local
-    torch.cuda.set_device(dev)
-    pkg = load_pkg()
-    p, init = pkg.cases.sloshing(nx=args.nx, ny=args.ny, nz=args.nz, dx=args.dx, cg_tol=args.cg_tol)
     s = pkg.Solver(p, device=dev)
     init(s)
     ext = torch.cuda.ExternalStream(s.stream_ptr, device=dev)
-    it = 0
+    it = it0
     for _ in range(args.warmup):
         it += 1
         s.step(it)
     s.synchronize()
-    # ---- timed region: device events on the library's stream, profiling counters on
     s.profile_enable(True)
     clocks = ClockSampler(dev)
     dist.barrier()
@@ -323,10 +318,16 @@ def run_ours(args):
     prof = s.profile_read()
     s.profile_enable(False)
     ms = dist.max(ms_local)
-    value = dist.world * args.steps / (ms / 1e3)
-    iters_per_step = prof["cg_iterations"] / args.steps
-    launches = sum(v["launches"] for k, v in prof.items() if isinstance(v, dict))
-    # ---- roofline of the dominant kernel (CG kernel A) and of the whole CG iteration
+    return {"solver": s, "it": it, "ms": ms, "value": dist.world * args.steps / (ms / 1e3), "prof": prof,
+            "stats": stats, "clocks": clk,
+            "iters_per_step": prof["cg_iterations"] / args.steps,
+            "launches": sum(v["launches"] for k, v in prof.items() if isinstance(v, dict)),
+            "kernels": {k: {"ms_per_step": v["ms"] / args.steps, "launches_per_step": v["launches"] / args.steps}
+                        for k, v in prof.items() if isinstance(v, dict)}}
+
+
+def cg_roofline(p, prof):
+    """Roofline of the plain path's dominant kernel (CG kernel A) and of a whole CG iteration."""
     N = p.nx * p.ny * p.nz
     faces = (p.nx + 1) * p.ny * p.nz + p.nx * (p.ny + 1) * p.nz + p.nx * p.ny * (p.nz + 1)
     bytes_spmv = 8 * (4 * N + faces)
@@ -336,19 +337,49 @@ def run_ours(args):
     t_upd = prof["cg_update"]["ms"] / n_it / 1e3
     peak, peak_kind = measured_peaks()
     ach = bytes_spmv / t_spmv / 1e9
-    traffic = profiled_traffic("cg_spmv_256x128x128", N)
-    roofline = {
-        "kernel": "k_cg_spmv (CG kernel A: p = r + beta p, q = A p, p.q)",
+    return {
+        "kernel": "k_cg_spmv (FP64 CG kernel A: p = r + beta p, q = A p, p.q)",
         "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
-        "traffic": traffic, "algorithmic_bytes_per_launch": bytes_spmv, "avg_launch_us": t_spmv * 1e6,
+        "traffic": profiled_traffic("cg_spmv_256x128x128", N), "algorithmic_bytes_per_launch": bytes_spmv,
+        "avg_launch_us": t_spmv * 1e6,
         "cg_iteration": {"kernels": "k_cg_spmv + k_cg_update", "bytes": bytes_spmv + bytes_upd,
                          "us": (t_spmv + t_upd) * 1e6,
                          "achieved_gbs": (bytes_spmv + bytes_upd) / (t_spmv + t_upd) / 1e9,
                          "frac": (bytes_spmv + bytes_upd) / (t_spmv + t_upd) / 1e9 / peak},
     }
-    kernels = {k: {"ms_per_step": v["ms"] / args.steps, "launches_per_step": v["launches"] / args.steps}
-               for k, v in prof.items() if isinstance(v, dict)}
+
+
+def mixed_params(p, args):
+    q = p.copy()
+    q.precision, q.cg_stop, q.cg_tol = 1, 1, args.cg_tol
+    q.inner_tol, q.refine_maxit = args.inner_tol, 30
+    return q
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    dist = Dist("nccl")
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    pkg = load_pkg()
+    p, init = pkg.cases.sloshing(nx=args.nx, ny=args.ny, nz=args.nz, dx=args.dx, cg_tol=args.cg_tol)
+    # plain FP64 path (the reference's Jacobi-scaled CG): timed for the comparison
+    plain = time_path(args, dist, pkg, p, init, dev)
+    plain["solver"].close()
+    roof_plain = cg_roofline(p, plain["prof"])
+    # headline path: mixed precision (FP32 multigrid-preconditioned inner CG, FP64 refinement)
+    q = mixed_params(p, args)
+    head = time_path(args, dist, pkg, q, init, dev)
+    s = head["solver"]
+    it = head["it"]
+    value, ms, prof, stats, clk = head["value"], head["ms"], head["prof"], head["stats"], head["clocks"]
+    iters_per_step = plain["iters_per_step"]
+    launches = head["launches"]
+    kernels = head["kernels"]
+    roofline = roof_plain
     # ---- end to end through the C-ABI: pinned host state in and out every step
     e2e = None
     if not args.no_e2e:
@@ -386,14 +417,22 @@ def run_ours(args):
                "detail": cs}
     s.close()
     if dist.rank == 0:
+        cfg = workload_config(q, args, "mixed: FP64 stencils, FP32 multigrid-preconditioned inner CG inside FP64 "
+                                       "iterative refinement to the same FP64 relative residual")
+        cfg["inner_tol"] = args.inner_tol
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(p, args, "plain-fp64 (reference Jacobi-scaled CG, FP64 everywhere)"),
+            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+            "config": cfg,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk, "cg_iters_per_step": iters_per_step,
+            "clocks": clk, "inner_iters_per_step": head["iters_per_step"],
             "max_div": stats[-1]["max_div"], "cg_resid": stats[-1]["cg_resid"], "kernels": kernels,
+            "plain_fp64": {"value": plain["value"], "ms_per_step": plain["ms"] / args.steps,
+                           "cg_iters_per_step": plain["iters_per_step"], "max_div": plain["stats"][-1]["max_div"],
+                           "cg_resid": plain["stats"][-1]["cg_resid"], "clocks": plain["clocks"],
+                           "gpu_launches": plain["launches"], "kernels": plain["kernels"]},
+            "speedup_vs_plain_fp64": value / plain["value"],
         }
         print(json.dumps(line), flush=True)
     dist.close()

@@ -216,6 +216,9 @@ enum suli_kernel {
     SULI_K_CG_FINAL,
     SULI_K_POSDIN,
     SULI_K_EST,
+    SULI_K_MG,             /* precision 1: FP32 inner PCG iterations (SpMV, update, multigrid
+                              V-cycle), launched as one CUDA graph per iteration */
+    SULI_K_REFINE,         /* precision 1: FP64 residual and correction of the refinement */
     SULI_K_COUNT
 };
 /* The CUDA stream (cudaStream_t) this context launches on, for callers ordering their own

@@ -238,5 +238,5 @@ EST_STATIC_MAX_BLOCKS = 8192   # SULI_EST_STATIC_MAX_BLOCKS
 # enum suli_kernel: kernel classes of the tracing counters
 KERNEL_NAMES = [
     "ls_advect", "reinit", "lsprops", "curv", "volfix", "visco", "convdiff", "tempo", "contorno",
-    "cg_setup", "cg_spmv", "cg_update", "cg_final", "posdin", "est",
+    "cg_setup", "cg_spmv", "cg_update", "cg_final", "posdin", "est", "mg", "refine",
 ]

@@ -28,6 +28,28 @@ struct CGState {
     int pad;
 };
 
+// State of the FP32 inner preconditioned CG of the mixed-precision solve (device resident).
+struct PCGState {
+    double rz;      // r.z of the current residual
+    double rr;      // r.r
+    double rr0;     // r.r of the right-hand side of this inner solve
+    double pq;
+    double alpha;
+    double beta;
+    double tol2;    // stop when r.r <= tol2
+    int iters;
+    int done;
+    int maxit;
+    int status;
+};
+
+// One level of the FP32 multigrid hierarchy: face conductances, Jacobi diagonal, vectors.
+struct MGLevel {
+    Geo g;
+    float *sx = nullptr, *sy = nullptr, *sz = nullptr, *dg = nullptr;
+    float *f = nullptr, *x = nullptr, *y = nullptr;
+};
+
 // Boundary planes of prescribed walls (velpre, 0_modules.f90:96-118), Fortran layout.
 struct Planes {
     const double *bxx0, *bxx1, *bxy0, *bxz0, *bxxf, *bxxf1, *bxyf, *bxzf;
@@ -79,6 +101,20 @@ struct suli_ctx {
     int last_reinit_iters = 0;
     int last_volfix_iters = 0;
     int cg_batch = 16;
+    // mixed-precision solve (precision = 1)
+    std::vector<suli::MGLevel> mg;
+    float *pc_x = nullptr, *pc_r = nullptr, *pc_pa = nullptr, *pc_pb = nullptr, *pc_q = nullptr;
+    double* cg_e2 = nullptr;
+    suli::PCGState* pcg = nullptr;
+    suli::PCGState* pcg_host = nullptr;
+    float* f32_arena = nullptr;
+    int coarse_sweeps = 40;
+    int inner_maxit = 200;
+    int inner_batch = 4;
+    int last_outer_iters = 0;
+    // one CUDA graph per ping-pong parity holding a whole inner PCG iteration
+    cudaGraphExec_t pcg_graph[2] = {nullptr, nullptr};
+    int pcg_graph_kernels = 0;
     // cached CUDA graphs of CG iteration batches (parity 0: p_old = pa)
     cudaGraphExec_t cg_graph = nullptr;
     bool use_graphs = true;
@@ -113,6 +149,9 @@ struct ProfScope {
     int slot = -1;
     ProfScope(suli_ctx* ctx, int kind, int n) : c(ctx) {
         auto& P = c->prof;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(c->stream, &cs);
+        if (cs != cudaStreamCaptureStatusNone) return;   // inside a graph capture: counted at launch
         P.launches[kind] += n;
         if (!P.on) return;
         if (P.used * 2 + 2 > (int)P.ev.size()) prof_resolve(c);
@@ -154,7 +193,13 @@ void launch_tempo(suli_ctx* c, int tt, int it);
 void launch_contorno(suli_ctx* c, int nlock);
 void launch_cg_setup(suli_ctx* c);
 void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new);
-void launch_cg_final(suli_ctx* c);
+void launch_cg_final(suli_ctx* c, const double* e);
+// ---- mixed-precision solve (k_mixed.cu) ----
+void launch_mx_setup(suli_ctx* c);
+void launch_mx_residual(suli_ctx* c, const double* e_in, double* e_out, bool apply);
+void launch_pcg_init(suli_ctx* c, int maxit);
+void launch_vcycle(suli_ctx* c);
+void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new);
 void launch_posdin(suli_ctx* c);
 void launch_est(suli_ctx* c);
 void launch_fill(suli_ctx* c, double* a, double v);

@@ -1,0 +1,447 @@
+// k_mixed.cu — mixed-precision pressure solve (precision = 1).
+//
+// The FP64 problem is the reference's scaled system A~ e = b~ (9_grad.f90:118-151).  It is
+// solved by iterative refinement: the FP64 residual r~ = A~e - b~ is formed from the FP64
+// coefficients, its unscaled form r_u = sqrt(d) r~ = A p - q is rounded to FP32, an FP32
+// preconditioned CG solves A dp = r_u on the unscaled operator A (rows sum_f s_f (p_c - p_nb),
+// ghost faces folded exactly as the reference's copies), and e <- e - sqrt(d) dp in FP64.  The
+// loop stops on the same FP64 test as the plain path: ||r~|| <= tol ||b~||.
+//
+// Preconditioner: a geometric multigrid V-cycle in FP32 — piecewise-constant prolongation,
+// restriction P^T/8 and Galerkin coarse faces (sum of the four fine faces)/8, two damped
+// Jacobi sweeps before and after, a one-block Jacobi solve on the coarsest grid.  Pre- and
+// post-smoothing mirror each other, so the V-cycle is a symmetric positive operator and plain
+// (not flexible) PCG applies.
+#include <cuda_runtime.h>
+#include <cmath>
+#include "ctx.cuh"
+#include "reduce.cuh"
+
+namespace suli {
+
+#define FI(a, i, j, k) (a)[G.idx((i), (j), (k))]
+
+__device__ __forceinline__ int clampi_m(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// neighbour offsets of cell (i,j,k) in a level's box; a Neumann face maps to the cell itself
+struct Nb {
+    int xm, xp, ym, yp, zm, zp;
+};
+__device__ __forceinline__ Nb neighbours(const Geo& G, const BC& bc, int i, int j, int k) {
+    Nb o;
+    const int px = G.px, pxy = (int)G.pxy;
+    o.xm = (i > 1) ? -1 : (bc.perx ? G.nx - 1 : 0);
+    o.xp = (i < G.nx) ? 1 : (bc.perx ? -(G.nx - 1) : 0);
+    o.ym = (j > 1) ? -px : (bc.pery ? (G.ny - 1) * px : 0);
+    o.yp = (j < G.ny) ? px : (bc.pery ? -(G.ny - 1) * px : 0);
+    o.zm = (k > 1) ? -pxy : (bc.perz ? (G.nz - 1) * pxy : 0);
+    o.zp = (k < G.nz) ? pxy : (bc.perz ? -(G.nz - 1) * pxy : 0);
+    return o;
+}
+// (A x)_c = sum over the six faces of s_f (x_c - x_nb)
+__device__ __forceinline__ float apply_A(const float* __restrict__ x, const float* __restrict__ sx,
+                                         const float* __restrict__ sy, const float* __restrict__ sz, int c,
+                                         const Nb& o, int px, int pxy) {
+    const float xc = x[c];
+    return sx[c] * (xc - x[c + o.xm]) + sx[c + 1] * (xc - x[c + o.xp]) + sy[c] * (xc - x[c + o.ym]) +
+           sy[c + px] * (xc - x[c + o.yp]) + sz[c] * (xc - x[c + o.zm]) + sz[c + pxy] * (xc - x[c + o.zp]);
+}
+
+// ------------------------------------------------------------------------------------
+// set-up: fine-level face conductances s = dt/(dx^2 rho_face) and the Jacobi diagonal
+// ------------------------------------------------------------------------------------
+__global__ void k_mx_faces0(Geo G, BC bc, const double* __restrict__ rho, double cx, double cy, double cz,
+                            float* sx, float* sy, float* sz, float* dg) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > G.nx || j > G.ny || k > G.nz) return;
+    auto fx = [&](int f) { const int fc = clampi_m(f, 2, G.nx); return cx / ((FI(rho, fc, j, k) + FI(rho, fc - 1, j, k)) * 0.5); };
+    auto fy = [&](int f) { const int fc = clampi_m(f, 2, G.ny); return cy / ((FI(rho, i, fc, k) + FI(rho, i, fc - 1, k)) * 0.5); };
+    auto fz = [&](int f) { const int fc = clampi_m(f, 2, G.nz); return cz / ((FI(rho, i, j, fc) + FI(rho, i, j, fc - 1)) * 0.5); };
+    const double xl = fx(i), xh = fx(i + 1), yl = fy(j), yh = fy(j + 1), zl = fz(k), zh = fz(k + 1);
+    const long long c = G.idx(i, j, k);
+    sx[c] = (float)xl; sy[c] = (float)yl; sz[c] = (float)zl;
+    if (i == G.nx) FI(sx, i + 1, j, k) = (float)xh;
+    if (j == G.ny) FI(sy, i, j + 1, k) = (float)yh;
+    if (k == G.nz) FI(sz, i, j, k + 1) = (float)zh;
+    double d = 0.;
+    if (i > 1 || bc.perx) d += xl;
+    if (i < G.nx || bc.perx) d += xh;
+    if (j > 1 || bc.pery) d += yl;
+    if (j < G.ny || bc.pery) d += yh;
+    if (k > 1 || bc.perz) d += zl;
+    if (k < G.nz || bc.perz) d += zh;
+    dg[c] = (float)(d > 0. ? d : 1.);
+}
+
+// Galerkin coarse faces: (sum of the 4 fine faces covering a coarse face) / 8
+__global__ void k_mg_coarsen(Geo Gf, Geo Gc, BC bc, const float* __restrict__ fx, const float* __restrict__ fy,
+                             const float* __restrict__ fz, float* cxs, float* cys, float* czs, float* dg) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int K = blockIdx.z + 1;
+    if (I > Gc.nx || J > Gc.ny || K > Gc.nz) return;
+    auto sumx = [&](int F) {   // coarse x-face F <-> fine x-face 2F-1
+        const int f = 2 * F - 1;
+        return fx[Gf.idx(f, 2 * J - 1, 2 * K - 1)] + fx[Gf.idx(f, 2 * J, 2 * K - 1)] + fx[Gf.idx(f, 2 * J - 1, 2 * K)] +
+               fx[Gf.idx(f, 2 * J, 2 * K)];
+    };
+    auto sumy = [&](int F) {
+        const int f = 2 * F - 1;
+        return fy[Gf.idx(2 * I - 1, f, 2 * K - 1)] + fy[Gf.idx(2 * I, f, 2 * K - 1)] + fy[Gf.idx(2 * I - 1, f, 2 * K)] +
+               fy[Gf.idx(2 * I, f, 2 * K)];
+    };
+    auto sumz = [&](int F) {
+        const int f = 2 * F - 1;
+        return fz[Gf.idx(2 * I - 1, 2 * J - 1, f)] + fz[Gf.idx(2 * I, 2 * J - 1, f)] + fz[Gf.idx(2 * I - 1, 2 * J, f)] +
+               fz[Gf.idx(2 * I, 2 * J, f)];
+    };
+    const float xl = 0.125f * sumx(I), xh = 0.125f * sumx(I + 1);
+    const float yl = 0.125f * sumy(J), yh = 0.125f * sumy(J + 1);
+    const float zl = 0.125f * sumz(K), zh = 0.125f * sumz(K + 1);
+    const long long c = Gc.idx(I, J, K);
+    cxs[c] = xl; cys[c] = yl; czs[c] = zl;
+    if (I == Gc.nx) cxs[Gc.idx(I + 1, J, K)] = xh;
+    if (J == Gc.ny) cys[Gc.idx(I, J + 1, K)] = yh;
+    if (K == Gc.nz) czs[Gc.idx(I, J, K + 1)] = zh;
+    float d = 0.f;
+    if (I > 1 || bc.perx) d += xl;
+    if (I < Gc.nx || bc.perx) d += xh;
+    if (J > 1 || bc.pery) d += yl;
+    if (J < Gc.ny || bc.pery) d += yh;
+    if (K > 1 || bc.perz) d += zl;
+    if (K < Gc.nz || bc.perz) d += zh;
+    dg[c] = d > 0.f ? d : 1.f;
+}
+
+// ------------------------------------------------------------------------------------
+// V-cycle kernels (all return at once when the inner solve has finished)
+// ------------------------------------------------------------------------------------
+struct MGOps {
+    const float *sx, *sy, *sz, *dg;
+};
+
+__global__ void __launch_bounds__(256) k_mg_jac0(Geo G, const float* __restrict__ f, const float* __restrict__ dg,
+                                                 float* x, float omega, const PCGState* st) {
+    if (st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > G.nx || j > G.ny || k > G.nz) return;
+    const int c = (int)G.idx(i, j, k);
+    x[c] = omega * f[c] / dg[c];
+}
+
+// x_out = x_in + omega (f - A x_in)/dg; optionally (level 0, last sweep) the dot f.x_out -> rz, beta
+__global__ void __launch_bounds__(256) k_mg_jac(Geo G, BC bc, const float* __restrict__ xin, const float* __restrict__ f,
+                                                MGOps A, float* __restrict__ xout, float omega, PCGState* st,
+                                                int do_dot, double* partial, unsigned int* counter) {
+    if (st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    double dot = 0.;
+    if (i <= G.nx && j <= G.ny && k <= G.nz) {
+        const int c = (int)G.idx(i, j, k);
+        const Nb o = neighbours(G, bc, i, j, k);
+        const float ax = apply_A(xin, A.sx, A.sy, A.sz, c, o, G.px, (int)G.pxy);
+        const float fv = f[c];
+        const float v = xin[c] + omega * (fv - ax) / A.dg[c];
+        xout[c] = v;
+        dot = (double)fv * (double)v;
+    }
+    if (do_dot) {
+        double t, u;
+        if (reduce2_last(dot, 0.0, partial, counter, t, u) && flat_tid() == 0) {
+            const double rz_old = st->rz;
+            st->rz = t;
+            st->beta = (st->iters == 0) ? 0.0 : t / rz_old;
+            if (!isfinite(t)) { st->status = SULI_ERR_NAN; st->done = 1; }
+        }
+    }
+}
+
+// f_c = (1/8) sum over the 8 children of (f - A x)
+__global__ void __launch_bounds__(256) k_mg_restrict(Geo Gf, Geo Gc, BC bc, const float* __restrict__ x,
+                                                     const float* __restrict__ f, MGOps A, float* fc, const PCGState* st) {
+    if (st->done) return;
+    const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int K = blockIdx.z + 1;
+    if (I > Gc.nx || J > Gc.ny || K > Gc.nz) return;
+    float s = 0.f;
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) {
+                const int i = 2 * I - 1 + dx, j = 2 * J - 1 + dy, k = 2 * K - 1 + dz;
+                const int c = (int)Gf.idx(i, j, k);
+                const Nb o = neighbours(Gf, bc, i, j, k);
+                s += f[c] - apply_A(x, A.sx, A.sy, A.sz, c, o, Gf.px, (int)Gf.pxy);
+            }
+    fc[Gc.idx(I, J, K)] = 0.125f * s;
+}
+
+// x_out = x' + omega (f - A x')/dg with x' = y + P xc (piecewise-constant prolongation)
+__global__ void __launch_bounds__(256) k_mg_prolong_jac(Geo Gf, Geo Gc, BC bc, const float* __restrict__ y,
+                                                        const float* __restrict__ xc, const float* __restrict__ f,
+                                                        MGOps A, float* __restrict__ xout, float omega,
+                                                        const PCGState* st) {
+    if (st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > Gf.nx || j > Gf.ny || k > Gf.nz) return;
+    const int c = (int)Gf.idx(i, j, k);
+    const Nb o = neighbours(Gf, bc, i, j, k);
+    auto xp = [&](int ii, int jj, int kk, int cc) { return y[cc] + xc[Gc.idx((ii + 1) >> 1, (jj + 1) >> 1, (kk + 1) >> 1)]; };
+    // neighbour coordinates follow the offsets (mapped to the cell itself on Neumann faces)
+    const int ixm = (o.xm == -1) ? i - 1 : (o.xm == 0 ? i : Gf.nx), ixp = (o.xp == 1) ? i + 1 : (o.xp == 0 ? i : 1);
+    const int jym = (o.ym == -Gf.px) ? j - 1 : (o.ym == 0 ? j : Gf.ny), jyp = (o.yp == Gf.px) ? j + 1 : (o.yp == 0 ? j : 1);
+    const int kzm = (o.zm == -(int)Gf.pxy) ? k - 1 : (o.zm == 0 ? k : Gf.nz), kzp = (o.zp == (int)Gf.pxy) ? k + 1 : (o.zp == 0 ? k : 1);
+    const float xcv = xp(i, j, k, c);
+    const float ax = A.sx[c] * (xcv - xp(ixm, j, k, c + o.xm)) + A.sx[c + 1] * (xcv - xp(ixp, j, k, c + o.xp)) +
+                     A.sy[c] * (xcv - xp(i, jym, k, c + o.ym)) + A.sy[c + Gf.px] * (xcv - xp(i, jyp, k, c + o.yp)) +
+                     A.sz[c] * (xcv - xp(i, j, kzm, c + o.zm)) + A.sz[c + (int)Gf.pxy] * (xcv - xp(i, j, kzp, c + o.zp));
+    xout[c] = xcv + omega * (f[c] - ax) / A.dg[c];
+}
+
+// coarsest grid (<= 1024 cells): damped Jacobi sweeps in shared memory, one block
+__global__ void __launch_bounds__(1024) k_mg_coarsest(Geo G, BC bc, const float* __restrict__ f, MGOps A,
+                                                      float* y, int sweeps, float omega, const PCGState* st) {
+    if (st->done) return;
+    __shared__ float xs[2][1024];
+    const int n = G.nx * G.ny * G.nz;
+    const int t = threadIdx.x;
+    int i = 0, j = 0, k = 0, c = 0;
+    float fv = 0.f, dgv = 1.f, s[6] = {0, 0, 0, 0, 0, 0};
+    int nb[6] = {0, 0, 0, 0, 0, 0};
+    if (t < n) {
+        i = t % G.nx + 1; j = (t / G.nx) % G.ny + 1; k = t / (G.nx * G.ny) + 1;
+        c = (int)G.idx(i, j, k);
+        fv = f[c]; dgv = A.dg[c];
+        s[0] = A.sx[c]; s[1] = A.sx[c + 1]; s[2] = A.sy[c]; s[3] = A.sy[c + G.px]; s[4] = A.sz[c]; s[5] = A.sz[c + (int)G.pxy];
+        const int im = (i > 1) ? i - 1 : (bc.perx ? G.nx : i), ip = (i < G.nx) ? i + 1 : (bc.perx ? 1 : i);
+        const int jm = (j > 1) ? j - 1 : (bc.pery ? G.ny : j), jp = (j < G.ny) ? j + 1 : (bc.pery ? 1 : j);
+        const int km = (k > 1) ? k - 1 : (bc.perz ? G.nz : k), kp = (k < G.nz) ? k + 1 : (bc.perz ? 1 : k);
+        auto lin = [&](int a, int b, int d) { return (a - 1) + G.nx * ((b - 1) + G.ny * (d - 1)); };
+        nb[0] = lin(im, j, k); nb[1] = lin(ip, j, k); nb[2] = lin(i, jm, k); nb[3] = lin(i, jp, k); nb[4] = lin(i, j, km); nb[5] = lin(i, j, kp);
+        xs[0][t] = omega * fv / dgv;
+    }
+    __syncthreads();
+    int cur = 0;
+    for (int sw = 1; sw < sweeps; ++sw) {
+        if (t < n) {
+            const float xc = xs[cur][t];
+            float ax = 0.f;
+#pragma unroll
+            for (int m = 0; m < 6; ++m) ax += s[m] * (xc - xs[cur][nb[m]]);
+            xs[cur ^ 1][t] = xc + omega * (fv - ax) / dgv;
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    if (t < n) y[c] = xs[cur][t];
+}
+
+// ------------------------------------------------------------------------------------
+// inner PCG on A (FP32 vectors, FP64 reductions)
+// ------------------------------------------------------------------------------------
+// p = z + beta p_old (also at the neighbours), q = A p, p.q -> alpha
+__global__ void __launch_bounds__(256) k_pcg_spmv(Geo G, BC bc, const float* __restrict__ z,
+                                                  const float* __restrict__ p_old, float* __restrict__ p_new,
+                                                  float* __restrict__ q, MGOps A, PCGState* st, double* partial,
+                                                  unsigned int* counter) {
+    if (st->done) return;
+    const float beta = (float)st->beta;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    double dot = 0.;
+    if (i <= G.nx && j <= G.ny && k <= G.nz) {
+        const int c = (int)G.idx(i, j, k);
+        const Nb o = neighbours(G, bc, i, j, k);
+        auto pn = [&](int cc) { return z[cc] + beta * p_old[cc]; };
+        const float pc = pn(c);
+        const float qv = A.sx[c] * (pc - pn(c + o.xm)) + A.sx[c + 1] * (pc - pn(c + o.xp)) +
+                         A.sy[c] * (pc - pn(c + o.ym)) + A.sy[c + G.px] * (pc - pn(c + o.yp)) +
+                         A.sz[c] * (pc - pn(c + o.zm)) + A.sz[c + (int)G.pxy] * (pc - pn(c + o.zp));
+        p_new[c] = pc;
+        q[c] = qv;
+        dot = (double)pc * (double)qv;
+    }
+    double t, u;
+    if (reduce2_last(dot, 0.0, partial, counter, t, u) && flat_tid() == 0) {
+        st->pq = t;
+        st->alpha = st->rz / t;
+        if (!isfinite(st->alpha)) { st->status = SULI_ERR_NAN; st->done = 1; }
+    }
+}
+
+// x += alpha p, r -= alpha q, r.r and the inner stopping test
+__global__ void __launch_bounds__(256) k_pcg_update(Geo G, float* __restrict__ x, float* __restrict__ r,
+                                                    const float* __restrict__ p, const float* __restrict__ q,
+                                                    PCGState* st, double* partial, unsigned int* counter) {
+    if (st->done) return;
+    const float alpha = (float)st->alpha;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    double rr = 0.;
+    if (i <= G.nx && j <= G.ny && k <= G.nz) {
+        const int c = (int)G.idx(i, j, k);
+        x[c] = x[c] + alpha * p[c];
+        const float rv = r[c] - alpha * q[c];
+        r[c] = rv;
+        rr = (double)rv * (double)rv;
+    }
+    double t, u;
+    if (reduce2_last(rr, 0.0, partial, counter, t, u) && flat_tid() == 0) {
+        st->rr = t;
+        st->iters = st->iters + 1;
+        bool go = t > st->tol2;
+        if (st->iters >= st->maxit) go = false;
+        if (!isfinite(t)) { go = false; st->status = SULI_ERR_NAN; }
+        st->done = go ? 0 : 1;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// FP64 refinement: e <- e - sqrt(d) dp, r~ = A~ e - b~, r_u = sqrt(d) r~ (FP32)
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_mx_outer(Geo G, BC bc, const double* __restrict__ e_in,
+                                                  const float* __restrict__ dp, const double* __restrict__ d,
+                                                  const double* __restrict__ ax, const double* __restrict__ ay,
+                                                  const double* __restrict__ az, const double* __restrict__ b,
+                                                  double* __restrict__ e_out, float* __restrict__ ru, int apply,
+                                                  CGState* cg, PCGState* pst, double* partial, unsigned int* counter) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    double rr = 0., ru2 = 0.;
+    if (i <= G.nx && j <= G.ny && k <= G.nz) {
+        const int c = (int)G.idx(i, j, k);
+        const Nb o = neighbours(G, bc, i, j, k);
+        auto en = [&](int cc) { return apply ? e_in[cc] - sqrt(d[cc]) * (double)dp[cc] : e_in[cc]; };
+        const double ec = en(c);
+        const double rv = ec - ax[c + 1] * en(c + o.xp) - ax[c] * en(c + o.xm) - ay[c + G.px] * en(c + o.yp) -
+                          ay[c] * en(c + o.ym) - az[c + (int)G.pxy] * en(c + o.zp) - az[c] * en(c + o.zm) - b[c];
+        e_out[c] = ec;
+        const double u = sqrt(d[c]) * rv;
+        ru[c] = (float)u;
+        rr = rv * rv;
+        ru2 = u * u;
+    }
+    double t1, t2;
+    if (reduce2_last(rr, ru2, partial, counter, t1, t2) && flat_tid() == 0) {
+        cg->rr = t1;
+        if (apply) cg->iters = cg->iters + 1;
+        cg->done = (t1 > cg->thr) ? 0 : 1;
+        if (!isfinite(t1)) { cg->status = SULI_ERR_NAN; cg->done = 1; }
+        pst->rr0 = t2;
+    }
+}
+
+__global__ void k_pcg_init(PCGState* st, double inner_tol, int maxit) {
+    st->tol2 = inner_tol * inner_tol * st->rr0;
+    st->iters = 0;
+    st->done = 0;
+    st->status = 0;
+    st->maxit = maxit;
+    st->beta = 0.;
+    st->rz = 0.;
+}
+
+__global__ void k_zero_f(float* a, long long n) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) a[q] = 0.f;
+}
+
+// ------------------------------------------------------------------------------------
+// launchers
+// ------------------------------------------------------------------------------------
+static const dim3 kB2(32, 8, 1);
+static inline dim3 cells3(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
+static inline MGOps ops(const MGLevel& L) { return MGOps{L.sx, L.sy, L.sz, L.dg}; }
+
+void launch_mx_setup(suli_ctx* c) {
+    ProfScope ps(c, SULI_K_CG_SETUP, (int)c->mg.size());
+    MGLevel& L0 = c->mg[0];
+    k_mx_faces0<<<cells3(L0.g), kB2, 0, c->stream>>>(L0.g, c->bc, c->f[SULI_F_RHO], c->dt / (c->P.dx * c->P.dx),
+                                                     c->dt / (c->P.dy * c->P.dy), c->dt / (c->P.dz * c->P.dz), L0.sx, L0.sy,
+                                                     L0.sz, L0.dg);
+    for (size_t l = 1; l < c->mg.size(); ++l) {
+        MGLevel& F = c->mg[l - 1];
+        MGLevel& C = c->mg[l];
+        k_mg_coarsen<<<cells3(C.g), kB2, 0, c->stream>>>(F.g, C.g, c->bc, F.sx, F.sy, F.sz, C.sx, C.sy, C.sz, C.dg);
+    }
+}
+
+// r_u from the FP64 first residual (no correction applied); also initialises the inner solve
+void launch_mx_residual(suli_ctx* c, const double* e_in, double* e_out, bool apply) {
+    ProfScope ps(c, SULI_K_REFINE, 1);
+    const Geo& G = c->g;
+    k_mx_outer<<<cells3(G), kB2, 0, c->stream>>>(G, c->bc, e_in, c->pc_x, c->cg_d, c->cg_ax, c->cg_ay, c->cg_az,
+                                                 c->cg_b, e_out, c->pc_r, apply ? 1 : 0, c->cg, c->pcg,
+                                                 c->red_partial, c->red_counter);
+}
+
+void launch_pcg_init(suli_ctx* c, int maxit) {
+    k_pcg_init<<<1, 1, 0, c->stream>>>(c->pcg, c->P.inner_tol, maxit);
+    const long long n = (long long)c->g.n;
+    k_zero_f<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->pc_x, n);
+}
+
+// z = M r: one V-cycle; the last level-0 sweep also forms r.z and beta
+void launch_vcycle(suli_ctx* c) {
+    const float om = 0.8f;
+    const int L = (int)c->mg.size();
+    const BC bc = c->bc;
+    for (int l = 0; l < L - 1; ++l) {
+        MGLevel& M = c->mg[l];
+        const float* f = (l == 0) ? c->pc_r : M.f;
+        k_mg_jac0<<<cells3(M.g), kB2, 0, c->stream>>>(M.g, f, M.dg, M.x, om, c->pcg);
+        k_mg_jac<<<cells3(M.g), kB2, 0, c->stream>>>(M.g, bc, M.x, f, ops(M), M.y, om, c->pcg, 0, c->red_partial,
+                                                     c->red_counter);
+        MGLevel& C = c->mg[l + 1];
+        k_mg_restrict<<<cells3(C.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, f, ops(M), C.f, c->pcg);
+    }
+    MGLevel& B = c->mg[L - 1];
+    if (L == 1) {   // a single level: coarsest sweeps, then one more sweep that forms r.z
+        k_mg_coarsest<<<1, 1024, 0, c->stream>>>(B.g, bc, c->pc_r, ops(B), B.x, c->coarse_sweeps, om, c->pcg);
+        k_mg_jac<<<cells3(B.g), kB2, 0, c->stream>>>(B.g, bc, B.x, c->pc_r, ops(B), B.y, om, c->pcg, 1,
+                                                     c->red_partial, c->red_counter);
+        return;
+    }
+    k_mg_coarsest<<<1, 1024, 0, c->stream>>>(B.g, bc, B.f, ops(B), B.y, c->coarse_sweeps, om, c->pcg);
+    for (int l = L - 2; l >= 0; --l) {
+        MGLevel& M = c->mg[l];
+        MGLevel& C = c->mg[l + 1];
+        const float* f = (l == 0) ? c->pc_r : M.f;
+        k_mg_prolong_jac<<<cells3(M.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, C.y, f, ops(M), M.x, om, c->pcg);
+        k_mg_jac<<<cells3(M.g), kB2, 0, c->stream>>>(M.g, bc, M.x, f, ops(M), M.y, om, c->pcg, l == 0 ? 1 : 0,
+                                                     c->red_partial, c->red_counter);
+    }
+}
+
+void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new) {
+    const Geo& G = c->g;
+    MGLevel& M0 = c->mg[0];
+    {
+        ProfScope ps(c, SULI_K_CG_SPMV, 1);
+        k_pcg_spmv<<<cells3(G), kB2, 0, c->stream>>>(G, c->bc, M0.y, p_old, p_new, c->pc_q, ops(M0), c->pcg,
+                                                     c->red_partial, c->red_counter);
+    }
+    {
+        ProfScope ps(c, SULI_K_CG_UPDATE, 1);
+        k_pcg_update<<<cells3(G), kB2, 0, c->stream>>>(G, c->pc_x, c->pc_r, p_new, c->pc_q, c->pcg, c->red_partial,
+                                                       c->red_counter);
+    }
+    ProfScope ps(c, SULI_K_MG, 5 * ((int)c->mg.size() - 1) + 1);
+    launch_vcycle(c);
+}
+
+}  // namespace suli

@@ -1,0 +1,87 @@
+// reduce.cuh — deterministic block and grid reductions shared by the kernel units.
+//
+// A block reduces with a fixed warp-shuffle tree; each block stores its partial, and the last
+// block to arrive (atomic counter) sums all partials in block order.  No floating-point
+// atomics, so a launch with the same configuration is bit-reproducible.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace suli {
+
+__device__ __forceinline__ int flat_tid() {
+    return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+}
+__device__ __forceinline__ int flat_bid() {
+    return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+}
+
+// Sum over the block; the result is valid in thread 0.  Fixed reduction tree.
+static __device__ double block_sum(double v) {
+    __shared__ double sh[32];
+    const int tid = flat_tid();
+    const int nt = blockDim.x * blockDim.y * blockDim.z;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((tid & 31) == 0) sh[tid >> 5] = v;
+    __syncthreads();
+    const int nw = (nt + 31) >> 5;
+    v = (tid < nw) ? sh[tid] : 0.0;
+    if (tid < 32) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+static __device__ double block_max(double v) {
+    __shared__ double sh[32];
+    const int tid = flat_tid();
+    const int nt = blockDim.x * blockDim.y * blockDim.z;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if ((tid & 31) == 0) sh[tid >> 5] = v;
+    __syncthreads();
+    const int nw = (nt + 31) >> 5;
+    v = (tid < nw) ? sh[tid] : 0.0;
+    if (tid < 32) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+// Two block partials per block; the last block to arrive sums all partials in block order
+// and returns true (totals valid in thread 0 of that block).  `is_max` selects max.
+static __device__ bool reduce2_last(double a, double b, double* partial, unsigned int* counter, double& ta,
+                                    double& tb, bool is_max = false) {
+    __shared__ bool last;
+    const int tid = flat_tid();
+    const int nt = blockDim.x * blockDim.y * blockDim.z;
+    const int bid = flat_bid();
+    const int nb = gridDim.x * gridDim.y * gridDim.z;
+    a = is_max ? block_max(a) : block_sum(a);
+    b = is_max ? block_max(b) : block_sum(b);
+    if (tid == 0) {
+        partial[2 * bid] = a;
+        partial[2 * bid + 1] = b;
+        __threadfence();
+        const unsigned int t = atomicAdd(counter, 1u);
+        last = (t == (unsigned int)(nb - 1));
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double sa = 0.0, sb = 0.0;
+    for (int q = tid; q < nb; q += nt) {
+        const double pa = __ldcg(&partial[2 * q]), pb = __ldcg(&partial[2 * q + 1]);
+        if (is_max) { sa = fmax(sa, pa); sb = fmax(sb, pb); }
+        else { sa += pa; sb += pb; }
+    }
+    sa = is_max ? block_max(sa) : block_sum(sa);
+    sb = is_max ? block_max(sb) : block_sum(sb);
+    if (tid == 0) { ta = sa; tb = sb; *counter = 0u; }
+    return true;
+}
+
+}  // namespace suli

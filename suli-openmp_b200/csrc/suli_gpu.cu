@@ -114,7 +114,20 @@ int validate(const suli_params* p, std::string& why) {
     if (p->der != 1 || p->adv_type != 1) { why = "only der = 1, adv_type = 1 (classic upwind advection) are built"; return SULI_ERR_UNSUPPORTED; }
     if (p->m_turb != 0 && p->m_turb != 1) { why = "only m_turb 0 and 1 are built"; return SULI_ERR_UNSUPPORTED; }
     if (p->t_tempo < 0 || p->t_tempo > 3) { why = "t_tempo out of range"; return SULI_ERR_ARG; }
-    if (p->precision != 0) { why = "precision 1 (mixed) is not built in this library version"; return SULI_ERR_UNSUPPORTED; }
+    if (p->precision != 0 && p->precision != 1) { why = "precision must be 0 (FP64) or 1 (mixed)"; return SULI_ERR_ARG; }
+    if (p->precision == 1) {
+        if (p->cg_stop != 1) { why = "precision 1 stops on the relative FP64 residual (cg_stop = 1)"; return SULI_ERR_ARG; }
+        if (p->refine_maxit < 1) { why = "refine_maxit must be >= 1"; return SULI_ERR_ARG; }
+        if (!(p->inner_tol > 0 && p->inner_tol < 1)) { why = "inner_tol must lie in (0, 1)"; return SULI_ERR_ARG; }
+        int nx = p->nx, ny = p->ny, nz = p->nz;
+        while ((long long)nx * ny * nz > 1024 && nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0 && nx >= 4 && ny >= 4 && nz >= 4) {
+            nx /= 2; ny /= 2; nz /= 2;
+        }
+        if ((long long)nx * ny * nz > 1024) {
+            why = "precision 1: the grid must halve to <= 1024 cells for the multigrid coarsest level";
+            return SULI_ERR_UNSUPPORTED;
+        }
+    }
     if (p->cg_stop != 0 && p->cg_stop != 1) { why = "cg_stop must be 0 or 1"; return SULI_ERR_ARG; }
     if (p->cg_maxit < 0) { why = "cg_maxit must be >= 0"; return SULI_ERR_ARG; }
     if (p->reinit_maxit < 1) { why = "reinit_maxit must be >= 1"; return SULI_ERR_ARG; }
@@ -214,6 +227,36 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
     if ((e = cudaMemsetAsync(c->cg, 0, sizeof(CGState), c->stream)) != cudaSuccess) return bail(e, "memset");
     if ((e = cudaMallocHost(&c->cg_host, 2 * sizeof(CGState))) != cudaSuccess) return bail(e, "pinned");
     if ((e = cudaMallocHost(&c->host_scalars, 16 * sizeof(double))) != cudaSuccess) return bail(e, "pinned");
+    if (p->precision == 1) {
+        // FP32 multigrid hierarchy + inner PCG vectors, one float arena
+        std::vector<Geo> gs;
+        int nx = p->nx, ny = p->ny, nz = p->nz;
+        gs.push_back(make_geo(nx, ny, nz));
+        while ((long long)nx * ny * nz > 1024 && nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0 && nx >= 4 && ny >= 4 && nz >= 4) {
+            nx /= 2; ny /= 2; nz /= 2;
+            gs.push_back(make_geo(nx, ny, nz));
+        }
+        size_t tot = 5 * (size_t)gs[0].n;
+        for (auto& g : gs) tot += 7 * (size_t)g.n;
+        if ((e = cudaMalloc(&c->f32_arena, tot * sizeof(float))) != cudaSuccess) return bail(e, "f32 arena");
+        if ((e = cudaMemsetAsync(c->f32_arena, 0, tot * sizeof(float), c->stream)) != cudaSuccess) return bail(e, "memset");
+        float* q = c->f32_arena;
+        auto take = [&](size_t n) { float* r = q; q += n; return r; };
+        c->pc_x = take(gs[0].n); c->pc_r = take(gs[0].n); c->pc_pa = take(gs[0].n); c->pc_pb = take(gs[0].n);
+        c->pc_q = take(gs[0].n);
+        for (auto& g : gs) {
+            MGLevel L;
+            L.g = g;
+            L.sx = take(g.n); L.sy = take(g.n); L.sz = take(g.n); L.dg = take(g.n);
+            L.f = take(g.n); L.x = take(g.n); L.y = take(g.n);
+            c->mg.push_back(L);
+        }
+        if ((e = cudaMalloc(&c->cg_e2, per * sizeof(double))) != cudaSuccess) return bail(e, "e2");
+        if ((e = cudaMemsetAsync(c->cg_e2, 0, per * sizeof(double), c->stream)) != cudaSuccess) return bail(e, "memset");
+        if ((e = cudaMalloc(&c->pcg, sizeof(PCGState))) != cudaSuccess) return bail(e, "pcg state");
+        if ((e = cudaMemsetAsync(c->pcg, 0, sizeof(PCGState), c->stream)) != cudaSuccess) return bail(e, "memset");
+        if ((e = cudaMallocHost(&c->pcg_host, 2 * sizeof(PCGState))) != cudaSuccess) return bail(e, "pinned");
+    }
     if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bail(e, "sync");
     c->dt = p->dt;
     c->dt1 = p->dt1;
@@ -228,6 +271,8 @@ int suli_destroy(suli_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->cg_graph) cudaGraphExecDestroy(c->cg_graph);
+    for (auto& g : c->pcg_graph)
+        if (g) cudaGraphExecDestroy(g);
     for (auto& e : c->prof.ev) cudaEventDestroy(e);
     cudaFree(c->arena);
     for (int f = SULI_F_BXX0; f < SULI_F_COUNT; ++f) cudaFree(c->f[f]);
@@ -235,6 +280,10 @@ int suli_destroy(suli_ctx* c) {
     cudaFree(c->red_counter);
     cudaFree(c->red_out);
     cudaFree(c->cg);
+    cudaFree(c->f32_arena);
+    cudaFree(c->cg_e2);
+    cudaFree(c->pcg);
+    if (c->pcg_host) cudaFreeHost(c->pcg_host);
     if (c->cg_host) cudaFreeHost(c->cg_host);
     if (c->host_scalars) cudaFreeHost(c->host_scalars);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -486,17 +535,17 @@ int suli_contorno(suli_ctx* c, int nlock) {
 }
 
 // graddin (9_grad.f90:10-278)
-int suli_graddin(suli_ctx* c, int* iters, double* resid) {
-    if (!c) return SULI_ERR_ARG;
-    cudaSetDevice(c->device);
-    launch_cg_setup(c);
-    CHECK_LAUNCH(c);
-    // iteration 1 uses p_old = r with beta = 0 (erroppr = erropr, :172)
-    launch_cg_iter(c, c->cg_r, c->cg_pa);
-    CHECK_LAUNCH(c);
+}  // extern "C"
+
+namespace {
+// Enqueue iterations in batches with a device-resident `done` flag: launches after
+// convergence return at once, and the host polls the flag through a pinned mirror one batch
+// behind the GPU, so the stream never drains while it waits.  `launch(parity)` enqueues one
+// iteration; iteration 0 is launched by the caller.
+template <class State, class Launch>
+int run_batches(suli_ctx* c, const State* dev, State* host2, long long cap, int batch, Launch launch) {
     long long issued = 1;
-    int parity = 0;   // next p_old: 0 -> pa, 1 -> pb
-    const long long cap = (long long)c->P.cg_maxit + 2;
+    int parity = 0;
     int slot = 0;
     cudaEvent_t ev[2];
     cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
@@ -504,21 +553,19 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
     bool pending[2] = {false, false};
     bool finished = false;
     while (!finished) {
-        // enqueue one batch; kernels after convergence return at once
-        for (int b = 0; b < c->cg_batch && issued < cap; ++b, ++issued) {
-            if (parity == 0) launch_cg_iter(c, c->cg_pa, c->cg_pb);
-            else launch_cg_iter(c, c->cg_pb, c->cg_pa);
+        for (int b = 0; b < batch && issued < cap; ++b, ++issued) {
+            launch(parity);
             parity ^= 1;
         }
         CHECK_LAUNCH(c);
-        cudaMemcpyAsync(&c->cg_host[slot], c->cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream);
+        cudaMemcpyAsync(&host2[slot], dev, sizeof(State), cudaMemcpyDeviceToHost, c->stream);
         cudaEventRecord(ev[slot], c->stream);
         pending[slot] = true;
         const int prev = slot ^ 1;
         if (pending[prev]) {
             cudaEventSynchronize(ev[prev]);
             pending[prev] = false;
-            if (c->cg_host[prev].done) finished = true;
+            if (host2[prev].done) finished = true;
         }
         if (issued >= cap) {
             cudaEventSynchronize(ev[slot]);
@@ -531,7 +578,97 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
         if (pending[s]) cudaEventSynchronize(ev[s]);
         cudaEventDestroy(ev[s]);
     }
-    launch_cg_final(c);
+    CHECK_LAUNCH(c);
+    return SULI_OK;
+}
+
+// Capture one inner PCG iteration (SpMV, update, V-cycle: every kernel reads its scalars from
+// device memory, so the launch parameters never change) into a graph per ping-pong parity.
+int ensure_pcg_graphs(suli_ctx* c) {
+    if (c->pcg_graph[0] && c->pcg_graph[1]) return SULI_OK;
+    for (int par = 0; par < 2; ++par) {
+        cudaGraph_t g = nullptr;
+        CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        if (par == 0) launch_pcg_iter(c, c->pc_pa, c->pc_pb);
+        else launch_pcg_iter(c, c->pc_pb, c->pc_pa);
+        CUDA_TRY(c, cudaStreamEndCapture(c->stream, &g));
+        const cudaError_t e = cudaGraphInstantiate(&c->pcg_graph[par], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(c, SULI_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    const int L = (int)c->mg.size();
+    c->pcg_graph_kernels = 2 + (L == 1 ? 2 : 5 * (L - 1) + 1);
+    return SULI_OK;
+}
+
+// Mixed-precision solve: FP64 refinement around an FP32 multigrid-preconditioned CG.
+int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
+    if (int rg = ensure_pcg_graphs(c)) return rg;
+    launch_cg_setup(c);   // FP64 diagonal, coefficients, b~, first residual and threshold
+    launch_mx_setup(c);   // FP32 faces of every multigrid level
+    double* ecur = c->cg_e;
+    double* enext = c->cg_e2;
+    launch_mx_residual(c, ecur, enext, false);
+    std::swap(ecur, enext);
+    CHECK_LAUNCH(c);
+    long long inner_total = 0;
+    int outer = 0, status = SULI_OK;
+    while (true) {
+        int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
+        if (r != SULI_OK) return r;
+        if (c->cg_host[0].status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the Poisson solve");
+        if (c->cg_host[0].done) break;
+        if (outer >= c->P.refine_maxit) { status = SULI_WARN_CG_MAXIT; break; }
+        launch_pcg_init(c, c->inner_maxit);
+        {
+            ProfScope ps(c, SULI_K_MG, 5 * ((int)c->mg.size() - 1) + 1);
+            launch_vcycle(c);
+        }
+        launch_pcg_iter(c, c->mg[0].y, c->pc_pa);   // p_old = z with beta = 0
+        r = run_batches(c, c->pcg, c->pcg_host, (long long)c->inner_maxit + 2, c->inner_batch, [&](int parity) {
+            ProfScope ps(c, SULI_K_MG, c->pcg_graph_kernels);
+            cudaGraphLaunch(c->pcg_graph[parity], c->stream);
+        });
+        if (r != SULI_OK) return r;
+        r = sync_read(c, c->pcg, c->pcg_host, sizeof(PCGState));
+        if (r != SULI_OK) return r;
+        if (c->pcg_host[0].status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the inner solve");
+        inner_total += c->pcg_host[0].iters;
+        launch_mx_residual(c, ecur, enext, true);
+        std::swap(ecur, enext);
+        CHECK_LAUNCH(c);
+        ++outer;
+    }
+    c->last_outer_iters = outer;
+    launch_cg_final(c, ecur);
+    CHECK_LAUNCH(c);
+    int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
+    if (r != SULI_OK) return r;
+    const CGState& s = c->cg_host[0];
+    c->prof.cg_iters += inner_total;
+    if (iters) *iters = (int)inner_total;
+    if (resid) *resid = (s.bb > 0.) ? std::sqrt(s.rr / s.bb) : 0.;
+    return status;
+}
+}  // namespace
+
+extern "C" {
+
+int suli_graddin(suli_ctx* c, int* iters, double* resid) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->P.precision == 1) return graddin_mixed(c, iters, resid);
+    launch_cg_setup(c);
+    CHECK_LAUNCH(c);
+    // iteration 1 uses p_old = r with beta = 0 (erroppr = erropr, :172)
+    launch_cg_iter(c, c->cg_r, c->cg_pa);
+    CHECK_LAUNCH(c);
+    int r0 = run_batches(c, c->cg, c->cg_host, (long long)c->P.cg_maxit + 2, c->cg_batch, [&](int parity) {
+        if (parity == 0) launch_cg_iter(c, c->cg_pa, c->cg_pb);
+        else launch_cg_iter(c, c->cg_pb, c->cg_pa);
+    });
+    if (r0 != SULI_OK) return r0;
+    launch_cg_final(c, c->cg_e);
     CHECK_LAUNCH(c);
     int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
     if (r != SULI_OK) return r;

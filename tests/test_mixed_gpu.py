@@ -1,0 +1,73 @@
+"""GPU tests of the mixed-precision pressure solve (precision = 1): FP32 multigrid-
+preconditioned CG inside FP64 iterative refinement, stopping on the same FP64 relative
+residual as the plain path.  Each result is checked against the FP64 CPU oracle solved to a
+tighter tolerance; the error bars are stated per test."""
+import numpy as np
+import pytest
+
+from helpers import STATE_FIELDS, load_state, rel_err, seeded_state, small_params
+
+pytestmark = pytest.mark.gpu
+
+
+def _prepared(pkg, orc, p, seed):
+    """Oracle-derived state (rho, viscosities, ghosts) uploaded to a GPU context."""
+    o = orc.Oracle(p)
+    st = seeded_state(p, seed)
+    load_state(o, st)
+    o.heaviside(); o.mod_ls1(); o.visco(); o.contorno(1)
+    full = {f: o.download(f) for f in STATE_FIELDS}
+    return o, full
+
+
+@pytest.mark.parametrize("shape", [(16, 12, 8), (14, 12, 10), (32, 16, 24)])
+def test_mixed_poisson_reaches_fp64_tolerance(pkg, orc, shape):
+    """Relative FP64 residual <= 1e-10 (the solver's own test), and the projected velocity
+    within 1e-7 of the oracle's FP64 CG at 1e-13 (both solutions are within the tolerance of
+    the exact discrete one)."""
+    p = small_params(nx=shape[0], ny=shape[1], nz=shape[2])
+    p.cg_stop, p.cg_maxit = 1, 20000
+    q = p.copy()
+    q.precision, q.cg_tol, q.inner_tol, q.refine_maxit = 1, 1e-10, 1e-3, 30
+    p.cg_tol = 1e-13
+    o, st = _prepared(pkg, orc, p, 31)
+    g = pkg.Solver(q)
+    load_state(g, st)
+    for m in (g, o):
+        m.set_dt(1e-3)
+        m.contorno(2)
+    ng, rg = g.graddin()
+    no, ro = o.graddin()
+    assert rg <= 1e-10, rg
+    assert ng < no, (ng, no)            # the preconditioned inner solve needs fewer iterations
+    for m in (g, o):
+        m.posdin()
+        m.contorno(1)
+    for f in ("u", "v", "w"):
+        assert rel_err(g.download(f), o.download(f)) <= 1e-7, f
+    assert g.est() <= 1e-6
+
+
+def test_mixed_steps_track_fp64(pkg, orc):
+    """Three dam-break steps with the mixed solve at 1e-10 against the FP64 oracle at 1e-12:
+    every field within 1e-6 relative (the difference is the solve tolerance, propagated)."""
+    p, init = pkg.cases.dam_break(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-12)
+    q = p.copy()
+    q.precision, q.cg_tol, q.inner_tol, q.refine_maxit = 1, 1e-10, 1e-3, 30
+    g = pkg.Solver(q)
+    o = orc.Oracle(p)
+    init(g)
+    init(o)
+    for it in range(1, 4):
+        sg, so = g.step(it), o.step(it)
+        assert sg["status"] == 0
+        assert max(sg["cg_resid"]) <= 1e-10
+    for f in ("u", "v", "w", "ls", "rho"):
+        assert rel_err(g.download(f), o.download(f)) <= 1e-6, f
+
+
+def test_mixed_rejects_unsupported(pkg):
+    p = small_params(nx=15, ny=13, nz=11)   # cannot halve to <= 1024 cells
+    p.precision, p.cg_stop = 1, 1
+    with pytest.raises(pkg.SuliError):
+        pkg.Solver(p)
