@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--dx", type=float, default=0.005)
     ap.add_argument("--cg-tol", type=float, default=1e-8)
     ap.add_argument("--inner-tol", type=float, default=1e-3, help="relative tolerance of each FP32 inner solve")
+    ap.add_argument("--path", choices=["both", "plain", "mixed"], default="both",
+                    help="time both solver paths (headline = mixed) or one of them (for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-cap", type=int, default=20, help="CG iterations per solve in the CPU sample")
@@ -367,12 +369,20 @@ def run_ours(args):
     pkg = load_pkg()
     p, init = pkg.cases.sloshing(nx=args.nx, ny=args.ny, nz=args.nz, dx=args.dx, cg_tol=args.cg_tol)
     # plain FP64 path (the reference's Jacobi-scaled CG): timed for the comparison
-    plain = time_path(args, dist, pkg, p, init, dev)
-    plain["solver"].close()
-    roof_plain = cg_roofline(p, plain["prof"])
-    # headline path: mixed precision (FP32 multigrid-preconditioned inner CG, FP64 refinement)
     q = mixed_params(p, args)
-    head = time_path(args, dist, pkg, q, init, dev)
+    if args.path in ("both", "plain"):
+        plain = time_path(args, dist, pkg, p, init, dev)
+        if args.path == "plain":
+            head = plain
+            q = p
+        else:
+            plain["solver"].close()
+        roof_plain = cg_roofline(p, plain["prof"])
+    if args.path in ("both", "mixed"):
+        # headline path: mixed precision (FP32 multigrid-preconditioned inner CG, FP64 refinement)
+        head = time_path(args, dist, pkg, q, init, dev)
+        if args.path == "mixed":
+            plain, roof_plain = head, None
     s = head["solver"]
     it = head["it"]
     value, ms, prof, stats, clk = head["value"], head["ms"], head["prof"], head["stats"], head["clocks"]
@@ -434,6 +444,10 @@ def run_ours(args):
                            "gpu_launches": plain["launches"], "kernels": plain["kernels"]},
             "speedup_vs_plain_fp64": value / plain["value"],
         }
+        if args.path != "both":   # a single path timed (profiling runs): no comparison block
+            line.pop("plain_fp64")
+            line.pop("speedup_vs_plain_fp64")
+            line["config"]["path"] = args.path
         print(json.dumps(line), flush=True)
     dist.close()
     return 0

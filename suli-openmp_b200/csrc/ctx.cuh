@@ -200,6 +200,7 @@ void launch_mx_residual(suli_ctx* c, const double* e_in, double* e_out, bool app
 void launch_pcg_init(suli_ctx* c, int maxit);
 void launch_vcycle(suli_ctx* c);
 void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new);
+int vcycle_kernels(const suli_ctx* c);
 void launch_posdin(suli_ctx* c);
 void launch_est(suli_ctx* c);
 void launch_fill(suli_ctx* c, double* a, double v);

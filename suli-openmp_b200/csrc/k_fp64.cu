@@ -603,21 +603,25 @@ __global__ void k_bc_z(Geo G, BC bc, BCArgs A) {
         if (bc.zf == 2) FIDX(w, i, j, nz1 + 1) = FIDX(w, i, j, nz1 - 1);
         if (bc.zf == 3) FIDX(w, i, j, nz1 + 1) = A.pl.bzzf1[i + lv * j];
     }
-    // capture: each thread copies within its own (i,j) column, after its own z writes
+    // capture of the k = 2 plane: each thread copies within its own (i,j) column, after its z writes
     if (bc.z0 == 2) {
         if (i <= nx + 2 && j <= ny + 1) FIDX(A.ub, i, j, 2) = FIDX(A.u, i, j, 2);
         if (i <= nx + 1 && j <= ny + 2) FIDX(A.vb, i, j, 2) = FIDX(A.v, i, j, 2);
         if (i <= nx + 1 && j <= ny + 1) FIDX(A.wb, i, j, 2) = FIDX(A.w, i, j, 2);
     }
-    if (bc.y0 == 2 && j == 2) {
-        if (i <= nx + 2) for (int k = 0; k <= nz + 1; ++k) FIDX(A.ub, i, 2, k) = FIDX(A.u, i, 2, k);
-        if (i <= nx + 1) for (int k = 0; k <= nz + 1; ++k) FIDX(A.vb, i, 2, k) = FIDX(A.v, i, 2, k);
-        if (i <= nx + 1) for (int k = 0; k <= nz + 2; ++k) FIDX(A.wb, i, 2, k) = FIDX(A.w, i, 2, k);
-    }
-    if (bc.yf == 2 && j == ny) {
-        if (i <= nx + 2) for (int k = 0; k <= nz + 1; ++k) FIDX(A.ub, i, ny, k) = FIDX(A.u, i, ny, k);
-        if (i <= nx + 1) for (int k = 0; k <= nz + 1; ++k) FIDX(A.vb, i, ny, k) = FIDX(A.v, i, ny, k);
-        if (i <= nx + 1) for (int k = 0; k <= nz + 2; ++k) FIDX(A.wb, i, ny, k) = FIDX(A.w, i, ny, k);
+}
+
+// capture of the j = 2 and j = ny planes (:254-264), after the z phase, thread per (i,k)
+__global__ void k_bc_capture_y(Geo G, BC bc, BCArgs A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    for (int side = 0; side < 2; ++side) {
+        if (side == 0 && bc.y0 != 2) continue;
+        if (side == 1 && bc.yf != 2) continue;
+        const int j = (side == 0) ? 2 : ny;
+        if (i <= nx + 2 && k <= nz + 1) FIDX(A.ub, i, j, k) = FIDX(A.u, i, j, k);
+        if (i <= nx + 1 && k <= nz + 1) FIDX(A.vb, i, j, k) = FIDX(A.v, i, j, k);
+        if (i <= nx + 1 && k <= nz + 2) FIDX(A.wb, i, j, k) = FIDX(A.w, i, j, k);
     }
 }
 
@@ -1036,11 +1040,13 @@ void launch_contorno(suli_ctx* c, int nlock) {
     A.pl = c->planes();
     A.nlock = nlock;
     const dim3 b2(32, 8);
-    ProfScope ps(c, SULI_K_CONTORNO, nlock == 2 ? 7 : 4);
+    const bool capy = (c->bc.y0 == 2 || c->bc.yf == 2);
+    ProfScope ps(c, SULI_K_CONTORNO, (nlock == 2 ? 7 : 4) + (capy ? 1 : 0));
     k_prd_ghosts<<<grid3(G.nx + 2, G.ny + 2, G.nz + 2, kBlk), kBlk, 0, c->stream>>>(G, c->bc, A.prd1);
     k_bc_y<<<grid3(G.nx + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
     k_bc_x<<<grid3(G.ny + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
     k_bc_z<<<grid3(G.nx + 3, G.ny + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
+    if (capy) k_bc_capture_y<<<grid3(G.nx + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
     if (nlock == 2) {
         k_bc_ny<<<grid3(G.nx + 2, G.nz + 2, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
         k_bc_nx<<<grid3(G.ny + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);

@@ -122,6 +122,124 @@ struct MGOps {
     const float *sx, *sy, *sz, *dg;
 };
 
+// Column kernels: a thread owns kKZ cells of one (i,j) column; z neighbours come from the
+// column's registers (with the ghost map on k), x/y neighbours through L1, and all loads of
+// the column are independent.
+constexpr int kKZ = 4;
+struct Col {
+    int i, j, k0, c0;
+    Nb o;      // x/y offsets (z offsets unused)
+    bool in;
+};
+__device__ __forceinline__ Col column(const Geo& G, const BC& bc) {
+    Col q;
+    q.i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    q.j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    q.k0 = blockIdx.z * kKZ + 1;
+    q.in = (q.i <= G.nx && q.j <= G.ny);
+    q.c0 = kBase + (q.i - 1) + G.px * q.j;
+    q.o = neighbours(G, bc, q.in ? q.i : 1, q.in ? q.j : 1, 1);
+    return q;
+}
+// load a field along the column, planes k0-1 .. k0+kKZ (ghost-mapped)
+template <class F>
+__device__ __forceinline__ void load_col(const Geo& G, const BC& bc, const Col& q, F val, float v[kKZ + 2]) {
+#pragma unroll
+    for (int m = 0; m < kKZ + 2; ++m) v[m] = val(q.c0 + (int)G.pxy * map_any(q.k0 - 1 + m, G.nz, bc.perz));
+}
+static inline dim3 colgrid(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kKZ - 1) / kKZ); }
+
+// two damped Jacobi sweeps from zero in one pass: x1 = w f/dg, y = x1 + w (f - A x1)/dg
+__global__ void __launch_bounds__(256) k_mg_pre(Geo G, BC bc, const float* __restrict__ f, MGOps A,
+                                                float* __restrict__ y, float omega, const PCGState* st) {
+    if (st->done) return;
+    const Col q = column(G, bc);
+    if (!q.in) return;
+    const int px = G.px, pxy = (int)G.pxy;
+    auto x1 = [&](int cc) { return omega * f[cc] / A.dg[cc]; };
+    float col[kKZ + 2];
+    load_col(G, bc, q, x1, col);
+#pragma unroll
+    for (int m = 0; m < kKZ; ++m) {
+        if (q.k0 + m > G.nz) break;
+        const int c = q.c0 + pxy * (q.k0 + m);
+        const float xc = col[m + 1];
+        const float ax = A.sx[c] * (xc - x1(c + q.o.xm)) + A.sx[c + 1] * (xc - x1(c + q.o.xp)) +
+                         A.sy[c] * (xc - x1(c + q.o.ym)) + A.sy[c + px] * (xc - x1(c + q.o.yp)) +
+                         A.sz[c] * (xc - col[m]) + A.sz[c + pxy] * (xc - col[m + 2]);
+        y[c] = xc + omega * (f[c] - ax) / A.dg[c];
+    }
+}
+
+// x_out = x_in + w (f - A x_in)/dg; with do_dot (last sweep of level 0) also f.x_out -> rz, beta
+__global__ void __launch_bounds__(256) k_mg_jacc(Geo G, BC bc, const float* __restrict__ xin, const float* __restrict__ f,
+                                                 MGOps A, float* __restrict__ xout, float omega, PCGState* st, int do_dot,
+                                                 double* partial, unsigned int* counter) {
+    if (st->done) return;
+    const Col q = column(G, bc);
+    double dot = 0.;
+    if (q.in) {
+        const int px = G.px, pxy = (int)G.pxy;
+        float col[kKZ + 2];
+        load_col(G, bc, q, [&](int cc) { return xin[cc]; }, col);
+#pragma unroll
+        for (int m = 0; m < kKZ; ++m) {
+            if (q.k0 + m > G.nz) break;
+            const int c = q.c0 + pxy * (q.k0 + m);
+            const float xc = col[m + 1];
+            const float ax = A.sx[c] * (xc - xin[c + q.o.xm]) + A.sx[c + 1] * (xc - xin[c + q.o.xp]) +
+                             A.sy[c] * (xc - xin[c + q.o.ym]) + A.sy[c + px] * (xc - xin[c + q.o.yp]) +
+                             A.sz[c] * (xc - col[m]) + A.sz[c + pxy] * (xc - col[m + 2]);
+            const float fv = f[c];
+            const float v = xc + omega * (fv - ax) / A.dg[c];
+            xout[c] = v;
+            dot += (double)fv * (double)v;
+        }
+    }
+    if (do_dot) {
+        double t, u;
+        if (reduce2_last(dot, 0.0, partial, counter, t, u) && flat_tid() == 0) {
+            const double rz_old = st->rz;
+            st->rz = t;
+            st->beta = (st->iters == 0) ? 0.0 : t / rz_old;
+            if (!isfinite(t)) { st->status = SULI_ERR_NAN; st->done = 1; }
+        }
+    }
+}
+
+// x_out = x' + w (f - A x')/dg with x' = y + P xc (piecewise-constant prolongation)
+__global__ void __launch_bounds__(256) k_mg_post(Geo Gf, Geo Gc, BC bc, const float* __restrict__ y,
+                                                 const float* __restrict__ xc, const float* __restrict__ f, MGOps A,
+                                                 float* __restrict__ xout, float omega, const PCGState* st) {
+    if (st->done) return;
+    const Col q = column(Gf, bc);
+    if (!q.in) return;
+    const int px = Gf.px, pxy = (int)Gf.pxy;
+    // parents: coarse (I,J) of this column and of its x/y neighbours (ghost-mapped)
+    const int ixm = map_any(q.i - 1, Gf.nx, bc.perx), ixp = map_any(q.i + 1, Gf.nx, bc.perx);
+    const int jym = map_any(q.j - 1, Gf.ny, bc.pery), jyp = map_any(q.j + 1, Gf.ny, bc.pery);
+    const int I = (q.i + 1) >> 1, J = (q.j + 1) >> 1;
+    auto par = [&](int ii, int jj, int kk) { return xc[Gc.idx((ii + 1) >> 1, (jj + 1) >> 1, (kk + 1) >> 1)]; };
+    float col[kKZ + 2];
+#pragma unroll
+    for (int m = 0; m < kKZ + 2; ++m) {
+        const int k = map_any(q.k0 - 1 + m, Gf.nz, bc.perz);
+        col[m] = y[q.c0 + pxy * k] + xc[Gc.idx(I, J, (k + 1) >> 1)];
+    }
+#pragma unroll
+    for (int m = 0; m < kKZ; ++m) {
+        const int k = q.k0 + m;
+        if (k > Gf.nz) break;
+        const int c = q.c0 + pxy * k;
+        const float xv = col[m + 1];
+        const float vxm = y[c + q.o.xm] + par(ixm, q.j, k), vxp = y[c + q.o.xp] + par(ixp, q.j, k);
+        const float vym = y[c + q.o.ym] + par(q.i, jym, k), vyp = y[c + q.o.yp] + par(q.i, jyp, k);
+        const float ax = A.sx[c] * (xv - vxm) + A.sx[c + 1] * (xv - vxp) + A.sy[c] * (xv - vym) +
+                         A.sy[c + px] * (xv - vyp) + A.sz[c] * (xv - col[m]) + A.sz[c + pxy] * (xv - col[m + 2]);
+        xout[c] = xv + omega * (f[c] - ax) / A.dg[c];
+    }
+}
+
 __global__ void __launch_bounds__(256) k_mg_jac0(Geo G, const float* __restrict__ f, const float* __restrict__ dg,
                                                  float* x, float omega, const PCGState* st) {
     if (st->done) return;
@@ -309,6 +427,73 @@ __global__ void __launch_bounds__(256) k_pcg_update(Geo G, float* __restrict__ x
     }
 }
 
+// column forms of the two PCG kernels
+__global__ void __launch_bounds__(256) k_pcg_spmvc(Geo G, BC bc, const float* __restrict__ z,
+                                                   const float* __restrict__ p_old, float* __restrict__ p_new,
+                                                   float* __restrict__ q, MGOps A, PCGState* st, double* partial,
+                                                   unsigned int* counter) {
+    if (st->done) return;
+    const float beta = (float)st->beta;
+    const Col cq = column(G, bc);
+    double dot = 0.;
+    if (cq.in) {
+        const int px = G.px, pxy = (int)G.pxy;
+        auto pn = [&](int cc) { return z[cc] + beta * p_old[cc]; };
+        float col[kKZ + 2];
+        load_col(G, bc, cq, pn, col);
+#pragma unroll
+        for (int m = 0; m < kKZ; ++m) {
+            if (cq.k0 + m > G.nz) break;
+            const int c = cq.c0 + pxy * (cq.k0 + m);
+            const float pc = col[m + 1];
+            const float qv = A.sx[c] * (pc - pn(c + cq.o.xm)) + A.sx[c + 1] * (pc - pn(c + cq.o.xp)) +
+                             A.sy[c] * (pc - pn(c + cq.o.ym)) + A.sy[c + px] * (pc - pn(c + cq.o.yp)) +
+                             A.sz[c] * (pc - col[m]) + A.sz[c + pxy] * (pc - col[m + 2]);
+            p_new[c] = pc;
+            q[c] = qv;
+            dot += (double)pc * (double)qv;
+        }
+    }
+    double t, u;
+    if (reduce2_last(dot, 0.0, partial, counter, t, u) && flat_tid() == 0) {
+        st->pq = t;
+        st->alpha = st->rz / t;
+        if (!isfinite(st->alpha)) { st->status = SULI_ERR_NAN; st->done = 1; }
+    }
+}
+
+constexpr int kKZU = 8;
+__global__ void __launch_bounds__(256) k_pcg_updc(Geo G, float* __restrict__ x, float* __restrict__ r,
+                                                  const float* __restrict__ p, const float* __restrict__ q,
+                                                  PCGState* st, double* partial, unsigned int* counter) {
+    if (st->done) return;
+    const float alpha = (float)st->alpha;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k0 = blockIdx.z * kKZU + 1;
+    double rr = 0.;
+    if (i <= G.nx && j <= G.ny) {
+        const int c0 = kBase + (i - 1) + G.px * j, pxy = (int)G.pxy;
+        const int k1 = min(k0 + kKZU - 1, G.nz);
+        for (int k = k0; k <= k1; ++k) {
+            const int c = c0 + pxy * k;
+            x[c] = x[c] + alpha * p[c];
+            const float rv = r[c] - alpha * q[c];
+            r[c] = rv;
+            rr += (double)rv * (double)rv;
+        }
+    }
+    double t, u;
+    if (reduce2_last(rr, 0.0, partial, counter, t, u) && flat_tid() == 0) {
+        st->rr = t;
+        st->iters = st->iters + 1;
+        bool go = t > st->tol2;
+        if (st->iters >= st->maxit) go = false;
+        if (!isfinite(t)) { go = false; st->status = SULI_ERR_NAN; }
+        st->done = go ? 0 : 1;
+    }
+}
+
 // ------------------------------------------------------------------------------------
 // FP64 refinement: e <- e - sqrt(d) dp, r~ = A~ e - b~, r_u = sqrt(d) r~ (FP32)
 // ------------------------------------------------------------------------------------
@@ -403,9 +588,7 @@ void launch_vcycle(suli_ctx* c) {
     for (int l = 0; l < L - 1; ++l) {
         MGLevel& M = c->mg[l];
         const float* f = (l == 0) ? c->pc_r : M.f;
-        k_mg_jac0<<<cells3(M.g), kB2, 0, c->stream>>>(M.g, f, M.dg, M.x, om, c->pcg);
-        k_mg_jac<<<cells3(M.g), kB2, 0, c->stream>>>(M.g, bc, M.x, f, ops(M), M.y, om, c->pcg, 0, c->red_partial,
-                                                     c->red_counter);
+        k_mg_pre<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, f, ops(M), M.y, om, c->pcg);
         MGLevel& C = c->mg[l + 1];
         k_mg_restrict<<<cells3(C.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, f, ops(M), C.f, c->pcg);
     }
@@ -421,9 +604,9 @@ void launch_vcycle(suli_ctx* c) {
         MGLevel& M = c->mg[l];
         MGLevel& C = c->mg[l + 1];
         const float* f = (l == 0) ? c->pc_r : M.f;
-        k_mg_prolong_jac<<<cells3(M.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, C.y, f, ops(M), M.x, om, c->pcg);
-        k_mg_jac<<<cells3(M.g), kB2, 0, c->stream>>>(M.g, bc, M.x, f, ops(M), M.y, om, c->pcg, l == 0 ? 1 : 0,
-                                                     c->red_partial, c->red_counter);
+        k_mg_post<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, C.y, f, ops(M), M.x, om, c->pcg);
+        k_mg_jacc<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, M.x, f, ops(M), M.y, om, c->pcg, l == 0 ? 1 : 0,
+                                                       c->red_partial, c->red_counter);
     }
 }
 
@@ -432,16 +615,22 @@ void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new) {
     MGLevel& M0 = c->mg[0];
     {
         ProfScope ps(c, SULI_K_CG_SPMV, 1);
-        k_pcg_spmv<<<cells3(G), kB2, 0, c->stream>>>(G, c->bc, M0.y, p_old, p_new, c->pc_q, ops(M0), c->pcg,
-                                                     c->red_partial, c->red_counter);
+        k_pcg_spmvc<<<colgrid(G), kB2, 0, c->stream>>>(G, c->bc, M0.y, p_old, p_new, c->pc_q, ops(M0), c->pcg,
+                                                       c->red_partial, c->red_counter);
     }
     {
         ProfScope ps(c, SULI_K_CG_UPDATE, 1);
-        k_pcg_update<<<cells3(G), kB2, 0, c->stream>>>(G, c->pc_x, c->pc_r, p_new, c->pc_q, c->pcg, c->red_partial,
-                                                       c->red_counter);
+        const dim3 gu((G.nx + 31) / 32, (G.ny + 7) / 8, (G.nz + kKZU - 1) / kKZU);
+        k_pcg_updc<<<gu, kB2, 0, c->stream>>>(G, c->pc_x, c->pc_r, p_new, c->pc_q, c->pcg, c->red_partial,
+                                              c->red_counter);
     }
-    ProfScope ps(c, SULI_K_MG, 5 * ((int)c->mg.size() - 1) + 1);
+    ProfScope ps(c, SULI_K_MG, vcycle_kernels(c));
     launch_vcycle(c);
+}
+
+int vcycle_kernels(const suli_ctx* c) {
+    const int L = (int)c->mg.size();
+    return (L == 1) ? 2 : 4 * (L - 1) + 1;
 }
 
 }  // namespace suli

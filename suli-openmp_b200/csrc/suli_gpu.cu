@@ -597,7 +597,8 @@ int ensure_pcg_graphs(suli_ctx* c) {
         if (e != cudaSuccess) return fail(c, SULI_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
     }
     const int L = (int)c->mg.size();
-    c->pcg_graph_kernels = 2 + (L == 1 ? 2 : 5 * (L - 1) + 1);
+    (void)L;
+    c->pcg_graph_kernels = 2 + vcycle_kernels(c);
     return SULI_OK;
 }
 
@@ -621,7 +622,7 @@ int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
         if (outer >= c->P.refine_maxit) { status = SULI_WARN_CG_MAXIT; break; }
         launch_pcg_init(c, c->inner_maxit);
         {
-            ProfScope ps(c, SULI_K_MG, 5 * ((int)c->mg.size() - 1) + 1);
+            ProfScope ps(c, SULI_K_MG, vcycle_kernels(c));
             launch_vcycle(c);
         }
         launch_pcg_iter(c, c->mg[0].y, c->pc_pa);   // p_old = z with beta = 0
