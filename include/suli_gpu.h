@@ -142,7 +142,8 @@ int suli_destroy(suli_ctx* c);
 const char* suli_last_error(const suli_ctx* c);
 int suli_synchronize(suli_ctx* c);
 
-/* Fortran-layout host copies (c_loc of the module array).  Synchronous. */
+/* Fortran-layout copies (c_loc of the module array).  Synchronous.  The pointer may be host
+   memory or device memory of any GPU (unified addressing decides the copy's direction). */
 int suli_upload(suli_ctx* c, int field, const double* host);
 int suli_download(suli_ctx* c, int field, double* host);
 int suli_set_scalar(suli_ctx* c, int scalar, double v);
@@ -177,6 +178,44 @@ typedef struct suli_step_stats {
 
 /* One time step it (1_principal.f90:64-108 without MMS/plot/restart), plus est(). */
 int suli_step(suli_ctx* c, int it, suli_step_stats* st);
+
+/* ---- learned initial guess / preconditioner of the pressure solve ------------------------
+   No counterpart in the reference (an addition of this build for the variable-density
+   Poisson solve of 9_grad.f90).  A 3-D U-Net (4 levels, 16/32/64/96 channels, 3x3x3
+   convolutions, BF16 weights, FP32 accumulation on the tensor cores) maps three channels
+   (scaled residual, density feature, scaled previous pressure) to the scaled correction of the
+   pressure.  Grid dimensions must be multiples of 8.  Device buffers: in3 [V][3] FP32 and
+   out/target [V] FP32, x fastest. */
+typedef struct suli_nn suli_nn;
+long long suli_nn_num_params(void);
+int suli_nn_create(int nx, int ny, int nz, int device, suli_nn** out);
+int suli_nn_destroy(suli_nn* n);
+const char* suli_nn_last_error(const suli_nn* n);
+int suli_nn_set_params(suli_nn* n, const float* host, long long count);   /* FP32 master weights */
+int suli_nn_get_params(suli_nn* n, float* host, long long count);
+int suli_nn_forward(suli_nn* n, const float* d_in3, float* d_out);
+/* mean squared error against d_target and its gradient (copied to host_grad if not null) */
+int suli_nn_loss_grad(suli_nn* n, const float* d_in3, const float* d_target, double* loss, float* host_grad);
+int suli_nn_train_step(suli_nn* n, const float* d_in3, const float* d_target, float lr, double* loss);
+/* the convolution primitive on caller buffers: channels-last BF16 x [V][cin], w [27][cout][cin]
+   (tap = dx + 3 dy + 9 dz), bias [cout] FP32 or NULL, out [V][cout] BF16 = relu?(conv(x) + b) */
+int suli_nn_conv3d(int nx, int ny, int nz, const void* x, int cin, const void* w, const float* bias, int cout,
+                   int relu, void* out);
+
+/* Attach a network to a context (same grid and device) for its pressure solves.
+   mode 0 detaches; mode 1 (precision 1 only) uses the network as the initial guess: after
+   graddin's set-up the network maps (r~0/s, H, (e0 - mean)/s_e) to a correction y of the
+   scaled pressure, and e0 <- e0 + alpha s y with alpha = -(r~0 . y)/(y . A~ y), the
+   energy-norm optimal step in FP64, so the guess never raises the A~-norm error of e0.  The
+   solve then runs to the same FP64 stopping test as without the network.  A network serves
+   one context at a time (it keeps its activations). */
+int suli_attach_nn(suli_ctx* c, suli_nn* net, int mode);
+/* graddin() that also records a training pair of the network: d_in3 [V][3] receives the
+   network's input features of the solve's starting state and d_target [V] the scaled
+   correction (e* - e0)/s to the converged solution, less its component along sqrt(d) (the
+   null vector of A~ for the all-Neumann pressure problem) (device FP32 buffers, x fastest
+   over the nx x ny x nz cells).  Any precision; an attached network is not applied. */
+int suli_graddin_record(suli_ctx* c, float* d_in3, float* d_target, int* iters, double* resid);
 
 /* ---- divergence check that allocates nothing ---------------------------------------------
    No counterpart in the reference: an extra way to run est() for callers that may not let a
@@ -219,6 +258,7 @@ enum suli_kernel {
     SULI_K_MG,             /* precision 1: FP32 inner PCG iterations (SpMV, update, multigrid
                               V-cycle), launched as one CUDA graph per iteration */
     SULI_K_REFINE,         /* precision 1: FP64 residual and correction of the refinement */
+    SULI_K_NN,             /* learned initial guess: features, network forward, FP64 step */
     SULI_K_COUNT
 };
 /* The CUDA stream (cudaStream_t) this context launches on, for callers ordering their own

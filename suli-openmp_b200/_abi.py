@@ -214,6 +214,18 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
         "suli_profile_read": (C.c_int, [vp, P(C.c_double), P(C.c_longlong), P(C.c_longlong)]),
         "suli_est_static": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                       C.c_double, vp, vp]),
+        "suli_nn_num_params": (C.c_longlong, []),
+        "suli_nn_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P(vp)]),
+        "suli_nn_destroy": (C.c_int, [vp]),
+        "suli_nn_last_error": (C.c_char_p, [vp]),
+        "suli_nn_set_params": (C.c_int, [vp, P(C.c_float), C.c_longlong]),
+        "suli_nn_get_params": (C.c_int, [vp, P(C.c_float), C.c_longlong]),
+        "suli_nn_forward": (C.c_int, [vp, vp, vp]),
+        "suli_nn_loss_grad": (C.c_int, [vp, vp, vp, P(C.c_double), P(C.c_float)]),
+        "suli_nn_train_step": (C.c_int, [vp, vp, vp, C.c_float, P(C.c_double)]),
+        "suli_nn_conv3d": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp]),
+        "suli_attach_nn": (C.c_int, [vp, vp, C.c_int]),
+        "suli_graddin_record": (C.c_int, [vp, vp, vp, P(C.c_int), P(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -232,11 +244,14 @@ HEADER_SYMBOLS = [
     "suli_tempo", "suli_contorno", "suli_graddin", "suli_posdin", "suli_est",
     "suli_set_dt", "suli_step", "suli_stream", "suli_profile_enable", "suli_profile_read",
     "suli_est_static",
+    "suli_nn_num_params", "suli_nn_create", "suli_nn_destroy", "suli_nn_last_error",
+    "suli_nn_set_params", "suli_nn_get_params", "suli_nn_forward", "suli_nn_loss_grad",
+    "suli_nn_train_step", "suli_nn_conv3d", "suli_attach_nn", "suli_graddin_record",
 ]
 EST_STATIC_MAX_BLOCKS = 8192   # SULI_EST_STATIC_MAX_BLOCKS
 
 # enum suli_kernel: kernel classes of the tracing counters
 KERNEL_NAMES = [
     "ls_advect", "reinit", "lsprops", "curv", "volfix", "visco", "convdiff", "tempo", "contorno",
-    "cg_setup", "cg_spmv", "cg_update", "cg_final", "posdin", "est", "mg", "refine",
+    "cg_setup", "cg_spmv", "cg_update", "cg_final", "posdin", "est", "mg", "refine", "nn",
 ]

@@ -43,6 +43,18 @@ struct PCGState {
     int status;
 };
 
+// Scales of the learned initial guess (device resident): rms of the first scaled residual,
+// mean and rms deviation of e0, the FP64 step length, the null-space coefficient of a
+// recorded target, and whether the guess applies.
+struct NNScale {
+    double sigma_r;
+    double mean_e;
+    double sigma_e;
+    double alpha;
+    double proj;
+    int active;
+};
+
 // One level of the FP32 multigrid hierarchy: face conductances, Jacobi diagonal, vectors.
 struct MGLevel {
     Geo g;
@@ -115,6 +127,13 @@ struct suli_ctx {
     // one CUDA graph per ping-pong parity holding a whole inner PCG iteration
     cudaGraphExec_t pcg_graph[2] = {nullptr, nullptr};
     int pcg_graph_kernels = 0;
+    // learned initial guess (suli_attach_nn) and training-pair recording (suli_graddin_record)
+    suli_nn* nn = nullptr;
+    int nn_mode = 0;
+    float *nn_in = nullptr, *nn_out = nullptr;   // [V][3], [V]
+    double* nn_e0 = nullptr;                     // e0 of a recorded solve (box layout)
+    suli::NNScale* nn_scale = nullptr;
+    float *rec_in = nullptr, *rec_target = nullptr;
     // cached CUDA graphs of CG iteration batches (parity 0: p_old = pa)
     cudaGraphExec_t cg_graph = nullptr;
     bool use_graphs = true;
@@ -199,6 +218,10 @@ void launch_mx_setup(suli_ctx* c);
 void launch_mx_residual(suli_ctx* c, const double* e_in, double* e_out, bool apply);
 void launch_pcg_init(suli_ctx* c, int maxit);
 void launch_vcycle(suli_ctx* c);
+// ---- learned initial guess (k_learned.cu) ----
+void launch_nn_features(suli_ctx* c, float* in3);
+void launch_nn_step(suli_ctx* c, const float* out, double* e);
+void launch_nn_target(suli_ctx* c, const double* e_star, float* target);
 void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new);
 int vcycle_kernels(const suli_ctx* c);
 void launch_posdin(suli_ctx* c);

@@ -54,4 +54,20 @@ __host__ __device__ inline int map_any(int i, int n, int per) {
     return (i < 1) ? (per ? n : 1) : ((i > n) ? (per ? 1 : n) : i);
 }
 
+// Neighbour offsets of cell (i,j,k) in a box; a Neumann face maps to the cell itself.
+struct Nb {
+    int xm, xp, ym, yp, zm, zp;
+};
+__host__ __device__ inline Nb neighbours(const Geo& G, const BC& bc, int i, int j, int k) {
+    Nb o;
+    const int px = G.px, pxy = (int)G.pxy;
+    o.xm = (i > 1) ? -1 : (bc.perx ? G.nx - 1 : 0);
+    o.xp = (i < G.nx) ? 1 : (bc.perx ? -(G.nx - 1) : 0);
+    o.ym = (j > 1) ? -px : (bc.pery ? (G.ny - 1) * px : 0);
+    o.yp = (j < G.ny) ? px : (bc.pery ? -(G.ny - 1) * px : 0);
+    o.zm = (k > 1) ? -pxy : (bc.perz ? (G.nz - 1) * pxy : 0);
+    o.zp = (k < G.nz) ? pxy : (bc.perz ? -(G.nz - 1) * pxy : 0);
+    return o;
+}
+
 }  // namespace suli

@@ -1,0 +1,168 @@
+// k_learned.cu — the network's place in the pressure solve (9_grad.f90:118-151 set-up).
+//
+// After graddin's set-up (scaled system A~ e = b~, first residual r~0 = A~ e0 - b~):
+//   features  in3[v] = (r~0/s, H, (e0 - mean e0)/s_e),  s = rms(r~0), s_e = rms(e0 - mean),
+//             H = (rho - rho_1)/(rho_2 - rho_1) (0 in phase 1, 1 in phase 2);
+//   step      y = network output, alpha = -(r~0 . y)/(y . A~ y), e <- e0 + alpha y (FP64);
+//   target    P(e* - e0)/s for training (e* the converged scaled solution), P removing the
+//             component along n = sqrt(d): A~ n = 0 for the all-Neumann pressure problem, so
+//             that component of e* is arbitrary (the FP32 inner solves may add some of it)
+//             and neither the step nor the solution depends on it.
+// Cells are enumerated v = (i-1) + nx ((j-1) + ny (k-1)).  All sums are FP64 block partials
+// finished by the last block.
+#include <cuda_runtime.h>
+#include <cmath>
+#include "ctx.cuh"
+#include "reduce.cuh"
+
+namespace suli {
+
+namespace {
+__device__ __forceinline__ long long cell_v(const Geo& G, int i, int j, int k) {
+    return (long long)(i - 1) + (long long)G.nx * ((j - 1) + (long long)G.ny * (k - 1));
+}
+
+// s = sqrt(rr/n) from graddin's set-up reduction; mean and rms deviation of e0
+__global__ void __launch_bounds__(256) k_nn_stats(Geo G, const double* __restrict__ e, const CGState* cg,
+                                                  NNScale* sc, double* partial, unsigned int* counter) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    double s1 = 0., s2 = 0.;
+    if (i <= G.nx && j <= G.ny && k <= G.nz) {
+        const double v = e[G.idx(i, j, k)];
+        s1 = v;
+        s2 = v * v;
+    }
+    double t1, t2;
+    if (reduce2_last(s1, s2, partial, counter, t1, t2) && flat_tid() == 0) {
+        const double n = (double)G.nx * G.ny * G.nz;
+        const double mean = t1 / n;
+        const double var = t2 / n - mean * mean;
+        const double sr = sqrt(cg->rr / n);
+        sc->mean_e = mean;
+        sc->sigma_e = var > 0. ? sqrt(var) : 0.;
+        sc->sigma_r = sr;
+        sc->alpha = 0.;
+        sc->active = (!cg->done && sr > 0. && isfinite(sr) && isfinite(mean) && isfinite(var)) ? 1 : 0;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_nn_features(Geo G, const double* __restrict__ r, const double* __restrict__ e,
+                                                     const double* __restrict__ rho, double rho1, double rho2,
+                                                     const NNScale* __restrict__ sc, float* __restrict__ in3) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > G.nx || j > G.ny || k > G.nz) return;
+    const long long c = G.idx(i, j, k), v = cell_v(G, i, j, k);
+    const double sr = sc->sigma_r, se = sc->sigma_e;
+    const double h = (rho2 != rho1) ? (rho[c] - rho1) / (rho2 - rho1) : 0.;
+    in3[3 * v + 0] = sc->active ? (float)(r[c] / sr) : 0.f;
+    in3[3 * v + 1] = (float)h;
+    in3[3 * v + 2] = se > 0. ? (float)((e[c] - sc->mean_e) / se) : 0.f;
+}
+
+// y into the box layout (FP64), so the operator can read its neighbours
+__global__ void __launch_bounds__(256) k_nn_scatter(Geo G, const float* __restrict__ out, double* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > G.nx || j > G.ny || k > G.nz) return;
+    y[G.idx(i, j, k)] = (double)out[cell_v(G, i, j, k)];
+}
+
+// r.y and y.A~y with A~ the set-up's scaled operator (ghost rules as the refinement residual)
+__global__ void __launch_bounds__(256) k_nn_dots(Geo G, BC bc, const double* __restrict__ y, const double* __restrict__ r,
+                                                 const double* __restrict__ ax, const double* __restrict__ ay,
+                                                 const double* __restrict__ az, NNScale* sc, double* partial,
+                                                 unsigned int* counter) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    double ry = 0., yay = 0.;
+    if (i <= G.nx && j <= G.ny && k <= G.nz) {
+        const int c = (int)G.idx(i, j, k);
+        const Nb o = neighbours(G, bc, i, j, k);
+        const double yc = y[c];
+        const double ayv = yc - ax[c + 1] * y[c + o.xp] - ax[c] * y[c + o.xm] - ay[c + G.px] * y[c + o.yp] -
+                           ay[c] * y[c + o.ym] - az[c + (int)G.pxy] * y[c + o.zp] - az[c] * y[c + o.zm];
+        ry = r[c] * yc;
+        yay = yc * ayv;
+    }
+    double t1, t2;
+    if (reduce2_last(ry, yay, partial, counter, t1, t2) && flat_tid() == 0) {
+        const bool ok = sc->active && t2 > 0. && isfinite(t1) && isfinite(t2);
+        sc->alpha = ok ? -t1 / t2 : 0.;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_nn_apply(Geo G, const double* __restrict__ y, const NNScale* __restrict__ sc,
+                                                  double* __restrict__ e) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > G.nx || j > G.ny || k > G.nz) return;
+    const double a = sc->alpha;
+    if (a == 0.) return;
+    const long long c = G.idx(i, j, k);
+    e[c] += a * y[c];
+}
+
+// n.(e* - e0) and n.n with n = sqrt(d) -> the projection coefficient
+__global__ void __launch_bounds__(256) k_nn_nullproj(Geo G, const double* __restrict__ es, const double* __restrict__ e0,
+                                                     const double* __restrict__ d, NNScale* sc, double* partial,
+                                                     unsigned int* counter) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    double s1 = 0., s2 = 0.;
+    if (i <= G.nx && j <= G.ny && k <= G.nz) {
+        const long long c = G.idx(i, j, k);
+        s1 = sqrt(d[c]) * (es[c] - e0[c]);
+        s2 = d[c];
+    }
+    double t1, t2;
+    if (reduce2_last(s1, s2, partial, counter, t1, t2) && flat_tid() == 0) sc->proj = t2 > 0. ? t1 / t2 : 0.;
+}
+
+__global__ void __launch_bounds__(256) k_nn_target(Geo G, const double* __restrict__ es, const double* __restrict__ e0,
+                                                   const double* __restrict__ d, const NNScale* __restrict__ sc,
+                                                   float* __restrict__ t) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > G.nx || j > G.ny || k > G.nz) return;
+    const long long c = G.idx(i, j, k);
+    const double sr = sc->sigma_r;
+    t[cell_v(G, i, j, k)] = sc->active ? (float)((es[c] - e0[c] - sc->proj * sqrt(d[c])) / sr) : 0.f;
+}
+
+const dim3 kBL(32, 8, 1);
+inline dim3 grid_cells(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
+}  // namespace
+
+void launch_nn_features(suli_ctx* c, float* in3) {
+    const Geo& G = c->g;
+    k_nn_stats<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_e, c->cg, c->nn_scale, c->red_partial, c->red_counter);
+    k_nn_features<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_r, c->cg_e, c->f[SULI_F_RHO], c->P.rho_f1,
+                                                         c->P.rho_f2, c->nn_scale, in3);
+}
+
+void launch_nn_step(suli_ctx* c, const float* out, double* e) {
+    const Geo& G = c->g;
+    double* y = c->cg_pa;   // free during the mixed solve's set-up
+    k_nn_scatter<<<grid_cells(G), kBL, 0, c->stream>>>(G, out, y);
+    k_nn_dots<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->bc, y, c->cg_r, c->cg_ax, c->cg_ay, c->cg_az, c->nn_scale,
+                                                      c->red_partial, c->red_counter);
+    k_nn_apply<<<grid_cells(G), kBL, 0, c->stream>>>(G, y, c->nn_scale, e);
+}
+
+void launch_nn_target(suli_ctx* c, const double* e_star, float* target) {
+    const Geo& G = c->g;
+    k_nn_nullproj<<<grid_cells(G), kBL, 0, c->stream>>>(G, e_star, c->nn_e0, c->cg_d, c->nn_scale, c->red_partial,
+                                                        c->red_counter);
+    k_nn_target<<<grid_cells(G), kBL, 0, c->stream>>>(G, e_star, c->nn_e0, c->cg_d, c->nn_scale, target);
+}
+
+}  // namespace suli

@@ -23,21 +23,6 @@ namespace suli {
 
 __device__ __forceinline__ int clampi_m(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// neighbour offsets of cell (i,j,k) in a level's box; a Neumann face maps to the cell itself
-struct Nb {
-    int xm, xp, ym, yp, zm, zp;
-};
-__device__ __forceinline__ Nb neighbours(const Geo& G, const BC& bc, int i, int j, int k) {
-    Nb o;
-    const int px = G.px, pxy = (int)G.pxy;
-    o.xm = (i > 1) ? -1 : (bc.perx ? G.nx - 1 : 0);
-    o.xp = (i < G.nx) ? 1 : (bc.perx ? -(G.nx - 1) : 0);
-    o.ym = (j > 1) ? -px : (bc.pery ? (G.ny - 1) * px : 0);
-    o.yp = (j < G.ny) ? px : (bc.pery ? -(G.ny - 1) * px : 0);
-    o.zm = (k > 1) ? -pxy : (bc.perz ? (G.nz - 1) * pxy : 0);
-    o.zp = (k < G.nz) ? pxy : (bc.perz ? -(G.nz - 1) * pxy : 0);
-    return o;
-}
 // (A x)_c = sum over the six faces of s_f (x_c - x_nb)
 __device__ __forceinline__ float apply_A(const float* __restrict__ x, const float* __restrict__ sx,
                                          const float* __restrict__ sy, const float* __restrict__ sz, int c,

@@ -1,0 +1,650 @@
+// nn.cu — the learned initial guess / preconditioner of the pressure solve: a 3-D U-Net
+// (4 levels, 16/32/64/96 channels, 3x3x3 convolutions, ReLU, 2x2x2 average pooling, nearest
+// upsampling with skip concatenation, 1x1x1 head), BF16 weights and activations, FP32
+// accumulation, FP32 master weights trained with Adam.  Forward convolutions and the
+// input-gradient (dgrad) convolutions run on the tensor cores (nn_conv.cuh); weight
+// gradients accumulate in FP32 on the CUDA cores.
+//
+// The network maps (residual r~0/s, density feature, previous pressure e0/s) to the scaled
+// correction (e* - e0)/s of the pressure solve, so it is both an initial guess
+// (e0 <- e0 + s net(.)) and an approximate inverse of A~ applied to a residual.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "../../include/suli_gpu.h"
+#include "nn_api.cuh"
+#include "nn_conv.cuh"
+
+namespace suli {
+namespace nn {
+
+constexpr int kLevels = 4;
+constexpr int kCh[kLevels] = {16, 32, 64, 96};
+constexpr int kInCh = 3;   // real input channels (padded to 16)
+
+// conv layers in order: enc0a enc0b enc1a enc1b enc2a enc2b enc3a enc3b dec2a dec2b dec1a dec1b dec0a dec0b
+struct LayerSpec {
+    int cin, cout, level;
+};
+constexpr int kConv = 14;
+constexpr LayerSpec kLayer[kConv] = {
+    {16, 16, 0}, {16, 16, 0}, {16, 32, 1}, {32, 32, 1}, {32, 64, 2}, {64, 64, 2}, {64, 96, 3},
+    {96, 96, 3}, {160, 64, 2}, {64, 64, 2}, {96, 32, 1}, {32, 32, 1}, {48, 16, 0}, {16, 16, 0},
+};
+
+__host__ __device__ inline long long conv_params(const LayerSpec& L) { return 27LL * L.cout * L.cin + L.cout; }
+
+// ------------------------------------------------------------------------------------
+// elementwise / small kernels
+// ------------------------------------------------------------------------------------
+__global__ void k_pack_input(long long V, const float* __restrict__ in3, __nv_bfloat16* __restrict__ out16) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    __nv_bfloat16 t[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) t[c] = __float2bfloat16(c < kInCh ? in3[v * kInCh + c] : 0.f);
+    uint4* o = reinterpret_cast<uint4*>(out16 + v * 16);
+    o[0] = *reinterpret_cast<uint4*>(&t[0]);
+    o[1] = *reinterpret_cast<uint4*>(&t[8]);
+}
+
+// 2x2x2 average pooling, channels last
+__global__ void k_pool(Vol fine, int C, const __nv_bfloat16* __restrict__ x, __nv_bfloat16* __restrict__ y) {
+    const int cx = fine.nx / 2, cy = fine.ny / 2, cz = fine.nz / 2;
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long Vc = (long long)cx * cy * cz;
+    if (q >= Vc * C) return;
+    const int c = (int)(q % C);
+    const long long vc = q / C;
+    const int X = (int)(vc % cx), Y = (int)((vc / cx) % cy), Z = (int)(vc / ((long long)cx * cy));
+    float s = 0.f;
+    for (int d = 0; d < 8; ++d) {
+        const int fx = 2 * X + (d & 1), fy = 2 * Y + ((d >> 1) & 1), fz = 2 * Z + (d >> 2);
+        s += __bfloat162float(x[((long long)fx + fine.nx * ((long long)fy + (long long)fine.ny * fz)) * C + c]);
+    }
+    y[q] = __float2bfloat16(0.125f * s);
+}
+
+// gradient of the pooling: dx[fine] += dy[parent] / 8
+__global__ void k_pool_bwd(Vol fine, int C, const __nv_bfloat16* __restrict__ dy, __nv_bfloat16* dx) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long V = (long long)fine.nx * fine.ny * fine.nz;
+    if (q >= V * C) return;
+    const int c = (int)(q % C);
+    const long long v = q / C;
+    const int x = (int)(v % fine.nx), y = (int)((v / fine.nx) % fine.ny), z = (int)(v / ((long long)fine.nx * fine.ny));
+    const int cx = fine.nx / 2, cy = fine.ny / 2;
+    const long long vc = (long long)(x >> 1) + cx * ((long long)(y >> 1) + (long long)cy * (z >> 1));
+    dx[q] = __float2bfloat16(__bfloat162float(dx[q]) + 0.125f * __bfloat162float(dy[vc * C + c]));
+}
+
+// dz = dy * (y > 0) in place
+__global__ void k_relu_bwd(long long n, const __nv_bfloat16* __restrict__ y, __nv_bfloat16* dy) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n && !(__bfloat162float(y[q]) > 0.f)) dy[q] = __float2bfloat16(0.f);
+}
+
+// split the gradient of concat(up(A), B): dA[coarse] = sum of the 8 children (channels < ca);
+// dB[fine] += channels >= ca
+__global__ void k_concat_bwd(Vol fine, int ca, int cb, const __nv_bfloat16* __restrict__ dcat,
+                             __nv_bfloat16* __restrict__ da, __nv_bfloat16* db) {
+    const int cx = fine.nx / 2, cy = fine.ny / 2, cz = fine.nz / 2;
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long Vc = (long long)cx * cy * cz, Vf = (long long)fine.nx * fine.ny * fine.nz;
+    const int C = ca + cb;
+    if (q < Vc * ca) {
+        const int c = (int)(q % ca);
+        const long long vc = q / ca;
+        const int X = (int)(vc % cx), Y = (int)((vc / cx) % cy), Z = (int)(vc / ((long long)cx * cy));
+        float s = 0.f;
+        for (int d = 0; d < 8; ++d) {
+            const int fx = 2 * X + (d & 1), fy = 2 * Y + ((d >> 1) & 1), fz = 2 * Z + (d >> 2);
+            s += __bfloat162float(dcat[((long long)fx + fine.nx * ((long long)fy + (long long)fine.ny * fz)) * C + c]);
+        }
+        da[q] = __float2bfloat16(s);
+    }
+    if (q < Vf * cb) {
+        const int c = (int)(q % cb);
+        const long long v = q / cb;
+        db[q] = __float2bfloat16(__bfloat162float(db[q]) + __bfloat162float(dcat[v * C + ca + c]));
+    }
+}
+
+// head: out[v] = sum_c w[c] x[v][c] + b  (FP32 out)
+__global__ void k_head_fwd(long long V, const __nv_bfloat16* __restrict__ x, const float* __restrict__ w,
+                           float* __restrict__ out) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    float s = w[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) s += w[c] * __bfloat162float(x[v * 16 + c]);
+    out[v] = s;
+}
+// head backward: dx[v][c] = w[c] dout[v]; dw[c] += sum_v x[v][c] dout[v]; db += sum dout
+__global__ void k_head_bwd(long long V, const __nv_bfloat16* __restrict__ x, const float* __restrict__ w,
+                           const float* __restrict__ dout, __nv_bfloat16* __restrict__ dx, float* dw) {
+    __shared__ float sh[17][8];
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    float g[17];
+#pragma unroll
+    for (int c = 0; c < 17; ++c) g[c] = 0.f;
+    if (v < V) {
+        const float d = dout[v];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+            dx[v * 16 + c] = __float2bfloat16(w[c] * d);
+            g[c] = __bfloat162float(x[v * 16 + c]) * d;
+        }
+        g[16] = d;
+    }
+#pragma unroll
+    for (int c = 0; c < 17; ++c)
+        for (int o = 16; o > 0; o >>= 1) g[c] += __shfl_xor_sync(0xffffffffu, g[c], o);
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int c = 0; c < 17; ++c) sh[c][wp] = g[c];
+    __syncthreads();
+    if (threadIdx.x < 17) {
+        float s = 0.f;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s += sh[threadIdx.x][q];
+        atomicAdd(&dw[threadIdx.x], s);
+    }
+}
+
+// W'[tap'][ci][co] = W[26 - tap'][co][ci]: weights of the input-gradient convolution
+__global__ void k_flip_weights(int cin, int cout, const __nv_bfloat16* __restrict__ w, __nv_bfloat16* __restrict__ wt) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = 27LL * cin * cout;
+    if (q >= n) return;
+    const int co = (int)(q % cout);
+    const int ci = (int)((q / cout) % cin);
+    const int tp = (int)(q / ((long long)cout * cin));
+    wt[q] = w[((long long)(26 - tp) * cout + co) * cin + ci];
+}
+
+// weight gradient of one layer: dW[tap][co][ci] += sum_v X[v + off(tap)][ci] dZ[v][co];
+// a CTA owns one tap and a chunk of voxels; threads hold a (CO16 x CI16) register block.
+constexpr int kWgChunk = 4096, kWgSub = 32;
+template <int CO16, int CI16>
+__global__ void __launch_bounds__(256) k_wgrad(Vol vol, ConvIn in, const __nv_bfloat16* __restrict__ dz, float* dw,
+                                               float* db) {
+    constexpr int COUT = CO16 * 16, CIN = CI16 * 16;
+    __shared__ float sx[kWgSub][CIN + 1];
+    __shared__ float sz[kWgSub][COUT + 1];
+    const int tap = blockIdx.y;
+    const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dzz = tap / 9 - 1;
+    const long long V = (long long)vol.nx * vol.ny * vol.nz;
+    const long long v0 = (long long)blockIdx.x * kWgChunk;
+    const int tc = threadIdx.x >> 4, ti = threadIdx.x & 15;
+    float acc[CO16][CI16];
+#pragma unroll
+    for (int a = 0; a < CO16; ++a)
+#pragma unroll
+        for (int b = 0; b < CI16; ++b) acc[a][b] = 0.f;
+    float bacc[CO16];
+#pragma unroll
+    for (int a = 0; a < CO16; ++a) bacc[a] = 0.f;
+    const int hxn = (vol.nx + 1) / 2, hyn = (vol.ny + 1) / 2;
+    for (long long vs = v0; vs < v0 + kWgChunk && vs < V; vs += kWgSub) {
+        // stage dZ and the shifted input of kWgSub voxels (FP32)
+        for (int q = threadIdx.x; q < kWgSub * COUT; q += 256) {
+            const int m = q / COUT, c = q % COUT;
+            const long long v = vs + m;
+            sz[m][c] = (v < V) ? __bfloat162float(dz[v * COUT + c]) : 0.f;
+        }
+        for (int q = threadIdx.x; q < kWgSub * CIN; q += 256) {
+            const int m = q / CIN, c = q % CIN;
+            const long long v = vs + m;
+            float val = 0.f;
+            if (v < V) {
+                const int x = (int)(v % vol.nx) + dx, y = (int)((v / vol.nx) % vol.ny) + dy,
+                          z = (int)(v / ((long long)vol.nx * vol.ny)) + dzz;
+                if (x >= 0 && x < vol.nx && y >= 0 && y < vol.ny && z >= 0 && z < vol.nz) {
+                    if (c < in.ca) {
+                        const long long vi = in.a_half ? ((long long)(x >> 1) + hxn * ((long long)(y >> 1) + (long long)hyn * (z >> 1)))
+                                                       : ((long long)x + vol.nx * ((long long)y + (long long)vol.ny * z));
+                        val = __bfloat162float(in.a[vi * in.ca + c]);
+                    } else {
+                        const long long vi = (long long)x + vol.nx * ((long long)y + (long long)vol.ny * z);
+                        val = __bfloat162float(in.b[vi * in.cb + (c - in.ca)]);
+                    }
+                }
+            }
+            sx[m][c] = val;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int m = 0; m < kWgSub; ++m) {
+            float zv[CO16], xv[CI16];
+#pragma unroll
+            for (int a = 0; a < CO16; ++a) zv[a] = sz[m][tc + 16 * a];
+#pragma unroll
+            for (int b = 0; b < CI16; ++b) xv[b] = sx[m][ti + 16 * b];
+#pragma unroll
+            for (int a = 0; a < CO16; ++a) {
+#pragma unroll
+                for (int b = 0; b < CI16; ++b) acc[a][b] += zv[a] * xv[b];
+                if (ti == 0 && tap == 13) bacc[a] += zv[a];
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < CO16; ++a) {
+#pragma unroll
+        for (int b = 0; b < CI16; ++b)
+            atomicAdd(&dw[((long long)tap * COUT + tc + 16 * a) * CIN + ti + 16 * b], acc[a][b]);
+        if (ti == 0 && tap == 13) atomicAdd(&db[tc + 16 * a], bacc[a]);
+    }
+}
+
+// squared error L = mean(e^2), e = pred - target; dout = 2 e / V
+__global__ void k_loss_sums(long long V, const float* __restrict__ pred, const float* __restrict__ tgt, double* sums) {
+    __shared__ double sh[2][8];
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0., e2 = 0.;
+    if (v < V) {
+        e = (double)pred[v] - (double)tgt[v];
+        e2 = e * e;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_xor_sync(0xffffffffu, e, o);
+        e2 += __shfl_xor_sync(0xffffffffu, e2, o);
+    }
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    if (lane == 0) { sh[0][wp] = e; sh[1][wp] = e2; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0., b = 0.;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { a += sh[0][q]; b += sh[1][q]; }
+        atomicAdd(&sums[0], a);
+        atomicAdd(&sums[1], b);
+    }
+}
+__global__ void k_loss_grad(long long V, const float* __restrict__ pred, const float* __restrict__ tgt,
+                            float* __restrict__ dout) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    dout[v] = (float)(2.0 / (double)V * ((double)pred[v] - (double)tgt[v]));
+}
+
+// Adam on the FP32 master weights, then the BF16 copy the convolutions read
+__global__ void k_adam(long long n, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, __nv_bfloat16* __restrict__ wb, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    if (lr != 0.f) {
+        const float gq = g[q];
+        const float mq = b1 * m[q] + (1.f - b1) * gq;
+        const float vq = b2 * v[q] + (1.f - b2) * gq * gq;
+        m[q] = mq;
+        v[q] = vq;
+        w[q] -= lr * (mq / c1) / (sqrtf(vq / c2) + eps);
+    }
+    wb[q] = __float2bfloat16(w[q]);
+}
+
+__global__ void k_zero_bf(long long n, __nv_bfloat16* a) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) a[q] = __float2bfloat16(0.f);
+}
+
+}  // namespace nn
+}  // namespace suli
+
+using namespace suli::nn;
+
+// ------------------------------------------------------------------------------------
+// host side: network object
+// ------------------------------------------------------------------------------------
+struct suli_nn {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Vol vol[kLevels];
+    long long V[kLevels];
+    long long nparam = 0;
+    long long off[kConv + 1];   // parameter offsets (head at off[kConv])
+    float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+    __nv_bfloat16* wb = nullptr;     // BF16 copy, same layout
+    __nv_bfloat16* wflip = nullptr;  // scratch: flipped weights for dgrad
+    unsigned char* frozen = nullptr;
+    long long step = 0;
+    // activations (BF16, channels last)
+    __nv_bfloat16 *in0 = nullptr, *a[kConv] = {nullptr}, *pool[kLevels - 1] = {nullptr};
+    // gradients
+    __nv_bfloat16 *gact[kConv] = {nullptr}, *gpool[kLevels - 1] = {nullptr}, *gcat = nullptr, *gtmp = nullptr;
+    float *out = nullptr, *dout = nullptr;
+    double* sums = nullptr;
+    double* host_sums = nullptr;
+    std::string err;
+};
+
+namespace {
+
+inline unsigned nb(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+template <int NF>
+void conv_launch(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu,
+                 __nv_bfloat16* out) {
+    const int cin = in.ca + in.cb;
+    const size_t smem = (size_t)HVOX * (cin * 2 + 16);
+    static bool attr_done[64] = {false};
+    if (!attr_done[N->device]) {
+        cudaFuncSetAttribute(k_conv3_fwd<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+        attr_done[N->device] = true;
+    }
+    const dim3 grid((vol.nx + TX - 1) / TX, (vol.ny + TY - 1) / TY, (vol.nz + TZ - 1) / TZ);
+    k_conv3_fwd<NF><<<grid, 256, smem, N->stream>>>(vol, in, W, bias, relu, out);
+}
+
+void conv(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu, int cout,
+          __nv_bfloat16* out) {
+    switch (cout) {
+    case 16: conv_launch<2>(N, vol, in, W, bias, relu, out); break;
+    case 32: conv_launch<4>(N, vol, in, W, bias, relu, out); break;
+    case 48: conv_launch<6>(N, vol, in, W, bias, relu, out); break;
+    case 64: conv_launch<8>(N, vol, in, W, bias, relu, out); break;
+    case 96: conv_launch<12>(N, vol, in, W, bias, relu, out); break;
+    case 160: conv_launch<20>(N, vol, in, W, bias, relu, out); break;
+    default: break;
+    }
+}
+
+template <int CO16, int CI16>
+void wgrad_launch(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* dz, float* dw, float* db) {
+    const long long V = (long long)vol.nx * vol.ny * vol.nz;
+    const dim3 grid((unsigned)((V + kWgChunk - 1) / kWgChunk), 27);
+    k_wgrad<CO16, CI16><<<grid, 256, 0, N->stream>>>(vol, in, dz, dw, db);
+}
+void wgrad(suli_nn* N, const Vol& vol, const ConvIn& in, int cout, const __nv_bfloat16* dz, float* dw, float* db) {
+    const int cin = in.ca + in.cb;
+    const int key = (cout / 16) * 100 + cin / 16;
+    switch (key) {
+    case 101: wgrad_launch<1, 1>(N, vol, in, dz, dw, db); break;
+    case 201: wgrad_launch<2, 1>(N, vol, in, dz, dw, db); break;
+    case 202: wgrad_launch<2, 2>(N, vol, in, dz, dw, db); break;
+    case 402: wgrad_launch<4, 2>(N, vol, in, dz, dw, db); break;
+    case 404: wgrad_launch<4, 4>(N, vol, in, dz, dw, db); break;
+    case 604: wgrad_launch<6, 4>(N, vol, in, dz, dw, db); break;
+    case 606: wgrad_launch<6, 6>(N, vol, in, dz, dw, db); break;
+    case 410: wgrad_launch<4, 10>(N, vol, in, dz, dw, db); break;
+    case 206: wgrad_launch<2, 6>(N, vol, in, dz, dw, db); break;
+    case 103: wgrad_launch<1, 3>(N, vol, in, dz, dw, db); break;
+    default: break;
+    }
+}
+
+// input of conv layer l (the decoder's first layers read concat(up(coarse), skip))
+ConvIn layer_input(suli_nn* N, int l) {
+    ConvIn in{nullptr, 0, 0, nullptr, 0};
+    switch (l) {
+    case 0: in.a = N->in0; in.ca = 16; break;
+    case 1: in.a = N->a[0]; in.ca = 16; break;
+    case 2: in.a = N->pool[0]; in.ca = 16; break;
+    case 3: in.a = N->a[2]; in.ca = 32; break;
+    case 4: in.a = N->pool[1]; in.ca = 32; break;
+    case 5: in.a = N->a[4]; in.ca = 64; break;
+    case 6: in.a = N->pool[2]; in.ca = 64; break;
+    case 7: in.a = N->a[6]; in.ca = 96; break;
+    case 8: in.a = N->a[7]; in.ca = 96; in.a_half = 1; in.b = N->a[5]; in.cb = 64; break;
+    case 9: in.a = N->a[8]; in.ca = 64; break;
+    case 10: in.a = N->a[9]; in.ca = 64; in.a_half = 1; in.b = N->a[3]; in.cb = 32; break;
+    case 11: in.a = N->a[10]; in.ca = 32; break;
+    case 12: in.a = N->a[11]; in.ca = 32; in.a_half = 1; in.b = N->a[1]; in.cb = 16; break;
+    case 13: in.a = N->a[12]; in.ca = 16; break;
+    }
+    return in;
+}
+
+// forward pass from N->in0; the head writes `out` [V] FP32
+void forward(suli_nn* N, float* out) {
+    for (int l = 0; l < kConv; ++l) {
+        const LayerSpec& L = kLayer[l];
+        const ConvIn in = layer_input(N, l);
+        conv(N, N->vol[L.level], in, N->wb + N->off[l], N->w + N->off[l] + 27LL * L.cout * L.cin, 1, L.cout, N->a[l]);
+        if (l == 1 || l == 3 || l == 5) {   // pooling after each encoder level but the last
+            const int lv = L.level;
+            k_pool<<<nb(N->V[lv + 1] * L.cout), 256, 0, N->stream>>>(N->vol[lv], L.cout, N->a[l], N->pool[lv]);
+        }
+    }
+    k_head_fwd<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->a[13], N->w + N->off[kConv], out);
+}
+
+// backward from N->dout; accumulates parameter gradients into N->g (zeroed by the caller)
+void backward(suli_nn* N) {
+    // gradients w.r.t. each layer's output, accumulated where a tensor feeds two consumers
+    for (int l = 0; l < kConv; ++l)
+        k_zero_bf<<<nb(N->V[kLayer[l].level] * kLayer[l].cout), 256, 0, N->stream>>>(N->V[kLayer[l].level] * kLayer[l].cout, N->gact[l]);
+    k_head_bwd<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->a[13], N->w + N->off[kConv], N->dout, N->gact[13],
+                                                  N->g + N->off[kConv]);
+    for (int l = kConv - 1; l >= 0; --l) {
+        const LayerSpec& L = kLayer[l];
+        const Vol& vol = N->vol[L.level];
+        const long long n = N->V[L.level] * L.cout;
+        k_relu_bwd<<<nb(n), 256, 0, N->stream>>>(n, N->a[l], N->gact[l]);
+        const ConvIn in = layer_input(N, l);
+        wgrad(N, vol, in, L.cout, N->gact[l], N->g + N->off[l], N->g + N->off[l] + 27LL * L.cout * L.cin);
+        if (l == 0) break;   // no gradient w.r.t. the network input
+        // dX = conv(dZ, flipped W) on the tensor cores
+        k_flip_weights<<<nb(27LL * L.cin * L.cout), 256, 0, N->stream>>>(L.cin, L.cout, N->wb + N->off[l], N->wflip);
+        ConvIn gin{N->gact[l], L.cout, 0, nullptr, 0};
+        if (in.cb > 0) {
+            // decoder concat(up(coarse), skip): coarse part -> sum over the 8 children (its only
+            // consumer), skip part accumulates (the skip also feeds the pooling)
+            conv(N, vol, gin, N->wflip, nullptr, 0, L.cin, N->gcat);
+            const int coarse = (l == 8) ? 7 : (l == 10 ? 9 : 11);
+            const int skip = (l == 8) ? 5 : (l == 10 ? 3 : 1);
+            const long long nf = N->V[L.level] * in.cb, nc = N->V[L.level + 1] * in.ca;
+            k_concat_bwd<<<nb(nf > nc ? nf : nc), 256, 0, N->stream>>>(vol, in.ca, in.cb, N->gcat, N->gact[coarse],
+                                                                       N->gact[skip]);
+        } else if (l == 2 || l == 4 || l == 6) {
+            // the input was pooled: gradient through the pooling into the encoder output
+            conv(N, vol, gin, N->wflip, nullptr, 0, L.cin, N->gtmp);
+            const int src = l - 1, lv = kLayer[src].level;
+            k_pool_bwd<<<nb(N->V[lv] * kLayer[src].cout), 256, 0, N->stream>>>(N->vol[lv], kLayer[src].cout, N->gtmp,
+                                                                             N->gact[src]);
+        } else {
+            // plain chain: this layer is the only consumer of the previous output
+            conv(N, vol, gin, N->wflip, nullptr, 0, L.cin, N->gact[l - 1]);
+        }
+    }
+}
+
+template <class T>
+cudaError_t alloc(T** p, long long n) {
+    return cudaMalloc(reinterpret_cast<void**>(p), (size_t)n * sizeof(T));
+}
+
+int nn_fail(suli_nn* N, int code, const std::string& m) {
+    if (N) N->err = m;
+    return code;
+}
+
+}  // namespace
+
+namespace suli {
+namespace nn {
+void dims(const suli_nn* N, int* nx, int* ny, int* nz, int* device) {
+    *nx = N->vol[0].nx;
+    *ny = N->vol[0].ny;
+    *nz = N->vol[0].nz;
+    *device = N->device;
+}
+void forward_on(suli_nn* N, cudaStream_t stream, const float* d_in3, float* d_out) {
+    const cudaStream_t own = N->stream;
+    N->stream = stream;
+    k_pack_input<<<nb(N->V[0]), 256, 0, stream>>>(N->V[0], d_in3, N->in0);
+    forward(N, d_out);
+    N->stream = own;
+}
+int forward_launches() { return 1 + kConv + (kLevels - 1) + 1; }
+}  // namespace nn
+}  // namespace suli
+
+extern "C" {
+
+long long suli_nn_num_params(void) {
+    long long n = 0;
+    for (int l = 0; l < kConv; ++l) n += conv_params(kLayer[l]);
+    return n + 17;
+}
+
+int suli_nn_create(int nx, int ny, int nz, int device, suli_nn** out) {
+    if (!out || nx < 8 || ny < 8 || nz < 8 || nx % 8 || ny % 8 || nz % 8) return SULI_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) { cudaGetLastError(); return SULI_ERR_NODEVICE; }
+    suli_nn* N = new suli_nn();
+    N->device = device;
+    // a blocking stream: work the caller queued on the legacy default stream (filling the
+    // input buffers) completes before the network's kernels read them
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&N->stream, cudaStreamDefault) != cudaSuccess) {
+        delete N;
+        return SULI_ERR_CUDA;
+    }
+    for (int l = 0; l < kLevels; ++l) {
+        N->vol[l] = Vol{nx >> l, ny >> l, nz >> l};
+        N->V[l] = (long long)(nx >> l) * (ny >> l) * (nz >> l);
+    }
+    long long o = 0;
+    for (int l = 0; l < kConv; ++l) { N->off[l] = o; o += conv_params(kLayer[l]); }
+    N->off[kConv] = o;
+    N->nparam = o + 17;
+    bool ok = true;
+    auto A = [&](cudaError_t e) { ok = ok && (e == cudaSuccess); };
+    A(alloc(&N->w, N->nparam)); A(alloc(&N->g, N->nparam)); A(alloc(&N->m, N->nparam)); A(alloc(&N->v, N->nparam));
+    A(alloc(&N->wb, N->nparam));
+    long long wmax = 0;
+    for (int l = 0; l < kConv; ++l) wmax = std::max(wmax, 27LL * kLayer[l].cin * kLayer[l].cout);
+    A(alloc(&N->wflip, wmax));
+    A(alloc(&N->in0, N->V[0] * 16));
+    for (int l = 0; l < kConv; ++l) {
+        A(alloc(&N->a[l], N->V[kLayer[l].level] * kLayer[l].cout));
+        A(alloc(&N->gact[l], N->V[kLayer[l].level] * kLayer[l].cout));
+    }
+    for (int l = 0; l < kLevels - 1; ++l) A(alloc(&N->pool[l], N->V[l + 1] * kCh[l]));
+    A(alloc(&N->gcat, N->V[0] * 48));
+    A(alloc(&N->gtmp, N->V[1] * 16));
+    A(alloc(&N->out, N->V[0]));
+    A(alloc(&N->dout, N->V[0]));
+    A(alloc(&N->sums, 4));
+    A(cudaMallocHost(&N->host_sums, 4 * sizeof(double)));
+    if (ok) {
+        A(cudaMemsetAsync(N->w, 0, N->nparam * 4, N->stream));
+        A(cudaMemsetAsync(N->m, 0, N->nparam * 4, N->stream));
+        A(cudaMemsetAsync(N->v, 0, N->nparam * 4, N->stream));
+        A(cudaMemsetAsync(N->wb, 0, N->nparam * 2, N->stream));
+        A(cudaStreamSynchronize(N->stream));
+    }
+    if (!ok) {
+        cudaGetLastError();
+        suli_nn_destroy(N);
+        return SULI_ERR_NOMEM;
+    }
+    *out = N;
+    return SULI_OK;
+}
+
+int suli_nn_destroy(suli_nn* N) {
+    if (!N) return SULI_OK;
+    cudaSetDevice(N->device);
+    if (N->stream) cudaStreamSynchronize(N->stream);
+    cudaFree(N->w); cudaFree(N->g); cudaFree(N->m); cudaFree(N->v); cudaFree(N->wb); cudaFree(N->wflip);
+    cudaFree(N->in0);
+    for (int l = 0; l < kConv; ++l) { cudaFree(N->a[l]); cudaFree(N->gact[l]); }
+    for (int l = 0; l < kLevels - 1; ++l) cudaFree(N->pool[l]);
+    cudaFree(N->gcat); cudaFree(N->gtmp); cudaFree(N->out); cudaFree(N->dout); cudaFree(N->sums);
+    if (N->host_sums) cudaFreeHost(N->host_sums);
+    if (N->stream) cudaStreamDestroy(N->stream);
+    delete N;
+    return SULI_OK;
+}
+
+const char* suli_nn_last_error(const suli_nn* N) { return N ? N->err.c_str() : "null network"; }
+
+int suli_nn_set_params(suli_nn* N, const float* host, long long n) {
+    if (!N || !host || n != N->nparam) return SULI_ERR_ARG;
+    cudaSetDevice(N->device);
+    if (cudaMemcpyAsync(N->w, host, n * 4, cudaMemcpyHostToDevice, N->stream) != cudaSuccess) return SULI_ERR_CUDA;
+    cudaMemsetAsync(N->m, 0, n * 4, N->stream);
+    cudaMemsetAsync(N->v, 0, n * 4, N->stream);
+    N->step = 0;
+    // the BF16 copy: an Adam pass with learning rate 0 leaves w unchanged
+    k_adam<<<nb(n), 256, 0, N->stream>>>(n, N->w, N->g, N->m, N->v, N->wb, 0.f, 0.9f, 0.999f, 1e-8f, 1.f, 1.f);
+    const cudaError_t e = cudaStreamSynchronize(N->stream);
+    return e == cudaSuccess ? SULI_OK : SULI_ERR_CUDA;
+}
+
+int suli_nn_get_params(suli_nn* N, float* host, long long n) {
+    if (!N || !host || n != N->nparam) return SULI_ERR_ARG;
+    cudaSetDevice(N->device);
+    if (cudaMemcpyAsync(host, N->w, n * 4, cudaMemcpyDeviceToHost, N->stream) != cudaSuccess) return SULI_ERR_CUDA;
+    return cudaStreamSynchronize(N->stream) == cudaSuccess ? SULI_OK : SULI_ERR_CUDA;
+}
+
+// forward on device buffers: in3 [V][3] FP32 (x fastest), out [V] FP32
+int suli_nn_forward(suli_nn* N, const float* d_in3, float* d_out) {
+    if (!N || !d_in3 || !d_out) return SULI_ERR_ARG;
+    cudaSetDevice(N->device);
+    k_pack_input<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], d_in3, N->in0);
+    forward(N, d_out);
+    const cudaError_t e = cudaStreamSynchronize(N->stream);
+    if (e != cudaSuccess) return nn_fail(N, SULI_ERR_CUDA, cudaGetErrorString(e));
+    return SULI_OK;
+}
+
+// loss and parameter gradient (host_grad may be null); the gradient stays in the device buffer
+int suli_nn_loss_grad(suli_nn* N, const float* d_in3, const float* d_target, double* loss, float* host_grad) {
+    if (!N || !d_in3 || !d_target) return SULI_ERR_ARG;
+    cudaSetDevice(N->device);
+    k_pack_input<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], d_in3, N->in0);
+    forward(N, N->out);
+    cudaMemsetAsync(N->sums, 0, 4 * sizeof(double), N->stream);
+    k_loss_sums<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->out, d_target, N->sums);
+    k_loss_grad<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->out, d_target, N->dout);
+    cudaMemsetAsync(N->g, 0, N->nparam * 4, N->stream);
+    backward(N);
+    cudaMemcpyAsync(N->host_sums, N->sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, N->stream);
+    if (host_grad) cudaMemcpyAsync(host_grad, N->g, N->nparam * 4, cudaMemcpyDeviceToHost, N->stream);
+    const cudaError_t e = cudaStreamSynchronize(N->stream);
+    if (e != cudaSuccess) return nn_fail(N, SULI_ERR_CUDA, cudaGetErrorString(e));
+    if (loss) *loss = N->host_sums[1] / (double)N->V[0];
+    return SULI_OK;
+}
+
+// one Adam step on the mean squared error between the prediction and d_target [V]
+int suli_nn_train_step(suli_nn* N, const float* d_in3, const float* d_target, float lr, double* loss) {
+    int r = suli_nn_loss_grad(N, d_in3, d_target, loss, nullptr);
+    if (r != SULI_OK) return r;
+    N->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - powf(b1, (float)N->step), c2 = 1.f - powf(b2, (float)N->step);
+    k_adam<<<nb(N->nparam), 256, 0, N->stream>>>(N->nparam, N->w, N->g, N->m, N->v, N->wb, lr, b1, b2, 1e-8f, c1, c2);
+    const cudaError_t e = cudaStreamSynchronize(N->stream);
+    return e == cudaSuccess ? SULI_OK : nn_fail(N, SULI_ERR_CUDA, cudaGetErrorString(e));
+}
+
+// The layer primitive on caller buffers (channels-last BF16), for tests: out = relu?(conv3(x) + b)
+int suli_nn_conv3d(int nx, int ny, int nz, const void* x, int cin, const void* w, const float* bias, int cout,
+                   int relu, void* out) {
+    if (!x || !w || !out || cin % 16 || cout % 8 || nx < 1 || ny < 1 || nz < 1) return SULI_ERR_ARG;
+    if (cout != 16 && cout != 32 && cout != 48 && cout != 64 && cout != 96 && cout != 160) return SULI_ERR_UNSUPPORTED;
+    if (cin > 160) return SULI_ERR_SIZE;
+    suli_nn tmp;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    tmp.device = dev;
+    tmp.stream = nullptr;
+    ConvIn in{static_cast<const __nv_bfloat16*>(x), cin, 0, nullptr, 0};
+    conv(&tmp, Vol{nx, ny, nz}, in, static_cast<const __nv_bfloat16*>(w), bias, relu, cout,
+         static_cast<__nv_bfloat16*>(out));
+    const cudaError_t e = cudaDeviceSynchronize();
+    return e == cudaSuccess ? SULI_OK : SULI_ERR_CUDA;
+}
+
+}  // extern "C"

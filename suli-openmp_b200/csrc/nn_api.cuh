@@ -1,0 +1,22 @@
+// nn_api.cuh — what the pressure solve needs from the network object (nn.cu), inside the
+// library: its grid, its device and a forward pass enqueued on the caller's stream.
+#pragma once
+#include <cuda_runtime.h>
+
+struct suli_nn;
+
+namespace suli {
+namespace nn {
+
+#define SULI_NN_INTERNAL __attribute__((visibility("hidden")))
+
+// Grid (cells) and device the network was created for.
+SULI_NN_INTERNAL void dims(const suli_nn* N, int* nx, int* ny, int* nz, int* device);
+// Forward pass on `stream` without synchronising: in3 [V][3] FP32 -> out [V] FP32 (device).
+// Uses the network's own activation buffers.
+SULI_NN_INTERNAL void forward_on(suli_nn* N, cudaStream_t stream, const float* d_in3, float* d_out);
+// Kernel launches of one forward pass (for the tracing counters).
+SULI_NN_INTERNAL int forward_launches();
+
+}  // namespace nn
+}  // namespace suli

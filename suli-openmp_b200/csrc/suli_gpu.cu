@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 #include "ctx.cuh"
+#include "nn_api.cuh"
 
 using namespace suli;
 
@@ -283,6 +284,10 @@ int suli_destroy(suli_ctx* c) {
     cudaFree(c->f32_arena);
     cudaFree(c->cg_e2);
     cudaFree(c->pcg);
+    cudaFree(c->nn_in);
+    cudaFree(c->nn_out);
+    cudaFree(c->nn_e0);
+    cudaFree(c->nn_scale);
     if (c->pcg_host) cudaFreeHost(c->pcg_host);
     if (c->cg_host) cudaFreeHost(c->cg_host);
     if (c->host_scalars) cudaFreeHost(c->host_scalars);
@@ -299,6 +304,16 @@ int suli_synchronize(suli_ctx* c) {
     return SULI_OK;
 }
 
+// true for pageable or pinned host memory, false for device or managed memory
+static bool host_memory(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered || a.type == cudaMemoryTypeHost;
+}
+
 int suli_upload(suli_ctx* c, int field, const double* host) {
     if (!c || !host || field < 0 || field >= SULI_F_COUNT) return fail(c, SULI_ERR_ARG, "upload: bad field");
     cudaSetDevice(c->device);
@@ -307,17 +322,21 @@ int suli_upload(suli_ctx* c, int field, const double* host) {
     const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
     const size_t n = (size_t)n0 * n1 * n2;
     if (is_plane(field)) {
-        CUDA_TRY(c, cudaMemcpyAsync(c->f[field], host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(c->f[field], host, n * sizeof(double), cudaMemcpyDefault, c->stream));
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
         return SULI_OK;
     }
     if (field == SULI_F_TF_U || field == SULI_F_TF_V || field == SULI_F_TF_W) {
-        for (size_t q = 0; q < n; ++q)
-            if (host[q] != 0.0) { c->tf_active = true; break; }
+        if (!host_memory(host)) {
+            c->tf_active = true;   // device data is not scanned: adding zeros changes nothing
+        } else {
+            for (size_t q = 0; q < n; ++q)
+                if (host[q] != 0.0) { c->tf_active = true; break; }
+        }
     }
     // stage through the CG q buffer (same size class as any field, free between calls)
     double* stage = c->cg_q;
-    CUDA_TRY(c, cudaMemcpyAsync(stage, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(stage, host, n * sizeof(double), cudaMemcpyDefault, c->stream));
     k_scatter<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->g, stage, c->f[field], lo[0], lo[1], lo[2], n0, n1, n2);
     CHECK_LAUNCH(c);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -332,14 +351,14 @@ int suli_download(suli_ctx* c, int field, double* host) {
     const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
     const size_t n = (size_t)n0 * n1 * n2;
     if (is_plane(field)) {
-        CUDA_TRY(c, cudaMemcpyAsync(host, c->f[field], n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(host, c->f[field], n * sizeof(double), cudaMemcpyDefault, c->stream));
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
         return SULI_OK;
     }
     double* stage = c->cg_q;
     k_gather<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->g, c->f[field], stage, lo[0], lo[1], lo[2], n0, n1, n2);
     CHECK_LAUNCH(c);
-    CUDA_TRY(c, cudaMemcpyAsync(host, stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(host, stage, n * sizeof(double), cudaMemcpyDefault, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return SULI_OK;
 }
@@ -603,10 +622,36 @@ int ensure_pcg_graphs(suli_ctx* c) {
 }
 
 // Mixed-precision solve: FP64 refinement around an FP32 multigrid-preconditioned CG.
+// Buffers of the learned guess and of recorded solves (allocated on first use).
+int ensure_nn_buffers(suli_ctx* c, bool net) {
+    const long long V = (long long)c->P.nx * c->P.ny * c->P.nz;
+    if (!c->nn_scale) CUDA_TRY(c, cudaMalloc(&c->nn_scale, sizeof(NNScale)));
+    if (!c->nn_e0) CUDA_TRY(c, cudaMalloc(&c->nn_e0, c->g.n * sizeof(double)));
+    if (net && !c->nn_in) CUDA_TRY(c, cudaMalloc(&c->nn_in, V * 3 * sizeof(float)));
+    if (net && !c->nn_out) CUDA_TRY(c, cudaMalloc(&c->nn_out, V * sizeof(float)));
+    return SULI_OK;
+}
+
+// After graddin's set-up: record the features and e0, or apply the learned initial guess.
+void nn_begin(suli_ctx* c) {
+    const bool rec = c->rec_in != nullptr;
+    const bool learn = !rec && c->nn && c->nn_mode == 1;
+    if (!rec && !learn) return;
+    ProfScope ps(c, SULI_K_NN, 2 + (learn ? suli::nn::forward_launches() + 3 : 0));
+    launch_nn_features(c, rec ? c->rec_in : c->nn_in);
+    if (rec) {
+        cudaMemcpyAsync(c->nn_e0, c->cg_e, c->g.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+        return;
+    }
+    suli::nn::forward_on(c->nn, c->stream, c->nn_in, c->nn_out);
+    launch_nn_step(c, c->nn_out, c->cg_e);
+}
+
 int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
     if (int rg = ensure_pcg_graphs(c)) return rg;
     launch_cg_setup(c);   // FP64 diagonal, coefficients, b~, first residual and threshold
     launch_mx_setup(c);   // FP32 faces of every multigrid level
+    nn_begin(c);
     double* ecur = c->cg_e;
     double* enext = c->cg_e2;
     launch_mx_residual(c, ecur, enext, false);
@@ -642,6 +687,7 @@ int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
     }
     c->last_outer_iters = outer;
     launch_cg_final(c, ecur);
+    if (c->rec_in) launch_nn_target(c, ecur, c->rec_target);
     CHECK_LAUNCH(c);
     int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
     if (r != SULI_OK) return r;
@@ -660,6 +706,7 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
     cudaSetDevice(c->device);
     if (c->P.precision == 1) return graddin_mixed(c, iters, resid);
     launch_cg_setup(c);
+    nn_begin(c);   // recording only: the learned guess needs the refinement loop
     CHECK_LAUNCH(c);
     // iteration 1 uses p_old = r with beta = 0 (erroppr = erropr, :172)
     launch_cg_iter(c, c->cg_r, c->cg_pa);
@@ -670,6 +717,7 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
     });
     if (r0 != SULI_OK) return r0;
     launch_cg_final(c, c->cg_e);
+    if (c->rec_in) launch_nn_target(c, c->cg_e, c->rec_target);
     CHECK_LAUNCH(c);
     int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
     if (r != SULI_OK) return r;
@@ -679,6 +727,38 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
     if (resid) *resid = (s.bb > 0.) ? std::sqrt(s.rr / s.bb) : 0.;
     if (s.status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the Poisson solve");
     return s.status;
+}
+
+int suli_attach_nn(suli_ctx* c, suli_nn* net, int mode) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (mode == 0) {
+        c->nn = nullptr;
+        c->nn_mode = 0;
+        return SULI_OK;
+    }
+    if (mode != 1 || !net) return fail(c, SULI_ERR_ARG, "attach_nn: mode must be 0 or 1 with a network");
+    if (c->P.precision != 1) return fail(c, SULI_ERR_UNSUPPORTED, "attach_nn: the learned guess needs precision 1");
+    int nx, ny, nz, dev;
+    suli::nn::dims(net, &nx, &ny, &nz, &dev);
+    if (nx != c->P.nx || ny != c->P.ny || nz != c->P.nz || dev != c->device)
+        return fail(c, SULI_ERR_ARG, "attach_nn: network grid or device differs from the context's");
+    if (int r = ensure_nn_buffers(c, true)) return r;
+    c->nn = net;
+    c->nn_mode = mode;
+    return SULI_OK;
+}
+
+int suli_graddin_record(suli_ctx* c, float* d_in3, float* d_target, int* iters, double* resid) {
+    if (!c || !d_in3 || !d_target) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (int r = ensure_nn_buffers(c, false)) return r;
+    c->rec_in = d_in3;
+    c->rec_target = d_target;
+    const int r = suli_graddin(c, iters, resid);
+    c->rec_in = nullptr;
+    c->rec_target = nullptr;
+    return r;
 }
 
 int suli_posdin(suli_ctx* c) {

@@ -81,6 +81,17 @@ class Solver:
         ptr = a.ctypes.data_as(C.POINTER(C.c_double))
         self._check(self.lib.suli_upload(self._h, FIELD[name], ptr), f"upload {name}")
 
+    def upload_device(self, name: str, t) -> None:
+        """Copy a field from device memory: `t` is a contiguous float64 torch tensor whose
+        shape is the field's Fortran shape reversed (so its memory order is Fortran order)."""
+        want = tuple(reversed(self.shape(name)))
+        if tuple(t.shape) != want or str(t.dtype) != "torch.float64" or not t.is_contiguous():
+            raise ValueError(f"upload_device {name}: need contiguous float64 of shape {want}")
+        import torch
+        torch.cuda.synchronize(t.device)   # the library copies on its own stream
+        ptr = C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_double))
+        self._check(self.lib.suli_upload(self._h, FIELD[name], ptr), f"upload {name}")
+
     def download(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
         """Copy a field to the host (into `out` if given: Fortran-ordered float64, e.g. a
         view of pinned memory)."""
@@ -167,6 +178,27 @@ class Solver:
         r = C.c_double()
         self._check(self.lib.suli_graddin(self._h, C.byref(n), C.byref(r)), "graddin")
         return n.value, r.value
+
+    def graddin_record(self, in3_ptr: int, target_ptr: int):
+        """graddin() that also writes the network's training pair for this solve into device
+        buffers: in3 [V][3] FP32 (input features) and target [V] FP32 (scaled correction)."""
+        import torch
+        torch.cuda.synchronize()   # buffers from torch's allocator: its pending work first
+        n = C.c_int()
+        r = C.c_double()
+        self._check(self.lib.suli_graddin_record(self._h, C.c_void_p(in3_ptr), C.c_void_p(target_ptr),
+                                                 C.byref(n), C.byref(r)), "graddin_record")
+        return n.value, r.value
+
+    def attach_nn(self, net, mode: int = 1) -> None:
+        """Use `net` (a `learned.Net` of the same grid) as the pressure solve's initial guess
+        (mode 1, precision 1), or detach it (mode 0 / net None)."""
+        if net is None or mode == 0:
+            self._check(self.lib.suli_attach_nn(self._h, None, 0), "attach_nn")
+            self._net = None
+            return
+        self._check(self.lib.suli_attach_nn(self._h, net.handle, int(mode)), "attach_nn")
+        self._net = net   # keep the network alive while attached
 
     def posdin(self) -> None:
         self._check(self.lib.suli_posdin(self._h), "posdin")

@@ -1,0 +1,117 @@
+"""GPU: the learned initial guess inside the mixed-precision pressure solve.
+
+* recorded training pairs: the density feature equals the downloaded density, the residual
+  feature has unit rms, and features and target are invariant to the scale of the RHS;
+* a network whose output is zero leaves the solve bit-for-bit unchanged (alpha = 0);
+* an untrained network still lets the solve reach the FP64 tolerance and the same pressure;
+* attaching is refused for the plain FP64 path and for a network of another grid.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+N = 32
+TOL = 1e-8
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as T
+    assert T.cuda.is_available()
+    return T
+
+
+def _problem(pkg, torch, seed, precision=1, scale=1.0):
+    p = pkg.snapshots.tank_params(n=N, precision=precision, cg_tol=TOL)
+    s = pkg.Solver(p)
+    gen = pkg.snapshots.SnapshotGenerator(s, seed)
+    ls = gen.level_set()
+    vel = gen.velocity()
+    return s, gen, ls, vel
+
+
+def _load(s, torch, ls, vel, scale=1.0):
+    s.upload_device("ls", ls.contiguous())
+    s.heaviside()
+    s.upload("prd1", 0.0)
+    for name, a in vel.items():
+        s.upload_device(name, (a * scale).contiguous())
+
+
+def test_record_features_and_scale_invariance(pkg, torch):
+    s, gen, ls, vel = _problem(pkg, torch, 3)
+    V = N ** 3
+    outs = []
+    for scale in (1.0, 2.0):
+        _load(s, torch, ls, vel, scale)
+        in3 = torch.empty(V * 3, dtype=torch.float32, device="cuda:0")
+        t = torch.empty(V, dtype=torch.float32, device="cuda:0")
+        iters, res = s.graddin_record(in3.data_ptr(), t.data_ptr())
+        assert res <= TOL and iters > 0
+        outs.append((in3.cpu().numpy().reshape(N, N, N, 3), t.cpu().numpy().reshape(N, N, N)))
+    (f1, t1), (f2, t2) = outs
+    p = s.params
+    rho = s.download("rho")                       # Fortran (nx, ny, nz)
+    h = (np.transpose(rho, (2, 1, 0)) - p.rho_f1) / (p.rho_f2 - p.rho_f1)
+    assert np.allclose(f1[..., 1], h, rtol=0, atol=1e-6)
+    assert abs(float(np.mean(f1[..., 0].astype(np.float64) ** 2)) - 1.0) < 1e-5
+    assert np.all(f1[..., 2] == 0)                 # e0 = 0: no previous-pressure feature
+    # doubling the RHS doubles r~0, s and e* - e0: the pair is unchanged
+    assert np.array_equal(f1, f2)
+    assert np.allclose(t1, t2, rtol=1e-6, atol=1e-6 * np.abs(t1).max())
+    assert np.abs(t1).max() > 0
+    s.close()
+
+
+def _solve(s, torch, ls, vel, net=None):
+    _load(s, torch, ls, vel)
+    s.attach_nn(net)
+    iters, res = s.graddin()
+    prd = s.download("prd1")
+    s.attach_nn(None)
+    return iters, res, prd
+
+
+def test_zero_network_is_a_no_op(pkg, torch):
+    s, gen, ls, vel = _problem(pkg, torch, 5)
+    it0, r0, p0 = _solve(s, torch, ls, vel)
+    net = pkg.learned.Net(N, N, N, params=np.zeros(pkg.learned.num_params(), np.float32))
+    it1, r1, p1 = _solve(s, torch, ls, vel, net)
+    assert (it1, r1) == (it0, r0)
+    assert np.array_equal(p1, p0)
+    s.close()
+    net.close()
+
+
+def test_untrained_network_converges_to_same_pressure(pkg, torch):
+    s, gen, ls, vel = _problem(pkg, torch, 7)
+    it0, r0, p0 = _solve(s, torch, ls, vel)
+    net = pkg.learned.Net(N, N, N, params=pkg.learned.init_params(1, head_scale=1.0))
+    it1, r1, p1 = _solve(s, torch, ls, vel, net)
+    assert r0 <= TOL and r1 <= TOL
+    # pressure is defined up to a constant (all-Neumann problem)
+    a = p0[1:-1, 1:-1, 1:-1] - p0[1:-1, 1:-1, 1:-1].mean()
+    b = p1[1:-1, 1:-1, 1:-1] - p1[1:-1, 1:-1, 1:-1].mean()
+    assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(a)
+    # the energy-optimal step cannot make the start worse; allow the count to wobble
+    assert it1 <= it0 + 3, (it0, it1)
+    s.close()
+    net.close()
+
+
+def test_attach_refusals(pkg, torch):
+    net = pkg.learned.Net(N, N, N)
+    p0 = pkg.snapshots.tank_params(n=N, precision=0)
+    s0 = pkg.Solver(p0)
+    with pytest.raises(pkg.SuliError) as e:
+        s0.attach_nn(net)
+    assert e.value.code == -4     # SULI_ERR_UNSUPPORTED
+    s0.close()
+    p1 = pkg.snapshots.tank_params(n=2 * N, precision=1)
+    s1 = pkg.Solver(p1)
+    with pytest.raises(pkg.SuliError) as e:
+        s1.attach_nn(net)
+    assert e.value.code == -1     # SULI_ERR_ARG
+    s1.close()
+    net.close()

@@ -1,0 +1,156 @@
+"""GPU: the network kernels (csrc/nn.cu, nn_conv.cuh) against references.
+
+* the tensor-core convolution against an FP64 convolution of the same BF16 inputs;
+* forward, loss and parameter gradient of the whole U-Net against the FP64 oracle
+  (oracle/unet_ref.py, itself pinned by finite differences), with the conv weights and the
+  input rounded to BF16 as the GPU reads them.  The GPU keeps activations and activation
+  gradients in BF16, so the tolerances are those of BF16 storage (2^-8 relative per value),
+  stated per check below;
+* Adam steps lower the loss; forward passes are deterministic.
+"""
+import numpy as np
+import pytest
+
+import unet_ref
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as T
+    assert T.cuda.is_available()
+    return T
+
+
+def _bf16(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(torch.bfloat16)
+
+
+@pytest.mark.parametrize("shape,cin,cout,relu", [
+    ((12, 10, 9), 16, 16, True),
+    ((8, 8, 8), 32, 48, False),
+    ((9, 5, 7), 160, 64, True),
+    ((16, 8, 4), 96, 96, False),
+    ((6, 6, 6), 64, 160, False),
+    ((10, 4, 12), 16, 32, True),
+])
+def test_conv3d_matches_fp64(pkg, torch, shape, cin, cout, relu):
+    nx, ny, nz = shape
+    rng = np.random.default_rng(cin * 1000 + cout)
+    x = _bf16(torch, rng.standard_normal((nz, ny, nx, cin)))
+    w = _bf16(torch, rng.standard_normal((27, cout, cin)) / np.sqrt(27 * cin))
+    b = torch.from_numpy(rng.standard_normal(cout).astype(np.float32))
+    out = torch.empty((nz, ny, nx, cout), dtype=torch.bfloat16, device="cuda:0")
+    xd, wd, bd = x.to("cuda:0"), w.to("cuda:0"), b.to("cuda:0")
+    pkg.learned.conv3d(xd, wd, bd, out, shape, cin, cout, relu)
+    torch.cuda.synchronize()
+    # FP64 reference: cross-correlation with zero padding, tap = dx + 3 dy + 9 dz
+    xin = x.double().permute(3, 0, 1, 2).unsqueeze(0)              # (1, cin, nz, ny, nx)
+    wt = w.double().reshape(3, 3, 3, cout, cin).permute(3, 4, 0, 1, 2)   # (cout, cin, dz, dy, dx)
+    ref = torch.nn.functional.conv3d(xin, wt, b.double(), padding=1)[0].permute(1, 2, 3, 0)
+    if relu:
+        ref = ref.clamp_min(0.0)
+    got = out.double().cpu()
+    err = (got - ref).abs()
+    # BF16 rounding of the output (<= 2^-9 relative) plus FP32 accumulation order
+    tol = 2.0 ** -8 * ref.abs() + 1e-5 * ref.abs().max()
+    assert bool((err <= tol).all()), float((err - tol).max())
+
+
+def _setup(torch, n, seed):
+    rng = np.random.default_rng(seed)
+    theta = unet_ref.init_params(seed)
+    o = 0
+    for ci, co, _ in unet_ref.LAYERS:
+        o += 27 * co * ci
+        theta[o:o + co] = 0.05 * rng.standard_normal(co)
+        o += co
+    theta[o:o + 16] = rng.standard_normal(16)
+    theta[o + 16] = 0.3
+    theta32 = theta.astype(np.float32)
+    x3 = rng.standard_normal((n, n, n, 3)).astype(np.float32)
+    tgt = rng.standard_normal((n, n, n)).astype(np.float32)
+    # what the GPU computes with: BF16 conv weights and input, FP32 biases and head
+    theta_ref = theta32.astype(np.float64)
+    o = 0
+    for ci, co, _ in unet_ref.LAYERS:
+        nw = 27 * co * ci
+        theta_ref[o:o + nw] = _bf16(torch, theta32[o:o + nw]).double().numpy()
+        o += nw + co
+    x3_ref = _bf16(torch, x3).double().numpy()
+    return theta32, theta_ref, x3, x3_ref, tgt
+
+
+def _layer_slices():
+    out, o = [], 0
+    for l, (ci, co, _) in enumerate(unet_ref.LAYERS):
+        out.append((f"W{l}", slice(o, o + 27 * co * ci)))
+        o += 27 * co * ci
+        out.append((f"b{l}", slice(o, o + co)))
+        o += co
+    out.append(("head", slice(o, o + 17)))
+    return out
+
+
+def test_forward_matches_oracle(pkg, torch):
+    n = 16
+    theta32, theta_ref, x3, x3_ref, _ = _setup(torch, n, 5)
+    net = pkg.learned.Net(n, n, n, params=theta32)
+    d_in = torch.from_numpy(x3).to("cuda:0")
+    d_out = torch.empty(n ** 3, dtype=torch.float32, device="cuda:0")
+    net.forward(d_in, d_out)
+    got = d_out.cpu().numpy().reshape(n, n, n)
+    ref, _ = unet_ref.forward(theta_ref, x3_ref)
+    rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    # 14 layers of BF16 activations: a few 2^-8 roundings per value, far below 5%
+    assert rel < 0.03, rel
+    # deterministic: a second pass gives the same bits
+    d_out2 = torch.empty_like(d_out)
+    net.forward(d_in, d_out2)
+    assert torch.equal(d_out, d_out2)
+    net.close()
+
+
+def test_loss_and_gradient_match_oracle(pkg, torch):
+    n = 16
+    theta32, theta_ref, x3, x3_ref, tgt = _setup(torch, n, 7)
+    net = pkg.learned.Net(n, n, n, params=theta32)
+    d_in = torch.from_numpy(x3).to("cuda:0")
+    d_t = torch.from_numpy(tgt.ravel()).to("cuda:0")
+    loss, g = net.loss_grad(d_in, d_t)
+    loss_ref, g_ref = unet_ref.loss_grad(theta_ref, x3_ref, tgt.astype(np.float64))
+    assert abs(loss - loss_ref) <= 0.03 * loss_ref, (loss, loss_ref)
+    g = g.astype(np.float64)
+    cos = float(g @ g_ref / (np.linalg.norm(g) * np.linalg.norm(g_ref)))
+    assert cos > 0.995, cos
+    worst = {}
+    for name, sl in _layer_slices():
+        if name == "W0":    # weights of the zero-padded input channels: compare the real ones
+            a = g[sl].reshape(27, 16, 16)[:, :, :3]
+            b = g_ref[sl].reshape(27, 16, 16)[:, :, :3]
+        else:
+            a, b = g[sl], g_ref[sl]
+        worst[name] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+    # BF16 activation gradients through up to 14 layers: per-block relative error under 10%
+    assert max(worst.values()) < 0.10, worst
+    net.close()
+
+
+def test_adam_lowers_loss_and_params_roundtrip(pkg, torch):
+    n = 16
+    theta32, _, x3, _, tgt = _setup(torch, n, 11)
+    net = pkg.learned.Net(n, n, n, params=theta32)
+    assert np.array_equal(net.get_params(), theta32)
+    d_in = torch.from_numpy(x3).to("cuda:0")
+    d_t = torch.from_numpy(tgt.ravel()).to("cuda:0")
+    losses = [net.train_step(d_in, d_t, 1e-3) for _ in range(40)]
+    assert losses[-1] < 0.7 * losses[0], losses[::8]
+    w = net.get_params()
+    assert not np.array_equal(w, theta32) and np.all(np.isfinite(w))
+    net.close()
+
+
+def test_bad_grid_refused(pkg):
+    with pytest.raises(pkg.learned.NetError):
+        pkg.learned.Net(12, 16, 16)
