@@ -59,8 +59,13 @@ def parse_args():
     ap.add_argument("--dx", type=float, default=0.005)
     ap.add_argument("--cg-tol", type=float, default=1e-8)
     ap.add_argument("--inner-tol", type=float, default=1e-3, help="relative tolerance of each FP32 inner solve")
-    ap.add_argument("--path", choices=["both", "plain", "mixed"], default="both",
-                    help="time both solver paths (headline = mixed) or one of them (for profiling)")
+    ap.add_argument("--mg-omega", type=float, default=0.8, help="damping of the multigrid Jacobi sweeps")
+    ap.add_argument("--mg-alpha", type=float, default=1.0, help="scale of the multigrid coarse-grid correction")
+    ap.add_argument("--path", choices=["all", "plain", "mixed", "learned"], default="all",
+                    help="time every solver path (headline = learned + mixed precision) or one of them")
+    ap.add_argument("--weights", default=None, help="network weights (.npy); default: the shipped ones")
+    ap.add_argument("--mms-n", type=int, default=128, help="grid of the manufactured-solution check (0: skip)")
+    ap.add_argument("--mms-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-cap", type=int, default=20, help="CG iterations per solve in the CPU sample")
@@ -288,12 +293,15 @@ def workload_config(p, args, path):
     }
 
 
-def time_path(args, dist, pkg, p, init, dev, it0=0):
-    """Warm up, then time K steps of one solver path with CUDA events on its own stream."""
+def time_path(args, dist, pkg, p, init, dev, it0=0, net=None):
+    """Warm up, then time K steps of one solver path with CUDA events on its own stream
+    (with `net` attached as the pressure solve's initial guess, if given)."""
     import torch
 
     s = pkg.Solver(p, device=dev)
     init(s)
+    if net is not None:
+        s.attach_nn(net)
     ext = torch.cuda.ExternalStream(s.stream_ptr, device=dev)
     it = it0
     for _ in range(args.warmup):
@@ -356,7 +364,46 @@ def mixed_params(p, args):
     q = p.copy()
     q.precision, q.cg_stop, q.cg_tol = 1, 1, args.cg_tol
     q.inner_tol, q.refine_maxit = args.inner_tol, 30
+    q.mg_omega, q.mg_alpha = args.mg_omega, args.mg_alpha
     return q
+
+
+def load_net(pkg, p, args, dev):
+    """The trained network for this grid, or None when no weights are available."""
+    import pathlib as _pl
+    path = _pl.Path(args.weights) if args.weights else pkg.learned.WEIGHTS_PATH
+    if not path.exists():
+        return None, f"no weights at {path}"
+    name = str(path.relative_to(ROOT)) if path.is_relative_to(ROOT) else str(path)
+    return pkg.learned.Net.load(p.nx, p.ny, p.nz, device=dev, path=path), name
+
+
+def mms_check(pkg, args, dev):
+    """Manufactured solution on the periodic box (cases.TaylorGreenMMS): errors of the FP64
+    and the mixed path against the exact fields, and of the mixed path against FP64."""
+    import numpy as np
+    out = {"grid": f"{args.mms_n}^3 periodic [0,2pi]^3, nu=0.01, dt=1e-3, RK3", "steps": args.mms_steps}
+    fields = {}
+    for prec, tag in ((0, "fp64"), (1, "mixed")):
+        m = pkg.cases.TaylorGreenMMS(args.mms_n, precision=prec, cg_tol=1e-10)
+        s = pkg.Solver(m.p, device=dev)
+        m.init(s)
+        divs = []
+        t0 = time.perf_counter()
+        for it in range(1, args.mms_steps + 1):
+            divs.append(m.step(s, it)["max_div"])
+        wall = time.perf_counter() - t0
+        out[tag] = {"vs_exact": m.errors(s, args.mms_steps * m.p.dt), "max_div": max(divs),
+                    "wall_s_incl_host_source_upload": wall}
+        f = {k: s.download(k) for k in ("u", "v", "w")}
+        pr = s.download("prd1")[1:-1, 1:-1, 1:-1]
+        f["prd1"] = pr - pr.mean()
+        fields[tag] = f
+        s.close()
+    out["mixed_vs_fp64_rel_max"] = {
+        k: float(np.abs(fields["mixed"][k] - fields["fp64"][k]).max() / max(np.abs(fields["fp64"][k]).max(), 1e-300))
+        for k in ("u", "v", "w", "prd1")}
+    return out
 
 
 def run_ours(args):
@@ -368,28 +415,31 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     pkg = load_pkg()
     p, init = pkg.cases.sloshing(nx=args.nx, ny=args.ny, nz=args.nz, dx=args.dx, cg_tol=args.cg_tol)
-    # plain FP64 path (the reference's Jacobi-scaled CG): timed for the comparison
     q = mixed_params(p, args)
-    if args.path in ("both", "plain"):
-        plain = time_path(args, dist, pkg, p, init, dev)
-        if args.path == "plain":
-            head = plain
-            q = p
-        else:
-            plain["solver"].close()
-        roof_plain = cg_roofline(p, plain["prof"])
-    if args.path in ("both", "mixed"):
-        # headline path: mixed precision (FP32 multigrid-preconditioned inner CG, FP64 refinement)
-        head = time_path(args, dist, pkg, q, init, dev)
-        if args.path == "mixed":
-            plain, roof_plain = head, None
+    runs = {}
+    # plain FP64 path (the reference's Jacobi-scaled CG): the comparison
+    if args.path in ("all", "plain"):
+        runs["plain"] = time_path(args, dist, pkg, p, init, dev)
+    # mixed precision: FP32 multigrid-preconditioned inner CG inside FP64 refinement
+    if args.path in ("all", "mixed"):
+        runs["mixed"] = time_path(args, dist, pkg, q, init, dev)
+    # learned + mixed: the network's guess starts every pressure solve
+    net, net_src = None, None
+    if args.path in ("all", "learned"):
+        net, net_src = load_net(pkg, q, args, dev)
+        if net is not None:
+            runs["learned"] = time_path(args, dist, pkg, q, init, dev, net=net)
+        elif args.path == "learned":
+            raise SystemExit(f"--path learned: {net_src}")
+    head_key = "learned" if "learned" in runs else ("mixed" if "mixed" in runs else "plain")
+    head = runs[head_key]
+    for k, r in runs.items():
+        if k != head_key:
+            r["solver"].close()
     s = head["solver"]
     it = head["it"]
     value, ms, prof, stats, clk = head["value"], head["ms"], head["prof"], head["stats"], head["clocks"]
-    iters_per_step = plain["iters_per_step"]
-    launches = head["launches"]
-    kernels = head["kernels"]
-    roofline = roof_plain
+    roofline = cg_roofline(p, runs["plain"]["prof"]) if "plain" in runs else None
     # ---- end to end through the C-ABI: pinned host state in and out every step
     e2e = None
     if not args.no_e2e:
@@ -415,39 +465,60 @@ def run_ours(args):
         s.synchronize()
         t_e2e = dist.max(time.perf_counter() - t0)
         e2e = {"value": dist.world * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": h2d, "fields": names}
+               "d2h_bytes_per_step": h2d, "fields": names, "path": head_key}
+    s.close()
+    if net is not None:
+        net.close()
     # ---- CPU baseline (rank 0, N = 1 only)
     cpu = None
+    ref_iters = runs["plain"]["iters_per_step"] if "plain" in runs else head["iters_per_step"]
     if dist.world == 1 and not args.no_cpu_baseline:
-        cs = cpu_sample(pkg, p, init, args.cpu_cap, iters_per_step)
+        cs = cpu_sample(pkg, p, init, args.cpu_cap, ref_iters)
         cpu = {"value": 1.0 / cs["t_step_s"], "unit": UNIT, "cores": cs["cores"], "kind": "port",
                "sample": (f"one step of the OpenMP FP64 restatement at full size with Poisson solves capped at "
-                          f"{args.cpu_cap} iterations, scaled to the {iters_per_step:.0f} iterations per step the GPU "
+                          f"{args.cpu_cap} iterations, scaled to the {ref_iters:.0f} iterations per step the GPU "
                           f"measured: non-Poisson {cs['t_noncg_s']:.2f} s + {cs['t_iter_s'] * 1e3:.2f} ms/iteration"),
                "detail": cs}
-    s.close()
+    mms = None
+    if dist.world == 1 and args.mms_n > 0:
+        mms = mms_check(pkg, args, dev)
     if dist.rank == 0:
-        cfg = workload_config(q, args, "mixed: FP64 stencils, FP32 multigrid-preconditioned inner CG inside FP64 "
-                                       "iterative refinement to the same FP64 relative residual")
+        desc = {"plain": "plain FP64: the reference's Jacobi-scaled CG",
+                "mixed": "mixed: FP64 stencils, FP32 multigrid-preconditioned inner CG inside FP64 iterative "
+                         "refinement to the same FP64 relative residual",
+                "learned": "learned + mixed: the U-Net's guess (energy-optimal FP64 step) starts every pressure "
+                           "solve of the mixed path, which then runs to the same FP64 relative residual"}
+        cfg = workload_config(q if head_key != "plain" else p, args, desc[head_key])
         cfg["inner_tol"] = args.inner_tol
+        cfg["mg_omega"], cfg["mg_alpha"] = args.mg_omega, args.mg_alpha
+        if net_src:
+            cfg["weights"] = net_src
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f64+f32+bf16" if head_key == "learned" else "f64+f32", "data": "synthetic",
             "config": cfg,
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk, "inner_iters_per_step": head["iters_per_step"],
-            "max_div": stats[-1]["max_div"], "cg_resid": stats[-1]["cg_resid"], "kernels": kernels,
-            "plain_fp64": {"value": plain["value"], "ms_per_step": plain["ms"] / args.steps,
-                           "cg_iters_per_step": plain["iters_per_step"], "max_div": plain["stats"][-1]["max_div"],
-                           "cg_resid": plain["stats"][-1]["cg_resid"], "clocks": plain["clocks"],
-                           "gpu_launches": plain["launches"], "kernels": plain["kernels"]},
-            "speedup_vs_plain_fp64": value / plain["value"],
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["launches"],
+            "clocks": clk, "poisson_iters_per_step": head["iters_per_step"],
+            "max_div": stats[-1]["max_div"], "cg_resid": stats[-1]["cg_resid"], "kernels": head["kernels"],
         }
-        if args.path != "both":   # a single path timed (profiling runs): no comparison block
-            line.pop("plain_fp64")
-            line.pop("speedup_vs_plain_fp64")
-            line["config"]["path"] = args.path
+        for k, r in runs.items():
+            if k == head_key:
+                continue
+            line[{"plain": "plain_fp64", "mixed": "mixed_no_net", "learned": "learned"}[k]] = {
+                "value": r["value"], "ms_per_step": r["ms"] / args.steps,
+                "poisson_iters_per_step": r["iters_per_step"], "max_div": r["stats"][-1]["max_div"],
+                "cg_resid": r["stats"][-1]["cg_resid"], "clocks": r["clocks"], "gpu_launches": r["launches"],
+                "kernels": r["kernels"]}
+        if "plain" in runs and head_key != "plain":
+            line["speedup_vs_plain_fp64"] = value / runs["plain"]["value"]
+        if "mixed" in runs and head_key == "learned":
+            line["learned_vs_mixed"] = {"speedup": value / runs["mixed"]["value"],
+                                        "poisson_iters_saved_per_step":
+                                            runs["mixed"]["iters_per_step"] - head["iters_per_step"]}
+        if mms is not None:
+            line["mms"] = mms
+        line["config"]["path"] = head_key
         print(json.dumps(line), flush=True)
     dist.close()
     return 0

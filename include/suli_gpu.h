@@ -85,7 +85,9 @@ typedef struct suli_params {
     int    precision;               /* 0 = plain FP64; 1 = FP32 stencils + FP32 inner CG with FP64 refinement */
     int    refine_maxit;            /* outer FP64 refinement sweeps for precision 1            */
     double inner_tol;               /* relative tolerance of each FP32 inner solve             */
-    int    reserved[8];
+    double mg_omega;                /* precision 1: damping of the multigrid Jacobi sweeps (0 = 0.8) */
+    double mg_alpha;                /* precision 1: scale of the coarse-grid correction (0 = 1)       */
+    int    reserved[4];
 } suli_params;
 
 /* ---- field identifiers (module arrays of 0_modules.f90) ------------------------------ */

@@ -41,7 +41,9 @@ class SuliParams(C.Structure):
         ("precision", C.c_int),
         ("refine_maxit", C.c_int),
         ("inner_tol", C.c_double),
-        ("reserved", C.c_int * 8),
+        ("mg_omega", C.c_double),
+        ("mg_alpha", C.c_double),
+        ("reserved", C.c_int * 4),
     ]
 
     def copy(self) -> "SuliParams":
@@ -164,6 +166,7 @@ def default_params() -> SuliParams:
     p.vol_tol = 0.1
     p.cg_stop, p.cg_tol, p.cg_maxit = 0, 0.0001, 10000
     p.precision, p.refine_maxit, p.inner_tol = 0, 20, 1e-3
+    p.mg_omega, p.mg_alpha = 0.8, 1.0
     return p
 
 

@@ -137,3 +137,118 @@ def random_state(p: SuliParams, seed: int = 0, *, vel=0.2, wave=0.03):
         out[name] = vel * rng.standard_normal(sh)
     out["prd1"] = 0.01 * rng.standard_normal(field_shape(p, "prd1"))
     return out
+
+
+class TaylorGreenMMS:
+    """Manufactured solution on the periodic box [0, 2 pi]^3, single phase (rho 1, nu):
+
+        u = sin x cos y cos z e^-t,  v = -cos x sin y cos z e^-t,  w = 0,
+        p = (cos 2x + cos 2y) e^-2t / 4.
+
+    The velocity is divergence-free; the source that makes it an exact solution of the
+    incompressible Navier-Stokes equations (d_t u + u.grad u = -grad p + nu lap u + f) is
+
+        f_u = (3 nu - 1) u - sin 2x sin^2 z e^-2t / 2,
+        f_v = (3 nu - 1) v - sin 2y sin^2 z e^-2t / 2,   f_w = 0,
+
+    added through the reference's source-term arrays tf_u/v/w (6_convdiff.f90:156,168,183),
+    refreshed once per step at t = it dt as the reference's MMS driver does
+    (1_principal.f90:69-71).  Unlike that driver, the projection runs (graddin, posdin), so the
+    solver's own pressure is checked too.  x, y, z periodic; RK3; the level set is constant
+    (one phase), so the interface terms vanish.
+    """
+
+    def __init__(self, n=128, nu=0.01, dt=1e-3, precision=0, cg_tol=1e-10):
+        p = default_params()
+        p.nx = p.ny = p.nz = n
+        p.dx = p.dy = p.dz = 2.0 * math.pi / n
+        p.dt = dt
+        p.ccx0 = p.ccxf = p.ccy0 = p.ccyf = p.ccz0 = p.cczf = 0
+        p.t_tempo = 2
+        p.m_turb = 0
+        p.rho_f1 = p.rho_f2 = 1.0
+        p.mi_f1 = p.mi_f2 = nu
+        p.sigma = 0.0
+        p.gx = p.gz = 0.0
+        p.cg_stop, p.cg_tol, p.cg_maxit = 1, cg_tol, 20000
+        p.precision = precision
+        p.dt1 = 0.1 * p.dx
+        self.p, self.nu = p, nu
+
+    def _grid(self, name):
+        """Coordinates of a field's points over its Fortran extents."""
+        from ._abi import field_extent
+        p = self.p
+        (i0, i1), (j0, j1), (k0, k1) = field_extent(p, name)
+        fx, fy, fz = {"u": (1, 0, 0), "tf_u": (1, 0, 0), "v": (0, 1, 0), "tf_v": (0, 1, 0),
+                      "w": (0, 0, 1), "tf_w": (0, 0, 1)}.get(name, (0, 0, 0))
+        x = (np.arange(i0, i1 + 1) - (1.0 if fx else 0.5)) * p.dx
+        y = (np.arange(j0, j1 + 1) - (1.0 if fy else 0.5)) * p.dy
+        z = (np.arange(k0, k1 + 1) - (1.0 if fz else 0.5)) * p.dz
+        return np.meshgrid(x, y, z, indexing="ij")
+
+    def exact(self, name, t):
+        X, Y, Z = self._grid(name)
+        e = math.exp(-t)
+        if name == "u":
+            return np.sin(X) * np.cos(Y) * np.cos(Z) * e
+        if name == "v":
+            return -np.cos(X) * np.sin(Y) * np.cos(Z) * e
+        if name == "w":
+            return np.zeros_like(X)
+        if name == "prd1":
+            return 0.25 * (np.cos(2 * X) + np.cos(2 * Y)) * e * e
+        raise KeyError(name)
+
+    def source(self, name, t):
+        # f = (3 nu - 1) e^-t A(x) - e^-2t B(x) / 2: the spatial factors are computed once
+        if not hasattr(self, "_src"):
+            self._src = {}
+        if name not in self._src:
+            X, Y, Z = self._grid(name)
+            if name == "tf_u":
+                self._src[name] = (np.sin(X) * np.cos(Y) * np.cos(Z), np.sin(2 * X) * np.sin(Z) ** 2)
+            elif name == "tf_v":
+                self._src[name] = (-np.cos(X) * np.sin(Y) * np.cos(Z), np.sin(2 * Y) * np.sin(Z) ** 2)
+            elif name == "tf_w":
+                self._src[name] = (np.zeros_like(X), np.zeros_like(X))
+            else:
+                raise KeyError(name)
+        a, b = self._src[name]
+        e = math.exp(-t)
+        return (3.0 * self.nu - 1.0) * e * a - 0.5 * e * e * b
+
+    def init(self, model):
+        model.iniciais(0.0)
+        model.upload("ls", 1.0)
+        model.level_set_ini()
+        for name in ("u", "v", "w", "prd1"):
+            model.upload(name, self.exact(name, 0.0))
+        model.contorno(1)
+        model.contorno(3)
+
+    def step(self, model, it):
+        t = it * self.p.dt
+        for name in ("tf_u", "tf_v", "tf_w"):
+            model.upload(name, self.source(name, t))
+        return model.step(it)
+
+    def errors(self, model, t):
+        """L2 (rms) and Linf errors of u, v, w (interior faces) and of the mean-free pressure
+        (cells) against the exact solution at time t."""
+        n = self.p.nx
+        out = {}
+        for name in ("u", "v", "w", "prd1"):
+            got = model.download(name)
+            ref = self.exact(name, t)
+            if name == "prd1":
+                g = got[1:n + 1, 1:n + 1, 1:n + 1]
+                r = ref[1:n + 1, 1:n + 1, 1:n + 1]
+                g, r = g - g.mean(), r - r.mean()
+            else:
+                sl = {"u": np.s_[1:n + 1, 1:n + 1, 1:n + 1], "v": np.s_[1:n + 1, 1:n + 1, 1:n + 1],
+                      "w": np.s_[1:n + 1, 1:n + 1, 1:n + 1]}[name]
+                g, r = got[sl], ref[sl]
+            d = g - r
+            out[name] = {"l2": float(np.sqrt(np.mean(d * d))), "linf": float(np.abs(d).max())}
+        return out

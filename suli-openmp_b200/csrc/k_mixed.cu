@@ -192,10 +192,12 @@ __global__ void __launch_bounds__(256) k_mg_jacc(Geo G, BC bc, const float* __re
     }
 }
 
-// x_out = x' + w (f - A x')/dg with x' = y + P xc (piecewise-constant prolongation)
+// x_out = x' + w (f - A x')/dg with x' = y + a P xc (piecewise-constant prolongation, the
+// coarse correction scaled by a)
 __global__ void __launch_bounds__(256) k_mg_post(Geo Gf, Geo Gc, BC bc, const float* __restrict__ y,
                                                  const float* __restrict__ xc, const float* __restrict__ f, MGOps A,
-                                                 float* __restrict__ xout, float omega, const PCGState* st) {
+                                                 float* __restrict__ xout, float omega, float alpha,
+                                                 const PCGState* st) {
     if (st->done) return;
     const Col q = column(Gf, bc);
     if (!q.in) return;
@@ -204,12 +206,12 @@ __global__ void __launch_bounds__(256) k_mg_post(Geo Gf, Geo Gc, BC bc, const fl
     const int ixm = map_any(q.i - 1, Gf.nx, bc.perx), ixp = map_any(q.i + 1, Gf.nx, bc.perx);
     const int jym = map_any(q.j - 1, Gf.ny, bc.pery), jyp = map_any(q.j + 1, Gf.ny, bc.pery);
     const int I = (q.i + 1) >> 1, J = (q.j + 1) >> 1;
-    auto par = [&](int ii, int jj, int kk) { return xc[Gc.idx((ii + 1) >> 1, (jj + 1) >> 1, (kk + 1) >> 1)]; };
+    auto par = [&](int ii, int jj, int kk) { return alpha * xc[Gc.idx((ii + 1) >> 1, (jj + 1) >> 1, (kk + 1) >> 1)]; };
     float col[kKZ + 2];
 #pragma unroll
     for (int m = 0; m < kKZ + 2; ++m) {
         const int k = map_any(q.k0 - 1 + m, Gf.nz, bc.perz);
-        col[m] = y[q.c0 + pxy * k] + xc[Gc.idx(I, J, (k + 1) >> 1)];
+        col[m] = y[q.c0 + pxy * k] + alpha * xc[Gc.idx(I, J, (k + 1) >> 1)];
     }
 #pragma unroll
     for (int m = 0; m < kKZ; ++m) {
@@ -567,7 +569,8 @@ void launch_pcg_init(suli_ctx* c, int maxit) {
 
 // z = M r: one V-cycle; the last level-0 sweep also forms r.z and beta
 void launch_vcycle(suli_ctx* c) {
-    const float om = 0.8f;
+    const float om = (float)c->P.mg_omega;
+    const float alpha = (float)c->P.mg_alpha;
     const int L = (int)c->mg.size();
     const BC bc = c->bc;
     for (int l = 0; l < L - 1; ++l) {
@@ -589,7 +592,7 @@ void launch_vcycle(suli_ctx* c) {
         MGLevel& M = c->mg[l];
         MGLevel& C = c->mg[l + 1];
         const float* f = (l == 0) ? c->pc_r : M.f;
-        k_mg_post<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, C.y, f, ops(M), M.x, om, c->pcg);
+        k_mg_post<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, C.y, f, ops(M), M.x, om, alpha, c->pcg);
         k_mg_jacc<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, M.x, f, ops(M), M.y, om, c->pcg, l == 0 ? 1 : 0,
                                                        c->red_partial, c->red_counter);
     }

@@ -120,6 +120,8 @@ int validate(const suli_params* p, std::string& why) {
         if (p->cg_stop != 1) { why = "precision 1 stops on the relative FP64 residual (cg_stop = 1)"; return SULI_ERR_ARG; }
         if (p->refine_maxit < 1) { why = "refine_maxit must be >= 1"; return SULI_ERR_ARG; }
         if (!(p->inner_tol > 0 && p->inner_tol < 1)) { why = "inner_tol must lie in (0, 1)"; return SULI_ERR_ARG; }
+        if (!(p->mg_omega >= 0 && p->mg_omega < 1)) { why = "mg_omega must lie in [0, 1)"; return SULI_ERR_ARG; }
+        if (!(p->mg_alpha >= 0 && p->mg_alpha <= 2)) { why = "mg_alpha must lie in [0, 2]"; return SULI_ERR_ARG; }
         int nx = p->nx, ny = p->ny, nz = p->nz;
         while ((long long)nx * ny * nz > 1024 && nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0 && nx >= 4 && ny >= 4 && nz >= 4) {
             nx /= 2; ny /= 2; nz /= 2;
@@ -170,6 +172,7 @@ int suli_params_default(suli_params* p) {
     p->reinit_maxit = 3; p->vol_tol = 0.1;
     p->cg_stop = 0; p->cg_tol = 0.0001; p->cg_maxit = 10000;
     p->precision = 0; p->refine_maxit = 20; p->inner_tol = 1e-3;
+    p->mg_omega = 0.8; p->mg_alpha = 1.0;
     return SULI_OK;
 }
 
@@ -187,6 +190,8 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
     }
     suli_ctx* c = new suli_ctx();
     c->P = *p;
+    if (c->P.mg_omega == 0.) c->P.mg_omega = 0.8;   // zero-initialised structs get the defaults
+    if (c->P.mg_alpha == 0.) c->P.mg_alpha = 1.0;
     c->device = device;
     c->g = make_geo(p->nx, p->ny, p->nz);
     c->bc.x0 = p->ccx0; c->bc.xf = p->ccxf; c->bc.y0 = p->ccy0; c->bc.yf = p->ccyf; c->bc.z0 = p->ccz0; c->bc.zf = p->cczf;
