@@ -85,8 +85,8 @@ typedef struct suli_params {
     int    precision;               /* 0 = plain FP64; 1 = FP32 stencils + FP32 inner CG with FP64 refinement */
     int    refine_maxit;            /* outer FP64 refinement sweeps for precision 1            */
     double inner_tol;               /* relative tolerance of each FP32 inner solve             */
-    double mg_omega;                /* precision 1: damping of the multigrid Jacobi sweeps (0 = 0.8) */
-    double mg_alpha;                /* precision 1: scale of the coarse-grid correction (0 = 1)       */
+    double mg_omega;                /* precision 1: damping of the multigrid Jacobi sweeps (0 = 0.9) */
+    double mg_alpha;                /* precision 1: scale of the coarse-grid correction (0 = 1.8)     */
     int    reserved[4];
 } suli_params;
 
@@ -202,7 +202,10 @@ int suli_nn_train_step(suli_nn* n, const float* d_in3, const float* d_target, fl
 /* the convolution primitive on caller buffers: channels-last BF16 x [V][cin], w [27][cout][cin]
    (tap = dx + 3 dy + 9 dz), bias [cout] FP32 or NULL, out [V][cout] BF16 = relu?(conv(x) + b) */
 int suli_nn_conv3d(int nx, int ny, int nz, const void* x, int cin, const void* w, const float* bias, int cout,
-                   int relu, void* out);
+                   int relu, void* out, int kernel);
+/* convolution kernel of a network (and of suli_nn_conv3d's last argument): 0 = tcgen05 tensor
+   cores with the accumulator in TMEM (default), 1 = mma.sync tensor cores */
+int suli_nn_set_kernel(suli_nn* n, int kernel);
 
 /* Attach a network to a context (same grid and device) for its pressure solves.
    mode 0 detaches; mode 1 (precision 1 only) uses the network as the initial guess: after

@@ -18,6 +18,7 @@
 #include "../../include/suli_gpu.h"
 #include "nn_api.cuh"
 #include "nn_conv.cuh"
+#include "nn_tc.cuh"
 
 namespace suli {
 namespace nn {
@@ -321,6 +322,8 @@ struct suli_nn {
     float *out = nullptr, *dout = nullptr;
     double* sums = nullptr;
     double* host_sums = nullptr;
+    int* err_flag = nullptr;         // set by a tensor-core convolution whose wait timed out
+    int kernel = 0;                  // convolution kernel: 0 tcgen05, 1 mma.sync
     std::string err;
 };
 
@@ -342,8 +345,25 @@ void conv_launch(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat
     k_conv3_fwd<NF><<<grid, 256, smem, N->stream>>>(vol, in, W, bias, relu, out);
 }
 
+void conv_tc(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu,
+             int cout, __nv_bfloat16* out) {
+    static bool attr_done[64] = {false};
+    if (!attr_done[N->device]) {
+        cudaFuncSetAttribute(k_conv3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr_done[N->device] = true;
+    }
+    int tcols = 32;
+    while (tcols < cout) tcols *= 2;
+    const dim3 grid((vol.nx + TCX - 1) / TCX, (vol.ny + TCY - 1) / TCY, vol.nz);
+    k_conv3_tc<<<grid, 128, tc_smem_bytes(cout), N->stream>>>(vol, in, W, bias, relu, cout, tcols, out, N->err_flag);
+}
+
 void conv(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu, int cout,
           __nv_bfloat16* out) {
+    if (N->kernel == 0) {
+        conv_tc(N, vol, in, W, bias, relu, cout, out);
+        return;
+    }
     switch (cout) {
     case 16: conv_launch<2>(N, vol, in, W, bias, relu, out); break;
     case 32: conv_launch<4>(N, vol, in, W, bias, relu, out); break;
@@ -465,6 +485,19 @@ int nn_fail(suli_nn* N, int code, const std::string& m) {
     return code;
 }
 
+// wait for the network's stream; report a CUDA error or a timed-out tensor-core wait
+int nn_sync(suli_nn* N) {
+    cudaError_t e = cudaStreamSynchronize(N->stream);
+    int flag = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&flag, N->err_flag, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return nn_fail(N, SULI_ERR_CUDA, cudaGetErrorString(e));
+    if (flag) {
+        cudaMemset(N->err_flag, 0, sizeof(int));
+        return nn_fail(N, SULI_ERR_CUDA, "tensor-core convolution: completion wait timed out");
+    }
+    return SULI_OK;
+}
+
 }  // namespace
 
 namespace suli {
@@ -483,6 +516,12 @@ void forward_on(suli_nn* N, cudaStream_t stream, const float* d_in3, float* d_ou
     N->stream = own;
 }
 int forward_launches() { return 1 + kConv + (kLevels - 1) + 1; }
+int take_error(suli_nn* N) {
+    int flag = 0;
+    if (cudaMemcpy(&flag, N->err_flag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+    if (flag) cudaMemset(N->err_flag, 0, sizeof(int));
+    return flag;
+}
 }  // namespace nn
 }  // namespace suli
 
@@ -533,12 +572,14 @@ int suli_nn_create(int nx, int ny, int nz, int device, suli_nn** out) {
     A(alloc(&N->out, N->V[0]));
     A(alloc(&N->dout, N->V[0]));
     A(alloc(&N->sums, 4));
+    A(alloc(&N->err_flag, 1));
     A(cudaMallocHost(&N->host_sums, 4 * sizeof(double)));
     if (ok) {
         A(cudaMemsetAsync(N->w, 0, N->nparam * 4, N->stream));
         A(cudaMemsetAsync(N->m, 0, N->nparam * 4, N->stream));
         A(cudaMemsetAsync(N->v, 0, N->nparam * 4, N->stream));
         A(cudaMemsetAsync(N->wb, 0, N->nparam * 2, N->stream));
+        A(cudaMemsetAsync(N->err_flag, 0, sizeof(int), N->stream));
         A(cudaStreamSynchronize(N->stream));
     }
     if (!ok) {
@@ -559,6 +600,7 @@ int suli_nn_destroy(suli_nn* N) {
     for (int l = 0; l < kConv; ++l) { cudaFree(N->a[l]); cudaFree(N->gact[l]); }
     for (int l = 0; l < kLevels - 1; ++l) cudaFree(N->pool[l]);
     cudaFree(N->gcat); cudaFree(N->gtmp); cudaFree(N->out); cudaFree(N->dout); cudaFree(N->sums);
+    cudaFree(N->err_flag);
     if (N->host_sums) cudaFreeHost(N->host_sums);
     if (N->stream) cudaStreamDestroy(N->stream);
     delete N;
@@ -593,9 +635,7 @@ int suli_nn_forward(suli_nn* N, const float* d_in3, float* d_out) {
     cudaSetDevice(N->device);
     k_pack_input<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], d_in3, N->in0);
     forward(N, d_out);
-    const cudaError_t e = cudaStreamSynchronize(N->stream);
-    if (e != cudaSuccess) return nn_fail(N, SULI_ERR_CUDA, cudaGetErrorString(e));
-    return SULI_OK;
+    return nn_sync(N);
 }
 
 // loss and parameter gradient (host_grad may be null); the gradient stays in the device buffer
@@ -611,8 +651,7 @@ int suli_nn_loss_grad(suli_nn* N, const float* d_in3, const float* d_target, dou
     backward(N);
     cudaMemcpyAsync(N->host_sums, N->sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, N->stream);
     if (host_grad) cudaMemcpyAsync(host_grad, N->g, N->nparam * 4, cudaMemcpyDeviceToHost, N->stream);
-    const cudaError_t e = cudaStreamSynchronize(N->stream);
-    if (e != cudaSuccess) return nn_fail(N, SULI_ERR_CUDA, cudaGetErrorString(e));
+    if (int r = nn_sync(N)) return r;
     if (loss) *loss = N->host_sums[1] / (double)N->V[0];
     return SULI_OK;
 }
@@ -625,14 +664,20 @@ int suli_nn_train_step(suli_nn* N, const float* d_in3, const float* d_target, fl
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.f - powf(b1, (float)N->step), c2 = 1.f - powf(b2, (float)N->step);
     k_adam<<<nb(N->nparam), 256, 0, N->stream>>>(N->nparam, N->w, N->g, N->m, N->v, N->wb, lr, b1, b2, 1e-8f, c1, c2);
-    const cudaError_t e = cudaStreamSynchronize(N->stream);
-    return e == cudaSuccess ? SULI_OK : nn_fail(N, SULI_ERR_CUDA, cudaGetErrorString(e));
+    return nn_sync(N);
+}
+
+int suli_nn_set_kernel(suli_nn* N, int kernel) {
+    if (!N || kernel < 0 || kernel > 1) return SULI_ERR_ARG;
+    N->kernel = kernel;
+    return SULI_OK;
 }
 
 // The layer primitive on caller buffers (channels-last BF16), for tests: out = relu?(conv3(x) + b)
 int suli_nn_conv3d(int nx, int ny, int nz, const void* x, int cin, const void* w, const float* bias, int cout,
-                   int relu, void* out) {
+                   int relu, void* out, int kernel) {
     if (!x || !w || !out || cin % 16 || cout % 8 || nx < 1 || ny < 1 || nz < 1) return SULI_ERR_ARG;
+    if (kernel < 0 || kernel > 1) return SULI_ERR_ARG;
     if (cout != 16 && cout != 32 && cout != 48 && cout != 64 && cout != 96 && cout != 160) return SULI_ERR_UNSUPPORTED;
     if (cin > 160) return SULI_ERR_SIZE;
     suli_nn tmp;
@@ -640,11 +685,18 @@ int suli_nn_conv3d(int nx, int ny, int nz, const void* x, int cin, const void* w
     cudaGetDevice(&dev);
     tmp.device = dev;
     tmp.stream = nullptr;
+    tmp.kernel = kernel;
+    if (cudaMalloc(&tmp.err_flag, sizeof(int)) != cudaSuccess) return SULI_ERR_NOMEM;
+    cudaMemset(tmp.err_flag, 0, sizeof(int));
     ConvIn in{static_cast<const __nv_bfloat16*>(x), cin, 0, nullptr, 0};
     conv(&tmp, Vol{nx, ny, nz}, in, static_cast<const __nv_bfloat16*>(w), bias, relu, cout,
          static_cast<__nv_bfloat16*>(out));
-    const cudaError_t e = cudaDeviceSynchronize();
-    return e == cudaSuccess ? SULI_OK : SULI_ERR_CUDA;
+    cudaError_t e = cudaDeviceSynchronize();
+    int flag = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&flag, tmp.err_flag, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(tmp.err_flag);
+    if (e != cudaSuccess) return SULI_ERR_CUDA;
+    return flag ? SULI_ERR_CUDA : SULI_OK;
 }
 
 }  // extern "C"

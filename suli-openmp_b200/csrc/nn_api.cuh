@@ -17,6 +17,9 @@ SULI_NN_INTERNAL void dims(const suli_nn* N, int* nx, int* ny, int* nz, int* dev
 SULI_NN_INTERNAL void forward_on(suli_nn* N, cudaStream_t stream, const float* d_in3, float* d_out);
 // Kernel launches of one forward pass (for the tracing counters).
 SULI_NN_INTERNAL int forward_launches();
+// Nonzero (and cleared) if a tensor-core convolution's completion wait timed out since the
+// last call.  Synchronous.
+SULI_NN_INTERNAL int take_error(suli_nn* N);
 
 }  // namespace nn
 }  // namespace suli

@@ -1,0 +1,226 @@
+// nn_tc.cuh — 3x3x3 convolution of channels-last BF16 volumes on the 5th-generation tensor
+// cores: tcgen05.mma (kind::f16, BF16 x BF16 -> FP32) with the accumulator in tensor memory.
+//
+// GEMM view (as nn_conv.cuh): out[v][co] = sum_{tap, ci} X[v + off(tap)][ci] W[tap][co][ci].
+// A CTA (128 threads) owns an 8 x 16 x 1 tile of output voxels: M = 128 rows of the MMA, row
+// m = tx + 8 ty, so row group m/8 is one x-run of 8 voxels at height ty.  N = Cout (16..160),
+// the accumulator D[128][Cout] FP32 lives in TMEM (lane m, column co).  K runs over channel
+// chunks of 16 (one MMA K-step) and the 27 taps.
+//
+// Shared-memory operands use the canonical K-major layout without swizzle: "core matrices" of
+// 8 rows x 16 bytes (8 BF16 of K), 128 contiguous bytes each; the descriptor gives the byte
+// distance between core matrices along K (LBO) and along M/N (SBO).
+//  * Input halo (10 x 18 x 3 voxels) of the current 16-channel chunk, stored three times, once
+//    per x-shift dx: copy dx holds for every halo (hy, hz) one x-run of 8 voxels starting at
+//    halo x = dx, as 2 core matrices (channels 0-7, 8-15).  For tap (dx, dy, dz) the 16 row
+//    groups of the A operand are then the 16 consecutive hy = ty + dy of plane hz = dz in copy
+//    dx: one uniform SBO (256 bytes), LBO = 128 bytes.
+//  * Weights of the chunk for all 27 taps: core matrix (tap, co/8, ci/8); SBO = 256 bytes
+//    between groups of 8 output channels, LBO = 128 bytes.
+// One thread issues the 27 MMAs of a chunk and commits them to an mbarrier; all threads wait on
+// it (bounded) before the buffers are restaged.  The epilogue reads TMEM with tcgen05.ld
+// (warp w owns lanes 32w..32w+31), adds the bias, applies the ReLU and stores BF16.
+//
+// Every wait is bounded: a timed-out wait sets *err and the CTA skips its output.
+#pragma once
+#include <cuda_bf16.h>
+#include <cstdint>
+#include "nn_conv.cuh"
+
+namespace suli {
+namespace nn {
+
+constexpr int TCX = 8, TCY = 16;                // output tile (z extent 1)
+constexpr int TC_HX = TCX + 2, TC_HY = TCY + 2, TC_HZ = 3;
+constexpr int TC_CC = 16;                       // channels per K chunk
+constexpr int TC_COPY_BYTES = TC_HZ * TC_HY * 2 * 128;   // one dx copy: 54 positions x 2 core matrices
+constexpr int TC_HALO_BYTES = 3 * TC_COPY_BYTES;         // 41472
+
+// shared memory of a CTA: halo copies, weights of one chunk (27 taps), barrier, TMEM address
+__host__ __device__ constexpr int tc_weight_bytes(int cout) { return 27 * cout * TC_CC * 2; }
+__host__ __device__ constexpr int tc_smem_bytes(int cout) { return TC_HALO_BYTES + tc_weight_bytes(cout) + 128; }
+
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;    // descriptor version for sm_100
+    // base offset 0, LBO mode 0, layout type 0 = no swizzle
+    return d;
+}
+
+// instruction descriptor, kind::f16: D F32, A and B BF16, both K-major, N, M = 128
+__host__ __device__ constexpr uint32_t tc_idesc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :
+        : "r"(dtmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait on an mbarrier phase; false if it did not complete
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t phase) {
+    for (int it = 0; it < (1 << 24); ++it)
+        if (mbar_try_wait(mbar, phase)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+// Forward 3x3x3 convolution on the tensor cores.  Same operands as k_conv3_fwd; Cout in
+// {16, 32, 48, 64, 96, 160}, Cin a multiple of 16.  `tcols` = TMEM columns to allocate (a
+// power of two >= max(32, Cout)).  Grid (ceil(nx/8), ceil(ny/16), nz), 128 threads.
+__global__ void __launch_bounds__(128) k_conv3_tc(Vol vol, ConvIn in, const __nv_bfloat16* __restrict__ W,
+                                                  const float* __restrict__ bias, int relu, int cout, int tcols,
+                                                  __nv_bfloat16* __restrict__ out, int* err) {
+    extern __shared__ __align__(1024) unsigned char smem_tc[];
+    unsigned char* halo = smem_tc;
+    unsigned char* wsm = smem_tc + TC_HALO_BYTES;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(wsm + tc_weight_bytes(cout));
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(wsm + tc_weight_bytes(cout) + 64);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int cin = in.ca + in.cb;
+    const int x0 = blockIdx.x * TCX, y0 = blockIdx.y * TCY, z0 = blockIdx.z;
+    const uint32_t mbar_a = smem_u32(mbar);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(tcols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar_a), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t idesc = tc_idesc(cout);
+    const int hxn = (vol.nx + 1) / 2, hyn = (vol.ny + 1) / 2;
+    const int nchunks = cin / TC_CC;
+    bool ok = true;
+    uint32_t phase = 0;
+
+    for (int ch = 0; ch < nchunks && ok; ++ch) {
+        const int c0 = ch * TC_CC;
+        // ---- stage the halo of channels c0..c0+15: 10 x 18 x 3 voxels x 2 chunks of 8 channels
+        for (int q = tid; q < TC_HX * TC_HY * TC_HZ * 2; q += 128) {
+            const int kc = q & 1, h = q >> 1;
+            const int hx = h % TC_HX, hy = (h / TC_HX) % TC_HY, hz = h / (TC_HX * TC_HY);
+            const int gx = x0 + hx - 1, gy = y0 + hy - 1, gz = z0 + hz - 1;
+            uint4 val = make_uint4(0u, 0u, 0u, 0u);
+            if (gx >= 0 && gx < vol.nx && gy >= 0 && gy < vol.ny && gz >= 0 && gz < vol.nz) {
+                const int c = c0 + kc * 8;
+                if (c < in.ca) {
+                    const long long vi = in.a_half
+                        ? (long long)(gx >> 1) + hxn * ((long long)(gy >> 1) + (long long)hyn * (gz >> 1))
+                        : (long long)gx + vol.nx * ((long long)gy + (long long)vol.ny * gz);
+                    val = *reinterpret_cast<const uint4*>(in.a + vi * in.ca + c);
+                } else {
+                    const long long vi = (long long)gx + vol.nx * ((long long)gy + (long long)vol.ny * gz);
+                    val = *reinterpret_cast<const uint4*>(in.b + vi * in.cb + (c - in.ca));
+                }
+            }
+            // copy dx holds this voxel as row hx - dx of the run at (hy, hz)
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) {
+                const int r = hx - dx;
+                if (r >= 0 && r < 8)
+                    *reinterpret_cast<uint4*>(halo + dx * TC_COPY_BYTES + ((hz * TC_HY + hy) * 2 + kc) * 128 + r * 16) =
+                        val;
+            }
+        }
+        // ---- stage the weights of the chunk: core matrix (tap, co/8, kc), row co%8, 16 bytes
+        const int ng = cout / 8;
+        for (int q = tid; q < 27 * cout * 2; q += 128) {
+            const int kc = q & 1, row = q >> 1;   // row = tap * cout + co
+            const int tap = row / cout, co = row - tap * cout;
+            const uint4 val = *reinterpret_cast<const uint4*>(W + ((long long)tap * cout + co) * cin + c0 + kc * 8);
+            *reinterpret_cast<uint4*>(wsm + (((tap * ng + (co >> 3)) * 2 + kc) * 8 + (co & 7)) * 16) = val;
+        }
+        // generic-proxy stores -> visible to the tensor core (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (tid == 0) {
+            const uint32_t hbase = smem_u32(halo), wbase = smem_u32(wsm);
+            for (int tap = 0; tap < 27; ++tap) {
+                const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
+                const uint64_t ad = tc_desc(hbase + dx * TC_COPY_BYTES + (dz * TC_HY + dy) * 256, 128, 256);
+                const uint64_t bd = tc_desc(wbase + tap * ng * 256, 128, 256);
+                tc_mma(tmem, ad, bd, idesc, (ch > 0 || tap > 0) ? 1u : 0u);
+            }
+            tc_commit(mbar_a);
+        }
+        __syncwarp();
+        ok = mbar_wait_bounded(mbar_a, phase);
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        ok = __syncthreads_and(ok);   // uniform; the next chunk overwrites the operands
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(err, 1);
+    } else {
+        // ---- epilogue: row m = 32 warp + lane <-> voxel (m % 8, m / 8)
+        const int m = warp * 32 + lane;
+        const int ox = x0 + (m & 7), oy = y0 + (m >> 3), oz = z0;
+        const bool store = ox < vol.nx && oy < vol.ny && oz < vol.nz;
+        const long long vo = (long long)ox + vol.nx * ((long long)oy + (long long)vol.ny * oz);
+        for (int cb = 0; cb < cout; cb += 16) {
+            uint32_t r[16];
+            tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (store) {
+                uint32_t packed[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    float v0 = __uint_as_float(r[2 * e]), v1 = __uint_as_float(r[2 * e + 1]);
+                    if (bias) { v0 += bias[cb + 2 * e]; v1 += bias[cb + 2 * e + 1]; }
+                    if (relu) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
+                    const __nv_bfloat162 b2 = __floats2bfloat162_rn(v0, v1);
+                    packed[e] = *reinterpret_cast<const uint32_t*>(&b2);
+                }
+                uint4* dst = reinterpret_cast<uint4*>(out + vo * cout + cb);
+                dst[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+                dst[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcols));
+}
+
+}  // namespace nn
+}  // namespace suli

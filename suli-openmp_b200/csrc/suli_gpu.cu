@@ -171,8 +171,8 @@ int suli_params_default(suli_params* p) {
     p->dt1 = 0.1 * std::fmax(p->dx, std::fmax(p->dy, p->dz));
     p->reinit_maxit = 3; p->vol_tol = 0.1;
     p->cg_stop = 0; p->cg_tol = 0.0001; p->cg_maxit = 10000;
-    p->precision = 0; p->refine_maxit = 20; p->inner_tol = 1e-3;
-    p->mg_omega = 0.8; p->mg_alpha = 1.0;
+    p->precision = 0; p->refine_maxit = 20; p->inner_tol = 1e-4;
+    p->mg_omega = 0.9; p->mg_alpha = 1.8;
     return SULI_OK;
 }
 
@@ -190,8 +190,8 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
     }
     suli_ctx* c = new suli_ctx();
     c->P = *p;
-    if (c->P.mg_omega == 0.) c->P.mg_omega = 0.8;   // zero-initialised structs get the defaults
-    if (c->P.mg_alpha == 0.) c->P.mg_alpha = 1.0;
+    if (c->P.mg_omega == 0.) c->P.mg_omega = 0.9;   // zero-initialised structs get the defaults
+    if (c->P.mg_alpha == 0.) c->P.mg_alpha = 1.8;
     c->device = device;
     c->g = make_geo(p->nx, p->ny, p->nz);
     c->bc.x0 = p->ccx0; c->bc.xf = p->ccxf; c->bc.y0 = p->ccy0; c->bc.yf = p->ccyf; c->bc.z0 = p->ccz0; c->bc.zf = p->cczf;
@@ -691,6 +691,8 @@ int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
         ++outer;
     }
     c->last_outer_iters = outer;
+    if (c->nn && c->nn_mode == 1 && !c->rec_in && suli::nn::take_error(c->nn))
+        return fail(c, SULI_ERR_CUDA, "graddin: the network's tensor-core convolution timed out");
     launch_cg_final(c, ecur);
     if (c->rec_in) launch_nn_target(c, ecur, c->rec_target);
     CHECK_LAUNCH(c);

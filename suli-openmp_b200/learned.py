@@ -135,6 +135,10 @@ class Net:
                                                C.byref(loss), gp), "loss_grad")
         return loss.value, g
 
+    def set_kernel(self, kernel: int) -> None:
+        """Convolution kernel: 0 = tcgen05 (accumulator in TMEM, the default), 1 = mma.sync."""
+        self._check(self.lib.suli_nn_set_kernel(self._h, int(kernel)), "set_kernel")
+
     def train_step(self, in3, target, lr: float) -> float:
         """One Adam step; returns the loss before the step."""
         loss = C.c_double()
@@ -143,12 +147,14 @@ class Net:
         return loss.value
 
 
-def conv3d(x, w, bias, out, shape, cin: int, cout: int, relu: bool = False, lib_path=None) -> None:
-    """The convolution primitive on device buffers (channels-last BF16, see suli_nn_conv3d)."""
+def conv3d(x, w, bias, out, shape, cin: int, cout: int, relu: bool = False, kernel: int = 0,
+           lib_path=None) -> None:
+    """The convolution primitive on device buffers (channels-last BF16, see suli_nn_conv3d);
+    kernel 0 = tcgen05, 1 = mma.sync."""
     lib = _abi.load_library(lib_path)
     nx, ny, nz = shape
     rc = lib.suli_nn_conv3d(int(nx), int(ny), int(nz), C.c_void_p(_ptr(x)), int(cin), C.c_void_p(_ptr(w)),
                             C.c_void_p(_ptr(bias)) if bias is not None else None, int(cout), int(relu),
-                            C.c_void_p(_ptr(out)))
+                            C.c_void_p(_ptr(out)), int(kernel))
     if rc != 0:
         raise NetError(rc, "suli_nn_conv3d failed")

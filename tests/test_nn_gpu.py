@@ -1,6 +1,7 @@
 """GPU: the network kernels (csrc/nn.cu, nn_conv.cuh) against references.
 
-* the tensor-core convolution against an FP64 convolution of the same BF16 inputs;
+* both tensor-core convolutions (tcgen05 with the accumulator in TMEM, and mma.sync) against
+  an FP64 convolution of the same BF16 inputs;
 * forward, loss and parameter gradient of the whole U-Net against the FP64 oracle
   (oracle/unet_ref.py, itself pinned by finite differences), with the conv weights and the
   input rounded to BF16 as the GPU reads them.  The GPU keeps activations and activation
@@ -27,6 +28,7 @@ def _bf16(torch, a):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(torch.bfloat16)
 
 
+@pytest.mark.parametrize("kernel", [0, 1], ids=["tcgen05", "mma_sync"])
 @pytest.mark.parametrize("shape,cin,cout,relu", [
     ((12, 10, 9), 16, 16, True),
     ((8, 8, 8), 32, 48, False),
@@ -34,8 +36,9 @@ def _bf16(torch, a):
     ((16, 8, 4), 96, 96, False),
     ((6, 6, 6), 64, 160, False),
     ((10, 4, 12), 16, 32, True),
+    ((8, 33, 3), 48, 16, True),
 ])
-def test_conv3d_matches_fp64(pkg, torch, shape, cin, cout, relu):
+def test_conv3d_matches_fp64(pkg, torch, shape, cin, cout, relu, kernel):
     nx, ny, nz = shape
     rng = np.random.default_rng(cin * 1000 + cout)
     x = _bf16(torch, rng.standard_normal((nz, ny, nx, cin)))
@@ -43,7 +46,7 @@ def test_conv3d_matches_fp64(pkg, torch, shape, cin, cout, relu):
     b = torch.from_numpy(rng.standard_normal(cout).astype(np.float32))
     out = torch.empty((nz, ny, nx, cout), dtype=torch.bfloat16, device="cuda:0")
     xd, wd, bd = x.to("cuda:0"), w.to("cuda:0"), b.to("cuda:0")
-    pkg.learned.conv3d(xd, wd, bd, out, shape, cin, cout, relu)
+    pkg.learned.conv3d(xd, wd, bd, out, shape, cin, cout, relu, kernel=kernel)
     torch.cuda.synchronize()
     # FP64 reference: cross-correlation with zero padding, tap = dx + 3 dy + 9 dz
     xin = x.double().permute(3, 0, 1, 2).unsqueeze(0)              # (1, cin, nz, ny, nx)
@@ -93,10 +96,12 @@ def _layer_slices():
     return out
 
 
-def test_forward_matches_oracle(pkg, torch):
+@pytest.mark.parametrize("kernel", [0, 1], ids=["tcgen05", "mma_sync"])
+def test_forward_matches_oracle(pkg, torch, kernel):
     n = 16
     theta32, theta_ref, x3, x3_ref, _ = _setup(torch, n, 5)
     net = pkg.learned.Net(n, n, n, params=theta32)
+    net.set_kernel(kernel)
     d_in = torch.from_numpy(x3).to("cuda:0")
     d_out = torch.empty(n ** 3, dtype=torch.float32, device="cuda:0")
     net.forward(d_in, d_out)
@@ -112,10 +117,12 @@ def test_forward_matches_oracle(pkg, torch):
     net.close()
 
 
-def test_loss_and_gradient_match_oracle(pkg, torch):
+@pytest.mark.parametrize("kernel", [0, 1], ids=["tcgen05", "mma_sync"])
+def test_loss_and_gradient_match_oracle(pkg, torch, kernel):
     n = 16
     theta32, theta_ref, x3, x3_ref, tgt = _setup(torch, n, 7)
     net = pkg.learned.Net(n, n, n, params=theta32)
+    net.set_kernel(kernel)
     d_in = torch.from_numpy(x3).to("cuda:0")
     d_t = torch.from_numpy(tgt.ravel()).to("cuda:0")
     loss, g = net.loss_grad(d_in, d_t)
