@@ -82,7 +82,7 @@ typedef struct suli_params {
     int    cg_stop;
     double cg_tol;
     int    cg_maxit;                /* 10000 in the reference                                  */
-    int    precision;               /* 0 = plain FP64; 1 = FP32 stencils + FP32 inner CG with FP64 refinement */
+    int    precision;               /* 0 = plain FP64; 1 = FP32 multigrid-preconditioned inner CG with FP64 refinement */
     int    refine_maxit;            /* outer FP64 refinement sweeps for precision 1            */
     double inner_tol;               /* relative tolerance of each FP32 inner solve             */
     double mg_omega;                /* precision 1: damping of the multigrid Jacobi sweeps (0 = 0.9) */
@@ -263,7 +263,8 @@ enum suli_kernel {
     SULI_K_MG,             /* precision 1: FP32 inner PCG iterations (SpMV, update, multigrid
                               V-cycle), launched as one CUDA graph per iteration */
     SULI_K_REFINE,         /* precision 1: FP64 residual and correction of the refinement */
-    SULI_K_NN,             /* learned initial guess: features, network forward, FP64 step */
+    SULI_K_NN,             /* learned initial guess: the network's forward pass (its input
+                              features and the FP64 step count as CG_SETUP) */
     SULI_K_COUNT
 };
 /* The CUDA stream (cudaStream_t) this context launches on, for callers ordering their own

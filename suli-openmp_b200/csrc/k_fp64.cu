@@ -1,8 +1,11 @@
 // k_fp64.cu — FP64 kernels of the SuLi-IC hot path for sm_100a.
 //
-// Compiled with -fmad=false: every expression below keeps the reference's order of
-// operations, so results match a contraction-free CPU evaluation bit for bit except where a
-// transcendental (sin/cos in heaviside) or a reduction order differs.  Reductions are
+// Every expression keeps the reference's order of operations except that divisions by a
+// constant or a shared divisor are done as one reciprocal and multiplications (cell sizes,
+// WENO weights, normals, the Jacobi-scaled coefficients), and FMA contraction is on: FP64
+// division and sqrt are multi-instruction sequences that bound these stencils, not memory.
+// Results differ from a literal CPU evaluation by rounding only (a few ulp per value); the
+// parity tests bound the difference per field.  Reductions are
 // deterministic: fixed warp-shuffle trees per block and a fixed-order sum of the block
 // partials done by the last block to finish (no floating-point atomics).
 #include <cuda_runtime.h>
@@ -84,7 +87,7 @@ __global__ void __launch_bounds__(256) k_lsprops(Geo G, LsConst L, const double*
             const double m = sqrt(a * a + b * b + cc * cc);
             mod_ls[c] = m;
             if (m == 0) { nrmx[c] = 0.; nrmy[c] = 0.; nrmz[c] = 0.; }
-            else { nrmx[c] = a / m; nrmy[c] = b / m; nrmz[c] = cc / m; }
+            else { const double im = 1. / m; nrmx[c] = a * im; nrmy[c] = b * im; nrmz[c] = cc * im; }
         }
         if (do_hs) {
             const double l = ls[c];
@@ -232,17 +235,17 @@ __global__ void __launch_bounds__(256) k_nut(Geo G, ViscConst V, const double* _
     const Thread3 t = tid3(1, 1, 1);
     if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
     const int i = t.i, j = t.j, k = t.k;
-    const double tdx = 2. * V.dx, tdy = 2. * V.dy, tdz = 2. * V.dz;
+    const double itdx = 1. / (2. * V.dx), itdy = 1. / (2. * V.dy), itdz = 1. / (2. * V.dz);
     // derivax/y/z of the staggered fields, then interp?_fc to the cell centre
-    const double dudx = ((FIDX(u, i + 1, j, k) - FIDX(u, i - 1, j, k)) / tdx + (FIDX(u, i + 2, j, k) - FIDX(u, i, j, k)) / tdx) * 0.5;
-    const double dudy = ((FIDX(u, i, j + 1, k) - FIDX(u, i, j - 1, k)) / tdy + (FIDX(u, i + 1, j + 1, k) - FIDX(u, i + 1, j - 1, k)) / tdy) * 0.5;
-    const double dudz = ((FIDX(u, i, j, k + 1) - FIDX(u, i, j, k - 1)) / tdz + (FIDX(u, i + 1, j, k + 1) - FIDX(u, i + 1, j, k - 1)) / tdz) * 0.5;
-    const double dvdx = ((FIDX(v, i + 1, j, k) - FIDX(v, i - 1, j, k)) / tdx + (FIDX(v, i + 1, j + 1, k) - FIDX(v, i - 1, j + 1, k)) / tdx) * 0.5;
-    const double dvdy = ((FIDX(v, i, j + 1, k) - FIDX(v, i, j - 1, k)) / tdy + (FIDX(v, i, j + 2, k) - FIDX(v, i, j, k)) / tdy) * 0.5;
-    const double dvdz = ((FIDX(v, i, j, k + 1) - FIDX(v, i, j, k - 1)) / tdz + (FIDX(v, i, j + 1, k + 1) - FIDX(v, i, j + 1, k - 1)) / tdz) * 0.5;
-    const double dwdx = ((FIDX(w, i + 1, j, k) - FIDX(w, i - 1, j, k)) / tdx + (FIDX(w, i + 1, j, k + 1) - FIDX(w, i - 1, j, k + 1)) / tdx) * 0.5;
-    const double dwdy = ((FIDX(w, i, j + 1, k) - FIDX(w, i, j - 1, k)) / tdy + (FIDX(w, i, j + 1, k + 1) - FIDX(w, i, j - 1, k + 1)) / tdy) * 0.5;
-    const double dwdz = ((FIDX(w, i, j, k + 1) - FIDX(w, i, j, k - 1)) / tdz + (FIDX(w, i, j, k + 2) - FIDX(w, i, j, k)) / tdz) * 0.5;
+    const double dudx = ((FIDX(u, i + 1, j, k) - FIDX(u, i - 1, j, k)) * itdx + (FIDX(u, i + 2, j, k) - FIDX(u, i, j, k)) * itdx) * 0.5;
+    const double dudy = ((FIDX(u, i, j + 1, k) - FIDX(u, i, j - 1, k)) * itdy + (FIDX(u, i + 1, j + 1, k) - FIDX(u, i + 1, j - 1, k)) * itdy) * 0.5;
+    const double dudz = ((FIDX(u, i, j, k + 1) - FIDX(u, i, j, k - 1)) * itdz + (FIDX(u, i + 1, j, k + 1) - FIDX(u, i + 1, j, k - 1)) * itdz) * 0.5;
+    const double dvdx = ((FIDX(v, i + 1, j, k) - FIDX(v, i - 1, j, k)) * itdx + (FIDX(v, i + 1, j + 1, k) - FIDX(v, i - 1, j + 1, k)) * itdx) * 0.5;
+    const double dvdy = ((FIDX(v, i, j + 1, k) - FIDX(v, i, j - 1, k)) * itdy + (FIDX(v, i, j + 2, k) - FIDX(v, i, j, k)) * itdy) * 0.5;
+    const double dvdz = ((FIDX(v, i, j, k + 1) - FIDX(v, i, j, k - 1)) * itdz + (FIDX(v, i, j + 1, k + 1) - FIDX(v, i, j + 1, k - 1)) * itdz) * 0.5;
+    const double dwdx = ((FIDX(w, i + 1, j, k) - FIDX(w, i - 1, j, k)) * itdx + (FIDX(w, i + 1, j, k + 1) - FIDX(w, i - 1, j, k + 1)) * itdx) * 0.5;
+    const double dwdy = ((FIDX(w, i, j + 1, k) - FIDX(w, i, j - 1, k)) * itdy + (FIDX(w, i, j + 1, k + 1) - FIDX(w, i, j - 1, k + 1)) * itdy) * 0.5;
+    const double dwdz = ((FIDX(w, i, j, k + 1) - FIDX(w, i, j, k - 1)) * itdz + (FIDX(w, i, j, k + 2) - FIDX(w, i, j, k)) * itdz) * 0.5;
     const double p1 = dudx + 0.5 * (dudy + dvdx + dudz + dwdx);
     const double p2 = dvdy + 0.5 * (dvdx + dudy + dvdz + dwdy);
     const double p3 = dwdz + 0.5 * (dwdy + dvdz + dudz + dwdx);
@@ -281,7 +284,7 @@ __global__ void __launch_bounds__(256) k_facenu(Geo G, int m_turb, const double*
 // convdiff + classico (6_convdiff.f90:14-189, 7_advectivo.f90:33-113)
 // ------------------------------------------------------------------------------------
 struct CDConst {
-    double dx, dy, dz, gx, gz, sigma, cz;   // cz = gz/(chezy*chezy)
+    double idx, idy, idz, gx, gz, sigma, cz;   // reciprocal cell sizes; cz = gz/(chezy*chezy)
     int tf;                                  // tf_u/v/w are non-zero
     int cap_z2, cap_y2, cap_yn;              // planes where ub/vb/wb are captured (3_contorno.f90:247-264)
 };
@@ -299,7 +302,7 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
     const Thread3 t = tid3(1, 1, 1);
     const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
     if (i > nx + 1 || j > ny + 1 || k > nz + 1) return;
-    const double dx = C.dx, dy = C.dy, dz = C.dz;
+    const double idx = C.idx, idy = C.idy, idz = C.idz;   // 1/dx, 1/dy, 1/dz
     const double* __restrict__ u = F.u;
     const double* __restrict__ v = F.v;
     const double* __restrict__ w = F.w;
@@ -309,30 +312,30 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
         const double bma4 = (FIDX(v, i, j, k) + FIDX(v, i - 1, j, k) + FIDX(v, i, j + 1, k) + FIDX(v, i - 1, j + 1, k)) * 0.25;
         const double dma4 = (FIDX(w, i, j, k) + FIDX(w, i - 1, j, k) + FIDX(w, i, j, k + 1) + FIDX(w, i - 1, j, k + 1)) * 0.25;
         double a1 = pmax(uc, 0.), a2 = pmin(uc, 0.);
-        const double dudx = a1 * (uc - FIDX(u, i - 1, j, k)) / dx + a2 * (FIDX(u, i + 1, j, k) - uc) / dx;
+        const double dudx = a1 * (uc - FIDX(u, i - 1, j, k)) * idx + a2 * (FIDX(u, i + 1, j, k) - uc) * idx;
         a1 = pmax(bma4, 0.); a2 = pmin(bma4, 0.);
-        const double dudy = a1 * (uc - FIDX(u, i, j - 1, k)) / dy + a2 * (FIDX(u, i, j + 1, k) - uc) / dy;
+        const double dudy = a1 * (uc - FIDX(u, i, j - 1, k)) * idy + a2 * (FIDX(u, i, j + 1, k) - uc) * idy;
         a1 = pmax(dma4, 0.); a2 = pmin(dma4, 0.);
-        const double dudz = a1 * (uc - FIDX(u, i, j, k - 1)) / dz + a2 * (FIDX(u, i, j, k + 1) - uc) / dz;
+        const double dudz = a1 * (uc - FIDX(u, i, j, k - 1)) * idz + a2 * (FIDX(u, i, j, k + 1) - uc) * idz;
         const double uint_ = dudx + dudy + dudz;
         const int ic = clampi(i, 2, nx);
         const double rhox = (FIDX(F.rho, ic, j, k) + FIDX(F.rho, ic - 1, j, k)) * 0.5;
         const double tx1 = FIDX(F.hsx, ic, j, k) * FIDX(F.kurv, ic, j, k) / FIDX(F.rho, ic, j, k);
         const double tx0 = FIDX(F.hsx, ic - 1, j, k) * FIDX(F.kurv, ic - 1, j, k) / FIDX(F.rho, ic - 1, j, k);
         const double dhsdx = (tx1 + tx0) * 0.5;
-        const double ama_i = FIDX(F.nut, clampi(i, 1, nx), j, k) / dx;
-        const double ama_m = FIDX(F.nut, clampi(i - 1, 1, nx), j, k) / dx;
+        const double ama_i = FIDX(F.nut, clampi(i, 1, nx), j, k) * idx;
+        const double ama_m = FIDX(F.nut, clampi(i - 1, 1, nx), j, k) * idx;
         const int jp = clampi(j + 1, 2, ny), jm = clampi(j, 2, ny);
-        const double bma_p = ((FIDX(F.xnut, i, jp, k) + FIDX(F.xnut, i, jp - 1, k)) * 0.5) / dy;
-        const double bma_m = ((FIDX(F.xnut, i, jm, k) + FIDX(F.xnut, i, jm - 1, k)) * 0.5) / dy;
+        const double bma_p = ((FIDX(F.xnut, i, jp, k) + FIDX(F.xnut, i, jp - 1, k)) * 0.5) * idy;
+        const double bma_m = ((FIDX(F.xnut, i, jm, k) + FIDX(F.xnut, i, jm - 1, k)) * 0.5) * idy;
         const int kp = clampi(k + 1, 2, nz), km = clampi(k, 2, nz);
-        const double dma_p = ((FIDX(F.xnut, i, j, kp) + FIDX(F.xnut, i, j, kp - 1)) * 0.5) / dz;
-        const double dma_m = ((FIDX(F.xnut, i, j, km) + FIDX(F.xnut, i, j, km - 1)) * 0.5) / dz;
-        const double Gv = (ama_i * 2. * (FIDX(u, i + 1, j, k) - uc) - ama_m * 2. * (uc - FIDX(u, i - 1, j, k))) / dx +
-                          bma_p * ((FIDX(u, i, j + 1, k) - uc) / dy + (FIDX(v, i, j + 1, k) - FIDX(v, i - 1, j + 1, k)) / dx) -
-                          bma_m * ((uc - FIDX(u, i, j - 1, k)) / dy + (FIDX(v, i, j, k) - FIDX(v, i - 1, j, k)) / dx) +
-                          dma_p * ((FIDX(u, i, j, k + 1) - uc) / dz + (FIDX(w, i, j, k + 1) - FIDX(w, i - 1, j, k + 1)) / dx) -
-                          dma_m * ((uc - FIDX(u, i, j, k - 1)) / dz + (FIDX(w, i, j, k) - FIDX(w, i - 1, j, k)) / dx);
+        const double dma_p = ((FIDX(F.xnut, i, j, kp) + FIDX(F.xnut, i, j, kp - 1)) * 0.5) * idz;
+        const double dma_m = ((FIDX(F.xnut, i, j, km) + FIDX(F.xnut, i, j, km - 1)) * 0.5) * idz;
+        const double Gv = (ama_i * 2. * (FIDX(u, i + 1, j, k) - uc) - ama_m * 2. * (uc - FIDX(u, i - 1, j, k))) * idx +
+                          bma_p * ((FIDX(u, i, j + 1, k) - uc) * idy + (FIDX(v, i, j + 1, k) - FIDX(v, i - 1, j + 1, k)) * idx) -
+                          bma_m * ((uc - FIDX(u, i, j - 1, k)) * idy + (FIDX(v, i, j, k) - FIDX(v, i - 1, j, k)) * idx) +
+                          dma_p * ((FIDX(u, i, j, k + 1) - uc) * idz + (FIDX(w, i, j, k + 1) - FIDX(w, i - 1, j, k + 1)) * idx) -
+                          dma_m * ((uc - FIDX(u, i, j, k - 1)) * idz + (FIDX(w, i, j, k) - FIDX(w, i - 1, j, k)) * idx);
         double r = -uint_ + Gv / rhox + C.gx - C.sigma * dhsdx;
         if (C.tf) r = r + FIDX(F.tfu, i, j, k);
         if (on_cap(C, j, k, ny)) { const double b = FIDX(F.ub, i, j, k); r = r - C.cz * sqrt(b * b) * uc; }
@@ -344,11 +347,11 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
         const double amb4 = (FIDX(u, i, j, k) + FIDX(u, i + 1, j, k) + FIDX(u, i, j - 1, k) + FIDX(u, i + 1, j - 1, k)) * 0.25;
         const double dmb4 = (FIDX(w, i, j, k) + FIDX(w, i, j - 1, k) + FIDX(w, i, j, k + 1) + FIDX(w, i, j - 1, k + 1)) * 0.25;
         double a1 = pmax(amb4, 0.), a2 = pmin(amb4, 0.);
-        const double dvdx = a1 * (vc - FIDX(v, i - 1, j, k)) / dx + a2 * (FIDX(v, i + 1, j, k) - vc) / dx;
+        const double dvdx = a1 * (vc - FIDX(v, i - 1, j, k)) * idx + a2 * (FIDX(v, i + 1, j, k) - vc) * idx;
         a1 = pmax(vc, 0.); a2 = pmin(vc, 0.);
-        const double dvdy = a1 * (vc - FIDX(v, i, j - 1, k)) / dy + a2 * (FIDX(v, i, j + 1, k) - vc) / dy;
+        const double dvdy = a1 * (vc - FIDX(v, i, j - 1, k)) * idy + a2 * (FIDX(v, i, j + 1, k) - vc) * idy;
         a1 = pmax(dmb4, 0.); a2 = pmin(dmb4, 0.);
-        const double dvdz = a1 * (vc - FIDX(v, i, j, k - 1)) / dz + a2 * (FIDX(v, i, j, k + 1) - vc) / dz;
+        const double dvdz = a1 * (vc - FIDX(v, i, j, k - 1)) * idz + a2 * (FIDX(v, i, j, k + 1) - vc) * idz;
         const double vint = dvdx + dvdy + dvdz;
         const int jc = clampi(j, 2, ny);
         const double rhoy = (FIDX(F.rho, i, jc, k) + FIDX(F.rho, i, jc - 1, k)) * 0.5;
@@ -356,18 +359,18 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
         const double ty0 = FIDX(F.hsy, i, jc - 1, k) * FIDX(F.kurv, i, jc - 1, k) / FIDX(F.rho, i, jc - 1, k);
         const double dhsdy = (ty1 + ty0) * 0.5;
         const int ip = clampi(i + 1, 2, nx), im = clampi(i, 2, nx);
-        const double amb_p = ((FIDX(F.ynut, ip, j, k) + FIDX(F.ynut, ip - 1, j, k)) * 0.5) / dx;
-        const double amb_m = ((FIDX(F.ynut, im, j, k) + FIDX(F.ynut, im - 1, j, k)) * 0.5) / dx;
-        const double bmb_j = FIDX(F.nut, i, clampi(j, 1, ny), k) / dy;
-        const double bmb_m = FIDX(F.nut, i, clampi(j - 1, 1, ny), k) / dy;
+        const double amb_p = ((FIDX(F.ynut, ip, j, k) + FIDX(F.ynut, ip - 1, j, k)) * 0.5) * idx;
+        const double amb_m = ((FIDX(F.ynut, im, j, k) + FIDX(F.ynut, im - 1, j, k)) * 0.5) * idx;
+        const double bmb_j = FIDX(F.nut, i, clampi(j, 1, ny), k) * idy;
+        const double bmb_m = FIDX(F.nut, i, clampi(j - 1, 1, ny), k) * idy;
         const int kp = clampi(k + 1, 2, nz), km = clampi(k, 2, nz);
-        const double dmb_p = ((FIDX(F.ynut, i, j, kp) + FIDX(F.ynut, i, j, kp - 1)) * 0.5) / dz;
-        const double dmb_m = ((FIDX(F.ynut, i, j, km) + FIDX(F.ynut, i, j, km - 1)) * 0.5) / dz;
-        const double Gv = amb_p * ((FIDX(v, i + 1, j, k) - vc) / dx + (FIDX(u, i + 1, j, k) - FIDX(u, i + 1, j - 1, k)) / dy) -
-                          amb_m * ((vc - FIDX(v, i - 1, j, k)) / dx + (FIDX(u, i, j, k) - FIDX(u, i, j - 1, k)) / dy) +
-                          (bmb_j * 2. * (FIDX(v, i, j + 1, k) - vc) - bmb_m * 2. * (vc - FIDX(v, i, j - 1, k))) / dy +
-                          dmb_p * ((FIDX(v, i, j, k + 1) - vc) / dz + (FIDX(w, i, j, k + 1) - FIDX(w, i, j - 1, k + 1)) / dy) -
-                          dmb_m * ((vc - FIDX(v, i, j, k - 1)) / dz + (FIDX(w, i, j, k) - FIDX(w, i, j - 1, k)) / dy);
+        const double dmb_p = ((FIDX(F.ynut, i, j, kp) + FIDX(F.ynut, i, j, kp - 1)) * 0.5) * idz;
+        const double dmb_m = ((FIDX(F.ynut, i, j, km) + FIDX(F.ynut, i, j, km - 1)) * 0.5) * idz;
+        const double Gv = amb_p * ((FIDX(v, i + 1, j, k) - vc) * idx + (FIDX(u, i + 1, j, k) - FIDX(u, i + 1, j - 1, k)) * idy) -
+                          amb_m * ((vc - FIDX(v, i - 1, j, k)) * idx + (FIDX(u, i, j, k) - FIDX(u, i, j - 1, k)) * idy) +
+                          (bmb_j * 2. * (FIDX(v, i, j + 1, k) - vc) - bmb_m * 2. * (vc - FIDX(v, i, j - 1, k))) * idy +
+                          dmb_p * ((FIDX(v, i, j, k + 1) - vc) * idz + (FIDX(w, i, j, k + 1) - FIDX(w, i, j - 1, k + 1)) * idy) -
+                          dmb_m * ((vc - FIDX(v, i, j, k - 1)) * idz + (FIDX(w, i, j, k) - FIDX(w, i, j - 1, k)) * idy);
         double r = -vint + Gv / rhoy - C.sigma * dhsdy;
         if (C.tf) r = r + FIDX(F.tfv, i, j, k);
         if (on_cap(C, j, k, ny)) { const double b = FIDX(F.vb, i, j, k); r = r - C.cz * sqrt(b * b) * vc; }
@@ -379,11 +382,11 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
         const double amd4 = (FIDX(u, i, j, k) + FIDX(u, i + 1, j, k) + FIDX(u, i, j, k - 1) + FIDX(u, i + 1, j, k - 1)) * 0.25;
         const double bmd4 = (FIDX(v, i, j, k) + FIDX(v, i, j + 1, k) + FIDX(v, i, j, k - 1) + FIDX(v, i, j + 1, k - 1)) * 0.25;
         double a1 = pmax(amd4, 0.), a2 = pmin(amd4, 0.);
-        const double dwdx = a1 * (wc - FIDX(w, i - 1, j, k)) / dx + a2 * (FIDX(w, i + 1, j, k) - wc) / dx;
+        const double dwdx = a1 * (wc - FIDX(w, i - 1, j, k)) * idx + a2 * (FIDX(w, i + 1, j, k) - wc) * idx;
         a1 = pmax(bmd4, 0.); a2 = pmin(bmd4, 0.);
-        const double dwdy = a1 * (wc - FIDX(w, i, j - 1, k)) / dy + a2 * (FIDX(w, i, j + 1, k) - wc) / dy;
+        const double dwdy = a1 * (wc - FIDX(w, i, j - 1, k)) * idy + a2 * (FIDX(w, i, j + 1, k) - wc) * idy;
         a1 = pmax(wc, 0.); a2 = pmin(wc, 0.);
-        const double dwdz = a1 * (wc - FIDX(w, i, j, k - 1)) / dz + a2 * (FIDX(w, i, j, k + 1) - wc) / dz;
+        const double dwdz = a1 * (wc - FIDX(w, i, j, k - 1)) * idz + a2 * (FIDX(w, i, j, k + 1) - wc) * idz;
         const double wint = dwdx + dwdy + dwdz;
         const int kc = clampi(k, 2, nz);
         const double rhoz = (FIDX(F.rho, i, j, kc) + FIDX(F.rho, i, j, kc - 1)) * 0.5;
@@ -391,18 +394,18 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
         const double tz0 = FIDX(F.hsz, i, j, kc - 1) * FIDX(F.kurv, i, j, kc - 1) / FIDX(F.rho, i, j, kc - 1);
         const double dhsdz = (tz1 + tz0) * 0.5;
         const int ip = clampi(i + 1, 2, nx), im = clampi(i, 2, nx);
-        const double amd_p = ((FIDX(F.znut, ip, j, k) + FIDX(F.znut, ip - 1, j, k)) * 0.5) / dx;
-        const double amd_m = ((FIDX(F.znut, im, j, k) + FIDX(F.znut, im - 1, j, k)) * 0.5) / dx;
+        const double amd_p = ((FIDX(F.znut, ip, j, k) + FIDX(F.znut, ip - 1, j, k)) * 0.5) * idx;
+        const double amd_m = ((FIDX(F.znut, im, j, k) + FIDX(F.znut, im - 1, j, k)) * 0.5) * idx;
         const int jp = clampi(j + 1, 2, ny), jm = clampi(j, 2, ny);
-        const double bmd_p = ((FIDX(F.znut, i, jp, k) + FIDX(F.znut, i, jp - 1, k)) * 0.5) / dy;
-        const double bmd_m = ((FIDX(F.znut, i, jm, k) + FIDX(F.znut, i, jm - 1, k)) * 0.5) / dy;
-        const double dmd_k = FIDX(F.nut, i, j, clampi(k, 1, nz)) / dz;
-        const double dmd_m = FIDX(F.nut, i, j, clampi(k - 1, 1, nz)) / dz;
-        const double Gv = amd_p * ((FIDX(w, i + 1, j, k) - wc) / dx + (FIDX(u, i + 1, j, k) - FIDX(u, i + 1, j, k - 1)) / dz) -
-                          amd_m * ((wc - FIDX(w, i - 1, j, k)) / dx + (FIDX(u, i, j, k) - FIDX(u, i, j, k - 1)) / dz) +
-                          bmd_p * ((FIDX(w, i, j + 1, k) - wc) / dy + (FIDX(v, i, j + 1, k) - FIDX(v, i, j + 1, k - 1)) / dz) -
-                          bmd_m * ((wc - FIDX(w, i, j - 1, k)) / dy + (FIDX(v, i, j, k) - FIDX(v, i, j, k - 1)) / dz) +
-                          (dmd_k * 2. * (FIDX(w, i, j, k + 1) - wc) - dmd_m * 2. * (wc - FIDX(w, i, j, k - 1))) / dz;
+        const double bmd_p = ((FIDX(F.znut, i, jp, k) + FIDX(F.znut, i, jp - 1, k)) * 0.5) * idy;
+        const double bmd_m = ((FIDX(F.znut, i, jm, k) + FIDX(F.znut, i, jm - 1, k)) * 0.5) * idy;
+        const double dmd_k = FIDX(F.nut, i, j, clampi(k, 1, nz)) * idz;
+        const double dmd_m = FIDX(F.nut, i, j, clampi(k - 1, 1, nz)) * idz;
+        const double Gv = amd_p * ((FIDX(w, i + 1, j, k) - wc) * idx + (FIDX(u, i + 1, j, k) - FIDX(u, i + 1, j, k - 1)) * idz) -
+                          amd_m * ((wc - FIDX(w, i - 1, j, k)) * idx + (FIDX(u, i, j, k) - FIDX(u, i, j, k - 1)) * idz) +
+                          bmd_p * ((FIDX(w, i, j + 1, k) - wc) * idy + (FIDX(v, i, j + 1, k) - FIDX(v, i, j + 1, k - 1)) * idz) -
+                          bmd_m * ((wc - FIDX(w, i, j - 1, k)) * idy + (FIDX(v, i, j, k) - FIDX(v, i, j, k - 1)) * idz) +
+                          (dmd_k * 2. * (FIDX(w, i, j, k + 1) - wc) - dmd_m * 2. * (wc - FIDX(w, i, j, k - 1))) * idz;
         double r = -wint + Gv / rhoz - C.gz - C.sigma * dhsdz;
         if (C.tf) r = r + FIDX(F.tfw, i, j, k);
         if (on_cap(C, j, k, ny)) { const double b = FIDX(F.wb, i, j, k); r = r - C.cz * sqrt(b * b) * wc; }
@@ -736,12 +739,12 @@ __global__ void __launch_bounds__(256) k_cg_coef(Geo G, BC bc, CGConst K, const 
             if (ii < 1 || ii > nx || jj < 1 || jj > ny || kk < 1 || kk > nz) return FIDX(prd1, ii, jj, kk) * sqrt(dd(ii, jj, kk));
             return FIDX(e, ii, jj, kk);
         };
-        const double app = face_s_x(G, rho, K.cx, i + 1, j, k) / sqrt(dc * dd(i + 1, j, k));
-        const double anp = face_s_x(G, rho, K.cx, i, j, k) / sqrt(dc * dd(i - 1, j, k));
-        const double bpp = face_s_y(G, rho, K.cy, i, j + 1, k) / sqrt(dc * dd(i, j + 1, k));
-        const double bnp = face_s_y(G, rho, K.cy, i, j, k) / sqrt(dc * dd(i, j - 1, k));
-        const double cpp = face_s_z(G, rho, K.cz, i, j, k + 1) / sqrt(dc * dd(i, j, k + 1));
-        const double cnp = face_s_z(G, rho, K.cz, i, j, k) / sqrt(dc * dd(i, j, k - 1));
+        const double app = face_s_x(G, rho, K.cx, i + 1, j, k) * rsqrt(dc * dd(i + 1, j, k));
+        const double anp = face_s_x(G, rho, K.cx, i, j, k) * rsqrt(dc * dd(i - 1, j, k));
+        const double bpp = face_s_y(G, rho, K.cy, i, j + 1, k) * rsqrt(dc * dd(i, j + 1, k));
+        const double bnp = face_s_y(G, rho, K.cy, i, j, k) * rsqrt(dc * dd(i, j - 1, k));
+        const double cpp = face_s_z(G, rho, K.cz, i, j, k + 1) * rsqrt(dc * dd(i, j, k + 1));
+        const double cnp = face_s_z(G, rho, K.cz, i, j, k) * rsqrt(dc * dd(i, j, k - 1));
         ax[c] = anp; ay[c] = bnp; az[c] = cnp;
         if (i == nx) FIDX(ax, nx + 1, j, k) = app;
         if (j == ny) FIDX(ay, i, ny + 1, k) = bpp;
@@ -1003,7 +1006,8 @@ void launch_visco(suli_ctx* c) {
 void launch_convdiff(suli_ctx* c) {
     const Geo& G = c->g;
     CDConst C;
-    C.dx = c->P.dx; C.dy = c->P.dy; C.dz = c->P.dz; C.gx = c->P.gx; C.gz = c->P.gz; C.sigma = c->P.sigma;
+    C.idx = 1. / c->P.dx; C.idy = 1. / c->P.dy; C.idz = 1. / c->P.dz;
+    C.gx = c->P.gx; C.gz = c->P.gz; C.sigma = c->P.sigma;
     C.cz = c->P.gz / (c->P.chezy * c->P.chezy);
     C.tf = c->tf_active ? 1 : 0;
     C.cap_z2 = (c->P.ccz0 == 2); C.cap_y2 = (c->P.ccy0 == 2); C.cap_yn = (c->P.ccyf == 2);

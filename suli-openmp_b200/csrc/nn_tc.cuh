@@ -10,13 +10,15 @@
 // Shared-memory operands use the canonical K-major layout without swizzle: "core matrices" of
 // 8 rows x 16 bytes (8 BF16 of K), 128 contiguous bytes each; the descriptor gives the byte
 // distance between core matrices along K (LBO) and along M/N (SBO).
-//  * Input halo (10 x 18 x 3 voxels) of the current 16-channel chunk, stored three times, once
-//    per x-shift dx: copy dx holds for every halo (hy, hz) one x-run of 8 voxels starting at
-//    halo x = dx, as 2 core matrices (channels 0-7, 8-15).  For tap (dx, dy, dz) the 16 row
-//    groups of the A operand are then the 16 consecutive hy = ty + dy of plane hz = dz in copy
-//    dx: one uniform SBO (256 bytes), LBO = 128 bytes.
+//  * Input halo (10 x 18 x 3 voxels) of the current 16-channel chunk, as [kc][hz][hy][hx] rows
+//    of 16 bytes (kc = channels 0-7 / 8-15).  For tap (dx, dy, dz) the core matrix of row
+//    group ty is the 8 consecutive rows hx = dx..dx+7 at (hz = dz, hy = ty + dy): it starts
+//    dx rows into the x-run, SBO = one x-run (160 bytes), LBO = one kc plane (8640 bytes).
+//    So one copy of the halo serves all 27 taps.
 //  * Weights of the chunk for all 27 taps: core matrix (tap, co/8, ci/8); SBO = 256 bytes
 //    between groups of 8 output channels, LBO = 128 bytes.
+// Both are copied global -> shared with cp.async (16 bytes each, zero-filled outside the
+// volume), no register staging.
 // One thread issues the 27 MMAs of a chunk and commits them to an mbarrier; all threads wait on
 // it (bounded) before the buffers are restaged.  The epilogue reads TMEM with tcgen05.ld
 // (warp w owns lanes 32w..32w+31), adds the bias, applies the ReLU and stores BF16.
@@ -33,8 +35,9 @@ namespace nn {
 constexpr int TCX = 8, TCY = 16;                // output tile (z extent 1)
 constexpr int TC_HX = TCX + 2, TC_HY = TCY + 2, TC_HZ = 3;
 constexpr int TC_CC = 16;                       // channels per K chunk
-constexpr int TC_COPY_BYTES = TC_HZ * TC_HY * 2 * 128;   // one dx copy: 54 positions x 2 core matrices
-constexpr int TC_HALO_BYTES = 3 * TC_COPY_BYTES;         // 41472
+constexpr int TC_RUN_BYTES = TC_HX * 16;                 // one x-run of 10 rows: 160
+constexpr int TC_KC_BYTES = TC_HZ * TC_HY * TC_RUN_BYTES;  // one 8-channel plane: 8640
+constexpr int TC_HALO_BYTES = 2 * TC_KC_BYTES;             // 17280
 
 // shared memory of a CTA: halo copies, weights of one chunk (27 taps), barrier, TMEM address
 __host__ __device__ constexpr int tc_weight_bytes(int cout) { return 27 * cout * TC_CC * 2; }
@@ -88,6 +91,11 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t phase)
     return false;
 }
 
+// 16-byte global -> shared copy; src_bytes = 0 fills zeros
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+
 __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&r)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
@@ -133,51 +141,48 @@ __global__ void __launch_bounds__(128) k_conv3_tc(Vol vol, ConvIn in, const __nv
 
     for (int ch = 0; ch < nchunks && ok; ++ch) {
         const int c0 = ch * TC_CC;
-        // ---- stage the halo of channels c0..c0+15: 10 x 18 x 3 voxels x 2 chunks of 8 channels
+        // ---- stage the halo of channels c0..c0+15: 10 x 18 x 3 voxels x 2 rows of 8 channels
+        const uint32_t hbase = smem_u32(halo), wbase = smem_u32(wsm);
         for (int q = tid; q < TC_HX * TC_HY * TC_HZ * 2; q += 128) {
             const int kc = q & 1, h = q >> 1;
             const int hx = h % TC_HX, hy = (h / TC_HX) % TC_HY, hz = h / (TC_HX * TC_HY);
             const int gx = x0 + hx - 1, gy = y0 + hy - 1, gz = z0 + hz - 1;
-            uint4 val = make_uint4(0u, 0u, 0u, 0u);
+            const void* src = in.a;
+            int bytes = 0;
             if (gx >= 0 && gx < vol.nx && gy >= 0 && gy < vol.ny && gz >= 0 && gz < vol.nz) {
                 const int c = c0 + kc * 8;
+                bytes = 16;
                 if (c < in.ca) {
                     const long long vi = in.a_half
                         ? (long long)(gx >> 1) + hxn * ((long long)(gy >> 1) + (long long)hyn * (gz >> 1))
                         : (long long)gx + vol.nx * ((long long)gy + (long long)vol.ny * gz);
-                    val = *reinterpret_cast<const uint4*>(in.a + vi * in.ca + c);
+                    src = in.a + vi * in.ca + c;
                 } else {
                     const long long vi = (long long)gx + vol.nx * ((long long)gy + (long long)vol.ny * gz);
-                    val = *reinterpret_cast<const uint4*>(in.b + vi * in.cb + (c - in.ca));
+                    src = in.b + vi * in.cb + (c - in.ca);
                 }
             }
-            // copy dx holds this voxel as row hx - dx of the run at (hy, hz)
-#pragma unroll
-            for (int dx = 0; dx < 3; ++dx) {
-                const int r = hx - dx;
-                if (r >= 0 && r < 8)
-                    *reinterpret_cast<uint4*>(halo + dx * TC_COPY_BYTES + ((hz * TC_HY + hy) * 2 + kc) * 128 + r * 16) =
-                        val;
-            }
+            cp_async16(hbase + kc * TC_KC_BYTES + (hz * TC_HY + hy) * TC_RUN_BYTES + hx * 16, src, bytes);
         }
         // ---- stage the weights of the chunk: core matrix (tap, co/8, kc), row co%8, 16 bytes
         const int ng = cout / 8;
         for (int q = tid; q < 27 * cout * 2; q += 128) {
             const int kc = q & 1, row = q >> 1;   // row = tap * cout + co
             const int tap = row / cout, co = row - tap * cout;
-            const uint4 val = *reinterpret_cast<const uint4*>(W + ((long long)tap * cout + co) * cin + c0 + kc * 8);
-            *reinterpret_cast<uint4*>(wsm + (((tap * ng + (co >> 3)) * 2 + kc) * 8 + (co & 7)) * 16) = val;
+            cp_async16(wbase + (((tap * ng + (co >> 3)) * 2 + kc) * 8 + (co & 7)) * 16,
+                       W + ((long long)tap * cout + co) * cin + c0 + kc * 8, 16);
         }
-        // generic-proxy stores -> visible to the tensor core (async proxy)
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+        // completed copies -> visible to the tensor core (async proxy)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;");
         if (tid == 0) {
-            const uint32_t hbase = smem_u32(halo), wbase = smem_u32(wsm);
             for (int tap = 0; tap < 27; ++tap) {
                 const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
-                const uint64_t ad = tc_desc(hbase + dx * TC_COPY_BYTES + (dz * TC_HY + dy) * 256, 128, 256);
+                const uint64_t ad =
+                    tc_desc(hbase + (dz * TC_HY + dy) * TC_RUN_BYTES + dx * 16, TC_KC_BYTES, TC_RUN_BYTES);
                 const uint64_t bd = tc_desc(wbase + tap * ng * 256, 128, 256);
                 tc_mma(tmem, ad, bd, idesc, (ch > 0 || tap > 0) ? 1u : 0u);
             }

@@ -642,13 +642,19 @@ void nn_begin(suli_ctx* c) {
     const bool rec = c->rec_in != nullptr;
     const bool learn = !rec && c->nn && c->nn_mode == 1;
     if (!rec && !learn) return;
-    ProfScope ps(c, SULI_K_NN, 2 + (learn ? suli::nn::forward_launches() + 3 : 0));
-    launch_nn_features(c, rec ? c->rec_in : c->nn_in);
+    {
+        ProfScope ps(c, SULI_K_CG_SETUP, 2);
+        launch_nn_features(c, rec ? c->rec_in : c->nn_in);
+    }
     if (rec) {
         cudaMemcpyAsync(c->nn_e0, c->cg_e, c->g.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
         return;
     }
-    suli::nn::forward_on(c->nn, c->stream, c->nn_in, c->nn_out);
+    {
+        ProfScope ps(c, SULI_K_NN, suli::nn::forward_launches());
+        suli::nn::forward_on(c->nn, c->stream, c->nn_in, c->nn_out);
+    }
+    ProfScope ps(c, SULI_K_CG_SETUP, 3);
     launch_nn_step(c, c->nn_out, c->cg_e);
 }
 

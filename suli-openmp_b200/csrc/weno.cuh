@@ -5,8 +5,9 @@
 // Ghost values outside 1..n are rebuilt from interior values with the pencil routine's own
 // rules (ihs, :530-570): 0 periodic with phi(0) = phi(n-1) (the reference's offset),
 // 1 one-sided extrapolation (1/5 rows at the low end, 1/11 rows at the high end),
-// 2 the 1/11 "zero derivative" rows at both ends.  Expressions keep the reference's order
-// of operations so that, compiled without FMA contraction, FP64 results are bit-identical.
+// 2 the 1/11 "zero derivative" rows at both ends.  The arithmetic is the reference's with its
+// divisions rearranged: one reciprocal of h per pencil, and the nonlinear weights
+// w_k/q_k^2 / sum_m w_m/q_m^2 formed over a common denominator (one division per side).
 #pragma once
 
 namespace suli {
@@ -52,14 +53,33 @@ __device__ __forceinline__ void pencil7(F at, int i, int n, int ihs, T P[7]) {
     }
 }
 
+// omega_k = (w_k/q_k^2) / sum_m (w_m/q_m^2), q_k = eps + is_k.  FP64: over the common
+// denominator q_1^2 q_2^2 q_3^2 (q >= eps = 1e-8, so the products stay far inside the FP64
+// range); other types: the three quotients and one reciprocal of their sum.
+template <typename T>
+__device__ __forceinline__ void nonlinear_weights(T is1, T is2, T is3, T eps, T w1, T w2, T w3, T& o1, T& o2,
+                                                  T& o3) {
+    const T a = (eps + is1) * (eps + is1), b = (eps + is2) * (eps + is2), c = (eps + is3) * (eps + is3);
+    if constexpr (sizeof(T) == 8) {
+        const T n1 = w1 * (b * c), n2 = w2 * (a * c), n3 = w3 * (a * b);
+        const T inv = T(1) / (n1 + n2 + n3);
+        o1 = n1 * inv; o2 = n2 * inv; o3 = n3 * inv;
+    } else {
+        const T al1 = w1 / a, al2 = w2 / b, al3 = w3 / c;
+        const T inv = T(1) / (al1 + al2 + al3);
+        o1 = al1 * inv; o2 = al2 * inv; o3 = al3 * inv;
+    }
+}
+
 // One-sided derivatives from the seven values P[0..6] = phi(i-3..i+3):
 // dp = phi_x^+ (dphidxp, right-biased), dn = phi_x^- (dphidxn, left-biased).
 template <typename T>
 __device__ __forceinline__ void weno_pair(const T P[7], T h, T& dp, T& dn) {
     // D[m] = (phi(i-2+m) - phi(i-3+m))/h; up(i-4..i) = D1..D5, un(i..i+4) = D0..D4
     T D[6];
+    const T ih = T(1) / h;
 #pragma unroll
-    for (int m = 0; m < 6; ++m) D[m] = (P[m + 1] - P[m]) / h;
+    for (int m = 0; m < 6; ++m) D[m] = (P[m + 1] - P[m]) * ih;
     const T aux1 = T(13. / 12.), aux2 = T(1. / 4.), aux3 = T(1. / 6.), aux6 = T(0.00000001);
     const T w1 = T(0.1), w2 = T(0.6), w3 = T(0.3);
     // right-biased: up(i)=D5, up(i-1)=D4, up(i-2)=D3, up(i-3)=D2, up(i-4)=D1
@@ -72,11 +92,8 @@ __device__ __forceinline__ void weno_pair(const T P[7], T h, T& dp, T& dn) {
         const T is2 = aux1 * a * a + aux2 * b * b;
         a = u2 - 2 * u3 + u4; b = 3 * u2 - 4 * u3 + u4;
         const T is3 = aux1 * a * a + aux2 * b * b;
-        const T al1 = w1 / ((aux6 + is1) * (aux6 + is1));
-        const T al2 = w2 / ((aux6 + is2) * (aux6 + is2));
-        const T al3 = w3 / ((aux6 + is3) * (aux6 + is3));
-        const T s = al1 + al2 + al3;
-        const T o1 = al1 / s, o2 = al2 / s, o3 = al3 / s;
+        T o1, o2, o3;
+        nonlinear_weights(is1, is2, is3, aux6, w1, w2, w3, o1, o2, o3);
         dp = aux3 * (o1 * (2 * u0 - 7 * u1 + 11 * u2) + o2 * (-u1 + 5 * u2 + 2 * u3) +
                      o3 * (2 * u2 + 5 * u3 - u4));
     }
@@ -90,11 +107,8 @@ __device__ __forceinline__ void weno_pair(const T P[7], T h, T& dp, T& dn) {
         const T is2 = aux1 * a * a + aux2 * b * b;
         a = v2 - 2 * v3 + v4; b = 3 * v2 - 4 * v3 + v4;
         const T is3 = aux1 * a * a + aux2 * b * b;
-        const T al1 = w1 / ((aux6 + is1) * (aux6 + is1));
-        const T al2 = w2 / ((aux6 + is2) * (aux6 + is2));
-        const T al3 = w3 / ((aux6 + is3) * (aux6 + is3));
-        const T s = al1 + al2 + al3;
-        const T o1 = al1 / s, o2 = al2 / s, o3 = al3 / s;
+        T o1, o2, o3;
+        nonlinear_weights(is1, is2, is3, aux6, w1, w2, w3, o1, o2, o3);
         dn = aux3 * (o1 * (2 * v0 - 7 * v1 + 11 * v2) + o2 * (-v1 + 5 * v2 + 2 * v3) +
                      o3 * (2 * v2 + 5 * v3 - v4));
     }

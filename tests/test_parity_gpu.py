@@ -124,7 +124,7 @@ def test_tempo(pkg, orc, t_tempo):
             for m in (g, o):
                 m.set_dt(dt)
                 m.tempo(tt, it)
-            compare(g, o, OUT_FIELDS["tempo"], tol=0.0, what=f"tempo t_tempo={t_tempo} tt={tt} it={it}")
+            compare(g, o, OUT_FIELDS["tempo"], what=f"tempo t_tempo={t_tempo} tt={tt} it={it}")
 
 
 @pytest.mark.parametrize("nlock", [1, 2])
