@@ -55,11 +55,14 @@ struct NNScale {
     int active;
 };
 
-// One level of the FP32 multigrid hierarchy: face conductances, Jacobi diagonal, vectors.
+// One level of the FP32 multigrid hierarchy: face conductances, inverse Jacobi diagonal,
+// vectors; level 0 also holds the FP32 density its kernels form the faces from, and the
+// dt-dependent face constants.
 struct MGLevel {
     Geo g;
-    float *sx = nullptr, *sy = nullptr, *sz = nullptr, *dg = nullptr;
+    float *sx = nullptr, *sy = nullptr, *sz = nullptr, *idg = nullptr;
     float *f = nullptr, *x = nullptr, *y = nullptr;
+    float *rho = nullptr, *c2 = nullptr;
 };
 
 // Boundary planes of prescribed walls (velpre, 0_modules.f90:96-118), Fortran layout.

@@ -23,46 +23,137 @@ namespace suli {
 
 __device__ __forceinline__ int clampi_m(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// (A x)_c = sum over the six faces of s_f (x_c - x_nb)
-__device__ __forceinline__ float apply_A(const float* __restrict__ x, const float* __restrict__ sx,
-                                         const float* __restrict__ sy, const float* __restrict__ sz, int c,
-                                         const Nb& o, int px, int pxy) {
-    const float xc = x[c];
-    return sx[c] * (xc - x[c + o.xm]) + sx[c + 1] * (xc - x[c + o.xp]) + sy[c] * (xc - x[c + o.ym]) +
-           sy[c + px] * (xc - x[c + o.yp]) + sz[c] * (xc - x[c + o.zm]) + sz[c + pxy] * (xc - x[c + o.zp]);
+// ------------------------------------------------------------------------------------
+// Operators.  Level 0 forms its face conductances on the fly from the FP32 density,
+// s = c2/(rho_a + rho_b) with c2 = 2 dt/dx^2 (the reference's c/((rho_a + rho_b)/2),
+// 9_grad.f90:46-87), reading one density array instead of three face arrays; the coarser
+// levels read their Galerkin faces.  Both keep the inverse Jacobi diagonal.  Boundary faces
+// take the first interior face's value (the reference's end-face copy); on a Neumann face the
+// neighbour is the cell itself, so that value only matters for periodic faces.
+// ------------------------------------------------------------------------------------
+struct Faces {
+    float xm, xp, ym, yp, zm, zp;
+};
+
+// Column kernels: a thread owns kKZ cells of one (i,j) column; z neighbours come from the
+// column's registers (with the ghost map on k), x/y neighbours through L1, and all loads of
+// the column are independent.
+constexpr int kKZ = 4;
+struct Col {
+    int i, j, k0, c0;
+    Nb o;      // x/y offsets (z offsets unused)
+    bool in;
+};
+__device__ __forceinline__ Col column(const Geo& G, const BC& bc) {
+    Col q;
+    q.i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    q.j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    q.k0 = blockIdx.z * kKZ + 1;
+    q.in = (q.i <= G.nx && q.j <= G.ny);
+    q.c0 = kBase + (q.i - 1) + G.px * q.j;
+    q.o = neighbours(G, bc, q.in ? q.i : 1, q.in ? q.j : 1, 1);
+    return q;
+}
+// load a field along the column, planes k0-1 .. k0+kKZ (ghost-mapped)
+template <class F>
+__device__ __forceinline__ void load_col(const Geo& G, const BC& bc, const Col& q, F val, float v[kKZ + 2]) {
+#pragma unroll
+    for (int m = 0; m < kKZ + 2; ++m) v[m] = val(q.c0 + (int)G.pxy * map_any(q.k0 - 1 + m, G.nz, bc.perz));
+}
+static inline dim3 colgrid(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kKZ - 1) / kKZ); }
+
+// stored faces: sx[c] is the face between cells c-1 and c (the cell's minus face)
+struct OpStored {
+    const float *sx, *sy, *sz, *idg;
+    struct ColState {};
+    __device__ __forceinline__ ColState col(const Geo&, const BC&, const Col&) const { return {}; }
+    __device__ __forceinline__ Faces at(const Geo& G, const Col&, const ColState&, int, int c) const {
+        return Faces{sx[c], sx[c + 1], sy[c], sy[c + G.px], sz[c], sz[c + (int)G.pxy]};
+    }
+    __device__ __forceinline__ Faces cell(const Geo& G, int, int, int, int c) const {
+        return Faces{sx[c], sx[c + 1], sy[c], sy[c + G.px], sz[c], sz[c + (int)G.pxy]};
+    }
+    __device__ __forceinline__ float inv_diag(int c) const { return idg[c]; }
+};
+
+// c2/(rho_a + rho_b) with the hardware reciprocal (2 ulp): the preconditioner's operator only
+// has to be the same everywhere it is formed, and this is the one formula used for it
+__device__ __forceinline__ float face_div(float c2, float rsum) { return __fdividef(c2, rsum); }
+
+// faces from the FP32 density (level 0); c2[0..2] = 2 dt/dx^2, 2 dt/dy^2, 2 dt/dz^2 in device
+// memory (dt changes per RK stage while the captured graphs stay the same)
+struct OpRho {
+    const float *rho, *idg, *c2;
+    struct ColState {
+        float r[kKZ + 2];
+        float cx2, cy2, cz2;
+    };
+    __device__ __forceinline__ ColState col(const Geo& G, const BC& bc, const Col& q) const {
+        ColState s;
+        load_col(G, bc, q, [&](int cc) { return rho[cc]; }, s.r);
+        s.cx2 = c2[0]; s.cy2 = c2[1]; s.cz2 = c2[2];
+        return s;
+    }
+    __device__ __forceinline__ Faces make(const Geo& G, int i, int j, int c, float rc, float rzm, float rzp, float cx2,
+                                          float cy2, float cz2) const {
+        const int px = G.px;
+        const float rxm = rho[(i > 1) ? c - 1 : c + 1], rxp = rho[(i < G.nx) ? c + 1 : c - 1];
+        const float rym = rho[(j > 1) ? c - px : c + px], ryp = rho[(j < G.ny) ? c + px : c - px];
+        return Faces{face_div(cx2, rc + rxm), face_div(cx2, rc + rxp), face_div(cy2, rc + rym),
+                     face_div(cy2, rc + ryp), face_div(cz2, rc + rzm), face_div(cz2, rc + rzp)};
+    }
+    __device__ __forceinline__ Faces at(const Geo& G, const Col& q, const ColState& s, int m, int c) const {
+        const int k = q.k0 + m;
+        const float rzm = (k > 1) ? s.r[m] : s.r[m + 2];
+        const float rzp = (k < G.nz) ? s.r[m + 2] : s.r[m];
+        return make(G, q.i, q.j, c, s.r[m + 1], rzm, rzp, s.cx2, s.cy2, s.cz2);
+    }
+    __device__ __forceinline__ Faces cell(const Geo& G, int i, int j, int k, int c) const {
+        const int pxy = (int)G.pxy;
+        const float rzm = rho[(k > 1) ? c - pxy : c + pxy], rzp = rho[(k < G.nz) ? c + pxy : c - pxy];
+        return make(G, i, j, c, rho[c], rzm, rzp, c2[0], c2[1], c2[2]);
+    }
+    __device__ __forceinline__ float inv_diag(int c) const { return idg[c]; }
+};
+
+// face conductance of the level-0 operator between two cells (FP32, the formula OpRho uses)
+__device__ __forceinline__ float face_rho(float c2, double ra, double rb) {
+    return face_div(c2, (float)ra + (float)rb);
 }
 
 // ------------------------------------------------------------------------------------
-// set-up: fine-level face conductances s = dt/(dx^2 rho_face) and the Jacobi diagonal
+// set-up: FP32 density, the fine faces (for the coarsening) and the inverse diagonal
 // ------------------------------------------------------------------------------------
-__global__ void k_mx_faces0(Geo G, BC bc, const double* __restrict__ rho, double cx, double cy, double cz,
-                            float* sx, float* sy, float* sz, float* dg) {
+__global__ void k_mx_faces0(Geo G, BC bc, const double* __restrict__ rho, float cx2, float cy2, float cz2,
+                            float* rho32, float* sx, float* sy, float* sz, float* idg, float* c2) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z + 1;
+    if (i == 1 && j == 1 && k == 1) { c2[0] = cx2; c2[1] = cy2; c2[2] = cz2; }
     if (i > G.nx || j > G.ny || k > G.nz) return;
-    auto fx = [&](int f) { const int fc = clampi_m(f, 2, G.nx); return cx / ((FI(rho, fc, j, k) + FI(rho, fc - 1, j, k)) * 0.5); };
-    auto fy = [&](int f) { const int fc = clampi_m(f, 2, G.ny); return cy / ((FI(rho, i, fc, k) + FI(rho, i, fc - 1, k)) * 0.5); };
-    auto fz = [&](int f) { const int fc = clampi_m(f, 2, G.nz); return cz / ((FI(rho, i, j, fc) + FI(rho, i, j, fc - 1)) * 0.5); };
-    const double xl = fx(i), xh = fx(i + 1), yl = fy(j), yh = fy(j + 1), zl = fz(k), zh = fz(k + 1);
+    auto fx = [&](int f) { const int fc = clampi_m(f, 2, G.nx); return face_rho(cx2, FI(rho, fc, j, k), FI(rho, fc - 1, j, k)); };
+    auto fy = [&](int f) { const int fc = clampi_m(f, 2, G.ny); return face_rho(cy2, FI(rho, i, fc, k), FI(rho, i, fc - 1, k)); };
+    auto fz = [&](int f) { const int fc = clampi_m(f, 2, G.nz); return face_rho(cz2, FI(rho, i, j, fc), FI(rho, i, j, fc - 1)); };
+    const float xl = fx(i), xh = fx(i + 1), yl = fy(j), yh = fy(j + 1), zl = fz(k), zh = fz(k + 1);
     const long long c = G.idx(i, j, k);
-    sx[c] = (float)xl; sy[c] = (float)yl; sz[c] = (float)zl;
-    if (i == G.nx) FI(sx, i + 1, j, k) = (float)xh;
-    if (j == G.ny) FI(sy, i, j + 1, k) = (float)yh;
-    if (k == G.nz) FI(sz, i, j, k + 1) = (float)zh;
-    double d = 0.;
+    rho32[c] = (float)rho[c];
+    sx[c] = xl; sy[c] = yl; sz[c] = zl;
+    if (i == G.nx) FI(sx, i + 1, j, k) = xh;
+    if (j == G.ny) FI(sy, i, j + 1, k) = yh;
+    if (k == G.nz) FI(sz, i, j, k + 1) = zh;
+    float d = 0.f;
     if (i > 1 || bc.perx) d += xl;
     if (i < G.nx || bc.perx) d += xh;
     if (j > 1 || bc.pery) d += yl;
     if (j < G.ny || bc.pery) d += yh;
     if (k > 1 || bc.perz) d += zl;
     if (k < G.nz || bc.perz) d += zh;
-    dg[c] = (float)(d > 0. ? d : 1.);
+    idg[c] = 1.f / (d > 0.f ? d : 1.f);
 }
 
 // Galerkin coarse faces: (sum of the 4 fine faces covering a coarse face) / 8
 __global__ void k_mg_coarsen(Geo Gf, Geo Gc, BC bc, const float* __restrict__ fx, const float* __restrict__ fy,
-                             const float* __restrict__ fz, float* cxs, float* cys, float* czs, float* dg) {
+                             const float* __restrict__ fz, float* cxs, float* cys, float* czs, float* idg) {
     const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int K = blockIdx.z + 1;
@@ -97,86 +188,65 @@ __global__ void k_mg_coarsen(Geo Gf, Geo Gc, BC bc, const float* __restrict__ fx
     if (J < Gc.ny || bc.pery) d += yh;
     if (K > 1 || bc.perz) d += zl;
     if (K < Gc.nz || bc.perz) d += zh;
-    dg[c] = d > 0.f ? d : 1.f;
+    idg[c] = 1.f / (d > 0.f ? d : 1.f);
 }
 
 // ------------------------------------------------------------------------------------
 // V-cycle kernels (all return at once when the inner solve has finished)
 // ------------------------------------------------------------------------------------
-struct MGOps {
-    const float *sx, *sy, *sz, *dg;
-};
-
-// Column kernels: a thread owns kKZ cells of one (i,j) column; z neighbours come from the
-// column's registers (with the ghost map on k), x/y neighbours through L1, and all loads of
-// the column are independent.
-constexpr int kKZ = 4;
-struct Col {
-    int i, j, k0, c0;
-    Nb o;      // x/y offsets (z offsets unused)
-    bool in;
-};
-__device__ __forceinline__ Col column(const Geo& G, const BC& bc) {
-    Col q;
-    q.i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    q.j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    q.k0 = blockIdx.z * kKZ + 1;
-    q.in = (q.i <= G.nx && q.j <= G.ny);
-    q.c0 = kBase + (q.i - 1) + G.px * q.j;
-    q.o = neighbours(G, bc, q.in ? q.i : 1, q.in ? q.j : 1, 1);
-    return q;
+__device__ __forceinline__ float apply_faces(const Faces& F, float xc, float xm, float xp, float ym, float yp, float zm,
+                                             float zp) {
+    return F.xm * (xc - xm) + F.xp * (xc - xp) + F.ym * (xc - ym) + F.yp * (xc - yp) + F.zm * (xc - zm) +
+           F.zp * (xc - zp);
 }
-// load a field along the column, planes k0-1 .. k0+kKZ (ghost-mapped)
-template <class F>
-__device__ __forceinline__ void load_col(const Geo& G, const BC& bc, const Col& q, F val, float v[kKZ + 2]) {
-#pragma unroll
-    for (int m = 0; m < kKZ + 2; ++m) v[m] = val(q.c0 + (int)G.pxy * map_any(q.k0 - 1 + m, G.nz, bc.perz));
-}
-static inline dim3 colgrid(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kKZ - 1) / kKZ); }
 
 // two damped Jacobi sweeps from zero in one pass: x1 = w f/dg, y = x1 + w (f - A x1)/dg
-__global__ void __launch_bounds__(256) k_mg_pre(Geo G, BC bc, const float* __restrict__ f, MGOps A,
+template <class Op>
+__global__ void __launch_bounds__(256) k_mg_pre(Geo G, BC bc, const float* __restrict__ f, Op A,
                                                 float* __restrict__ y, float omega, const PCGState* st) {
     if (st->done) return;
     const Col q = column(G, bc);
     if (!q.in) return;
-    const int px = G.px, pxy = (int)G.pxy;
-    auto x1 = [&](int cc) { return omega * f[cc] / A.dg[cc]; };
+    const int pxy = (int)G.pxy;
+    auto x1 = [&](int cc) { return omega * f[cc] * A.inv_diag(cc); };
     float col[kKZ + 2];
     load_col(G, bc, q, x1, col);
+    const typename Op::ColState cs = A.col(G, bc, q);
 #pragma unroll
     for (int m = 0; m < kKZ; ++m) {
         if (q.k0 + m > G.nz) break;
         const int c = q.c0 + pxy * (q.k0 + m);
         const float xc = col[m + 1];
-        const float ax = A.sx[c] * (xc - x1(c + q.o.xm)) + A.sx[c + 1] * (xc - x1(c + q.o.xp)) +
-                         A.sy[c] * (xc - x1(c + q.o.ym)) + A.sy[c + px] * (xc - x1(c + q.o.yp)) +
-                         A.sz[c] * (xc - col[m]) + A.sz[c + pxy] * (xc - col[m + 2]);
-        y[c] = xc + omega * (f[c] - ax) / A.dg[c];
+        const Faces F = A.at(G, q, cs, m, c);
+        const float ax = apply_faces(F, xc, x1(c + q.o.xm), x1(c + q.o.xp), x1(c + q.o.ym), x1(c + q.o.yp), col[m],
+                                     col[m + 2]);
+        y[c] = xc + omega * (f[c] - ax) * A.inv_diag(c);
     }
 }
 
 // x_out = x_in + w (f - A x_in)/dg; with do_dot (last sweep of level 0) also f.x_out -> rz, beta
+template <class Op>
 __global__ void __launch_bounds__(256) k_mg_jacc(Geo G, BC bc, const float* __restrict__ xin, const float* __restrict__ f,
-                                                 MGOps A, float* __restrict__ xout, float omega, PCGState* st, int do_dot,
+                                                 Op A, float* __restrict__ xout, float omega, PCGState* st, int do_dot,
                                                  double* partial, unsigned int* counter) {
     if (st->done) return;
     const Col q = column(G, bc);
     double dot = 0.;
     if (q.in) {
-        const int px = G.px, pxy = (int)G.pxy;
+        const int pxy = (int)G.pxy;
         float col[kKZ + 2];
         load_col(G, bc, q, [&](int cc) { return xin[cc]; }, col);
+        const typename Op::ColState cs = A.col(G, bc, q);
 #pragma unroll
         for (int m = 0; m < kKZ; ++m) {
             if (q.k0 + m > G.nz) break;
             const int c = q.c0 + pxy * (q.k0 + m);
             const float xc = col[m + 1];
-            const float ax = A.sx[c] * (xc - xin[c + q.o.xm]) + A.sx[c + 1] * (xc - xin[c + q.o.xp]) +
-                             A.sy[c] * (xc - xin[c + q.o.ym]) + A.sy[c + px] * (xc - xin[c + q.o.yp]) +
-                             A.sz[c] * (xc - col[m]) + A.sz[c + pxy] * (xc - col[m + 2]);
+            const Faces F = A.at(G, q, cs, m, c);
+            const float ax = apply_faces(F, xc, xin[c + q.o.xm], xin[c + q.o.xp], xin[c + q.o.ym], xin[c + q.o.yp],
+                                         col[m], col[m + 2]);
             const float fv = f[c];
-            const float v = xc + omega * (fv - ax) / A.dg[c];
+            const float v = xc + omega * (fv - ax) * A.inv_diag(c);
             xout[c] = v;
             dot += (double)fv * (double)v;
         }
@@ -194,14 +264,15 @@ __global__ void __launch_bounds__(256) k_mg_jacc(Geo G, BC bc, const float* __re
 
 // x_out = x' + w (f - A x')/dg with x' = y + a P xc (piecewise-constant prolongation, the
 // coarse correction scaled by a)
+template <class Op>
 __global__ void __launch_bounds__(256) k_mg_post(Geo Gf, Geo Gc, BC bc, const float* __restrict__ y,
-                                                 const float* __restrict__ xc, const float* __restrict__ f, MGOps A,
+                                                 const float* __restrict__ xc, const float* __restrict__ f, Op A,
                                                  float* __restrict__ xout, float omega, float alpha,
                                                  const PCGState* st) {
     if (st->done) return;
     const Col q = column(Gf, bc);
     if (!q.in) return;
-    const int px = Gf.px, pxy = (int)Gf.pxy;
+    const int pxy = (int)Gf.pxy;
     // parents: coarse (I,J) of this column and of its x/y neighbours (ghost-mapped)
     const int ixm = map_any(q.i - 1, Gf.nx, bc.perx), ixp = map_any(q.i + 1, Gf.nx, bc.perx);
     const int jym = map_any(q.j - 1, Gf.ny, bc.pery), jyp = map_any(q.j + 1, Gf.ny, bc.pery);
@@ -213,34 +284,24 @@ __global__ void __launch_bounds__(256) k_mg_post(Geo Gf, Geo Gc, BC bc, const fl
         const int k = map_any(q.k0 - 1 + m, Gf.nz, bc.perz);
         col[m] = y[q.c0 + pxy * k] + alpha * xc[Gc.idx(I, J, (k + 1) >> 1)];
     }
+    const typename Op::ColState cs = A.col(Gf, bc, q);
 #pragma unroll
     for (int m = 0; m < kKZ; ++m) {
         const int k = q.k0 + m;
         if (k > Gf.nz) break;
         const int c = q.c0 + pxy * k;
         const float xv = col[m + 1];
-        const float vxm = y[c + q.o.xm] + par(ixm, q.j, k), vxp = y[c + q.o.xp] + par(ixp, q.j, k);
-        const float vym = y[c + q.o.ym] + par(q.i, jym, k), vyp = y[c + q.o.yp] + par(q.i, jyp, k);
-        const float ax = A.sx[c] * (xv - vxm) + A.sx[c + 1] * (xv - vxp) + A.sy[c] * (xv - vym) +
-                         A.sy[c + px] * (xv - vyp) + A.sz[c] * (xv - col[m]) + A.sz[c + pxy] * (xv - col[m + 2]);
-        xout[c] = xv + omega * (f[c] - ax) / A.dg[c];
+        const Faces F = A.at(Gf, q, cs, m, c);
+        const float ax = apply_faces(F, xv, y[c + q.o.xm] + par(ixm, q.j, k), y[c + q.o.xp] + par(ixp, q.j, k),
+                                     y[c + q.o.ym] + par(q.i, jym, k), y[c + q.o.yp] + par(q.i, jyp, k), col[m],
+                                     col[m + 2]);
+        xout[c] = xv + omega * (f[c] - ax) * A.inv_diag(c);
     }
-}
-
-__global__ void __launch_bounds__(256) k_mg_jac0(Geo G, const float* __restrict__ f, const float* __restrict__ dg,
-                                                 float* x, float omega, const PCGState* st) {
-    if (st->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k = blockIdx.z + 1;
-    if (i > G.nx || j > G.ny || k > G.nz) return;
-    const int c = (int)G.idx(i, j, k);
-    x[c] = omega * f[c] / dg[c];
 }
 
 // x_out = x_in + omega (f - A x_in)/dg; optionally (level 0, last sweep) the dot f.x_out -> rz, beta
 __global__ void __launch_bounds__(256) k_mg_jac(Geo G, BC bc, const float* __restrict__ xin, const float* __restrict__ f,
-                                                MGOps A, float* __restrict__ xout, float omega, PCGState* st,
+                                                OpStored A, float* __restrict__ xout, float omega, PCGState* st,
                                                 int do_dot, double* partial, unsigned int* counter) {
     if (st->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -250,9 +311,12 @@ __global__ void __launch_bounds__(256) k_mg_jac(Geo G, BC bc, const float* __res
     if (i <= G.nx && j <= G.ny && k <= G.nz) {
         const int c = (int)G.idx(i, j, k);
         const Nb o = neighbours(G, bc, i, j, k);
-        const float ax = apply_A(xin, A.sx, A.sy, A.sz, c, o, G.px, (int)G.pxy);
+        const Faces F = A.cell(G, i, j, k, c);
+        const float xc = xin[c];
+        const float ax = apply_faces(F, xc, xin[c + o.xm], xin[c + o.xp], xin[c + o.ym], xin[c + o.yp], xin[c + o.zm],
+                                     xin[c + o.zp]);
         const float fv = f[c];
-        const float v = xin[c] + omega * (fv - ax) / A.dg[c];
+        const float v = xc + omega * (fv - ax) * A.inv_diag(c);
         xout[c] = v;
         dot = (double)fv * (double)v;
     }
@@ -268,8 +332,9 @@ __global__ void __launch_bounds__(256) k_mg_jac(Geo G, BC bc, const float* __res
 }
 
 // f_c = (1/8) sum over the 8 children of (f - A x)
+template <class Op>
 __global__ void __launch_bounds__(256) k_mg_restrict(Geo Gf, Geo Gc, BC bc, const float* __restrict__ x,
-                                                     const float* __restrict__ f, MGOps A, float* fc, const PCGState* st) {
+                                                     const float* __restrict__ f, Op A, float* fc, const PCGState* st) {
     if (st->done) return;
     const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -285,56 +350,36 @@ __global__ void __launch_bounds__(256) k_mg_restrict(Geo Gf, Geo Gc, BC bc, cons
                 const int i = 2 * I - 1 + dx, j = 2 * J - 1 + dy, k = 2 * K - 1 + dz;
                 const int c = (int)Gf.idx(i, j, k);
                 const Nb o = neighbours(Gf, bc, i, j, k);
-                s += f[c] - apply_A(x, A.sx, A.sy, A.sz, c, o, Gf.px, (int)Gf.pxy);
+                const Faces F = A.cell(Gf, i, j, k, c);
+                const float xv = x[c];
+                s += f[c] - apply_faces(F, xv, x[c + o.xm], x[c + o.xp], x[c + o.ym], x[c + o.yp], x[c + o.zm],
+                                        x[c + o.zp]);
             }
     fc[Gc.idx(I, J, K)] = 0.125f * s;
 }
 
-// x_out = x' + omega (f - A x')/dg with x' = y + P xc (piecewise-constant prolongation)
-__global__ void __launch_bounds__(256) k_mg_prolong_jac(Geo Gf, Geo Gc, BC bc, const float* __restrict__ y,
-                                                        const float* __restrict__ xc, const float* __restrict__ f,
-                                                        MGOps A, float* __restrict__ xout, float omega,
-                                                        const PCGState* st) {
-    if (st->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k = blockIdx.z + 1;
-    if (i > Gf.nx || j > Gf.ny || k > Gf.nz) return;
-    const int c = (int)Gf.idx(i, j, k);
-    const Nb o = neighbours(Gf, bc, i, j, k);
-    auto xp = [&](int ii, int jj, int kk, int cc) { return y[cc] + xc[Gc.idx((ii + 1) >> 1, (jj + 1) >> 1, (kk + 1) >> 1)]; };
-    // neighbour coordinates follow the offsets (mapped to the cell itself on Neumann faces)
-    const int ixm = (o.xm == -1) ? i - 1 : (o.xm == 0 ? i : Gf.nx), ixp = (o.xp == 1) ? i + 1 : (o.xp == 0 ? i : 1);
-    const int jym = (o.ym == -Gf.px) ? j - 1 : (o.ym == 0 ? j : Gf.ny), jyp = (o.yp == Gf.px) ? j + 1 : (o.yp == 0 ? j : 1);
-    const int kzm = (o.zm == -(int)Gf.pxy) ? k - 1 : (o.zm == 0 ? k : Gf.nz), kzp = (o.zp == (int)Gf.pxy) ? k + 1 : (o.zp == 0 ? k : 1);
-    const float xcv = xp(i, j, k, c);
-    const float ax = A.sx[c] * (xcv - xp(ixm, j, k, c + o.xm)) + A.sx[c + 1] * (xcv - xp(ixp, j, k, c + o.xp)) +
-                     A.sy[c] * (xcv - xp(i, jym, k, c + o.ym)) + A.sy[c + Gf.px] * (xcv - xp(i, jyp, k, c + o.yp)) +
-                     A.sz[c] * (xcv - xp(i, j, kzm, c + o.zm)) + A.sz[c + (int)Gf.pxy] * (xcv - xp(i, j, kzp, c + o.zp));
-    xout[c] = xcv + omega * (f[c] - ax) / A.dg[c];
-}
-
 // coarsest grid (<= 1024 cells): damped Jacobi sweeps in shared memory, one block
-__global__ void __launch_bounds__(1024) k_mg_coarsest(Geo G, BC bc, const float* __restrict__ f, MGOps A,
+__global__ void __launch_bounds__(1024) k_mg_coarsest(Geo G, BC bc, const float* __restrict__ f, OpStored A,
                                                       float* y, int sweeps, float omega, const PCGState* st) {
     if (st->done) return;
     __shared__ float xs[2][1024];
     const int n = G.nx * G.ny * G.nz;
     const int t = threadIdx.x;
-    int i = 0, j = 0, k = 0, c = 0;
-    float fv = 0.f, dgv = 1.f, s[6] = {0, 0, 0, 0, 0, 0};
+    int c = 0;
+    float fv = 0.f, idgv = 1.f, s[6] = {0, 0, 0, 0, 0, 0};
     int nb[6] = {0, 0, 0, 0, 0, 0};
     if (t < n) {
-        i = t % G.nx + 1; j = (t / G.nx) % G.ny + 1; k = t / (G.nx * G.ny) + 1;
+        const int i = t % G.nx + 1, j = (t / G.nx) % G.ny + 1, k = t / (G.nx * G.ny) + 1;
         c = (int)G.idx(i, j, k);
-        fv = f[c]; dgv = A.dg[c];
-        s[0] = A.sx[c]; s[1] = A.sx[c + 1]; s[2] = A.sy[c]; s[3] = A.sy[c + G.px]; s[4] = A.sz[c]; s[5] = A.sz[c + (int)G.pxy];
+        fv = f[c]; idgv = A.inv_diag(c);
+        const Faces F = A.cell(G, i, j, k, c);
+        s[0] = F.xm; s[1] = F.xp; s[2] = F.ym; s[3] = F.yp; s[4] = F.zm; s[5] = F.zp;
         const int im = (i > 1) ? i - 1 : (bc.perx ? G.nx : i), ip = (i < G.nx) ? i + 1 : (bc.perx ? 1 : i);
         const int jm = (j > 1) ? j - 1 : (bc.pery ? G.ny : j), jp = (j < G.ny) ? j + 1 : (bc.pery ? 1 : j);
         const int km = (k > 1) ? k - 1 : (bc.perz ? G.nz : k), kp = (k < G.nz) ? k + 1 : (bc.perz ? 1 : k);
         auto lin = [&](int a, int b, int d) { return (a - 1) + G.nx * ((b - 1) + G.ny * (d - 1)); };
         nb[0] = lin(im, j, k); nb[1] = lin(ip, j, k); nb[2] = lin(i, jm, k); nb[3] = lin(i, jp, k); nb[4] = lin(i, j, km); nb[5] = lin(i, j, kp);
-        xs[0][t] = omega * fv / dgv;
+        xs[0][t] = omega * fv * idgv;
     }
     __syncthreads();
     int cur = 0;
@@ -344,7 +389,7 @@ __global__ void __launch_bounds__(1024) k_mg_coarsest(Geo G, BC bc, const float*
             float ax = 0.f;
 #pragma unroll
             for (int m = 0; m < 6; ++m) ax += s[m] * (xc - xs[cur][nb[m]]);
-            xs[cur ^ 1][t] = xc + omega * (fv - ax) / dgv;
+            xs[cur ^ 1][t] = xc + omega * (fv - ax) * idgv;
         }
         __syncthreads();
         cur ^= 1;
@@ -356,86 +401,29 @@ __global__ void __launch_bounds__(1024) k_mg_coarsest(Geo G, BC bc, const float*
 // inner PCG on A (FP32 vectors, FP64 reductions)
 // ------------------------------------------------------------------------------------
 // p = z + beta p_old (also at the neighbours), q = A p, p.q -> alpha
-__global__ void __launch_bounds__(256) k_pcg_spmv(Geo G, BC bc, const float* __restrict__ z,
-                                                  const float* __restrict__ p_old, float* __restrict__ p_new,
-                                                  float* __restrict__ q, MGOps A, PCGState* st, double* partial,
-                                                  unsigned int* counter) {
-    if (st->done) return;
-    const float beta = (float)st->beta;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k = blockIdx.z + 1;
-    double dot = 0.;
-    if (i <= G.nx && j <= G.ny && k <= G.nz) {
-        const int c = (int)G.idx(i, j, k);
-        const Nb o = neighbours(G, bc, i, j, k);
-        auto pn = [&](int cc) { return z[cc] + beta * p_old[cc]; };
-        const float pc = pn(c);
-        const float qv = A.sx[c] * (pc - pn(c + o.xm)) + A.sx[c + 1] * (pc - pn(c + o.xp)) +
-                         A.sy[c] * (pc - pn(c + o.ym)) + A.sy[c + G.px] * (pc - pn(c + o.yp)) +
-                         A.sz[c] * (pc - pn(c + o.zm)) + A.sz[c + (int)G.pxy] * (pc - pn(c + o.zp));
-        p_new[c] = pc;
-        q[c] = qv;
-        dot = (double)pc * (double)qv;
-    }
-    double t, u;
-    if (reduce2_last(dot, 0.0, partial, counter, t, u) && flat_tid() == 0) {
-        st->pq = t;
-        st->alpha = st->rz / t;
-        if (!isfinite(st->alpha)) { st->status = SULI_ERR_NAN; st->done = 1; }
-    }
-}
-
-// x += alpha p, r -= alpha q, r.r and the inner stopping test
-__global__ void __launch_bounds__(256) k_pcg_update(Geo G, float* __restrict__ x, float* __restrict__ r,
-                                                    const float* __restrict__ p, const float* __restrict__ q,
-                                                    PCGState* st, double* partial, unsigned int* counter) {
-    if (st->done) return;
-    const float alpha = (float)st->alpha;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k = blockIdx.z + 1;
-    double rr = 0.;
-    if (i <= G.nx && j <= G.ny && k <= G.nz) {
-        const int c = (int)G.idx(i, j, k);
-        x[c] = x[c] + alpha * p[c];
-        const float rv = r[c] - alpha * q[c];
-        r[c] = rv;
-        rr = (double)rv * (double)rv;
-    }
-    double t, u;
-    if (reduce2_last(rr, 0.0, partial, counter, t, u) && flat_tid() == 0) {
-        st->rr = t;
-        st->iters = st->iters + 1;
-        bool go = t > st->tol2;
-        if (st->iters >= st->maxit) go = false;
-        if (!isfinite(t)) { go = false; st->status = SULI_ERR_NAN; }
-        st->done = go ? 0 : 1;
-    }
-}
-
-// column forms of the two PCG kernels
+template <class Op>
 __global__ void __launch_bounds__(256) k_pcg_spmvc(Geo G, BC bc, const float* __restrict__ z,
                                                    const float* __restrict__ p_old, float* __restrict__ p_new,
-                                                   float* __restrict__ q, MGOps A, PCGState* st, double* partial,
+                                                   float* __restrict__ q, Op A, PCGState* st, double* partial,
                                                    unsigned int* counter) {
     if (st->done) return;
     const float beta = (float)st->beta;
     const Col cq = column(G, bc);
     double dot = 0.;
     if (cq.in) {
-        const int px = G.px, pxy = (int)G.pxy;
+        const int pxy = (int)G.pxy;
         auto pn = [&](int cc) { return z[cc] + beta * p_old[cc]; };
         float col[kKZ + 2];
         load_col(G, bc, cq, pn, col);
+        const typename Op::ColState cs = A.col(G, bc, cq);
 #pragma unroll
         for (int m = 0; m < kKZ; ++m) {
             if (cq.k0 + m > G.nz) break;
             const int c = cq.c0 + pxy * (cq.k0 + m);
             const float pc = col[m + 1];
-            const float qv = A.sx[c] * (pc - pn(c + cq.o.xm)) + A.sx[c + 1] * (pc - pn(c + cq.o.xp)) +
-                             A.sy[c] * (pc - pn(c + cq.o.ym)) + A.sy[c + px] * (pc - pn(c + cq.o.yp)) +
-                             A.sz[c] * (pc - col[m]) + A.sz[c + pxy] * (pc - col[m + 2]);
+            const Faces F = A.at(G, cq, cs, m, c);
+            const float qv = apply_faces(F, pc, pn(c + cq.o.xm), pn(c + cq.o.xp), pn(c + cq.o.ym), pn(c + cq.o.yp),
+                                         col[m], col[m + 2]);
             p_new[c] = pc;
             q[c] = qv;
             dot += (double)pc * (double)qv;
@@ -537,18 +525,20 @@ __global__ void k_zero_f(float* a, long long n) {
 // ------------------------------------------------------------------------------------
 static const dim3 kB2(32, 8, 1);
 static inline dim3 cells3(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
-static inline MGOps ops(const MGLevel& L) { return MGOps{L.sx, L.sy, L.sz, L.dg}; }
+static inline OpStored stored(const MGLevel& L) { return OpStored{L.sx, L.sy, L.sz, L.idg}; }
+static inline OpRho from_rho(const MGLevel& L) { return OpRho{L.rho, L.idg, L.c2}; }
 
 void launch_mx_setup(suli_ctx* c) {
     ProfScope ps(c, SULI_K_CG_SETUP, (int)c->mg.size());
     MGLevel& L0 = c->mg[0];
-    k_mx_faces0<<<cells3(L0.g), kB2, 0, c->stream>>>(L0.g, c->bc, c->f[SULI_F_RHO], c->dt / (c->P.dx * c->P.dx),
-                                                     c->dt / (c->P.dy * c->P.dy), c->dt / (c->P.dz * c->P.dz), L0.sx, L0.sy,
-                                                     L0.sz, L0.dg);
+    const float cx2 = (float)(2. * c->dt / (c->P.dx * c->P.dx)), cy2 = (float)(2. * c->dt / (c->P.dy * c->P.dy)),
+                cz2 = (float)(2. * c->dt / (c->P.dz * c->P.dz));
+    k_mx_faces0<<<cells3(L0.g), kB2, 0, c->stream>>>(L0.g, c->bc, c->f[SULI_F_RHO], cx2, cy2, cz2, L0.rho, L0.sx,
+                                                     L0.sy, L0.sz, L0.idg, L0.c2);
     for (size_t l = 1; l < c->mg.size(); ++l) {
         MGLevel& F = c->mg[l - 1];
         MGLevel& C = c->mg[l];
-        k_mg_coarsen<<<cells3(C.g), kB2, 0, c->stream>>>(F.g, C.g, c->bc, F.sx, F.sy, F.sz, C.sx, C.sy, C.sz, C.dg);
+        k_mg_coarsen<<<cells3(C.g), kB2, 0, c->stream>>>(F.g, C.g, c->bc, F.sx, F.sy, F.sz, C.sx, C.sy, C.sz, C.idg);
     }
 }
 
@@ -575,26 +565,37 @@ void launch_vcycle(suli_ctx* c) {
     const BC bc = c->bc;
     for (int l = 0; l < L - 1; ++l) {
         MGLevel& M = c->mg[l];
-        const float* f = (l == 0) ? c->pc_r : M.f;
-        k_mg_pre<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, f, ops(M), M.y, om, c->pcg);
         MGLevel& C = c->mg[l + 1];
-        k_mg_restrict<<<cells3(C.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, f, ops(M), C.f, c->pcg);
+        if (l == 0) {
+            k_mg_pre<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, c->pc_r, from_rho(M), M.y, om, c->pcg);
+            k_mg_restrict<<<cells3(C.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, c->pc_r, from_rho(M), C.f, c->pcg);
+        } else {
+            k_mg_pre<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, M.f, stored(M), M.y, om, c->pcg);
+            k_mg_restrict<<<cells3(C.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, M.f, stored(M), C.f, c->pcg);
+        }
     }
     MGLevel& B = c->mg[L - 1];
     if (L == 1) {   // a single level: coarsest sweeps, then one more sweep that forms r.z
-        k_mg_coarsest<<<1, 1024, 0, c->stream>>>(B.g, bc, c->pc_r, ops(B), B.x, c->coarse_sweeps, om, c->pcg);
-        k_mg_jac<<<cells3(B.g), kB2, 0, c->stream>>>(B.g, bc, B.x, c->pc_r, ops(B), B.y, om, c->pcg, 1,
+        k_mg_coarsest<<<1, 1024, 0, c->stream>>>(B.g, bc, c->pc_r, stored(B), B.x, c->coarse_sweeps, om, c->pcg);
+        k_mg_jac<<<cells3(B.g), kB2, 0, c->stream>>>(B.g, bc, B.x, c->pc_r, stored(B), B.y, om, c->pcg, 1,
                                                      c->red_partial, c->red_counter);
         return;
     }
-    k_mg_coarsest<<<1, 1024, 0, c->stream>>>(B.g, bc, B.f, ops(B), B.y, c->coarse_sweeps, om, c->pcg);
+    k_mg_coarsest<<<1, 1024, 0, c->stream>>>(B.g, bc, B.f, stored(B), B.y, c->coarse_sweeps, om, c->pcg);
     for (int l = L - 2; l >= 0; --l) {
         MGLevel& M = c->mg[l];
         MGLevel& C = c->mg[l + 1];
-        const float* f = (l == 0) ? c->pc_r : M.f;
-        k_mg_post<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, C.y, f, ops(M), M.x, om, alpha, c->pcg);
-        k_mg_jacc<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, M.x, f, ops(M), M.y, om, c->pcg, l == 0 ? 1 : 0,
-                                                       c->red_partial, c->red_counter);
+        if (l == 0) {
+            k_mg_post<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, C.y, c->pc_r, from_rho(M), M.x, om, alpha,
+                                                           c->pcg);
+            k_mg_jacc<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, M.x, c->pc_r, from_rho(M), M.y, om, c->pcg, 1,
+                                                           c->red_partial, c->red_counter);
+        } else {
+            k_mg_post<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, C.y, M.f, stored(M), M.x, om, alpha,
+                                                           c->pcg);
+            k_mg_jacc<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, M.x, M.f, stored(M), M.y, om, c->pcg, 0,
+                                                           c->red_partial, c->red_counter);
+        }
     }
 }
 
@@ -603,8 +604,12 @@ void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new) {
     MGLevel& M0 = c->mg[0];
     {
         ProfScope ps(c, SULI_K_CG_SPMV, 1);
-        k_pcg_spmvc<<<colgrid(G), kB2, 0, c->stream>>>(G, c->bc, M0.y, p_old, p_new, c->pc_q, ops(M0), c->pcg,
-                                                       c->red_partial, c->red_counter);
+        if (c->mg.size() > 1)
+            k_pcg_spmvc<<<colgrid(G), kB2, 0, c->stream>>>(G, c->bc, M0.y, p_old, p_new, c->pc_q, from_rho(M0), c->pcg,
+                                                           c->red_partial, c->red_counter);
+        else
+            k_pcg_spmvc<<<colgrid(G), kB2, 0, c->stream>>>(G, c->bc, M0.y, p_old, p_new, c->pc_q, stored(M0), c->pcg,
+                                                           c->red_partial, c->red_counter);
     }
     {
         ProfScope ps(c, SULI_K_CG_UPDATE, 1);

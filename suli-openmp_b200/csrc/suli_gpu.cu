@@ -242,7 +242,7 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
             nx /= 2; ny /= 2; nz /= 2;
             gs.push_back(make_geo(nx, ny, nz));
         }
-        size_t tot = 5 * (size_t)gs[0].n;
+        size_t tot = 6 * (size_t)gs[0].n + 64;
         for (auto& g : gs) tot += 7 * (size_t)g.n;
         if ((e = cudaMalloc(&c->f32_arena, tot * sizeof(float))) != cudaSuccess) return bail(e, "f32 arena");
         if ((e = cudaMemsetAsync(c->f32_arena, 0, tot * sizeof(float), c->stream)) != cudaSuccess) return bail(e, "memset");
@@ -253,8 +253,9 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
         for (auto& g : gs) {
             MGLevel L;
             L.g = g;
-            L.sx = take(g.n); L.sy = take(g.n); L.sz = take(g.n); L.dg = take(g.n);
+            L.sx = take(g.n); L.sy = take(g.n); L.sz = take(g.n); L.idg = take(g.n);
             L.f = take(g.n); L.x = take(g.n); L.y = take(g.n);
+            if (c->mg.empty()) { L.rho = take(g.n); L.c2 = take(64); }
             c->mg.push_back(L);
         }
         if ((e = cudaMalloc(&c->cg_e2, per * sizeof(double))) != cudaSuccess) return bail(e, "e2");
