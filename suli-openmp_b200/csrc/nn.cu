@@ -345,17 +345,27 @@ void conv_launch(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat
     k_conv3_fwd<NF><<<grid, 256, smem, N->stream>>>(vol, in, W, bias, relu, out);
 }
 
-void conv_tc(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu,
-             int cout, __nv_bfloat16* out) {
+template <int NZ>
+void conv_tc_nz(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu,
+                int cout, int tcols, __nv_bfloat16* out) {
     static bool attr_done[64] = {false};
     if (!attr_done[N->device]) {
-        cudaFuncSetAttribute(k_conv3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(k_conv3_tc<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         attr_done[N->device] = true;
     }
+    const dim3 grid((vol.nx + TCX - 1) / TCX, (vol.ny + TCY - 1) / TCY, (vol.nz + NZ - 1) / NZ);
+    k_conv3_tc<NZ><<<grid, 128, tc_smem_bytes<NZ>(cout), N->stream>>>(vol, in, W, bias, relu, cout, tcols, out,
+                                                                       N->err_flag);
+}
+
+// z-planes per CTA: as many as keep the CTA's accumulators within 128 TMEM columns
+void conv_tc(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu,
+             int cout, __nv_bfloat16* out) {
     int tcols = 32;
     while (tcols < cout) tcols *= 2;
-    const dim3 grid((vol.nx + TCX - 1) / TCX, (vol.ny + TCY - 1) / TCY, vol.nz);
-    k_conv3_tc<<<grid, 128, tc_smem_bytes(cout), N->stream>>>(vol, in, W, bias, relu, cout, tcols, out, N->err_flag);
+    if (tcols <= 32) conv_tc_nz<4>(N, vol, in, W, bias, relu, cout, tcols, out);
+    else if (tcols <= 64) conv_tc_nz<2>(N, vol, in, W, bias, relu, cout, tcols, out);
+    else conv_tc_nz<1>(N, vol, in, W, bias, relu, cout, tcols, out);
 }
 
 void conv(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu, int cout,

@@ -32,16 +32,24 @@
 namespace suli {
 namespace nn {
 
-constexpr int TCX = 8, TCY = 16;                // output tile (z extent 1)
-constexpr int TC_HX = TCX + 2, TC_HY = TCY + 2, TC_HZ = 3;
+constexpr int TCX = 8, TCY = 16;                // one MMA tile: 8 x 16 voxels of a z-plane
+constexpr int TC_HX = TCX + 2, TC_HY = TCY + 2;
 constexpr int TC_CC = 16;                       // channels per K chunk
-constexpr int TC_RUN_BYTES = TC_HX * 16;                 // one x-run of 10 rows: 160
-constexpr int TC_KC_BYTES = TC_HZ * TC_HY * TC_RUN_BYTES;  // one 8-channel plane: 8640
-constexpr int TC_HALO_BYTES = 2 * TC_KC_BYTES;             // 17280
+constexpr int TC_RUN_BYTES = TC_HX * 16;        // one x-run of 10 rows: 160
 
-// shared memory of a CTA: halo copies, weights of one chunk (27 taps), barrier, TMEM address
+// A CTA owns NZ consecutive z-planes of an 8 x 16 column (NZ MMA tiles, NZ accumulators):
+// the halo has NZ + 2 planes and the weights are staged once for all of them.
+template <int NZ>
+struct TcTile {
+    static constexpr int HZ = NZ + 2;
+    static constexpr int KC_BYTES = HZ * TC_HY * TC_RUN_BYTES;   // one 8-channel plane of the halo
+    static constexpr int HALO_BYTES = 2 * KC_BYTES;
+};
 __host__ __device__ constexpr int tc_weight_bytes(int cout) { return 27 * cout * TC_CC * 2; }
-__host__ __device__ constexpr int tc_smem_bytes(int cout) { return TC_HALO_BYTES + tc_weight_bytes(cout) + 128; }
+template <int NZ>
+__host__ __device__ constexpr int tc_smem_bytes(int cout) {
+    return TcTile<NZ>::HALO_BYTES + tc_weight_bytes(cout) + 128;
+}
 
 __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
     uint64_t d = 0;
@@ -105,24 +113,27 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 
 // Forward 3x3x3 convolution on the tensor cores.  Same operands as k_conv3_fwd; Cout in
-// {16, 32, 48, 64, 96, 160}, Cin a multiple of 16.  `tcols` = TMEM columns to allocate (a
-// power of two >= max(32, Cout)).  Grid (ceil(nx/8), ceil(ny/16), nz), 128 threads.
+// {16, 32, 48, 64, 96, 160}, Cin a multiple of 16.  `tcols` = TMEM columns of one accumulator
+// (a power of two >= max(32, Cout)); the CTA allocates NZ of them.  Grid (ceil(nx/8),
+// ceil(ny/16), ceil(nz/NZ)), 128 threads.
+template <int NZ>
 __global__ void __launch_bounds__(128) k_conv3_tc(Vol vol, ConvIn in, const __nv_bfloat16* __restrict__ W,
                                                   const float* __restrict__ bias, int relu, int cout, int tcols,
                                                   __nv_bfloat16* __restrict__ out, int* err) {
+    using T = TcTile<NZ>;
     extern __shared__ __align__(1024) unsigned char smem_tc[];
     unsigned char* halo = smem_tc;
-    unsigned char* wsm = smem_tc + TC_HALO_BYTES;
+    unsigned char* wsm = smem_tc + T::HALO_BYTES;
     uint64_t* mbar = reinterpret_cast<uint64_t*>(wsm + tc_weight_bytes(cout));
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(wsm + tc_weight_bytes(cout) + 64);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int cin = in.ca + in.cb;
-    const int x0 = blockIdx.x * TCX, y0 = blockIdx.y * TCY, z0 = blockIdx.z;
+    const int x0 = blockIdx.x * TCX, y0 = blockIdx.y * TCY, z0 = blockIdx.z * NZ;
     const uint32_t mbar_a = smem_u32(mbar);
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(tcols));
+                     "r"(NZ * tcols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
@@ -136,14 +147,15 @@ __global__ void __launch_bounds__(128) k_conv3_tc(Vol vol, ConvIn in, const __nv
     const uint32_t idesc = tc_idesc(cout);
     const int hxn = (vol.nx + 1) / 2, hyn = (vol.ny + 1) / 2;
     const int nchunks = cin / TC_CC;
+    const int ng = cout / 8;
+    const uint32_t hbase = smem_u32(halo), wbase = smem_u32(wsm);
     bool ok = true;
     uint32_t phase = 0;
 
     for (int ch = 0; ch < nchunks && ok; ++ch) {
         const int c0 = ch * TC_CC;
-        // ---- stage the halo of channels c0..c0+15: 10 x 18 x 3 voxels x 2 rows of 8 channels
-        const uint32_t hbase = smem_u32(halo), wbase = smem_u32(wsm);
-        for (int q = tid; q < TC_HX * TC_HY * TC_HZ * 2; q += 128) {
+        // ---- halo of channels c0..c0+15: 10 x 18 x (NZ+2) voxels x 2 rows of 8 channels
+        for (int q = tid; q < TC_HX * TC_HY * T::HZ * 2; q += 128) {
             const int kc = q & 1, h = q >> 1;
             const int hx = h % TC_HX, hy = (h / TC_HX) % TC_HY, hz = h / (TC_HX * TC_HY);
             const int gx = x0 + hx - 1, gy = y0 + hy - 1, gz = z0 + hz - 1;
@@ -162,10 +174,9 @@ __global__ void __launch_bounds__(128) k_conv3_tc(Vol vol, ConvIn in, const __nv
                     src = in.b + vi * in.cb + (c - in.ca);
                 }
             }
-            cp_async16(hbase + kc * TC_KC_BYTES + (hz * TC_HY + hy) * TC_RUN_BYTES + hx * 16, src, bytes);
+            cp_async16(hbase + kc * T::KC_BYTES + (hz * TC_HY + hy) * TC_RUN_BYTES + hx * 16, src, bytes);
         }
-        // ---- stage the weights of the chunk: core matrix (tap, co/8, kc), row co%8, 16 bytes
-        const int ng = cout / 8;
+        // ---- weights of the chunk: core matrix (tap, co/8, kc), row co%8, 16 bytes
         for (int q = tid; q < 27 * cout * 2; q += 128) {
             const int kc = q & 1, row = q >> 1;   // row = tap * cout + co
             const int tap = row / cout, co = row - tap * cout;
@@ -179,12 +190,19 @@ __global__ void __launch_bounds__(128) k_conv3_tc(Vol vol, ConvIn in, const __nv
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;");
         if (tid == 0) {
-            for (int tap = 0; tap < 27; ++tap) {
-                const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
-                const uint64_t ad =
-                    tc_desc(hbase + (dz * TC_HY + dy) * TC_RUN_BYTES + dx * 16, TC_KC_BYTES, TC_RUN_BYTES);
-                const uint64_t bd = tc_desc(wbase + tap * ng * 256, 128, 256);
-                tc_mma(tmem, ad, bd, idesc, (ch > 0 || tap > 0) ? 1u : 0u);
+            // descriptors differ per tap only in their start address (field in 16-byte units)
+            const uint64_t a0 = tc_desc(hbase, T::KC_BYTES, TC_RUN_BYTES);
+            const uint64_t b0 = tc_desc(wbase, 128, 256);
+#pragma unroll
+            for (int s = 0; s < NZ; ++s) {
+                const uint32_t d = tmem + (uint32_t)(s * tcols);
+#pragma unroll
+                for (int tap = 0; tap < 27; ++tap) {
+                    const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
+                    const uint32_t aoff = (uint32_t)((((s + dz) * TC_HY + dy) * TC_RUN_BYTES + dx * 16) >> 4);
+                    const uint32_t boff = (uint32_t)((tap * ng * 256) >> 4);
+                    tc_mma(d, a0 + aoff, b0 + boff, idesc, (ch > 0 || tap > 0) ? 1u : 0u);
+                }
             }
             tc_commit(mbar_a);
         }
@@ -197,34 +215,38 @@ __global__ void __launch_bounds__(128) k_conv3_tc(Vol vol, ConvIn in, const __nv
     if (!ok) {
         if (tid == 0) atomicExch(err, 1);
     } else {
-        // ---- epilogue: row m = 32 warp + lane <-> voxel (m % 8, m / 8)
+        // ---- epilogue: row m = 32 warp + lane <-> voxel (m % 8, m / 8) of plane z0 + s
         const int m = warp * 32 + lane;
-        const int ox = x0 + (m & 7), oy = y0 + (m >> 3), oz = z0;
-        const bool store = ox < vol.nx && oy < vol.ny && oz < vol.nz;
-        const long long vo = (long long)ox + vol.nx * ((long long)oy + (long long)vol.ny * oz);
-        for (int cb = 0; cb < cout; cb += 16) {
-            uint32_t r[16];
-            tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, r);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (store) {
-                uint32_t packed[8];
+        const int ox = x0 + (m & 7), oy = y0 + (m >> 3);
 #pragma unroll
-                for (int e = 0; e < 8; ++e) {
-                    float v0 = __uint_as_float(r[2 * e]), v1 = __uint_as_float(r[2 * e + 1]);
-                    if (bias) { v0 += bias[cb + 2 * e]; v1 += bias[cb + 2 * e + 1]; }
-                    if (relu) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
-                    const __nv_bfloat162 b2 = __floats2bfloat162_rn(v0, v1);
-                    packed[e] = *reinterpret_cast<const uint32_t*>(&b2);
+        for (int s = 0; s < NZ; ++s) {
+            const int oz = z0 + s;
+            const bool store = ox < vol.nx && oy < vol.ny && oz < vol.nz;
+            const long long vo = (long long)ox + vol.nx * ((long long)oy + (long long)vol.ny * oz);
+            for (int cb = 0; cb < cout; cb += 16) {
+                uint32_t r[16];
+                tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * tcols + cb), r);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (store) {
+                    uint32_t packed[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        float v0 = __uint_as_float(r[2 * e]), v1 = __uint_as_float(r[2 * e + 1]);
+                        if (bias) { v0 += bias[cb + 2 * e]; v1 += bias[cb + 2 * e + 1]; }
+                        if (relu) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
+                        const __nv_bfloat162 b2 = __floats2bfloat162_rn(v0, v1);
+                        packed[e] = *reinterpret_cast<const uint32_t*>(&b2);
+                    }
+                    uint4* dst = reinterpret_cast<uint4*>(out + vo * cout + cb);
+                    dst[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+                    dst[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
                 }
-                uint4* dst = reinterpret_cast<uint4*>(out + vo * cout + cb);
-                dst[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
-                dst[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
             }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcols));
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NZ * tcols));
 }
 
 }  // namespace nn
