@@ -360,6 +360,66 @@ def cg_roofline(p, prof):
     }
 
 
+def unet_flops(pkg, p):
+    """Algorithmic FLOPs of one U-Net forward: 2 * 27 * Cin * Cout per voxel of each layer's
+    level, plus the 1x1x1 head."""
+    V0 = p.nx * p.ny * p.nz
+    f = sum(2 * 27 * ci * co * V0 // (8 ** lv) for ci, co, lv in pkg.learned.LAYERS)
+    return f + 2 * 16 * V0
+
+
+def mg_iteration_bytes(p):
+    """Algorithmic HBM bytes of one inner FP32 PCG iteration (4-byte values, N-sized passes):
+    level 0 forms its faces from the density, so SpMV 5, update 6, pre-smoothing 4, restriction
+    3 1/8, prolongation + smoothing 5 1/8, last smoothing sweep 5 passes; each coarser level
+    (stored faces) 25 1/4 passes of its own size."""
+    N = p.nx * p.ny * p.nz
+    fine = 5 + 6 + 4 + 3.125 + 5.125 + 5
+    coarse, n = 0.0, N
+    nx, ny, nz = p.nx, p.ny, p.nz
+    while nx * ny * nz > 1024 and nx % 2 == 0 and ny % 2 == 0 and nz % 2 == 0:
+        nx, ny, nz = nx // 2, ny // 2, nz // 2
+        coarse += 25.25 * (nx * ny * nz) / N
+    return 4 * N * (fine + coarse)
+
+
+def headline_rooflines(pkg, p, head, peaks):
+    """Rooflines of the two kernel classes that dominate the learned + mixed step."""
+    peak_hbm, kind = peaks
+    out = {}
+    k = head["kernels"]
+    it = max(head["iters_per_step"], 1e-9)
+    if k.get("mg", {}).get("ms_per_step", 0) > 0:
+        t = k["mg"]["ms_per_step"] / it / 1e3
+        b = mg_iteration_bytes(p)
+        out["inner_pcg_iteration"] = {
+            "kernel": "one FP32 inner PCG iteration (CUDA graph: SpMV, update, multigrid V-cycle)",
+            "bound": "hbm", "achieved": b / t / 1e9, "peak": peak_hbm, "unit": "GB/s", "frac": b / t / 1e9 / peak_hbm,
+            "algorithmic_bytes": b, "us": t * 1e6, "traffic": None}
+    if k.get("nn", {}).get("launches_per_step", 0) > 0:
+        fwd = k["nn"]["launches_per_step"] / (1 + len(pkg.learned.LAYERS) + 3 + 1)
+        t = k["nn"]["ms_per_step"] / max(fwd, 1e-9) / 1e3
+        fl = unet_flops(pkg, p)
+        pk = measured_tensor_peak()
+        out["unet_forward"] = {
+            "kernel": "U-Net forward (14 x k_conv3_tc tcgen05 + pack, 3 pool, head)",
+            "bound": "tensor", "achieved": fl / t / 1e12, "peak": pk, "unit": "TFLOP/s", "frac": fl / t / 1e12 / pk,
+            "peak_source": "measured bf16_tflops_sustained (MEASURED_PEAKS.json)",
+            "algorithmic_flops": fl, "ms": t * 1e3,
+            "traffic": profiled_traffic("unet_forward_256x128x128", p.nx * p.ny * p.nz)}
+    return out
+
+
+def measured_tensor_peak():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return float(json.loads(f.read_text())["bf16_tflops_sustained"])
+        except (KeyError, ValueError):
+            pass
+    return 1400.0
+
+
 def mixed_params(p, args):
     q = p.copy()
     q.precision, q.cg_stop, q.cg_tol = 1, 1, args.cg_tol
@@ -439,7 +499,15 @@ def run_ours(args):
     s = head["solver"]
     it = head["it"]
     value, ms, prof, stats, clk = head["value"], head["ms"], head["prof"], head["stats"], head["clocks"]
-    roofline = cg_roofline(p, runs["plain"]["prof"]) if "plain" in runs else None
+    roof_plain = cg_roofline(p, runs["plain"]["prof"]) if "plain" in runs else None
+    roof_head = headline_rooflines(pkg, p, head, measured_peaks()) if head_key != "plain" else {}
+    # the dominant kernel of the headline path: the class with the most device time
+    if roof_head:
+        dom = max(roof_head, key=lambda k: {"inner_pcg_iteration": head["kernels"].get("mg", {}).get("ms_per_step", 0),
+                                            "unet_forward": head["kernels"].get("nn", {}).get("ms_per_step", 0)}[k])
+        roofline = dict(roof_head[dom], name=dom)
+    else:
+        roofline = roof_plain
     # ---- end to end through the C-ABI: pinned host state in and out every step
     e2e = None
     if not args.no_e2e:
@@ -498,7 +566,8 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64+f32+bf16" if head_key == "learned" else "f64+f32", "data": "synthetic",
             "config": cfg,
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["launches"],
+            "roofline": roofline, "roofline_classes": roof_head, "roofline_plain_fp64": roof_plain,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["launches"],
             "clocks": clk, "poisson_iters_per_step": head["iters_per_step"],
             "max_div": max(st["max_div"] for st in stats),
             "cg_resid_max": max(max(st["cg_resid"]) for st in stats), "kernels": head["kernels"],

@@ -82,7 +82,9 @@ typedef struct suli_params {
     int    cg_stop;
     double cg_tol;
     int    cg_maxit;                /* 10000 in the reference                                  */
-    int    precision;               /* 0 = plain FP64; 1 = FP32 multigrid-preconditioned inner CG with FP64 refinement */
+    int    precision;               /* 0 = plain FP64; 1 = FP32 stencil arithmetic (convdiff, Smagorinsky, WENO
+                                       level set) over FP64 fields, FP32 multigrid-preconditioned inner CG
+                                       with FP64 residual/refinement, FP64 projection, divergence, volume */
     int    refine_maxit;            /* outer FP64 refinement sweeps for precision 1            */
     double inner_tol;               /* relative tolerance of each FP32 inner solve             */
     double mg_omega;                /* precision 1: damping of the multigrid Jacobi sweeps (0 = 0.9) */

@@ -23,8 +23,12 @@ namespace suli {
 // ------------------------------------------------------------------------------------
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 // Fortran MAX(x,0.) / MIN(x,0.)
-__device__ __forceinline__ double pmax(double a, double b) { return a > b ? a : b; }
-__device__ __forceinline__ double pmin(double a, double b) { return a < b ? a : b; }
+template <typename R>
+__device__ __forceinline__ R pmax(R a, R b) { return a > b ? a : b; }
+template <typename R>
+__device__ __forceinline__ R pmin(R a, R b) { return a < b ? a : b; }
+// read a stored FP64 value in the compute type R of the kernel
+#define RLD(a, i, j, k) R(FIDX((a), (i), (j), (k)))
 
 struct Thread3 {
     int i, j, k;
@@ -41,24 +45,26 @@ static inline dim3 grid3(int ni, int nj, int nk, dim3 b) {
 }
 static const dim3 kBlk(32, 8, 1);
 
+template <typename R>
 struct Weno3 {
-    double dpx, dnx, dpy, dny, dpz, dnz;
+    R dpx, dnx, dpy, dny, dpz, dnz;
 };
-// der_weno at one cell (14_level_set.f90:343-384) of a cell field f.
-__device__ __forceinline__ Weno3 der_weno_at(const Geo& G, const double* __restrict__ f, int i, int j,
-                                             int k, int ihx, int ihy, int ihz, double dx, double dy,
-                                             double dz) {
-    Weno3 W;
-    double P[7];
-    pencil7<double>([&](int q) { return FIDX(f, q, j, k); }, i, G.nx, ihx, P);
-    weno_pair<double>(P, dx, W.dpx, W.dnx);
-    pencil7<double>([&](int q) { return FIDX(f, i, q, k); }, j, G.ny, ihy, P);
-    weno_pair<double>(P, dy, W.dpy, W.dny);
-    pencil7<double>([&](int q) { return FIDX(f, i, j, q); }, k, G.nz, ihz, P);
-    weno_pair<double>(P, dz, W.dpz, W.dnz);
+// der_weno at one cell (14_level_set.f90:343-384) of a cell field f, in compute type R.
+template <typename R>
+__device__ __forceinline__ Weno3<R> der_weno_at(const Geo& G, const double* __restrict__ f, int i, int j, int k,
+                                                int ihx, int ihy, int ihz, double dx, double dy, double dz) {
+    Weno3<R> W;
+    R P[7];
+    pencil7<R>([&](int q) { return R(FIDX(f, q, j, k)); }, i, G.nx, ihx, P);
+    weno_pair<R>(P, R(dx), W.dpx, W.dnx);
+    pencil7<R>([&](int q) { return R(FIDX(f, i, q, k)); }, j, G.ny, ihy, P);
+    weno_pair<R>(P, R(dy), W.dpy, W.dny);
+    pencil7<R>([&](int q) { return R(FIDX(f, i, j, q)); }, k, G.nz, ihz, P);
+    weno_pair<R>(P, R(dz), W.dpz, W.dnz);
     return W;
 }
-__device__ __forceinline__ double larger(double a, double b) { return (fabs(a) > fabs(b)) ? a : b; }
+template <typename R>
+__device__ __forceinline__ R larger(R a, R b) { return (fabs(a) > fabs(b)) ? a : b; }
 
 struct LsConst {
     int ihx, ihy, ihz, ihn;
@@ -71,6 +77,7 @@ struct LsConst {
 // ------------------------------------------------------------------------------------
 // level set: mod_ls1 part A + heaviside + volume (14_level_set.f90:612-722, 743-759)
 // ------------------------------------------------------------------------------------
+template <typename R>
 __global__ void __launch_bounds__(256) k_lsprops(Geo G, LsConst L, const double* __restrict__ ls,
                                                  double* mod_ls, double* nrmx, double* nrmy, double* nrmz,
                                                  double* hs, double* hsx, double* hsy, double* hsz, double* rho,
@@ -81,14 +88,15 @@ __global__ void __launch_bounds__(256) k_lsprops(Geo G, LsConst L, const double*
     double vol = 0.0;
     if (in) {
         const long long c = G.idx(t.i, t.j, t.k);
-        const Weno3 W = der_weno_at(G, ls, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
-        const double a = larger(W.dpx, W.dnx), b = larger(W.dpy, W.dny), cc = larger(W.dpz, W.dnz);
+        const Weno3<R> W = der_weno_at<R>(G, ls, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
+        const R ar = larger(W.dpx, W.dnx), br = larger(W.dpy, W.dny), cr = larger(W.dpz, W.dnz);
         if (do_mod) {
-            const double m = sqrt(a * a + b * b + cc * cc);
-            mod_ls[c] = m;
-            if (m == 0) { nrmx[c] = 0.; nrmy[c] = 0.; nrmz[c] = 0.; }
-            else { const double im = 1. / m; nrmx[c] = a * im; nrmy[c] = b * im; nrmz[c] = cc * im; }
+            const R m = sqrt(ar * ar + br * br + cr * cr);
+            mod_ls[c] = (double)m;
+            if (m == R(0)) { nrmx[c] = 0.; nrmy[c] = 0.; nrmz[c] = 0.; }
+            else { const R im = R(1) / m; nrmx[c] = (double)(ar * im); nrmy[c] = (double)(br * im); nrmz[c] = (double)(cr * im); }
         }
+        const double a = (double)ar, b = (double)br, cc = (double)cr;   // the Heaviside stays FP64
         if (do_hs) {
             const double l = ls[c];
             double h;
@@ -116,27 +124,29 @@ __global__ void __launch_bounds__(256) k_lsprops(Geo G, LsConst L, const double*
 }
 
 // mod_ls1 part B: curvature from the WENO derivatives of the normal (14_level_set.f90:761-803)
+template <typename R>
 __global__ void __launch_bounds__(256) k_curv(Geo G, LsConst L, const double* __restrict__ nx_,
                                               const double* __restrict__ ny_, const double* __restrict__ nz_,
                                               double* ddx, double* ddy, double* ddz, double* kurv) {
     const Thread3 t = tid3(1, 1, 1);
     if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
-    double P[7], dp, dn;
-    pencil7<double>([&](int q) { return FIDX(nx_, q, t.j, t.k); }, t.i, G.nx, L.ihn, P);
-    weno_pair<double>(P, L.dx, dp, dn);
-    const double ax = (fabs(dn) > fabs(dp)) ? dn : dp;
-    pencil7<double>([&](int q) { return FIDX(ny_, t.i, q, t.k); }, t.j, G.ny, L.ihn, P);
-    weno_pair<double>(P, L.dy, dp, dn);
-    const double ay = (fabs(dn) > fabs(dp)) ? dn : dp;
-    pencil7<double>([&](int q) { return FIDX(nz_, t.i, t.j, q); }, t.k, G.nz, L.ihn, P);
-    weno_pair<double>(P, L.dz, dp, dn);
-    const double az = (fabs(dn) > fabs(dp)) ? dn : dp;
+    R P[7], dp, dn;
+    pencil7<R>([&](int q) { return R(FIDX(nx_, q, t.j, t.k)); }, t.i, G.nx, L.ihn, P);
+    weno_pair<R>(P, R(L.dx), dp, dn);
+    const R ax = (fabs(dn) > fabs(dp)) ? dn : dp;
+    pencil7<R>([&](int q) { return R(FIDX(ny_, t.i, q, t.k)); }, t.j, G.ny, L.ihn, P);
+    weno_pair<R>(P, R(L.dy), dp, dn);
+    const R ay = (fabs(dn) > fabs(dp)) ? dn : dp;
+    pencil7<R>([&](int q) { return R(FIDX(nz_, t.i, t.j, q)); }, t.k, G.nz, L.ihn, P);
+    weno_pair<R>(P, R(L.dz), dp, dn);
+    const R az = (fabs(dn) > fabs(dp)) ? dn : dp;
     const long long c = G.idx(t.i, t.j, t.k);
-    ddx[c] = ax; ddy[c] = ay; ddz[c] = az;
-    kurv[c] = ax + ay + az;
+    ddx[c] = (double)ax; ddy[c] = (double)ay; ddz[c] = (double)az;
+    kurv[c] = (double)(ax + ay + az);
 }
 
 // conv_weno + intt_ls: one TVD-RK3 stage of level-set transport (14_level_set.f90:287-341)
+template <typename R>
 __global__ void __launch_bounds__(256) k_ls_advect(Geo G, LsConst L, const double* __restrict__ cur,
                                                    const double* phi0, double* out,
                                                    const double* __restrict__ u, const double* __restrict__ v,
@@ -144,25 +154,26 @@ __global__ void __launch_bounds__(256) k_ls_advect(Geo G, LsConst L, const doubl
     const Thread3 t = tid3(1, 1, 1);
     if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
     const int i = t.i, j = t.j, k = t.k;
-    const Weno3 W = der_weno_at(G, cur, i, j, k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
-    const double ua = (FIDX(u, i, j, k) + FIDX(u, i + 1, j, k)) * 0.5;
-    const double va = (FIDX(v, i, j, k) + FIDX(v, i, j + 1, k)) * 0.5;
-    const double wa = (FIDX(w, i, j, k) + FIDX(w, i, j, k + 1)) * 0.5;
-    const double apos = pmax(ua, 0.), aneg = pmin(ua, 0.);
-    const double bpos = pmax(va, 0.), bneg = pmin(va, 0.);
-    const double cpos = pmax(wa, 0.), cneg = pmin(wa, 0.);
-    const double sy7 = -(apos * W.dnx + aneg * W.dpx + bpos * W.dny + bneg * W.dpy + cpos * W.dnz + cneg * W.dpz);
+    const Weno3<R> W = der_weno_at<R>(G, cur, i, j, k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
+    const R ua = (RLD(u, i, j, k) + RLD(u, i + 1, j, k)) * R(0.5);
+    const R va = (RLD(v, i, j, k) + RLD(v, i, j + 1, k)) * R(0.5);
+    const R wa = (RLD(w, i, j, k) + RLD(w, i, j, k + 1)) * R(0.5);
+    const R apos = pmax(ua, R(0)), aneg = pmin(ua, R(0));
+    const R bpos = pmax(va, R(0)), bneg = pmin(va, R(0));
+    const R cpos = pmax(wa, R(0)), cneg = pmin(wa, R(0));
+    const R sy7 = -(apos * W.dnx + aneg * W.dpx + bpos * W.dny + bneg * W.dpy + cpos * W.dnz + cneg * W.dpz);
     const long long c = G.idx(i, j, k);
     const double p0 = phi0[c];
     const double gxv = cur[c];
-    out[c] = a * p0 + b * gxv + gd * sy7;
+    out[c] = a * p0 + b * gxv + gd * (double)sy7;   // the stage combination in FP64
 }
 
 // reinic_weno selection (14_level_set.f90:406-431)
-__device__ __forceinline__ double reinit_mod(double l, const Weno3& W) {
-    const double cst = 0.00000001;
-    double a, b, c;
-    if (l > 0.) {
+template <typename R>
+__device__ __forceinline__ R reinit_mod(R l, const Weno3<R>& W) {
+    const R cst = R(0.00000001);
+    R a, b, c;
+    if (l > R(0)) {
         a = pmax(pmax(W.dnx, cst), -pmin(W.dpx, cst));
         b = pmax(pmax(W.dny, cst), -pmin(W.dpy, cst));
         c = pmax(pmax(W.dnz, cst), -pmin(W.dpz, cst));
@@ -174,30 +185,33 @@ __device__ __forceinline__ double reinit_mod(double l, const Weno3& W) {
     return sqrt(a * a + b * b + c * c);
 }
 
+template <typename R>
 __global__ void __launch_bounds__(256) k_reinit_funcs(Geo G, LsConst L, const double* __restrict__ ls,
                                                       double* funcs) {
     const Thread3 t = tid3(1, 1, 1);
     if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
-    const Weno3 W = der_weno_at(G, ls, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
+    const Weno3<R> W = der_weno_at<R>(G, ls, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
     const long long c = G.idx(t.i, t.j, t.k);
-    const double l = ls[c];
-    const double m = reinit_mod(l, W);
-    funcs[c] = l / sqrt(l * l + m * m * L.dx1 * L.dx1);
+    const R l = R(ls[c]);
+    const R m = reinit_mod(l, W);
+    const R dx1 = R(L.dx1);
+    funcs[c] = (double)(l / sqrt(l * l + m * m * dx1 * dx1));
 }
 
+template <typename R>
 __global__ void __launch_bounds__(256) k_reinit_stage(Geo G, LsConst L, const double* __restrict__ cur,
                                                       const double* phi0, double* out,
                                                       const double* __restrict__ funcs, double a, double b,
                                                       double gd) {
     const Thread3 t = tid3(1, 1, 1);
     if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
-    const Weno3 W = der_weno_at(G, cur, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
+    const Weno3<R> W = der_weno_at<R>(G, cur, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
     const long long c = G.idx(t.i, t.j, t.k);
     const double l = cur[c];
-    const double m = reinit_mod(l, W);
-    const double sy7 = funcs[c] * (1. - m);
+    const R m = reinit_mod(R(l), W);
+    const R sy7 = R(funcs[c]) * (R(1) - m);
     const double p0 = phi0[c];
-    out[c] = a * p0 + b * l + gd * sy7;
+    out[c] = a * p0 + b * l + gd * (double)sy7;   // the stage combination in FP64
 }
 
 // signed band error of the reinitialisation (14_level_set.f90:492-503): sum and count
@@ -229,28 +243,29 @@ __global__ void k_volfix(Geo G, double* ls, const double* __restrict__ mod_ls, d
 struct ViscConst {
     double dx, dy, dz, cdel, csmag;   // cdel = (dx*dy*dz)**(2/3) computed on the host
 };
+template <typename R>
 __global__ void __launch_bounds__(256) k_nut(Geo G, ViscConst V, const double* __restrict__ u,
                                              const double* __restrict__ v, const double* __restrict__ w,
                                              const double* __restrict__ rho, double* nut) {
     const Thread3 t = tid3(1, 1, 1);
     if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
     const int i = t.i, j = t.j, k = t.k;
-    const double itdx = 1. / (2. * V.dx), itdy = 1. / (2. * V.dy), itdz = 1. / (2. * V.dz);
+    const R itdx = R(1. / (2. * V.dx)), itdy = R(1. / (2. * V.dy)), itdz = R(1. / (2. * V.dz));
     // derivax/y/z of the staggered fields, then interp?_fc to the cell centre
-    const double dudx = ((FIDX(u, i + 1, j, k) - FIDX(u, i - 1, j, k)) * itdx + (FIDX(u, i + 2, j, k) - FIDX(u, i, j, k)) * itdx) * 0.5;
-    const double dudy = ((FIDX(u, i, j + 1, k) - FIDX(u, i, j - 1, k)) * itdy + (FIDX(u, i + 1, j + 1, k) - FIDX(u, i + 1, j - 1, k)) * itdy) * 0.5;
-    const double dudz = ((FIDX(u, i, j, k + 1) - FIDX(u, i, j, k - 1)) * itdz + (FIDX(u, i + 1, j, k + 1) - FIDX(u, i + 1, j, k - 1)) * itdz) * 0.5;
-    const double dvdx = ((FIDX(v, i + 1, j, k) - FIDX(v, i - 1, j, k)) * itdx + (FIDX(v, i + 1, j + 1, k) - FIDX(v, i - 1, j + 1, k)) * itdx) * 0.5;
-    const double dvdy = ((FIDX(v, i, j + 1, k) - FIDX(v, i, j - 1, k)) * itdy + (FIDX(v, i, j + 2, k) - FIDX(v, i, j, k)) * itdy) * 0.5;
-    const double dvdz = ((FIDX(v, i, j, k + 1) - FIDX(v, i, j, k - 1)) * itdz + (FIDX(v, i, j + 1, k + 1) - FIDX(v, i, j + 1, k - 1)) * itdz) * 0.5;
-    const double dwdx = ((FIDX(w, i + 1, j, k) - FIDX(w, i - 1, j, k)) * itdx + (FIDX(w, i + 1, j, k + 1) - FIDX(w, i - 1, j, k + 1)) * itdx) * 0.5;
-    const double dwdy = ((FIDX(w, i, j + 1, k) - FIDX(w, i, j - 1, k)) * itdy + (FIDX(w, i, j + 1, k + 1) - FIDX(w, i, j - 1, k + 1)) * itdy) * 0.5;
-    const double dwdz = ((FIDX(w, i, j, k + 1) - FIDX(w, i, j, k - 1)) * itdz + (FIDX(w, i, j, k + 2) - FIDX(w, i, j, k)) * itdz) * 0.5;
-    const double p1 = dudx + 0.5 * (dudy + dvdx + dudz + dwdx);
-    const double p2 = dvdy + 0.5 * (dvdx + dudy + dvdz + dwdy);
-    const double p3 = dwdz + 0.5 * (dwdy + dvdz + dudz + dwdx);
+    const R dudx = ((RLD(u, i + 1, j, k) - RLD(u, i - 1, j, k)) * itdx + (RLD(u, i + 2, j, k) - RLD(u, i, j, k)) * itdx) * R(0.5);
+    const R dudy = ((RLD(u, i, j + 1, k) - RLD(u, i, j - 1, k)) * itdy + (RLD(u, i + 1, j + 1, k) - RLD(u, i + 1, j - 1, k)) * itdy) * R(0.5);
+    const R dudz = ((RLD(u, i, j, k + 1) - RLD(u, i, j, k - 1)) * itdz + (RLD(u, i + 1, j, k + 1) - RLD(u, i + 1, j, k - 1)) * itdz) * R(0.5);
+    const R dvdx = ((RLD(v, i + 1, j, k) - RLD(v, i - 1, j, k)) * itdx + (RLD(v, i + 1, j + 1, k) - RLD(v, i - 1, j + 1, k)) * itdx) * R(0.5);
+    const R dvdy = ((RLD(v, i, j + 1, k) - RLD(v, i, j - 1, k)) * itdy + (RLD(v, i, j + 2, k) - RLD(v, i, j, k)) * itdy) * R(0.5);
+    const R dvdz = ((RLD(v, i, j, k + 1) - RLD(v, i, j, k - 1)) * itdz + (RLD(v, i, j + 1, k + 1) - RLD(v, i, j + 1, k - 1)) * itdz) * R(0.5);
+    const R dwdx = ((RLD(w, i + 1, j, k) - RLD(w, i - 1, j, k)) * itdx + (RLD(w, i + 1, j, k + 1) - RLD(w, i - 1, j, k + 1)) * itdx) * R(0.5);
+    const R dwdy = ((RLD(w, i, j + 1, k) - RLD(w, i, j - 1, k)) * itdy + (RLD(w, i, j + 1, k + 1) - RLD(w, i, j - 1, k + 1)) * itdy) * R(0.5);
+    const R dwdz = ((RLD(w, i, j, k + 1) - RLD(w, i, j, k - 1)) * itdz + (RLD(w, i, j, k + 2) - RLD(w, i, j, k)) * itdz) * R(0.5);
+    const R p1 = dudx + R(0.5) * (dudy + dvdx + dudz + dwdx);
+    const R p2 = dvdy + R(0.5) * (dvdx + dudy + dvdz + dwdy);
+    const R p3 = dwdz + R(0.5) * (dwdy + dvdz + dudz + dwdx);
     const long long c = G.idx(i, j, k);
-    nut[c] = V.cdel * V.csmag * V.csmag * sqrt(2. * (p1 + p2 + p3) * (p1 + p2 + p3)) * rho[c];
+    nut[c] = (double)(R(V.cdel * V.csmag * V.csmag) * sqrt(R(2.) * (p1 + p2 + p3) * (p1 + p2 + p3)) * R(rho[c]));
 }
 
 // xnut/ynut/znut = face(ls_nu) + face(nut) with the end-face copy of interp?_cf
@@ -298,118 +313,119 @@ __device__ __forceinline__ bool on_cap(const CDConst& C, int j, int k, int ny) {
     return (C.cap_z2 && k == 2) || (C.cap_y2 && j == 2) || (C.cap_yn && j == ny);
 }
 
+template <typename R>
 __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) {
     const Thread3 t = tid3(1, 1, 1);
     const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
     if (i > nx + 1 || j > ny + 1 || k > nz + 1) return;
-    const double idx = C.idx, idy = C.idy, idz = C.idz;   // 1/dx, 1/dy, 1/dz
+    const R idx = R(C.idx), idy = R(C.idy), idz = R(C.idz);   // 1/dx, 1/dy, 1/dz
     const double* __restrict__ u = F.u;
     const double* __restrict__ v = F.v;
     const double* __restrict__ w = F.w;
     // ---- Fu on u-faces (i = 1..nx+1, j = 1..ny, k = 1..nz)
     if (j <= ny && k <= nz) {
-        const double uc = FIDX(u, i, j, k);
-        const double bma4 = (FIDX(v, i, j, k) + FIDX(v, i - 1, j, k) + FIDX(v, i, j + 1, k) + FIDX(v, i - 1, j + 1, k)) * 0.25;
-        const double dma4 = (FIDX(w, i, j, k) + FIDX(w, i - 1, j, k) + FIDX(w, i, j, k + 1) + FIDX(w, i - 1, j, k + 1)) * 0.25;
-        double a1 = pmax(uc, 0.), a2 = pmin(uc, 0.);
-        const double dudx = a1 * (uc - FIDX(u, i - 1, j, k)) * idx + a2 * (FIDX(u, i + 1, j, k) - uc) * idx;
-        a1 = pmax(bma4, 0.); a2 = pmin(bma4, 0.);
-        const double dudy = a1 * (uc - FIDX(u, i, j - 1, k)) * idy + a2 * (FIDX(u, i, j + 1, k) - uc) * idy;
-        a1 = pmax(dma4, 0.); a2 = pmin(dma4, 0.);
-        const double dudz = a1 * (uc - FIDX(u, i, j, k - 1)) * idz + a2 * (FIDX(u, i, j, k + 1) - uc) * idz;
-        const double uint_ = dudx + dudy + dudz;
+        const R uc = RLD(u, i, j, k);
+        const R bma4 = (RLD(v, i, j, k) + RLD(v, i - 1, j, k) + RLD(v, i, j + 1, k) + RLD(v, i - 1, j + 1, k)) * R(0.25);
+        const R dma4 = (RLD(w, i, j, k) + RLD(w, i - 1, j, k) + RLD(w, i, j, k + 1) + RLD(w, i - 1, j, k + 1)) * R(0.25);
+        R a1 = pmax(uc, R(0.)), a2 = pmin(uc, R(0.));
+        const R dudx = a1 * (uc - RLD(u, i - 1, j, k)) * idx + a2 * (RLD(u, i + 1, j, k) - uc) * idx;
+        a1 = pmax(bma4, R(0.)); a2 = pmin(bma4, R(0.));
+        const R dudy = a1 * (uc - RLD(u, i, j - 1, k)) * idy + a2 * (RLD(u, i, j + 1, k) - uc) * idy;
+        a1 = pmax(dma4, R(0.)); a2 = pmin(dma4, R(0.));
+        const R dudz = a1 * (uc - RLD(u, i, j, k - 1)) * idz + a2 * (RLD(u, i, j, k + 1) - uc) * idz;
+        const R uint_ = dudx + dudy + dudz;
         const int ic = clampi(i, 2, nx);
-        const double rhox = (FIDX(F.rho, ic, j, k) + FIDX(F.rho, ic - 1, j, k)) * 0.5;
-        const double tx1 = FIDX(F.hsx, ic, j, k) * FIDX(F.kurv, ic, j, k) / FIDX(F.rho, ic, j, k);
-        const double tx0 = FIDX(F.hsx, ic - 1, j, k) * FIDX(F.kurv, ic - 1, j, k) / FIDX(F.rho, ic - 1, j, k);
-        const double dhsdx = (tx1 + tx0) * 0.5;
-        const double ama_i = FIDX(F.nut, clampi(i, 1, nx), j, k) * idx;
-        const double ama_m = FIDX(F.nut, clampi(i - 1, 1, nx), j, k) * idx;
+        const R rhox = (RLD(F.rho, ic, j, k) + RLD(F.rho, ic - 1, j, k)) * R(0.5);
+        const R tx1 = RLD(F.hsx, ic, j, k) * RLD(F.kurv, ic, j, k) / RLD(F.rho, ic, j, k);
+        const R tx0 = RLD(F.hsx, ic - 1, j, k) * RLD(F.kurv, ic - 1, j, k) / RLD(F.rho, ic - 1, j, k);
+        const R dhsdx = (tx1 + tx0) * R(0.5);
+        const R ama_i = RLD(F.nut, clampi(i, 1, nx), j, k) * idx;
+        const R ama_m = RLD(F.nut, clampi(i - 1, 1, nx), j, k) * idx;
         const int jp = clampi(j + 1, 2, ny), jm = clampi(j, 2, ny);
-        const double bma_p = ((FIDX(F.xnut, i, jp, k) + FIDX(F.xnut, i, jp - 1, k)) * 0.5) * idy;
-        const double bma_m = ((FIDX(F.xnut, i, jm, k) + FIDX(F.xnut, i, jm - 1, k)) * 0.5) * idy;
+        const R bma_p = ((RLD(F.xnut, i, jp, k) + RLD(F.xnut, i, jp - 1, k)) * R(0.5)) * idy;
+        const R bma_m = ((RLD(F.xnut, i, jm, k) + RLD(F.xnut, i, jm - 1, k)) * R(0.5)) * idy;
         const int kp = clampi(k + 1, 2, nz), km = clampi(k, 2, nz);
-        const double dma_p = ((FIDX(F.xnut, i, j, kp) + FIDX(F.xnut, i, j, kp - 1)) * 0.5) * idz;
-        const double dma_m = ((FIDX(F.xnut, i, j, km) + FIDX(F.xnut, i, j, km - 1)) * 0.5) * idz;
-        const double Gv = (ama_i * 2. * (FIDX(u, i + 1, j, k) - uc) - ama_m * 2. * (uc - FIDX(u, i - 1, j, k))) * idx +
-                          bma_p * ((FIDX(u, i, j + 1, k) - uc) * idy + (FIDX(v, i, j + 1, k) - FIDX(v, i - 1, j + 1, k)) * idx) -
-                          bma_m * ((uc - FIDX(u, i, j - 1, k)) * idy + (FIDX(v, i, j, k) - FIDX(v, i - 1, j, k)) * idx) +
-                          dma_p * ((FIDX(u, i, j, k + 1) - uc) * idz + (FIDX(w, i, j, k + 1) - FIDX(w, i - 1, j, k + 1)) * idx) -
-                          dma_m * ((uc - FIDX(u, i, j, k - 1)) * idz + (FIDX(w, i, j, k) - FIDX(w, i - 1, j, k)) * idx);
-        double r = -uint_ + Gv / rhox + C.gx - C.sigma * dhsdx;
-        if (C.tf) r = r + FIDX(F.tfu, i, j, k);
-        if (on_cap(C, j, k, ny)) { const double b = FIDX(F.ub, i, j, k); r = r - C.cz * sqrt(b * b) * uc; }
-        FIDX(F.Fu, i, j, k) = r;
+        const R dma_p = ((RLD(F.xnut, i, j, kp) + RLD(F.xnut, i, j, kp - 1)) * R(0.5)) * idz;
+        const R dma_m = ((RLD(F.xnut, i, j, km) + RLD(F.xnut, i, j, km - 1)) * R(0.5)) * idz;
+        const R Gv = (ama_i * R(2.) * (RLD(u, i + 1, j, k) - uc) - ama_m * R(2.) * (uc - RLD(u, i - 1, j, k))) * idx +
+                          bma_p * ((RLD(u, i, j + 1, k) - uc) * idy + (RLD(v, i, j + 1, k) - RLD(v, i - 1, j + 1, k)) * idx) -
+                          bma_m * ((uc - RLD(u, i, j - 1, k)) * idy + (RLD(v, i, j, k) - RLD(v, i - 1, j, k)) * idx) +
+                          dma_p * ((RLD(u, i, j, k + 1) - uc) * idz + (RLD(w, i, j, k + 1) - RLD(w, i - 1, j, k + 1)) * idx) -
+                          dma_m * ((uc - RLD(u, i, j, k - 1)) * idz + (RLD(w, i, j, k) - RLD(w, i - 1, j, k)) * idx);
+        R r = -uint_ + Gv / rhox + R(C.gx) - R(C.sigma) * dhsdx;
+        if (C.tf) r = r + RLD(F.tfu, i, j, k);
+        if (on_cap(C, j, k, ny)) { const R b = RLD(F.ub, i, j, k); r = r - R(C.cz) * sqrt(b * b) * uc; }
+        FIDX(F.Fu, i, j, k) = (double)r;
     }
     // ---- Fv on v-faces (i = 1..nx, j = 1..ny+1, k = 1..nz)
     if (i <= nx && k <= nz) {
-        const double vc = FIDX(v, i, j, k);
-        const double amb4 = (FIDX(u, i, j, k) + FIDX(u, i + 1, j, k) + FIDX(u, i, j - 1, k) + FIDX(u, i + 1, j - 1, k)) * 0.25;
-        const double dmb4 = (FIDX(w, i, j, k) + FIDX(w, i, j - 1, k) + FIDX(w, i, j, k + 1) + FIDX(w, i, j - 1, k + 1)) * 0.25;
-        double a1 = pmax(amb4, 0.), a2 = pmin(amb4, 0.);
-        const double dvdx = a1 * (vc - FIDX(v, i - 1, j, k)) * idx + a2 * (FIDX(v, i + 1, j, k) - vc) * idx;
-        a1 = pmax(vc, 0.); a2 = pmin(vc, 0.);
-        const double dvdy = a1 * (vc - FIDX(v, i, j - 1, k)) * idy + a2 * (FIDX(v, i, j + 1, k) - vc) * idy;
-        a1 = pmax(dmb4, 0.); a2 = pmin(dmb4, 0.);
-        const double dvdz = a1 * (vc - FIDX(v, i, j, k - 1)) * idz + a2 * (FIDX(v, i, j, k + 1) - vc) * idz;
-        const double vint = dvdx + dvdy + dvdz;
+        const R vc = RLD(v, i, j, k);
+        const R amb4 = (RLD(u, i, j, k) + RLD(u, i + 1, j, k) + RLD(u, i, j - 1, k) + RLD(u, i + 1, j - 1, k)) * R(0.25);
+        const R dmb4 = (RLD(w, i, j, k) + RLD(w, i, j - 1, k) + RLD(w, i, j, k + 1) + RLD(w, i, j - 1, k + 1)) * R(0.25);
+        R a1 = pmax(amb4, R(0.)), a2 = pmin(amb4, R(0.));
+        const R dvdx = a1 * (vc - RLD(v, i - 1, j, k)) * idx + a2 * (RLD(v, i + 1, j, k) - vc) * idx;
+        a1 = pmax(vc, R(0.)); a2 = pmin(vc, R(0.));
+        const R dvdy = a1 * (vc - RLD(v, i, j - 1, k)) * idy + a2 * (RLD(v, i, j + 1, k) - vc) * idy;
+        a1 = pmax(dmb4, R(0.)); a2 = pmin(dmb4, R(0.));
+        const R dvdz = a1 * (vc - RLD(v, i, j, k - 1)) * idz + a2 * (RLD(v, i, j, k + 1) - vc) * idz;
+        const R vint = dvdx + dvdy + dvdz;
         const int jc = clampi(j, 2, ny);
-        const double rhoy = (FIDX(F.rho, i, jc, k) + FIDX(F.rho, i, jc - 1, k)) * 0.5;
-        const double ty1 = FIDX(F.hsy, i, jc, k) * FIDX(F.kurv, i, jc, k) / FIDX(F.rho, i, jc, k);
-        const double ty0 = FIDX(F.hsy, i, jc - 1, k) * FIDX(F.kurv, i, jc - 1, k) / FIDX(F.rho, i, jc - 1, k);
-        const double dhsdy = (ty1 + ty0) * 0.5;
+        const R rhoy = (RLD(F.rho, i, jc, k) + RLD(F.rho, i, jc - 1, k)) * R(0.5);
+        const R ty1 = RLD(F.hsy, i, jc, k) * RLD(F.kurv, i, jc, k) / RLD(F.rho, i, jc, k);
+        const R ty0 = RLD(F.hsy, i, jc - 1, k) * RLD(F.kurv, i, jc - 1, k) / RLD(F.rho, i, jc - 1, k);
+        const R dhsdy = (ty1 + ty0) * R(0.5);
         const int ip = clampi(i + 1, 2, nx), im = clampi(i, 2, nx);
-        const double amb_p = ((FIDX(F.ynut, ip, j, k) + FIDX(F.ynut, ip - 1, j, k)) * 0.5) * idx;
-        const double amb_m = ((FIDX(F.ynut, im, j, k) + FIDX(F.ynut, im - 1, j, k)) * 0.5) * idx;
-        const double bmb_j = FIDX(F.nut, i, clampi(j, 1, ny), k) * idy;
-        const double bmb_m = FIDX(F.nut, i, clampi(j - 1, 1, ny), k) * idy;
+        const R amb_p = ((RLD(F.ynut, ip, j, k) + RLD(F.ynut, ip - 1, j, k)) * R(0.5)) * idx;
+        const R amb_m = ((RLD(F.ynut, im, j, k) + RLD(F.ynut, im - 1, j, k)) * R(0.5)) * idx;
+        const R bmb_j = RLD(F.nut, i, clampi(j, 1, ny), k) * idy;
+        const R bmb_m = RLD(F.nut, i, clampi(j - 1, 1, ny), k) * idy;
         const int kp = clampi(k + 1, 2, nz), km = clampi(k, 2, nz);
-        const double dmb_p = ((FIDX(F.ynut, i, j, kp) + FIDX(F.ynut, i, j, kp - 1)) * 0.5) * idz;
-        const double dmb_m = ((FIDX(F.ynut, i, j, km) + FIDX(F.ynut, i, j, km - 1)) * 0.5) * idz;
-        const double Gv = amb_p * ((FIDX(v, i + 1, j, k) - vc) * idx + (FIDX(u, i + 1, j, k) - FIDX(u, i + 1, j - 1, k)) * idy) -
-                          amb_m * ((vc - FIDX(v, i - 1, j, k)) * idx + (FIDX(u, i, j, k) - FIDX(u, i, j - 1, k)) * idy) +
-                          (bmb_j * 2. * (FIDX(v, i, j + 1, k) - vc) - bmb_m * 2. * (vc - FIDX(v, i, j - 1, k))) * idy +
-                          dmb_p * ((FIDX(v, i, j, k + 1) - vc) * idz + (FIDX(w, i, j, k + 1) - FIDX(w, i, j - 1, k + 1)) * idy) -
-                          dmb_m * ((vc - FIDX(v, i, j, k - 1)) * idz + (FIDX(w, i, j, k) - FIDX(w, i, j - 1, k)) * idy);
-        double r = -vint + Gv / rhoy - C.sigma * dhsdy;
-        if (C.tf) r = r + FIDX(F.tfv, i, j, k);
-        if (on_cap(C, j, k, ny)) { const double b = FIDX(F.vb, i, j, k); r = r - C.cz * sqrt(b * b) * vc; }
-        FIDX(F.Fv, i, j, k) = r;
+        const R dmb_p = ((RLD(F.ynut, i, j, kp) + RLD(F.ynut, i, j, kp - 1)) * R(0.5)) * idz;
+        const R dmb_m = ((RLD(F.ynut, i, j, km) + RLD(F.ynut, i, j, km - 1)) * R(0.5)) * idz;
+        const R Gv = amb_p * ((RLD(v, i + 1, j, k) - vc) * idx + (RLD(u, i + 1, j, k) - RLD(u, i + 1, j - 1, k)) * idy) -
+                          amb_m * ((vc - RLD(v, i - 1, j, k)) * idx + (RLD(u, i, j, k) - RLD(u, i, j - 1, k)) * idy) +
+                          (bmb_j * R(2.) * (RLD(v, i, j + 1, k) - vc) - bmb_m * R(2.) * (vc - RLD(v, i, j - 1, k))) * idy +
+                          dmb_p * ((RLD(v, i, j, k + 1) - vc) * idz + (RLD(w, i, j, k + 1) - RLD(w, i, j - 1, k + 1)) * idy) -
+                          dmb_m * ((vc - RLD(v, i, j, k - 1)) * idz + (RLD(w, i, j, k) - RLD(w, i, j - 1, k)) * idy);
+        R r = -vint + Gv / rhoy - R(C.sigma) * dhsdy;
+        if (C.tf) r = r + RLD(F.tfv, i, j, k);
+        if (on_cap(C, j, k, ny)) { const R b = RLD(F.vb, i, j, k); r = r - R(C.cz) * sqrt(b * b) * vc; }
+        FIDX(F.Fv, i, j, k) = (double)r;
     }
     // ---- Fw on w-faces (i = 1..nx, j = 1..ny, k = 1..nz+1)
     if (i <= nx && j <= ny) {
-        const double wc = FIDX(w, i, j, k);
-        const double amd4 = (FIDX(u, i, j, k) + FIDX(u, i + 1, j, k) + FIDX(u, i, j, k - 1) + FIDX(u, i + 1, j, k - 1)) * 0.25;
-        const double bmd4 = (FIDX(v, i, j, k) + FIDX(v, i, j + 1, k) + FIDX(v, i, j, k - 1) + FIDX(v, i, j + 1, k - 1)) * 0.25;
-        double a1 = pmax(amd4, 0.), a2 = pmin(amd4, 0.);
-        const double dwdx = a1 * (wc - FIDX(w, i - 1, j, k)) * idx + a2 * (FIDX(w, i + 1, j, k) - wc) * idx;
-        a1 = pmax(bmd4, 0.); a2 = pmin(bmd4, 0.);
-        const double dwdy = a1 * (wc - FIDX(w, i, j - 1, k)) * idy + a2 * (FIDX(w, i, j + 1, k) - wc) * idy;
-        a1 = pmax(wc, 0.); a2 = pmin(wc, 0.);
-        const double dwdz = a1 * (wc - FIDX(w, i, j, k - 1)) * idz + a2 * (FIDX(w, i, j, k + 1) - wc) * idz;
-        const double wint = dwdx + dwdy + dwdz;
+        const R wc = RLD(w, i, j, k);
+        const R amd4 = (RLD(u, i, j, k) + RLD(u, i + 1, j, k) + RLD(u, i, j, k - 1) + RLD(u, i + 1, j, k - 1)) * R(0.25);
+        const R bmd4 = (RLD(v, i, j, k) + RLD(v, i, j + 1, k) + RLD(v, i, j, k - 1) + RLD(v, i, j + 1, k - 1)) * R(0.25);
+        R a1 = pmax(amd4, R(0.)), a2 = pmin(amd4, R(0.));
+        const R dwdx = a1 * (wc - RLD(w, i - 1, j, k)) * idx + a2 * (RLD(w, i + 1, j, k) - wc) * idx;
+        a1 = pmax(bmd4, R(0.)); a2 = pmin(bmd4, R(0.));
+        const R dwdy = a1 * (wc - RLD(w, i, j - 1, k)) * idy + a2 * (RLD(w, i, j + 1, k) - wc) * idy;
+        a1 = pmax(wc, R(0.)); a2 = pmin(wc, R(0.));
+        const R dwdz = a1 * (wc - RLD(w, i, j, k - 1)) * idz + a2 * (RLD(w, i, j, k + 1) - wc) * idz;
+        const R wint = dwdx + dwdy + dwdz;
         const int kc = clampi(k, 2, nz);
-        const double rhoz = (FIDX(F.rho, i, j, kc) + FIDX(F.rho, i, j, kc - 1)) * 0.5;
-        const double tz1 = FIDX(F.hsz, i, j, kc) * FIDX(F.kurv, i, j, kc) / FIDX(F.rho, i, j, kc);
-        const double tz0 = FIDX(F.hsz, i, j, kc - 1) * FIDX(F.kurv, i, j, kc - 1) / FIDX(F.rho, i, j, kc - 1);
-        const double dhsdz = (tz1 + tz0) * 0.5;
+        const R rhoz = (RLD(F.rho, i, j, kc) + RLD(F.rho, i, j, kc - 1)) * R(0.5);
+        const R tz1 = RLD(F.hsz, i, j, kc) * RLD(F.kurv, i, j, kc) / RLD(F.rho, i, j, kc);
+        const R tz0 = RLD(F.hsz, i, j, kc - 1) * RLD(F.kurv, i, j, kc - 1) / RLD(F.rho, i, j, kc - 1);
+        const R dhsdz = (tz1 + tz0) * R(0.5);
         const int ip = clampi(i + 1, 2, nx), im = clampi(i, 2, nx);
-        const double amd_p = ((FIDX(F.znut, ip, j, k) + FIDX(F.znut, ip - 1, j, k)) * 0.5) * idx;
-        const double amd_m = ((FIDX(F.znut, im, j, k) + FIDX(F.znut, im - 1, j, k)) * 0.5) * idx;
+        const R amd_p = ((RLD(F.znut, ip, j, k) + RLD(F.znut, ip - 1, j, k)) * R(0.5)) * idx;
+        const R amd_m = ((RLD(F.znut, im, j, k) + RLD(F.znut, im - 1, j, k)) * R(0.5)) * idx;
         const int jp = clampi(j + 1, 2, ny), jm = clampi(j, 2, ny);
-        const double bmd_p = ((FIDX(F.znut, i, jp, k) + FIDX(F.znut, i, jp - 1, k)) * 0.5) * idy;
-        const double bmd_m = ((FIDX(F.znut, i, jm, k) + FIDX(F.znut, i, jm - 1, k)) * 0.5) * idy;
-        const double dmd_k = FIDX(F.nut, i, j, clampi(k, 1, nz)) * idz;
-        const double dmd_m = FIDX(F.nut, i, j, clampi(k - 1, 1, nz)) * idz;
-        const double Gv = amd_p * ((FIDX(w, i + 1, j, k) - wc) * idx + (FIDX(u, i + 1, j, k) - FIDX(u, i + 1, j, k - 1)) * idz) -
-                          amd_m * ((wc - FIDX(w, i - 1, j, k)) * idx + (FIDX(u, i, j, k) - FIDX(u, i, j, k - 1)) * idz) +
-                          bmd_p * ((FIDX(w, i, j + 1, k) - wc) * idy + (FIDX(v, i, j + 1, k) - FIDX(v, i, j + 1, k - 1)) * idz) -
-                          bmd_m * ((wc - FIDX(w, i, j - 1, k)) * idy + (FIDX(v, i, j, k) - FIDX(v, i, j, k - 1)) * idz) +
-                          (dmd_k * 2. * (FIDX(w, i, j, k + 1) - wc) - dmd_m * 2. * (wc - FIDX(w, i, j, k - 1))) * idz;
-        double r = -wint + Gv / rhoz - C.gz - C.sigma * dhsdz;
-        if (C.tf) r = r + FIDX(F.tfw, i, j, k);
-        if (on_cap(C, j, k, ny)) { const double b = FIDX(F.wb, i, j, k); r = r - C.cz * sqrt(b * b) * wc; }
-        FIDX(F.Fw, i, j, k) = r;
+        const R bmd_p = ((RLD(F.znut, i, jp, k) + RLD(F.znut, i, jp - 1, k)) * R(0.5)) * idy;
+        const R bmd_m = ((RLD(F.znut, i, jm, k) + RLD(F.znut, i, jm - 1, k)) * R(0.5)) * idy;
+        const R dmd_k = RLD(F.nut, i, j, clampi(k, 1, nz)) * idz;
+        const R dmd_m = RLD(F.nut, i, j, clampi(k - 1, 1, nz)) * idz;
+        const R Gv = amd_p * ((RLD(w, i + 1, j, k) - wc) * idx + (RLD(u, i + 1, j, k) - RLD(u, i + 1, j, k - 1)) * idz) -
+                          amd_m * ((wc - RLD(w, i - 1, j, k)) * idx + (RLD(u, i, j, k) - RLD(u, i, j, k - 1)) * idz) +
+                          bmd_p * ((RLD(w, i, j + 1, k) - wc) * idy + (RLD(v, i, j + 1, k) - RLD(v, i, j + 1, k - 1)) * idz) -
+                          bmd_m * ((wc - RLD(w, i, j - 1, k)) * idy + (RLD(v, i, j, k) - RLD(v, i, j, k - 1)) * idz) +
+                          (dmd_k * R(2.) * (RLD(w, i, j, k + 1) - wc) - dmd_m * R(2.) * (wc - RLD(w, i, j, k - 1))) * idz;
+        R r = -wint + Gv / rhoz - R(C.gz) - R(C.sigma) * dhsdz;
+        if (C.tf) r = r + RLD(F.tfw, i, j, k);
+        if (on_cap(C, j, k, ny)) { const R b = RLD(F.wb, i, j, k); r = r - R(C.cz) * sqrt(b * b) * wc; }
+        FIDX(F.Fw, i, j, k) = (double)r;
     }
 }
 
@@ -949,10 +965,18 @@ static LsConst ls_const(const suli_ctx* c) {
 static dim3 cells_grid(const Geo& g) { return grid3(g.nx, g.ny, g.nz, kBlk); }
 static dim3 faces_grid(const Geo& g) { return grid3(g.nx + 1, g.ny + 1, g.nz + 1, kBlk); }
 
+// stencil arithmetic in FP32 for the mixed-precision path (precision 1), FP64 otherwise; the
+// fields stay FP64 either way
+#define LAUNCH_R(kern, grid, block, ...)                                                   \
+    do {                                                                                   \
+        if (c->P.precision == 1) kern<float><<<(grid), (block), 0, c->stream>>>(__VA_ARGS__);  \
+        else kern<double><<<(grid), (block), 0, c->stream>>>(__VA_ARGS__);                 \
+    } while (0)
+
 void launch_lsprops(suli_ctx* c, const double* ls, bool do_mod, bool do_hs, bool do_vol) {
     const Geo& G = c->g;
     ProfScope ps(c, SULI_K_LSPROPS, 1);
-    k_lsprops<<<cells_grid(G), kBlk, 0, c->stream>>>(
+    LAUNCH_R(k_lsprops, cells_grid(G), kBlk,
         G, ls_const(c), ls, c->f[SULI_F_MOD_LS], c->nrmx, c->nrmy, c->nrmz, c->f[SULI_F_HS], c->f[SULI_F_HSX],
         c->f[SULI_F_HSY], c->f[SULI_F_HSZ], c->f[SULI_F_RHO], c->f[SULI_F_LS_NU], do_mod, do_hs, do_vol,
         c->red_partial, c->red_counter, c->red_out);
@@ -960,24 +984,24 @@ void launch_lsprops(suli_ctx* c, const double* ls, bool do_mod, bool do_hs, bool
 void launch_curv(suli_ctx* c) {
     const Geo& G = c->g;
     ProfScope ps(c, SULI_K_CURV, 1);
-    k_curv<<<cells_grid(G), kBlk, 0, c->stream>>>(G, ls_const(c), c->nrmx, c->nrmy, c->nrmz, c->f[SULI_F_DDLSDX],
+    LAUNCH_R(k_curv, cells_grid(G), kBlk, G, ls_const(c), c->nrmx, c->nrmy, c->nrmz, c->f[SULI_F_DDLSDX],
                                                    c->f[SULI_F_DDLSDY], c->f[SULI_F_DDLSDZ], c->f[SULI_F_KURV]);
 }
 void launch_ls_advect(suli_ctx* c, const double* cur, const double* phi0, double* out, double a, double b, double gd) {
     const Geo& G = c->g;
     ProfScope ps(c, SULI_K_LS_ADVECT, 1);
-    k_ls_advect<<<cells_grid(G), kBlk, 0, c->stream>>>(G, ls_const(c), cur, phi0, out, c->f[SULI_F_U], c->f[SULI_F_V],
+    LAUNCH_R(k_ls_advect, cells_grid(G), kBlk, G, ls_const(c), cur, phi0, out, c->f[SULI_F_U], c->f[SULI_F_V],
                                                         c->f[SULI_F_W], a, b, gd);
 }
 void launch_reinit_funcs(suli_ctx* c) {
     const Geo& G = c->g;
     ProfScope ps(c, SULI_K_REINIT, 1);
-    k_reinit_funcs<<<cells_grid(G), kBlk, 0, c->stream>>>(G, ls_const(c), c->f[SULI_F_LS], c->funcs);
+    LAUNCH_R(k_reinit_funcs, cells_grid(G), kBlk, G, ls_const(c), c->f[SULI_F_LS], c->funcs);
 }
 void launch_reinit_stage(suli_ctx* c, const double* cur, const double* phi0, double* out, double a, double b, double gd) {
     const Geo& G = c->g;
     ProfScope ps(c, SULI_K_REINIT, 1);
-    k_reinit_stage<<<cells_grid(G), kBlk, 0, c->stream>>>(G, ls_const(c), cur, phi0, out, c->funcs, a, b, gd);
+    LAUNCH_R(k_reinit_stage, cells_grid(G), kBlk, G, ls_const(c), cur, phi0, out, c->funcs, a, b, gd);
 }
 void launch_reinit_err(suli_ctx* c, const double* after, const double* before, double band) {
     const Geo& G = c->g;
@@ -997,8 +1021,12 @@ void launch_visco(suli_ctx* c) {
         ViscConst V;
         V.dx = c->P.dx; V.dy = c->P.dy; V.dz = c->P.dz; V.csmag = c->P.csmag;
         V.cdel = pow(c->P.dx * c->P.dy * c->P.dz, 2. / 3.);
-        k_nut<<<cells_grid(G), kBlk, 0, c->stream>>>(G, V, c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W],
-                                                      c->f[SULI_F_RHO], c->f[SULI_F_NUT]);
+        if (c->P.precision == 1)   // FP32 arithmetic over the FP64 state
+            k_nut<float><<<cells_grid(G), kBlk, 0, c->stream>>>(G, V, c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W],
+                                                               c->f[SULI_F_RHO], c->f[SULI_F_NUT]);
+        else
+            k_nut<double><<<cells_grid(G), kBlk, 0, c->stream>>>(G, V, c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W],
+                                                                c->f[SULI_F_RHO], c->f[SULI_F_NUT]);
     }
     k_facenu<<<faces_grid(G), kBlk, 0, c->stream>>>(G, c->P.m_turb, c->f[SULI_F_LS_NU], c->f[SULI_F_NUT],
                                                      c->f[SULI_F_XNUT], c->f[SULI_F_YNUT], c->f[SULI_F_ZNUT]);
@@ -1020,7 +1048,10 @@ void launch_convdiff(suli_ctx* c) {
     F.Fu = c->f[SULI_F_FU]; F.Fv = c->f[SULI_F_FV]; F.Fw = c->f[SULI_F_FW];
     ProfScope ps(c, SULI_K_CONVDIFF, 1);
     cudaMemcpyAsync(c->f[SULI_F_PRD0], c->f[SULI_F_PRD1], G.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
-    k_convdiff<<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F);
+    if (c->P.precision == 1)   // FP32 arithmetic over the FP64 state
+        k_convdiff<float><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F);
+    else
+        k_convdiff<double><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F);
 }
 void launch_tempo(suli_ctx* c, int tt, int it) {
     const Geo& G = c->g;

@@ -1,6 +1,6 @@
-"""GPU tests of the mixed-precision pressure solve (precision = 1): FP32 multigrid-
-preconditioned CG inside FP64 iterative refinement, stopping on the same FP64 relative
-residual as the plain path.  Each result is checked against the FP64 CPU oracle solved to a
+"""GPU tests of the mixed-precision path (precision = 1): FP32 stencil arithmetic over the FP64
+fields, and the pressure solve as FP32 multigrid-preconditioned CG inside FP64 iterative
+refinement, stopping on the same FP64 relative residual as the plain path.  Each result is checked against the FP64 CPU oracle solved to a
 tighter tolerance; the error bars are stated per test."""
 import numpy as np
 import pytest
@@ -49,8 +49,10 @@ def test_mixed_poisson_reaches_fp64_tolerance(pkg, orc, shape):
 
 
 def test_mixed_steps_track_fp64(pkg, orc):
-    """Three dam-break steps with the mixed solve at 1e-10 against the FP64 oracle at 1e-12:
-    every field within 1e-6 relative (the difference is the solve tolerance, propagated)."""
+    """Three dam-break steps of the mixed path (FP32 stencil arithmetic, FP32 inner solves,
+    FP64 refinement to 1e-10) against the FP64 oracle at 1e-12: every field within 1e-6 of its
+    own scale, the velocity components within 1e-6 of the velocity scale (v, across the tank,
+    is about 1e-6 of u in this nearly two-dimensional flow, so its own maximum is no scale)."""
     p, init = pkg.cases.dam_break(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-12)
     q = p.copy()
     q.precision, q.cg_tol, q.inner_tol, q.refine_maxit = 1, 1e-10, 1e-3, 30
@@ -62,7 +64,11 @@ def test_mixed_steps_track_fp64(pkg, orc):
         sg, so = g.step(it), o.step(it)
         assert sg["status"] == 0
         assert max(sg["cg_resid"]) <= 1e-10
-    for f in ("u", "v", "w", "ls", "rho"):
+    vel = {f: (g.download(f), o.download(f)) for f in ("u", "v", "w")}
+    vs = max(float(np.abs(b).max()) for _, b in vel.values())
+    for f, (a, b) in vel.items():
+        assert float(np.abs(a - b).max()) <= 1e-6 * vs, f
+    for f in ("ls", "rho"):
         assert rel_err(g.download(f), o.download(f)) <= 1e-6, f
 
 
