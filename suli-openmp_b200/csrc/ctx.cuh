@@ -128,8 +128,10 @@ struct suli_ctx {
     int inner_batch = 4;
     int last_outer_iters = 0;
     // one CUDA graph per ping-pong parity holding a whole inner PCG iteration
-    cudaGraphExec_t pcg_graph[2] = {nullptr, nullptr};
-    int pcg_graph_kernels = 0;
+    // the inner PCG loop as one graph: a WHILE node repeats two iterations (ping-pong) and a
+    // kernel that clears the condition once the inner solve is done
+    cudaGraphExec_t pcg_loop = nullptr;
+    int pcg_graph_kernels = 0;   // kernels of one inner iteration
     // learned initial guess (suli_attach_nn) and training-pair recording (suli_graddin_record)
     suli_nn* nn = nullptr;
     int nn_mode = 0;
@@ -220,6 +222,8 @@ void launch_cg_final(suli_ctx* c, const double* e);
 void launch_mx_setup(suli_ctx* c);
 void launch_mx_residual(suli_ctx* c, const double* e_in, double* e_out, bool apply);
 void launch_pcg_init(suli_ctx* c, int maxit);
+// the loop condition of the inner-solve graph: non-zero while the inner solve is not done
+void launch_pcg_cond(suli_ctx* c, cudaGraphConditionalHandle h);
 void launch_vcycle(suli_ctx* c);
 // ---- learned initial guess (k_learned.cu) ----
 void launch_nn_features(suli_ctx* c, float* in3);

@@ -515,6 +515,10 @@ __global__ void k_pcg_init(PCGState* st, double inner_tol, int maxit) {
     st->rz = 0.;
 }
 
+__global__ void k_pcg_cond(cudaGraphConditionalHandle h, const PCGState* st) {
+    cudaGraphSetConditional(h, st->done ? 0u : 1u);
+}
+
 __global__ void k_zero_f(float* a, long long n) {
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q < n) a[q] = 0.f;
@@ -550,6 +554,8 @@ void launch_mx_residual(suli_ctx* c, const double* e_in, double* e_out, bool app
                                                  c->cg_b, e_out, c->pc_r, apply ? 1 : 0, c->cg, c->pcg,
                                                  c->red_partial, c->red_counter);
 }
+
+void launch_pcg_cond(suli_ctx* c, cudaGraphConditionalHandle h) { k_pcg_cond<<<1, 1, 0, c->stream>>>(h, c->pcg); }
 
 void launch_pcg_init(suli_ctx* c, int maxit) {
     k_pcg_init<<<1, 1, 0, c->stream>>>(c->pcg, c->P.inner_tol, maxit);

@@ -6,6 +6,7 @@
 // Poisson stopping test) is decided from device-resident scalars; the host reads them back
 // only where the reference branches on them.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -278,8 +279,7 @@ int suli_destroy(suli_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->cg_graph) cudaGraphExecDestroy(c->cg_graph);
-    for (auto& g : c->pcg_graph)
-        if (g) cudaGraphExecDestroy(g);
+    if (c->pcg_loop) cudaGraphExecDestroy(c->pcg_loop);
     for (auto& e : c->prof.ev) cudaEventDestroy(e);
     cudaFree(c->arena);
     for (int f = SULI_F_BXX0; f < SULI_F_COUNT; ++f) cudaFree(c->f[f]);
@@ -607,22 +607,40 @@ int run_batches(suli_ctx* c, const State* dev, State* host2, long long cap, int 
     return SULI_OK;
 }
 
-// Capture one inner PCG iteration (SpMV, update, V-cycle: every kernel reads its scalars from
-// device memory, so the launch parameters never change) into a graph per ping-pong parity.
-int ensure_pcg_graphs(suli_ctx* c) {
-    if (c->pcg_graph[0] && c->pcg_graph[1]) return SULI_OK;
-    for (int par = 0; par < 2; ++par) {
-        cudaGraph_t g = nullptr;
-        CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        if (par == 0) launch_pcg_iter(c, c->pc_pa, c->pc_pb);
-        else launch_pcg_iter(c, c->pc_pb, c->pc_pa);
-        CUDA_TRY(c, cudaStreamEndCapture(c->stream, &g));
-        const cudaError_t e = cudaGraphInstantiate(&c->pcg_graph[par], g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) return fail(c, SULI_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+// The inner PCG loop as one graph launch: a WHILE conditional node whose body is two inner
+// iterations (p ping-pongs between pa and pb; every kernel reads its scalars from device
+// memory, so the captured parameters never change) and k_pcg_cond, which clears the condition
+// once the inner solve has converged or hit its cap.  The GPU iterates without host round trips,
+// and no iteration is launched after convergence except the rest of the last body (kernels that
+// return at once).
+int ensure_pcg_loop(suli_ctx* c) {
+    if (c->pcg_loop) return SULI_OK;
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(c, cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+    if (e == cudaSuccess)
+        e = cudaStreamBeginCaptureToGraph(c->stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        launch_pcg_iter(c, c->pc_pa, c->pc_pb);
+        launch_pcg_iter(c, c->pc_pb, c->pc_pa);
+        launch_pcg_cond(c, h);
+        cudaGraph_t body = nullptr;
+        e = cudaStreamEndCapture(c->stream, &body);
     }
-    const int L = (int)c->mg.size();
-    (void)L;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&c->pcg_loop, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, SULI_ERR_CUDA, std::string("inner-solve graph: ") + cudaGetErrorString(e));
+    }
     c->pcg_graph_kernels = 2 + vcycle_kernels(c);
     return SULI_OK;
 }
@@ -660,7 +678,7 @@ void nn_begin(suli_ctx* c) {
 }
 
 int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
-    if (int rg = ensure_pcg_graphs(c)) return rg;
+    if (int rg = ensure_pcg_loop(c)) return rg;
     launch_cg_setup(c);   // FP64 diagonal, coefficients, b~, first residual and threshold
     launch_mx_setup(c);   // FP32 faces of every multigrid level
     nn_begin(c);
@@ -683,15 +701,16 @@ int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
             launch_vcycle(c);
         }
         launch_pcg_iter(c, c->mg[0].y, c->pc_pa);   // p_old = z with beta = 0
-        r = run_batches(c, c->pcg, c->pcg_host, (long long)c->inner_maxit + 2, c->inner_batch, [&](int parity) {
-            ProfScope ps(c, SULI_K_MG, c->pcg_graph_kernels);
-            cudaGraphLaunch(c->pcg_graph[parity], c->stream);
-        });
-        if (r != SULI_OK) return r;
+        {
+            ProfScope ps(c, SULI_K_MG, 0);   // kernel launches are counted below, once known
+            CUDA_TRY(c, cudaGraphLaunch(c->pcg_loop, c->stream));
+        }
         r = sync_read(c, c->pcg, c->pcg_host, sizeof(PCGState));
         if (r != SULI_OK) return r;
         if (c->pcg_host[0].status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the inner solve");
         inner_total += c->pcg_host[0].iters;
+        const long long bodies = std::max(1, (c->pcg_host[0].iters - 1 + 1) / 2);
+        c->prof.launches[SULI_K_MG] += bodies * (2LL * c->pcg_graph_kernels + 1);
         launch_mx_residual(c, ecur, enext, true);
         std::swap(ecur, enext);
         CHECK_LAUNCH(c);
