@@ -205,8 +205,9 @@ int suli_nn_train_step(suli_nn* n, const float* d_in3, const float* d_target, fl
    (tap = dx + 3 dy + 9 dz), bias [cout] FP32 or NULL, out [V][cout] BF16 = relu?(conv(x) + b) */
 int suli_nn_conv3d(int nx, int ny, int nz, const void* x, int cin, const void* w, const float* bias, int cout,
                    int relu, void* out, int kernel);
-/* convolution kernel of a network (and of suli_nn_conv3d's last argument): 0 = tcgen05 tensor
-   cores with the accumulator in TMEM (default), 1 = mma.sync tensor cores */
+/* convolution kernel of a network (and of suli_nn_conv3d's last argument): 0 = persistent
+   tcgen05 pipeline (TMA loads, accumulators in TMEM; default), 1 = mma.sync tensor cores,
+   2 = tcgen05 with one output tile per CTA */
 int suli_nn_set_kernel(suli_nn* n, int kernel);
 
 /* Attach a network to a context (same grid and device) for its pressure solves.

@@ -8,6 +8,8 @@
 // The network maps (residual r~0/s, density feature, previous pressure e0/s) to the scaled
 // correction (e* - e0)/s of the pressure solve, so it is both an initial guess
 // (e0 <- e0 + s net(.)) and an approximate inverse of A~ applied to a residual.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <algorithm>
@@ -19,6 +21,7 @@
 #include "nn_api.cuh"
 #include "nn_conv.cuh"
 #include "nn_tc.cuh"
+#include "nn_tp.cuh"
 
 namespace suli {
 namespace nn {
@@ -323,7 +326,7 @@ struct suli_nn {
     double* sums = nullptr;
     double* host_sums = nullptr;
     int* err_flag = nullptr;         // set by a tensor-core convolution whose wait timed out
-    int kernel = 0;                  // convolution kernel: 0 tcgen05, 1 mma.sync
+    int kernel = 0;                  // convolution kernel: 0 tcgen05 pipeline, 1 mma.sync, 2 tcgen05 one tile per CTA
     std::string err;
 };
 
@@ -359,18 +362,135 @@ void conv_tc_nz(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat1
 }
 
 // z-planes per CTA: as many as keep the CTA's accumulators within 128 TMEM columns
-void conv_tc(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu,
-             int cout, __nv_bfloat16* out) {
+int tc_cols(int cout) {
     int tcols = 32;
     while (tcols < cout) tcols *= 2;
+    return tcols;
+}
+void conv_tc(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu,
+             int cout, __nv_bfloat16* out) {
+    const int tcols = tc_cols(cout);
     if (tcols <= 32) conv_tc_nz<4>(N, vol, in, W, bias, relu, cout, tcols, out);
     else if (tcols <= 64) conv_tc_nz<2>(N, vol, in, W, bias, relu, cout, tcols, out);
     else conv_tc_nz<1>(N, vol, in, W, bias, relu, cout, tcols, out);
 }
 
+// ---- the pipelined tcgen05 convolution (nn_tp.cuh): TMA descriptors and launch shape
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+// channels-last volume [nz][ny][nx][C]; box {8 channels, hx, hy, hz}, zero fill outside
+bool map_volume(CUtensorMap* m, const __nv_bfloat16* p, int C, const Vol& v, int hx, int hy, int hz) {
+    auto enc = tensor_map_encoder();
+    if (!enc || !p || (reinterpret_cast<uintptr_t>(p) & 15) || C % 8) return false;
+    cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)v.nx, (cuuint64_t)v.ny, (cuuint64_t)v.nz};
+    cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)C * 2 * v.nx, (cuuint64_t)C * 2 * v.nx * v.ny};
+    cuuint32_t box[4] = {8, (cuuint32_t)hx, (cuuint32_t)hy, (cuuint32_t)hz};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(p), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+// weights [27][cout][cin]; box {8 input channels, cout, 27 taps}
+bool map_weights(CUtensorMap* m, const __nv_bfloat16* W, int cin, int cout) {
+    auto enc = tensor_map_encoder();
+    if (!enc || (reinterpret_cast<uintptr_t>(W) & 15) || cout > 256) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)cin, (cuuint64_t)cout, 27};
+    cuuint64_t strides[2] = {(cuuint64_t)cin * 2, (cuuint64_t)cin * cout * 2};
+    cuuint32_t box[3] = {8, (cuuint32_t)cout, 27};
+    cuuint32_t es[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(W), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+int sm_count(int device) {
+    static int n[64] = {0};
+    if (device < 0 || device >= 64) return 148;
+    if (!n[device] && cudaDeviceGetAttribute(&n[device], cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        n[device] = 148;
+    }
+    return n[device];
+}
+constexpr int kTpSmemMax = 227 * 1024;
+
+// false: this shape is not supported by the pipeline (the caller uses k_conv3_tc)
+template <int NZ, bool FOLD>
+bool conv_tp_nz(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu,
+                int cout, int tcols, __nv_bfloat16* out) {
+    using G = TpGeo<FOLD>;
+    const int cin = in.ca + in.cb;
+    if (in.ca % TC_CC || in.cb % TC_CC || 2 * NZ * tcols > 512 || cout > 256) return false;
+    TpCfg cfg{};
+    cfg.cout = cout;
+    cfg.tcols = tcols;
+    cfg.nchunks = cin / TC_CC;
+    cfg.ca = in.ca;
+    cfg.a_tma = in.a_half ? 0 : 1;
+    cfg.relu = relu;
+    cfg.kc_bytes = (G::HXR * G::HYR * 16 * (NZ + 2) + 127) / 128 * 128;
+    cfg.wchunk_bytes = 27 * cout * TC_CC * 2;
+    const int wall = cfg.nchunks * cfg.wchunk_bytes;
+    const int budget = kTpSmemMax - TP_TAIL_BYTES;
+    // the layer's weights stay resident when three halo slots still fit beside them
+    cfg.w_resident = (wall + 3 * (2 * cfg.kc_bytes) <= budget) ? 1 : 0;
+    cfg.w_bytes = cfg.w_resident ? wall : 0;
+    cfg.stage_bytes = 2 * cfg.kc_bytes + (cfg.w_resident ? 0 : cfg.wchunk_bytes);
+    cfg.stages = std::min(TP_MAX_STAGES, (budget - cfg.w_bytes) / cfg.stage_bytes);
+    if (cfg.stages < 1) return false;
+    cfg.tiles_x = (vol.nx + G::OX - 1) / G::OX;
+    cfg.tiles_y = (vol.ny + G::OY - 1) / G::OY;
+    const long long tiles = (long long)cfg.tiles_x * cfg.tiles_y * ((vol.nz + NZ - 1) / NZ);
+    if (tiles > (1LL << 30)) return false;
+    cfg.tiles = (int)tiles;
+    CUtensorMap ma, mb, mw;
+    if (!map_weights(&mw, W, cin, cout)) return false;
+    if (in.cb > 0 && !map_volume(&mb, in.b, in.cb, vol, G::HXR, G::HYR, NZ + 2)) return false;
+    if (cfg.a_tma) {
+        if (!map_volume(&ma, in.a, in.ca, vol, G::HXR, G::HYR, NZ + 2)) return false;
+    } else if (reinterpret_cast<uintptr_t>(in.a) & 15) {
+        return false;   // 16-byte cp.async sources
+    }
+    if (in.cb == 0) mb = mw;      // not read
+    if (!cfg.a_tma) ma = mw;      // not read
+    const size_t smem = (size_t)(cfg.w_bytes + cfg.stages * cfg.stage_bytes + TP_TAIL_BYTES);
+    static bool attr_done[64] = {false};
+    if (!attr_done[N->device]) {
+        cudaFuncSetAttribute(k_conv3_tp<NZ, FOLD>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTpSmemMax);
+        attr_done[N->device] = true;
+    }
+    const int grid = (int)std::min<long long>(tiles, sm_count(N->device));
+    k_conv3_tp<NZ, FOLD><<<grid, TP_THREADS, smem, N->stream>>>(vol, in, ma, mb, mw, bias, cfg, out, N->err_flag);
+    return true;
+}
+
+// Cout 16 and 32 fold the x taps into N (N = 48 -> 64 TMEM columns a plane, 4 planes; N = 96 ->
+// 128 columns, 2 planes); wider layers use the 8 x 16 tile.  Two accumulator sets <= 512 columns.
+bool conv_tp(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu,
+             int cout, __nv_bfloat16* out) {
+    if (cout == 16) return conv_tp_nz<4, true>(N, vol, in, W, bias, relu, cout, 64, out);
+    if (cout == 32) return conv_tp_nz<2, true>(N, vol, in, W, bias, relu, cout, 128, out);
+    const int tcols = tc_cols(cout);
+    if (tcols <= 64) return conv_tp_nz<2, false>(N, vol, in, W, bias, relu, cout, tcols, out);
+    return conv_tp_nz<1, false>(N, vol, in, W, bias, relu, cout, tcols, out);
+}
+
 void conv(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu, int cout,
           __nv_bfloat16* out) {
-    if (N->kernel == 0) {
+    if (N->kernel == 0 && conv_tp(N, vol, in, W, bias, relu, cout, out)) return;
+    if (N->kernel == 0 || N->kernel == 2) {
         conv_tc(N, vol, in, W, bias, relu, cout, out);
         return;
     }
@@ -678,7 +798,7 @@ int suli_nn_train_step(suli_nn* N, const float* d_in3, const float* d_target, fl
 }
 
 int suli_nn_set_kernel(suli_nn* N, int kernel) {
-    if (!N || kernel < 0 || kernel > 1) return SULI_ERR_ARG;
+    if (!N || kernel < 0 || kernel > 2) return SULI_ERR_ARG;
     N->kernel = kernel;
     return SULI_OK;
 }
@@ -687,7 +807,7 @@ int suli_nn_set_kernel(suli_nn* N, int kernel) {
 int suli_nn_conv3d(int nx, int ny, int nz, const void* x, int cin, const void* w, const float* bias, int cout,
                    int relu, void* out, int kernel) {
     if (!x || !w || !out || cin % 16 || cout % 8 || nx < 1 || ny < 1 || nz < 1) return SULI_ERR_ARG;
-    if (kernel < 0 || kernel > 1) return SULI_ERR_ARG;
+    if (kernel < 0 || kernel > 2) return SULI_ERR_ARG;
     if (cout != 16 && cout != 32 && cout != 48 && cout != 64 && cout != 96 && cout != 160) return SULI_ERR_UNSUPPORTED;
     if (cin > 160) return SULI_ERR_SIZE;
     suli_nn tmp;

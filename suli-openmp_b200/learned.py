@@ -136,7 +136,8 @@ class Net:
         return loss.value, g
 
     def set_kernel(self, kernel: int) -> None:
-        """Convolution kernel: 0 = tcgen05 (accumulator in TMEM, the default), 1 = mma.sync."""
+        """Convolution kernel: 0 = the pipelined tcgen05 kernel (TMA loads, accumulators in TMEM,
+        the default), 1 = mma.sync, 2 = tcgen05 with one tile per CTA."""
         self._check(self.lib.suli_nn_set_kernel(self._h, int(kernel)), "set_kernel")
 
     def train_step(self, in3, target, lr: float) -> float:
@@ -150,7 +151,7 @@ class Net:
 def conv3d(x, w, bias, out, shape, cin: int, cout: int, relu: bool = False, kernel: int = 0,
            lib_path=None) -> None:
     """The convolution primitive on device buffers (channels-last BF16, see suli_nn_conv3d);
-    kernel 0 = tcgen05, 1 = mma.sync."""
+    kernel 0 = pipelined tcgen05, 1 = mma.sync, 2 = tcgen05 one tile per CTA."""
     lib = _abi.load_library(lib_path)
     nx, ny, nz = shape
     rc = lib.suli_nn_conv3d(int(nx), int(ny), int(nz), C.c_void_p(_ptr(x)), int(cin), C.c_void_p(_ptr(w)),

@@ -1,7 +1,9 @@
 """GPU: the network kernels (csrc/nn.cu, nn_conv.cuh) against references.
 
-* both tensor-core convolutions (tcgen05 with the accumulator in TMEM, and mma.sync) against
-  an FP64 convolution of the same BF16 inputs;
+* the three tensor-core convolutions (the persistent tcgen05 pipeline with TMA loads, tcgen05
+  with one tile per CTA, and mma.sync) against an FP64 convolution of the same BF16 inputs,
+  including the decoder's input (half-resolution tensor upsampled and concatenated with a
+  full-resolution skip);
 * forward, loss and parameter gradient of the whole U-Net against the FP64 oracle
   (oracle/unet_ref.py, itself pinned by finite differences), with the conv weights and the
   input rounded to BF16 as the GPU reads them.  The GPU keeps activations and activation
@@ -28,7 +30,7 @@ def _bf16(torch, a):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(torch.bfloat16)
 
 
-@pytest.mark.parametrize("kernel", [0, 1], ids=["tcgen05", "mma_sync"])
+@pytest.mark.parametrize("kernel", [0, 1, 2], ids=["tcgen05_pipe", "mma_sync", "tcgen05_tile"])
 @pytest.mark.parametrize("shape,cin,cout,relu", [
     ((12, 10, 9), 16, 16, True),
     ((8, 8, 8), 32, 48, False),
@@ -59,6 +61,60 @@ def test_conv3d_matches_fp64(pkg, torch, shape, cin, cout, relu, kernel):
     # BF16 rounding of the output (<= 2^-9 relative) plus FP32 accumulation order
     tol = 2.0 ** -8 * ref.abs() + 1e-5 * ref.abs().max()
     assert bool((err <= tol).all()), float((err - tol).max())
+
+
+@pytest.mark.parametrize("shape,cin,cout", [
+    ((64, 64, 64), 16, 16),      # 512+ tiles: several per CTA, resident weights, x taps folded into N
+    ((128, 64, 48), 32, 32),     # the ring of halo slots wraps around
+    ((64, 64, 32), 96, 32),      # six chunks per tile
+    ((40, 48, 22), 32, 64),      # 8 x 16 tiles, two planes per tile, ragged in every direction
+    ((24, 32, 13), 64, 96),      # weights streamed with each chunk, one plane per tile
+    ((16, 16, 9), 64, 160),      # the widest input-gradient shape: 512 TMEM columns, one slot
+])
+def test_pipeline_kernel_at_scale(pkg, torch, shape, cin, cout):
+    """The pipelined kernel where every CTA walks many tiles, against an FP64 convolution of the
+    same BF16 inputs (BF16 output rounding).  Where it keeps the one-tile kernel's 8 x 16 tile
+    (Cout >= 48) it issues the same MMAs in the same order, so the two agree bit for bit."""
+    nx, ny, nz = shape
+    g = torch.Generator(device="cuda:0").manual_seed(cin + cout)
+    x = torch.randn((nz, ny, nx, cin), generator=g, device="cuda:0").to(torch.bfloat16)
+    w = (torch.randn((27, cout, cin), generator=g, device="cuda:0") / (27 * cin) ** 0.5).to(torch.bfloat16)
+    b = torch.randn(cout, generator=g, device="cuda:0")
+    outs = []
+    for kernel in (0, 2):
+        out = torch.full((nz, ny, nx, cout), float("nan"), dtype=torch.bfloat16, device="cuda:0")
+        pkg.learned.conv3d(x, w, b, out, shape, cin, cout, True, kernel=kernel)
+        outs.append(out)
+    torch.cuda.synchronize()
+    xin = x.double().permute(3, 0, 1, 2).unsqueeze(0)
+    wt = w.double().reshape(3, 3, 3, cout, cin).permute(3, 4, 0, 1, 2)
+    ref = torch.nn.functional.conv3d(xin, wt, b.double(), padding=1)[0].permute(1, 2, 3, 0).clamp_min(0.0)
+    err = (outs[0].double() - ref).abs()
+    tol = 2.0 ** -8 * ref.abs() + 1e-5 * ref.abs().max()
+    assert bool((err <= tol).all()), float((err - tol).max())
+    if cout >= 48:
+        assert torch.equal(outs[0], outs[1])
+
+
+def test_network_forward_pipeline_matches_tile_kernel(pkg, torch):
+    """Whole network at 128 x 128 x 64 (many tiles per CTA on every level), including the
+    decoder's upsampled half-resolution inputs gathered with cp.async: the pipelined kernel and
+    the one-tile kernel agree to BF16 activation rounding (the folded layers sum the three x
+    taps in another order)."""
+    nx, ny, nz = 128, 128, 64
+    net = pkg.learned.Net.load(nx, ny, nz)
+    g = torch.Generator(device="cuda:0").manual_seed(3)
+    d_in = torch.randn(nx * ny * nz * 3, generator=g, device="cuda:0")
+    outs = []
+    for kernel in (0, 2):
+        net.set_kernel(kernel)
+        y = torch.empty(nx * ny * nz, device="cuda:0")
+        net.forward(d_in, y)
+        outs.append(y)
+    assert torch.isfinite(outs[0]).all() and outs[0].abs().max() > 0
+    rel = float((outs[0] - outs[1]).norm() / outs[1].norm())
+    assert rel < 1e-2, rel
+    net.close()
 
 
 def _setup(torch, n, seed):
@@ -96,7 +152,7 @@ def _layer_slices():
     return out
 
 
-@pytest.mark.parametrize("kernel", [0, 1], ids=["tcgen05", "mma_sync"])
+@pytest.mark.parametrize("kernel", [0, 1, 2], ids=["tcgen05_pipe", "mma_sync", "tcgen05_tile"])
 def test_forward_matches_oracle(pkg, torch, kernel):
     n = 16
     theta32, theta_ref, x3, x3_ref, _ = _setup(torch, n, 5)
@@ -117,7 +173,7 @@ def test_forward_matches_oracle(pkg, torch, kernel):
     net.close()
 
 
-@pytest.mark.parametrize("kernel", [0, 1], ids=["tcgen05", "mma_sync"])
+@pytest.mark.parametrize("kernel", [0, 1, 2], ids=["tcgen05_pipe", "mma_sync", "tcgen05_tile"])
 def test_loss_and_gradient_match_oracle(pkg, torch, kernel):
     n = 16
     theta32, theta_ref, x3, x3_ref, tgt = _setup(torch, n, 7)
