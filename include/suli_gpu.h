@@ -205,6 +205,12 @@ int suli_nn_train_step(suli_nn* n, const float* d_in3, const float* d_target, fl
    (tap = dx + 3 dy + 9 dz), bias [cout] FP32 or NULL, out [V][cout] BF16 = relu?(conv(x) + b) */
 int suli_nn_conv3d(int nx, int ny, int nz, const void* x, int cin, const void* w, const float* bias, int cout,
                    int relu, void* out, int kernel);
+/* as suli_nn_conv3d, plus what the network fuses into a convolution: pool_out (or NULL) gets the
+   2x2x2 average of the BF16 output [V/8][cout] BF16 (even grid); head_w (17 floats: 16 weights,
+   bias; cout = 16) and head_out [V] FP32 (or NULL) the 1x1x1 head of the BF16 output.  Kernel 0
+   computes them in the convolution's epilogue, kernels 1 and 2 with separate kernels. */
+int suli_nn_conv3d_ex(int nx, int ny, int nz, const void* x, int cin, const void* w, const float* bias, int cout,
+                      int relu, void* out, void* pool_out, const float* head_w, float* head_out, int kernel);
 /* convolution kernel of a network (and of suli_nn_conv3d's last argument): 0 = persistent
    tcgen05 pipeline (TMA loads, accumulators in TMEM; default), 1 = mma.sync tensor cores,
    2 = tcgen05 with one output tile per CTA */

@@ -227,6 +227,8 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
         "suli_nn_loss_grad": (C.c_int, [vp, vp, vp, P(C.c_double), P(C.c_float)]),
         "suli_nn_train_step": (C.c_int, [vp, vp, vp, C.c_float, P(C.c_double)]),
         "suli_nn_conv3d": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, C.c_int]),
+        "suli_nn_conv3d_ex": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp, vp,
+                                        vp, C.c_int]),
         "suli_nn_set_kernel": (C.c_int, [vp, C.c_int]),
         "suli_attach_nn": (C.c_int, [vp, vp, C.c_int]),
         "suli_graddin_record": (C.c_int, [vp, vp, vp, P(C.c_int), P(C.c_double)]),
@@ -250,7 +252,7 @@ HEADER_SYMBOLS = [
     "suli_est_static",
     "suli_nn_num_params", "suli_nn_create", "suli_nn_destroy", "suli_nn_last_error",
     "suli_nn_set_params", "suli_nn_get_params", "suli_nn_forward", "suli_nn_loss_grad",
-    "suli_nn_train_step", "suli_nn_conv3d", "suli_nn_set_kernel", "suli_attach_nn", "suli_graddin_record",
+    "suli_nn_train_step", "suli_nn_conv3d", "suli_nn_conv3d_ex", "suli_nn_set_kernel", "suli_attach_nn", "suli_graddin_record",
 ]
 EST_STATIC_MAX_BLOCKS = 8192   # SULI_EST_STATIC_MAX_BLOCKS
 

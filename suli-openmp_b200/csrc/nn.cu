@@ -429,10 +429,12 @@ constexpr int kTpSmemMax = 227 * 1024;
 // false: this shape is not supported by the pipeline (the caller uses k_conv3_tc)
 template <int NZ, bool FOLD>
 bool conv_tp_nz(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu,
-                int cout, int tcols, __nv_bfloat16* out) {
+                int cout, int tcols, __nv_bfloat16* out, const TpEpi& epi) {
     using G = TpGeo<FOLD>;
     const int cin = in.ca + in.cb;
     if (in.ca % TC_CC || in.cb % TC_CC || 2 * NZ * tcols > 512 || cout > 256) return false;
+    if (epi.pool && (NZ < 2 || vol.nx % 2 || vol.ny % 2 || vol.nz % 2)) return false;
+    if (epi.head_w && cout != 16) return false;
     TpCfg cfg{};
     cfg.cout = cout;
     cfg.tcols = tcols;
@@ -472,24 +474,24 @@ bool conv_tp_nz(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat1
         attr_done[N->device] = true;
     }
     const int grid = (int)std::min<long long>(tiles, sm_count(N->device));
-    k_conv3_tp<NZ, FOLD><<<grid, TP_THREADS, smem, N->stream>>>(vol, in, ma, mb, mw, bias, cfg, out, N->err_flag);
+    k_conv3_tp<NZ, FOLD><<<grid, TP_THREADS, smem, N->stream>>>(vol, in, ma, mb, mw, bias, cfg, epi, out, N->err_flag);
     return true;
 }
 
 // Cout 16 and 32 fold the x taps into N (N = 48 -> 64 TMEM columns a plane, 4 planes; N = 96 ->
 // 128 columns, 2 planes); wider layers use the 8 x 16 tile.  Two accumulator sets <= 512 columns.
 bool conv_tp(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu,
-             int cout, __nv_bfloat16* out) {
-    if (cout == 16) return conv_tp_nz<4, true>(N, vol, in, W, bias, relu, cout, 64, out);
-    if (cout == 32) return conv_tp_nz<2, true>(N, vol, in, W, bias, relu, cout, 128, out);
+             int cout, __nv_bfloat16* out, const TpEpi& epi) {
+    if (cout == 16) return conv_tp_nz<4, true>(N, vol, in, W, bias, relu, cout, 64, out, epi);
+    if (cout == 32) return conv_tp_nz<2, true>(N, vol, in, W, bias, relu, cout, 128, out, epi);
     const int tcols = tc_cols(cout);
-    if (tcols <= 64) return conv_tp_nz<2, false>(N, vol, in, W, bias, relu, cout, tcols, out);
-    return conv_tp_nz<1, false>(N, vol, in, W, bias, relu, cout, tcols, out);
+    if (tcols <= 64) return conv_tp_nz<2, false>(N, vol, in, W, bias, relu, cout, tcols, out, epi);
+    return conv_tp_nz<1, false>(N, vol, in, W, bias, relu, cout, tcols, out, epi);
 }
 
 void conv(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, const float* bias, int relu, int cout,
           __nv_bfloat16* out) {
-    if (N->kernel == 0 && conv_tp(N, vol, in, W, bias, relu, cout, out)) return;
+    if (N->kernel == 0 && conv_tp(N, vol, in, W, bias, relu, cout, out, TpEpi{nullptr, nullptr, nullptr, 1})) return;
     if (N->kernel == 0 || N->kernel == 2) {
         conv_tc(N, vol, in, W, bias, relu, cout, out);
         return;
@@ -551,18 +553,42 @@ ConvIn layer_input(suli_nn* N, int l) {
     return in;
 }
 
-// forward pass from N->in0; the head writes `out` [V] FP32
-void forward(suli_nn* N, float* out) {
+// forward pass from N->in0; the head writes `out` [V] FP32.  With the pipelined kernel the
+// pooling after each encoder level and the head run in the convolutions' epilogues (same
+// arithmetic and order as k_pool / k_head_fwd); `keep` = 0 (inference) also skips storing the last
+// layer's activation, which only the backward pass reads.  Returns the kernels launched.
+int forward(suli_nn* N, float* out, bool keep) {
+    int launches = 0;
+    bool head_done = false;
     for (int l = 0; l < kConv; ++l) {
         const LayerSpec& L = kLayer[l];
         const ConvIn in = layer_input(N, l);
-        conv(N, N->vol[L.level], in, N->wb + N->off[l], N->w + N->off[l] + 27LL * L.cout * L.cin, 1, L.cout, N->a[l]);
-        if (l == 1 || l == 3 || l == 5) {   // pooling after each encoder level but the last
-            const int lv = L.level;
+        const int lv = L.level;
+        const bool pools = (l == 1 || l == 3 || l == 5);   // pooling after each encoder level but the last
+        const __nv_bfloat16* W = N->wb + N->off[l];
+        const float* b = N->w + N->off[l] + 27LL * L.cout * L.cin;
+        TpEpi epi{pools ? N->pool[lv] : nullptr, nullptr, nullptr, 1};
+        if (l == kConv - 1) {
+            epi.head_w = N->w + N->off[kConv];
+            epi.head_out = out;
+            epi.store = keep ? 1 : 0;
+        }
+        ++launches;
+        if (N->kernel == 0 && conv_tp(N, N->vol[lv], in, W, b, 1, L.cout, N->a[l], epi)) {
+            if (l == kConv - 1) head_done = true;
+            continue;
+        }
+        conv(N, N->vol[lv], in, W, b, 1, L.cout, N->a[l]);
+        if (pools) {
             k_pool<<<nb(N->V[lv + 1] * L.cout), 256, 0, N->stream>>>(N->vol[lv], L.cout, N->a[l], N->pool[lv]);
+            ++launches;
         }
     }
-    k_head_fwd<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->a[13], N->w + N->off[kConv], out);
+    if (!head_done) {
+        k_head_fwd<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->a[13], N->w + N->off[kConv], out);
+        ++launches;
+    }
+    return launches;
 }
 
 // backward from N->dout; accumulates parameter gradients into N->g (zeroed by the caller)
@@ -638,14 +664,14 @@ void dims(const suli_nn* N, int* nx, int* ny, int* nz, int* device) {
     *nz = N->vol[0].nz;
     *device = N->device;
 }
-void forward_on(suli_nn* N, cudaStream_t stream, const float* d_in3, float* d_out) {
+int forward_on(suli_nn* N, cudaStream_t stream, const float* d_in3, float* d_out) {
     const cudaStream_t own = N->stream;
     N->stream = stream;
     k_pack_input<<<nb(N->V[0]), 256, 0, stream>>>(N->V[0], d_in3, N->in0);
-    forward(N, d_out);
+    const int n = 1 + forward(N, d_out, false);
     N->stream = own;
+    return n;
 }
-int forward_launches() { return 1 + kConv + (kLevels - 1) + 1; }
 int take_error(suli_nn* N) {
     int flag = 0;
     if (cudaMemcpy(&flag, N->err_flag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
@@ -764,7 +790,7 @@ int suli_nn_forward(suli_nn* N, const float* d_in3, float* d_out) {
     if (!N || !d_in3 || !d_out) return SULI_ERR_ARG;
     cudaSetDevice(N->device);
     k_pack_input<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], d_in3, N->in0);
-    forward(N, d_out);
+    forward(N, d_out, false);
     return nn_sync(N);
 }
 
@@ -773,7 +799,7 @@ int suli_nn_loss_grad(suli_nn* N, const float* d_in3, const float* d_target, dou
     if (!N || !d_in3 || !d_target) return SULI_ERR_ARG;
     cudaSetDevice(N->device);
     k_pack_input<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], d_in3, N->in0);
-    forward(N, N->out);
+    forward(N, N->out, true);
     cudaMemsetAsync(N->sums, 0, 4 * sizeof(double), N->stream);
     k_loss_sums<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->out, d_target, N->sums);
     k_loss_grad<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->out, d_target, N->dout);
@@ -803,13 +829,16 @@ int suli_nn_set_kernel(suli_nn* N, int kernel) {
     return SULI_OK;
 }
 
-// The layer primitive on caller buffers (channels-last BF16), for tests: out = relu?(conv3(x) + b)
-int suli_nn_conv3d(int nx, int ny, int nz, const void* x, int cin, const void* w, const float* bias, int cout,
-                   int relu, void* out, int kernel) {
+// The layer primitive on caller buffers (channels-last BF16), for tests: out = relu?(conv3(x) + b),
+// with the pooling and head the network fuses into its convolutions
+int suli_nn_conv3d_ex(int nx, int ny, int nz, const void* x, int cin, const void* w, const float* bias, int cout,
+                      int relu, void* out, void* pool_out, const float* head_w, float* head_out, int kernel) {
     if (!x || !w || !out || cin % 16 || cout % 8 || nx < 1 || ny < 1 || nz < 1) return SULI_ERR_ARG;
     if (kernel < 0 || kernel > 2) return SULI_ERR_ARG;
     if (cout != 16 && cout != 32 && cout != 48 && cout != 64 && cout != 96 && cout != 160) return SULI_ERR_UNSUPPORTED;
     if (cin > 160) return SULI_ERR_SIZE;
+    if (pool_out && (nx % 2 || ny % 2 || nz % 2)) return SULI_ERR_ARG;
+    if ((head_w != nullptr) != (head_out != nullptr) || (head_w && cout != 16)) return SULI_ERR_ARG;
     suli_nn tmp;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -818,15 +847,28 @@ int suli_nn_conv3d(int nx, int ny, int nz, const void* x, int cin, const void* w
     tmp.kernel = kernel;
     if (cudaMalloc(&tmp.err_flag, sizeof(int)) != cudaSuccess) return SULI_ERR_NOMEM;
     cudaMemset(tmp.err_flag, 0, sizeof(int));
+    const Vol vol{nx, ny, nz};
+    const long long V = (long long)nx * ny * nz;
     ConvIn in{static_cast<const __nv_bfloat16*>(x), cin, 0, nullptr, 0};
-    conv(&tmp, Vol{nx, ny, nz}, in, static_cast<const __nv_bfloat16*>(w), bias, relu, cout,
-         static_cast<__nv_bfloat16*>(out));
+    const auto* W = static_cast<const __nv_bfloat16*>(w);
+    auto* o = static_cast<__nv_bfloat16*>(out);
+    auto* po = static_cast<__nv_bfloat16*>(pool_out);
+    const TpEpi epi{po, head_w, head_out, 1};
+    if (!(kernel == 0 && conv_tp(&tmp, vol, in, W, bias, relu, cout, o, epi))) {
+        conv(&tmp, vol, in, W, bias, relu, cout, o);
+        if (po) k_pool<<<nb(V / 8 * cout), 256>>>(vol, cout, o, po);
+        if (head_w) k_head_fwd<<<nb(V), 256>>>(V, o, head_w, head_out);
+    }
     cudaError_t e = cudaDeviceSynchronize();
     int flag = 0;
     if (e == cudaSuccess) e = cudaMemcpy(&flag, tmp.err_flag, sizeof(int), cudaMemcpyDeviceToHost);
     cudaFree(tmp.err_flag);
     if (e != cudaSuccess) return SULI_ERR_CUDA;
     return flag ? SULI_ERR_CUDA : SULI_OK;
+}
+int suli_nn_conv3d(int nx, int ny, int nz, const void* x, int cin, const void* w, const float* bias, int cout,
+                   int relu, void* out, int kernel) {
+    return suli_nn_conv3d_ex(nx, ny, nz, x, cin, w, bias, cout, relu, out, nullptr, nullptr, nullptr, kernel);
 }
 
 }  // extern "C"

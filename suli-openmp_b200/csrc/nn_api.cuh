@@ -13,10 +13,8 @@ namespace nn {
 // Grid (cells) and device the network was created for.
 SULI_NN_INTERNAL void dims(const suli_nn* N, int* nx, int* ny, int* nz, int* device);
 // Forward pass on `stream` without synchronising: in3 [V][3] FP32 -> out [V] FP32 (device).
-// Uses the network's own activation buffers.
-SULI_NN_INTERNAL void forward_on(suli_nn* N, cudaStream_t stream, const float* d_in3, float* d_out);
-// Kernel launches of one forward pass (for the tracing counters).
-SULI_NN_INTERNAL int forward_launches();
+// Uses the network's own activation buffers.  Returns the kernels it launched (tracing counters).
+SULI_NN_INTERNAL int forward_on(suli_nn* N, cudaStream_t stream, const float* d_in3, float* d_out);
 // Nonzero (and cleared) if a tensor-core convolution's completion wait timed out since the
 // last call.  Synchronous.
 SULI_NN_INTERNAL int take_error(suli_nn* N);

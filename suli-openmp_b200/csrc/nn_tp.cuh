@@ -72,6 +72,14 @@ struct TpGeo<true> {
     static constexpr int MMAS = 9;
 };
 
+// what the epilogue writes besides (or instead of) the BF16 activation
+struct TpEpi {
+    __nv_bfloat16* pool;   // 2x2x2 average of the BF16 output at half resolution (null: none)
+    const float* head_w;   // 1x1x1 head, 16 weights + bias (null: none; Cout = 16 only)
+    float* head_out;       // head output [V] FP32
+    int store;             // 1: store the BF16 activation
+};
+
 struct TpCfg {
     int cout, tcols, nchunks;
     int ca, a_tma;        // channels of input A; 1: A is full resolution (TMA), 0: half resolution
@@ -124,7 +132,7 @@ __device__ __forceinline__ bool tp_wait(uint32_t bar, uint32_t parity, volatile 
 template <int NZ, bool FOLD>
 __global__ void __launch_bounds__(TP_THREADS, 1)
     k_conv3_tp(Vol vol, ConvIn in, const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
-               const __grid_constant__ CUtensorMap map_w, const float* __restrict__ bias, TpCfg cfg,
+               const __grid_constant__ CUtensorMap map_w, const float* __restrict__ bias, TpCfg cfg, TpEpi epi,
                __nv_bfloat16* __restrict__ out, int* err) {
     using G = TpGeo<FOLD>;
     constexpr int RUN = G::HXR * 16;   // bytes of one x-run of the halo
@@ -173,6 +181,7 @@ __global__ void __launch_bounds__(TP_THREADS, 1)
         if (cfg.a_tma) asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_a)) : "memory");
     }
     for (int i = tid; i < cfg.cout; i += TP_THREADS) sbias[i] = bias ? bias[i] : 0.f;
+    if (epi.head_w && tid < 17) sbias[cfg.cout + tid] = epi.head_w[tid];
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
@@ -309,8 +318,14 @@ __global__ void __launch_bounds__(TP_THREADS, 1)
         // for hx in 1..14; else output voxel (m % 8, m / 8)
         const int rx = FOLD ? (m & 15) - 1 : (m & 7), ry = FOLD ? (m >> 4) : (m >> 3);
         const bool row_ok = !FOLD || (rx >= 0 && rx < G::OX);
-        const int ncb = cfg.cout / 16, nitems = NZ * ncb;
-        constexpr int LD = FOLD ? 3 : 1;   // 16-column TMEM loads per item
+        // A warp's work unit is (pair of z-planes, 16-channel block): both planes of a 2x2x2
+        // pooling block stay in one warp.  x / y neighbours of the pooling block are lanes +DX, +DY.
+        constexpr int ZU = NZ >= 2 ? 2 : 1;
+        constexpr int DX = 1, DY = FOLD ? 16 : 8;
+        const int ncb = cfg.cout / 16, nunits = (NZ / ZU) * ncb;
+        constexpr int LD = FOLD ? 3 : 1;   // 16-column TMEM loads per (plane, block)
+        const bool pool_lead = ((FOLD ? rx : (m & 7)) & 1) == 0 && (ry & 1) == 0 && row_ok;
+        const int pcx = vol.nx / 2, pcy = vol.ny / 2;
         int it = 0;
         for (int t = blockIdx.x; t < cfg.tiles; t += gridDim.x, ++it) {
             const int a = it & 1;
@@ -322,35 +337,40 @@ __global__ void __launch_bounds__(TP_THREADS, 1)
             asm volatile("tcgen05.fence::after_thread_sync;");
             const int bz = t / txy, rem = t - bz * txy, by = rem / cfg.tiles_x, bx = rem - by * cfg.tiles_x;
             const int ox = bx * G::OX + rx, oy = by * G::OY + ry;
+            const bool in_xy = row_ok && ox < vol.nx && oy < vol.ny;
             const uint32_t colq = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * acc_cols);
-            // items of this warp: i = half, half + 2, ...
-            for (int i = half; i < nitems; i += 2) {
-                const int sz = i / ncb, cb = (i - sz * ncb) * 16;
-                uint32_t r[LD][16];
+            for (int u = half; u < nunits; u += 2) {
+                const int zp = u / ncb, cb = (u - zp * ncb) * 16;
+                float pacc[16];   // pooling: the first plane's four values, summed in k_pool's order
 #pragma unroll
-                for (int l = 0; l < LD; ++l) tc_ld16(colq + (uint32_t)(sz * cfg.tcols + l * cfg.cout + cb), r[l]);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (i + 2 >= nitems) {
-                    // last TMEM read of this tile: hand the accumulator set back to the MMA warps
-                    asm volatile("tcgen05.fence::before_thread_sync;");
-                    tp_arrive(tempty(a));
-                }
-                const int oz = bz * NZ + sz;
-                float v[16];
-                if (FOLD) {
+                for (int zz = 0; zz < ZU; ++zz) {
+                    const int sz = zp * ZU + zz;
+                    uint32_t r[LD][16];
 #pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        const float pm = __shfl_up_sync(0xffffffffu, __uint_as_float(r[0][e]), 1);
-                        const float pp = __shfl_down_sync(0xffffffffu, __uint_as_float(r[LD - 1][e]), 1);
-                        v[e] = (pm + __uint_as_float(r[LD > 1 ? 1 : 0][e])) + pp;
+                    for (int l = 0; l < LD; ++l) tc_ld16(colq + (uint32_t)(sz * cfg.tcols + l * cfg.cout + cb), r[l]);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    if (u + 2 >= nunits && zz == ZU - 1) {
+                        // last TMEM read of this tile: hand the accumulator set back to the MMA warps
+                        asm volatile("tcgen05.fence::before_thread_sync;");
+                        tp_arrive(tempty(a));
                     }
-                } else {
+                    const int oz = bz * NZ + sz;
+                    const bool inside = in_xy && oz < vol.nz;
+                    float v[16];
+                    if (FOLD) {
 #pragma unroll
-                    for (int e = 0; e < 16; ++e) v[e] = __uint_as_float(r[0][e]);
-                }
-                if (row_ok && ox < vol.nx && oy < vol.ny && oz < vol.nz) {
-                    const long long vo = (long long)ox + vol.nx * ((long long)oy + (long long)vol.ny * oz);
+                        for (int e = 0; e < 16; ++e) {
+                            const float pm = __shfl_up_sync(0xffffffffu, __uint_as_float(r[0][e]), 1);
+                            const float pp = __shfl_down_sync(0xffffffffu, __uint_as_float(r[LD - 1][e]), 1);
+                            v[e] = (pm + __uint_as_float(r[LD > 1 ? 1 : 0][e])) + pp;
+                        }
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) v[e] = __uint_as_float(r[0][e]);
+                    }
+                    // bias, ReLU, BF16 rounding; rv = the rounded values as the next layer reads them
                     uint32_t packed[8];
+                    float rv[16];
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
                         const float2 b2 = reinterpret_cast<const float2*>(sbias + cb)[e];
@@ -358,14 +378,58 @@ __global__ void __launch_bounds__(TP_THREADS, 1)
                         if (cfg.relu) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
                         const __nv_bfloat162 h2 = __floats2bfloat162_rn(v0, v1);
                         packed[e] = *reinterpret_cast<const uint32_t*>(&h2);
+                        rv[2 * e] = __low2float(h2);
+                        rv[2 * e + 1] = __high2float(h2);
                     }
-                    uint4* o = reinterpret_cast<uint4*>(out + vo * cfg.cout + cb);
-                    o[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
-                    o[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+                    const long long vo = (long long)ox + vol.nx * ((long long)oy + (long long)vol.ny * oz);
+                    if (inside && epi.store) {
+                        uint4* o = reinterpret_cast<uint4*>(out + vo * cfg.cout + cb);
+                        o[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+                        o[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+                    }
+                    if (epi.head_out && inside) {
+                        // 1x1x1 head on the BF16 activations (Cout = 16), k_head_fwd's order
+                        float hs = sbias[cfg.cout + 16];
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) hs += sbias[cfg.cout + e] * rv[e];
+                        epi.head_out[vo] = hs;
+                    }
+                    if (epi.pool) {
+                        // 2x2x2 average: (x0,y0), (x1,y0), (x0,y1), (x1,y1) of plane z0, then of z1
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) {
+                            const float n1 = __shfl_down_sync(0xffffffffu, rv[e], DX);
+                            const float n2 = __shfl_down_sync(0xffffffffu, rv[e], DY);
+                            const float n3 = __shfl_down_sync(0xffffffffu, rv[e], DX + DY);
+                            if (zz == 0) {
+                                pacc[e] = ((rv[e] + n1) + n2) + n3;
+                            } else {
+                                float sum = pacc[e];
+                                sum += rv[e];
+                                sum += n1;
+                                sum += n2;
+                                sum += n3;
+                                pacc[e] = 0.125f * sum;
+                            }
+                        }
+                        if (zz == ZU - 1 && pool_lead && inside) {
+                            const long long pv =
+                                (long long)(ox >> 1) + pcx * ((long long)(oy >> 1) + (long long)pcy * (oz >> 1));
+                            uint32_t pk[8];
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) {
+                                const __nv_bfloat162 h2 = __floats2bfloat162_rn(pacc[2 * e], pacc[2 * e + 1]);
+                                pk[e] = *reinterpret_cast<const uint32_t*>(&h2);
+                            }
+                            uint4* o = reinterpret_cast<uint4*>(epi.pool + pv * cfg.cout + cb);
+                            o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                            o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                        }
+                    }
                 }
             }
-            if (half >= nitems) {
-                // no item in this tile for this warp (one-item tiles)
+            if (half >= nunits) {
+                // no unit in this tile for this warp
                 asm volatile("tcgen05.fence::before_thread_sync;");
                 tp_arrive(tempty(a));
             }

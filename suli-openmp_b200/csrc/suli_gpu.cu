@@ -670,8 +670,8 @@ void nn_begin(suli_ctx* c) {
         return;
     }
     {
-        ProfScope ps(c, SULI_K_NN, suli::nn::forward_launches());
-        suli::nn::forward_on(c->nn, c->stream, c->nn_in, c->nn_out);
+        ProfScope ps(c, SULI_K_NN, 0);
+        c->prof.launches[SULI_K_NN] += suli::nn::forward_on(c->nn, c->stream, c->nn_in, c->nn_out);
     }
     ProfScope ps(c, SULI_K_CG_SETUP, 3);
     launch_nn_step(c, c->nn_out, c->cg_e);

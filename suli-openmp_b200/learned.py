@@ -149,13 +149,16 @@ class Net:
 
 
 def conv3d(x, w, bias, out, shape, cin: int, cout: int, relu: bool = False, kernel: int = 0,
-           lib_path=None) -> None:
-    """The convolution primitive on device buffers (channels-last BF16, see suli_nn_conv3d);
-    kernel 0 = pipelined tcgen05, 1 = mma.sync, 2 = tcgen05 one tile per CTA."""
+           lib_path=None, pool=None, head_w=None, head_out=None) -> None:
+    """The convolution primitive on device buffers (channels-last BF16, see suli_nn_conv3d_ex);
+    kernel 0 = pipelined tcgen05, 1 = mma.sync, 2 = tcgen05 one tile per CTA.  `pool` (BF16
+    [V/8][cout]) receives the 2x2x2 average of the output, `head_w` (17 FP32) / `head_out` (FP32
+    [V]) the 1x1x1 head, as the network fuses them into its convolutions."""
     lib = _abi.load_library(lib_path)
     nx, ny, nz = shape
-    rc = lib.suli_nn_conv3d(int(nx), int(ny), int(nz), C.c_void_p(_ptr(x)), int(cin), C.c_void_p(_ptr(w)),
-                            C.c_void_p(_ptr(bias)) if bias is not None else None, int(cout), int(relu),
-                            C.c_void_p(_ptr(out)), int(kernel))
+    opt = lambda a: C.c_void_p(_ptr(a)) if a is not None else None
+    rc = lib.suli_nn_conv3d_ex(int(nx), int(ny), int(nz), C.c_void_p(_ptr(x)), int(cin), C.c_void_p(_ptr(w)),
+                               opt(bias), int(cout), int(relu), C.c_void_p(_ptr(out)), opt(pool), opt(head_w),
+                               opt(head_out), int(kernel))
     if rc != 0:
-        raise NetError(rc, "suli_nn_conv3d failed")
+        raise NetError(rc, "suli_nn_conv3d_ex failed")

@@ -96,6 +96,45 @@ def test_pipeline_kernel_at_scale(pkg, torch, shape, cin, cout):
         assert torch.equal(outs[0], outs[1])
 
 
+def _pool_ref(torch, out):
+    """k_pool's arithmetic on a BF16 [nz][ny][nx][C] tensor: FP32 sum of the 8 children in the
+    order (x, y, z) = (0,0,0), (1,0,0), (0,1,0), (1,1,0), then z = 1, times 1/8, rounded to BF16."""
+    f = out.float()
+    s = torch.zeros_like(f[::2, ::2, ::2])
+    for d in range(8):
+        dx, dy, dz = d & 1, (d >> 1) & 1, d >> 2
+        s = s + f[dz::2, dy::2, dx::2]
+    return (0.125 * s).to(torch.bfloat16)
+
+
+@pytest.mark.parametrize("kernel", [0, 2], ids=["tcgen05_pipe", "tcgen05_tile"])
+@pytest.mark.parametrize("shape,cin,cout,head", [
+    ((64, 48, 32), 16, 16, True),    # x taps folded, 4 planes a tile: pooling and head in the epilogue
+    ((32, 32, 16), 32, 32, False),   # x taps folded, 2 planes a tile
+    ((16, 32, 16), 32, 64, False),   # 8 x 16 tile, 2 planes
+])
+def test_fused_pool_and_head(pkg, torch, shape, cin, cout, head, kernel):
+    """The pooling and the head the network fuses into its convolutions: the pooled tensor equals
+    k_pool's arithmetic on the convolution's own BF16 output bit for bit, the head equals
+    w . x + b of that output to FP32 rounding."""
+    nx, ny, nz = shape
+    g = torch.Generator(device="cuda:0").manual_seed(cin * 7 + cout)
+    x = torch.randn((nz, ny, nx, cin), generator=g, device="cuda:0").to(torch.bfloat16)
+    w = (torch.randn((27, cout, cin), generator=g, device="cuda:0") / (27 * cin) ** 0.5).to(torch.bfloat16)
+    b = torch.randn(cout, generator=g, device="cuda:0") * 0.1
+    out = torch.empty((nz, ny, nx, cout), dtype=torch.bfloat16, device="cuda:0")
+    pool = torch.full((nz // 2, ny // 2, nx // 2, cout), float("nan"), dtype=torch.bfloat16, device="cuda:0")
+    hw = torch.randn(17, generator=g, device="cuda:0") if head else None
+    ho = torch.full((nz, ny, nx), float("nan"), device="cuda:0") if head else None
+    pkg.learned.conv3d(x, w, b, out, shape, cin, cout, True, kernel=kernel, pool=pool, head_w=hw, head_out=ho)
+    torch.cuda.synchronize()
+    assert torch.equal(pool, _pool_ref(torch, out))
+    if head:
+        ref = (out.double() * hw[:16].double()).sum(-1) + float(hw[16])
+        scale = (out.double().abs() * hw[:16].double().abs()).sum(-1) + abs(float(hw[16]))
+        assert bool(((ho.double() - ref).abs() <= 1e-6 * scale).all())
+
+
 def test_network_forward_pipeline_matches_tile_kernel(pkg, torch):
     """Whole network at 128 x 128 x 64 (many tiles per CTA on every level), including the
     decoder's upsampled half-resolution inputs gathered with cp.async: the pipelined kernel and
