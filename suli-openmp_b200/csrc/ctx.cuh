@@ -120,6 +120,8 @@ struct suli_ctx {
     std::vector<suli::MGLevel> mg;
     float *pc_x = nullptr, *pc_r = nullptr, *pc_pa = nullptr, *pc_pb = nullptr, *pc_q = nullptr;
     double* cg_e2 = nullptr;
+    double* cg_sd = nullptr;    // sqrt(d), stored once per solve (ghost values, the refinement's scaling)
+    double* cg_isd = nullptr;   // 1/sqrt(d) (the coefficient scaling)
     suli::PCGState* pcg = nullptr;
     suli::PCGState* pcg_host = nullptr;
     float* f32_arena = nullptr;

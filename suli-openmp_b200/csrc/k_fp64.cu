@@ -715,59 +715,91 @@ __device__ __forceinline__ double face_s_z(const Geo& G, const double* rho, doub
     return cz / ((FIDX(rho, i, j, fc) + FIDX(rho, i, j, fc - 1)) * 0.5);
 }
 
-// diagonal d, scaled unknown e = prd1*sqrt(d), scaled right-hand side b = q/sqrt(d) (:46-87, :118-124)
-__global__ void __launch_bounds__(256) k_cg_diag(Geo G, CGConst K, const double* __restrict__ rho,
-                                                 const double* __restrict__ u, const double* __restrict__ v,
-                                                 const double* __restrict__ w, const double* __restrict__ prd1,
-                                                 double* d, double* e, double* b) {
+// Set-up of the scaled system in three passes, so that each face conductance is divided once:
+// faces -> diagonal, e and b -> scaled coefficients and first residual.  The face values, their
+// sums and the scaled coefficients are the same expressions, in the same order, as forming
+// every face where it is used.
+
+// minus-face conductances of every cell, the reference's c/((rho_a + rho_b)/2) with the clamped
+// end faces (:46-87): sx(i) = face between i-1 and i (at i = 1 the face of i = 2)
+__global__ void __launch_bounds__(256) k_cg_faces(Geo G, CGConst K, const double* __restrict__ rho, double* sx,
+                                                  double* sy, double* sz) {
     const Thread3 t = tid3(1, 1, 1);
     const int i = t.i, j = t.j, k = t.k;
     if (i > G.nx || j > G.ny || k > G.nz) return;
-    const double dv = face_s_x(G, rho, K.cx, i + 1, j, k) + face_s_x(G, rho, K.cx, i, j, k) +
-                      face_s_y(G, rho, K.cy, i, j + 1, k) + face_s_y(G, rho, K.cy, i, j, k) +
-                      face_s_z(G, rho, K.cz, i, j, k + 1) + face_s_z(G, rho, K.cz, i, j, k);
+    const long long c = G.idx(i, j, k);
+    sx[c] = face_s_x(G, rho, K.cx, i, j, k);
+    sy[c] = face_s_y(G, rho, K.cy, i, j, k);
+    sz[c] = face_s_z(G, rho, K.cz, i, j, k);
+}
+
+// the plus face of a cell: the next cell's minus face, or at the last cell the same clamped face
+struct PlusFaces {
+    double xp, yp, zp;
+};
+__device__ __forceinline__ PlusFaces plus_faces(const Geo& G, int i, int j, int k, long long c, const double* sx,
+                                                const double* sy, const double* sz) {
+    return PlusFaces{(i < G.nx) ? sx[c + 1] : sx[c], (j < G.ny) ? sy[c + G.px] : sy[c],
+                     (k < G.nz) ? sz[c + G.pxy] : sz[c]};
+}
+
+// diagonal d, scaled unknown e = prd1*sqrt(d), scaled right-hand side b = q/sqrt(d) (:46-87, :118-124)
+__global__ void __launch_bounds__(256) k_cg_diag(Geo G, CGConst K, const double* __restrict__ sx,
+                                                 const double* __restrict__ sy, const double* __restrict__ sz,
+                                                 const double* __restrict__ u, const double* __restrict__ v,
+                                                 const double* __restrict__ w, const double* __restrict__ prd1,
+                                                 double* d, double* e, double* b, double* sdo, double* isdo) {
+    const Thread3 t = tid3(1, 1, 1);
+    const int i = t.i, j = t.j, k = t.k;
+    if (i > G.nx || j > G.ny || k > G.nz) return;
+    const long long c = G.idx(i, j, k);
+    const PlusFaces P = plus_faces(G, i, j, k, c, sx, sy, sz);
+    const double dv = P.xp + sx[c] + P.yp + sy[c] + P.zp + sz[c];
     const double q = (FIDX(u, i, j, k) - FIDX(u, i + 1, j, k)) / K.dx + (FIDX(v, i, j, k) - FIDX(v, i, j + 1, k)) / K.dy +
                      (FIDX(w, i, j, k) - FIDX(w, i, j, k + 1)) / K.dz;
-    const long long c = G.idx(i, j, k);
     const double sd = sqrt(dv);
     d[c] = dv;
     e[c] = prd1[c] * sd;
     b[c] = q / sd;
+    sdo[c] = sd;
+    isdo[c] = 1.0 / sd;
 }
 
-// scaled face coefficients and the first residual (:126-151); reduction of r.r and b.b
-__global__ void __launch_bounds__(256) k_cg_coef(Geo G, BC bc, CGConst K, const double* __restrict__ rho,
-                                                 const double* __restrict__ d, const double* __restrict__ e,
-                                                 const double* __restrict__ b, const double* __restrict__ prd1,
-                                                 double* ax, double* ay, double* az, double* r, CGState* st,
-                                                 double* partial, unsigned int* counter) {
+// scaled face coefficients s/sqrt(d_c d_nb) = s * (1/sqrt(d_c)) * (1/sqrt(d_nb)) and the first
+// residual (:126-151); reduction of r.r and b.b
+__global__ void __launch_bounds__(256, 4) k_cg_coef(Geo G, BC bc, CGConst K, const double* __restrict__ sx,
+                                                    const double* __restrict__ sy, const double* __restrict__ sz,
+                                                    const double* __restrict__ sd, const double* __restrict__ isd,
+                                                    const double* __restrict__ e, const double* __restrict__ b,
+                                                    const double* __restrict__ prd1, double* ax, double* ay,
+                                                    double* az, double* r, CGState* st, double* partial,
+                                                    unsigned int* counter) {
     const Thread3 t = tid3(1, 1, 1);
     const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
     double rr = 0.0, bbv = 0.0;
     if (i <= nx && j <= ny && k <= nz) {
-        const long long c = G.idx(i, j, k);
-        const double dc = d[c];
-        auto dd = [&](int ii, int jj, int kk) {
-            return FIDX(d, map_any(ii, nx, bc.perx), map_any(jj, ny, bc.pery), map_any(kk, nz, bc.perz));
-        };
-        // e at a neighbour: interior value, or the halo value prd1(ghost)*sqrt(d(ghost))
-        auto ee = [&](int ii, int jj, int kk) {
-            if (ii < 1 || ii > nx || jj < 1 || jj > ny || kk < 1 || kk > nz) return FIDX(prd1, ii, jj, kk) * sqrt(dd(ii, jj, kk));
-            return FIDX(e, ii, jj, kk);
-        };
-        const double app = face_s_x(G, rho, K.cx, i + 1, j, k) * rsqrt(dc * dd(i + 1, j, k));
-        const double anp = face_s_x(G, rho, K.cx, i, j, k) * rsqrt(dc * dd(i - 1, j, k));
-        const double bpp = face_s_y(G, rho, K.cy, i, j + 1, k) * rsqrt(dc * dd(i, j + 1, k));
-        const double bnp = face_s_y(G, rho, K.cy, i, j, k) * rsqrt(dc * dd(i, j - 1, k));
-        const double cpp = face_s_z(G, rho, K.cz, i, j, k + 1) * rsqrt(dc * dd(i, j, k + 1));
-        const double cnp = face_s_z(G, rho, K.cz, i, j, k) * rsqrt(dc * dd(i, j, k - 1));
+        const int c = (int)G.idx(i, j, k);
+        const int px = G.px, pxy = (int)G.pxy;
+        const Nb o = neighbours(G, bc, i, j, k);   // ghost-mapped neighbours (periodic wrap / Neumann self)
+        const double ic = isd[c];
+        const double sxp = (i < nx) ? sx[c + 1] : sx[c], syp = (j < ny) ? sy[c + px] : sy[c],
+                     szp = (k < nz) ? sz[c + pxy] : sz[c];
+        const double app = sxp * ic * isd[c + o.xp];
+        const double anp = sx[c] * ic * isd[c + o.xm];
+        const double bpp = syp * ic * isd[c + o.yp];
+        const double bnp = sy[c] * ic * isd[c + o.ym];
+        const double cpp = szp * ic * isd[c + o.zp];
+        const double cnp = sz[c] * ic * isd[c + o.zm];
         ax[c] = anp; ay[c] = bnp; az[c] = cnp;
-        if (i == nx) FIDX(ax, nx + 1, j, k) = app;
-        if (j == ny) FIDX(ay, i, ny + 1, k) = bpp;
-        if (k == nz) FIDX(az, i, j, nz + 1) = cpp;
+        if (i == nx) ax[c + 1] = app;
+        if (j == ny) ay[c + px] = bpp;
+        if (k == nz) az[c + pxy] = cpp;
+        // e at a neighbour: interior value, or the halo value prd1(ghost)*sqrt(d(mapped ghost))
+        auto ee = [&](bool ghost, int cg, int off) { return ghost ? prd1[cg] * sd[c + off] : e[c + off]; };
         const double bv = b[c];
-        const double rv = e[c] - app * ee(i + 1, j, k) - anp * ee(i - 1, j, k) - bpp * ee(i, j + 1, k) -
-                          bnp * ee(i, j - 1, k) - cpp * ee(i, j, k + 1) - cnp * ee(i, j, k - 1) - bv;
+        const double rv = e[c] - app * ee(i == nx, c + 1, o.xp) - anp * ee(i == 1, c - 1, o.xm) -
+                          bpp * ee(j == ny, c + px, o.yp) - bnp * ee(j == 1, c - px, o.ym) -
+                          cpp * ee(k == nz, c + pxy, o.zp) - cnp * ee(k == 1, c - pxy, o.zm) - bv;
         r[c] = rv;
         rr = rv * rv;
         bbv = bv * bv;
@@ -882,14 +914,14 @@ __global__ void __launch_bounds__(kTX * kTY) k_cg_update(Geo G, double* __restri
 }
 
 // de-normalisation over the halo box (:268-274)
-__global__ void k_cg_final(Geo G, BC bc, const double* __restrict__ d, const double* __restrict__ e,
+__global__ void k_cg_final(Geo G, BC bc, const double* __restrict__ sdv, const double* __restrict__ e,
                            double* prd1, const CGState* st) {
     const Thread3 t = tid3(0, 0, 0);
     const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
     if (i > nx + 1 || j > ny + 1 || k > nz + 1) return;
     const int mi = map_any(i, nx, bc.perx), mj = map_any(j, ny, bc.pery), mk = map_any(k, nz, bc.perz);
     const bool gh = (mi != i || mj != j || mk != k);
-    const double sd = sqrt(FIDX(d, mi, mj, mk));
+    const double sd = FIDX(sdv, mi, mj, mk);   // sqrt(d), stored by the set-up
     if (!gh) {
         FIDX(prd1, i, j, k) = FIDX(e, i, j, k) / sd;
     } else if (st->iters == 0) {
@@ -1103,10 +1135,13 @@ static CGConst cg_const(const suli_ctx* c) {
 void launch_cg_setup(suli_ctx* c) {
     const Geo& G = c->g;
     const CGConst K = cg_const(c);
-    ProfScope ps(c, SULI_K_CG_SETUP, 2);
-    k_cg_diag<<<cells_grid(G), kBlk, 0, c->stream>>>(G, K, c->f[SULI_F_RHO], c->f[SULI_F_U], c->f[SULI_F_V],
-                                                      c->f[SULI_F_W], c->f[SULI_F_PRD1], c->cg_d, c->cg_e, c->cg_b);
-    k_cg_coef<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->bc, K, c->f[SULI_F_RHO], c->cg_d, c->cg_e, c->cg_b,
+    ProfScope ps(c, SULI_K_CG_SETUP, 3);
+    // face scratch: the CG direction and product vectors, written again before the iterations read them
+    double *sx = c->cg_pa, *sy = c->cg_pb, *sz = c->cg_q;
+    k_cg_faces<<<cells_grid(G), kBlk, 0, c->stream>>>(G, K, c->f[SULI_F_RHO], sx, sy, sz);
+    k_cg_diag<<<cells_grid(G), kBlk, 0, c->stream>>>(G, K, sx, sy, sz, c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W],
+                                                      c->f[SULI_F_PRD1], c->cg_d, c->cg_e, c->cg_b, c->cg_sd, c->cg_isd);
+    k_cg_coef<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->bc, K, sx, sy, sz, c->cg_sd, c->cg_isd, c->cg_e, c->cg_b,
                                                       c->f[SULI_F_PRD1], c->cg_ax, c->cg_ay, c->cg_az, c->cg_r, c->cg,
                                                       c->red_partial, c->red_counter);
 }
@@ -1126,7 +1161,7 @@ void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new) {
 void launch_cg_final(suli_ctx* c, const double* e) {
     const Geo& G = c->g;
     ProfScope ps(c, SULI_K_CG_FINAL, 1);
-    k_cg_final<<<grid3(G.nx + 2, G.ny + 2, G.nz + 2, kBlk), kBlk, 0, c->stream>>>(G, c->bc, c->cg_d, e,
+    k_cg_final<<<grid3(G.nx + 2, G.ny + 2, G.nz + 2, kBlk), kBlk, 0, c->stream>>>(G, c->bc, c->cg_sd, e,
                                                                                    c->f[SULI_F_PRD1], c->cg);
 }
 void launch_posdin(suli_ctx* c) {

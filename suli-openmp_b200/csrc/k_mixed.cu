@@ -470,10 +470,11 @@ __global__ void __launch_bounds__(256) k_pcg_updc(Geo G, float* __restrict__ x, 
 }
 
 // ------------------------------------------------------------------------------------
-// FP64 refinement: e <- e - sqrt(d) dp, r~ = A~ e - b~, r_u = sqrt(d) r~ (FP32)
+// FP64 refinement: e <- e - sqrt(d) dp, r~ = A~ e - b~, r_u = sqrt(d) r~ (FP32); sqrt(d) is the
+// set-up's stored value (sd)
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_mx_outer(Geo G, BC bc, const double* __restrict__ e_in,
-                                                  const float* __restrict__ dp, const double* __restrict__ d,
+                                                  const float* __restrict__ dp, const double* __restrict__ sd,
                                                   const double* __restrict__ ax, const double* __restrict__ ay,
                                                   const double* __restrict__ az, const double* __restrict__ b,
                                                   double* __restrict__ e_out, float* __restrict__ ru, int apply,
@@ -485,12 +486,12 @@ __global__ void __launch_bounds__(256) k_mx_outer(Geo G, BC bc, const double* __
     if (i <= G.nx && j <= G.ny && k <= G.nz) {
         const int c = (int)G.idx(i, j, k);
         const Nb o = neighbours(G, bc, i, j, k);
-        auto en = [&](int cc) { return apply ? e_in[cc] - sqrt(d[cc]) * (double)dp[cc] : e_in[cc]; };
+        auto en = [&](int cc) { return apply ? e_in[cc] - sd[cc] * (double)dp[cc] : e_in[cc]; };
         const double ec = en(c);
         const double rv = ec - ax[c + 1] * en(c + o.xp) - ax[c] * en(c + o.xm) - ay[c + G.px] * en(c + o.yp) -
                           ay[c] * en(c + o.ym) - az[c + (int)G.pxy] * en(c + o.zp) - az[c] * en(c + o.zm) - b[c];
         e_out[c] = ec;
-        const double u = sqrt(d[c]) * rv;
+        const double u = sd[c] * rv;
         ru[c] = (float)u;
         rr = rv * rv;
         ru2 = u * u;
@@ -550,7 +551,7 @@ void launch_mx_setup(suli_ctx* c) {
 void launch_mx_residual(suli_ctx* c, const double* e_in, double* e_out, bool apply) {
     ProfScope ps(c, SULI_K_REFINE, 1);
     const Geo& G = c->g;
-    k_mx_outer<<<cells3(G), kB2, 0, c->stream>>>(G, c->bc, e_in, c->pc_x, c->cg_d, c->cg_ax, c->cg_ay, c->cg_az,
+    k_mx_outer<<<cells3(G), kB2, 0, c->stream>>>(G, c->bc, e_in, c->pc_x, c->cg_sd, c->cg_ax, c->cg_ay, c->cg_az,
                                                  c->cg_b, e_out, c->pc_r, apply ? 1 : 0, c->cg, c->pcg,
                                                  c->red_partial, c->red_counter);
 }

@@ -72,11 +72,25 @@ static __device__ bool reduce2_last(double a, double b, double* partial, unsigne
     __syncthreads();
     if (!last) return false;
     __threadfence();
+    // each thread folds partials tid, tid + nt, ... in that order; eight loads are issued ahead
+    // of the additions (the partials sit in L2, and one dependent load per step would make this
+    // single block the kernel's tail)
+    constexpr int U = 8;
     double sa = 0.0, sb = 0.0;
-    for (int q = tid; q < nb; q += nt) {
-        const double pa = __ldcg(&partial[2 * q]), pb = __ldcg(&partial[2 * q + 1]);
-        if (is_max) { sa = fmax(sa, pa); sb = fmax(sb, pb); }
-        else { sa += pa; sb += pb; }
+    for (int q0 = tid; q0 < nb; q0 += U * nt) {
+        double pa[U], pb[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int q = q0 + u * nt;
+            pa[u] = (q < nb) ? __ldcg(&partial[2 * q]) : 0.0;
+            pb[u] = (q < nb) ? __ldcg(&partial[2 * q + 1]) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (q0 + u * nt >= nb) break;
+            if (is_max) { sa = fmax(sa, pa[u]); sb = fmax(sb, pb[u]); }
+            else { sa += pa[u]; sb += pb[u]; }
+        }
     }
     sa = is_max ? block_max(sa) : block_sum(sa);
     sb = is_max ? block_max(sb) : block_sum(sb);

@@ -205,17 +205,18 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
     cudaError_t e;
     if ((e = cudaSetDevice(device)) != cudaSuccess) return bail(e, "cudaSetDevice");
     if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
-    // arena: 40 module fields + 16 work arrays, all in the shared padded box
+    // arena: 40 module fields + 18 work arrays, all in the shared padded box
     const int n3d = SULI_F_BXX0;
-    const int nwork = 16;
+    const int nwork = 18;
     const size_t per = (size_t)c->g.n;
     c->arena_elems = per * (size_t)(n3d + nwork);
     if ((e = cudaMalloc(&c->arena, c->arena_elems * sizeof(double))) != cudaSuccess) return bail(e, "arena");
     if ((e = cudaMemsetAsync(c->arena, 0, c->arena_elems * sizeof(double), c->stream)) != cudaSuccess) return bail(e, "memset");
     for (int f = 0; f < n3d; ++f) c->f[f] = c->arena + per * f;
     double* wk = c->arena + per * n3d;
-    double** work[16] = {&c->ls1, &c->ls2, &c->funcs, &c->nrmx, &c->nrmy, &c->nrmz, &c->cg_d, &c->cg_e,
-                         &c->cg_r, &c->cg_b, &c->cg_pa, &c->cg_pb, &c->cg_q, &c->cg_ax, &c->cg_ay, &c->cg_az};
+    double** work[18] = {&c->ls1, &c->ls2, &c->funcs, &c->nrmx, &c->nrmy, &c->nrmz, &c->cg_d, &c->cg_e,
+                         &c->cg_r, &c->cg_b, &c->cg_pa, &c->cg_pb, &c->cg_q, &c->cg_ax, &c->cg_ay, &c->cg_az,
+                         &c->cg_sd, &c->cg_isd};
     for (int q = 0; q < nwork; ++q) *work[q] = wk + per * q;
     for (int f = SULI_F_BXX0; f < SULI_F_COUNT; ++f) {
         int lo[3], hi[3];
