@@ -21,6 +21,10 @@ namespace suli {
 
 #define FI(a, i, j, k) (a)[G.idx((i), (j), (k))]
 
+// Programmatic dependent launch: the inner-solve kernels are launched while their predecessor is
+// still running and wait here, before reading anything it wrote (a no-op for a plain launch).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ int clampi_m(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 // ------------------------------------------------------------------------------------
@@ -204,6 +208,7 @@ __device__ __forceinline__ float apply_faces(const Faces& F, float xc, float xm,
 template <class Op>
 __global__ void __launch_bounds__(256) k_mg_pre(Geo G, BC bc, const float* __restrict__ f, Op A,
                                                 float* __restrict__ y, float omega, const PCGState* st) {
+    pdl_wait();
     if (st->done) return;
     const Col q = column(G, bc);
     if (!q.in) return;
@@ -229,6 +234,7 @@ template <class Op>
 __global__ void __launch_bounds__(256) k_mg_jacc(Geo G, BC bc, const float* __restrict__ xin, const float* __restrict__ f,
                                                  Op A, float* __restrict__ xout, float omega, PCGState* st, int do_dot,
                                                  double* partial, unsigned int* counter) {
+    pdl_wait();
     if (st->done) return;
     const Col q = column(G, bc);
     double dot = 0.;
@@ -269,6 +275,7 @@ __global__ void __launch_bounds__(256) k_mg_post(Geo Gf, Geo Gc, BC bc, const fl
                                                  const float* __restrict__ xc, const float* __restrict__ f, Op A,
                                                  float* __restrict__ xout, float omega, float alpha,
                                                  const PCGState* st) {
+    pdl_wait();
     if (st->done) return;
     const Col q = column(Gf, bc);
     if (!q.in) return;
@@ -303,6 +310,7 @@ __global__ void __launch_bounds__(256) k_mg_post(Geo Gf, Geo Gc, BC bc, const fl
 __global__ void __launch_bounds__(256) k_mg_jac(Geo G, BC bc, const float* __restrict__ xin, const float* __restrict__ f,
                                                 OpStored A, float* __restrict__ xout, float omega, PCGState* st,
                                                 int do_dot, double* partial, unsigned int* counter) {
+    pdl_wait();
     if (st->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -335,6 +343,7 @@ __global__ void __launch_bounds__(256) k_mg_jac(Geo G, BC bc, const float* __res
 template <class Op>
 __global__ void __launch_bounds__(256) k_mg_restrict(Geo Gf, Geo Gc, BC bc, const float* __restrict__ x,
                                                      const float* __restrict__ f, Op A, float* fc, const PCGState* st) {
+    pdl_wait();
     if (st->done) return;
     const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -361,6 +370,7 @@ __global__ void __launch_bounds__(256) k_mg_restrict(Geo Gf, Geo Gc, BC bc, cons
 // coarsest grid (<= 1024 cells): damped Jacobi sweeps in shared memory, one block
 __global__ void __launch_bounds__(1024) k_mg_coarsest(Geo G, BC bc, const float* __restrict__ f, OpStored A,
                                                       float* y, int sweeps, float omega, const PCGState* st) {
+    pdl_wait();
     if (st->done) return;
     __shared__ float xs[2][1024];
     const int n = G.nx * G.ny * G.nz;
@@ -406,6 +416,7 @@ __global__ void __launch_bounds__(256) k_pcg_spmvc(Geo G, BC bc, const float* __
                                                    const float* __restrict__ p_old, float* __restrict__ p_new,
                                                    float* __restrict__ q, Op A, PCGState* st, double* partial,
                                                    unsigned int* counter) {
+    pdl_wait();
     if (st->done) return;
     const float beta = (float)st->beta;
     const Col cq = column(G, bc);
@@ -441,6 +452,7 @@ constexpr int kKZU = 8;
 __global__ void __launch_bounds__(256) k_pcg_updc(Geo G, float* __restrict__ x, float* __restrict__ r,
                                                   const float* __restrict__ p, const float* __restrict__ q,
                                                   PCGState* st, double* partial, unsigned int* counter) {
+    pdl_wait();
     if (st->done) return;
     const float alpha = (float)st->alpha;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -517,6 +529,7 @@ __global__ void k_pcg_init(PCGState* st, double inner_tol, int maxit) {
 }
 
 __global__ void k_pcg_cond(cudaGraphConditionalHandle h, const PCGState* st) {
+    pdl_wait();
     cudaGraphSetConditional(h, st->done ? 0u : 1u);
 }
 
@@ -529,6 +542,22 @@ __global__ void k_zero_f(float* a, long long n) {
 // launchers
 // ------------------------------------------------------------------------------------
 static const dim3 kB2(32, 8, 1);
+
+// launch with programmatic stream serialisation (the kernel calls pdl_wait before its loads)
+template <typename... KArgs, typename... Args>
+static void pdl_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
 static inline dim3 cells3(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
 static inline OpStored stored(const MGLevel& L) { return OpStored{L.sx, L.sy, L.sz, L.idg}; }
 static inline OpRho from_rho(const MGLevel& L) { return OpRho{L.rho, L.idg, L.c2}; }
@@ -556,7 +585,7 @@ void launch_mx_residual(suli_ctx* c, const double* e_in, double* e_out, bool app
                                                  c->red_partial, c->red_counter);
 }
 
-void launch_pcg_cond(suli_ctx* c, cudaGraphConditionalHandle h) { k_pcg_cond<<<1, 1, 0, c->stream>>>(h, c->pcg); }
+void launch_pcg_cond(suli_ctx* c, cudaGraphConditionalHandle h) { pdl_launch(k_pcg_cond, 1, 1, c->stream, h, c->pcg); }
 
 void launch_pcg_init(suli_ctx* c, int maxit) {
     k_pcg_init<<<1, 1, 0, c->stream>>>(c->pcg, c->P.inner_tol, maxit);
@@ -574,33 +603,33 @@ void launch_vcycle(suli_ctx* c) {
         MGLevel& M = c->mg[l];
         MGLevel& C = c->mg[l + 1];
         if (l == 0) {
-            k_mg_pre<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, c->pc_r, from_rho(M), M.y, om, c->pcg);
-            k_mg_restrict<<<cells3(C.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, c->pc_r, from_rho(M), C.f, c->pcg);
+            pdl_launch(k_mg_pre<OpRho>, colgrid(M.g), kB2, c->stream, M.g, bc, c->pc_r, from_rho(M), M.y, om, c->pcg);
+            pdl_launch(k_mg_restrict<OpRho>, cells3(C.g), kB2, c->stream, M.g, C.g, bc, M.y, c->pc_r, from_rho(M), C.f, c->pcg);
         } else {
-            k_mg_pre<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, M.f, stored(M), M.y, om, c->pcg);
-            k_mg_restrict<<<cells3(C.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, M.f, stored(M), C.f, c->pcg);
+            pdl_launch(k_mg_pre<OpStored>, colgrid(M.g), kB2, c->stream, M.g, bc, M.f, stored(M), M.y, om, c->pcg);
+            pdl_launch(k_mg_restrict<OpStored>, cells3(C.g), kB2, c->stream, M.g, C.g, bc, M.y, M.f, stored(M), C.f, c->pcg);
         }
     }
     MGLevel& B = c->mg[L - 1];
     if (L == 1) {   // a single level: coarsest sweeps, then one more sweep that forms r.z
-        k_mg_coarsest<<<1, 1024, 0, c->stream>>>(B.g, bc, c->pc_r, stored(B), B.x, c->coarse_sweeps, om, c->pcg);
-        k_mg_jac<<<cells3(B.g), kB2, 0, c->stream>>>(B.g, bc, B.x, c->pc_r, stored(B), B.y, om, c->pcg, 1,
+        pdl_launch(k_mg_coarsest, 1, 1024, c->stream, B.g, bc, c->pc_r, stored(B), B.x, c->coarse_sweeps, om, c->pcg);
+        pdl_launch(k_mg_jac, cells3(B.g), kB2, c->stream, B.g, bc, B.x, c->pc_r, stored(B), B.y, om, c->pcg, 1,
                                                      c->red_partial, c->red_counter);
         return;
     }
-    k_mg_coarsest<<<1, 1024, 0, c->stream>>>(B.g, bc, B.f, stored(B), B.y, c->coarse_sweeps, om, c->pcg);
+    pdl_launch(k_mg_coarsest, 1, 1024, c->stream, B.g, bc, B.f, stored(B), B.y, c->coarse_sweeps, om, c->pcg);
     for (int l = L - 2; l >= 0; --l) {
         MGLevel& M = c->mg[l];
         MGLevel& C = c->mg[l + 1];
         if (l == 0) {
-            k_mg_post<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, C.y, c->pc_r, from_rho(M), M.x, om, alpha,
+            pdl_launch(k_mg_post<OpRho>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, C.y, c->pc_r, from_rho(M), M.x, om, alpha,
                                                            c->pcg);
-            k_mg_jacc<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, M.x, c->pc_r, from_rho(M), M.y, om, c->pcg, 1,
+            pdl_launch(k_mg_jacc<OpRho>, colgrid(M.g), kB2, c->stream, M.g, bc, M.x, c->pc_r, from_rho(M), M.y, om, c->pcg, 1,
                                                            c->red_partial, c->red_counter);
         } else {
-            k_mg_post<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, C.g, bc, M.y, C.y, M.f, stored(M), M.x, om, alpha,
+            pdl_launch(k_mg_post<OpStored>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, C.y, M.f, stored(M), M.x, om, alpha,
                                                            c->pcg);
-            k_mg_jacc<<<colgrid(M.g), kB2, 0, c->stream>>>(M.g, bc, M.x, M.f, stored(M), M.y, om, c->pcg, 0,
+            pdl_launch(k_mg_jacc<OpStored>, colgrid(M.g), kB2, c->stream, M.g, bc, M.x, M.f, stored(M), M.y, om, c->pcg, 0,
                                                            c->red_partial, c->red_counter);
         }
     }
@@ -612,16 +641,16 @@ void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new) {
     {
         ProfScope ps(c, SULI_K_CG_SPMV, 1);
         if (c->mg.size() > 1)
-            k_pcg_spmvc<<<colgrid(G), kB2, 0, c->stream>>>(G, c->bc, M0.y, p_old, p_new, c->pc_q, from_rho(M0), c->pcg,
+            pdl_launch(k_pcg_spmvc<OpRho>, colgrid(G), kB2, c->stream, G, c->bc, M0.y, p_old, p_new, c->pc_q, from_rho(M0), c->pcg,
                                                            c->red_partial, c->red_counter);
         else
-            k_pcg_spmvc<<<colgrid(G), kB2, 0, c->stream>>>(G, c->bc, M0.y, p_old, p_new, c->pc_q, stored(M0), c->pcg,
+            pdl_launch(k_pcg_spmvc<OpStored>, colgrid(G), kB2, c->stream, G, c->bc, M0.y, p_old, p_new, c->pc_q, stored(M0), c->pcg,
                                                            c->red_partial, c->red_counter);
     }
     {
         ProfScope ps(c, SULI_K_CG_UPDATE, 1);
         const dim3 gu((G.nx + 31) / 32, (G.ny + 7) / 8, (G.nz + kKZU - 1) / kKZU);
-        k_pcg_updc<<<gu, kB2, 0, c->stream>>>(G, c->pc_x, c->pc_r, p_new, c->pc_q, c->pcg, c->red_partial,
+        pdl_launch(k_pcg_updc, gu, kB2, c->stream, G, c->pc_x, c->pc_r, p_new, c->pc_q, c->pcg, c->red_partial,
                                               c->red_counter);
     }
     ProfScope ps(c, SULI_K_MG, vcycle_kernels(c));
