@@ -89,7 +89,10 @@ typedef struct suli_params {
     double inner_tol;               /* relative tolerance of each FP32 inner solve             */
     double mg_omega;                /* precision 1: damping of the multigrid Jacobi sweeps (0 = 0.9) */
     double mg_alpha;                /* precision 1: scale of the coarse-grid correction (0 = 1.8)     */
-    int    reserved[4];
+    int    mg_kernels;              /* precision 1: 0 = vectorised multigrid/PCG kernels (4 cells a
+                                       thread, float4 loads; default), 1 = one cell a thread (same
+                                       arithmetic, kept as the reference the tests compare with) */
+    int    reserved[3];
 } suli_params;
 
 /* ---- field identifiers (module arrays of 0_modules.f90) ------------------------------ */

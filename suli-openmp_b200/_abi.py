@@ -43,7 +43,8 @@ class SuliParams(C.Structure):
         ("inner_tol", C.c_double),
         ("mg_omega", C.c_double),
         ("mg_alpha", C.c_double),
-        ("reserved", C.c_int * 4),
+        ("mg_kernels", C.c_int),
+        ("reserved", C.c_int * 3),
     ]
 
     def copy(self) -> "SuliParams":

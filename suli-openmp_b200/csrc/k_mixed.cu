@@ -538,6 +538,10 @@ __global__ void k_zero_f(float* a, long long n) {
     if (q < n) a[q] = 0.f;
 }
 
+}  // namespace suli
+#include "k_mg_vec.cuh"
+namespace suli {
+
 // ------------------------------------------------------------------------------------
 // launchers
 // ------------------------------------------------------------------------------------
@@ -593,65 +597,117 @@ void launch_pcg_init(suli_ctx* c, int maxit) {
     k_zero_f<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->pc_x, n);
 }
 
+static inline OpRho4 from_rho4(const MGLevel& L) { return OpRho4{L.rho, L.idg, L.c2}; }
+static inline OpStored4 stored4(const MGLevel& L) { return OpStored4{L.sx, L.sy, L.sz, L.idg}; }
+// the 4-cells-a-thread kernels on a level (mg_kernels = 0 and x divisible by 4)
+static inline bool vec_level(const suli_ctx* c, const Geo& g) { return c->P.mg_kernels == 0 && g.nx % kVX == 0; }
+
+// pre-smoothing and restriction of level l (level 0 forms its faces from the density)
+static void vc_down(suli_ctx* c, int l, const float* f, float om) {
+    MGLevel& M = c->mg[l];
+    MGLevel& C = c->mg[l + 1];
+    const BC bc = c->bc;
+    if (vec_level(c, M.g)) {
+        if (l == 0) {
+            pdl_launch(k_mgv_pre<OpRho4>, vgrid(M.g, kKZ), kB2, c->stream, M.g, bc, f, from_rho4(M), M.y, om, c->pcg);
+            pdl_launch(k_mgv_restrict<OpRho4>, vgrid_restrict(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, from_rho4(M),
+                       C.f, c->pcg);
+        } else {
+            pdl_launch(k_mgv_pre<OpStored4>, vgrid(M.g, kKZ), kB2, c->stream, M.g, bc, f, stored4(M), M.y, om, c->pcg);
+            pdl_launch(k_mgv_restrict<OpStored4>, vgrid_restrict(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, stored4(M),
+                       C.f, c->pcg);
+        }
+        return;
+    }
+    if (l == 0) {
+        pdl_launch(k_mg_pre<OpRho>, colgrid(M.g), kB2, c->stream, M.g, bc, f, from_rho(M), M.y, om, c->pcg);
+        pdl_launch(k_mg_restrict<OpRho>, cells3(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, from_rho(M), C.f, c->pcg);
+    } else {
+        pdl_launch(k_mg_pre<OpStored>, colgrid(M.g), kB2, c->stream, M.g, bc, f, stored(M), M.y, om, c->pcg);
+        pdl_launch(k_mg_restrict<OpStored>, cells3(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, stored(M), C.f, c->pcg);
+    }
+}
+
+// prolongation + post-smoothing of level l, then the last sweep (level 0: with r.z and beta)
+static void vc_up(suli_ctx* c, int l, const float* f, float om, float alpha) {
+    MGLevel& M = c->mg[l];
+    MGLevel& C = c->mg[l + 1];
+    const BC bc = c->bc;
+    const int dot = (l == 0) ? 1 : 0;
+    if (vec_level(c, M.g)) {
+        const dim3 g = vgrid(M.g, kKZ);
+        if (l == 0) {
+            pdl_launch(k_mgv_post<OpRho4>, g, kB2, c->stream, M.g, C.g, bc, M.y, C.y, f, from_rho4(M), M.x, om, alpha,
+                       c->pcg);
+            pdl_launch(k_mgv_jacc<OpRho4>, g, kB2, c->stream, M.g, bc, M.x, f, from_rho4(M), M.y, om, c->pcg, dot,
+                       c->red_partial, c->red_counter);
+        } else {
+            pdl_launch(k_mgv_post<OpStored4>, g, kB2, c->stream, M.g, C.g, bc, M.y, C.y, f, stored4(M), M.x, om, alpha,
+                       c->pcg);
+            pdl_launch(k_mgv_jacc<OpStored4>, g, kB2, c->stream, M.g, bc, M.x, f, stored4(M), M.y, om, c->pcg, dot,
+                       c->red_partial, c->red_counter);
+        }
+        return;
+    }
+    if (l == 0) {
+        pdl_launch(k_mg_post<OpRho>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, C.y, f, from_rho(M), M.x, om,
+                   alpha, c->pcg);
+        pdl_launch(k_mg_jacc<OpRho>, colgrid(M.g), kB2, c->stream, M.g, bc, M.x, f, from_rho(M), M.y, om, c->pcg, dot,
+                   c->red_partial, c->red_counter);
+    } else {
+        pdl_launch(k_mg_post<OpStored>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, C.y, f, stored(M), M.x, om,
+                   alpha, c->pcg);
+        pdl_launch(k_mg_jacc<OpStored>, colgrid(M.g), kB2, c->stream, M.g, bc, M.x, f, stored(M), M.y, om, c->pcg, dot,
+                   c->red_partial, c->red_counter);
+    }
+}
+
 // z = M r: one V-cycle; the last level-0 sweep also forms r.z and beta
 void launch_vcycle(suli_ctx* c) {
     const float om = (float)c->P.mg_omega;
     const float alpha = (float)c->P.mg_alpha;
     const int L = (int)c->mg.size();
     const BC bc = c->bc;
-    for (int l = 0; l < L - 1; ++l) {
-        MGLevel& M = c->mg[l];
-        MGLevel& C = c->mg[l + 1];
-        if (l == 0) {
-            pdl_launch(k_mg_pre<OpRho>, colgrid(M.g), kB2, c->stream, M.g, bc, c->pc_r, from_rho(M), M.y, om, c->pcg);
-            pdl_launch(k_mg_restrict<OpRho>, cells3(C.g), kB2, c->stream, M.g, C.g, bc, M.y, c->pc_r, from_rho(M), C.f, c->pcg);
-        } else {
-            pdl_launch(k_mg_pre<OpStored>, colgrid(M.g), kB2, c->stream, M.g, bc, M.f, stored(M), M.y, om, c->pcg);
-            pdl_launch(k_mg_restrict<OpStored>, cells3(C.g), kB2, c->stream, M.g, C.g, bc, M.y, M.f, stored(M), C.f, c->pcg);
-        }
-    }
+    for (int l = 0; l < L - 1; ++l) vc_down(c, l, l == 0 ? c->pc_r : c->mg[l].f, om);
     MGLevel& B = c->mg[L - 1];
     if (L == 1) {   // a single level: coarsest sweeps, then one more sweep that forms r.z
         pdl_launch(k_mg_coarsest, 1, 1024, c->stream, B.g, bc, c->pc_r, stored(B), B.x, c->coarse_sweeps, om, c->pcg);
         pdl_launch(k_mg_jac, cells3(B.g), kB2, c->stream, B.g, bc, B.x, c->pc_r, stored(B), B.y, om, c->pcg, 1,
-                                                     c->red_partial, c->red_counter);
+                   c->red_partial, c->red_counter);
         return;
     }
     pdl_launch(k_mg_coarsest, 1, 1024, c->stream, B.g, bc, B.f, stored(B), B.y, c->coarse_sweeps, om, c->pcg);
-    for (int l = L - 2; l >= 0; --l) {
-        MGLevel& M = c->mg[l];
-        MGLevel& C = c->mg[l + 1];
-        if (l == 0) {
-            pdl_launch(k_mg_post<OpRho>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, C.y, c->pc_r, from_rho(M), M.x, om, alpha,
-                                                           c->pcg);
-            pdl_launch(k_mg_jacc<OpRho>, colgrid(M.g), kB2, c->stream, M.g, bc, M.x, c->pc_r, from_rho(M), M.y, om, c->pcg, 1,
-                                                           c->red_partial, c->red_counter);
-        } else {
-            pdl_launch(k_mg_post<OpStored>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, C.y, M.f, stored(M), M.x, om, alpha,
-                                                           c->pcg);
-            pdl_launch(k_mg_jacc<OpStored>, colgrid(M.g), kB2, c->stream, M.g, bc, M.x, M.f, stored(M), M.y, om, c->pcg, 0,
-                                                           c->red_partial, c->red_counter);
-        }
-    }
+    for (int l = L - 2; l >= 0; --l) vc_up(c, l, l == 0 ? c->pc_r : c->mg[l].f, om, alpha);
 }
 
 void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new) {
     const Geo& G = c->g;
     MGLevel& M0 = c->mg[0];
+    const bool vec = vec_level(c, G);
     {
         ProfScope ps(c, SULI_K_CG_SPMV, 1);
-        if (c->mg.size() > 1)
-            pdl_launch(k_pcg_spmvc<OpRho>, colgrid(G), kB2, c->stream, G, c->bc, M0.y, p_old, p_new, c->pc_q, from_rho(M0), c->pcg,
-                                                           c->red_partial, c->red_counter);
-        else
-            pdl_launch(k_pcg_spmvc<OpStored>, colgrid(G), kB2, c->stream, G, c->bc, M0.y, p_old, p_new, c->pc_q, stored(M0), c->pcg,
-                                                           c->red_partial, c->red_counter);
+        if (c->mg.size() > 1) {
+            if (vec)
+                pdl_launch(k_pcgv_spmvc<OpRho4>, vgrid(G, kKZ), kB2, c->stream, G, c->bc, M0.y, p_old, p_new, c->pc_q,
+                           from_rho4(M0), c->pcg, c->red_partial, c->red_counter);
+            else
+                pdl_launch(k_pcg_spmvc<OpRho>, colgrid(G), kB2, c->stream, G, c->bc, M0.y, p_old, p_new, c->pc_q,
+                           from_rho(M0), c->pcg, c->red_partial, c->red_counter);
+        } else {
+            pdl_launch(k_pcg_spmvc<OpStored>, colgrid(G), kB2, c->stream, G, c->bc, M0.y, p_old, p_new, c->pc_q,
+                       stored(M0), c->pcg, c->red_partial, c->red_counter);
+        }
     }
     {
         ProfScope ps(c, SULI_K_CG_UPDATE, 1);
-        const dim3 gu((G.nx + 31) / 32, (G.ny + 7) / 8, (G.nz + kKZU - 1) / kKZU);
-        pdl_launch(k_pcg_updc, gu, kB2, c->stream, G, c->pc_x, c->pc_r, p_new, c->pc_q, c->pcg, c->red_partial,
-                                              c->red_counter);
+        if (vec) {
+            pdl_launch(k_pcgv_updc, vgrid_upd(G), kB2, c->stream, G, c->pc_x, c->pc_r, p_new, c->pc_q, c->pcg,
+                       c->red_partial, c->red_counter);
+        } else {
+            const dim3 gu((G.nx + 31) / 32, (G.ny + 7) / 8, (G.nz + kKZU - 1) / kKZU);
+            pdl_launch(k_pcg_updc, gu, kB2, c->stream, G, c->pc_x, c->pc_r, p_new, c->pc_q, c->pcg, c->red_partial,
+                       c->red_counter);
+        }
     }
     ProfScope ps(c, SULI_K_MG, vcycle_kernels(c));
     launch_vcycle(c);
