@@ -27,6 +27,11 @@ struct Geo {
     __host__ __device__ inline long long idx(int i, int j, int k) const {
         return (long long)kBase + (i - 1) + (long long)px * j + pxy * k;
     }
+    // the same index in 32-bit arithmetic (a field holds fewer than 2^31 elements; suli_create
+    // refuses larger grids)
+    __host__ __device__ inline int idx32(int i, int j, int k) const {
+        return kBase + (i - 1) + px * j + (int)pxy * k;
+    }
 };
 
 inline Geo make_geo(int nx, int ny, int nz) {

@@ -16,7 +16,7 @@
 
 namespace suli {
 
-#define FIDX(a, i, j, k) (a)[G.idx((i), (j), (k))]
+#define FIDX(a, i, j, k) (a)[G.idx32((i), (j), (k))]
 
 // ------------------------------------------------------------------------------------
 // small helpers of 8_derivadas.f90
@@ -319,114 +319,119 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
     const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
     if (i > nx + 1 || j > ny + 1 || k > nz + 1) return;
     const R idx = R(C.idx), idy = R(C.idy), idz = R(C.idz);   // 1/dx, 1/dy, 1/dz
+    // every load is the face's own index plus a constant offset (32-bit): a field value at
+    // (i + di, j + dj, k + dk), read in the compute type R
+    const int px = G.px, pxy = (int)G.pxy, c0 = (int)G.idx(i, j, k);
+#define AT(a, di, dj, dk) R((a)[c0 + (di) + (dj) * px + (dk) * pxy])
     const double* __restrict__ u = F.u;
     const double* __restrict__ v = F.v;
     const double* __restrict__ w = F.w;
     // ---- Fu on u-faces (i = 1..nx+1, j = 1..ny, k = 1..nz)
     if (j <= ny && k <= nz) {
-        const R uc = RLD(u, i, j, k);
-        const R bma4 = (RLD(v, i, j, k) + RLD(v, i - 1, j, k) + RLD(v, i, j + 1, k) + RLD(v, i - 1, j + 1, k)) * R(0.25);
-        const R dma4 = (RLD(w, i, j, k) + RLD(w, i - 1, j, k) + RLD(w, i, j, k + 1) + RLD(w, i - 1, j, k + 1)) * R(0.25);
+        const R uc = AT(u, 0, 0, 0);
+        const R bma4 = (AT(v, 0, 0, 0) + AT(v, -1, 0, 0) + AT(v, 0, 1, 0) + AT(v, -1, 1, 0)) * R(0.25);
+        const R dma4 = (AT(w, 0, 0, 0) + AT(w, -1, 0, 0) + AT(w, 0, 0, 1) + AT(w, -1, 0, 1)) * R(0.25);
         R a1 = pmax(uc, R(0.)), a2 = pmin(uc, R(0.));
-        const R dudx = a1 * (uc - RLD(u, i - 1, j, k)) * idx + a2 * (RLD(u, i + 1, j, k) - uc) * idx;
+        const R dudx = a1 * (uc - AT(u, -1, 0, 0)) * idx + a2 * (AT(u, 1, 0, 0) - uc) * idx;
         a1 = pmax(bma4, R(0.)); a2 = pmin(bma4, R(0.));
-        const R dudy = a1 * (uc - RLD(u, i, j - 1, k)) * idy + a2 * (RLD(u, i, j + 1, k) - uc) * idy;
+        const R dudy = a1 * (uc - AT(u, 0, -1, 0)) * idy + a2 * (AT(u, 0, 1, 0) - uc) * idy;
         a1 = pmax(dma4, R(0.)); a2 = pmin(dma4, R(0.));
-        const R dudz = a1 * (uc - RLD(u, i, j, k - 1)) * idz + a2 * (RLD(u, i, j, k + 1) - uc) * idz;
+        const R dudz = a1 * (uc - AT(u, 0, 0, -1)) * idz + a2 * (AT(u, 0, 0, 1) - uc) * idz;
         const R uint_ = dudx + dudy + dudz;
         const int ic = clampi(i, 2, nx);
-        const R rhox = (RLD(F.rho, ic, j, k) + RLD(F.rho, ic - 1, j, k)) * R(0.5);
-        const R tx1 = RLD(F.hsx, ic, j, k) * RLD(F.kurv, ic, j, k) / RLD(F.rho, ic, j, k);
-        const R tx0 = RLD(F.hsx, ic - 1, j, k) * RLD(F.kurv, ic - 1, j, k) / RLD(F.rho, ic - 1, j, k);
+        const R rhox = (AT(F.rho, (ic) - i, 0, 0) + AT(F.rho, (ic - 1) - i, 0, 0)) * R(0.5);
+        const R tx1 = AT(F.hsx, (ic) - i, 0, 0) * AT(F.kurv, (ic) - i, 0, 0) / AT(F.rho, (ic) - i, 0, 0);
+        const R tx0 = AT(F.hsx, (ic - 1) - i, 0, 0) * AT(F.kurv, (ic - 1) - i, 0, 0) / AT(F.rho, (ic - 1) - i, 0, 0);
         const R dhsdx = (tx1 + tx0) * R(0.5);
-        const R ama_i = RLD(F.nut, clampi(i, 1, nx), j, k) * idx;
-        const R ama_m = RLD(F.nut, clampi(i - 1, 1, nx), j, k) * idx;
+        const R ama_i = AT(F.nut, (clampi(i, 1, nx)) - i, 0, 0) * idx;
+        const R ama_m = AT(F.nut, (clampi(i - 1, 1, nx)) - i, 0, 0) * idx;
         const int jp = clampi(j + 1, 2, ny), jm = clampi(j, 2, ny);
-        const R bma_p = ((RLD(F.xnut, i, jp, k) + RLD(F.xnut, i, jp - 1, k)) * R(0.5)) * idy;
-        const R bma_m = ((RLD(F.xnut, i, jm, k) + RLD(F.xnut, i, jm - 1, k)) * R(0.5)) * idy;
+        const R bma_p = ((AT(F.xnut, 0, (jp) - j, 0) + AT(F.xnut, 0, (jp - 1) - j, 0)) * R(0.5)) * idy;
+        const R bma_m = ((AT(F.xnut, 0, (jm) - j, 0) + AT(F.xnut, 0, (jm - 1) - j, 0)) * R(0.5)) * idy;
         const int kp = clampi(k + 1, 2, nz), km = clampi(k, 2, nz);
-        const R dma_p = ((RLD(F.xnut, i, j, kp) + RLD(F.xnut, i, j, kp - 1)) * R(0.5)) * idz;
-        const R dma_m = ((RLD(F.xnut, i, j, km) + RLD(F.xnut, i, j, km - 1)) * R(0.5)) * idz;
-        const R Gv = (ama_i * R(2.) * (RLD(u, i + 1, j, k) - uc) - ama_m * R(2.) * (uc - RLD(u, i - 1, j, k))) * idx +
-                          bma_p * ((RLD(u, i, j + 1, k) - uc) * idy + (RLD(v, i, j + 1, k) - RLD(v, i - 1, j + 1, k)) * idx) -
-                          bma_m * ((uc - RLD(u, i, j - 1, k)) * idy + (RLD(v, i, j, k) - RLD(v, i - 1, j, k)) * idx) +
-                          dma_p * ((RLD(u, i, j, k + 1) - uc) * idz + (RLD(w, i, j, k + 1) - RLD(w, i - 1, j, k + 1)) * idx) -
-                          dma_m * ((uc - RLD(u, i, j, k - 1)) * idz + (RLD(w, i, j, k) - RLD(w, i - 1, j, k)) * idx);
+        const R dma_p = ((AT(F.xnut, 0, 0, (kp) - k) + AT(F.xnut, 0, 0, (kp - 1) - k)) * R(0.5)) * idz;
+        const R dma_m = ((AT(F.xnut, 0, 0, (km) - k) + AT(F.xnut, 0, 0, (km - 1) - k)) * R(0.5)) * idz;
+        const R Gv = (ama_i * R(2.) * (AT(u, 1, 0, 0) - uc) - ama_m * R(2.) * (uc - AT(u, -1, 0, 0))) * idx +
+                          bma_p * ((AT(u, 0, 1, 0) - uc) * idy + (AT(v, 0, 1, 0) - AT(v, -1, 1, 0)) * idx) -
+                          bma_m * ((uc - AT(u, 0, -1, 0)) * idy + (AT(v, 0, 0, 0) - AT(v, -1, 0, 0)) * idx) +
+                          dma_p * ((AT(u, 0, 0, 1) - uc) * idz + (AT(w, 0, 0, 1) - AT(w, -1, 0, 1)) * idx) -
+                          dma_m * ((uc - AT(u, 0, 0, -1)) * idz + (AT(w, 0, 0, 0) - AT(w, -1, 0, 0)) * idx);
         R r = -uint_ + Gv / rhox + R(C.gx) - R(C.sigma) * dhsdx;
-        if (C.tf) r = r + RLD(F.tfu, i, j, k);
-        if (on_cap(C, j, k, ny)) { const R b = RLD(F.ub, i, j, k); r = r - R(C.cz) * sqrt(b * b) * uc; }
-        FIDX(F.Fu, i, j, k) = (double)r;
+        if (C.tf) r = r + AT(F.tfu, 0, 0, 0);
+        if (on_cap(C, j, k, ny)) { const R b = AT(F.ub, 0, 0, 0); r = r - R(C.cz) * sqrt(b * b) * uc; }
+        F.Fu[c0] = (double)r;
     }
     // ---- Fv on v-faces (i = 1..nx, j = 1..ny+1, k = 1..nz)
     if (i <= nx && k <= nz) {
-        const R vc = RLD(v, i, j, k);
-        const R amb4 = (RLD(u, i, j, k) + RLD(u, i + 1, j, k) + RLD(u, i, j - 1, k) + RLD(u, i + 1, j - 1, k)) * R(0.25);
-        const R dmb4 = (RLD(w, i, j, k) + RLD(w, i, j - 1, k) + RLD(w, i, j, k + 1) + RLD(w, i, j - 1, k + 1)) * R(0.25);
+        const R vc = AT(v, 0, 0, 0);
+        const R amb4 = (AT(u, 0, 0, 0) + AT(u, 1, 0, 0) + AT(u, 0, -1, 0) + AT(u, 1, -1, 0)) * R(0.25);
+        const R dmb4 = (AT(w, 0, 0, 0) + AT(w, 0, -1, 0) + AT(w, 0, 0, 1) + AT(w, 0, -1, 1)) * R(0.25);
         R a1 = pmax(amb4, R(0.)), a2 = pmin(amb4, R(0.));
-        const R dvdx = a1 * (vc - RLD(v, i - 1, j, k)) * idx + a2 * (RLD(v, i + 1, j, k) - vc) * idx;
+        const R dvdx = a1 * (vc - AT(v, -1, 0, 0)) * idx + a2 * (AT(v, 1, 0, 0) - vc) * idx;
         a1 = pmax(vc, R(0.)); a2 = pmin(vc, R(0.));
-        const R dvdy = a1 * (vc - RLD(v, i, j - 1, k)) * idy + a2 * (RLD(v, i, j + 1, k) - vc) * idy;
+        const R dvdy = a1 * (vc - AT(v, 0, -1, 0)) * idy + a2 * (AT(v, 0, 1, 0) - vc) * idy;
         a1 = pmax(dmb4, R(0.)); a2 = pmin(dmb4, R(0.));
-        const R dvdz = a1 * (vc - RLD(v, i, j, k - 1)) * idz + a2 * (RLD(v, i, j, k + 1) - vc) * idz;
+        const R dvdz = a1 * (vc - AT(v, 0, 0, -1)) * idz + a2 * (AT(v, 0, 0, 1) - vc) * idz;
         const R vint = dvdx + dvdy + dvdz;
         const int jc = clampi(j, 2, ny);
-        const R rhoy = (RLD(F.rho, i, jc, k) + RLD(F.rho, i, jc - 1, k)) * R(0.5);
-        const R ty1 = RLD(F.hsy, i, jc, k) * RLD(F.kurv, i, jc, k) / RLD(F.rho, i, jc, k);
-        const R ty0 = RLD(F.hsy, i, jc - 1, k) * RLD(F.kurv, i, jc - 1, k) / RLD(F.rho, i, jc - 1, k);
+        const R rhoy = (AT(F.rho, 0, (jc) - j, 0) + AT(F.rho, 0, (jc - 1) - j, 0)) * R(0.5);
+        const R ty1 = AT(F.hsy, 0, (jc) - j, 0) * AT(F.kurv, 0, (jc) - j, 0) / AT(F.rho, 0, (jc) - j, 0);
+        const R ty0 = AT(F.hsy, 0, (jc - 1) - j, 0) * AT(F.kurv, 0, (jc - 1) - j, 0) / AT(F.rho, 0, (jc - 1) - j, 0);
         const R dhsdy = (ty1 + ty0) * R(0.5);
         const int ip = clampi(i + 1, 2, nx), im = clampi(i, 2, nx);
-        const R amb_p = ((RLD(F.ynut, ip, j, k) + RLD(F.ynut, ip - 1, j, k)) * R(0.5)) * idx;
-        const R amb_m = ((RLD(F.ynut, im, j, k) + RLD(F.ynut, im - 1, j, k)) * R(0.5)) * idx;
-        const R bmb_j = RLD(F.nut, i, clampi(j, 1, ny), k) * idy;
-        const R bmb_m = RLD(F.nut, i, clampi(j - 1, 1, ny), k) * idy;
+        const R amb_p = ((AT(F.ynut, (ip) - i, 0, 0) + AT(F.ynut, (ip - 1) - i, 0, 0)) * R(0.5)) * idx;
+        const R amb_m = ((AT(F.ynut, (im) - i, 0, 0) + AT(F.ynut, (im - 1) - i, 0, 0)) * R(0.5)) * idx;
+        const R bmb_j = AT(F.nut, 0, (clampi(j, 1, ny)) - j, 0) * idy;
+        const R bmb_m = AT(F.nut, 0, (clampi(j - 1, 1, ny)) - j, 0) * idy;
         const int kp = clampi(k + 1, 2, nz), km = clampi(k, 2, nz);
-        const R dmb_p = ((RLD(F.ynut, i, j, kp) + RLD(F.ynut, i, j, kp - 1)) * R(0.5)) * idz;
-        const R dmb_m = ((RLD(F.ynut, i, j, km) + RLD(F.ynut, i, j, km - 1)) * R(0.5)) * idz;
-        const R Gv = amb_p * ((RLD(v, i + 1, j, k) - vc) * idx + (RLD(u, i + 1, j, k) - RLD(u, i + 1, j - 1, k)) * idy) -
-                          amb_m * ((vc - RLD(v, i - 1, j, k)) * idx + (RLD(u, i, j, k) - RLD(u, i, j - 1, k)) * idy) +
-                          (bmb_j * R(2.) * (RLD(v, i, j + 1, k) - vc) - bmb_m * R(2.) * (vc - RLD(v, i, j - 1, k))) * idy +
-                          dmb_p * ((RLD(v, i, j, k + 1) - vc) * idz + (RLD(w, i, j, k + 1) - RLD(w, i, j - 1, k + 1)) * idy) -
-                          dmb_m * ((vc - RLD(v, i, j, k - 1)) * idz + (RLD(w, i, j, k) - RLD(w, i, j - 1, k)) * idy);
+        const R dmb_p = ((AT(F.ynut, 0, 0, (kp) - k) + AT(F.ynut, 0, 0, (kp - 1) - k)) * R(0.5)) * idz;
+        const R dmb_m = ((AT(F.ynut, 0, 0, (km) - k) + AT(F.ynut, 0, 0, (km - 1) - k)) * R(0.5)) * idz;
+        const R Gv = amb_p * ((AT(v, 1, 0, 0) - vc) * idx + (AT(u, 1, 0, 0) - AT(u, 1, -1, 0)) * idy) -
+                          amb_m * ((vc - AT(v, -1, 0, 0)) * idx + (AT(u, 0, 0, 0) - AT(u, 0, -1, 0)) * idy) +
+                          (bmb_j * R(2.) * (AT(v, 0, 1, 0) - vc) - bmb_m * R(2.) * (vc - AT(v, 0, -1, 0))) * idy +
+                          dmb_p * ((AT(v, 0, 0, 1) - vc) * idz + (AT(w, 0, 0, 1) - AT(w, 0, -1, 1)) * idy) -
+                          dmb_m * ((vc - AT(v, 0, 0, -1)) * idz + (AT(w, 0, 0, 0) - AT(w, 0, -1, 0)) * idy);
         R r = -vint + Gv / rhoy - R(C.sigma) * dhsdy;
-        if (C.tf) r = r + RLD(F.tfv, i, j, k);
-        if (on_cap(C, j, k, ny)) { const R b = RLD(F.vb, i, j, k); r = r - R(C.cz) * sqrt(b * b) * vc; }
-        FIDX(F.Fv, i, j, k) = (double)r;
+        if (C.tf) r = r + AT(F.tfv, 0, 0, 0);
+        if (on_cap(C, j, k, ny)) { const R b = AT(F.vb, 0, 0, 0); r = r - R(C.cz) * sqrt(b * b) * vc; }
+        F.Fv[c0] = (double)r;
     }
     // ---- Fw on w-faces (i = 1..nx, j = 1..ny, k = 1..nz+1)
     if (i <= nx && j <= ny) {
-        const R wc = RLD(w, i, j, k);
-        const R amd4 = (RLD(u, i, j, k) + RLD(u, i + 1, j, k) + RLD(u, i, j, k - 1) + RLD(u, i + 1, j, k - 1)) * R(0.25);
-        const R bmd4 = (RLD(v, i, j, k) + RLD(v, i, j + 1, k) + RLD(v, i, j, k - 1) + RLD(v, i, j + 1, k - 1)) * R(0.25);
+        const R wc = AT(w, 0, 0, 0);
+        const R amd4 = (AT(u, 0, 0, 0) + AT(u, 1, 0, 0) + AT(u, 0, 0, -1) + AT(u, 1, 0, -1)) * R(0.25);
+        const R bmd4 = (AT(v, 0, 0, 0) + AT(v, 0, 1, 0) + AT(v, 0, 0, -1) + AT(v, 0, 1, -1)) * R(0.25);
         R a1 = pmax(amd4, R(0.)), a2 = pmin(amd4, R(0.));
-        const R dwdx = a1 * (wc - RLD(w, i - 1, j, k)) * idx + a2 * (RLD(w, i + 1, j, k) - wc) * idx;
+        const R dwdx = a1 * (wc - AT(w, -1, 0, 0)) * idx + a2 * (AT(w, 1, 0, 0) - wc) * idx;
         a1 = pmax(bmd4, R(0.)); a2 = pmin(bmd4, R(0.));
-        const R dwdy = a1 * (wc - RLD(w, i, j - 1, k)) * idy + a2 * (RLD(w, i, j + 1, k) - wc) * idy;
+        const R dwdy = a1 * (wc - AT(w, 0, -1, 0)) * idy + a2 * (AT(w, 0, 1, 0) - wc) * idy;
         a1 = pmax(wc, R(0.)); a2 = pmin(wc, R(0.));
-        const R dwdz = a1 * (wc - RLD(w, i, j, k - 1)) * idz + a2 * (RLD(w, i, j, k + 1) - wc) * idz;
+        const R dwdz = a1 * (wc - AT(w, 0, 0, -1)) * idz + a2 * (AT(w, 0, 0, 1) - wc) * idz;
         const R wint = dwdx + dwdy + dwdz;
         const int kc = clampi(k, 2, nz);
-        const R rhoz = (RLD(F.rho, i, j, kc) + RLD(F.rho, i, j, kc - 1)) * R(0.5);
-        const R tz1 = RLD(F.hsz, i, j, kc) * RLD(F.kurv, i, j, kc) / RLD(F.rho, i, j, kc);
-        const R tz0 = RLD(F.hsz, i, j, kc - 1) * RLD(F.kurv, i, j, kc - 1) / RLD(F.rho, i, j, kc - 1);
+        const R rhoz = (AT(F.rho, 0, 0, (kc) - k) + AT(F.rho, 0, 0, (kc - 1) - k)) * R(0.5);
+        const R tz1 = AT(F.hsz, 0, 0, (kc) - k) * AT(F.kurv, 0, 0, (kc) - k) / AT(F.rho, 0, 0, (kc) - k);
+        const R tz0 = AT(F.hsz, 0, 0, (kc - 1) - k) * AT(F.kurv, 0, 0, (kc - 1) - k) / AT(F.rho, 0, 0, (kc - 1) - k);
         const R dhsdz = (tz1 + tz0) * R(0.5);
         const int ip = clampi(i + 1, 2, nx), im = clampi(i, 2, nx);
-        const R amd_p = ((RLD(F.znut, ip, j, k) + RLD(F.znut, ip - 1, j, k)) * R(0.5)) * idx;
-        const R amd_m = ((RLD(F.znut, im, j, k) + RLD(F.znut, im - 1, j, k)) * R(0.5)) * idx;
+        const R amd_p = ((AT(F.znut, (ip) - i, 0, 0) + AT(F.znut, (ip - 1) - i, 0, 0)) * R(0.5)) * idx;
+        const R amd_m = ((AT(F.znut, (im) - i, 0, 0) + AT(F.znut, (im - 1) - i, 0, 0)) * R(0.5)) * idx;
         const int jp = clampi(j + 1, 2, ny), jm = clampi(j, 2, ny);
-        const R bmd_p = ((RLD(F.znut, i, jp, k) + RLD(F.znut, i, jp - 1, k)) * R(0.5)) * idy;
-        const R bmd_m = ((RLD(F.znut, i, jm, k) + RLD(F.znut, i, jm - 1, k)) * R(0.5)) * idy;
-        const R dmd_k = RLD(F.nut, i, j, clampi(k, 1, nz)) * idz;
-        const R dmd_m = RLD(F.nut, i, j, clampi(k - 1, 1, nz)) * idz;
-        const R Gv = amd_p * ((RLD(w, i + 1, j, k) - wc) * idx + (RLD(u, i + 1, j, k) - RLD(u, i + 1, j, k - 1)) * idz) -
-                          amd_m * ((wc - RLD(w, i - 1, j, k)) * idx + (RLD(u, i, j, k) - RLD(u, i, j, k - 1)) * idz) +
-                          bmd_p * ((RLD(w, i, j + 1, k) - wc) * idy + (RLD(v, i, j + 1, k) - RLD(v, i, j + 1, k - 1)) * idz) -
-                          bmd_m * ((wc - RLD(w, i, j - 1, k)) * idy + (RLD(v, i, j, k) - RLD(v, i, j, k - 1)) * idz) +
-                          (dmd_k * R(2.) * (RLD(w, i, j, k + 1) - wc) - dmd_m * R(2.) * (wc - RLD(w, i, j, k - 1))) * idz;
+        const R bmd_p = ((AT(F.znut, 0, (jp) - j, 0) + AT(F.znut, 0, (jp - 1) - j, 0)) * R(0.5)) * idy;
+        const R bmd_m = ((AT(F.znut, 0, (jm) - j, 0) + AT(F.znut, 0, (jm - 1) - j, 0)) * R(0.5)) * idy;
+        const R dmd_k = AT(F.nut, 0, 0, (clampi(k, 1, nz)) - k) * idz;
+        const R dmd_m = AT(F.nut, 0, 0, (clampi(k - 1, 1, nz)) - k) * idz;
+        const R Gv = amd_p * ((AT(w, 1, 0, 0) - wc) * idx + (AT(u, 1, 0, 0) - AT(u, 1, 0, -1)) * idz) -
+                          amd_m * ((wc - AT(w, -1, 0, 0)) * idx + (AT(u, 0, 0, 0) - AT(u, 0, 0, -1)) * idz) +
+                          bmd_p * ((AT(w, 0, 1, 0) - wc) * idy + (AT(v, 0, 1, 0) - AT(v, 0, 1, -1)) * idz) -
+                          bmd_m * ((wc - AT(w, 0, -1, 0)) * idy + (AT(v, 0, 0, 0) - AT(v, 0, 0, -1)) * idz) +
+                          (dmd_k * R(2.) * (AT(w, 0, 0, 1) - wc) - dmd_m * R(2.) * (wc - AT(w, 0, 0, -1))) * idz;
         R r = -wint + Gv / rhoz - R(C.gz) - R(C.sigma) * dhsdz;
-        if (C.tf) r = r + RLD(F.tfw, i, j, k);
-        if (on_cap(C, j, k, ny)) { const R b = RLD(F.wb, i, j, k); r = r - R(C.cz) * sqrt(b * b) * wc; }
-        FIDX(F.Fw, i, j, k) = (double)r;
+        if (C.tf) r = r + AT(F.tfw, 0, 0, 0);
+        if (on_cap(C, j, k, ny)) { const R b = AT(F.wb, 0, 0, 0); r = r - R(C.cz) * sqrt(b * b) * wc; }
+        F.Fw[c0] = (double)r;
     }
+#undef AT
 }
 
 // ------------------------------------------------------------------------------------

@@ -104,6 +104,7 @@ int sync_read(suli_ctx* c, const void* dev, void* host, size_t bytes) {
 
 int validate(const suli_params* p, std::string& why) {
     if (p->nx < 4 || p->ny < 4 || p->nz < 4) { why = "nx, ny, nz must be >= 4 (WENO stencil)"; return SULI_ERR_ARG; }
+    if (make_geo(p->nx, p->ny, p->nz).n >= (1LL << 31)) { why = "a field of this grid exceeds 2^31 elements"; return SULI_ERR_SIZE; }
     if (!(p->dx > 0 && p->dy > 0 && p->dz > 0)) { why = "dx, dy, dz must be positive"; return SULI_ERR_ARG; }
     if ((p->ccx0 == 0) != (p->ccxf == 0)) { why = "periodic x needs ccx0 = ccxf = 0 (0_modules.f90:56)"; return SULI_ERR_ARG; }
     if ((p->ccy0 == 0) != (p->ccyf == 0)) { why = "periodic y needs ccy0 = ccyf = 0"; return SULI_ERR_ARG; }
