@@ -115,7 +115,6 @@ struct suli_ctx {
     bool tf_active = false;             // tf_u/v/w uploaded non-zero
     int last_reinit_iters = 0;
     int last_volfix_iters = 0;
-    int cg_batch = 16;
     // mixed-precision solve (precision = 1)
     std::vector<suli::MGLevel> mg;
     float *pc_x = nullptr, *pc_r = nullptr, *pc_pa = nullptr, *pc_pb = nullptr, *pc_q = nullptr;
@@ -133,6 +132,7 @@ struct suli_ctx {
     // the inner PCG loop as one graph: a WHILE node repeats two iterations (ping-pong) and a
     // kernel that clears the condition once the inner solve is done
     cudaGraphExec_t pcg_loop = nullptr;
+    cudaGraphExec_t cg_loop = nullptr;   // the plain FP64 CG iterations as one device-side loop
     int pcg_graph_kernels = 0;   // kernels of one inner iteration
     // learned initial guess (suli_attach_nn) and training-pair recording (suli_graddin_record)
     suli_nn* nn = nullptr;
@@ -219,6 +219,7 @@ void launch_tempo(suli_ctx* c, int tt, int it);
 void launch_contorno(suli_ctx* c, int nlock);
 void launch_cg_setup(suli_ctx* c);
 void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new);
+void launch_cg_cond(suli_ctx* c, cudaGraphConditionalHandle h);
 void launch_cg_final(suli_ctx* c, const double* e);
 // ---- mixed-precision solve (k_mixed.cu) ----
 void launch_mx_setup(suli_ctx* c);

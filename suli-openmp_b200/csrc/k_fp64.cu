@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <cmath>
 #include "ctx.cuh"
+#include "pdl.cuh"
 #include "reduce.cuh"
 #include "weno.cuh"
 
@@ -836,6 +837,7 @@ __global__ void __launch_bounds__(kTX * kTY) k_cg_spmv(Geo G, BC bc, const doubl
                                                        double* __restrict__ q, const double* __restrict__ ax,
                                                        const double* __restrict__ ay, const double* __restrict__ az,
                                                        CGState* st, double* partial, unsigned int* counter) {
+    pdl_wait();
     if (st->done) return;
     const double beta = st->beta;
     const int nx = G.nx, ny = G.ny, nz = G.nz, px = G.px, pxy = (int)G.pxy;
@@ -886,6 +888,7 @@ __global__ void __launch_bounds__(kTX * kTY) k_cg_spmv(Geo G, BC bc, const doubl
 __global__ void __launch_bounds__(kTX * kTY) k_cg_update(Geo G, double* __restrict__ e, double* __restrict__ r,
                                                          const double* __restrict__ p, const double* __restrict__ q,
                                                          CGState* st, double* partial, unsigned int* counter) {
+    pdl_wait();
     if (st->done) return;
     const double alpha = st->alpha;
     const int i = blockIdx.x * kTX + threadIdx.x + 1, j = blockIdx.y * kTY + threadIdx.y + 1;
@@ -916,6 +919,12 @@ __global__ void __launch_bounds__(kTX * kTY) k_cg_update(Geo G, double* __restri
         if (!isfinite(trr)) { go = false; st->status = SULI_ERR_NAN; }
         st->done = go ? 0 : 1;
     }
+}
+
+// loop condition of the CG iteration graph: repeat until the state says done
+__global__ void k_cg_cond(cudaGraphConditionalHandle h, const CGState* st) {
+    pdl_wait();
+    cudaGraphSetConditional(h, st->done ? 0u : 1u);
 }
 
 // de-normalisation over the halo box (:268-274)
@@ -1157,12 +1166,15 @@ void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new) {
     const dim3 gb((G.nx + kTX - 1) / kTX, (G.ny + kTY - 1) / kTY, (G.nz + kCGZB - 1) / kCGZB);
     {
         ProfScope ps(c, SULI_K_CG_SPMV, 1);
-        k_cg_spmv<<<ga, b, 0, c->stream>>>(G, c->bc, c->cg_r, p_old, p_new, c->cg_q, c->cg_ax, c->cg_ay, c->cg_az, c->cg,
-                                           c->red_partial, c->red_counter);
+        pdl_launch(k_cg_spmv, ga, b, c->stream, G, c->bc, (const double*)c->cg_r, p_old, p_new, c->cg_q,
+                   (const double*)c->cg_ax, (const double*)c->cg_ay, (const double*)c->cg_az, c->cg, c->red_partial,
+                   c->red_counter);
     }
     ProfScope ps(c, SULI_K_CG_UPDATE, 1);
-    k_cg_update<<<gb, b, 0, c->stream>>>(G, c->cg_e, c->cg_r, p_new, c->cg_q, c->cg, c->red_partial, c->red_counter);
+    pdl_launch(k_cg_update, gb, b, c->stream, G, c->cg_e, c->cg_r, (const double*)p_new, (const double*)c->cg_q, c->cg,
+               c->red_partial, c->red_counter);
 }
+void launch_cg_cond(suli_ctx* c, cudaGraphConditionalHandle h) { pdl_launch(k_cg_cond, 1, 1, c->stream, h, c->cg); }
 void launch_cg_final(suli_ctx* c, const double* e) {
     const Geo& G = c->g;
     ProfScope ps(c, SULI_K_CG_FINAL, 1);

@@ -15,15 +15,14 @@
 #include <cuda_runtime.h>
 #include <cmath>
 #include "ctx.cuh"
+#include "pdl.cuh"
 #include "reduce.cuh"
 
 namespace suli {
 
 #define FI(a, i, j, k) (a)[G.idx((i), (j), (k))]
 
-// Programmatic dependent launch: the inner-solve kernels are launched while their predecessor is
-// still running and wait here, before reading anything it wrote (a no-op for a plain launch).
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 
 __device__ __forceinline__ int clampi_m(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -547,21 +546,6 @@ namespace suli {
 // ------------------------------------------------------------------------------------
 static const dim3 kB2(32, 8, 1);
 
-// launch with programmatic stream serialisation (the kernel calls pdl_wait before its loads)
-template <typename... KArgs, typename... Args>
-static void pdl_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t stream, Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
-}
 static inline dim3 cells3(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
 static inline OpStored stored(const MGLevel& L) { return OpStored{L.sx, L.sy, L.sz, L.idg}; }
 static inline OpRho from_rho(const MGLevel& L) { return OpRho{L.rho, L.idg, L.c2}; }

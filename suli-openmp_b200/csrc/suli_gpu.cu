@@ -283,6 +283,7 @@ int suli_destroy(suli_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->cg_graph) cudaGraphExecDestroy(c->cg_graph);
     if (c->pcg_loop) cudaGraphExecDestroy(c->pcg_loop);
+    if (c->cg_loop) cudaGraphExecDestroy(c->cg_loop);
     for (auto& e : c->prof.ev) cudaEventDestroy(e);
     cudaFree(c->arena);
     for (int f = SULI_F_BXX0; f < SULI_F_COUNT; ++f) cudaFree(c->f[f]);
@@ -566,58 +567,14 @@ int suli_contorno(suli_ctx* c, int nlock) {
 }  // extern "C"
 
 namespace {
-// Enqueue iterations in batches with a device-resident `done` flag: launches after
-// convergence return at once, and the host polls the flag through a pinned mirror one batch
-// behind the GPU, so the stream never drains while it waits.  `launch(parity)` enqueues one
-// iteration; iteration 0 is launched by the caller.
-template <class State, class Launch>
-int run_batches(suli_ctx* c, const State* dev, State* host2, long long cap, int batch, Launch launch) {
-    long long issued = 1;
-    int parity = 0;
-    int slot = 0;
-    cudaEvent_t ev[2];
-    cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
-    bool pending[2] = {false, false};
-    bool finished = false;
-    while (!finished) {
-        for (int b = 0; b < batch && issued < cap; ++b, ++issued) {
-            launch(parity);
-            parity ^= 1;
-        }
-        CHECK_LAUNCH(c);
-        cudaMemcpyAsync(&host2[slot], dev, sizeof(State), cudaMemcpyDeviceToHost, c->stream);
-        cudaEventRecord(ev[slot], c->stream);
-        pending[slot] = true;
-        const int prev = slot ^ 1;
-        if (pending[prev]) {
-            cudaEventSynchronize(ev[prev]);
-            pending[prev] = false;
-            if (host2[prev].done) finished = true;
-        }
-        if (issued >= cap) {
-            cudaEventSynchronize(ev[slot]);
-            pending[slot] = false;
-            finished = true;
-        }
-        slot = prev;
-    }
-    for (int s = 0; s < 2; ++s) {
-        if (pending[s]) cudaEventSynchronize(ev[s]);
-        cudaEventDestroy(ev[s]);
-    }
-    CHECK_LAUNCH(c);
-    return SULI_OK;
-}
-
-// The inner PCG loop as one graph launch: a WHILE conditional node whose body is two inner
-// iterations (p ping-pongs between pa and pb; every kernel reads its scalars from device
-// memory, so the captured parameters never change) and k_pcg_cond, which clears the condition
-// once the inner solve has converged or hit its cap.  The GPU iterates without host round trips,
-// and no iteration is launched after convergence except the rest of the last body (kernels that
-// return at once).
-int ensure_pcg_loop(suli_ctx* c) {
-    if (c->pcg_loop) return SULI_OK;
+// A solver's iterations as one graph launch: a WHILE conditional node whose body is two
+// iterations (the direction vector ping-pongs between two buffers; every kernel reads its
+// scalars from device memory, so the captured parameters never change) and a kernel that clears
+// the condition once the solve has converged or hit its cap.  The GPU iterates without host
+// round trips, and no iteration is launched after convergence except the rest of the last body
+// (kernels that return at once).
+template <class Body, class Cond>
+int make_loop_graph(suli_ctx* c, cudaGraphExec_t* out, Body body, Cond cond, const char* what) {
     cudaGraph_t g = nullptr;
     CUDA_TRY(c, cudaGraphCreate(&g, 0));
     cudaGraphConditionalHandle h;
@@ -632,20 +589,45 @@ int ensure_pcg_loop(suli_ctx* c) {
         e = cudaStreamBeginCaptureToGraph(c->stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                           cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        launch_pcg_iter(c, c->pc_pa, c->pc_pb);
-        launch_pcg_iter(c, c->pc_pb, c->pc_pa);
-        launch_pcg_cond(c, h);
-        cudaGraph_t body = nullptr;
-        e = cudaStreamEndCapture(c->stream, &body);
+        body();
+        cond(h);
+        cudaGraph_t captured = nullptr;
+        e = cudaStreamEndCapture(c->stream, &captured);
     }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&c->pcg_loop, g, 0);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        return fail(c, SULI_ERR_CUDA, std::string("inner-solve graph: ") + cudaGetErrorString(e));
+        return fail(c, SULI_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
     }
+    return SULI_OK;
+}
+
+// the inner FP32 PCG of the mixed path
+int ensure_pcg_loop(suli_ctx* c) {
+    if (c->pcg_loop) return SULI_OK;
+    if (int r = make_loop_graph(
+            c, &c->pcg_loop,
+            [&] {
+                launch_pcg_iter(c, c->pc_pa, c->pc_pb);
+                launch_pcg_iter(c, c->pc_pb, c->pc_pa);
+            },
+            [&](cudaGraphConditionalHandle h) { launch_pcg_cond(c, h); }, "inner-solve graph"))
+        return r;
     c->pcg_graph_kernels = 2 + vcycle_kernels(c);
     return SULI_OK;
+}
+
+// the plain FP64 CG
+int ensure_cg_loop(suli_ctx* c) {
+    if (c->cg_loop) return SULI_OK;
+    return make_loop_graph(
+        c, &c->cg_loop,
+        [&] {
+            launch_cg_iter(c, c->cg_pa, c->cg_pb);
+            launch_cg_iter(c, c->cg_pb, c->cg_pa);
+        },
+        [&](cudaGraphConditionalHandle h) { launch_cg_cond(c, h); }, "CG graph");
 }
 
 // Mixed-precision solve: FP64 refinement around an FP32 multigrid-preconditioned CG.
@@ -741,17 +723,17 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
     if (!c) return SULI_ERR_ARG;
     cudaSetDevice(c->device);
     if (c->P.precision == 1) return graddin_mixed(c, iters, resid);
+    if (int rg = ensure_cg_loop(c)) return rg;
     launch_cg_setup(c);
     nn_begin(c);   // recording only: the learned guess needs the refinement loop
     CHECK_LAUNCH(c);
-    // iteration 1 uses p_old = r with beta = 0 (erroppr = erropr, :172)
+    // iteration 1 uses p_old = r with beta = 0 (erroppr = erropr, :172); then the device loop
     launch_cg_iter(c, c->cg_r, c->cg_pa);
+    {
+        ProfScope ps(c, SULI_K_CG_SPMV, 0);   // kernel launches are counted below, once known
+        CUDA_TRY(c, cudaGraphLaunch(c->cg_loop, c->stream));
+    }
     CHECK_LAUNCH(c);
-    int r0 = run_batches(c, c->cg, c->cg_host, (long long)c->P.cg_maxit + 2, c->cg_batch, [&](int parity) {
-        if (parity == 0) launch_cg_iter(c, c->cg_pa, c->cg_pb);
-        else launch_cg_iter(c, c->cg_pb, c->cg_pa);
-    });
-    if (r0 != SULI_OK) return r0;
     launch_cg_final(c, c->cg_e);
     if (c->rec_in) launch_nn_target(c, c->cg_e, c->rec_target);
     CHECK_LAUNCH(c);
@@ -759,6 +741,11 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
     if (r != SULI_OK) return r;
     const CGState& s = c->cg_host[0];
     c->prof.cg_iters += s.iters;
+    {   // the loop ran ceil((iters - 1) / 2) two-iteration bodies (at least one)
+        const long long bodies = std::max(1, s.iters / 2);
+        c->prof.launches[SULI_K_CG_SPMV] += 2 * bodies;
+        c->prof.launches[SULI_K_CG_UPDATE] += 2 * bodies;
+    }
     if (iters) *iters = s.iters;
     if (resid) *resid = (s.bb > 0.) ? std::sqrt(s.rr / s.bb) : 0.;
     if (s.status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the Poisson solve");
