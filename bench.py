@@ -366,20 +366,20 @@ def cg_roofline(p, prof):
     bytes_upd = 8 * 6 * N
     n_it = max(prof["cg_iterations"], 1)
     t_it = (prof["cg_spmv"]["ms"] + prof["cg_update"]["ms"]) / n_it / 1e3
-    share = launch_share("launches_sloshing_256x128x128_fp64", "k_cg_spmv", ("k_cg_spmv", "k_cg_update"))
+    share = launch_share("launches_sloshing_256x128x128_fp64", "k_cg_spmv2", ("k_cg_spmv2", "k_cg_update"))
     peak, peak_kind = measured_peaks()
-    it = {"kernels": "k_cg_spmv + k_cg_update (one graph loop)", "bytes": bytes_spmv + bytes_upd, "us": t_it * 1e6,
+    it = {"kernels": "k_cg_spmv2 + k_cg_update (one graph loop)", "bytes": bytes_spmv + bytes_upd, "us": t_it * 1e6,
           "achieved_gbs": (bytes_spmv + bytes_upd) / t_it / 1e9,
           "frac": (bytes_spmv + bytes_upd) / t_it / 1e9 / peak}
     t_spmv = t_it * (share if share else 1.0)
     ach = bytes_spmv / t_spmv / 1e9
     return {
-        "kernel": "k_cg_spmv (FP64 CG kernel A: p = r + beta p, q = A p, p.q)",
+        "kernel": "k_cg_spmv2 (FP64 CG kernel A, two cells a thread: p = r + beta p, q = A p, p.q)",
         "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
-        "traffic": profiled_traffic("cg_spmv_256x128x128", N), "algorithmic_bytes_per_launch": bytes_spmv,
+        "traffic": profiled_traffic("cg_spmv2_256x128x128", N), "algorithmic_bytes_per_launch": bytes_spmv,
         "avg_launch_us": t_spmv * 1e6,
-        "duration": ("CUDA-event time of a CG iteration x k_cg_spmv's share of the two CG kernels in "
+        "duration": ("CUDA-event time of a CG iteration x k_cg_spmv2's share of the two CG kernels in "
                      "profiles/launches_sloshing_256x128x128_fp64.txt" if share else
                      "CUDA-event time of a whole CG iteration (no launch list to apportion it)"),
         "cg_iteration": it,

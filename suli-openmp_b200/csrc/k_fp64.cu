@@ -884,6 +884,67 @@ __global__ void __launch_bounds__(kTX * kTY) k_cg_spmv(Geo G, BC bc, const doubl
     }
 }
 
+// CG kernel A with two x cells a thread: every field row is read as 16-byte pairs (a warp moves
+// 512 contiguous bytes a load), the pair's inner x neighbours come from the pair itself and only
+// its two outer x neighbours are scalar loads.  Per cell the same expression as k_cg_spmv; only
+// the p.q partial sums are grouped differently.  Needs nx even.
+__global__ void __launch_bounds__(kTX * kTY) k_cg_spmv2(Geo G, BC bc, const double* __restrict__ r,
+                                                        const double* __restrict__ p_old, double* __restrict__ p_new,
+                                                        double* __restrict__ q, const double* __restrict__ ax,
+                                                        const double* __restrict__ ay, const double* __restrict__ az,
+                                                        CGState* st, double* partial, unsigned int* counter) {
+    pdl_wait();
+    if (st->done) return;
+    const double beta = st->beta;
+    const int nx = G.nx, ny = G.ny, nz = G.nz, px = G.px, pxy = (int)G.pxy;
+    const int i0 = 2 * (blockIdx.x * kTX + threadIdx.x) + 1, j = blockIdx.y * kTY + threadIdx.y + 1;
+    const int k0 = blockIdx.z * kCGZA + 1;
+    double dot = 0.;
+    if (i0 <= nx && j <= ny) {
+        const int oxm = (i0 > 1) ? -1 : (bc.perx ? nx - 1 : 0);            // of cell i0
+        const int oxp = (i0 + 1 < nx) ? 1 : (bc.perx ? -(nx - 1) : 0);     // of cell i0 + 1
+        const int oym = (j > 1) ? -px : (bc.pery ? (ny - 1) * px : 0);
+        const int oyp = (j < ny) ? px : (bc.pery ? -(ny - 1) * px : 0);
+        const int c0 = kBase + (i0 - 1) + px * j;
+        auto ld2 = [](const double* a, int c) { return *reinterpret_cast<const double2*>(a + c); };
+        auto pn2 = [&](int c) {
+            const double2 a = ld2(r, c), b = ld2(p_old, c);
+            return make_double2(a.x + beta * b.x, a.y + beta * b.y);
+        };
+        double2 col[kCGZA + 2];   // p of the pair at k0-1 .. k0+kCGZA
+#pragma unroll
+        for (int m = 0; m < kCGZA + 2; ++m) col[m] = pn2(c0 + pxy * map_any(k0 - 1 + m, nz, bc.perz));
+#pragma unroll
+        for (int m = 0; m < kCGZA; ++m) {
+            const int k = k0 + m;
+            if (k > nz) break;
+            const int c = c0 + pxy * k;
+            const double pxm = r[c + oxm] + beta * p_old[c + oxm];                 // left of cell i0
+            const double pxp = r[c + 1 + oxp] + beta * p_old[c + 1 + oxp];         // right of cell i0 + 1
+            const double2 pym = pn2(c + oym), pyp = pn2(c + oyp);
+            const double2 pc = col[m + 1], pzm = col[m], pzp = col[m + 2];
+            const double2 axc = ld2(ax, c), ayc = ld2(ay, c), ayp = ld2(ay, c + px), azc = ld2(az, c),
+                          azp = ld2(az, c + pxy);
+            const double ax2 = ax[c + 2];
+            const double q0 = pc.x - pc.y * axc.y - pxm * axc.x - pyp.x * ayp.x - pym.x * ayc.x - pzp.x * azp.x -
+                              pzm.x * azc.x;
+            const double q1 = pc.y - pxp * ax2 - pc.x * axc.y - pyp.y * ayp.y - pym.y * ayc.y - pzp.y * azp.y -
+                              pzm.y * azc.y;
+            *reinterpret_cast<double2*>(q + c) = make_double2(q0, q1);
+            *reinterpret_cast<double2*>(p_new + c) = pc;
+            dot += pc.x * q0;
+            dot += pc.y * q1;
+        }
+    }
+    double tpq, tdum;
+    if (reduce2_last(dot, 0.0, partial, counter, tpq, tdum) && flat_tid() == 0) {
+        st->rr_start = st->rr;
+        st->pq = tpq;
+        st->alpha = st->rr / tpq;
+        if (!isfinite(st->alpha)) { st->status = SULI_ERR_NAN; st->done = 1; }
+    }
+}
+
 // CG kernel B: e -= alpha p, r -= alpha q, reduction of r.r, beta and the stopping test (:210-221, :175)
 __global__ void __launch_bounds__(kTX * kTY) k_cg_update(Geo G, double* __restrict__ e, double* __restrict__ r,
                                                          const double* __restrict__ p, const double* __restrict__ q,
@@ -1166,9 +1227,16 @@ void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new) {
     const dim3 gb((G.nx + kTX - 1) / kTX, (G.ny + kTY - 1) / kTY, (G.nz + kCGZB - 1) / kCGZB);
     {
         ProfScope ps(c, SULI_K_CG_SPMV, 1);
-        pdl_launch(k_cg_spmv, ga, b, c->stream, G, c->bc, (const double*)c->cg_r, p_old, p_new, c->cg_q,
-                   (const double*)c->cg_ax, (const double*)c->cg_ay, (const double*)c->cg_az, c->cg, c->red_partial,
-                   c->red_counter);
+        if (G.nx % 2 == 0) {
+            const dim3 g2((G.nx / 2 + kTX - 1) / kTX, (G.ny + kTY - 1) / kTY, (G.nz + kCGZA - 1) / kCGZA);
+            pdl_launch(k_cg_spmv2, g2, b, c->stream, G, c->bc, (const double*)c->cg_r, p_old, p_new, c->cg_q,
+                       (const double*)c->cg_ax, (const double*)c->cg_ay, (const double*)c->cg_az, c->cg,
+                       c->red_partial, c->red_counter);
+        } else {
+            pdl_launch(k_cg_spmv, ga, b, c->stream, G, c->bc, (const double*)c->cg_r, p_old, p_new, c->cg_q,
+                       (const double*)c->cg_ax, (const double*)c->cg_ay, (const double*)c->cg_az, c->cg,
+                       c->red_partial, c->red_counter);
+        }
     }
     ProfScope ps(c, SULI_K_CG_UPDATE, 1);
     pdl_launch(k_cg_update, gb, b, c->stream, G, c->cg_e, c->cg_r, (const double*)p_new, (const double*)c->cg_q, c->cg,
