@@ -106,7 +106,7 @@ __device__ __forceinline__ void apply4(const Faces (&F)[kVX], const float (&xc)[
 
 // two damped Jacobi sweeps from zero (k_mg_pre): x1 = w f/dg, y = x1 + w (f - A x1)/dg
 template <class Op4>
-__global__ void __launch_bounds__(256) k_mgv_pre(Geo G, BC bc, const float* __restrict__ f, Op4 A,
+__global__ void __launch_bounds__(256, 3) k_mgv_pre(Geo G, BC bc, const float* __restrict__ f, Op4 A,
                                                  float* __restrict__ y, float omega, const PCGState* st) {
     pdl_wait();
     if (st->done) return;
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(256) k_mgv_pre(Geo G, BC bc, const float* __re
 
 // x_out = x_in + w (f - A x_in)/dg; with do_dot also f.x_out -> rz, beta (k_mg_jacc)
 template <class Op4>
-__global__ void __launch_bounds__(256) k_mgv_jacc(Geo G, BC bc, const float* __restrict__ xin,
+__global__ void __launch_bounds__(256, 3) k_mgv_jacc(Geo G, BC bc, const float* __restrict__ xin,
                                                   const float* __restrict__ f, Op4 A, float* __restrict__ xout,
                                                   float omega, PCGState* st, int do_dot, double* partial,
                                                   unsigned int* counter) {
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(256) k_mgv_jacc(Geo G, BC bc, const float* __r
 
 // x_out = x' + w (f - A x')/dg with x' = y + a P xc (k_mg_post)
 template <class Op4>
-__global__ void __launch_bounds__(256) k_mgv_post(Geo Gf, Geo Gc, BC bc, const float* __restrict__ y,
+__global__ void __launch_bounds__(256, 3) k_mgv_post(Geo Gf, Geo Gc, BC bc, const float* __restrict__ y,
                                                   const float* __restrict__ xc, const float* __restrict__ f, Op4 A,
                                                   float* __restrict__ xout, float omega, float alpha,
                                                   const PCGState* st) {
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(256) k_mgv_post(Geo Gf, Geo Gc, BC bc, const f
 // f_c = (1/8) sum over the 8 children of (f - A x) (k_mg_restrict); a thread makes the two coarse
 // cells whose children are one fine quad, in the children order (x, y, z) of the one-cell kernel
 template <class Op4>
-__global__ void __launch_bounds__(256) k_mgv_restrict(Geo Gf, Geo Gc, BC bc, const float* __restrict__ x,
+__global__ void __launch_bounds__(256, 3) k_mgv_restrict(Geo Gf, Geo Gc, BC bc, const float* __restrict__ x,
                                                       const float* __restrict__ f, Op4 A, float* fc,
                                                       const PCGState* st) {
     pdl_wait();
@@ -280,7 +280,7 @@ static inline dim3 vgrid_restrict(const Geo& gc) { return dim3((gc.nx / 2 + 31) 
 
 // p = z + beta p_old (also at the neighbours), q = A p, p.q -> alpha (k_pcg_spmvc)
 template <class Op4>
-__global__ void __launch_bounds__(256) k_pcgv_spmvc(Geo G, BC bc, const float* __restrict__ z,
+__global__ void __launch_bounds__(256, 3) k_pcgv_spmvc(Geo G, BC bc, const float* __restrict__ z,
                                                     const float* __restrict__ p_old, float* __restrict__ p_new,
                                                     float* __restrict__ qv, Op4 A, PCGState* st, double* partial,
                                                     unsigned int* counter) {
