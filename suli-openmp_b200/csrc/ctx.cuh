@@ -137,7 +137,7 @@ struct suli_ctx {
     // learned initial guess (suli_attach_nn) and training-pair recording (suli_graddin_record)
     suli_nn* nn = nullptr;
     int nn_mode = 0;
-    float *nn_in = nullptr, *nn_out = nullptr;   // [V][3], [V]
+    float* nn_out = nullptr;   // the network's output [V]
     double* nn_e0 = nullptr;                     // e0 of a recorded solve (box layout)
     suli::NNScale* nn_scale = nullptr;
     float *rec_in = nullptr, *rec_target = nullptr;
@@ -230,6 +230,7 @@ void launch_pcg_cond(suli_ctx* c, cudaGraphConditionalHandle h);
 void launch_vcycle(suli_ctx* c);
 // ---- learned initial guess (k_learned.cu) ----
 void launch_nn_features(suli_ctx* c, float* in3);
+void launch_nn_features16(suli_ctx* c, void* in16);
 void launch_nn_step(suli_ctx* c, const float* out, double* e);
 void launch_nn_target(suli_ctx* c, const double* e_star, float* target);
 void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new);

@@ -10,6 +10,7 @@
 //             and neither the step nor the solution depends on it.
 // Cells are enumerated v = (i-1) + nx ((j-1) + ny (k-1)).  All sums are FP64 block partials
 // finished by the last block.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cmath>
 #include "ctx.cuh"
@@ -48,6 +49,17 @@ __global__ void __launch_bounds__(256) k_nn_stats(Geo G, const double* __restric
     }
 }
 
+// the three features of cell c (FP32, as the network's input receives them)
+struct Feat3 {
+    float r, h, e;
+};
+__device__ __forceinline__ Feat3 features_at(const double* r, const double* e, const double* rho, double rho1,
+                                             double rho2, const NNScale* sc, long long c) {
+    const double sr = sc->sigma_r, se = sc->sigma_e;
+    const double h = (rho2 != rho1) ? (rho[c] - rho1) / (rho2 - rho1) : 0.;
+    return Feat3{sc->active ? (float)(r[c] / sr) : 0.f, (float)h, se > 0. ? (float)((e[c] - sc->mean_e) / se) : 0.f};
+}
+// FP32 [V][3] (recorded training inputs, suli_nn_forward's input format)
 __global__ void __launch_bounds__(256) k_nn_features(Geo G, const double* __restrict__ r, const double* __restrict__ e,
                                                      const double* __restrict__ rho, double rho1, double rho2,
                                                      const NNScale* __restrict__ sc, float* __restrict__ in3) {
@@ -55,38 +67,54 @@ __global__ void __launch_bounds__(256) k_nn_features(Geo G, const double* __rest
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z + 1;
     if (i > G.nx || j > G.ny || k > G.nz) return;
-    const long long c = G.idx(i, j, k), v = cell_v(G, i, j, k);
-    const double sr = sc->sigma_r, se = sc->sigma_e;
-    const double h = (rho2 != rho1) ? (rho[c] - rho1) / (rho2 - rho1) : 0.;
-    in3[3 * v + 0] = sc->active ? (float)(r[c] / sr) : 0.f;
-    in3[3 * v + 1] = (float)h;
-    in3[3 * v + 2] = se > 0. ? (float)((e[c] - sc->mean_e) / se) : 0.f;
+    const long long v = cell_v(G, i, j, k);
+    const Feat3 f = features_at(r, e, rho, rho1, rho2, sc, G.idx(i, j, k));
+    in3[3 * v + 0] = f.r;
+    in3[3 * v + 1] = f.h;
+    in3[3 * v + 2] = f.e;
 }
-
-// y into the box layout (FP64), so the operator can read its neighbours
-__global__ void __launch_bounds__(256) k_nn_scatter(Geo G, const float* __restrict__ out, double* __restrict__ y) {
+// the network's own input layout, BF16 [V][16] with channels 3-15 zero: the same values the
+// network's packing of the FP32 features produces, written once
+__global__ void __launch_bounds__(256) k_nn_features16(Geo G, const double* __restrict__ r,
+                                                       const double* __restrict__ e, const double* __restrict__ rho,
+                                                       double rho1, double rho2, const NNScale* __restrict__ sc,
+                                                       __nv_bfloat16* __restrict__ in16) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z + 1;
     if (i > G.nx || j > G.ny || k > G.nz) return;
-    y[G.idx(i, j, k)] = (double)out[cell_v(G, i, j, k)];
+    const long long v = cell_v(G, i, j, k);
+    const Feat3 f = features_at(r, e, rho, rho1, rho2, sc, G.idx(i, j, k));
+    __nv_bfloat16 t[16];
+    t[0] = __float2bfloat16(f.r);
+    t[1] = __float2bfloat16(f.h);
+    t[2] = __float2bfloat16(f.e);
+#pragma unroll
+    for (int ch = 3; ch < 16; ++ch) t[ch] = __float2bfloat16(0.f);
+    uint4* o = reinterpret_cast<uint4*>(in16 + v * 16);
+    o[0] = *reinterpret_cast<const uint4*>(&t[0]);
+    o[1] = *reinterpret_cast<const uint4*>(&t[8]);
 }
 
-// r.y and y.A~y with A~ the set-up's scaled operator (ghost rules as the refinement residual)
-__global__ void __launch_bounds__(256) k_nn_dots(Geo G, BC bc, const double* __restrict__ y, const double* __restrict__ r,
-                                                 const double* __restrict__ ax, const double* __restrict__ ay,
-                                                 const double* __restrict__ az, NNScale* sc, double* partial,
-                                                 unsigned int* counter) {
+// r.y and y.A~y with A~ the set-up's scaled operator (ghost rules as the refinement residual);
+// y is the network output, read in place at the ghost-mapped neighbours
+__global__ void __launch_bounds__(256) k_nn_dots(Geo G, BC bc, const float* __restrict__ out,
+                                                 const double* __restrict__ r, const double* __restrict__ ax,
+                                                 const double* __restrict__ ay, const double* __restrict__ az,
+                                                 NNScale* sc, double* partial, unsigned int* counter) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z + 1;
     double ry = 0., yay = 0.;
     if (i <= G.nx && j <= G.ny && k <= G.nz) {
         const int c = (int)G.idx(i, j, k);
-        const Nb o = neighbours(G, bc, i, j, k);
-        const double yc = y[c];
-        const double ayv = yc - ax[c + 1] * y[c + o.xp] - ax[c] * y[c + o.xm] - ay[c + G.px] * y[c + o.yp] -
-                           ay[c] * y[c + o.ym] - az[c + (int)G.pxy] * y[c + o.zp] - az[c] * y[c + o.zm];
+        auto y = [&](int ii, int jj, int kk) {
+            return (double)out[cell_v(G, map_any(ii, G.nx, bc.perx), map_any(jj, G.ny, bc.pery),
+                                      map_any(kk, G.nz, bc.perz))];
+        };
+        const double yc = y(i, j, k);
+        const double ayv = yc - ax[c + 1] * y(i + 1, j, k) - ax[c] * y(i - 1, j, k) - ay[c + G.px] * y(i, j + 1, k) -
+                           ay[c] * y(i, j - 1, k) - az[c + (int)G.pxy] * y(i, j, k + 1) - az[c] * y(i, j, k - 1);
         ry = r[c] * yc;
         yay = yc * ayv;
     }
@@ -97,7 +125,7 @@ __global__ void __launch_bounds__(256) k_nn_dots(Geo G, BC bc, const double* __r
     }
 }
 
-__global__ void __launch_bounds__(256) k_nn_apply(Geo G, const double* __restrict__ y, const NNScale* __restrict__ sc,
+__global__ void __launch_bounds__(256) k_nn_apply(Geo G, const float* __restrict__ out, const NNScale* __restrict__ sc,
                                                   double* __restrict__ e) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -106,7 +134,7 @@ __global__ void __launch_bounds__(256) k_nn_apply(Geo G, const double* __restric
     const double a = sc->alpha;
     if (a == 0.) return;
     const long long c = G.idx(i, j, k);
-    e[c] += a * y[c];
+    e[c] += a * (double)out[cell_v(G, i, j, k)];
 }
 
 // n.(e* - e0) and n.n with n = sqrt(d) -> the projection coefficient
@@ -149,13 +177,19 @@ void launch_nn_features(suli_ctx* c, float* in3) {
                                                          c->P.rho_f2, c->nn_scale, in3);
 }
 
+void launch_nn_features16(suli_ctx* c, void* in16) {
+    const Geo& G = c->g;
+    k_nn_stats<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_e, c->cg, c->nn_scale, c->red_partial, c->red_counter);
+    k_nn_features16<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_r, c->cg_e, c->f[SULI_F_RHO], c->P.rho_f1,
+                                                           c->P.rho_f2, c->nn_scale,
+                                                           static_cast<__nv_bfloat16*>(in16));
+}
+
 void launch_nn_step(suli_ctx* c, const float* out, double* e) {
     const Geo& G = c->g;
-    double* y = c->cg_pa;   // free during the mixed solve's set-up
-    k_nn_scatter<<<grid_cells(G), kBL, 0, c->stream>>>(G, out, y);
-    k_nn_dots<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->bc, y, c->cg_r, c->cg_ax, c->cg_ay, c->cg_az, c->nn_scale,
+    k_nn_dots<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->bc, out, c->cg_r, c->cg_ax, c->cg_ay, c->cg_az, c->nn_scale,
                                                       c->red_partial, c->red_counter);
-    k_nn_apply<<<grid_cells(G), kBL, 0, c->stream>>>(G, y, c->nn_scale, e);
+    k_nn_apply<<<grid_cells(G), kBL, 0, c->stream>>>(G, out, c->nn_scale, e);
 }
 
 void launch_nn_target(suli_ctx* c, const double* e_star, float* target) {

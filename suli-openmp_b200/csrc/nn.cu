@@ -672,6 +672,14 @@ int forward_on(suli_nn* N, cudaStream_t stream, const float* d_in3, float* d_out
     N->stream = own;
     return n;
 }
+void* input16(suli_nn* N) { return N->in0; }
+int forward_packed_on(suli_nn* N, cudaStream_t stream, float* d_out) {
+    const cudaStream_t own = N->stream;
+    N->stream = stream;
+    const int n = forward(N, d_out, false);
+    N->stream = own;
+    return n;
+}
 int take_error(suli_nn* N) {
     int flag = 0;
     if (cudaMemcpy(&flag, N->err_flag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;

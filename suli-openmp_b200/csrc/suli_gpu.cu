@@ -294,7 +294,6 @@ int suli_destroy(suli_ctx* c) {
     cudaFree(c->f32_arena);
     cudaFree(c->cg_e2);
     cudaFree(c->pcg);
-    cudaFree(c->nn_in);
     cudaFree(c->nn_out);
     cudaFree(c->nn_e0);
     cudaFree(c->nn_scale);
@@ -636,7 +635,6 @@ int ensure_nn_buffers(suli_ctx* c, bool net) {
     const long long V = (long long)c->P.nx * c->P.ny * c->P.nz;
     if (!c->nn_scale) CUDA_TRY(c, cudaMalloc(&c->nn_scale, sizeof(NNScale)));
     if (!c->nn_e0) CUDA_TRY(c, cudaMalloc(&c->nn_e0, c->g.n * sizeof(double)));
-    if (net && !c->nn_in) CUDA_TRY(c, cudaMalloc(&c->nn_in, V * 3 * sizeof(float)));
     if (net && !c->nn_out) CUDA_TRY(c, cudaMalloc(&c->nn_out, V * sizeof(float)));
     return SULI_OK;
 }
@@ -646,19 +644,23 @@ void nn_begin(suli_ctx* c) {
     const bool rec = c->rec_in != nullptr;
     const bool learn = !rec && c->nn && c->nn_mode == 1;
     if (!rec && !learn) return;
-    {
-        ProfScope ps(c, SULI_K_CG_SETUP, 2);
-        launch_nn_features(c, rec ? c->rec_in : c->nn_in);
-    }
     if (rec) {
+        {
+            ProfScope ps(c, SULI_K_CG_SETUP, 2);
+            launch_nn_features(c, c->rec_in);
+        }
         cudaMemcpyAsync(c->nn_e0, c->cg_e, c->g.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
         return;
     }
+    {   // the features go straight into the network's BF16 input
+        ProfScope ps(c, SULI_K_CG_SETUP, 2);
+        launch_nn_features16(c, suli::nn::input16(c->nn));
+    }
     {
         ProfScope ps(c, SULI_K_NN, 0);
-        c->prof.launches[SULI_K_NN] += suli::nn::forward_on(c->nn, c->stream, c->nn_in, c->nn_out);
+        c->prof.launches[SULI_K_NN] += suli::nn::forward_packed_on(c->nn, c->stream, c->nn_out);
     }
-    ProfScope ps(c, SULI_K_CG_SETUP, 3);
+    ProfScope ps(c, SULI_K_CG_SETUP, 2);
     launch_nn_step(c, c->nn_out, c->cg_e);
 }
 
