@@ -517,6 +517,56 @@ __global__ void __launch_bounds__(256) k_mx_outer(Geo G, BC bc, const double* __
     }
 }
 
+// k_mx_outer with two x cells a thread (16-byte row loads; needs nx even): per cell the same
+// expressions, only the two reductions group their terms differently
+__global__ void __launch_bounds__(256) k_mx_outer2(Geo G, BC bc, const double* __restrict__ e_in,
+                                                   const float* __restrict__ dp, const double* __restrict__ sd,
+                                                   const double* __restrict__ ax, const double* __restrict__ ay,
+                                                   const double* __restrict__ az, const double* __restrict__ b,
+                                                   double* __restrict__ e_out, float* __restrict__ ru, int apply,
+                                                   CGState* cg, PCGState* pst, double* partial, unsigned int* counter) {
+    const int i0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    double rr = 0., ru2 = 0.;
+    if (i0 <= G.nx && j <= G.ny && k <= G.nz) {
+        const int c = (int)G.idx(i0, j, k), px = G.px, pxy = (int)G.pxy;
+        const Nb o0 = neighbours(G, bc, i0, j, k), o1 = neighbours(G, bc, i0 + 1, j, k);
+        auto en = [&](int cc) { return apply ? e_in[cc] - sd[cc] * (double)dp[cc] : e_in[cc]; };
+        auto en2 = [&](int cc) {
+            const double2 e = *reinterpret_cast<const double2*>(e_in + cc);
+            if (!apply) return e;
+            const double2 s2 = *reinterpret_cast<const double2*>(sd + cc);
+            const float2 d2 = *reinterpret_cast<const float2*>(dp + cc);
+            return make_double2(e.x - s2.x * (double)d2.x, e.y - s2.y * (double)d2.y);
+        };
+        auto ld2 = [](const double* a, int cc) { return *reinterpret_cast<const double2*>(a + cc); };
+        const double2 ec = en2(c), eym = en2(c + o0.ym), eyp = en2(c + o0.yp), ezm = en2(c + o0.zm),
+                      ezp = en2(c + o0.zp);
+        const double exm = en(c + o0.xm), exp_ = en(c + 1 + o1.xp);
+        const double2 axc = ld2(ax, c), ayc = ld2(ay, c), ayp = ld2(ay, c + px), azc = ld2(az, c),
+                      azp = ld2(az, c + pxy), bc2 = ld2(b, c), sdc = ld2(sd, c);
+        const double ax2 = ax[c + 2];
+        const double r0 = ec.x - axc.y * ec.y - axc.x * exm - ayp.x * eyp.x - ayc.x * eym.x - azp.x * ezp.x -
+                          azc.x * ezm.x - bc2.x;
+        const double r1 = ec.y - ax2 * exp_ - axc.y * ec.x - ayp.y * eyp.y - ayc.y * eym.y - azp.y * ezp.y -
+                          azc.y * ezm.y - bc2.y;
+        *reinterpret_cast<double2*>(e_out + c) = ec;
+        const double u0 = sdc.x * r0, u1 = sdc.y * r1;
+        *reinterpret_cast<float2*>(ru + c) = make_float2((float)u0, (float)u1);
+        rr = r0 * r0 + r1 * r1;
+        ru2 = u0 * u0 + u1 * u1;
+    }
+    double t1, t2;
+    if (reduce2_last(rr, ru2, partial, counter, t1, t2) && flat_tid() == 0) {
+        cg->rr = t1;
+        if (apply) cg->iters = cg->iters + 1;
+        cg->done = (t1 > cg->thr) ? 0 : 1;
+        if (!isfinite(t1)) { cg->status = SULI_ERR_NAN; cg->done = 1; }
+        pst->rr0 = t2;
+    }
+}
+
 __global__ void k_pcg_init(PCGState* st, double inner_tol, int maxit) {
     st->tol2 = inner_tol * inner_tol * st->rr0;
     st->iters = 0;
@@ -568,9 +618,16 @@ void launch_mx_setup(suli_ctx* c) {
 void launch_mx_residual(suli_ctx* c, const double* e_in, double* e_out, bool apply) {
     ProfScope ps(c, SULI_K_REFINE, 1);
     const Geo& G = c->g;
-    k_mx_outer<<<cells3(G), kB2, 0, c->stream>>>(G, c->bc, e_in, c->pc_x, c->cg_sd, c->cg_ax, c->cg_ay, c->cg_az,
-                                                 c->cg_b, e_out, c->pc_r, apply ? 1 : 0, c->cg, c->pcg,
-                                                 c->red_partial, c->red_counter);
+    if (G.nx % 2 == 0) {
+        const dim3 g2((G.nx / 2 + 31) / 32, (G.ny + 7) / 8, G.nz);
+        k_mx_outer2<<<g2, kB2, 0, c->stream>>>(G, c->bc, e_in, c->pc_x, c->cg_sd, c->cg_ax, c->cg_ay, c->cg_az,
+                                               c->cg_b, e_out, c->pc_r, apply ? 1 : 0, c->cg, c->pcg,
+                                               c->red_partial, c->red_counter);
+    } else {
+        k_mx_outer<<<cells3(G), kB2, 0, c->stream>>>(G, c->bc, e_in, c->pc_x, c->cg_sd, c->cg_ax, c->cg_ay, c->cg_az,
+                                                     c->cg_b, e_out, c->pc_r, apply ? 1 : 0, c->cg, c->pcg,
+                                                     c->red_partial, c->red_counter);
+    }
 }
 
 void launch_pcg_cond(suli_ctx* c, cudaGraphConditionalHandle h) { pdl_launch(k_pcg_cond, 1, 1, c->stream, h, c->pcg); }
