@@ -2,8 +2,10 @@
 // (4 levels, 16/32/64/96 channels, 3x3x3 convolutions, ReLU, 2x2x2 average pooling, nearest
 // upsampling with skip concatenation, 1x1x1 head), BF16 weights and activations, FP32
 // accumulation, FP32 master weights trained with Adam.  Forward convolutions and the
-// input-gradient (dgrad) convolutions run on the tensor cores (nn_conv.cuh); weight
-// gradients accumulate in FP32 on the CUDA cores.
+// input-gradient (dgrad) convolutions run on the tensor cores: by default the persistent
+// TMA + tcgen05 pipeline (nn_tp.cuh), which also computes the encoder's pooling and the head in
+// its epilogues; the one-tile tcgen05 kernel (nn_tc.cuh) and mma.sync (nn_conv.cuh) remain
+// selectable.  Weight gradients accumulate in FP32 on the CUDA cores.
 //
 // The network maps (residual r~0/s, density feature, previous pressure e0/s) to the scaled
 // correction (e* - e0)/s of the pressure solve, so it is both an initial guess
