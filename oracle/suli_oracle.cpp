@@ -571,11 +571,94 @@ static void interpz_cf(const Arr& a, int dimx, int dimy, int dimz, Arr& out) {
         }
 }
 
-/* visco — 5_viscosidade.f90:12-219 (m_turb 0 and 1). */
+/* face -> centre averages interp?_fc (8_derivadas.f90:331-349, 384-402, 438-455) along
+ * direction d (0 x, 1 y, 2 z): out has one point fewer than n[] along d. */
+static void interp_fc(const Arr& a, int d, const int n[3], Arr& out) {
+    const int ex = d == 0, ey = d == 1, ez = d == 2;
+    out.init(1, n[0] - ex, 1, n[1] - ey, 1, n[2] - ez);
+    for (int k = 1; k <= n[2] - ez; ++k)
+        for (int j = 1; j <= n[1] - ey; ++j)
+            for (int i = 1; i <= n[0] - ex; ++i) out(i, j, k) = (a(i, j, k) + a(i + ex, j + ey, k + ez)) * 0.5;
+}
+
+/* Derivatives of 8_derivadas.f90 along direction d of a field with one halo layer, over the
+ * points (1..n[0], 1..n[1], 1..n[2]):
+ *   deriva     centred (derivax/y/z, :1-68);
+ *   deriva_u2p second-order forward one-sided, centred on the last point (derivax/y/zu2p, :83-179);
+ *   deriva_u2n second-order backward one-sided, centred on the first point (derivax/y/zu2n,
+ *              :194-290). */
+static void deriva(const Arr& a, int d, const int n[3], double h, Arr& out) {
+    const int ex = d == 0, ey = d == 1, ez = d == 2;
+    out.init(1, n[0], 1, n[1], 1, n[2]);
+    for (int k = 1; k <= n[2]; ++k)
+        for (int j = 1; j <= n[1]; ++j)
+            for (int i = 1; i <= n[0]; ++i)
+                out(i, j, k) = (a(i + ex, j + ey, k + ez) - a(i - ex, j - ey, k - ez)) / (2. * h);
+}
+static void deriva_u2p(const Arr& a, int d, const int n[3], double h, Arr& out) {
+    const int ex = d == 0, ey = d == 1, ez = d == 2;
+    out.init(1, n[0], 1, n[1], 1, n[2]);
+    for (int k = 1; k <= n[2]; ++k)
+        for (int j = 1; j <= n[1]; ++j)
+            for (int i = 1; i <= n[0]; ++i) {
+                const int m = d == 0 ? i : (d == 1 ? j : k);
+                if (m < n[d])
+                    out(i, j, k) = 0.5 * (-a(i + 2 * ex, j + 2 * ey, k + 2 * ez) + 4. * a(i + ex, j + ey, k + ez) -
+                                          3. * a(i, j, k)) / h;
+                else
+                    out(i, j, k) = 0.5 * (a(i + ex, j + ey, k + ez) - a(i - ex, j - ey, k - ez)) / h;
+            }
+}
+static void deriva_u2n(const Arr& a, int d, const int n[3], double h, Arr& out) {
+    const int ex = d == 0, ey = d == 1, ez = d == 2;
+    out.init(1, n[0], 1, n[1], 1, n[2]);
+    for (int k = 1; k <= n[2]; ++k)
+        for (int j = 1; j <= n[1]; ++j)
+            for (int i = 1; i <= n[0]; ++i) {
+                const int m = d == 0 ? i : (d == 1 ? j : k);
+                if (m > 1)
+                    out(i, j, k) = 0.5 * (a(i - 2 * ex, j - 2 * ey, k - 2 * ez) - 4. * a(i - ex, j - ey, k - ez) +
+                                          3. * a(i, j, k)) / h;
+                else
+                    out(i, j, k) = 0.5 * (a(i + ex, j + ey, k + ez) - a(i - ex, j - ey, k - ez)) / h;
+            }
+}
+
+/* visco — 5_viscosidade.f90:12-219 (m_turb 0, 1 and 2). */
 void Oracle::visco() {
     Arr xa, ya, za;
     xa.init(1, nx1, 1, ny, 1, nz); ya.init(1, nx, 1, ny1, 1, nz); za.init(1, nx, 1, ny, 1, nz1);
-    if (P.m_turb == 1) {
+    if (P.m_turb == 2) {
+        /* directional Smagorinsky (:58-61, 104-164): each face's eddy viscosity from the strain
+           of its own velocity component, without the density factor; the cross derivatives go
+           face -> edge (interp?_cf, end copy) -> face (interp?_fc).  nut is not written. */
+        const int du[3] = {nx1, ny, nz}, dv[3] = {nx, ny1, nz}, dw[3] = {nx, ny, nz1};
+        Arr dudx_i, dudy_i, dudz_i, dvdx_i, dvdy_i, dvdz_i, dwdx_i, dwdy_i, dwdz_i;
+        deriva(u, 0, du, dx, dudx_i); deriva(v, 0, dv, dx, dvdx_i); deriva(w, 0, dw, dx, dwdx_i);
+        deriva(u, 1, du, dy, dudy_i); deriva(v, 1, dv, dy, dvdy_i); deriva(w, 1, dw, dy, dwdy_i);
+        deriva(u, 2, du, dz, dudz_i); deriva(v, 2, dv, dz, dvdz_i); deriva(w, 2, dw, dz, dwdz_i);
+        const int exy[3] = {nx1, ny1, nz}, exz[3] = {nx1, ny, nz1}, eyz[3] = {nx, ny1, nz1};
+        Arr t, dvdx_x, dwdx_x, dudy_y, dwdy_y, dudz_z, dvdz_z;
+        interpx_cf(dvdx_i, nx, ny1, nz, t);  interp_fc(t, 1, exy, dvdx_x);
+        interpx_cf(dwdx_i, nx, ny, nz1, t);  interp_fc(t, 2, exz, dwdx_x);
+        interpy_cf(dudy_i, nx1, ny, nz, t);  interp_fc(t, 0, exy, dudy_y);
+        interpy_cf(dwdy_i, nx, ny, nz1, t);  interp_fc(t, 2, eyz, dwdy_y);
+        interpz_cf(dudz_i, nx1, ny, nz, t);  interp_fc(t, 0, exz, dudz_z);
+        interpz_cf(dvdz_i, nx, ny1, nz, t);  interp_fc(t, 1, eyz, dvdz_z);
+        const double cs = P.csmag;
+        for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx1; ++i) {
+            const double p1 = dudx_i(i, j, k) + 0.5 * (dudy_i(i, j, k) + dvdx_x(i, j, k) + dudz_i(i, j, k) + dwdx_x(i, j, k));
+            xa(i, j, k) = dx * dx * cs * cs * std::sqrt(2. * p1 * p1);
+        }
+        for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny1; ++j) for (int i = 1; i <= nx; ++i) {
+            const double p1 = dvdy_i(i, j, k) + 0.5 * (dvdx_i(i, j, k) + dudy_y(i, j, k) + dvdz_i(i, j, k) + dwdy_y(i, j, k));
+            ya(i, j, k) = dy * dy * cs * cs * std::sqrt(2. * p1 * p1);
+        }
+        for (int k = 1; k <= nz1; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i) {
+            const double p1 = dwdz_i(i, j, k) + 0.5 * (dwdy_i(i, j, k) + dvdz_z(i, j, k) + dudz_z(i, j, k) + dwdx_i(i, j, k));
+            za(i, j, k) = dz * dz * cs * cs * std::sqrt(2. * p1 * p1);
+        }
+    } else if (P.m_turb == 1) {
         /* centred derivatives on the staggered grids (derivax/y/z, 8_derivadas.f90:1-68)
            then face -> centre averages (interp?_fc); fused per cell here, same arithmetic */
         const double cdel = std::pow(dx * dy * dz, 2. / 3.);
@@ -625,8 +708,55 @@ void Oracle::visco() {
         znut(i, j, k) = lz(i, j, k) + za(i, j, k);
 }
 
-/* classico, der = 1 (first-order upwind) — 7_advectivo.f90:33-113. */
+/* classico, der = 2 (centred, 7_advectivo.f90:115-170) and der = 3 (second-order upwind,
+ * :174-285) for one velocity component `a` on its faces (extents n[]): vel[d] is the velocity
+ * that advects it along direction d (the component itself along its own direction). */
+static void classico_hi(int der, const Arr& a, const int n[3], const Arr* const vel[3], const double h[3], Arr& out) {
+    Arr D[3], Dn[3], Dp[3];
+    for (int d = 0; d < 3; ++d) {
+        if (der == 2) {
+            deriva(a, d, n, h[d], D[d]);
+        } else {
+            deriva_u2n(a, d, n, h[d], Dn[d]);
+            deriva_u2p(a, d, n, h[d], Dp[d]);
+        }
+    }
+    for (int k = 1; k <= n[2]; ++k)
+        for (int j = 1; j <= n[1]; ++j)
+            for (int i = 1; i <= n[0]; ++i) {
+                double s = 0.;
+                for (int d = 0; d < 3; ++d) {
+                    const double c = (*vel[d])(i, j, k);
+                    const double term = der == 2 ? c * D[d](i, j, k)
+                                                 : fmax2(c, 0.) * Dn[d](i, j, k) + fmin2(c, 0.) * Dp[d](i, j, k);
+                    s = d == 0 ? term : s + term;
+                }
+                out(i, j, k) = s;
+            }
+}
+
+/* classico — 7_advectivo.f90:3-290.  der = 1 first-order upwind with 4-point transverse
+ * averages (:33-113); der = 2, 3 average the transverse velocities face -> centre
+ * (interp?_fc) -> face (interp?_cf, end faces copied). */
 void Oracle::classico(Arr& uint_, Arr& vint, Arr& wint) {
+    if (P.der == 2 || P.der == 3) {
+        const int du[3] = {nx1, ny, nz}, dv[3] = {nx, ny1, nz}, dw[3] = {nx, ny, nz1};
+        Arr t, bma, dma, amb, dmb, amd, bmd;
+        interp_fc(v, 1, dv, t); interpx_cf(t, nx, ny, nz, bma);   /* :134-135 (:178-179) */
+        interp_fc(w, 2, dw, t); interpx_cf(t, nx, ny, nz, dma);
+        interp_fc(u, 0, du, t); interpy_cf(t, nx, ny, nz, amb);
+        interp_fc(w, 2, dw, t); interpy_cf(t, nx, ny, nz, dmb);
+        interp_fc(u, 0, du, t); interpz_cf(t, nx, ny, nz, amd);
+        interp_fc(v, 1, dv, t); interpz_cf(t, nx, ny, nz, bmd);
+        const double h[3] = {dx, dy, dz};
+        const Arr* const vu[3] = {&u, &bma, &dma};
+        const Arr* const vv[3] = {&amb, &v, &dmb};
+        const Arr* const vw[3] = {&amd, &bmd, &w};
+        classico_hi(P.der, u, du, vu, h, uint_);
+        classico_hi(P.der, v, dv, vv, h, vint);
+        classico_hi(P.der, w, dw, vw, h, wint);
+        return;
+    }
     if (P.der != 1) { std::fprintf(stderr, "oracle: der=%d not restated\n", P.der); std::abort(); }
     OMP_FOR
     for (int k = 1; k <= nz; ++k)

@@ -239,7 +239,7 @@ __global__ void k_volfix(Geo G, double* ls, const double* __restrict__ mod_ls, d
 }
 
 // ------------------------------------------------------------------------------------
-// visco (5_viscosidade.f90:12-219), m_turb 0 / 1
+// visco (5_viscosidade.f90:12-219), m_turb 0 / 1 (m_turb 2: k_facenu_dir below)
 // ------------------------------------------------------------------------------------
 struct ViscConst {
     double dx, dy, dz, cdel, csmag;   // cdel = (dx*dy*dz)**(2/3) computed on the host
@@ -296,8 +296,66 @@ __global__ void __launch_bounds__(256) k_facenu(Geo G, int m_turb, const double*
     }
 }
 
+// m_turb = 2, directional Smagorinsky (5_viscosidade.f90:58-61, 104-164): each face's eddy
+// viscosity from the strain of its own velocity component, without the density factor:
+//   xnut_a = dx*dx*Cs*Cs*sqrt(2 p1 p1),  p1 = du/dx + (du/dy + dv/dx + du/dz + dw/dx)/2,
+// with dv/dx, dw/dx averaged face -> edge (interpx_cf, end copy) -> u-face (interpy_fc /
+// interpz_fc), and likewise for ynut_a, znut_a.  nut is not written.  Then
+// xnut = face(ls_nu) + xnut_a as in k_facenu.
+struct ViscDirConst {
+    double itdx, itdy, itdz;   // 1/(2 dx), 1/(2 dy), 1/(2 dz)
+    double cx, cy, cz;         // dx*dx*Cs*Cs, dy*dy*Cs*Cs, dz*dz*Cs*Cs in the reference's order
+};
+template <typename R>
+__global__ void __launch_bounds__(256) k_facenu_dir(Geo G, ViscDirConst V, const double* __restrict__ u,
+                                                    const double* __restrict__ v, const double* __restrict__ w,
+                                                    const double* __restrict__ ls_nu, double* xnut, double* ynut,
+                                                    double* znut) {
+    const Thread3 t = tid3(1, 1, 1);
+    const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
+    if (i > nx + 1 || j > ny + 1 || k > nz + 1) return;
+    const int px = G.px, pxy = (int)G.pxy, c0 = G.idx32(i, j, k);
+    const R itdx = R(V.itdx), itdy = R(V.itdy), itdz = R(V.itdz);
+#define AT(a, di, dj, dk) R((a)[c0 + (di) + (dj) * px + (dk) * pxy])
+    // centred derivatives (derivax/y/z, 8_derivadas.f90:1-68) at an offset from this face
+#define DX(a, di, dj, dk) ((AT(a, (di) + 1, dj, dk) - AT(a, (di) - 1, dj, dk)) * itdx)
+#define DY(a, di, dj, dk) ((AT(a, di, (dj) + 1, dk) - AT(a, di, (dj) - 1, dk)) * itdy)
+#define DZ(a, di, dj, dk) ((AT(a, di, dj, (dk) + 1) - AT(a, di, dj, (dk) - 1)) * itdz)
+    if (j <= ny && k <= nz) {   // u-faces i = 1..nx+1
+        const int ic = clampi(i, 2, nx), o1 = ic - i, o0 = ic - 1 - i;
+        const R dvdx_x = ((DX(v, o1, 0, 0) + DX(v, o0, 0, 0)) * R(0.5) + (DX(v, o1, 1, 0) + DX(v, o0, 1, 0)) * R(0.5)) * R(0.5);
+        const R dwdx_x = ((DX(w, o1, 0, 0) + DX(w, o0, 0, 0)) * R(0.5) + (DX(w, o1, 0, 1) + DX(w, o0, 0, 1)) * R(0.5)) * R(0.5);
+        const R p1 = DX(u, 0, 0, 0) + R(0.5) * (DY(u, 0, 0, 0) + dvdx_x + DZ(u, 0, 0, 0) + dwdx_x);
+        const R xa = R(V.cx) * sqrt(R(2.) * p1 * p1);
+        const double lx = (ls_nu[c0 + o1] + ls_nu[c0 + o0]) * 0.5;
+        xnut[c0] = lx + (double)xa;
+    }
+    if (i <= nx && k <= nz) {   // v-faces j = 1..ny+1
+        const int jc = clampi(j, 2, ny), q1 = jc - j, q0 = jc - 1 - j;
+        const R dudy_y = ((DY(u, 0, q1, 0) + DY(u, 0, q0, 0)) * R(0.5) + (DY(u, 1, q1, 0) + DY(u, 1, q0, 0)) * R(0.5)) * R(0.5);
+        const R dwdy_y = ((DY(w, 0, q1, 0) + DY(w, 0, q0, 0)) * R(0.5) + (DY(w, 0, q1, 1) + DY(w, 0, q0, 1)) * R(0.5)) * R(0.5);
+        const R p1 = DY(v, 0, 0, 0) + R(0.5) * (DX(v, 0, 0, 0) + dudy_y + DZ(v, 0, 0, 0) + dwdy_y);
+        const R ya = R(V.cy) * sqrt(R(2.) * p1 * p1);
+        const double ly = (ls_nu[c0 + q1 * px] + ls_nu[c0 + q0 * px]) * 0.5;
+        ynut[c0] = ly + (double)ya;
+    }
+    if (i <= nx && j <= ny) {   // w-faces k = 1..nz+1
+        const int kc = clampi(k, 2, nz), r1 = kc - k, r0 = kc - 1 - k;
+        const R dvdz_z = ((DZ(v, 0, 0, r1) + DZ(v, 0, 0, r0)) * R(0.5) + (DZ(v, 0, 1, r1) + DZ(v, 0, 1, r0)) * R(0.5)) * R(0.5);
+        const R dudz_z = ((DZ(u, 0, 0, r1) + DZ(u, 0, 0, r0)) * R(0.5) + (DZ(u, 1, 0, r1) + DZ(u, 1, 0, r0)) * R(0.5)) * R(0.5);
+        const R p1 = DZ(w, 0, 0, 0) + R(0.5) * (DY(w, 0, 0, 0) + dvdz_z + dudz_z + DX(w, 0, 0, 0));
+        const R za = R(V.cz) * sqrt(R(2.) * p1 * p1);
+        const double lz = (ls_nu[c0 + r1 * pxy] + ls_nu[c0 + r0 * pxy]) * 0.5;
+        znut[c0] = lz + (double)za;
+    }
+#undef DZ
+#undef DY
+#undef DX
+#undef AT
+}
+
 // ------------------------------------------------------------------------------------
-// convdiff + classico (6_convdiff.f90:14-189, 7_advectivo.f90:33-113)
+// convdiff + classico (6_convdiff.f90:14-189, 7_advectivo.f90:3-290)
 // ------------------------------------------------------------------------------------
 struct CDConst {
     double idx, idy, idz, gx, gz, sigma, cz;   // reciprocal cell sizes; cz = gz/(chezy*chezy)
@@ -314,7 +372,40 @@ __device__ __forceinline__ bool on_cap(const CDConst& C, int j, int k, int ny) {
     return (C.cap_z2 && k == 2) || (C.cap_y2 && j == 2) || (C.cap_yn && j == ny);
 }
 
-template <typename R>
+// classico der = 2 (centred, 7_advectivo.f90:115-170) and der = 3 (second-order upwind,
+// :174-285) for one velocity component a at its face c: along direction d (element stride
+// s[d]) the face sits at m[d] of the component's n[d] points, vel[d] is the advecting
+// velocity, ih[d] = 1/h.  Terms summed in direction order, as the reference does.
+template <typename R, int DER>
+__device__ __forceinline__ R classico_hi(const double* __restrict__ a, int c, const int s[3], const int m[3],
+                                         const int n[3], const R vel[3], const R ih[3]) {
+    R acc = R(0.);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const R ap = R(a[c + s[d]]), am = R(a[c - s[d]]);
+        R term;
+        if constexpr (DER == 2) {
+            term = vel[d] * ((ap - am) * (R(0.5) * ih[d]));   // derivax/y/z (8_derivadas.f90:1-68)
+        } else {
+            const R a0 = R(a[c]);
+            // the points two away, where the one-sided formulas use them (else this face):
+            // every load stays inside the component's halo
+            const R amm = R(a[c - (m[d] > 1 ? 2 * s[d] : 0)]);
+            const R app = R(a[c + (m[d] < n[d] ? 2 * s[d] : 0)]);
+            // derivax/y/zu2n (:194-290): backward one-sided, centred on the first point
+            const R dn = m[d] > 1 ? R(0.5) * (amm - R(4.) * am + R(3.) * a0) * ih[d]
+                                  : R(0.5) * (ap - am) * ih[d];
+            // derivax/y/zu2p (:83-179): forward one-sided, centred on the last point
+            const R dp = m[d] < n[d] ? R(0.5) * (-app + R(4.) * ap - R(3.) * a0) * ih[d]
+                                     : R(0.5) * (ap - am) * ih[d];
+            term = pmax(vel[d], R(0.)) * dn + pmin(vel[d], R(0.)) * dp;
+        }
+        acc = d == 0 ? term : acc + term;
+    }
+    return acc;
+}
+
+template <typename R, int DER>
 __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) {
     const Thread3 t = tid3(1, 1, 1);
     const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
@@ -330,16 +421,27 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
     // ---- Fu on u-faces (i = 1..nx+1, j = 1..ny, k = 1..nz)
     if (j <= ny && k <= nz) {
         const R uc = AT(u, 0, 0, 0);
-        const R bma4 = (AT(v, 0, 0, 0) + AT(v, -1, 0, 0) + AT(v, 0, 1, 0) + AT(v, -1, 1, 0)) * R(0.25);
-        const R dma4 = (AT(w, 0, 0, 0) + AT(w, -1, 0, 0) + AT(w, 0, 0, 1) + AT(w, -1, 0, 1)) * R(0.25);
-        R a1 = pmax(uc, R(0.)), a2 = pmin(uc, R(0.));
-        const R dudx = a1 * (uc - AT(u, -1, 0, 0)) * idx + a2 * (AT(u, 1, 0, 0) - uc) * idx;
-        a1 = pmax(bma4, R(0.)); a2 = pmin(bma4, R(0.));
-        const R dudy = a1 * (uc - AT(u, 0, -1, 0)) * idy + a2 * (AT(u, 0, 1, 0) - uc) * idy;
-        a1 = pmax(dma4, R(0.)); a2 = pmin(dma4, R(0.));
-        const R dudz = a1 * (uc - AT(u, 0, 0, -1)) * idz + a2 * (AT(u, 0, 0, 1) - uc) * idz;
-        const R uint_ = dudx + dudy + dudz;
         const int ic = clampi(i, 2, nx);
+        R uint_;
+        if constexpr (DER == 1) {
+            const R bma4 = (AT(v, 0, 0, 0) + AT(v, -1, 0, 0) + AT(v, 0, 1, 0) + AT(v, -1, 1, 0)) * R(0.25);
+            const R dma4 = (AT(w, 0, 0, 0) + AT(w, -1, 0, 0) + AT(w, 0, 0, 1) + AT(w, -1, 0, 1)) * R(0.25);
+            R a1 = pmax(uc, R(0.)), a2 = pmin(uc, R(0.));
+            const R dudx = a1 * (uc - AT(u, -1, 0, 0)) * idx + a2 * (AT(u, 1, 0, 0) - uc) * idx;
+            a1 = pmax(bma4, R(0.)); a2 = pmin(bma4, R(0.));
+            const R dudy = a1 * (uc - AT(u, 0, -1, 0)) * idy + a2 * (AT(u, 0, 1, 0) - uc) * idy;
+            a1 = pmax(dma4, R(0.)); a2 = pmin(dma4, R(0.));
+            const R dudz = a1 * (uc - AT(u, 0, 0, -1)) * idz + a2 * (AT(u, 0, 0, 1) - uc) * idz;
+            uint_ = dudx + dudy + dudz;
+        } else {
+            // transverse velocities face -> centre (interp?_fc) -> u-face (interpx_cf, end copy)
+            const int o1 = ic - i, o0 = ic - 1 - i;
+            const R bma = ((AT(v, o1, 0, 0) + AT(v, o1, 1, 0)) * R(0.5) + (AT(v, o0, 0, 0) + AT(v, o0, 1, 0)) * R(0.5)) * R(0.5);
+            const R dma = ((AT(w, o1, 0, 0) + AT(w, o1, 0, 1)) * R(0.5) + (AT(w, o0, 0, 0) + AT(w, o0, 0, 1)) * R(0.5)) * R(0.5);
+            const int s[3] = {1, px, pxy}, m[3] = {i, j, k}, n[3] = {nx + 1, ny, nz};
+            const R vel[3] = {uc, bma, dma}, ih[3] = {idx, idy, idz};
+            uint_ = classico_hi<R, DER>(u, c0, s, m, n, vel, ih);
+        }
         const R rhox = (AT(F.rho, (ic) - i, 0, 0) + AT(F.rho, (ic - 1) - i, 0, 0)) * R(0.5);
         const R tx1 = AT(F.hsx, (ic) - i, 0, 0) * AT(F.kurv, (ic) - i, 0, 0) / AT(F.rho, (ic) - i, 0, 0);
         const R tx0 = AT(F.hsx, (ic - 1) - i, 0, 0) * AT(F.kurv, (ic - 1) - i, 0, 0) / AT(F.rho, (ic - 1) - i, 0, 0);
@@ -365,16 +467,26 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
     // ---- Fv on v-faces (i = 1..nx, j = 1..ny+1, k = 1..nz)
     if (i <= nx && k <= nz) {
         const R vc = AT(v, 0, 0, 0);
-        const R amb4 = (AT(u, 0, 0, 0) + AT(u, 1, 0, 0) + AT(u, 0, -1, 0) + AT(u, 1, -1, 0)) * R(0.25);
-        const R dmb4 = (AT(w, 0, 0, 0) + AT(w, 0, -1, 0) + AT(w, 0, 0, 1) + AT(w, 0, -1, 1)) * R(0.25);
-        R a1 = pmax(amb4, R(0.)), a2 = pmin(amb4, R(0.));
-        const R dvdx = a1 * (vc - AT(v, -1, 0, 0)) * idx + a2 * (AT(v, 1, 0, 0) - vc) * idx;
-        a1 = pmax(vc, R(0.)); a2 = pmin(vc, R(0.));
-        const R dvdy = a1 * (vc - AT(v, 0, -1, 0)) * idy + a2 * (AT(v, 0, 1, 0) - vc) * idy;
-        a1 = pmax(dmb4, R(0.)); a2 = pmin(dmb4, R(0.));
-        const R dvdz = a1 * (vc - AT(v, 0, 0, -1)) * idz + a2 * (AT(v, 0, 0, 1) - vc) * idz;
-        const R vint = dvdx + dvdy + dvdz;
         const int jc = clampi(j, 2, ny);
+        R vint;
+        if constexpr (DER == 1) {
+            const R amb4 = (AT(u, 0, 0, 0) + AT(u, 1, 0, 0) + AT(u, 0, -1, 0) + AT(u, 1, -1, 0)) * R(0.25);
+            const R dmb4 = (AT(w, 0, 0, 0) + AT(w, 0, -1, 0) + AT(w, 0, 0, 1) + AT(w, 0, -1, 1)) * R(0.25);
+            R a1 = pmax(amb4, R(0.)), a2 = pmin(amb4, R(0.));
+            const R dvdx = a1 * (vc - AT(v, -1, 0, 0)) * idx + a2 * (AT(v, 1, 0, 0) - vc) * idx;
+            a1 = pmax(vc, R(0.)); a2 = pmin(vc, R(0.));
+            const R dvdy = a1 * (vc - AT(v, 0, -1, 0)) * idy + a2 * (AT(v, 0, 1, 0) - vc) * idy;
+            a1 = pmax(dmb4, R(0.)); a2 = pmin(dmb4, R(0.));
+            const R dvdz = a1 * (vc - AT(v, 0, 0, -1)) * idz + a2 * (AT(v, 0, 0, 1) - vc) * idz;
+            vint = dvdx + dvdy + dvdz;
+        } else {
+            const int q1 = jc - j, q0 = jc - 1 - j;
+            const R amb = ((AT(u, 0, q1, 0) + AT(u, 1, q1, 0)) * R(0.5) + (AT(u, 0, q0, 0) + AT(u, 1, q0, 0)) * R(0.5)) * R(0.5);
+            const R dmb = ((AT(w, 0, q1, 0) + AT(w, 0, q1, 1)) * R(0.5) + (AT(w, 0, q0, 0) + AT(w, 0, q0, 1)) * R(0.5)) * R(0.5);
+            const int s[3] = {1, px, pxy}, m[3] = {i, j, k}, n[3] = {nx, ny + 1, nz};
+            const R vel[3] = {amb, vc, dmb}, ih[3] = {idx, idy, idz};
+            vint = classico_hi<R, DER>(v, c0, s, m, n, vel, ih);
+        }
         const R rhoy = (AT(F.rho, 0, (jc) - j, 0) + AT(F.rho, 0, (jc - 1) - j, 0)) * R(0.5);
         const R ty1 = AT(F.hsy, 0, (jc) - j, 0) * AT(F.kurv, 0, (jc) - j, 0) / AT(F.rho, 0, (jc) - j, 0);
         const R ty0 = AT(F.hsy, 0, (jc - 1) - j, 0) * AT(F.kurv, 0, (jc - 1) - j, 0) / AT(F.rho, 0, (jc - 1) - j, 0);
@@ -400,16 +512,26 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
     // ---- Fw on w-faces (i = 1..nx, j = 1..ny, k = 1..nz+1)
     if (i <= nx && j <= ny) {
         const R wc = AT(w, 0, 0, 0);
-        const R amd4 = (AT(u, 0, 0, 0) + AT(u, 1, 0, 0) + AT(u, 0, 0, -1) + AT(u, 1, 0, -1)) * R(0.25);
-        const R bmd4 = (AT(v, 0, 0, 0) + AT(v, 0, 1, 0) + AT(v, 0, 0, -1) + AT(v, 0, 1, -1)) * R(0.25);
-        R a1 = pmax(amd4, R(0.)), a2 = pmin(amd4, R(0.));
-        const R dwdx = a1 * (wc - AT(w, -1, 0, 0)) * idx + a2 * (AT(w, 1, 0, 0) - wc) * idx;
-        a1 = pmax(bmd4, R(0.)); a2 = pmin(bmd4, R(0.));
-        const R dwdy = a1 * (wc - AT(w, 0, -1, 0)) * idy + a2 * (AT(w, 0, 1, 0) - wc) * idy;
-        a1 = pmax(wc, R(0.)); a2 = pmin(wc, R(0.));
-        const R dwdz = a1 * (wc - AT(w, 0, 0, -1)) * idz + a2 * (AT(w, 0, 0, 1) - wc) * idz;
-        const R wint = dwdx + dwdy + dwdz;
         const int kc = clampi(k, 2, nz);
+        R wint;
+        if constexpr (DER == 1) {
+            const R amd4 = (AT(u, 0, 0, 0) + AT(u, 1, 0, 0) + AT(u, 0, 0, -1) + AT(u, 1, 0, -1)) * R(0.25);
+            const R bmd4 = (AT(v, 0, 0, 0) + AT(v, 0, 1, 0) + AT(v, 0, 0, -1) + AT(v, 0, 1, -1)) * R(0.25);
+            R a1 = pmax(amd4, R(0.)), a2 = pmin(amd4, R(0.));
+            const R dwdx = a1 * (wc - AT(w, -1, 0, 0)) * idx + a2 * (AT(w, 1, 0, 0) - wc) * idx;
+            a1 = pmax(bmd4, R(0.)); a2 = pmin(bmd4, R(0.));
+            const R dwdy = a1 * (wc - AT(w, 0, -1, 0)) * idy + a2 * (AT(w, 0, 1, 0) - wc) * idy;
+            a1 = pmax(wc, R(0.)); a2 = pmin(wc, R(0.));
+            const R dwdz = a1 * (wc - AT(w, 0, 0, -1)) * idz + a2 * (AT(w, 0, 0, 1) - wc) * idz;
+            wint = dwdx + dwdy + dwdz;
+        } else {
+            const int r1 = kc - k, r0 = kc - 1 - k;
+            const R amd = ((AT(u, 0, 0, r1) + AT(u, 1, 0, r1)) * R(0.5) + (AT(u, 0, 0, r0) + AT(u, 1, 0, r0)) * R(0.5)) * R(0.5);
+            const R bmd = ((AT(v, 0, 0, r1) + AT(v, 0, 1, r1)) * R(0.5) + (AT(v, 0, 0, r0) + AT(v, 0, 1, r0)) * R(0.5)) * R(0.5);
+            const int s[3] = {1, px, pxy}, m[3] = {i, j, k}, n[3] = {nx, ny, nz + 1};
+            const R vel[3] = {amd, bmd, wc}, ih[3] = {idx, idy, idz};
+            wint = classico_hi<R, DER>(w, c0, s, m, n, vel, ih);
+        }
         const R rhoz = (AT(F.rho, 0, 0, (kc) - k) + AT(F.rho, 0, 0, (kc - 1) - k)) * R(0.5);
         const R tz1 = AT(F.hsz, 0, 0, (kc) - k) * AT(F.kurv, 0, 0, (kc) - k) / AT(F.rho, 0, 0, (kc) - k);
         const R tz0 = AT(F.hsz, 0, 0, (kc - 1) - k) * AT(F.kurv, 0, 0, (kc - 1) - k) / AT(F.rho, 0, 0, (kc - 1) - k);
@@ -1124,6 +1246,23 @@ void launch_volfix(suli_ctx* c, double dt1fac) {
 void launch_visco(suli_ctx* c) {
     const Geo& G = c->g;
     ProfScope ps(c, SULI_K_VISCO, c->P.m_turb == 1 ? 2 : 1);
+    if (c->P.m_turb == 2) {
+        ViscDirConst V;
+        const double cs = c->P.csmag;
+        V.itdx = 1. / (2. * c->P.dx); V.itdy = 1. / (2. * c->P.dy); V.itdz = 1. / (2. * c->P.dz);
+        V.cx = c->P.dx * c->P.dx * cs * cs; V.cy = c->P.dy * c->P.dy * cs * cs; V.cz = c->P.dz * c->P.dz * cs * cs;
+        if (c->P.precision == 1)
+            k_facenu_dir<float><<<faces_grid(G), kBlk, 0, c->stream>>>(G, V, c->f[SULI_F_U], c->f[SULI_F_V],
+                                                                     c->f[SULI_F_W], c->f[SULI_F_LS_NU],
+                                                                     c->f[SULI_F_XNUT], c->f[SULI_F_YNUT],
+                                                                     c->f[SULI_F_ZNUT]);
+        else
+            k_facenu_dir<double><<<faces_grid(G), kBlk, 0, c->stream>>>(G, V, c->f[SULI_F_U], c->f[SULI_F_V],
+                                                                      c->f[SULI_F_W], c->f[SULI_F_LS_NU],
+                                                                      c->f[SULI_F_XNUT], c->f[SULI_F_YNUT],
+                                                                      c->f[SULI_F_ZNUT]);
+        return;
+    }
     if (c->P.m_turb == 1) {
         ViscConst V;
         V.dx = c->P.dx; V.dy = c->P.dy; V.dz = c->P.dz; V.csmag = c->P.csmag;
@@ -1137,6 +1276,15 @@ void launch_visco(suli_ctx* c) {
     }
     k_facenu<<<faces_grid(G), kBlk, 0, c->stream>>>(G, c->P.m_turb, c->f[SULI_F_LS_NU], c->f[SULI_F_NUT],
                                                      c->f[SULI_F_XNUT], c->f[SULI_F_YNUT], c->f[SULI_F_ZNUT]);
+}
+template <typename R>
+static void convdiff_der(suli_ctx* c, const CDConst& C, const CDFields& F) {
+    const Geo& G = c->g;
+    switch (c->P.der) {
+    case 2: k_convdiff<R, 2><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F); break;
+    case 3: k_convdiff<R, 3><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F); break;
+    default: k_convdiff<R, 1><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F); break;
+    }
 }
 void launch_convdiff(suli_ctx* c) {
     const Geo& G = c->g;
@@ -1156,9 +1304,9 @@ void launch_convdiff(suli_ctx* c) {
     ProfScope ps(c, SULI_K_CONVDIFF, 1);
     cudaMemcpyAsync(c->f[SULI_F_PRD0], c->f[SULI_F_PRD1], G.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
     if (c->P.precision == 1)   // FP32 arithmetic over the FP64 state
-        k_convdiff<float><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F);
+        convdiff_der<float>(c, C, F);
     else
-        k_convdiff<double><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F);
+        convdiff_der<double>(c, C, F);
 }
 void launch_tempo(suli_ctx* c, int tt, int it) {
     const Geo& G = c->g;

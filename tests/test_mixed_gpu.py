@@ -105,6 +105,26 @@ def test_vector_kernels_match_one_cell_kernels(pkg, case):
         assert float(np.abs(v0[f] - v1[f]).max()) <= 1e-9 * vs, f
 
 
+@pytest.mark.parametrize("der, m_turb", [(1, 1), (2, 2), (3, 2)])
+def test_mixed_stencils_track_fp64(pkg, orc, der, m_turb):
+    """visco and convdiff in FP32 arithmetic (precision 1), every advection scheme and both
+    Smagorinsky models, against the FP64 oracle on the same state: face viscosities and
+    forces within 1e-5 of each field's scale (FP32 rounding of terms no larger than the
+    field's scale)."""
+    p = small_params(nx=16, ny=12, nz=8, m_turb=m_turb)
+    p.der = der
+    q = p.copy()
+    q.precision, q.cg_stop = 1, 1
+    o, st = _prepared(pkg, orc, p, 41)
+    g = pkg.Solver(q)
+    load_state(g, st)
+    for m in (g, o):
+        m.visco()
+        m.convdiff()
+    for f in ("xnut", "ynut", "znut", "Fu", "Fv", "Fw"):
+        assert rel_err(g.download(f), o.download(f)) <= 1e-5, f
+
+
 def test_mixed_rejects_unsupported(pkg):
     p = small_params(nx=15, ny=13, nz=11)   # cannot halve to <= 1024 cells
     p.precision, p.cg_stop = 1, 1

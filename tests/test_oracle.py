@@ -269,3 +269,231 @@ def test_dam_break_invariants(orc, pkg):
     assert abs(o.get_scalar("vol_ins") - v0) / v0 < 1e-3
     prd = o.download("prd1")
     assert 0 < prd.max() < 2 * 1000 * 9.81 * 0.3 * (18 * 0.02 / 0.48)
+
+
+# ------------------------------------------- classico der = 2, 3 and visco m_turb = 2
+E3 = ((1, 0, 0), (0, 1, 0), (0, 0, 1))
+
+
+def fortran_view(o, p, name):
+    """A downloaded module array addressed by its Fortran indices."""
+    a = o.download(name)
+    lo = [l for l, _ in pkg_abi().field_extent(p, name)]
+    return lambda i, j, k: float(a[i - lo[0], j - lo[1], k - lo[2]])
+
+
+def pkg_abi():
+    from helpers import pkg
+    return pkg._abi
+
+
+def fmax2(a, b):
+    return a if a > b else b
+
+
+def fmin2(a, b):
+    return a if a < b else b
+
+
+def classico_hi_py(p, U, V, W, der):
+    """Loop restatement of classico der = 2 (7_advectivo.f90:115-170) and der = 3 (:174-285),
+    with derivax/y/z, derivax/y/zu2p, derivax/y/zu2n and interp?_fc / interp?_cf
+    (8_derivadas.f90) written out per point.  Returns {"u": {(i,j,k): uint}, "v": ..., "w": ...}."""
+    nx, ny, nz = p.nx, p.ny, p.nz
+    h = (p.dx, p.dy, p.dz)
+
+    def sh(i, j, k, d, s):
+        e = E3[d]
+        return i + s * e[0], j + s * e[1], k + s * e[2]
+
+    def cen(F, d, i, j, k):
+        return (F(*sh(i, j, k, d, 1)) - F(*sh(i, j, k, d, -1))) / (2. * h[d])
+
+    def u2p(F, d, n, i, j, k):
+        if (i, j, k)[d] < n[d]:
+            return 0.5 * (-F(*sh(i, j, k, d, 2)) + 4. * F(*sh(i, j, k, d, 1)) - 3. * F(i, j, k)) / h[d]
+        return 0.5 * (F(*sh(i, j, k, d, 1)) - F(*sh(i, j, k, d, -1))) / h[d]
+
+    def u2n(F, d, n, i, j, k):
+        if (i, j, k)[d] > 1:
+            return 0.5 * (F(*sh(i, j, k, d, -2)) - 4. * F(*sh(i, j, k, d, -1)) + 3. * F(i, j, k)) / h[d]
+        return 0.5 * (F(*sh(i, j, k, d, 1)) - F(*sh(i, j, k, d, -1))) / h[d]
+
+    # face -> centre (interp?_fc)
+    def uc(i, j, k): return (U(i, j, k) + U(i + 1, j, k)) * 0.5
+    def vc(i, j, k): return (V(i, j, k) + V(i, j + 1, k)) * 0.5
+    def wc(i, j, k): return (W(i, j, k) + W(i, j, k + 1)) * 0.5
+
+    # centre -> face along d (interp?_cf): the end faces copy their neighbour
+    def cf(C, d, n, i, j, k):
+        m = min(max((i, j, k)[d], 2), n)
+        idx1 = [i, j, k]; idx1[d] = m
+        idx0 = [i, j, k]; idx0[d] = m - 1
+        return (C(*idx1) + C(*idx0)) * 0.5
+
+    comps = {
+        "u": (U, (nx + 1, ny, nz), lambda i, j, k: (U(i, j, k), cf(vc, 0, nx, i, j, k), cf(wc, 0, nx, i, j, k))),
+        "v": (V, (nx, ny + 1, nz), lambda i, j, k: (cf(uc, 1, ny, i, j, k), V(i, j, k), cf(wc, 1, ny, i, j, k))),
+        "w": (W, (nx, ny, nz + 1), lambda i, j, k: (cf(uc, 2, nz, i, j, k), cf(vc, 2, nz, i, j, k), W(i, j, k))),
+    }
+    out = {}
+    for name, (F, n, vel) in comps.items():
+        res = {}
+        for k in range(1, n[2] + 1):
+            for j in range(1, n[1] + 1):
+                for i in range(1, n[0] + 1):
+                    c = vel(i, j, k)
+                    s = 0.
+                    for d in range(3):
+                        if der == 2:
+                            term = c[d] * cen(F, d, i, j, k)
+                        else:
+                            term = fmax2(c[d], 0.) * u2n(F, d, n, i, j, k) + fmin2(c[d], 0.) * u2p(F, d, n, i, j, k)
+                        s = term if d == 0 else s + term
+                    res[(i, j, k)] = s
+        out[name] = res
+    return out
+
+
+def advection_only(orc, p, st):
+    """An oracle holding state st with every convdiff term but the advective one zeroed
+    (no viscosity, surface tension, gravity, wall friction or source), so that
+    Fu = -uint, Fv = -vint, Fw = -wint exactly."""
+    p = p.copy()
+    p.sigma, p.gx, p.gz, p.m_turb = 0.0, 0.0, 0.0, 0
+    o = orc.Oracle(p)
+    load_state(o, st)
+    for f in ("nut", "xnut", "ynut", "znut", "ub", "vb", "wb"):
+        o.upload(f, np.zeros(o.shape(f)))
+    o.upload("rho", np.ones(o.shape("rho")))
+    return o, p
+
+
+@pytest.mark.parametrize("der", [2, 3])
+@pytest.mark.parametrize("bc", [(2, 2, 2, 2, 2, 1), (0, 0, 1, 1, 2, 1)])
+def test_classico_matches_loop_restatement(orc, der, bc):
+    p = small_params(nx=6, ny=5, nz=4, bc=bc)
+    p.der = der
+    o, p = advection_only(orc, p, seeded_state(p, 21))
+    o.contorno(1)
+    U, V, W = (fortran_view(o, p, f) for f in ("u", "v", "w"))
+    want = classico_hi_py(p, U, V, W, der)
+    o.convdiff()
+    for comp, F in (("u", "Fu"), ("v", "Fv"), ("w", "Fw")):
+        got = fortran_view(o, p, F)
+        bad = [(ijk, got(*ijk), -x) for ijk, x in want[comp].items() if got(*ijk) != -x]
+        assert not bad, (comp, bad[:3])
+
+
+@pytest.mark.parametrize("der", [1, 2, 3])
+def test_classico_exact_on_linear_velocity(orc, der):
+    """u = a x, v = -a y, w = 0 (halo included): every scheme gives u.grad u = (a^2 x, a^2 y, 0)
+    at every face, end faces included."""
+    p = small_params(nx=7, ny=6, nz=5)
+    p.der = der
+    a = 1.7
+    st = seeded_state(p, 22)
+    (l0, h0), _, _ = pkg_abi().field_extent(p, "u")
+    xf = (np.arange(l0, h0 + 1) - 1) * p.dx                      # u-face positions
+    st["u"] = np.broadcast_to((a * xf)[:, None, None], pkg_abi().field_shape(p, "u")).copy()
+    _, (l1, h1), _ = pkg_abi().field_extent(p, "v")
+    yf = (np.arange(l1, h1 + 1) - 1) * p.dy
+    st["v"] = np.broadcast_to((-a * yf)[None, :, None], pkg_abi().field_shape(p, "v")).copy()
+    st["w"] = np.zeros(pkg_abi().field_shape(p, "w"))
+    o, p = advection_only(orc, p, st)
+    o.convdiff()
+    Fu, Fv, Fw = o.download("Fu"), o.download("Fv"), o.download("Fw")
+    np.testing.assert_allclose(-Fu, np.broadcast_to((a * a * xf[1:-1])[:, None, None], Fu.shape),
+                               rtol=0, atol=1e-12 * a * a)
+    np.testing.assert_allclose(-Fv, np.broadcast_to((a * a * yf[1:-1])[None, :, None], Fv.shape),
+                               rtol=0, atol=1e-12 * a * a)
+    assert np.abs(Fw).max() <= 1e-12 * a * a
+
+
+def visco_dir_py(p, U, V, W):
+    """Loop restatement of visco m_turb = 2 (5_viscosidade.f90:104-164): xnut_a, ynut_a,
+    znut_a per face.  The cross derivatives go face -> edge (interp?_cf, end copy) -> face
+    (interp?_fc)."""
+    nx, ny, nz = p.nx, p.ny, p.nz
+    dx, dy, dz, cs = p.dx, p.dy, p.dz, p.csmag
+    DX = lambda F, i, j, k: (F(i + 1, j, k) - F(i - 1, j, k)) / (2. * dx)
+    DY = lambda F, i, j, k: (F(i, j + 1, k) - F(i, j - 1, k)) / (2. * dy)
+    DZ = lambda F, i, j, k: (F(i, j, k + 1) - F(i, j, k - 1)) / (2. * dz)
+
+    def ex(D, F, i, j, k):
+        c = min(max(i, 2), nx)
+        return (D(F, c, j, k) + D(F, c - 1, j, k)) * 0.5
+
+    def ey(D, F, i, j, k):
+        c = min(max(j, 2), ny)
+        return (D(F, i, c, k) + D(F, i, c - 1, k)) * 0.5
+
+    def ez(D, F, i, j, k):
+        c = min(max(k, 2), nz)
+        return (D(F, i, j, c) + D(F, i, j, c - 1)) * 0.5
+
+    xa, ya, za = {}, {}, {}
+    for k in range(1, nz + 1):
+        for j in range(1, ny + 1):
+            for i in range(1, nx + 2):
+                dvdx_x = (ex(DX, V, i, j, k) + ex(DX, V, i, j + 1, k)) * 0.5
+                dwdx_x = (ex(DX, W, i, j, k) + ex(DX, W, i, j, k + 1)) * 0.5
+                p1 = DX(U, i, j, k) + 0.5 * (DY(U, i, j, k) + dvdx_x + DZ(U, i, j, k) + dwdx_x)
+                xa[(i, j, k)] = dx * dx * cs * cs * math.sqrt(2. * p1 * p1)
+    for k in range(1, nz + 1):
+        for j in range(1, ny + 2):
+            for i in range(1, nx + 1):
+                dudy_y = (ey(DY, U, i, j, k) + ey(DY, U, i + 1, j, k)) * 0.5
+                dwdy_y = (ey(DY, W, i, j, k) + ey(DY, W, i, j, k + 1)) * 0.5
+                p1 = DY(V, i, j, k) + 0.5 * (DX(V, i, j, k) + dudy_y + DZ(V, i, j, k) + dwdy_y)
+                ya[(i, j, k)] = dy * dy * cs * cs * math.sqrt(2. * p1 * p1)
+    for k in range(1, nz + 2):
+        for j in range(1, ny + 1):
+            for i in range(1, nx + 1):
+                dvdz_z = (ez(DZ, V, i, j, k) + ez(DZ, V, i, j + 1, k)) * 0.5
+                dudz_z = (ez(DZ, U, i, j, k) + ez(DZ, U, i + 1, j, k)) * 0.5
+                p1 = DZ(W, i, j, k) + 0.5 * (DY(W, i, j, k) + dvdz_z + dudz_z + DX(W, i, j, k))
+                za[(i, j, k)] = dz * dz * cs * cs * math.sqrt(2. * p1 * p1)
+    return {"xnut": xa, "ynut": ya, "znut": za}
+
+
+def test_visco_directional_matches_loop_restatement(orc):
+    """With ls_nu = 0 the face viscosities are xnut_a, ynut_a, znut_a themselves; nut is not
+    written by m_turb = 2."""
+    p = small_params(nx=6, ny=5, nz=4, m_turb=2)
+    o = orc.Oracle(p)
+    st = seeded_state(p, 23)
+    load_state(o, st)
+    o.contorno(1)
+    o.upload("ls_nu", np.zeros(o.shape("ls_nu")))
+    nut0 = np.random.default_rng(5).standard_normal(o.shape("nut"))
+    o.upload("nut", nut0)
+    U, V, W = (fortran_view(o, p, f) for f in ("u", "v", "w"))
+    want = visco_dir_py(p, U, V, W)
+    o.visco()
+    for f, vals in want.items():
+        got = fortran_view(o, p, f)
+        bad = [(ijk, got(*ijk), x) for ijk, x in vals.items() if got(*ijk) != x]
+        assert not bad, (f, bad[:3])
+    np.testing.assert_array_equal(o.download("nut"), nut0)
+
+
+def test_visco_directional_on_shear(orc):
+    """u = g z, v = w = 0: du/dz = g is the only strain, so xnut_a = znut_a = h^2 Cs^2 |g|/sqrt(2)
+    (p1 = g/2) and ynut_a = 0."""
+    p = small_params(nx=6, ny=5, nz=7, m_turb=2)
+    g = -2.5
+    o = orc.Oracle(p)
+    st = seeded_state(p, 24)
+    _, _, (l2, h2) = pkg_abi().field_extent(p, "u")
+    zc = (np.arange(l2, h2 + 1) - 0.5) * p.dz                    # u sits at cell-centre heights
+    st["u"] = np.broadcast_to((g * zc)[None, None, :], pkg_abi().field_shape(p, "u")).copy()
+    st["v"] = np.zeros(pkg_abi().field_shape(p, "v"))
+    st["w"] = np.zeros(pkg_abi().field_shape(p, "w"))
+    st["ls_nu"] = np.zeros(pkg_abi().field_shape(p, "ls_nu"))
+    load_state(o, st)
+    o.visco()
+    want = p.dx * p.dx * p.csmag ** 2 * abs(g) / math.sqrt(2.)
+    np.testing.assert_allclose(o.download("xnut"), want, rtol=1e-12)
+    np.testing.assert_allclose(o.download("znut"), p.dz * p.dz * p.csmag ** 2 * abs(g) / math.sqrt(2.), rtol=1e-12)
+    assert np.abs(o.download("ynut")).max() <= 1e-14 * want

@@ -74,23 +74,27 @@ def test_heaviside_mod_ls1(pkg, orc, bc):
     compare(g, o, OUT_FIELDS["heaviside"] + OUT_FIELDS["mod_ls1"], what="heaviside/mod_ls1")
 
 
-@pytest.mark.parametrize("m_turb", [0, 1])
+@pytest.mark.parametrize("m_turb", [0, 1, 2])
 @pytest.mark.parametrize("bc", BCS[:3])
 def test_visco(pkg, orc, bc, m_turb):
     p = small_params(nx=13, ny=11, nz=9, bc=bc, m_turb=m_turb)
     g, o = pair(pkg, orc, p, seed=2)
     for m in (g, o):
         m.visco()
-    compare(g, o, OUT_FIELDS["visco"], what="visco")
+    compare(g, o, OUT_FIELDS["visco"], what=f"visco m_turb={m_turb}")
 
 
+@pytest.mark.parametrize("der", [1, 2, 3])
 @pytest.mark.parametrize("bc", BCS)
-def test_convdiff(pkg, orc, bc):
+def test_convdiff(pkg, orc, bc, der):
+    """Advection schemes of classico (7_advectivo.f90:33-285): 1 upwind, 2 centred,
+    3 second-order upwind."""
     p = small_params(nx=13, ny=11, nz=9, bc=bc)
+    p.der = der
     g, o = pair(pkg, orc, p, seed=3)
     for m in (g, o):
         m.convdiff()
-    compare(g, o, OUT_FIELDS["convdiff"], what="convdiff")
+    compare(g, o, OUT_FIELDS["convdiff"], what=f"convdiff der={der}")
 
 
 def test_convdiff_with_forcing(pkg, orc):
@@ -270,6 +274,31 @@ def test_step_parity_dam_break(pkg, orc):
     worst["prd1(mean-free)"] = rel_err(pg - pg.mean(), po - po.mean())
     assert max(worst.values()) <= 1e-10, worst
     assert sg["max_div"] <= 1e-8
+
+
+@pytest.mark.parametrize("der", [2, 3])
+def test_step_parity_schemes(pkg, orc, der):
+    """Five whole dam-break steps with the centred / second-order upwind advection and the
+    directional Smagorinsky model (m_turb = 2): every state field within 1e-10 of its own
+    scale, the velocity components within 1e-10 of the velocity scale (v, across the tank,
+    is orders of magnitude below u in this nearly two-dimensional flow)."""
+    p, init = pkg.cases.dam_break(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-12)
+    p.der, p.m_turb = der, 2
+    g = pkg.Solver(p)
+    o = orc.Oracle(p)
+    init(g)
+    init(o)
+    for it in range(1, 6):
+        sg, so = g.step(it), o.step(it)
+        assert sg["status"] == 0 and so["status"] == 0
+        assert max(abs(a - b) for a, b in zip(sg["cg_iters"], so["cg_iters"])) <= 3
+    vel = {f: (g.download(f), o.download(f)) for f in ("u", "v", "w")}
+    vs = max(float(np.abs(b).max()) for _, b in vel.values())
+    worst = {f: float(np.abs(a - b).max()) / vs for f, (a, b) in vel.items()}
+    worst.update({f: rel_err(g.download(f), o.download(f)) for f in ("ls", "xnut", "znut")})
+    pg, po = g.download("prd1"), o.download("prd1")
+    worst["prd1(mean-free)"] = rel_err(pg - pg.mean(), po - po.mean())
+    assert max(worst.values()) <= 1e-10, worst
 
 
 def test_nan_is_reported_not_faulted(pkg, orc):
