@@ -248,6 +248,11 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        # torchrun starts every rank with OMP_NUM_THREADS=1; the other ranks exit without
+        # work, so rank 0 takes every host core it may run on (read when the OpenMP oracle
+        # library loads, below)
+        os.environ["OMP_NUM_THREADS"] = str(len(os.sched_getaffinity(0)))
     pkg = load_pkg()
     p, init = pkg.cases.sloshing(nx=args.nx, ny=args.ny, nz=args.nz, dx=args.dx, cg_tol=args.cg_tol)
     sys.path.insert(0, str(ROOT / "oracle"))
