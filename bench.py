@@ -69,6 +69,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-cap", type=int, default=20, help="CG iterations per solve in the CPU sample")
+    ap.add_argument("--cpu-serial-cap", type=int, default=5,
+                    help="CG iterations per solve in the one-thread CPU sample (0: skip it)")
     return ap.parse_args()
 
 
@@ -196,8 +198,9 @@ def profiled_traffic(kernel: str, ncell: int):
 
 
 # ------------------------------------------------------------------------------ CPU sample
-def cpu_sample(pkg, p, init, cap: int, full_iters: float | None):
-    """Time one step of the CPU restatement (OpenMP) on the host cores.
+def cpu_sample(pkg, p, init, cap: int, full_iters: float | None, openmp: bool = True):
+    """Time one step of the CPU restatement on the host cores (OpenMP build), or on one
+    thread (serial build, like the reference's own single-threaded program).
 
     Sample: one full step of everything but the Poisson iterations, with each of the three
     Poisson solves capped at `cap` iterations, plus two more capped solves to separate the
@@ -208,7 +211,7 @@ def cpu_sample(pkg, p, init, cap: int, full_iters: float | None):
 
     q = p.copy()
     q.cg_maxit = cap
-    o = oracle.Oracle(q, openmp=True)
+    o = oracle.Oracle(q, openmp=openmp)
     init(o)
     t0 = time.perf_counter()
     t_cg = 0.0
@@ -227,7 +230,7 @@ def cpu_sample(pkg, p, init, cap: int, full_iters: float | None):
     o.contorno(2)
     t1 = time.perf_counter(); o.graddin(); ta = time.perf_counter() - t1
     q2 = q.copy(); q2.cg_maxit = 2 * cap
-    o2 = oracle.Oracle(q2, openmp=True)
+    o2 = oracle.Oracle(q2, openmp=openmp)
     for name in ("u", "v", "w", "prd1", "rho", "ls"):
         o2.upload(name, o.download(name))
     o2.set_dt(o.a_dt[0]); o2.contorno(2)
@@ -236,7 +239,7 @@ def cpu_sample(pkg, p, init, cap: int, full_iters: float | None):
     t_setup = max(ta - cap * t_iter, 0.0)
     iters = full_iters if full_iters is not None else 3 * cap
     t_step = t_noncg + 3 * t_setup + iters * t_iter
-    cores = oracle.num_threads(True)
+    cores = oracle.num_threads(openmp)
     return {
         "t_step_s": t_step, "t_noncg_s": t_noncg, "t_iter_s": t_iter, "t_setup_s": t_setup,
         "iters_per_step": iters, "cores": cores, "sample_wall_s": t_step_capped + ta + tb,
@@ -579,6 +582,14 @@ def run_ours(args):
                           f"{args.cpu_cap} iterations, scaled to the {ref_iters:.0f} iterations per step the GPU "
                           f"measured: non-Poisson {cs['t_noncg_s']:.2f} s + {cs['t_iter_s'] * 1e3:.2f} ms/iteration"),
                "detail": cs}
+        if args.cpu_serial_cap > 0:
+            ss = cpu_sample(pkg, p, init, args.cpu_serial_cap, ref_iters, openmp=False)
+            cpu["one_thread"] = {
+                "value": 1.0 / ss["t_step_s"], "unit": UNIT, "cores": ss["cores"], "kind": "port",
+                "sample": (f"the same step on one thread (serial build, as the reference runs), Poisson solves "
+                           f"capped at {args.cpu_serial_cap} iterations and scaled to {ref_iters:.0f}: non-Poisson "
+                           f"{ss['t_noncg_s']:.2f} s + {ss['t_iter_s'] * 1e3:.2f} ms/iteration"),
+                "detail": ss}
     mms = None
     if dist.world == 1 and args.mms_n > 0:
         mms = mms_check(pkg, args, dev)

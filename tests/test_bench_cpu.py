@@ -67,3 +67,17 @@ def test_plain_roofline_from_tracer(bench, pkg):
     assert abs(r["cg_iteration"]["us"] - t_it * 1e6) < 1e-9
     assert abs(r["avg_launch_us"] - t_it * share * 1e6) < 1e-9
     assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
+
+
+@pytest.mark.parametrize("openmp", [False, True])
+def test_cpu_sample_scaling(bench, pkg, openmp):
+    """The CPU baseline's step estimate: the capped step's non-Poisson time plus three solve
+    set-ups plus the measured iteration count times the per-iteration cost; the serial build
+    runs on one thread."""
+    p, init = pkg.cases.sloshing(nx=16, ny=8, nz=8, dx=0.04, cg_tol=1e-8)
+    s = bench.cpu_sample(pkg, p, init, 3, 40.0, openmp=openmp)
+    assert s["t_noncg_s"] > 0 and s["t_iter_s"] > 0 and s["iters_per_step"] == 40.0
+    want = s["t_noncg_s"] + 3 * s["t_setup_s"] + 40.0 * s["t_iter_s"]
+    assert abs(s["t_step_s"] - want) <= 1e-12 * want
+    if not openmp:
+        assert s["cores"] == 1
