@@ -100,6 +100,8 @@ struct Oracle {
     void level_set();
     void visco();
     void classico(Arr& uint_, Arr& vint, Arr& wint);
+    void rotacional(Arr& uint_, Arr& vint, Arr& wint);
+    void antissim(Arr& uint_, Arr& vint, Arr& wint);
     void convdiff();
     void tempo(int tt, int it);
     void contorno(int nlock);
@@ -802,13 +804,203 @@ void Oracle::classico(Arr& uint_, Arr& vint, Arr& wint) {
             }
 }
 
+/* The velocity splits c+ = max(c, 0), c- = min(c, 0) of rotacional and antissim, held in
+ * arrays of extents (0:nx1+1, 0:ny1+1, 0:nz1+1) shared by the three components. */
+struct Splits {
+    Arr ap, an, bp, bn, dp, dn;
+    Splits(int nx1, int ny1, int nz1) {
+        for (Arr* a : {&ap, &an, &bp, &bn, &dp, &dn}) a->init(0, nx1 + 1, 0, ny1 + 1, 0, nz1 + 1);
+    }
+    void set(int i, int j, int k, double a, double b, double d) {
+        ap(i, j, k) = fmax2(a, 0.); an(i, j, k) = fmin2(a, 0.);
+        bp(i, j, k) = fmax2(b, 0.); bn(i, j, k) = fmin2(b, 0.);
+        dp(i, j, k) = fmax2(d, 0.); dn(i, j, k) = fmin2(d, 0.);
+    }
+};
+
+/* rotacional — 7_advectivo.f90:293-457 (der = 1; the reference stops for any other scheme):
+ * first-order upwind differences of the fluxes c+ a and c- a.  The reference's w part sets
+ * dp where dn is meant one plane above the top w-face (:433), leaving dn there unset (its
+ * value is indeterminate); here it is min(w, 0) of that ghost, as the u and v parts do at
+ * their ends.  It enters only Fw on the top face, which the boundary fill overwrites. */
+void Oracle::rotacional(Arr& uint_, Arr& vint, Arr& wint) {
+    if (P.der != 1) { std::fprintf(stderr, "oracle: rotacional needs der = 1\n"); std::abort(); }
+    Splits S(nx1, ny1, nz1);
+    Arr &ap = S.ap, &an = S.an, &bp = S.bp, &bn = S.bn, &dp = S.dp, &dn = S.dn;
+    /* u (:335-370) */
+    for (int k = 0; k <= nz + 1; ++k)
+        for (int j = 0; j <= ny + 1; ++j)
+            for (int i = 1; i <= nx + 1; ++i) {
+                const double bma = (v(i, j, k) + v(i - 1, j, k) + v(i, j + 1, k) + v(i - 1, j + 1, k)) * 0.25;
+                const double dma = (w(i, j, k) + w(i - 1, j, k) + w(i, j, k + 1) + w(i - 1, j, k + 1)) * 0.25;
+                S.set(i, j, k, u(i, j, k), bma, dma);
+            }
+    for (int k = 0; k <= nz + 1; ++k)
+        for (int j = 0; j <= ny + 1; ++j) {
+            ap(0, j, k) = fmax2(u(0, j, k), 0.);
+            an(nx1 + 1, j, k) = fmin2(u(nx1 + 1, j, k), 0.);
+        }
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx1; ++i) {
+                const double dudx = (ap(i, j, k) * u(i, j, k) - ap(i - 1, j, k) * u(i - 1, j, k)) / dx +
+                                    (an(i + 1, j, k) * u(i + 1, j, k) - an(i, j, k) * u(i, j, k)) / dx;
+                const double dudy = (bp(i, j, k) * u(i, j, k) - bp(i, j - 1, k) * u(i, j - 1, k)) / dy +
+                                    (bn(i, j + 1, k) * u(i, j + 1, k) - bn(i, j, k) * u(i, j, k)) / dy;
+                const double dudz = (dp(i, j, k) * u(i, j, k) - dp(i, j, k - 1) * u(i, j, k - 1)) / dz +
+                                    (dn(i, j, k + 1) * u(i, j, k + 1) - dn(i, j, k) * u(i, j, k)) / dz;
+                uint_(i, j, k) = dudx + dudy + dudz;
+            }
+    /* v (:373-409) */
+    for (int k = 0; k <= nz + 1; ++k)
+        for (int j = 1; j <= ny + 1; ++j)
+            for (int i = 0; i <= nx + 1; ++i) {
+                const double amb = (u(i, j, k) + u(i + 1, j, k) + u(i, j - 1, k) + u(i + 1, j - 1, k)) * 0.25;
+                const double dmb = (w(i, j, k) + w(i, j - 1, k) + w(i, j, k + 1) + w(i, j - 1, k + 1)) * 0.25;
+                S.set(i, j, k, amb, v(i, j, k), dmb);
+            }
+    for (int k = 0; k <= nz + 1; ++k)
+        for (int i = 0; i <= nx + 1; ++i) {
+            bp(i, 0, k) = fmax2(v(i, 0, k), 0.);
+            bn(i, ny1 + 1, k) = fmin2(v(i, ny1 + 1, k), 0.);
+        }
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny1; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                const double dvdx = (ap(i, j, k) * v(i, j, k) - ap(i - 1, j, k) * v(i - 1, j, k)) / dx +
+                                    (an(i + 1, j, k) * v(i + 1, j, k) - an(i, j, k) * v(i, j, k)) / dx;
+                const double dvdy = (bp(i, j, k) * v(i, j, k) - bp(i, j - 1, k) * v(i, j - 1, k)) / dy +
+                                    (bn(i, j + 1, k) * v(i, j + 1, k) - bn(i, j, k) * v(i, j, k)) / dy;
+                const double dvdz = (dp(i, j, k) * v(i, j, k) - dp(i, j, k - 1) * v(i, j, k - 1)) / dz +
+                                    (dn(i, j, k + 1) * v(i, j, k + 1) - dn(i, j, k) * v(i, j, k)) / dz;
+                vint(i, j, k) = dvdx + dvdy + dvdz;
+            }
+    /* w (:412-446) */
+    for (int k = 1; k <= nz + 1; ++k)
+        for (int j = 0; j <= ny + 1; ++j)
+            for (int i = 0; i <= nx + 1; ++i) {
+                const double amd = (u(i, j, k) + u(i + 1, j, k) + u(i, j, k - 1) + u(i + 1, j, k - 1)) * 0.25;
+                const double bmd = (v(i, j, k) + v(i, j + 1, k) + v(i, j, k - 1) + v(i, j + 1, k - 1)) * 0.25;
+                S.set(i, j, k, amd, bmd, w(i, j, k));
+            }
+    for (int j = 0; j <= ny + 1; ++j)
+        for (int i = 0; i <= nx + 1; ++i) {
+            dp(i, j, 0) = fmax2(w(i, j, 0), 0.);
+            dn(i, j, nz1 + 1) = fmin2(w(i, j, nz1 + 1), 0.);
+        }
+    for (int k = 1; k <= nz1; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                const double dwdx = (ap(i, j, k) * w(i, j, k) - ap(i - 1, j, k) * w(i - 1, j, k)) / dx +
+                                    (an(i + 1, j, k) * w(i + 1, j, k) - an(i, j, k) * w(i, j, k)) / dx;
+                const double dwdy = (bp(i, j, k) * w(i, j, k) - bp(i, j - 1, k) * w(i, j - 1, k)) / dy +
+                                    (bn(i, j + 1, k) * w(i, j + 1, k) - bn(i, j, k) * w(i, j, k)) / dy;
+                const double dwdz = (dp(i, j, k) * w(i, j, k) - dp(i, j, k - 1) * w(i, j, k - 1)) / dz +
+                                    (dn(i, j, k + 1) * w(i, j, k + 1) - dn(i, j, k) * w(i, j, k)) / dz;
+                wint(i, j, k) = dwdx + dwdy + dwdz;
+            }
+}
+
+/* antissim — 7_advectivo.f90:460-653 (der = 1 only): the mean of the flux-difference form of
+ * rotacional and the advective upwind form, with the split arrays' end planes filled by
+ * copies of their neighbours (:521-524, 571-574, 618-621). */
+void Oracle::antissim(Arr& uint_, Arr& vint, Arr& wint) {
+    if (P.der != 1) { std::fprintf(stderr, "oracle: antissim needs der = 1\n"); std::abort(); }
+    Splits S(nx1, ny1, nz1);
+    Arr &ap = S.ap, &an = S.an, &bp = S.bp, &bn = S.bn, &dp = S.dp, &dn = S.dn;
+    /* the copies ap(0,:,:) = ap(1,:,:), bp(:,0,:) = bp(:,1,:), dp(:,:,0) = dp(:,:,1) */
+    auto low_copies = [&]() {
+        for (int k = 0; k <= nz1 + 1; ++k)
+            for (int j = 0; j <= ny1 + 1; ++j) ap(0, j, k) = ap(1, j, k);
+        for (int k = 0; k <= nz1 + 1; ++k)
+            for (int i = 0; i <= nx1 + 1; ++i) bp(i, 0, k) = bp(i, 1, k);
+        for (int j = 0; j <= ny1 + 1; ++j)
+            for (int i = 0; i <= nx1 + 1; ++i) dp(i, j, 0) = dp(i, j, 1);
+    };
+    /* one direction of one component: F at m-1, m, m+1, the splits P, N at m-1, m, m+1 */
+    auto term = [](double Fm, double F0, double Fp, double Pm, double P0, double N0, double Np, double h) {
+        return ((P0 * F0 - Pm * Fm) / h + (Np * Fp - N0 * F0) / h + P0 * (F0 - Fm) / h + N0 * (Fp - F0) / h) * 0.5;
+    };
+    /* u (:503-545) */
+    for (int k = 1; k <= nz + 1; ++k)
+        for (int j = 1; j <= ny + 1; ++j)
+            for (int i = 1; i <= nx + 1; ++i) {
+                const double bma = (v(i, j, k) + v(i - 1, j, k) + v(i, j + 1, k) + v(i - 1, j + 1, k)) * 0.25;
+                const double dma = (w(i, j, k) + w(i - 1, j, k) + w(i, j, k + 1) + w(i - 1, j, k + 1)) * 0.25;
+                S.set(i, j, k, u(i, j, k), bma, dma);
+            }
+    low_copies();
+    for (int k = 0; k <= nz1 + 1; ++k)
+        for (int j = 0; j <= ny1 + 1; ++j) an(nx1 + 1, j, k) = an(nx1, j, k);
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx1; ++i) {
+                const double dudx = term(u(i - 1, j, k), u(i, j, k), u(i + 1, j, k), ap(i - 1, j, k), ap(i, j, k),
+                                         an(i, j, k), an(i + 1, j, k), dx);
+                const double dudy = term(u(i, j - 1, k), u(i, j, k), u(i, j + 1, k), bp(i, j - 1, k), bp(i, j, k),
+                                         bn(i, j, k), bn(i, j + 1, k), dy);
+                const double dudz = term(u(i, j, k - 1), u(i, j, k), u(i, j, k + 1), dp(i, j, k - 1), dp(i, j, k),
+                                         dn(i, j, k), dn(i, j, k + 1), dz);
+                uint_(i, j, k) = dudx + dudy + dudz;
+            }
+    /* v (:549-595) */
+    for (int k = 1; k <= nz + 1; ++k)
+        for (int j = 1; j <= ny + 1; ++j)
+            for (int i = 1; i <= nx + 1; ++i) {
+                const double amb = (u(i, j, k) + u(i + 1, j, k) + u(i, j - 1, k) + u(i + 1, j - 1, k)) * 0.25;
+                const double dmb = (w(i, j, k) + w(i, j - 1, k) + w(i, j, k + 1) + w(i, j - 1, k + 1)) * 0.25;
+                S.set(i, j, k, amb, v(i, j, k), dmb);
+            }
+    low_copies();
+    for (int k = 0; k <= nz1 + 1; ++k)
+        for (int i = 0; i <= nx1 + 1; ++i) bn(i, ny1 + 1, k) = bn(i, ny1, k);
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny1; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                const double dvdx = term(v(i - 1, j, k), v(i, j, k), v(i + 1, j, k), ap(i - 1, j, k), ap(i, j, k),
+                                         an(i, j, k), an(i + 1, j, k), dx);
+                const double dvdy = term(v(i, j - 1, k), v(i, j, k), v(i, j + 1, k), bp(i, j - 1, k), bp(i, j, k),
+                                         bn(i, j, k), bn(i, j + 1, k), dy);
+                const double dvdz = term(v(i, j, k - 1), v(i, j, k), v(i, j, k + 1), dp(i, j, k - 1), dp(i, j, k),
+                                         dn(i, j, k), dn(i, j, k + 1), dz);
+                vint(i, j, k) = dvdx + dvdy + dvdz;
+            }
+    /* w (:598-640) */
+    for (int k = 1; k <= nz + 1; ++k)
+        for (int j = 1; j <= ny + 1; ++j)
+            for (int i = 1; i <= nx + 1; ++i) {
+                const double amd = (u(i, j, k) + u(i + 1, j, k) + u(i, j, k - 1) + u(i + 1, j, k - 1)) * 0.25;
+                const double bmd = (v(i, j, k) + v(i, j + 1, k) + v(i, j, k - 1) + v(i, j + 1, k - 1)) * 0.25;
+                S.set(i, j, k, amd, bmd, w(i, j, k));
+            }
+    low_copies();
+    for (int j = 0; j <= ny1 + 1; ++j)
+        for (int i = 0; i <= nx1 + 1; ++i) dn(i, j, nz1 + 1) = dn(i, j, nz1);
+    for (int k = 1; k <= nz1; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                const double dwdx = term(w(i - 1, j, k), w(i, j, k), w(i + 1, j, k), ap(i - 1, j, k), ap(i, j, k),
+                                         an(i, j, k), an(i + 1, j, k), dx);
+                const double dwdy = term(w(i, j - 1, k), w(i, j, k), w(i, j + 1, k), bp(i, j - 1, k), bp(i, j, k),
+                                         bn(i, j, k), bn(i, j + 1, k), dy);
+                const double dwdz = term(w(i, j, k - 1), w(i, j, k), w(i, j, k + 1), dp(i, j, k - 1), dp(i, j, k),
+                                         dn(i, j, k), dn(i, j, k + 1), dz);
+                wint(i, j, k) = dwdx + dwdy + dwdz;
+            }
+}
+
 /* convdiff — 6_convdiff.f90:14-189.  The sponge term -(w-0)*epis_z with epis_z = 0
  * (:65, call commented out at :86) is omitted; it changes at most the sign of a zero. */
 void Oracle::convdiff() {
     prd0.a = prd1.a;                                    /* :62 */
     Arr uint_, vint, wint;
     uint_.init(1, nx1, 1, ny, 1, nz); vint.init(1, nx, 1, ny1, 1, nz); wint.init(1, nx, 1, ny, 1, nz1);
-    classico(uint_, vint, wint);
+    if (P.adv_type == 2)                                /* :72-79 */
+        rotacional(uint_, vint, wint);
+    else if (P.adv_type == 3)
+        antissim(uint_, vint, wint);
+    else
+        classico(uint_, vint, wint);
     Arr rhox, rhoy, rhoz, dhsdx, dhsdy, dhsdz, tx, ty, tz;
     interpx_cf(rho, nx, ny, nz, rhox);
     interpy_cf(rho, nx, ny, nz, rhoy);

@@ -10,6 +10,7 @@
 // partials done by the last block to finish (no floating-point atomics).
 #include <cuda_runtime.h>
 #include <cmath>
+#include "advect.cuh"
 #include "ctx.cuh"
 #include "pdl.cuh"
 #include "reduce.cuh"
@@ -405,7 +406,8 @@ __device__ __forceinline__ R classico_hi(const double* __restrict__ a, int c, co
     return acc;
 }
 
-template <typename R, int DER>
+// DER: classico's scheme (adv_type = 1); ADV: 2 rotacional, 3 antissim (advect.cuh; der = 1)
+template <typename R, int DER, int ADV>
 __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) {
     const Thread3 t = tid3(1, 1, 1);
     const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
@@ -423,7 +425,9 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
         const R uc = AT(u, 0, 0, 0);
         const int ic = clampi(i, 2, nx);
         R uint_;
-        if constexpr (DER == 1) {
+        if constexpr (ADV != 1) {
+            uint_ = split_form_u<R, ADV>(FaceTaps<R>{c0, px, pxy}, u, v, w, i, j, k, nx, idx, idy, idz);
+        } else if constexpr (DER == 1) {
             const R bma4 = (AT(v, 0, 0, 0) + AT(v, -1, 0, 0) + AT(v, 0, 1, 0) + AT(v, -1, 1, 0)) * R(0.25);
             const R dma4 = (AT(w, 0, 0, 0) + AT(w, -1, 0, 0) + AT(w, 0, 0, 1) + AT(w, -1, 0, 1)) * R(0.25);
             R a1 = pmax(uc, R(0.)), a2 = pmin(uc, R(0.));
@@ -469,7 +473,9 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
         const R vc = AT(v, 0, 0, 0);
         const int jc = clampi(j, 2, ny);
         R vint;
-        if constexpr (DER == 1) {
+        if constexpr (ADV != 1) {
+            vint = split_form_v<R, ADV>(FaceTaps<R>{c0, px, pxy}, u, v, w, i, j, k, ny, idx, idy, idz);
+        } else if constexpr (DER == 1) {
             const R amb4 = (AT(u, 0, 0, 0) + AT(u, 1, 0, 0) + AT(u, 0, -1, 0) + AT(u, 1, -1, 0)) * R(0.25);
             const R dmb4 = (AT(w, 0, 0, 0) + AT(w, 0, -1, 0) + AT(w, 0, 0, 1) + AT(w, 0, -1, 1)) * R(0.25);
             R a1 = pmax(amb4, R(0.)), a2 = pmin(amb4, R(0.));
@@ -514,7 +520,9 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
         const R wc = AT(w, 0, 0, 0);
         const int kc = clampi(k, 2, nz);
         R wint;
-        if constexpr (DER == 1) {
+        if constexpr (ADV != 1) {
+            wint = split_form_w<R, ADV>(FaceTaps<R>{c0, px, pxy}, u, v, w, i, j, k, nz, idx, idy, idz);
+        } else if constexpr (DER == 1) {
             const R amd4 = (AT(u, 0, 0, 0) + AT(u, 1, 0, 0) + AT(u, 0, 0, -1) + AT(u, 1, 0, -1)) * R(0.25);
             const R bmd4 = (AT(v, 0, 0, 0) + AT(v, 0, 1, 0) + AT(v, 0, 0, -1) + AT(v, 0, 1, -1)) * R(0.25);
             R a1 = pmax(amd4, R(0.)), a2 = pmin(amd4, R(0.));
@@ -1280,10 +1288,18 @@ void launch_visco(suli_ctx* c) {
 template <typename R>
 static void convdiff_der(suli_ctx* c, const CDConst& C, const CDFields& F) {
     const Geo& G = c->g;
+    if (c->P.adv_type == 2) {
+        k_convdiff<R, 1, 2><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F);
+        return;
+    }
+    if (c->P.adv_type == 3) {
+        k_convdiff<R, 1, 3><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F);
+        return;
+    }
     switch (c->P.der) {
-    case 2: k_convdiff<R, 2><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F); break;
-    case 3: k_convdiff<R, 3><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F); break;
-    default: k_convdiff<R, 1><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F); break;
+    case 2: k_convdiff<R, 2, 1><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F); break;
+    case 3: k_convdiff<R, 3, 1><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F); break;
+    default: k_convdiff<R, 1, 1><<<faces_grid(G), kBlk, 0, c->stream>>>(G, C, F); break;
     }
 }
 void launch_convdiff(suli_ctx* c) {

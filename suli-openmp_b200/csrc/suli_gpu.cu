@@ -114,8 +114,11 @@ int validate(const suli_params* p, std::string& why) {
     if (p->ccz0 < 0 || p->ccz0 > 3 || p->cczf < 0 || p->cczf > 3) { why = "ccz0/cczf out of range"; return SULI_ERR_ARG; }
     if (p->obst_t != 0) { why = "obstacles (obst_t != 0) are not built"; return SULI_ERR_UNSUPPORTED; }
     if (p->t_hs != 0) { why = "t_hs != 0 is not built"; return SULI_ERR_UNSUPPORTED; }
-    if (p->adv_type != 1) { why = "only adv_type = 1 (classic advective form) is built"; return SULI_ERR_UNSUPPORTED; }
+    if (p->adv_type < 1 || p->adv_type > 3) { why = "adv_type must be 1 (classico), 2 (rotacional) or 3 (antissim)"; return SULI_ERR_ARG; }
     if (p->der < 1 || p->der > 3) { why = "der must be 1 (upwind), 2 (centred) or 3 (2nd-order upwind)"; return SULI_ERR_ARG; }
+    if (p->adv_type != 1 && p->der != 1) {   // the reference stops there (7_advectivo.f90:450-451, 646-647)
+        why = "adv_type 2 and 3 exist only with der = 1"; return SULI_ERR_ARG;
+    }
     if (p->m_turb < 0 || p->m_turb > 2) { why = "m_turb must be 0, 1 or 2"; return SULI_ERR_ARG; }
     if (p->t_tempo < 0 || p->t_tempo > 3) { why = "t_tempo out of range"; return SULI_ERR_ARG; }
     if (p->precision != 0 && p->precision != 1) { why = "precision must be 0 (FP64) or 1 (mixed)"; return SULI_ERR_ARG; }

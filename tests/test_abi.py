@@ -85,15 +85,17 @@ def test_invalid_parameters_rejected(pkg):
     p.obst_t = 3                    # obstacles are not built
     assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_UNSUPPORTED
     p = pkg.default_params()
-    p.adv_type = 2                  # rotational form is not built
-    assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_UNSUPPORTED
-    p = pkg.default_params()
     p.nx = 3                        # WENO needs 4 cells per direction
     assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_ARG
-    for field, bad in (("der", 0), ("der", 4), ("m_turb", -1), ("m_turb", 3)):
+    # the reference defines der 1-3, adv_type 1-3 and m_turb 0-2 (0_modules.f90:26-31)
+    for field, bad in (("der", 0), ("der", 4), ("m_turb", -1), ("m_turb", 3), ("adv_type", 0), ("adv_type", 4)):
         p = pkg.default_params()
-        setattr(p, field, bad)      # the reference defines der 1-3 and m_turb 0-2 (0_modules.f90:26,31)
+        setattr(p, field, bad)
         assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_ARG, (field, bad)
+    for adv in (2, 3):              # rotacional and antissim stop for any scheme but upwind
+        p = pkg.default_params()
+        p.adv_type, p.der = adv, 2
+        assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_ARG, adv
 
 
 def test_no_oracle_in_product(pkg):

@@ -105,14 +105,14 @@ def test_vector_kernels_match_one_cell_kernels(pkg, case):
         assert float(np.abs(v0[f] - v1[f]).max()) <= 1e-9 * vs, f
 
 
-@pytest.mark.parametrize("der, m_turb", [(1, 1), (2, 2), (3, 2)])
-def test_mixed_stencils_track_fp64(pkg, orc, der, m_turb):
-    """visco and convdiff in FP32 arithmetic (precision 1), every advection scheme and both
-    Smagorinsky models, against the FP64 oracle on the same state: face viscosities and
-    forces within 1e-5 of each field's scale (FP32 rounding of terms no larger than the
+@pytest.mark.parametrize("der, adv, m_turb", [(1, 1, 1), (2, 1, 2), (3, 1, 2), (1, 2, 1), (1, 3, 2)])
+def test_mixed_stencils_track_fp64(pkg, orc, der, adv, m_turb):
+    """visco and convdiff in FP32 arithmetic (precision 1), every advective form and scheme
+    and both Smagorinsky models, against the FP64 oracle on the same state: face viscosities
+    and forces within 1e-5 of each field's scale (FP32 rounding of terms no larger than the
     field's scale)."""
     p = small_params(nx=16, ny=12, nz=8, m_turb=m_turb)
-    p.der = der
+    p.der, p.adv_type = der, adv
     q = p.copy()
     q.precision, q.cg_stop = 1, 1
     o, st = _prepared(pkg, orc, p, 41)

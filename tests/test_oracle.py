@@ -497,3 +497,97 @@ def test_visco_directional_on_shear(orc):
     np.testing.assert_allclose(o.download("xnut"), want, rtol=1e-12)
     np.testing.assert_allclose(o.download("znut"), p.dz * p.dz * p.csmag ** 2 * abs(g) / math.sqrt(2.), rtol=1e-12)
     assert np.abs(o.download("ynut")).max() <= 1e-14 * want
+
+
+# ------------------------------------------- rotacional and antissim (adv_type 2, 3)
+def split_form_py(p, U, V, W, adv):
+    """Per-face restatement of rotacional (adv = 2, 7_advectivo.f90:293-457) and antissim
+    (adv = 3, :460-653), first-order upwind: every value of the split arrays c+ = max(c, 0),
+    c- = min(c, 0) is written as the point it is read from.  antissim's end-plane copies
+    (:521-524, 571-574, 618-621) read c+ below the first point at the first point and c-
+    past a component's last face at that face.  rotacional's unset c- above the top w-face
+    (:433 sets c+ there) is taken as min(w, 0) of that ghost."""
+    nx, ny, nz = p.nx, p.ny, p.nz
+    h = (p.dx, p.dy, p.dz)
+    bma = lambda i, j, k: (V(i, j, k) + V(i - 1, j, k) + V(i, j + 1, k) + V(i - 1, j + 1, k)) * 0.25
+    dma = lambda i, j, k: (W(i, j, k) + W(i - 1, j, k) + W(i, j, k + 1) + W(i - 1, j, k + 1)) * 0.25
+    amb = lambda i, j, k: (U(i, j, k) + U(i + 1, j, k) + U(i, j - 1, k) + U(i + 1, j - 1, k)) * 0.25
+    dmb = lambda i, j, k: (W(i, j, k) + W(i, j - 1, k) + W(i, j, k + 1) + W(i, j - 1, k + 1)) * 0.25
+    amd = lambda i, j, k: (U(i, j, k) + U(i + 1, j, k) + U(i, j, k - 1) + U(i + 1, j, k - 1)) * 0.25
+    bmd = lambda i, j, k: (V(i, j, k) + V(i, j + 1, k) + V(i, j, k - 1) + V(i, j + 1, k - 1)) * 0.25
+    comps = {"u": (U, (nx + 1, ny, nz), (U, bma, dma), 0),
+             "v": (V, (nx, ny + 1, nz), (amb, V, dmb), 1),
+             "w": (W, (nx, ny, nz + 1), (amd, bmd, W), 2)}
+    out = {}
+    for name, (F, n, vel, own) in comps.items():
+        res = {}
+        for k in range(1, n[2] + 1):
+            for j in range(1, n[1] + 1):
+                for i in range(1, n[0] + 1):
+                    s = 0.
+                    for d in range(3):
+                        e, m = E3[d], (i, j, k)[d]
+                        at = lambda f, o: f(i + o * e[0], j + o * e[1], k + o * e[2])
+                        om = -1 if (adv == 2 or m > 1) else 0
+                        op = 1 if (adv == 2 or d != own or m < n[d]) else 0
+                        c0 = at(vel[d], 0)
+                        Pm, P0 = fmax2(at(vel[d], om), 0.), fmax2(c0, 0.)
+                        N0, Np = fmin2(c0, 0.), fmin2(at(vel[d], op), 0.)
+                        Fm, F0, Fp = at(F, -1), at(F, 0), at(F, 1)
+                        t = (P0 * F0 - Pm * Fm) / h[d] + (Np * Fp - N0 * F0) / h[d]
+                        if adv == 3:
+                            t = (t + P0 * (F0 - Fm) / h[d] + N0 * (Fp - F0) / h[d]) * 0.5
+                        s = t if d == 0 else s + t
+                    res[(i, j, k)] = s
+        out[name] = res
+    return out
+
+
+@pytest.mark.parametrize("adv", [2, 3])
+@pytest.mark.parametrize("bc", [(2, 2, 2, 2, 2, 1), (0, 0, 1, 1, 2, 1)])
+def test_split_forms_match_per_face_restatement(orc, adv, bc):
+    p = small_params(nx=6, ny=5, nz=4, bc=bc)
+    p.adv_type = adv
+    o, p = advection_only(orc, p, seeded_state(p, 25))
+    o.contorno(1)
+    # the ghosts beyond the walls take arbitrary values, so that every end-plane rule matters
+    rng = np.random.default_rng(26)
+    for f in ("u", "v", "w"):
+        a = o.download(f)
+        ghost = np.ones(a.shape, bool)
+        ghost[1:-1, 1:-1, 1:-1] = False
+        a[ghost] = rng.standard_normal(int(ghost.sum()))
+        o.upload(f, a)
+    U, V, W = (fortran_view(o, p, f) for f in ("u", "v", "w"))
+    want = split_form_py(p, U, V, W, adv)
+    o.convdiff()
+    for comp, F in (("u", "Fu"), ("v", "Fv"), ("w", "Fw")):
+        got = fortran_view(o, p, F)
+        bad = [(ijk, got(*ijk), -x) for ijk, x in want[comp].items() if got(*ijk) != -x]
+        assert not bad, (comp, bad[:3])
+
+
+def test_rotational_form_on_linear_velocity(orc):
+    """rotacional is the upwind difference of the fluxes: for u = a (x + x0) > 0 and
+    v = -a (y + y0) < 0 everywhere (halo included), w = 0, the u-term is
+    (u_i^2 - u_{i-1}^2)/dx + u (v_{j+1/2} - v_{j-1/2})/dy-averaged = a^2 (x + x0 - dx), exactly
+    up to rounding, and the v-term a^2 (y + y0 + dy)."""
+    p = small_params(nx=7, ny=6, nz=5)
+    p.adv_type = 2
+    a, x0, y0 = 1.3, 0.1, 0.1
+    abi = pkg_abi()
+    st = seeded_state(p, 27)
+    (l0, h0), _, _ = abi.field_extent(p, "u")
+    xf = (np.arange(l0, h0 + 1) - 1) * p.dx + x0
+    st["u"] = np.broadcast_to((a * xf)[:, None, None], abi.field_shape(p, "u")).copy()
+    _, (l1, h1), _ = abi.field_extent(p, "v")
+    yf = (np.arange(l1, h1 + 1) - 1) * p.dy + y0
+    st["v"] = np.broadcast_to((-a * yf)[None, :, None], abi.field_shape(p, "v")).copy()
+    st["w"] = np.zeros(abi.field_shape(p, "w"))
+    o, p = advection_only(orc, p, st)
+    o.convdiff()
+    Fu, Fv = o.download("Fu"), o.download("Fv")
+    np.testing.assert_allclose(-Fu, np.broadcast_to((a * a * (xf[1:-1] - p.dx))[:, None, None], Fu.shape),
+                               rtol=0, atol=1e-11 * a * a)
+    np.testing.assert_allclose(-Fv, np.broadcast_to((a * a * (yf[1:-1] + p.dy))[None, :, None], Fv.shape),
+                               rtol=0, atol=1e-11 * a * a)

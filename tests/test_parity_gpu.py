@@ -84,17 +84,18 @@ def test_visco(pkg, orc, bc, m_turb):
     compare(g, o, OUT_FIELDS["visco"], what=f"visco m_turb={m_turb}")
 
 
-@pytest.mark.parametrize("der", [1, 2, 3])
+@pytest.mark.parametrize("der, adv", [(1, 1), (2, 1), (3, 1), (1, 2), (1, 3)])
 @pytest.mark.parametrize("bc", BCS)
-def test_convdiff(pkg, orc, bc, der):
-    """Advection schemes of classico (7_advectivo.f90:33-285): 1 upwind, 2 centred,
-    3 second-order upwind."""
+def test_convdiff(pkg, orc, bc, der, adv):
+    """Advective forms of 6_convdiff.f90:72-79: classico (adv_type 1) with its schemes
+    1 upwind, 2 centred, 3 second-order upwind (7_advectivo.f90:33-285); rotacional
+    (adv_type 2, :293-457) and antissim (adv_type 3, :460-653), upwind."""
     p = small_params(nx=13, ny=11, nz=9, bc=bc)
-    p.der = der
+    p.der, p.adv_type = der, adv
     g, o = pair(pkg, orc, p, seed=3)
     for m in (g, o):
         m.convdiff()
-    compare(g, o, OUT_FIELDS["convdiff"], what=f"convdiff der={der}")
+    compare(g, o, OUT_FIELDS["convdiff"], what=f"convdiff der={der} adv_type={adv}")
 
 
 def test_convdiff_with_forcing(pkg, orc):
@@ -276,14 +277,15 @@ def test_step_parity_dam_break(pkg, orc):
     assert sg["max_div"] <= 1e-8
 
 
-@pytest.mark.parametrize("der", [2, 3])
-def test_step_parity_schemes(pkg, orc, der):
-    """Five whole dam-break steps with the centred / second-order upwind advection and the
-    directional Smagorinsky model (m_turb = 2): every state field within 1e-10 of its own
-    scale, the velocity components within 1e-10 of the velocity scale (v, across the tank,
-    is orders of magnitude below u in this nearly two-dimensional flow)."""
+@pytest.mark.parametrize("der, adv", [(2, 1), (3, 1), (1, 2), (1, 3)])
+def test_step_parity_schemes(pkg, orc, der, adv):
+    """Five whole dam-break steps with the centred or second-order upwind classico, the
+    rotacional or antissim form, and the directional Smagorinsky model (m_turb = 2): every
+    state field within 1e-10 of its own scale, the velocity components within 1e-10 of the
+    velocity scale (v, across the tank, is orders of magnitude below u in this nearly
+    two-dimensional flow)."""
     p, init = pkg.cases.dam_break(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-12)
-    p.der, p.m_turb = der, 2
+    p.der, p.adv_type, p.m_turb = der, adv, 2
     g = pkg.Solver(p)
     o = orc.Oracle(p)
     init(g)
