@@ -62,7 +62,7 @@ typedef struct suli_params {
     int    ccz0, cczf;              /* z walls: 1 free-slip 2 no-slip 3 prescribed; 0 periodic is an extension (both ends) */
     int    t_tempo;                 /* 0 Euler, 1 RK2, 2 RK3, 3 AB2 (0_modules.f90:24)         */
     int    der;                     /* advection scheme: 1 upwind, 2 centred, 3 2nd-order upwind (0_modules.f90:26) */
-    int    adv_type;                /* advective form: 1 classic (0_modules.f90:27)            */
+    int    adv_type;                /* advective form: 1 classico, 2 rotacional, 3 antissim (2, 3 with der = 1) (0_modules.f90:27) */
     int    m_turb;                  /* 0 none, 1 Smagorinsky, 2 directional Smagorinsky (0_modules.f90:31) */
     int    obst_t;                  /* obstacles: only 0 is supported (0_modules.f90:29)       */
     int    t_hs;                    /* Heaviside type: only 0 (0_modules.f90:199)              */
