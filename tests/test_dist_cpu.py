@@ -14,7 +14,7 @@ import sys
 ROOT = pathlib.Path(__file__).resolve().parent.parent
 
 WORKER = """
-import importlib.util, json, sys
+import importlib.util, json, pathlib, sys
 spec = importlib.util.spec_from_file_location("bench_mod", sys.argv[1])
 bench = importlib.util.module_from_spec(spec)
 spec.loader.exec_module(bench)
@@ -22,7 +22,8 @@ d = bench.Dist("gloo")
 d.barrier()
 m = d.max(0.5 + d.rank)
 d.barrier()
-print(json.dumps({"rank": d.rank, "world": d.world, "max": m}), flush=True)
+out = pathlib.Path(sys.argv[2]) / f"rank{d.rank}.json"
+out.write_text(json.dumps({"rank": d.rank, "world": d.world, "max": m}))
 d.close()
 """
 
@@ -46,9 +47,10 @@ def test_barrier_and_max_over_ranks(tmp_path):
     """Every rank gets the slowest rank's time (the benchmark's max over ranks)."""
     w = tmp_path / "worker.py"
     w.write_text(WORKER)
-    r, lines = torchrun(str(w), str(ROOT / "bench.py"))
+    r, _ = torchrun(str(w), str(ROOT / "bench.py"), str(tmp_path))
     assert r.returncode == 0, r.stderr[-2000:]
-    assert sorted(l["rank"] for l in lines) == [0, 1]
+    lines = [json.loads((tmp_path / f"rank{n}.json").read_text()) for n in (0, 1)]
+    assert [l["rank"] for l in lines] == [0, 1]
     assert all(l["world"] == 2 and l["max"] == 1.5 for l in lines), lines
 
 
