@@ -64,7 +64,7 @@ typedef struct suli_params {
     int    der;                     /* advection scheme: 1 upwind, 2 centred, 3 2nd-order upwind (0_modules.f90:26) */
     int    adv_type;                /* advective form: 1 classico, 2 rotacional, 3 antissim (2, 3 with der = 1) (0_modules.f90:27) */
     int    m_turb;                  /* 0 none, 1 Smagorinsky, 2 directional Smagorinsky (0_modules.f90:31) */
-    int    obst_t;                  /* obstacles: only 0 is supported (0_modules.f90:29)       */
+    int    obst_t;                  /* 0 none; 1..10 the obstaculo presets, masks set by suli_set_obstacle (0_modules.f90:29) */
     int    t_hs;                    /* Heaviside type: only 0 (0_modules.f90:199)              */
     double csmag;                   /* Smagorinsky constant (0_modules.f90:181)                */
     double gx, gz;                  /* gravity components, gz acts downward (0_modules.f90:143) */
@@ -161,6 +161,15 @@ int suli_get_scalar(suli_ctx* c, int scalar, double* v);
 int suli_iniciais(suli_ctx* c, double u_init);
 /* heaviside(); vol_ini = sum(hs) dV; mod_ls1() (14_level_set.f90:205-217). */
 int suli_level_set_ini(suli_ctx* c);
+/* The bottom-obstacle masks that obstaculo() computes (3_contorno.f90:494-762; module obst,
+   0_modules.f90:76-79): for each column, the k up to which the velocities are zeroed.
+   Host arrays in Fortran order: ku(0:nx+2, 0:ny+1), kv(0:nx+1, 0:ny+2), kw(0:nx+1, 0:ny+1);
+   ku and kv within [-1, nz], kw within [-1, nz+1] (else SULI_ERR_ARG, as obstaculo clamps
+   them).  Needs obst_t != 0.  Set them before suli_iniciais, which zeroes the inflow planes
+   below ku (2_iniciais.f90:60-65); contorno(1), contorno(2) then zero the columns and capture
+   the wall-friction velocities above them, contorno(3) extends the level set into the
+   obstacle (3_contorno.f90:266-294, 445-487). */
+int suli_set_obstacle(suli_ctx* c, const int* ku, const int* kv, const int* kw);
 
 /* Hot-path subroutines. */
 int suli_level_set(suli_ctx* c, double* vol_ins);          /* 14_level_set.f90:221-285 */

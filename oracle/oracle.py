@@ -78,6 +78,7 @@ def load(openmp: bool = False) -> C.CDLL:
         "orc_step": (i, [vp, i, P(abi.SuliStepStats)]),
         "orc_last_reinit_iters": (i, [vp]),
         "orc_num_threads": (i, []),
+        "orc_set_obstacle": (i, [vp, P(i), P(i), P(i)]),
         "orc_field_extent": (i, [P(abi.SuliParams), i, P(i), P(i)]),
     }
     for name, (res, args) in sig.items():
@@ -144,6 +145,17 @@ class Oracle:
 
     def synchronize(self):
         pass
+
+    def set_obstacle(self, ku, kv, kw):
+        """Obstacle masks (integer arrays in Fortran layout, see suli_set_obstacle)."""
+        m = [np.asfortranarray(a, dtype=np.int32) for a in (ku, kv, kw)]
+        for a, s in zip(m, self._abi.mask_shapes(self.params)):
+            if a.shape != s:
+                raise ValueError(f"mask shape {a.shape} != {s}")
+        rc = self.lib.orc_set_obstacle(self._h, *[a.ctypes.data_as(C.POINTER(C.c_int)) for a in m])
+        if rc != 0:
+            raise ValueError("oracle: mask values out of range")
+        self.obstacle = tuple(a.copy() for a in m)
 
     def iniciais(self, u_init=0.0):
         self.lib.orc_iniciais(self._h, float(u_init))

@@ -79,6 +79,15 @@ struct Oracle {
     Arr bxx0, bxx1, bxy0, bxz0, bxxf, bxxf1, bxyf, bxzf;
     Arr byx0, byy0, byy1, byz0, byxf, byyf, byyf1, byzf;
     Arr bzx0, bzy0, bzz0, bzz1, bzxf, bzyf, bzzf, bzzf1;
+    /* obstacle masks (0_modules.f90:76-79): ku(0:nx1+1,0:ny+1), kv(0:nx+1,0:ny1+1),
+       kw(0:nx+1,0:ny+1), the k up to which a column's velocity is zeroed */
+    std::vector<int> ku, kv, kw;
+    bool has_obstacle = false;
+    int KU(int i, int j) const { return ku[(size_t)i + (size_t)(nx + 3) * j]; }
+    int KV(int i, int j) const { return kv[(size_t)i + (size_t)(nx + 2) * j]; }
+    int KW(int i, int j) const { return kw[(size_t)i + (size_t)(nx + 2) * j]; }
+    void contorno_obstacle();
+    void level_set_obstacle();
     /* statistics of the last calls */
     int last_cg_iters = 0;
     double last_cg_resid = 0.0;
@@ -1117,6 +1126,58 @@ void Oracle::tempo(int tt, int it) {
 /* contorno — 3_contorno.f90:10-492 (obst_t = 0, mms_t = 0).  prd_corr (:872-950) returns
  * zeros, so the "+ dpdx" terms vanish.  ccz0 = cczf = 0 (periodic z) is an extension that
  * mirrors the reference's periodic-x rows. */
+/* Obstacle columns of contorno(1/2) (3_contorno.f90:266-294): velocities zeroed from k = 0 up
+ * to the column's mask, and the first value above it captured for the wall friction. */
+void Oracle::contorno_obstacle() {
+    if (!has_obstacle) { std::fprintf(stderr, "oracle: obst_t != 0 without masks\n"); std::abort(); }
+    for (int j = 0; j <= ny + 1; ++j)
+        for (int i = 0; i <= nx + 1; ++i) {
+            for (int k = 0; k <= KU(i, j); ++k) u(i, j, k) = 0.;
+            for (int k = 0; k <= KV(i, j); ++k) v(i, j, k) = 0.;
+            for (int k = 0; k <= KW(i, j); ++k) w(i, j, k) = 0.;
+            ub(i, j, KU(i, j) + 1) = u(i, j, KU(i, j) + 1);
+            vb(i, j, KV(i, j) + 1) = v(i, j, KV(i, j) + 1);
+            wb(i, j, KW(i, j) + 1) = w(i, j, KW(i, j) + 1);
+        }
+    for (int j = 0; j <= ny + 1; ++j)
+        for (int k = 0; k <= KU(nx1 + 1, j); ++k) u(nx1 + 1, j, k) = 0.;
+    for (int i = 0; i <= nx + 1; ++i)
+        for (int k = 0; k <= KV(i, ny1 + 1); ++k) v(i, ny1 + 1, k) = 0.;
+}
+
+/* contorno(3) (3_contorno.f90:445-481): the level set inside the obstacle (k < kw) taken
+ * from the neighbouring fluid cells at the same height, or from the cell above at the
+ * obstacle's top.  A neighbour outside 1..nx, 1..ny is never read: the reference reads ls
+ * outside its bounds there, and here that neighbour's "fluid" test is false.  A cell whose
+ * fluid neighbours are read is itself never rewritten (its own mask is below k), so the
+ * loop order does not matter. */
+void Oracle::level_set_obstacle() {
+    for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i)
+            for (int k = 1; k <= KW(i, j) - 1; ++k) {
+                auto fluid = [&](int ii, int jj) { return ii >= 1 && ii <= nx && jj >= 1 && jj <= ny && KW(ii, jj) < k; };
+                auto solid = [&](int ii, int jj) { return KW(ii, jj) >= k; };
+                if (fluid(i - 1, j) && fluid(i, j - 1))
+                    ls(i, j, k) = (ls(i - 1, j, k) + ls(i, j - 1, k)) * 0.5;
+                else if (fluid(i + 1, j) && fluid(i, j - 1))
+                    ls(i, j, k) = (ls(i + 1, j, k) + ls(i, j - 1, k)) * 0.5;
+                else if (fluid(i + 1, j) && fluid(i, j + 1))
+                    ls(i, j, k) = (ls(i + 1, j, k) + ls(i, j + 1, k)) * 0.5;
+                else if (fluid(i - 1, j) && fluid(i, j + 1))
+                    ls(i, j, k) = (ls(i - 1, j, k) + ls(i, j + 1, k)) * 0.5;
+                else if (fluid(i - 1, j) && solid(i, j - 1) && solid(i, j + 1))
+                    ls(i, j, k) = ls(i - 1, j, k);
+                else if (fluid(i, j - 1) && solid(i - 1, j) && solid(i + 1, j))
+                    ls(i, j, k) = ls(i, j - 1, k);
+                else if (fluid(i + 1, j) && solid(i, j - 1) && solid(i, j + 1))
+                    ls(i, j, k) = ls(i + 1, j, k);
+                else if (fluid(i, j + 1) && solid(i - 1, j) && solid(i + 1, j))
+                    ls(i, j, k) = ls(i, j + 1, k);
+                else if (k == KW(i, j) - 1 && k < nz)
+                    ls(i, j, k) = ls(i, j, k + 1);
+            }
+}
+
 void Oracle::contorno(int nlock) {
     const int X0 = P.ccx0, XF = P.ccxf, Y0 = P.ccy0, YF = P.ccyf, Z0 = P.ccz0, ZF = P.cczf;
     const int I1 = nx1 + 1, J1 = ny1 + 1, K1 = nz1 + 1;   /* u/v/w outer ghost index */
@@ -1187,22 +1248,30 @@ void Oracle::contorno(int nlock) {
         if (ZF == 1) { Z_all(u, [&](int i, int j) { u(i, j, nz + 1) = u(i, j, nz); }); Z_all(v, [&](int i, int j) { v(i, j, nz + 1) = v(i, j, nz); }); Z_all(w, [&](int i, int j) { w(i, j, K1) = -w(i, j, nz1 - 1); }); }
         if (ZF == 2) { Z_all(u, [&](int i, int j) { u(i, j, nz + 1) = -u(i, j, nz); }); Z_all(v, [&](int i, int j) { v(i, j, nz + 1) = -v(i, j, nz); }); Z_all(w, [&](int i, int j) { w(i, j, K1) = w(i, j, nz1 - 1); }); }
         if (ZF == 3) { Z_all(u, [&](int i, int j) { u(i, j, nz + 1) = bzxf(i, j, 0); }); Z_all(v, [&](int i, int j) { v(i, j, nz + 1) = bzyf(i, j, 0); }); Z_all(w, [&](int i, int j) { w(i, j, K1) = bzzf1(i, j, 0); }); }
-        /* wall-friction capture (:247-264) */
-        if (Z0 == 2) {
-            Z_all(u, [&](int i, int j) { ub(i, j, 2) = u(i, j, 2); });
-            Z_all(v, [&](int i, int j) { vb(i, j, 2) = v(i, j, 2); });
-            Z_all(w, [&](int i, int j) { wb(i, j, 2) = w(i, j, 2); });
+        /* wall-friction capture (:247-264), or the obstacle columns (:266-294) */
+        if (P.obst_t != 0) {
+            contorno_obstacle();
+        } else {
+            if (Z0 == 2) {
+                Z_all(u, [&](int i, int j) { ub(i, j, 2) = u(i, j, 2); });
+                Z_all(v, [&](int i, int j) { vb(i, j, 2) = v(i, j, 2); });
+                Z_all(w, [&](int i, int j) { wb(i, j, 2) = w(i, j, 2); });
+            }
+            if (Y0 == 2) {
+                Y_all(u, [&](int i, int k) { ub(i, 2, k) = u(i, 2, k); });
+                Y_all(v, [&](int i, int k) { vb(i, 2, k) = v(i, 2, k); });
+                Y_all(w, [&](int i, int k) { wb(i, 2, k) = w(i, 2, k); });
+            }
+            if (YF == 2) {
+                Y_all(u, [&](int i, int k) { ub(i, ny1 - 1, k) = u(i, ny1 - 1, k); });
+                Y_all(v, [&](int i, int k) { vb(i, ny1 - 1, k) = v(i, ny1 - 1, k); });
+                Y_all(w, [&](int i, int k) { wb(i, ny1 - 1, k) = w(i, ny1 - 1, k); });
+            }
         }
-        if (Y0 == 2) {
-            Y_all(u, [&](int i, int k) { ub(i, 2, k) = u(i, 2, k); });
-            Y_all(v, [&](int i, int k) { vb(i, 2, k) = v(i, 2, k); });
-            Y_all(w, [&](int i, int k) { wb(i, 2, k) = w(i, 2, k); });
-        }
-        if (YF == 2) {
-            Y_all(u, [&](int i, int k) { ub(i, ny1 - 1, k) = u(i, ny1 - 1, k); });
-            Y_all(v, [&](int i, int k) { vb(i, ny1 - 1, k) = v(i, ny1 - 1, k); });
-            Y_all(w, [&](int i, int k) { wb(i, ny1 - 1, k) = w(i, ny1 - 1, k); });
-        }
+    }
+    if (nlock == 3 && P.obst_t != 0) {                  /* :445-487 */
+        level_set_obstacle();
+        heaviside();
     }
     if (nlock == 2) {
         /* boundary-normal velocities (:297-441) */
@@ -1473,6 +1542,16 @@ int orc_iniciais(void* h, double u_init) {
     std::fill(o->wb.a.begin(), o->wb.a.end(), 0.);
     std::fill(o->bxx0.a.begin(), o->bxx0.a.end(), u_init);
     std::fill(o->bxx1.a.begin(), o->bxx1.a.end(), u_init);
+    if (o->P.obst_t != 0) {
+        /* 2_iniciais.f90:60-65: bxx1(:,0:ku(1,j)) = 0 for every j, i.e. whole rows of the
+           plane up to each column's mask (the reference's index order, kept) */
+        if (!o->has_obstacle) { std::fprintf(stderr, "oracle: obst_t != 0 without masks\n"); std::abort(); }
+        for (int j = 0; j <= o->ny + 1; ++j)
+            for (int jj = 0; jj <= o->ny + 1; ++jj) {
+                for (int k = 0; k <= o->KU(1, j); ++k) o->bxx1(jj, k, 0) = 0.;
+                for (int k = 0; k <= o->KU(0, j); ++k) o->bxx0(jj, k, 0) = 0.;
+            }
+    }
     const int tm = o->P.t_tempo;
     const double dt = o->P.dt;
     o->dt = dt;
@@ -1558,6 +1637,21 @@ int orc_step(void* h, int it, suli_step_stats* st) {
     return status;
 }
 int orc_last_reinit_iters(void* h) { return static_cast<Oracle*>(h)->last_reinit_iters; }
+/* the masks of obstaculo (3_contorno.f90:741-760), Fortran order, checked like
+   suli_set_obstacle: ku, kv in [-1, nz], kw in [-1, nz+1] */
+int orc_set_obstacle(void* h, const int* ku, const int* kv, const int* kw) {
+    Oracle* o = static_cast<Oracle*>(h);
+    const int nx = o->nx, ny = o->ny, nz = o->nz;
+    const size_t nu = (size_t)(nx + 3) * (ny + 2), nv = (size_t)(nx + 2) * (ny + 3), nw = (size_t)(nx + 2) * (ny + 2);
+    for (size_t q = 0; q < nu; ++q) if (ku[q] < -1 || ku[q] > nz) return SULI_ERR_ARG;
+    for (size_t q = 0; q < nv; ++q) if (kv[q] < -1 || kv[q] > nz) return SULI_ERR_ARG;
+    for (size_t q = 0; q < nw; ++q) if (kw[q] < -1 || kw[q] > nz + 1) return SULI_ERR_ARG;
+    o->ku.assign(ku, ku + nu);
+    o->kv.assign(kv, kv + nv);
+    o->kw.assign(kw, kw + nw);
+    o->has_obstacle = true;
+    return 0;
+}
 int orc_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

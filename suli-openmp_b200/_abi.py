@@ -136,6 +136,12 @@ def field_extent(p: SuliParams, name: str):
     raise KeyError(name)
 
 
+def mask_shapes(p: SuliParams):
+    """numpy shapes of the obstacle masks ku(0:nx+2, 0:ny+1), kv(0:nx+1, 0:ny+2),
+    kw(0:nx+1, 0:ny+1) (0_modules.f90:76-79)."""
+    return (p.nx + 3, p.ny + 2), (p.nx + 2, p.ny + 3), (p.nx + 2, p.ny + 2)
+
+
 def field_shape(p: SuliParams, name: str):
     """numpy shape (Fortran order: pass order='F') of a module array."""
     return tuple(h - l + 1 for l, h in field_extent(p, name))
@@ -212,6 +218,7 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
         "suli_posdin": (C.c_int, [vp]),
         "suli_est": (C.c_int, [vp, P(C.c_double)]),
         "suli_set_dt": (C.c_int, [vp, C.c_double]),
+        "suli_set_obstacle": (C.c_int, [vp, P(C.c_int), P(C.c_int), P(C.c_int)]),
         "suli_step": (C.c_int, [vp, C.c_int, P(SuliStepStats)]),
         "suli_stream": (C.c_int, [vp, P(vp)]),
         "suli_profile_enable": (C.c_int, [vp, C.c_int]),
@@ -249,7 +256,7 @@ HEADER_SYMBOLS = [
     "suli_set_scalar", "suli_get_scalar", "suli_iniciais", "suli_level_set_ini",
     "suli_level_set", "suli_heaviside", "suli_mod_ls1", "suli_visco", "suli_convdiff",
     "suli_tempo", "suli_contorno", "suli_graddin", "suli_posdin", "suli_est",
-    "suli_set_dt", "suli_step", "suli_stream", "suli_profile_enable", "suli_profile_read",
+    "suli_set_dt", "suli_set_obstacle", "suli_step", "suli_stream", "suli_profile_enable", "suli_profile_read",
     "suli_est_static",
     "suli_nn_num_params", "suli_nn_create", "suli_nn_destroy", "suli_nn_last_error",
     "suli_nn_set_params", "suli_nn_get_params", "suli_nn_forward", "suli_nn_loss_grad",

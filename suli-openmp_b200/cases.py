@@ -35,8 +35,10 @@ def _two_phase(p: SuliParams, *, cs=0.1, cfl_dt=None):
     return p
 
 
-def standard_init(model, ls0: np.ndarray, u_init: float = 0.0):
-    """iniciais + level-set preset + level_set_ini + contorno(1), contorno(3)."""
+def standard_init(model, ls0: np.ndarray, u_init: float = 0.0, masks=None):
+    """[obstacle masks +] iniciais + level-set preset + level_set_ini + contorno(1), contorno(3)."""
+    if masks is not None:
+        model.set_obstacle(*masks)
     model.iniciais(u_init)
     model.upload("ls", ls0)
     model.level_set_ini()
@@ -119,6 +121,152 @@ def reference_default(nx=None, ny=None, nz=None):
         standard_init(model, ls0, u_init=0.31)
 
     return p, init
+
+
+def _nint(v: np.ndarray) -> np.ndarray:
+    """Fortran NINT: nearest integer, halves away from zero."""
+    a = np.abs(v)
+    r = np.floor(a)
+    r = r + (a - r >= 0.5)
+    return (np.sign(v) * r).astype(np.int64)
+
+
+def obstacle_masks(p: SuliParams, height) -> tuple:
+    """ku, kv, kw from a bottom height on the half-cell grid (3_contorno.f90:741-760).
+
+    `height(i, j)` takes integer arrays of half-cell indices i = -1 .. 2(nx+1)+2,
+    j = -1 .. 2(ny+1)+2 and returns the height there; then
+    ku(i,j) = nint(h(2i-1, 2j)/dz + 0.5) and kv(i,j) = nint(h(2i, 2j-1)/dz + 0.5), at most nz,
+    kw(i,j) = floor(h(2i, 2j)/dz + 1), at most nz+1; Fortran order, shapes _abi.mask_shapes."""
+    nx, ny, nz, dz = p.nx, p.ny, p.nz, p.dz
+    I = np.arange(-1, 2 * (nx + 1) + 3)
+    J = np.arange(-1, 2 * (ny + 1) + 3)
+    aux = np.asarray(height(I[:, None], J[None, :]), dtype=np.float64) * np.ones((I.size, J.size))
+    A = lambda i, j: aux[i + 1, j + 1]                         # auxx(i, j), i, j from -1
+    iu, ju = np.meshgrid(np.arange(0, nx + 3), np.arange(0, ny + 2), indexing="ij")
+    ku = np.minimum(_nint(A(iu * 2 - 1, ju * 2) / dz + 0.5), nz)
+    iv, jv = np.meshgrid(np.arange(0, nx + 2), np.arange(0, ny + 3), indexing="ij")
+    kv = np.minimum(_nint(A(iv * 2, jv * 2 - 1) / dz + 0.5), nz)
+    iw, jw = np.meshgrid(np.arange(0, nx + 2), np.arange(0, ny + 2), indexing="ij")
+    kw = np.minimum(np.floor(A(iw * 2, jw * 2) / dz + 1.).astype(np.int64), nz + 1)
+    return tuple(np.asfortranarray(m, dtype=np.int32) for m in (ku, kv, kw))
+
+
+def obstaculo(p: SuliParams, obst_t: int) -> tuple:
+    """The masks of the reference's bottom presets 1..10 (obstaculo, 3_contorno.f90:494-740).
+
+    Heights at x = (i-1) dx/2, y = (j-1) dy/2 on the half-cell grid (preset 5: x = (i-2) dx/2).
+    Presets 2, 8 and 9 read values the reference leaves unset: preset 2's running offsets
+    before the first segment that sets them are 0 here, and presets 8 and 9 are -dz (no
+    obstacle) outside the wall, as preset 10 sets explicitly."""
+    dx, dy, dz, ny, nz = p.dx, p.dy, p.dz, p.ny, p.nz
+    pi = math.pi
+
+    def xs(i, shift=1.0):
+        return (i - shift) * (dx * 0.5)
+
+    def ys(j):
+        return (j - 1.) * (dy * 0.5)
+
+    if obst_t == 1:      # dunes (:524-533): elev is an integer parameter, int(50 dz) (0_modules.f90:80)
+        elev, amp, comp, fase = int(50. * dz), 0.50, .5, -pi / 2.
+        return obstacle_masks(p, lambda i, j: elev + amp * (1. + np.sin(fase + 2. * pi * xs(i) / comp)) + 0. * j)
+    if obst_t == 2:      # Yue et al. (2003) dune (:534-568), evaluated in the reference's loop order
+        def h2(i, j):
+            out = np.empty((i.size, j.size))
+            aux1 = aux2 = 0.0
+            for jj in range(j.size):
+                for ii in range(i.size):
+                    x = xs(float(i[ii, 0]))
+                    if x <= 0.01:
+                        v = 0.02
+                    elif x <= 0.05:
+                        v = -math.tan(26. * pi / 180.) * x + 0.02
+                    elif x <= 0.075:
+                        v = 0.0005
+                    elif x <= 0.1375:
+                        v = math.tan(1.8 * pi / 180.) * x + 0.0005
+                        aux1 = v
+                    elif x <= 0.325:
+                        v = math.tan(5. * pi / 180.) * x + aux1
+                        aux2 = v
+                    elif x <= 0.39:
+                        v = math.tan(1.8 * pi / 180.) * x + aux2
+                    else:
+                        v = 0.02
+                    out[ii, jj] = v
+            return out
+        return obstacle_masks(p, h2)
+    if obst_t == 3:      # 3-D Gaussian bump (:570-591)
+        d, x0, y0, a, sigx, sigy = 0.2, 3., ny / 2. * dy, 2.0, 0.5, 0.5
+        def h3(i, j):
+            aux1 = (ys(j) - y0) * (ys(j) - y0) / (2. * sigy * sigy)
+            aux2 = (xs(i) - x0) * (xs(i) - x0) / (2. * sigx * sigx)
+            return np.exp(-aux2 - aux1) * a + d
+        return obstacle_masks(p, h3)
+    if obst_t == 4:      # Beji and Battjes (1994) bar (:593-618)
+        def h4(i, j):
+            x = xs(i) + 0. * j
+            return np.select([x < 6., x < 12., x < 14., x < 17.],
+                             [0. * x, math.tan(1. / 20.) * (x - 6.), 0.30 + 0. * x, -math.tan(1. / 10.) * (x - 14.) + 0.30],
+                             0. * x)
+        return obstacle_masks(p, h4)
+    if obst_t == 5:      # Delft 1980 channel 0 (:620-633)
+        return obstacle_masks(p, lambda i, j: np.where(xs(i, 2.0) + 0. * j <= 1.0, 0.2, 0.))
+    if obst_t == 6:      # Delft 1980 channel 1_2 (:635-659)
+        def h6(i, j):
+            x = xs(i) + 0. * j
+            return np.select([x < 1., x < 1.4, x < 2.4, x < 2.8],
+                             [0.2 + 0. * x, -1. / 2. * (x - 1.) + 0.2, 0. * x, 1. / 2. * (x - 2.4)], 0.2 + 0. * x)
+        return obstacle_masks(p, h6)
+    if obst_t == 7:      # holes and bumps (:661-681)
+        raio = 0.12
+        def h7(i, j):
+            x = xs(i) + 0. * j
+            inner = np.sqrt(np.maximum(-(x - 1.) ** 2. + raio ** 2., 0.))
+            return np.select([x < (1. - raio), x < 1.], [0. * x, inner], raio + 0. * x)
+        return obstacle_masks(p, h7)
+    if obst_t in (8, 9, 10):   # walls with an opening (:683-740)
+        lo, hi, wall, ylo, yhi = {8: (90., 100., (nz + 1) * dz, 95., 170.),
+                                  9: (0.8, 0.825, (nz + 1) * dz, 0.45, 0.75),
+                                  10: (0.75 - 0.16 * 0.5, 0.75 + 0.16 * 0.5, 0.16, 0.5 - 0.4 * 0.5, 0.5 + 0.4 * 0.5)}[obst_t]
+        def h8(i, j):
+            x, y = xs(i) + 0. * j, ys(j) + 0. * i
+            h = np.full(x.shape, -dz)
+            h = np.where((x >= lo) & (x <= hi), wall, h)
+            return np.where((y > ylo) & (y < yhi), -dz, h)
+        return obstacle_masks(p, h8)
+    raise ValueError(f"obst_t {obst_t}: the reference defines presets 1..10")
+
+
+def bump_channel(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-10, u_init=0.1):
+    """A small two-phase channel over a Gaussian bottom bump (the obst_t = 3 shape scaled to the
+    box): water 0.6 of the depth, inflow u_init at x = 0 (ccx0 = 3), outflow at x = xf
+    (ccxf = 4), periodic y, free-slip top."""
+    p = default_params()
+    p.nx, p.ny, p.nz = nx, ny, nz
+    p.dx = p.dy = p.dz = dx
+    p.ccx0, p.ccxf = 3, 4
+    p.ccy0 = p.ccyf = 0
+    p.ccz0, p.cczf = 2, 1
+    _two_phase(p, cs=0.1)
+    p.cg_tol = cg_tol
+    p.obst_t = 3
+    p.dt = 0.2 * dx / (u_init + math.sqrt(9.81 * 0.6 * nz * dx))
+    Lx, Ly, H = nx * dx, ny * dx, nz * dx
+
+    def height(i, j):
+        x, y = (i - 1.) * (dx * 0.5), (j - 1.) * (dx * 0.5)
+        return 0.25 * H * np.exp(-((x - 0.5 * Lx) ** 2 + (y - 0.5 * Ly) ** 2) / (2. * (0.15 * Lx) ** 2)) + 0.1 * H
+
+    masks = obstacle_masks(p, height)
+    X, Y, Z = _centres(p)
+    ls0 = 0.6 * H - Z
+
+    def init(model):
+        standard_init(model, ls0, u_init, masks=masks)
+
+    return p, init, masks
 
 
 def random_state(p: SuliParams, seed: int = 0, *, vel=0.2, wave=0.03):

@@ -113,6 +113,11 @@ struct suli_ctx {
     int ntt = 1;
     double a_dt[3] = {0, 0, 0};
     bool tf_active = false;             // tf_u/v/w uploaded non-zero
+    // obstacle masks (suli_set_obstacle): ku (nx+3)x(ny+2), kv (nx+2)x(ny+3), kw (nx+2)x(ny+2),
+    // Fortran order, one device allocation; host copies for suli_iniciais
+    int* obst_k = nullptr;
+    const int *obst_ku = nullptr, *obst_kv = nullptr, *obst_kw = nullptr;   // into obst_k
+    std::vector<int> obst_ku_host;
     int last_reinit_iters = 0;
     int last_volfix_iters = 0;
     // mixed-precision solve (precision = 1)

@@ -12,6 +12,7 @@
 #include <cmath>
 #include "advect.cuh"
 #include "ctx.cuh"
+#include "obstacle.cuh"
 #include "pdl.cuh"
 #include "reduce.cuh"
 #include "weno.cuh"
@@ -362,6 +363,7 @@ struct CDConst {
     double idx, idy, idz, gx, gz, sigma, cz;   // reciprocal cell sizes; cz = gz/(chezy*chezy)
     int tf;                                  // tf_u/v/w are non-zero
     int cap_z2, cap_y2, cap_yn;              // planes where ub/vb/wb are captured (3_contorno.f90:247-264)
+    int obst;                                // obstacles: captured above each column, friction read everywhere
 };
 struct CDFields {
     const double *u, *v, *w, *rho, *hsx, *hsy, *hsz, *kurv, *nut, *xnut, *ynut, *znut, *ub, *vb, *wb;
@@ -369,8 +371,10 @@ struct CDFields {
     double *Fu, *Fv, *Fw;
 };
 
+// the reference subtracts (gz/C^2)|ub| u at every face (6_convdiff.f90:156,168,183); ub is zero
+// except where contorno captured it, so only those faces are read
 __device__ __forceinline__ bool on_cap(const CDConst& C, int j, int k, int ny) {
-    return (C.cap_z2 && k == 2) || (C.cap_y2 && j == 2) || (C.cap_yn && j == ny);
+    return C.obst || (C.cap_z2 && k == 2) || (C.cap_y2 && j == 2) || (C.cap_yn && j == ny);
 }
 
 // classico der = 2 (centred, 7_advectivo.f90:115-170) and der = 3 (second-order upwind,
@@ -618,6 +622,7 @@ struct BCArgs {
     double *u, *v, *w, *ub, *vb, *wb, *prd1;
     Planes pl;
     int nlock;
+    int obst;   // obstacle columns replace the wall-friction capture of the walls
 };
 // pressure ghosts: composition of the x, y, z copies (:37-54) = value at the mapped index
 __global__ void k_prd_ghosts(Geo G, BC bc, double* prd1) {
@@ -759,7 +764,7 @@ __global__ void k_bc_z(Geo G, BC bc, BCArgs A) {
         if (bc.zf == 3) FIDX(w, i, j, nz1 + 1) = A.pl.bzzf1[i + lv * j];
     }
     // capture of the k = 2 plane: each thread copies within its own (i,j) column, after its z writes
-    if (bc.z0 == 2) {
+    if (bc.z0 == 2 && !A.obst) {
         if (i <= nx + 2 && j <= ny + 1) FIDX(A.ub, i, j, 2) = FIDX(A.u, i, j, 2);
         if (i <= nx + 1 && j <= ny + 2) FIDX(A.vb, i, j, 2) = FIDX(A.v, i, j, 2);
         if (i <= nx + 1 && j <= ny + 1) FIDX(A.wb, i, j, 2) = FIDX(A.w, i, j, 2);
@@ -777,6 +782,24 @@ __global__ void k_bc_capture_y(Geo G, BC bc, BCArgs A) {
         if (i <= nx + 2 && k <= nz + 1) FIDX(A.ub, i, j, k) = FIDX(A.u, i, j, k);
         if (i <= nx + 1 && k <= nz + 1) FIDX(A.vb, i, j, k) = FIDX(A.v, i, j, k);
         if (i <= nx + 1 && k <= nz + 2) FIDX(A.wb, i, j, k) = FIDX(A.w, i, j, k);
+    }
+}
+
+// obstacle columns (:266-294) in place of the capture, thread per (i, j), 0..nx+2 x 0..ny+2
+__global__ void k_bc_obst(Geo G, ObstMasks M, BCArgs A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > G.nx + 2 || j > G.ny + 2) return;
+    obst_columns(G, M, A.u, A.v, A.w, A.ub, A.vb, A.wb, i, j);
+}
+
+// contorno(3): level set inside the obstacle (:445-481), thread per column (i, j)
+__global__ void k_ls_obst(Geo G, const int* __restrict__ kw, double* ls) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i > G.nx || j > G.ny) return;
+    const int top = kw[i + (G.nx + 2) * j] - 1;
+    for (int k = 1; k <= top; ++k) {
+        double val;
+        if (obst_ls_value(G, kw, ls, i, j, k, &val)) ls[G.idx32(i, j, k)] = val;
     }
 }
 
@@ -1310,6 +1333,7 @@ void launch_convdiff(suli_ctx* c) {
     C.cz = c->P.gz / (c->P.chezy * c->P.chezy);
     C.tf = c->tf_active ? 1 : 0;
     C.cap_z2 = (c->P.ccz0 == 2); C.cap_y2 = (c->P.ccy0 == 2); C.cap_yn = (c->P.ccyf == 2);
+    C.obst = (c->P.obst_t != 0);
     CDFields F;
     F.u = c->f[SULI_F_U]; F.v = c->f[SULI_F_V]; F.w = c->f[SULI_F_W]; F.rho = c->f[SULI_F_RHO];
     F.hsx = c->f[SULI_F_HSX]; F.hsy = c->f[SULI_F_HSY]; F.hsz = c->f[SULI_F_HSZ]; F.kurv = c->f[SULI_F_KURV];
@@ -1338,21 +1362,36 @@ void launch_tempo(suli_ctx* c, int tt, int it) {
 }
 void launch_contorno(suli_ctx* c, int nlock) {
     const Geo& G = c->g;
-    if (nlock != 1 && nlock != 2) return;   // nlock 3 acts only with obstacles
+    const bool obst = (c->P.obst_t != 0);
+    const dim3 b2(32, 8);
+    if (nlock == 3) {   // acts only with obstacles (3_contorno.f90:445-487)
+        if (!obst) return;
+        {
+            ProfScope ps(c, SULI_K_CONTORNO, 1);
+            k_ls_obst<<<grid3(G.nx, G.ny, 1, b2), b2, 0, c->stream>>>(G, c->obst_kw, c->f[SULI_F_LS]);
+        }
+        launch_lsprops(c, c->f[SULI_F_LS], false, true, false);   // heaviside()
+        return;
+    }
+    if (nlock != 1 && nlock != 2) return;
     BCArgs A;
     A.u = c->f[SULI_F_U]; A.v = c->f[SULI_F_V]; A.w = c->f[SULI_F_W];
     A.ub = c->f[SULI_F_UB]; A.vb = c->f[SULI_F_VB]; A.wb = c->f[SULI_F_WB];
     A.prd1 = c->f[SULI_F_PRD1];
     A.pl = c->planes();
     A.nlock = nlock;
-    const dim3 b2(32, 8);
-    const bool capy = (c->bc.y0 == 2 || c->bc.yf == 2);
-    ProfScope ps(c, SULI_K_CONTORNO, (nlock == 2 ? 7 : 4) + (capy ? 1 : 0));
+    A.obst = obst ? 1 : 0;
+    const bool capy = !obst && (c->bc.y0 == 2 || c->bc.yf == 2);
+    ProfScope ps(c, SULI_K_CONTORNO, (nlock == 2 ? 7 : 4) + (capy || obst ? 1 : 0));
     k_prd_ghosts<<<grid3(G.nx + 2, G.ny + 2, G.nz + 2, kBlk), kBlk, 0, c->stream>>>(G, c->bc, A.prd1);
     k_bc_y<<<grid3(G.nx + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
     k_bc_x<<<grid3(G.ny + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
     k_bc_z<<<grid3(G.nx + 3, G.ny + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
     if (capy) k_bc_capture_y<<<grid3(G.nx + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
+    if (obst) {
+        const ObstMasks M{c->obst_ku, c->obst_kv, c->obst_kw};
+        k_bc_obst<<<grid3(G.nx + 3, G.ny + 3, 1, b2), b2, 0, c->stream>>>(G, M, A);
+    }
     if (nlock == 2) {
         k_bc_ny<<<grid3(G.nx + 2, G.nz + 2, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
         k_bc_nx<<<grid3(G.ny + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);

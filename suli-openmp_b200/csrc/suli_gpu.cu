@@ -112,7 +112,7 @@ int validate(const suli_params* p, std::string& why) {
     if (p->ccx0 < 0 || p->ccx0 > 4 || p->ccxf < 0 || p->ccxf > 4) { why = "ccx0/ccxf out of range"; return SULI_ERR_ARG; }
     if (p->ccy0 < 0 || p->ccy0 > 3 || p->ccyf < 0 || p->ccyf > 3) { why = "ccy0/ccyf out of range"; return SULI_ERR_ARG; }
     if (p->ccz0 < 0 || p->ccz0 > 3 || p->cczf < 0 || p->cczf > 3) { why = "ccz0/cczf out of range"; return SULI_ERR_ARG; }
-    if (p->obst_t != 0) { why = "obstacles (obst_t != 0) are not built"; return SULI_ERR_UNSUPPORTED; }
+    if (p->obst_t < 0 || p->obst_t > 10) { why = "obst_t must be 0 (none) or an obstaculo preset 1..10"; return SULI_ERR_ARG; }
     if (p->t_hs != 0) { why = "t_hs != 0 is not built"; return SULI_ERR_UNSUPPORTED; }
     if (p->adv_type < 1 || p->adv_type > 3) { why = "adv_type must be 1 (classico), 2 (rotacional) or 3 (antissim)"; return SULI_ERR_ARG; }
     if (p->der < 1 || p->der > 3) { why = "der must be 1 (upwind), 2 (centred) or 3 (2nd-order upwind)"; return SULI_ERR_ARG; }
@@ -290,6 +290,7 @@ int suli_destroy(suli_ctx* c) {
     if (c->cg_loop) cudaGraphExecDestroy(c->cg_loop);
     for (auto& e : c->prof.ev) cudaEventDestroy(e);
     cudaFree(c->arena);
+    cudaFree(c->obst_k);
     for (int f = SULI_F_BXX0; f < SULI_F_COUNT; ++f) cudaFree(c->f[f]);
     cudaFree(c->red_partial);
     cudaFree(c->red_counter);
@@ -415,6 +416,30 @@ int suli_set_dt(suli_ctx* c, double dt) {
 }
 
 // iniciais (2_iniciais.f90:36-46 and 85-104), without obstacle/wave/level-set presets
+int suli_set_obstacle(suli_ctx* c, const int* ku, const int* kv, const int* kw) {
+    if (!c || !ku || !kv || !kw) return SULI_ERR_ARG;
+    if (c->P.obst_t == 0) return fail(c, SULI_ERR_ARG, "set_obstacle: obst_t is 0");
+    const int nx = c->P.nx, ny = c->P.ny, nz = c->P.nz;
+    const size_t nu = (size_t)(nx + 3) * (ny + 2), nv = (size_t)(nx + 2) * (ny + 3), nw = (size_t)(nx + 2) * (ny + 2);
+    // the column kernels index k from -1 + 1 = 0 up to mask + 1: keep it inside the halo
+    for (size_t q = 0; q < nu; ++q) if (ku[q] < -1 || ku[q] > nz) return fail(c, SULI_ERR_ARG, "set_obstacle: ku outside [-1, nz]");
+    for (size_t q = 0; q < nv; ++q) if (kv[q] < -1 || kv[q] > nz) return fail(c, SULI_ERR_ARG, "set_obstacle: kv outside [-1, nz]");
+    for (size_t q = 0; q < nw; ++q) if (kw[q] < -1 || kw[q] > nz + 1) return fail(c, SULI_ERR_ARG, "set_obstacle: kw outside [-1, nz+1]");
+    cudaSetDevice(c->device);
+    if (!c->obst_k) {
+        CUDA_TRY(c, cudaMalloc(&c->obst_k, (nu + nv + nw) * sizeof(int)));
+        c->obst_ku = c->obst_k;
+        c->obst_kv = c->obst_k + nu;
+        c->obst_kw = c->obst_k + nu + nv;
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(c->obst_k, ku, nu * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->obst_k + nu, kv, nv * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->obst_k + nu + nv, kw, nw * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->obst_ku_host.assign(ku, ku + nu);
+    return SULI_OK;
+}
+
 int suli_iniciais(suli_ctx* c, double u_init) {
     if (!c) return SULI_ERR_ARG;
     cudaSetDevice(c->device);
@@ -428,9 +453,20 @@ int suli_iniciais(suli_ctx* c, double u_init) {
     launch_fill(c, c->f[SULI_F_VB], 0.);
     launch_fill(c, c->f[SULI_F_WB], 0.);
     CHECK_LAUNCH(c);
-    std::vector<double> bx(c->plane_elems[SULI_F_BXX0], u_init);
-    CUDA_TRY(c, cudaMemcpyAsync(c->f[SULI_F_BXX0], bx.data(), bx.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CUDA_TRY(c, cudaMemcpyAsync(c->f[SULI_F_BXX1], bx.data(), bx.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    std::vector<double> bx0(c->plane_elems[SULI_F_BXX0], u_init), bx1(bx0);
+    if (c->P.obst_t != 0) {
+        // 2_iniciais.f90:60-65: bxx1(:,0:ku(1,j)) = 0 for every j zeroes whole rows of the
+        // (0:ny+1, 0:nz+1) plane up to the highest ku(1,j) (likewise bxx0 with ku(0,j))
+        if (c->obst_ku_host.empty()) return fail(c, SULI_ERR_ARG, "iniciais: obst_t != 0 needs suli_set_obstacle first");
+        const int nx = c->P.nx, ny = c->P.ny, rows = ny + 2;
+        for (int j = 0; j <= ny + 1; ++j) {
+            const int k1 = c->obst_ku_host[1 + (size_t)(nx + 3) * j], k0 = c->obst_ku_host[0 + (size_t)(nx + 3) * j];
+            for (int k = 0; k <= k1; ++k) std::fill_n(bx1.begin() + (size_t)rows * k, rows, 0.);
+            for (int k = 0; k <= k0; ++k) std::fill_n(bx0.begin() + (size_t)rows * k, rows, 0.);
+        }
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(c->f[SULI_F_BXX0], bx0.data(), bx0.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->f[SULI_F_BXX1], bx1.data(), bx1.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     const int tm = c->P.t_tempo;
     const double dt = c->P.dt;
     c->dt = dt;
@@ -560,6 +596,7 @@ int suli_tempo(suli_ctx* c, int tt, int it) {
 int suli_contorno(suli_ctx* c, int nlock) {
     if (!c) return SULI_ERR_ARG;
     if (nlock < 1 || nlock > 3) return fail(c, SULI_ERR_ARG, "contorno: nlock must be 1..3");
+    if (c->P.obst_t != 0 && !c->obst_k) return fail(c, SULI_ERR_ARG, "contorno: obst_t != 0 needs suli_set_obstacle first");
     cudaSetDevice(c->device);
     launch_contorno(c, nlock);
     CHECK_LAUNCH(c);
@@ -853,6 +890,7 @@ int suli_step(suli_ctx* c, int it, suli_step_stats* st) {
     c->t = it * c->dt;
     int r = suli_level_set(c, nullptr);
     if (r < 0) return r;
+    if (c->P.obst_t != 0 && (r = suli_contorno(c, 3)) < 0) return r;   // 1_principal.f90:75
     for (int tt = 1; tt <= c->ntt; ++tt) {
         c->dt = c->a_dt[tt - 1];
         if ((r = suli_visco(c)) < 0) return r;

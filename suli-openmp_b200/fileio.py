@@ -17,8 +17,8 @@
 
 Every function takes any object with the solver's surface (`params`, `shape`, `download`,
 `upload`, `get_scalar`, `set_scalar`): `Solver` on the GPU or the CPU restatement used by
-the tests.  Obstacles are not built, so the masks ku, kv, kw are written as zeros and a
-restart file with non-zero masks is refused.
+the tests.  The obstacle masks ku, kv, kw are those the model was given by `set_obstacle`
+(its `obstacle` attribute; zeros without obstacles).
 """
 from __future__ import annotations
 
@@ -79,7 +79,9 @@ def write_restart(model, path, *, d_max: float = 0.0, d_min: float = 0.0, ls_m: 
     with open(path, "w") as f:
         for name in RESTART_ORDER:
             if name in MASKS:
-                np.zeros(int(np.prod(mask_shape(p, name))), np.int64).tofile(f, sep="\n", format="%d")
+                masks = getattr(model, "obstacle", None)
+                m = masks[MASKS.index(name)] if masks is not None else np.zeros(mask_shape(p, name), np.int64)
+                np.ravel(np.asarray(m, np.int64), order="F").tofile(f, sep="\n", format="%d")
             elif name in RESTART_SCALARS:
                 np.array([scal[name]]).tofile(f, sep="\n", format="%.17g")
             else:
@@ -114,26 +116,30 @@ def read_restart(model, path) -> dict:
     """restart_ini (11_diversos.f90:232-312): load a restart file into `model`.
 
     Uploads every array, sets vol_ini and vol_ins, and sets the time-step table from t_tempo
-    with t = 0, as restart_ini does.  Returns the scalars d_max, d_min, ls_m.  Refuses a file
-    whose length does not match this grid, or whose obstacle masks are not all zero."""
+    with t = 0, as restart_ini does.  Non-zero obstacle masks are passed to
+    `model.set_obstacle` (the model's obst_t must be non-zero).  Returns the scalars d_max,
+    d_min, ls_m.  Refuses a file whose length does not match this grid."""
     p = model.params
     vals = _parse_list_directed(pathlib.Path(path).read_bytes())
     want = restart_count(p)
     if vals.size != want:
         raise ValueError(f"restart file holds {vals.size} values, a {p.nx}x{p.ny}x{p.nz} grid needs {want}")
-    pos, scal = 0, {}
+    pos, scal, masks = 0, {}, {}
     for name in RESTART_ORDER:
         shape = restart_shape(p, name)
         n = int(np.prod(shape))
         chunk = vals[pos:pos + n]
         pos += n
         if name in MASKS:
-            if np.any(chunk != 0):
-                raise ValueError(f"restart file has obstacles ({name} != 0); obstacles are not built")
+            masks[name] = chunk.reshape(shape, order="F").astype(np.int32)
         elif name in RESTART_SCALARS:
             scal[name] = float(chunk[0])
         else:
             model.upload(name, chunk.reshape(field_shape(p, name), order="F"))
+    if any(m.any() for m in masks.values()):
+        if p.obst_t == 0:
+            raise ValueError("restart file has obstacle masks; the model has obst_t = 0")
+        model.set_obstacle(*(masks[n] for n in MASKS))
     model.set_scalar("vol_ini", scal["vol_ini"])
     model.set_scalar("vol_ins", scal["vol_ins"])
     # time-step table of restart_ini (:252-270); the time restarts at zero
@@ -159,11 +165,11 @@ def _interp_cf(a: np.ndarray, axis: int) -> np.ndarray:
     return np.concatenate([first, inner, last], axis=axis)
 
 
-def campos_arrays(p, fields: dict, t_plot: int = 1) -> list:
+def campos_arrays(p, fields: dict, t_plot: int = 1, kw=None) -> list:
     """The arrays of one campos file (4_plot.f90:255-340), in FP64 before the float32 store.
 
     `fields` holds u, v, w, ls (and prd1, nut for t_plot = 1) as downloaded (Fortran extents
-    with halos, 0-based numpy indices)."""
+    with halos, 0-based numpy indices); `kw` is the w obstacle mask, if any."""
     nx, ny, nz = p.nx, p.ny, p.nz
     u, v, w = fields["u"], fields["v"], fields["w"]
     # corner coordinates: x1(0) = -dx, x1(i) = x1(i-1) + dx summed in order (:252-264)
@@ -180,7 +186,11 @@ def campos_arrays(p, fields: dict, t_plot: int = 1) -> list:
     uaux = (u[I, J, K] + u[I, Jm, K] + u[I, J, Km] + u[I, Jm, Km]) * 0.25
     vaux = (v[I, J, K] + v[Im, J, K] + v[I, J, Km] + v[Im, J, Km]) * 0.25
     waux = (w[I, J, K] + w[I, Jm, K] + w[Im, J, K] + w[Im, Jm, K]) * 0.25
-    kaux = np.zeros((nx, ny, nz))          # obstacle mask (obst_t = 0, :285-286)
+    # obstacle cells: kaux(i,j,k) = 1 for k = 1 .. kw(i,j)-1 (:285-296)
+    kaux = np.zeros((nx, ny, nz))
+    if kw is not None:
+        kk = np.arange(1, nz + 1)[None, None, :]
+        kaux[kk < np.asarray(kw)[1:nx + 1, 1:ny + 1, None]] = 1.
     out = [x11, y11, z11, uaux, vaux, waux, fields["ls"], kaux]
     if t_plot == 1:
         c = (slice(1, nx + 1), slice(1, ny + 1), slice(1, nz + 1))
@@ -321,9 +331,9 @@ class FieldWriter:
             job = self.q.get()
             if job is None:
                 return
-            path, fields = job
+            path, fields, kw = job
             try:
-                write_campos(path, campos_arrays(self.p, fields, self.t_plot))
+                write_campos(path, campos_arrays(self.p, fields, self.t_plot, kw))
             except BaseException as e:   # reported by the next snapshot() or close()
                 self.error = e
 
@@ -335,9 +345,10 @@ class FieldWriter:
     def snapshot(self, model) -> pathlib.Path:
         self._raise()
         fields = {n: model.download(n) for n in CAMPOS_FIELDS[self.t_plot]}
+        masks = getattr(model, "obstacle", None)
         path = self.dir / campos_name(self.next)
         self.next += 1
-        self.q.put((path, fields))
+        self.q.put((path, fields, None if masks is None else masks[2]))
         return path
 
     def close(self) -> None:

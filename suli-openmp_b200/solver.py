@@ -144,6 +144,17 @@ class Solver:
         return out
 
     # ---------------------------------------------------------------- reference surface
+    def set_obstacle(self, ku, kv, kw) -> None:
+        """Bottom-obstacle masks (integer arrays in Fortran layout, shapes _abi.mask_shapes);
+        needs obst_t != 0, before iniciais.  See cases.obstaculo for the reference's presets."""
+        m = [np.asfortranarray(a, dtype=np.int32) for a in (ku, kv, kw)]
+        for a, s in zip(m, _abi.mask_shapes(self.params)):
+            if a.shape != s:
+                raise ValueError(f"mask shape {a.shape} != {s}")
+        P = C.POINTER(C.c_int)
+        self._check(self.lib.suli_set_obstacle(self._h, *[a.ctypes.data_as(P) for a in m]), "set_obstacle")
+        self.obstacle = tuple(a.copy() for a in m)
+
     def iniciais(self, u_init: float = 0.0) -> None:
         self._check(self.lib.suli_iniciais(self._h, float(u_init)), "iniciais")
 

@@ -82,8 +82,11 @@ def test_invalid_parameters_rejected(pkg):
     p.ccx0, p.ccxf = 0, 2           # periodic on one side only (0_modules.f90:56)
     assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_ARG
     p = pkg.default_params()
-    p.obst_t = 3                    # obstacles are not built
+    p.t_hs = 1                      # the second Heaviside form is not built
     assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_UNSUPPORTED
+    p = pkg.default_params()
+    p.obst_t = 11                   # obstaculo has presets 1..10
+    assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_ARG
     p = pkg.default_params()
     p.nx = 3                        # WENO needs 4 cells per direction
     assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_ARG

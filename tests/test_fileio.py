@@ -93,7 +93,9 @@ def test_restart_reads_list_directed_forms(orc, tmp_path):
     assert o.get_scalar("vol_ins") == ref["vol_ins"][0]
 
 
-def test_restart_refuses_other_grids_and_obstacles(orc, tmp_path):
+def test_restart_refuses_other_grids_and_unexpected_obstacles(orc, tmp_path):
+    """A file of another grid is refused, and so is one with obstacle masks for a model run
+    without obstacles (obst_t = 0)."""
     p, o = stepped_oracle(orc, steps=1)
     f = tmp_path / "arquivorestart"
     fileio.write_restart(o, f)
@@ -106,7 +108,7 @@ def test_restart_refuses_other_grids_and_obstacles(orc, tmp_path):
     k = sum(int(np.prod(fileio.restart_shape(p, n))) for n in ("u", "v", "w"))
     lines[k] = "3"
     f.write_text("\n".join(lines))
-    with pytest.raises(ValueError, match="obstacles"):
+    with pytest.raises(ValueError, match="obst_t = 0"):
         fileio.read_restart(orc.Oracle(p), f)
 
 
