@@ -92,7 +92,8 @@ typedef struct suli_params {
     int    mg_kernels;              /* precision 1: 0 = vectorised multigrid/PCG kernels (4 cells a
                                        thread, float4 loads; default), 1 = one cell a thread (same
                                        arithmetic, kept as the reference the tests compare with) */
-    int    reserved[3];
+    int    wave_t;                  /* wave inflow at x = 0: 0 none, 1 Stokes I, 2 Stokes II, 5 Stokes V (0_modules.f90:35) */
+    int    reserved[2];
 } suli_params;
 
 /* ---- field identifiers (module arrays of 0_modules.f90) ------------------------------ */
@@ -183,6 +184,10 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid); /* 9_grad.f90:10-278; 
 int suli_posdin(suli_ctx* c);                              /* 10_pos.f90:1-96          */
 int suli_est(suli_ctx* c, double* max_div);                /* 4_plot.f90:500-525 (FP64) */
 int suli_set_dt(suli_ctx* c, double dt);                   /* dt = a_dt(tt), 1_principal.f90:78 */
+/* boundary_waves() (3_contorno.f90:952-1082): with wave_t != 0, the wave's inflow planes
+   bxx0, bxx1, bxz0 at the context's time t, the level set of column i = 1, and the reference's
+   single-precision round trip of the whole level set; the step calls it after tempo. */
+int suli_boundary_waves(suli_ctx* c);
 
 typedef struct suli_step_stats {
     int    cg_iters[3];     /* Poisson iterations of each RK stage (inner FP32 iterations for precision 1) */

@@ -79,6 +79,7 @@ def load(openmp: bool = False) -> C.CDLL:
         "orc_last_reinit_iters": (i, [vp]),
         "orc_num_threads": (i, []),
         "orc_set_obstacle": (i, [vp, P(i), P(i), P(i)]),
+        "orc_boundary_waves": (i, [vp]),
         "orc_field_extent": (i, [P(abi.SuliParams), i, P(i), P(i)]),
     }
     for name, (res, args) in sig.items():
@@ -156,6 +157,9 @@ class Oracle:
         if rc != 0:
             raise ValueError("oracle: mask values out of range")
         self.obstacle = tuple(a.copy() for a in m)
+
+    def boundary_waves(self):
+        assert self.lib.orc_boundary_waves(self._h) == 0
 
     def iniciais(self, u_init=0.0):
         self.lib.orc_iniciais(self._h, float(u_init))

@@ -88,6 +88,12 @@ struct Oracle {
     int KW(int i, int j) const { return kw[(size_t)i + (size_t)(nx + 2) * j]; }
     void contorno_obstacle();
     void level_set_obstacle();
+    /* wave inflow (module wave_c, 0_modules.f90:164-174) */
+    double p_w = 0, n_w = 0, c_w = 0, l_w = 0, a_w = 0, f_w = 0, h0_f = 0, l0_w = 0;
+    double avel[6] = {0}, aeta[6] = {0};   /* avel1..5, aeta1..5 at [1..5] */
+    std::vector<double> kp;                /* kp(0:nz+1) */
+    void waves_coef();
+    void boundary_waves();
     /* statistics of the last calls */
     int last_cg_iters = 0;
     double last_cg_resid = 0.0;
@@ -1178,6 +1184,137 @@ void Oracle::level_set_obstacle() {
             }
 }
 
+/* waves_coef — 3_contorno.f90:1084-1205: Stokes I/II wavelength by fixed-point iteration of
+ * the dispersion relation; Stokes V by scanning wavelengths for the two conditions on lamb. */
+void Oracle::waves_coef() {
+    const double pi = std::acos(-1.), gz = P.gz;
+    kp.assign(nz + 2, 0.);
+    for (int k = 0; k <= nz + 1; ++k) kp[k] = (k - 0.5) * dz;
+    a_w = 0.03; p_w = 2.5; h0_f = 1.;
+    l0_w = gz * p_w * p_w / (2. * pi);
+    if (P.wave_t <= 2) {
+        l_w = gz * p_w * p_w / (2. * pi);
+        for (int i = 1; i <= 1000; ++i) l_w = gz * p_w * p_w / (2. * pi) * std::tanh(2. * pi * h0_f / l_w);
+        c_w = l_w / p_w; f_w = 2. * pi / p_w; n_w = 2. * pi / l_w;
+        return;
+    }
+    /* wave_t == 5 */
+    auto pw = [](double x, double e) { return std::pow(x, e); };
+    double erro0 = 999., lamb = 0.;
+    const int nxii = 10000;
+    double s, c, b33, b35, b55, c1, c2;
+    auto coefs = [&](double lw) {
+        s = std::sinh(2. * pi * h0_f / lw);
+        c = std::cosh(2. * pi * h0_f / lw);
+        b33 = 3. * (8. * pw(c, 6.) + 1.) / (64. * pw(s, 6.));
+        b35 = (88128. * pw(c, 14.) - 208224. * pw(c, 12) + 70848. * pw(c, 10.) + 54000. * pw(c, 8.) - 21816. * pw(c, 6.) +
+               6264. * pw(c, 4.) - 54. * c * c - 81.) / (12288. * pw(s, 12.) * (6. * c * c - 1.));
+        b55 = (192000. * pw(c, 16.) - 262720. * pw(c, 14.) + 83680. * pw(c, 12) + 20160. * pw(c, 10.) - 7280. * pw(c, 8.) +
+               7160. * pw(c, 6.) - 1800. * pw(c, 4.) - 1050. * c * c + 225.) /
+              (12288 * pw(s, 10.) * (6. * c * c - 1.) * (8. * pw(c, 4.) - 11. * c * c + 3.));
+        c1 = (8. * pw(c, 4.) - 8. * c * c + 9.) / (8. * pw(s, 4.));
+        c2 = (3840. * pw(c, 12.) - 4096. * pw(c, 10.) + 2592. * pw(c, 8.) - 1008. * pw(c, 6.) + 5944. * pw(c, 4.) - 1830. * c * c +
+              147.) / (512. * pw(s, 10.) * (6. * c * c - 1.));
+    };
+    for (int ii = 1; ii <= nxii; ++ii) {
+        double lamb1 = 0., lamb2 = 0.;
+        const double l_w1 = l0_w * 0.5 + l0_w * ((double)ii / nxii) * 2.5;
+        coefs(l_w1);
+        for (int i = 1; i <= 10000; ++i) lamb1 = pi * a_w * 2. / l_w1 - pw(lamb1, 3.) * b33 - pw(lamb1, 5.) * (b35 + b55);
+        for (int i = 1; i <= 10000; ++i)
+            lamb2 = std::sqrt((l_w1 / (l0_w * std::tanh(2. * pi * h0_f / l_w1)) - 1.) / (c1 + pw(lamb2, 2.) * c2));
+        const double erro = std::fabs(lamb1 - lamb2);
+        if (erro < erro0) { erro0 = erro; lamb = lamb1; l_w = l_w1; }
+    }
+    c_w = l_w / p_w; f_w = 2. * pi / p_w; n_w = 2. * pi / l_w;
+    coefs(l_w);
+    const double a11 = 1. / s;
+    const double a13 = -c * c * (5. * c * c + 1.) / (8. * pw(s, 5.));
+    const double a15 = -(1184. * pw(c, 10.) - 1440. * pw(c, 8.) - 1992. * pw(c, 6.) + 2641. * pw(c, 4.) - 249. * pw(c, 2.) + 18.) /
+                       (1536. * pw(s, 11.));
+    const double a22 = 3. / (8. * pw(s, 4.));
+    const double a24 = (192. * pw(c, 8.) - 424. * pw(c, 6.) - 312. * pw(c, 4.) + 480. * c * c - 17.) / (768. * pw(s, 10.));
+    const double a33 = (13. - 4. * c * c) / (64. * pw(s, 7.));
+    const double a35 = (512. * pw(c, 12.) + 4224. * pw(c, 10.) - 6800. * pw(c, 8.) - 12808. * pw(c, 6.) + 16704. * pw(c, 4.) -
+                        3154. * c * c + 107.) / (4096. * pw(s, 13.) * (6. * c * c - 1.));
+    const double a44 = (80. * pw(c, 6.) - 816. * pw(c, 4.) + 1338. * c * c - 197.) / (1536. * pw(s, 10.) * (6. * c * c - 1.));
+    const double a55 = -(2880. * pw(c, 10.) - 72480. * pw(c, 8.) + 324000. * pw(c, 6.) - 432000. * pw(c, 4.) + 163470. * c * c - 16245.) /
+                       (61440. * pw(s, 11.) * (6. * c * c - 1.) * (8. * pw(c, 4.) - 11. * c * c + 3.));
+    const double b22 = c * (2. * c * c + 1.) / (4. * pw(s, 3.));
+    const double b24 = c * (272. * pw(c, 8.) - 504. * pw(c, 6.) - 192. * pw(c, 4.) + 322 * c * c + 21.) / (384. * pw(s, 9.));
+    const double b44 = c * (768. * pw(c, 10.) - 448. * pw(c, 8.) - 48. * pw(c, 6.) + 48. * pw(c, 4.) + 106. * c * c - 21.) /
+                       (384. * pw(s, 9.) * (6. * c * c - 1.));
+    aeta[1] = lamb / n_w;
+    aeta[2] = (lamb * lamb * b22 + pw(lamb, 4.) * b24) / n_w;
+    aeta[3] = (pw(lamb, 3.) * b33 + pw(lamb, 5.) * b35) / n_w;
+    aeta[4] = pw(lamb, 4.) * b44 / n_w;
+    aeta[5] = pw(lamb, 5.) * b55 / n_w;
+    avel[1] = 1. * 2. * pi / (p_w * n_w) * (lamb * a11 + pw(lamb, 3.) * a13 + pw(lamb, 5.) * a15);
+    avel[2] = 2. * 2. * pi / (p_w * n_w) * (pw(lamb, 2.) * a22 + pw(lamb, 4.) * a24);
+    avel[3] = 3. * 2. * pi / (p_w * n_w) * (pw(lamb, 3.) * a33 + pw(lamb, 5.) * a35);
+    avel[4] = 4. * 2. * pi / (p_w * n_w) * (pw(lamb, 4.) * a44);
+    avel[5] = 5. * 2. * pi / (p_w * n_w) * (pw(lamb, 5.) * a55);
+}
+
+/* boundary_waves — 3_contorno.f90:952-1082: the wave's elevation, u and w at the inflow
+ * columns i = 0, 1 at time t.  The reference works on a single-precision copy ls1 of the
+ * level set and copies all of it back, so every call rounds ls to float32; the inflow column
+ * i = 1 takes the elevation's distance h_f(1) - kp(k).  Of the planes it writes, bxy0 comes
+ * from an array v1 that is never set and the top row of bxz0 from an unset w1(0,:,nz+2):
+ * both are 0 here. */
+void Oracle::boundary_waves() {
+    if (kp.empty()) waves_coef();
+    const int W = P.wave_t;
+    const double tanhh = std::tanh(n_w * h0_f), shh = std::sinh(n_w * h0_f);
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) ls(i, j, k) = (double)(float)ls(i, j, k);
+    for (auto& x : bxy0.a) x = 0.;
+    for (int j = 0; j <= ny + 1; ++j) bxz0(j, nz1 + 1, 0) = 0.;
+    for (int k = 0; k <= nz + 1; ++k)
+        for (int j = 0; j <= ny + 1; ++j)
+            for (int i = 0; i <= 1; ++i) {
+                double hf, u1, w1;
+                const double aux2 = n_w * dx * (i - 0.5) - f_w * t, aux3 = n_w * dx * (i - 1.) - f_w * t;
+                if (W == 1) {
+                    hf = h0_f + a_w * std::cos(n_w * dx * (i - 0.5) - f_w * t);
+                } else if (W == 2) {
+                    hf = h0_f + a_w * std::cos(aux2) + n_w * a_w * a_w * (3. - tanhh * tanhh) / (4. * tanhh * tanhh * tanhh) * std::cos(2. * aux2);
+                } else {
+                    hf = h0_f + aeta[1] * std::cos(aux2) + aeta[2] * std::cos(2. * aux2) + aeta[3] * std::cos(3. * aux2) +
+                         aeta[4] * std::cos(4. * aux2) + aeta[5] * std::cos(5. * aux2);
+                }
+                const float ls1 = (float)(hf - kp[k]);
+                if (ls1 >= 0.f) {
+                    if (W == 1) {
+                        u1 = a_w * f_w * std::cosh(n_w * kp[k]) / shh * std::cos(n_w * dx * (i - 1.) - f_w * t);
+                        w1 = a_w * f_w * std::sinh(n_w * (kp[k] - 0.5 * dz)) / shh * std::sin(n_w * dx * (i - 0.5) - f_w * t);
+                    } else if (W == 2) {
+                        u1 = a_w * f_w * std::cosh(n_w * kp[k]) / shh * std::cos(aux3) +
+                             3. / 4. * a_w * a_w * f_w * n_w * std::cosh(2. * n_w * kp[k]) / std::pow(shh, 4.) * std::cos(2 * aux3);
+                        w1 = a_w * f_w * std::sinh(n_w * (kp[k] - 0.5 * dz)) / shh * std::sin(aux2) +
+                             3. / 4. * a_w * a_w * f_w * n_w * std::sinh(2. * n_w * (kp[k] - 0.5 * dz)) / std::pow(shh, 4.) *
+                                 std::sin(2. * aux3);
+                    } else {
+                        const double aux4 = n_w * kp[k], aux5 = n_w * (kp[k] - 0.5 * dz);
+                        u1 = avel[1] * std::cosh(aux4) * std::cos(aux3) + avel[2] * std::cosh(2 * aux4) * std::cos(2 * aux3) +
+                             avel[3] * std::cosh(3 * aux4) * std::cos(3 * aux3) + avel[4] * std::cosh(4 * aux4) * std::cos(4 * aux3) +
+                             avel[5] * std::cosh(5 * aux4) * std::cos(5 * aux3);
+                        w1 = avel[1] * std::sinh(aux5) * std::sin(aux2) + avel[2] * std::sinh(2 * aux5) * std::sin(2 * aux2) +
+                             avel[3] * std::sinh(3 * aux5) * std::sin(3 * aux2) + avel[4] * std::sinh(4 * aux5) * std::sin(4 * aux2) +
+                             avel[5] * std::sinh(5 * aux5) * std::sin(5 * aux2);
+                    }
+                } else {
+                    u1 = 0.; w1 = 0.;
+                }
+                if (i == 0) { bxx0(j, k, 0) = u1; bxz0(j, k, 0) = w1; }
+                else {
+                    bxx1(j, k, 0) = u1;
+                    if (j >= 1 && j <= ny && k >= 1 && k <= nz) ls(1, j, k) = (double)ls1;
+                }
+            }
+}
+
 void Oracle::contorno(int nlock) {
     const int X0 = P.ccx0, XF = P.ccxf, Y0 = P.ccy0, YF = P.ccyf, Z0 = P.ccz0, ZF = P.cczf;
     const int I1 = nx1 + 1, J1 = ny1 + 1, K1 = nz1 + 1;   /* u/v/w outer ghost index */
@@ -1540,6 +1677,9 @@ int orc_iniciais(void* h, double u_init) {
     std::fill(o->ub.a.begin(), o->ub.a.end(), 0.);
     std::fill(o->vb.a.begin(), o->vb.a.end(), 0.);
     std::fill(o->wb.a.begin(), o->wb.a.end(), 0.);
+    if (o->P.wave_t > 0) {                               /* 2_iniciais.f90:52-66 */
+        o->waves_coef();
+    } else {
     std::fill(o->bxx0.a.begin(), o->bxx0.a.end(), u_init);
     std::fill(o->bxx1.a.begin(), o->bxx1.a.end(), u_init);
     if (o->P.obst_t != 0) {
@@ -1551,6 +1691,7 @@ int orc_iniciais(void* h, double u_init) {
                 for (int k = 0; k <= o->KU(1, j); ++k) o->bxx1(jj, k, 0) = 0.;
                 for (int k = 0; k <= o->KU(0, j); ++k) o->bxx0(jj, k, 0) = 0.;
             }
+    }
     }
     const int tm = o->P.t_tempo;
     const double dt = o->P.dt;
@@ -1622,6 +1763,7 @@ int orc_step(void* h, int it, suli_step_stats* st) {
         o->visco();
         o->convdiff();
         o->tempo(tt, it);
+        if (o->P.wave_t > 0) o->boundary_waves();      /* 1_principal.f90:84 */
         o->contorno(2);
         const int n = o->graddin();
         if (n >= o->P.cg_maxit) status = SULI_WARN_CG_MAXIT;
@@ -1637,6 +1779,12 @@ int orc_step(void* h, int it, suli_step_stats* st) {
     return status;
 }
 int orc_last_reinit_iters(void* h) { return static_cast<Oracle*>(h)->last_reinit_iters; }
+int orc_boundary_waves(void* h) {
+    Oracle* o = static_cast<Oracle*>(h);
+    if (o->P.wave_t != 1 && o->P.wave_t != 2 && o->P.wave_t != 5) return SULI_ERR_ARG;
+    o->boundary_waves();
+    return 0;
+}
 /* the masks of obstaculo (3_contorno.f90:741-760), Fortran order, checked like
    suli_set_obstacle: ku, kv in [-1, nz], kw in [-1, nz+1] */
 int orc_set_obstacle(void* h, const int* ku, const int* kv, const int* kw) {

@@ -44,7 +44,8 @@ class SuliParams(C.Structure):
         ("mg_omega", C.c_double),
         ("mg_alpha", C.c_double),
         ("mg_kernels", C.c_int),
-        ("reserved", C.c_int * 3),
+        ("wave_t", C.c_int),
+        ("reserved", C.c_int * 2),
     ]
 
     def copy(self) -> "SuliParams":
@@ -219,6 +220,7 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
         "suli_est": (C.c_int, [vp, P(C.c_double)]),
         "suli_set_dt": (C.c_int, [vp, C.c_double]),
         "suli_set_obstacle": (C.c_int, [vp, P(C.c_int), P(C.c_int), P(C.c_int)]),
+        "suli_boundary_waves": (C.c_int, [vp]),
         "suli_step": (C.c_int, [vp, C.c_int, P(SuliStepStats)]),
         "suli_stream": (C.c_int, [vp, P(vp)]),
         "suli_profile_enable": (C.c_int, [vp, C.c_int]),
@@ -256,7 +258,7 @@ HEADER_SYMBOLS = [
     "suli_set_scalar", "suli_get_scalar", "suli_iniciais", "suli_level_set_ini",
     "suli_level_set", "suli_heaviside", "suli_mod_ls1", "suli_visco", "suli_convdiff",
     "suli_tempo", "suli_contorno", "suli_graddin", "suli_posdin", "suli_est",
-    "suli_set_dt", "suli_set_obstacle", "suli_step", "suli_stream", "suli_profile_enable", "suli_profile_read",
+    "suli_set_dt", "suli_set_obstacle", "suli_boundary_waves", "suli_step", "suli_stream", "suli_profile_enable", "suli_profile_read",
     "suli_est_static",
     "suli_nn_num_params", "suli_nn_create", "suli_nn_destroy", "suli_nn_last_error",
     "suli_nn_set_params", "suli_nn_get_params", "suli_nn_forward", "suli_nn_loss_grad",

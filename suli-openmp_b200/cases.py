@@ -269,6 +269,32 @@ def bump_channel(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-10, u_init=0.1):
     return p, init, masks
 
 
+def wave_channel(wave_t=1, nx=32, ny=8, nz=12, dx=0.1, dz=0.1, cg_tol=1e-10):
+    """A wave flume for the wave inflow of boundary_waves (3_contorno.f90:952-1082): still water
+    1 m deep (h0_f of waves_coef), the wave entering at x = 0 (ccx0 = 3), outflow at x = xf
+    (ccxf = 4), periodic y, no-slip bottom, free-slip top; dt from CFL 0.2 with sqrt(g h).
+    With this inflow and outflow the reference's Poisson solve (all-Neumann, 9_grad.f90) stays
+    convergent on cubic cells; with dz = dx/2 it diverges after a step, with or without the wave."""
+    p = default_params()
+    p.nx, p.ny, p.nz = nx, ny, nz
+    p.dx = p.dy = dx
+    p.dz = dz
+    p.ccx0, p.ccxf = 3, 4
+    p.ccy0 = p.ccyf = 0
+    p.ccz0, p.cczf = 2, 1
+    _two_phase(p, cs=0.1)
+    p.cg_tol = cg_tol
+    p.wave_t = wave_t
+    p.dt = 0.2 * min(dx, dz) / math.sqrt(9.81 * 1.0)
+    X, Y, Z = _centres(p)
+    ls0 = 1.0 - Z
+
+    def init(model):
+        standard_init(model, ls0)
+
+    return p, init
+
+
 def random_state(p: SuliParams, seed: int = 0, *, vel=0.2, wave=0.03):
     """Seeded random-but-smooth state for kernel-level parity tests."""
     rng = np.random.default_rng(seed)

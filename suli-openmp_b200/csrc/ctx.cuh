@@ -6,6 +6,7 @@
 #include <vector>
 #include "../../include/suli_gpu.h"
 #include "geom.cuh"
+#include "waves.cuh"
 
 namespace suli {
 
@@ -118,6 +119,7 @@ struct suli_ctx {
     int* obst_k = nullptr;
     const int *obst_ku = nullptr, *obst_kv = nullptr, *obst_kw = nullptr;   // into obst_k
     std::vector<int> obst_ku_host;
+    suli::WaveCoef wave;                // waves_coef of the wave inflow (wave_t != 0)
     int last_reinit_iters = 0;
     int last_volfix_iters = 0;
     // mixed-precision solve (precision = 1)
@@ -210,6 +212,7 @@ inline suli::Planes suli_ctx::planes() const {
 namespace suli {
 // ---- kernel launchers (k_fp64.cu) ----
 void launch_lsprops(suli_ctx* c, const double* ls, bool do_mod, bool do_hs, bool do_vol);
+void launch_boundary_waves(suli_ctx* c);
 void launch_curv(suli_ctx* c);
 void launch_ls_advect(suli_ctx* c, const double* cur, const double* phi0, double* out,
                       double a, double b, double gd);

@@ -803,6 +803,29 @@ __global__ void k_ls_obst(Geo G, const int* __restrict__ kw, double* ls) {
     }
 }
 
+// boundary_waves (3_contorno.f90:952-1082).  The reference rounds the whole level set through
+// a single-precision copy on every call (thread per cell), then writes the inflow planes and
+// the level set of column i = 1 from the wave (thread per (j, k), 0..ny+1 x 0..nz+2; k = nz+2
+// is the top row of bxz0, which the reference leaves unset: 0 here).
+__global__ void k_ls_round_float(Geo G, double* ls) {
+    const Thread3 t = tid3(1, 1, 1);
+    if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
+    const int c = G.idx32(t.i, t.j, t.k);
+    ls[c] = (double)(float)ls[c];
+}
+__global__ void k_waves(Geo G, WaveCoef W, double dx, double dz, double time, double* ls, double* bxx0, double* bxx1,
+                        double* bxz0) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    const int ny = G.ny, nz = G.nz, row = ny + 2;
+    if (j > ny + 1 || k > nz + 2) return;
+    if (k == nz + 2) { bxz0[j + row * k] = 0.; return; }
+    const WavePoint P0 = wave_point(W, 0, k, dx, dz, time), P1 = wave_point(W, 1, k, dx, dz, time);
+    bxx0[j + row * k] = P0.u;
+    bxz0[j + row * k] = P0.w;
+    bxx1[j + row * k] = P1.u;
+    if (j >= 1 && j <= ny && k >= 1 && k <= nz) ls[G.idx32(1, j, k)] = (double)P1.ls;
+}
+
 // nlock = 2: boundary-normal velocities, y then x then z (:297-441)
 __global__ void k_bc_ny(Geo G, BC bc, BCArgs A) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1359,6 +1382,15 @@ void launch_tempo(suli_ctx* c, int tt, int it) {
     T.tm = c->P.t_tempo; T.tt = tt; T.it = it; T.dt = c->dt;
     ProfScope ps(c, SULI_K_TEMPO, 1);
     k_tempo<<<faces_grid(G), kBlk, 0, c->stream>>>(G, T);
+}
+void launch_boundary_waves(suli_ctx* c) {
+    const Geo& G = c->g;
+    const dim3 b2(32, 8);
+    ProfScope ps(c, SULI_K_CONTORNO, 2);
+    k_ls_round_float<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->f[SULI_F_LS]);
+    cudaMemsetAsync(c->f[SULI_F_BXY0], 0, c->plane_elems[SULI_F_BXY0] * sizeof(double), c->stream);   // v1 never set
+    k_waves<<<grid3(G.ny + 2, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->wave, c->P.dx, c->P.dz, c->t, c->f[SULI_F_LS],
+                                                                     c->f[SULI_F_BXX0], c->f[SULI_F_BXX1], c->f[SULI_F_BXZ0]);
 }
 void launch_contorno(suli_ctx* c, int nlock) {
     const Geo& G = c->g;

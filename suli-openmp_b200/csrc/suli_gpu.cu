@@ -113,6 +113,9 @@ int validate(const suli_params* p, std::string& why) {
     if (p->ccy0 < 0 || p->ccy0 > 3 || p->ccyf < 0 || p->ccyf > 3) { why = "ccy0/ccyf out of range"; return SULI_ERR_ARG; }
     if (p->ccz0 < 0 || p->ccz0 > 3 || p->cczf < 0 || p->cczf > 3) { why = "ccz0/cczf out of range"; return SULI_ERR_ARG; }
     if (p->obst_t < 0 || p->obst_t > 10) { why = "obst_t must be 0 (none) or an obstaculo preset 1..10"; return SULI_ERR_ARG; }
+    if (p->wave_t != 0 && p->wave_t != 1 && p->wave_t != 2 && p->wave_t != 5) {
+        why = "wave_t must be 0 (none), 1 (Stokes I), 2 (Stokes II) or 5 (Stokes V)"; return SULI_ERR_ARG;
+    }
     if (p->t_hs != 0) { why = "t_hs != 0 is not built"; return SULI_ERR_UNSUPPORTED; }
     if (p->adv_type < 1 || p->adv_type > 3) { why = "adv_type must be 1 (classico), 2 (rotacional) or 3 (antissim)"; return SULI_ERR_ARG; }
     if (p->der < 1 || p->der > 3) { why = "der must be 1 (upwind), 2 (centred) or 3 (2nd-order upwind)"; return SULI_ERR_ARG; }
@@ -440,6 +443,16 @@ int suli_set_obstacle(suli_ctx* c, const int* ku, const int* kv, const int* kw) 
     return SULI_OK;
 }
 
+int suli_boundary_waves(suli_ctx* c) {
+    if (!c) return SULI_ERR_ARG;
+    if (c->P.wave_t == 0) return fail(c, SULI_ERR_ARG, "boundary_waves: wave_t is 0");
+    cudaSetDevice(c->device);
+    if (c->wave.type != c->P.wave_t) c->wave = wave_coefficients(c->P.wave_t, c->P.gz);
+    launch_boundary_waves(c);
+    CHECK_LAUNCH(c);
+    return SULI_OK;
+}
+
 int suli_iniciais(suli_ctx* c, double u_init) {
     if (!c) return SULI_ERR_ARG;
     cudaSetDevice(c->device);
@@ -454,7 +467,11 @@ int suli_iniciais(suli_ctx* c, double u_init) {
     launch_fill(c, c->f[SULI_F_WB], 0.);
     CHECK_LAUNCH(c);
     std::vector<double> bx0(c->plane_elems[SULI_F_BXX0], u_init), bx1(bx0);
-    if (c->P.obst_t != 0) {
+    if (c->P.wave_t > 0) {
+        // 2_iniciais.f90:52-54: waves_coef instead of the uniform inflow; boundary_waves writes
+        // the inflow planes at every stage
+        c->wave = wave_coefficients(c->P.wave_t, c->P.gz);
+    } else if (c->P.obst_t != 0) {
         // 2_iniciais.f90:60-65: bxx1(:,0:ku(1,j)) = 0 for every j zeroes whole rows of the
         // (0:ny+1, 0:nz+1) plane up to the highest ku(1,j) (likewise bxx0 with ku(0,j))
         if (c->obst_ku_host.empty()) return fail(c, SULI_ERR_ARG, "iniciais: obst_t != 0 needs suli_set_obstacle first");
@@ -465,8 +482,10 @@ int suli_iniciais(suli_ctx* c, double u_init) {
             for (int k = 0; k <= k0; ++k) std::fill_n(bx0.begin() + (size_t)rows * k, rows, 0.);
         }
     }
-    CUDA_TRY(c, cudaMemcpyAsync(c->f[SULI_F_BXX0], bx0.data(), bx0.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CUDA_TRY(c, cudaMemcpyAsync(c->f[SULI_F_BXX1], bx1.data(), bx1.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (c->P.wave_t == 0) {
+        CUDA_TRY(c, cudaMemcpyAsync(c->f[SULI_F_BXX0], bx0.data(), bx0.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(c->f[SULI_F_BXX1], bx1.data(), bx1.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
     const int tm = c->P.t_tempo;
     const double dt = c->P.dt;
     c->dt = dt;
@@ -896,6 +915,7 @@ int suli_step(suli_ctx* c, int it, suli_step_stats* st) {
         if ((r = suli_visco(c)) < 0) return r;
         if ((r = suli_convdiff(c)) < 0) return r;
         if ((r = suli_tempo(c, tt, it)) < 0) return r;
+        if (c->P.wave_t > 0 && (r = suli_boundary_waves(c)) < 0) return r;   // 1_principal.f90:84
         if ((r = suli_contorno(c, 2)) < 0) return r;
         int n = 0;
         double res = 0.;

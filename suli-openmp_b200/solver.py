@@ -155,6 +155,9 @@ class Solver:
         self._check(self.lib.suli_set_obstacle(self._h, *[a.ctypes.data_as(P) for a in m]), "set_obstacle")
         self.obstacle = tuple(a.copy() for a in m)
 
+    def boundary_waves(self) -> None:
+        self._check(self.lib.suli_boundary_waves(self._h), "boundary_waves")
+
     def iniciais(self, u_init: float = 0.0) -> None:
         self._check(self.lib.suli_iniciais(self._h, float(u_init)), "iniciais")
 
