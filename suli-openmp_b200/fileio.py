@@ -69,8 +69,8 @@ def restart_count(p) -> int:
 def write_restart(model, path, *, d_max: float = 0.0, d_min: float = 0.0, ls_m: float = 0.0) -> None:
     """restart_salva (11_diversos.f90:314-330): the state of `model` as a list-directed file.
 
-    d_max and d_min (0_modules.f90:124) are set to zero by `iniciais` and changed only by the
-    wave inflow, which is not built; ls_m (14_level_set.f90:46-51) is zero for t_hs = 0."""
+    d_max and d_min (0_modules.f90:124) are set to zero by `iniciais` (2_iniciais.f90:45-46)
+    and written nowhere else; ls_m (14_level_set.f90:46-51) is zero for t_hs = 0."""
     p = model.params
     scal = {"d_max": d_max, "d_min": d_min, "ls_m": ls_m,
             "vol_ini": model.get_scalar("vol_ini"), "vol_ins": model.get_scalar("vol_ins")}
