@@ -269,6 +269,55 @@ def bump_channel(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-10, u_init=0.1):
     return p, init, masks
 
 
+def les_channel(nx=512, ny=256, nz=256, cg_tol=1e-8, seed=0, x0=3.0):
+    """The LES channel over a bottom bump: 6 x 3 x 3 m (dx = dy = dz = 6/nx at the default
+    size, 0.01171875), water 2 m deep, the obst_t = 3 Gaussian bump with height 0.3 m, no flat
+    base (d = 0), sigma 0.5 m, centred at (x0, Ly/2); inflow u = 1 + 0.05 U(-1, 1) (seeded,
+    per inflow-plane point) at x = 0, outflow at x = xf, periodic y, no-slip bottom, free-slip
+    top, Smagorinsky Cs = 0.12, RK3, dt from CFL 0.3 with the inflow speed plus sqrt(g h).
+    Smaller nx, ny, nz keep the 6 x 3 x 3 m box at the coarser spacing.
+
+    The reference's pressure solve has Neumann conditions on every face and no correction of
+    the net flux (9_grad.f90:96-116): with this fluctuating inflow and the boundary layer the
+    outflow copy carries, the problem is inconsistent and its CG diverges within the first
+    steps (in this library and in the CPU restatement of the tests alike), as it does for the
+    wave flume; a uniform flow
+    through the same faces stays exactly steady."""
+    p = default_params()
+    p.nx, p.ny, p.nz = nx, ny, nz
+    p.dx, p.dy, p.dz = 6.0 / nx, 3.0 / ny, 3.0 / nz
+    p.ccx0, p.ccxf = 3, 4
+    p.ccy0 = p.ccyf = 0
+    p.ccz0, p.cczf = 2, 1
+    _two_phase(p, cs=0.12)
+    p.cg_tol = cg_tol
+    p.obst_t = 3
+    p.dt = 0.3 * min(p.dx, p.dy, p.dz) / (1.05 + math.sqrt(9.81 * 2.0))
+    ly = ny * p.dy
+
+    def height(i, j):
+        x, y = (i - 1.) * (p.dx * 0.5), (j - 1.) * (p.dy * 0.5)
+        return np.exp(-((x - x0) * (x - x0) / (2. * 0.5 * 0.5)) - (y - ly / 2.) * (y - ly / 2.) / (2. * 0.5 * 0.5)) * 0.3
+
+    masks = obstacle_masks(p, height)
+    X, Y, Z = _centres(p)
+    ls0 = 2.0 - Z
+    rng = np.random.default_rng(seed)
+    from ._abi import field_shape
+    inflow = 1.0 + 0.05 * rng.uniform(-1.0, 1.0, field_shape(p, "bxx0"))
+
+    def init(model):
+        standard_init(model, ls0, 1.0, masks=masks)
+        # the inflow planes with the seeded fluctuation, zero inside the bump as iniciais makes
+        # them (2_iniciais.f90:60-65)
+        for name in ("bxx0", "bxx1"):
+            plane = model.download(name)
+            model.upload(name, np.where(plane == 0.0, 0.0, inflow))
+        model.contorno(1)
+
+    return p, init, masks
+
+
 def wave_channel(wave_t=1, nx=32, ny=8, nz=12, dx=0.1, dz=0.1, cg_tol=1e-10):
     """A wave flume for the wave inflow of boundary_waves (3_contorno.f90:952-1082): still water
     1 m deep (h0_f of waves_coef), the wave entering at x = 0 (ccx0 = 3), outflow at x = xf

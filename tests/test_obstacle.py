@@ -256,3 +256,14 @@ def test_restart_and_campos_carry_the_masks(orc, tmp_path):
     kw = masks[2]
     for i, j in ((1, 1), (16, 8), (20, 3)):
         assert (kaux[i - 1, j - 1, :] == (np.arange(1, p.nz + 1) < kw[i, j])).all()
+
+
+def test_les_channel_case():
+    """Config C5 built at a small size: the 6 x 3 x 3 m box, the 0.3 m bump's masks, the seeded
+    inflow 1 +- 0.05."""
+    p, init, masks = cases.les_channel(nx=48, ny=24, nz=24)
+    assert (p.nx * p.dx, p.ny * p.dy, p.nz * p.dz) == (6.0, 3.0, 3.0) and p.obst_t == 3
+    kw = masks[2]
+    assert kw.max() == int(np.floor(0.3 * np.exp(-(((2 * 24 - 1) * p.dx / 2 - 3.0) ** 2 / 0.5)
+                                                   - ((2 * 12 - 1) * p.dy / 2 - 1.5) ** 2 / 0.5) / p.dz + 1.))
+    assert kw.min() == 1

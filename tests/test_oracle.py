@@ -591,3 +591,21 @@ def test_rotational_form_on_linear_velocity(orc):
                                rtol=0, atol=1e-11 * a * a)
     np.testing.assert_allclose(-Fv, np.broadcast_to((a * a * (yf[1:-1] + p.dy))[None, :, None], Fv.shape),
                                rtol=0, atol=1e-11 * a * a)
+
+
+def test_uniform_inflow_outflow_stays_steady(orc):
+    """Uniform u = 1 entering through a prescribed face (ccx0 = 3, 3_contorno.f90:139-197) and
+    leaving through the outflow copy (ccxf = 4, :362-409), with a free surface under gravity:
+    the flow stays exactly uniform and divergence-free over three steps."""
+    p = small_params(nx=24, ny=8, nz=12, bc=(3, 4, 0, 0, 1, 1), dx=0.1)
+    p.cg_stop, p.cg_tol, p.cg_maxit = 1, 1e-10, 20000
+    p.dt = 0.01
+    o = orc.Oracle(p)
+    z = (np.arange(1, p.nz + 1) - 0.5) * p.dz
+    pkg_cases = __import__("helpers").pkg.cases
+    pkg_cases.standard_init(o, np.broadcast_to(0.7 - z, o.shape("ls")).copy(), 1.0)
+    for it in range(1, 4):
+        st = o.step(it)
+        assert st["status"] == 0 and st["max_div"] < 1e-12
+    u = o.download("u")[1:p.nx + 2, 1:p.ny + 1, 1:p.nz + 1]
+    assert np.abs(u - 1.0).max() < 1e-12
