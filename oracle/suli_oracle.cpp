@@ -411,7 +411,7 @@ void Oracle::reinic_weno() {
     last_reinit_iters = il;
 }
 
-/* heaviside — 14_level_set.f90:612-707 (t_hs = 0). */
+/* heaviside — 14_level_set.f90:612-707 (t_hs = 0 and 1). */
 void Oracle::heaviside() {
     Arr ta1, tb1, tc1, td1, te1, tf1;
     cell(ta1); cell(tb1); cell(tc1); cell(td1); cell(te1); cell(tf1);
@@ -439,8 +439,13 @@ void Oracle::heaviside() {
                     hsz(i, j, k) = 0.5 * gzv * (1. + cs) / ad;
                 }
                 hs(i, j, k) = h;
-                rho(i, j, k) = P.rho_f1 * (1. - h) + P.rho_f2 * h;
-                ls_nu(i, j, k) = P.mi_f1 * (1. - h) + P.mi_f2 * h;
+                if (P.t_hs == 0) {
+                    rho(i, j, k) = P.rho_f1 * (1. - h) + P.rho_f2 * h;
+                    ls_nu(i, j, k) = P.mi_f1 * (1. - h) + P.mi_f2 * h;
+                } else {                                /* :700-701, aux1 = mi_f1*10000 (:656-657) */
+                    rho(i, j, k) = std::pow(P.rho_f1, 1. - h) + std::pow(P.rho_f2, h) - 1.;
+                    ls_nu(i, j, k) = (std::pow(P.mi_f1 * 10000., 1. - h) + std::pow(P.mi_f2 * 10000., h) - 1.) / 10000.;
+                }
             }
 }
 
@@ -1703,6 +1708,12 @@ int orc_iniciais(void* h, double u_init) {
 }
 int orc_level_set_ini(void* h) {
     Oracle* o = static_cast<Oracle*>(h);
+    if (o->P.t_hs != 0) {                              /* 14_level_set.f90:47-51, 196-202 */
+        const double ls_m = 0.481803535 * o->dx1 * o->P.alpha1;
+        for (int k = 1; k <= o->nz; ++k)
+            for (int j = 1; j <= o->ny; ++j)
+                for (int i = 1; i <= o->nx; ++i) o->ls(i, j, k) = o->ls(i, j, k) + ls_m;
+    }
     o->heaviside();
     o->vol_ini = o->volume();
     o->mod_ls1();

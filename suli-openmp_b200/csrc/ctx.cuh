@@ -221,6 +221,7 @@ void launch_reinit_stage(suli_ctx* c, const double* cur, const double* phi0, dou
                          double a, double b, double gd);
 void launch_reinit_err(suli_ctx* c, const double* after, const double* before, double band);
 void launch_volfix(suli_ctx* c, double fac);
+void launch_ls_shift(suli_ctx* c, double shift);
 void launch_visco(suli_ctx* c);
 void launch_convdiff(suli_ctx* c);
 void launch_tempo(suli_ctx* c, int tt, int it);

@@ -75,6 +75,8 @@ struct LsConst {
     double ad;          // alpha1*dx1
     double pi;
     double rho1, rho2, mi1, mi2;
+    int t_hs;           // 0 linear mix of rho and mu in H, 1 geometric (14_level_set.f90:696-703)
+    double mu1s, mu2s;  // mi_f1 * 10000, mi_f2 * 10000
 };
 
 // ------------------------------------------------------------------------------------
@@ -115,8 +117,13 @@ __global__ void __launch_bounds__(256) k_lsprops(Geo G, LsConst L, const double*
                 hsz[c] = 0.5 * cc * (1. + cs) / L.ad;
             }
             hs[c] = h;
-            rho[c] = L.rho1 * (1. - h) + L.rho2 * h;
-            ls_nu[c] = L.mi1 * (1. - h) + L.mi2 * h;
+            if (L.t_hs == 0) {
+                rho[c] = L.rho1 * (1. - h) + L.rho2 * h;
+                ls_nu[c] = L.mi1 * (1. - h) + L.mi2 * h;
+            } else {
+                rho[c] = pow(L.rho1, 1. - h) + pow(L.rho2, h) - 1.;
+                ls_nu[c] = (pow(L.mu1s, 1. - h) + pow(L.mu2s, h) - 1.) / 10000.;
+            }
             if (do_vol) vol = (1. - (1. - h)) * L.dx * L.dy * L.dz;
         }
     }
@@ -230,6 +237,14 @@ __global__ void __launch_bounds__(256) k_reinit_err(Geo G, const double* __restr
     }
     double ta, tb;
     if (reduce2_last(s, n, partial, counter, ta, tb) && flat_tid() == 0) { out[0] = ta; out[1] = tb; }
+}
+
+// ls = ls + ls_m over the cells (14_level_set.f90:196-202)
+__global__ void k_ls_shift(Geo G, double* ls, double shift) {
+    const Thread3 t = tid3(1, 1, 1);
+    if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
+    const long long c = G.idx(t.i, t.j, t.k);
+    ls[c] = ls[c] + shift;
 }
 
 // volume correction step (14_level_set.f90:259-265)
@@ -1243,6 +1258,8 @@ static LsConst ls_const(const suli_ctx* c) {
     L.ad = c->P.alpha1 * L.dx1;
     L.pi = acos(-1.0);
     L.rho1 = c->P.rho_f1; L.rho2 = c->P.rho_f2; L.mi1 = c->P.mi_f1; L.mi2 = c->P.mi_f2;
+    L.t_hs = c->P.t_hs;
+    L.mu1s = c->P.mi_f1 * 10000.; L.mu2s = c->P.mi_f2 * 10000.;
     return L;
 }
 static dim3 cells_grid(const Geo& g) { return grid3(g.nx, g.ny, g.nz, kBlk); }
@@ -1291,6 +1308,11 @@ void launch_reinit_err(suli_ctx* c, const double* after, const double* before, d
     ProfScope ps(c, SULI_K_REINIT, 1);
     k_reinit_err<<<cells_grid(G), kBlk, 0, c->stream>>>(G, after, before, band, c->red_partial, c->red_counter,
                                                          c->red_out);
+}
+void launch_ls_shift(suli_ctx* c, double shift) {
+    const Geo& G = c->g;
+    ProfScope ps(c, SULI_K_VOLFIX, 1);
+    k_ls_shift<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->f[SULI_F_LS], shift);
 }
 void launch_volfix(suli_ctx* c, double dt1fac) {
     const Geo& G = c->g;

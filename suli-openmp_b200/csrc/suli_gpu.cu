@@ -116,7 +116,7 @@ int validate(const suli_params* p, std::string& why) {
     if (p->wave_t != 0 && p->wave_t != 1 && p->wave_t != 2 && p->wave_t != 5) {
         why = "wave_t must be 0 (none), 1 (Stokes I), 2 (Stokes II) or 5 (Stokes V)"; return SULI_ERR_ARG;
     }
-    if (p->t_hs != 0) { why = "t_hs != 0 is not built"; return SULI_ERR_UNSUPPORTED; }
+    if (p->t_hs != 0 && p->t_hs != 1) { why = "t_hs must be 0 (linear) or 1 (geometric) (14_level_set.f90:696-703)"; return SULI_ERR_ARG; }
     if (p->adv_type < 1 || p->adv_type > 3) { why = "adv_type must be 1 (classico), 2 (rotacional) or 3 (antissim)"; return SULI_ERR_ARG; }
     if (p->der < 1 || p->der > 3) { why = "der must be 1 (upwind), 2 (centred) or 3 (2nd-order upwind)"; return SULI_ERR_ARG; }
     if (p->adv_type != 1 && p->der != 1) {   // the reference stops there (7_advectivo.f90:450-451, 646-647)
@@ -516,6 +516,10 @@ int suli_mod_ls1(suli_ctx* c) {
 int suli_level_set_ini(suli_ctx* c) {
     if (!c) return SULI_ERR_ARG;
     cudaSetDevice(c->device);
+    if (c->P.t_hs != 0) {   // the preset shifted by ls_m for the geometric mix (14_level_set.f90:47-51, 196-202)
+        const double dx1 = fmax(c->P.dx, fmax(c->P.dy, c->P.dz));
+        launch_ls_shift(c, 0.481803535 * dx1 * c->P.alpha1);
+    }
     launch_lsprops(c, c->f[SULI_F_LS], true, true, true);
     launch_curv(c);
     CHECK_LAUNCH(c);

@@ -66,12 +66,15 @@ def restart_count(p) -> int:
 
 
 # ---------------------------------------------------------------------------------- restart
-def write_restart(model, path, *, d_max: float = 0.0, d_min: float = 0.0, ls_m: float = 0.0) -> None:
+def write_restart(model, path, *, d_max: float = 0.0, d_min: float = 0.0, ls_m: float | None = None) -> None:
     """restart_salva (11_diversos.f90:314-330): the state of `model` as a list-directed file.
 
     d_max and d_min (0_modules.f90:124) are set to zero by `iniciais` (2_iniciais.f90:45-46)
-    and written nowhere else; ls_m (14_level_set.f90:46-51) is zero for t_hs = 0."""
+    and written nowhere else; ls_m (14_level_set.f90:46-51) is zero for t_hs = 0 and
+    0.481803535 max(dx, dy, dz) alpha1 for t_hs = 1."""
     p = model.params
+    if ls_m is None:
+        ls_m = 0.0 if p.t_hs == 0 else 0.481803535 * max(p.dx, p.dy, p.dz) * p.alpha1
     scal = {"d_max": d_max, "d_min": d_min, "ls_m": ls_m,
             "vol_ini": model.get_scalar("vol_ini"), "vol_ins": model.get_scalar("vol_ins")}
     path = pathlib.Path(path)

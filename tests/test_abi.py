@@ -82,8 +82,12 @@ def test_invalid_parameters_rejected(pkg):
     p.ccx0, p.ccxf = 0, 2           # periodic on one side only (0_modules.f90:56)
     assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_ARG
     p = pkg.default_params()
-    p.t_hs = 1                      # the second Heaviside form is not built
+    p.nx, p.ny, p.nz = 15, 13, 11   # the mixed path's multigrid needs a grid that halves
+    p.precision, p.cg_stop = 1, 1
     assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_UNSUPPORTED
+    p = pkg.default_params()
+    p.t_hs = 2                      # the reference defines t_hs 0 and 1 (14_level_set.f90:696-703)
+    assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_ARG
     p = pkg.default_params()
     p.obst_t = 11                   # obstaculo has presets 1..10
     assert lib.suli_create(C.byref(p), 0, C.byref(h)) == pkg._abi.ERR_ARG

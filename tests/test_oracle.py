@@ -609,3 +609,27 @@ def test_uniform_inflow_outflow_stays_steady(orc):
         assert st["status"] == 0 and st["max_div"] < 1e-12
     u = o.download("u")[1:p.nx + 2, 1:p.ny + 1, 1:p.nz + 1]
     assert np.abs(u - 1.0).max() < 1e-12
+
+
+def test_geometric_heaviside(orc):
+    """t_hs = 1: rho = rho1^(1-H) + rho2^H - 1 and mu = ((1e4 mu1)^(1-H) + (1e4 mu2)^H - 1)/1e4
+    (14_level_set.f90:696-703), and level_set_ini shifts the preset by
+    ls_m = 0.481803535 max(dx,dy,dz) alpha1 first (:47-51, 196-202)."""
+    p = small_params(nx=8, ny=6, nz=20)
+    p.t_hs = 1
+    o = orc.Oracle(p)
+    z = (np.arange(1, p.nz + 1) - 0.5) * p.dz
+    ls0 = np.broadcast_to(0.2 - z, o.shape("ls")).copy()
+    o.upload("ls", ls0)
+    o.level_set_ini()
+    ls_m = 0.481803535 * max(p.dx, p.dy, p.dz) * p.alpha1
+    assert np.array_equal(o.download("ls"), ls0 + ls_m)
+    h = o.download("hs")
+    assert 0 < h.min() < 1e-12 or h.min() == 0.0
+    want_rho = p.rho_f1 ** (1. - h) + p.rho_f2 ** h - 1.
+    want_mu = ((p.mi_f1 * 1e4) ** (1. - h) + (p.mi_f2 * 1e4) ** h - 1.) / 1e4
+    np.testing.assert_allclose(o.download("rho"), want_rho, rtol=1e-15)
+    np.testing.assert_allclose(o.download("ls_nu"), want_mu, rtol=1e-15)
+    # the mix is geometric: at H = 1/2 rho is sqrt(rho1 rho2) + ... - 1, not the mean
+    mid = np.abs(h - 0.5).argmin()
+    assert abs(o.download("rho").ravel(order="F")[mid] - (p.rho_f1 + p.rho_f2) / 2) > 100

@@ -74,6 +74,17 @@ def test_heaviside_mod_ls1(pkg, orc, bc):
     compare(g, o, OUT_FIELDS["heaviside"] + OUT_FIELDS["mod_ls1"], what="heaviside/mod_ls1")
 
 
+def test_geometric_heaviside_gpu(pkg, orc):
+    """t_hs = 1: level_set_ini's ls_m shift and the geometric density and viscosity mix,
+    within 1e-13 (pow of the device and of the host differ in the last bits)."""
+    p = small_params(nx=13, ny=11, nz=9)
+    p.t_hs = 1
+    g, o = pair(pkg, orc, p, seed=1, derived=False)
+    for m in (g, o):
+        m.level_set_ini()
+    compare(g, o, ["ls"] + OUT_FIELDS["heaviside"] + OUT_FIELDS["mod_ls1"], what="t_hs = 1")
+
+
 @pytest.mark.parametrize("m_turb", [0, 1, 2])
 @pytest.mark.parametrize("bc", BCS[:3])
 def test_visco(pkg, orc, bc, m_turb):
