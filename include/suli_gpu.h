@@ -65,7 +65,7 @@ typedef struct suli_params {
     int    adv_type;                /* advective form: 1 classico, 2 rotacional, 3 antissim (2, 3 with der = 1) (0_modules.f90:27) */
     int    m_turb;                  /* 0 none, 1 Smagorinsky, 2 directional Smagorinsky (0_modules.f90:31) */
     int    obst_t;                  /* 0 none; 1..10 the obstaculo presets, masks set by suli_set_obstacle (0_modules.f90:29) */
-    int    t_hs;                    /* Heaviside type: only 0 (0_modules.f90:199)              */
+    int    t_hs;                    /* density/viscosity mix in H: 0 linear, 1 geometric (0_modules.f90:199) */
     double csmag;                   /* Smagorinsky constant (0_modules.f90:181)                */
     double gx, gz;                  /* gravity components, gz acts downward (0_modules.f90:143) */
     double chezy;                   /* wall-friction Chezy coefficient (0_modules.f90:141)     */
