@@ -160,7 +160,8 @@ int suli_get_scalar(suli_ctx* c, int scalar, double* v);
 /* iniciais() without the presets: u = u_init, v = w = 0, prd = 0, ub = 0, RK table
    (2_iniciais.f90:36-46, 85-104).  The level-set preset is written by the caller. */
 int suli_iniciais(suli_ctx* c, double u_init);
-/* heaviside(); vol_ini = sum(hs) dV; mod_ls1() (14_level_set.f90:205-217). */
+/* The tail of level_set_ini after the caller's preset: ls += ls_m for t_hs = 1, heaviside();
+   vol_ini = sum(hs) dV; mod_ls1() (14_level_set.f90:196-217). */
 int suli_level_set_ini(suli_ctx* c);
 /* The bottom-obstacle masks that obstaculo() computes (3_contorno.f90:494-762; module obst,
    0_modules.f90:76-79): for each column, the k up to which the velocities are zeroed.
