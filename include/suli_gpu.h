@@ -93,7 +93,12 @@ typedef struct suli_params {
                                        thread, float4 loads; default), 1 = one cell a thread (same
                                        arithmetic, kept as the reference the tests compare with) */
     int    wave_t;                  /* wave inflow at x = 0: 0 none, 1 Stokes I, 2 Stokes II, 5 Stokes V (0_modules.f90:35) */
-    int    reserved[2];
+    int    outflow_fix;             /* 0 = the reference's outflow copy (3_contorno.f90:193-197, 362-409);
+                                       1 (extension, needs ccxf = 4) = contorno(2) then shifts the
+                                       outflow plane u(nx+1,:,:) above the obstacle mask by one uniform
+                                       value so that the net boundary flux is zero and graddin's
+                                       all-Neumann system (9_grad.f90:96-116) is consistent */
+    int    reserved[1];
 } suli_params;
 
 /* ---- field identifiers (module arrays of 0_modules.f90) ------------------------------ */

@@ -88,6 +88,7 @@ struct Oracle {
     int KW(int i, int j) const { return kw[(size_t)i + (size_t)(nx + 2) * j]; }
     void contorno_obstacle();
     void level_set_obstacle();
+    void outflow_fix();
     /* wave inflow (module wave_c, 0_modules.f90:164-174) */
     double p_w = 0, n_w = 0, c_w = 0, l_w = 0, a_w = 0, f_w = 0, h0_f = 0, l0_w = 0;
     double avel[6] = {0}, aeta[6] = {0};   /* avel1..5, aeta1..5 at [1..5] */
@@ -1156,6 +1157,27 @@ void Oracle::contorno_obstacle() {
         for (int k = 0; k <= KV(i, ny1 + 1); ++k) v(i, ny1 + 1, k) = 0.;
 }
 
+/* Option outflow_fix = 1 (an extension; the reference has no counterpart): after
+ * contorno(2) has copied the outflow plane (ccxf = 4, 3_contorno.f90:193-197, 362-409), shift
+ * u(nx+1,j,k) by one uniform delta over the outflow faces above the obstacle mask so that the
+ * net volume flux through the boundary is zero.  graddin's all-Neumann system (9_grad.f90:96-116)
+ * is then consistent: the sum of its right-hand side over the cells, which telescopes to the
+ * net boundary flux, vanishes.  Sums in the order written here (j fastest, then k). */
+void Oracle::outflow_fix() {
+    double fx = 0., fy = 0., fz = 0.;
+    for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) fx = fx + (u(nx1, j, k) - u(1, j, k));
+    for (int k = 1; k <= nz; ++k) for (int i = 1; i <= nx; ++i) fy = fy + (v(i, ny1, k) - v(i, 1, k));
+    for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i) fz = fz + (w(i, j, nz1) - w(i, j, 1));
+    const double net = fx * (dy * dz) + fy * (dx * dz) + fz * (dx * dy);
+    long long open = 0;
+    for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) open += (!has_obstacle || k > KU(nx1, j)) ? 1 : 0;
+    if (open == 0) return;
+    const double delta = -net / ((double)open * (dy * dz));
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny; ++j)
+            if (!has_obstacle || k > KU(nx1, j)) u(nx1, j, k) = u(nx1, j, k) + delta;
+}
+
 /* contorno(3) (3_contorno.f90:445-481): the level set inside the obstacle (k < kw) taken
  * from the neighbouring fluid cells at the same height, or from the cell above at the
  * obstacle's top.  A neighbour outside 1..nx, 1..ny is never read: the reference reads ls
@@ -1442,6 +1464,7 @@ void Oracle::contorno(int nlock) {
         if (Z0 == 0 && ZF == 0) Z_all(w, [&](int i, int j) { w(i, j, nz1) = w(i, j, 1); });
         if (ZF == 1 || ZF == 2) Z_all(w, [&](int i, int j) { w(i, j, nz1) = 0.; });
         if (ZF == 3) Z_all(w, [&](int i, int j) { w(i, j, nz1) = bzzf(i, j, 0); });
+        if (P.outflow_fix == 1 && XF == 4) outflow_fix();
     }
     /* nlock = 3 acts only with obstacles (obst_t != 0, :445-487): nothing to do here. */
 }

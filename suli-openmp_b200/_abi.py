@@ -45,7 +45,8 @@ class SuliParams(C.Structure):
         ("mg_alpha", C.c_double),
         ("mg_kernels", C.c_int),
         ("wave_t", C.c_int),
-        ("reserved", C.c_int * 2),
+        ("outflow_fix", C.c_int),
+        ("reserved", C.c_int * 1),
     ]
 
     def copy(self) -> "SuliParams":

@@ -239,10 +239,16 @@ def obstaculo(p: SuliParams, obst_t: int) -> tuple:
     raise ValueError(f"obst_t {obst_t}: the reference defines presets 1..10")
 
 
-def bump_channel(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-10, u_init=0.1):
+def bump_channel(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-10, u_init=0.1, outflow_fix=0):
     """A small two-phase channel over a Gaussian bottom bump (the obst_t = 3 shape scaled to the
     box): water 0.6 of the depth, inflow u_init at x = 0 (ccx0 = 3), outflow at x = xf
-    (ccxf = 4), periodic y, free-slip top."""
+    (ccxf = 4), periodic y, free-slip top.
+
+    With the reference's outflow copy (outflow_fix = 0) the outflow plane carries a different
+    flux than the inflow once the flow passes the bump, graddin's all-Neumann system is
+    inconsistent and its CG reports convergence on a recurrence residual that has left the true
+    one (a second solve from the result takes as many iterations again).  outflow_fix = 1 makes
+    the system consistent."""
     p = default_params()
     p.nx, p.ny, p.nz = nx, ny, nz
     p.dx = p.dy = p.dz = dx
@@ -252,6 +258,7 @@ def bump_channel(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-10, u_init=0.1):
     _two_phase(p, cs=0.1)
     p.cg_tol = cg_tol
     p.obst_t = 3
+    p.outflow_fix = outflow_fix
     p.dt = 0.2 * dx / (u_init + math.sqrt(9.81 * 0.6 * nz * dx))
     Lx, Ly, H = nx * dx, ny * dx, nz * dx
 
@@ -269,7 +276,7 @@ def bump_channel(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-10, u_init=0.1):
     return p, init, masks
 
 
-def les_channel(nx=512, ny=256, nz=256, cg_tol=1e-8, seed=0, x0=3.0):
+def les_channel(nx=512, ny=256, nz=256, cg_tol=1e-8, seed=0, x0=3.0, outflow_fix=1):
     """The LES channel over a bottom bump: 6 x 3 x 3 m (dx = dy = dz = 6/nx at the default
     size, 0.01171875), water 2 m deep, the obst_t = 3 Gaussian bump with height 0.3 m, no flat
     base (d = 0), sigma 0.5 m, centred at (x0, Ly/2); inflow u = 1 + 0.05 U(-1, 1) (seeded,
@@ -281,8 +288,8 @@ def les_channel(nx=512, ny=256, nz=256, cg_tol=1e-8, seed=0, x0=3.0):
     the net flux (9_grad.f90:96-116): with this fluctuating inflow and the boundary layer the
     outflow copy carries, the problem is inconsistent and its CG diverges within the first
     steps (in this library and in the CPU restatement of the tests alike), as it does for the
-    wave flume; a uniform flow
-    through the same faces stays exactly steady."""
+    wave flume; a uniform flow through the same faces stays exactly steady.  The case therefore
+    turns on outflow_fix (the outflow plane shifted to balance the inflow) unless told not to."""
     p = default_params()
     p.nx, p.ny, p.nz = nx, ny, nz
     p.dx, p.dy, p.dz = 6.0 / nx, 3.0 / ny, 3.0 / nz
@@ -292,6 +299,7 @@ def les_channel(nx=512, ny=256, nz=256, cg_tol=1e-8, seed=0, x0=3.0):
     _two_phase(p, cs=0.12)
     p.cg_tol = cg_tol
     p.obst_t = 3
+    p.outflow_fix = outflow_fix
     p.dt = 0.3 * min(p.dx, p.dy, p.dz) / (1.05 + math.sqrt(9.81 * 2.0))
     ly = ny * p.dy
 
@@ -318,12 +326,14 @@ def les_channel(nx=512, ny=256, nz=256, cg_tol=1e-8, seed=0, x0=3.0):
     return p, init, masks
 
 
-def wave_channel(wave_t=1, nx=32, ny=8, nz=12, dx=0.1, dz=0.1, cg_tol=1e-10):
+def wave_channel(wave_t=1, nx=32, ny=8, nz=12, dx=0.1, dz=0.1, cg_tol=1e-10, outflow_fix=0):
     """A wave flume for the wave inflow of boundary_waves (3_contorno.f90:952-1082): still water
     1 m deep (h0_f of waves_coef), the wave entering at x = 0 (ccx0 = 3), outflow at x = xf
     (ccxf = 4), periodic y, no-slip bottom, free-slip top; dt from CFL 0.2 with sqrt(g h).
-    With this inflow and outflow the reference's Poisson solve (all-Neumann, 9_grad.f90) stays
-    convergent on cubic cells; with dz = dx/2 it diverges after a step, with or without the wave."""
+    The wave's inflow flux varies in time and the outflow copy does not follow it, so with the
+    reference's outflow (outflow_fix = 0) the all-Neumann Poisson system (9_grad.f90) is
+    inconsistent: its CG stops on a recurrence residual that no longer matches the true one.
+    outflow_fix = 1 balances the flux and makes the solve well posed."""
     p = default_params()
     p.nx, p.ny, p.nz = nx, ny, nz
     p.dx = p.dy = dx
@@ -334,6 +344,7 @@ def wave_channel(wave_t=1, nx=32, ny=8, nz=12, dx=0.1, dz=0.1, cg_tol=1e-10):
     _two_phase(p, cs=0.1)
     p.cg_tol = cg_tol
     p.wave_t = wave_t
+    p.outflow_fix = outflow_fix
     p.dt = 0.2 * min(dx, dz) / math.sqrt(9.81 * 1.0)
     X, Y, Z = _centres(p)
     ls0 = 1.0 - Z

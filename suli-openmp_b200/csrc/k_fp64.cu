@@ -889,6 +889,45 @@ __global__ void k_bc_nz(Geo G, BC bc, BCArgs A) {
     if (bc.zf == 3) FIDX(w, i, j, nz1) = A.pl.bzzf[i + lv * j];
 }
 
+// outflow_fix = 1 (an extension, after contorno(2) with ccxf = 4): one block sums the net
+// volume flux through the boundary planes (the sum of graddin's right-hand side over the cells,
+// telescoped), then shifts the outflow faces u(nx+1, j, k) above the obstacle mask ku(nx+1, j)
+// by one uniform value so that the net flux vanishes.  Fixed-order tree sums (deterministic).
+constexpr int kFixThreads = 1024;
+__global__ void __launch_bounds__(kFixThreads) k_outflow_fix(Geo G, BCArgs A, const int* __restrict__ ku, double dx,
+                                                            double dy, double dz) {
+    __shared__ double s_delta;
+    const int nx = G.nx, ny = G.ny, nz = G.nz, tid = threadIdx.x;
+    double fx = 0., fy = 0., fz = 0., open = 0.;
+    for (int q = tid; q < ny * nz; q += kFixThreads) {
+        const int j = 1 + q % ny, k = 1 + q / ny;
+        fx += FIDX(A.u, nx + 1, j, k) - FIDX(A.u, 1, j, k);
+        open += (!ku || k > ku[(nx + 1) + (nx + 3) * j]) ? 1. : 0.;
+    }
+    for (int q = tid; q < nx * nz; q += kFixThreads) {
+        const int i = 1 + q % nx, k = 1 + q / nx;
+        fy += FIDX(A.v, i, ny + 1, k) - FIDX(A.v, i, 1, k);
+    }
+    for (int q = tid; q < nx * ny; q += kFixThreads) {
+        const int i = 1 + q % nx, j = 1 + q / nx;
+        fz += FIDX(A.w, i, j, nz + 1) - FIDX(A.w, i, j, 1);
+    }
+    fx = block_sum(fx);
+    fy = block_sum(fy);
+    fz = block_sum(fz);
+    open = block_sum(open);
+    if (tid == 0) {
+        const double net = fx * (dy * dz) + fy * (dx * dz) + fz * (dx * dy);
+        s_delta = (open > 0.) ? -net / (open * (dy * dz)) : 0.;
+    }
+    __syncthreads();
+    const double delta = s_delta;
+    for (int q = tid; q < ny * nz; q += kFixThreads) {
+        const int j = 1 + q % ny, k = 1 + q / ny;
+        if (!ku || k > ku[(nx + 1) + (nx + 3) * j]) FIDX(A.u, nx + 1, j, k) += delta;
+    }
+}
+
 // ------------------------------------------------------------------------------------
 // graddin (9_grad.f90:10-278)
 // ------------------------------------------------------------------------------------
@@ -1436,7 +1475,8 @@ void launch_contorno(suli_ctx* c, int nlock) {
     A.nlock = nlock;
     A.obst = obst ? 1 : 0;
     const bool capy = !obst && (c->bc.y0 == 2 || c->bc.yf == 2);
-    ProfScope ps(c, SULI_K_CONTORNO, (nlock == 2 ? 7 : 4) + (capy || obst ? 1 : 0));
+    ProfScope ps(c, SULI_K_CONTORNO, (nlock == 2 ? 7 + (c->P.outflow_fix == 1 && c->bc.xf == 4 ? 1 : 0) : 4) +
+                                         (capy || obst ? 1 : 0));
     k_prd_ghosts<<<grid3(G.nx + 2, G.ny + 2, G.nz + 2, kBlk), kBlk, 0, c->stream>>>(G, c->bc, A.prd1);
     k_bc_y<<<grid3(G.nx + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
     k_bc_x<<<grid3(G.ny + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
@@ -1450,6 +1490,9 @@ void launch_contorno(suli_ctx* c, int nlock) {
         k_bc_ny<<<grid3(G.nx + 2, G.nz + 2, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
         k_bc_nx<<<grid3(G.ny + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
         k_bc_nz<<<grid3(G.nx + 2, G.ny + 2, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
+        if (c->P.outflow_fix == 1 && c->bc.xf == 4)
+            k_outflow_fix<<<1, kFixThreads, 0, c->stream>>>(G, A, obst ? c->obst_ku : nullptr, c->P.dx, c->P.dy,
+                                                            c->P.dz);
     }
 }
 static CGConst cg_const(const suli_ctx* c) {

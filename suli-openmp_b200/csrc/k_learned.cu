@@ -2,7 +2,9 @@
 //
 // After graddin's set-up (scaled system A~ e = b~, first residual r~0 = A~ e0 - b~):
 //   features  in3[v] = (r~0/s, H, (e0 - mean e0)/s_e),  s = rms(r~0), s_e = rms(e0 - mean),
-//             H = (rho - rho_1)/(rho_2 - rho_1) (0 in phase 1, 1 in phase 2);
+//             H the smoothed Heaviside hs that heaviside() mixed rho from (0 in phase 1, 1 in
+//             phase 2), read as stored, so that the feature is the same for the linear
+//             (t_hs = 0) and the geometric (t_hs = 1) mix of rho (14_level_set.f90:696-703);
 //   step      y = network output, alpha = -(r~0 . y)/(y . A~ y), e <- e0 + alpha y (FP64);
 //   target    P(e* - e0)/s for training (e* the converged scaled solution), P removing the
 //             component along n = sqrt(d): A~ n = 0 for the all-Neumann pressure problem, so
@@ -53,22 +55,21 @@ __global__ void __launch_bounds__(256) k_nn_stats(Geo G, const double* __restric
 struct Feat3 {
     float r, h, e;
 };
-__device__ __forceinline__ Feat3 features_at(const double* r, const double* e, const double* rho, double rho1,
-                                             double rho2, const NNScale* sc, long long c) {
+__device__ __forceinline__ Feat3 features_at(const double* r, const double* e, const double* hs, const NNScale* sc,
+                                             long long c) {
     const double sr = sc->sigma_r, se = sc->sigma_e;
-    const double h = (rho2 != rho1) ? (rho[c] - rho1) / (rho2 - rho1) : 0.;
-    return Feat3{sc->active ? (float)(r[c] / sr) : 0.f, (float)h, se > 0. ? (float)((e[c] - sc->mean_e) / se) : 0.f};
+    return Feat3{sc->active ? (float)(r[c] / sr) : 0.f, (float)hs[c], se > 0. ? (float)((e[c] - sc->mean_e) / se) : 0.f};
 }
 // FP32 [V][3] (recorded training inputs, suli_nn_forward's input format)
 __global__ void __launch_bounds__(256) k_nn_features(Geo G, const double* __restrict__ r, const double* __restrict__ e,
-                                                     const double* __restrict__ rho, double rho1, double rho2,
-                                                     const NNScale* __restrict__ sc, float* __restrict__ in3) {
+                                                     const double* __restrict__ hs, const NNScale* __restrict__ sc,
+                                                     float* __restrict__ in3) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z + 1;
     if (i > G.nx || j > G.ny || k > G.nz) return;
     const long long v = cell_v(G, i, j, k);
-    const Feat3 f = features_at(r, e, rho, rho1, rho2, sc, G.idx(i, j, k));
+    const Feat3 f = features_at(r, e, hs, sc, G.idx(i, j, k));
     in3[3 * v + 0] = f.r;
     in3[3 * v + 1] = f.h;
     in3[3 * v + 2] = f.e;
@@ -76,15 +77,15 @@ __global__ void __launch_bounds__(256) k_nn_features(Geo G, const double* __rest
 // the network's own input layout, BF16 [V][16] with channels 3-15 zero: the same values the
 // network's packing of the FP32 features produces, written once
 __global__ void __launch_bounds__(256) k_nn_features16(Geo G, const double* __restrict__ r,
-                                                       const double* __restrict__ e, const double* __restrict__ rho,
-                                                       double rho1, double rho2, const NNScale* __restrict__ sc,
+                                                       const double* __restrict__ e, const double* __restrict__ hs,
+                                                       const NNScale* __restrict__ sc,
                                                        __nv_bfloat16* __restrict__ in16) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z + 1;
     if (i > G.nx || j > G.ny || k > G.nz) return;
     const long long v = cell_v(G, i, j, k);
-    const Feat3 f = features_at(r, e, rho, rho1, rho2, sc, G.idx(i, j, k));
+    const Feat3 f = features_at(r, e, hs, sc, G.idx(i, j, k));
     __nv_bfloat16 t[16];
     t[0] = __float2bfloat16(f.r);
     t[1] = __float2bfloat16(f.h);
@@ -173,15 +174,13 @@ inline dim3 grid_cells(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) 
 void launch_nn_features(suli_ctx* c, float* in3) {
     const Geo& G = c->g;
     k_nn_stats<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_e, c->cg, c->nn_scale, c->red_partial, c->red_counter);
-    k_nn_features<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_r, c->cg_e, c->f[SULI_F_RHO], c->P.rho_f1,
-                                                         c->P.rho_f2, c->nn_scale, in3);
+    k_nn_features<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_r, c->cg_e, c->f[SULI_F_HS], c->nn_scale, in3);
 }
 
 void launch_nn_features16(suli_ctx* c, void* in16) {
     const Geo& G = c->g;
     k_nn_stats<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_e, c->cg, c->nn_scale, c->red_partial, c->red_counter);
-    k_nn_features16<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_r, c->cg_e, c->f[SULI_F_RHO], c->P.rho_f1,
-                                                           c->P.rho_f2, c->nn_scale,
+    k_nn_features16<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_r, c->cg_e, c->f[SULI_F_HS], c->nn_scale,
                                                            static_cast<__nv_bfloat16*>(in16));
 }
 

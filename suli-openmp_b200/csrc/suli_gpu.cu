@@ -116,6 +116,8 @@ int validate(const suli_params* p, std::string& why) {
     if (p->wave_t != 0 && p->wave_t != 1 && p->wave_t != 2 && p->wave_t != 5) {
         why = "wave_t must be 0 (none), 1 (Stokes I), 2 (Stokes II) or 5 (Stokes V)"; return SULI_ERR_ARG;
     }
+    if (p->outflow_fix != 0 && p->outflow_fix != 1) { why = "outflow_fix must be 0 or 1"; return SULI_ERR_ARG; }
+    if (p->outflow_fix == 1 && p->ccxf != 4) { why = "outflow_fix = 1 corrects the outflow plane: it needs ccxf = 4"; return SULI_ERR_ARG; }
     if (p->t_hs != 0 && p->t_hs != 1) { why = "t_hs must be 0 (linear) or 1 (geometric) (14_level_set.f90:696-703)"; return SULI_ERR_ARG; }
     if (p->adv_type < 1 || p->adv_type > 3) { why = "adv_type must be 1 (classico), 2 (rotacional) or 3 (antissim)"; return SULI_ERR_ARG; }
     if (p->der < 1 || p->der > 3) { why = "der must be 1 (upwind), 2 (centred) or 3 (2nd-order upwind)"; return SULI_ERR_ARG; }

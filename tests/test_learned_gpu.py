@@ -1,6 +1,6 @@
 """GPU: the learned initial guess inside the mixed-precision pressure solve.
 
-* recorded training pairs: the density feature equals the downloaded density, the residual
+* recorded training pairs: the density feature equals the stored Heaviside, the residual
   feature has unit rms, and features and target are invariant to the scale of the RHS;
 * a network whose output is zero leaves the solve bit-for-bit unchanged (alpha = 0);
 * an untrained network still lets the solve reach the FP64 tolerance and the same pressure;
@@ -63,6 +63,33 @@ def test_record_features_and_scale_invariance(pkg, torch):
     assert np.allclose(t1, t2, rtol=1e-6, atol=1e-6 * np.abs(t1).max())
     assert np.abs(t1).max() > 0
     s.close()
+
+
+def test_density_feature_is_the_heaviside_for_both_mixes(pkg, torch):
+    """The density feature is H itself for the linear (t_hs = 0) and the geometric (t_hs = 1)
+    mix of rho (14_level_set.f90:696-703): the geometric rho is not linear in H, so H is read
+    from the stored Heaviside, not inverted from rho."""
+    for t_hs in (0, 1):
+        q = pkg.snapshots.tank_params(n=N, precision=1, cg_tol=TOL)
+        q.t_hs = t_hs
+        s = pkg.Solver(q)
+        gen = pkg.snapshots.SnapshotGenerator(s, 5)
+        ls, vel = gen.level_set(), gen.velocity()
+        _load(s, torch, ls, vel)
+        in3 = torch.empty(N ** 3 * 3, dtype=torch.float32, device="cuda:0")
+        t = torch.empty(N ** 3, dtype=torch.float32, device="cuda:0")
+        s.graddin_record(in3.data_ptr(), t.data_ptr())
+        f = in3.cpu().numpy().reshape(N, N, N, 3)
+        hs = np.transpose(s.download("hs"), (2, 1, 0))
+        assert np.array_equal(f[..., 1], hs.astype(np.float32)), t_hs
+        band = (hs > 0.05) & (hs < 0.95)
+        assert band.any()
+        lin = (np.transpose(s.download("rho"), (2, 1, 0)) - q.rho_f1) / (q.rho_f2 - q.rho_f1)
+        if t_hs == 1:   # the linear inverse of the geometric mix is far from H in the band
+            assert np.abs(lin - hs)[band].max() > 0.1
+        else:
+            assert np.abs(lin - hs).max() < 1e-12
+        s.close()
 
 
 def _solve(s, torch, ls, vel, net=None):

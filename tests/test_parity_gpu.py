@@ -288,6 +288,33 @@ def test_step_parity_dam_break(pkg, orc):
     assert sg["max_div"] <= 1e-8
 
 
+def test_step_parity_c1_dam_break(pkg, orc):
+    """The dam break at its own size, 64 x 32 x 48 cells of 0.01 m (RK3, Smagorinsky 0.1,
+    no-slip walls, free-slip top, 1_principal.f90:64-108): ten whole steps, every state field
+    within 1e-10 relative and the Poisson iteration counts within 3.  Both sides solve to a
+    relative residual of 1e-12 (tighter than the run's 1e-10) so that the comparison measures
+    the arithmetic, not where two converging CGs happen to stop."""
+    p, init = pkg.cases.dam_break(cg_tol=1e-12)
+    assert (p.nx, p.ny, p.nz, p.dx) == (64, 32, 48, 0.01)
+    g = pkg.Solver(p)
+    o = orc.Oracle(p)
+    init(g)
+    init(o)
+    for it in range(1, 11):
+        sg, so = g.step(it), o.step(it)
+        assert sg["status"] == 0 and so["status"] == 0
+        assert max(abs(a - b) for a, b in zip(sg["cg_iters"], so["cg_iters"])) <= 3, (it, sg, so)
+    worst = {}
+    for f in ("u", "v", "w", "ls", "rho", "hs", "kurv", "nut", "xnut", "ynut", "znut"):
+        worst[f] = rel_err(g.download(f), o.download(f))
+    pg, po = g.download("prd1"), o.download("prd1")
+    worst["prd1(mean-free)"] = rel_err(pg - pg.mean(), po - po.mean())
+    assert max(worst.values()) <= 1e-10, worst
+    assert sg["max_div"] <= 1e-8
+    assert sg["vol_ins"] == pytest.approx(so["vol_ins"], rel=1e-12)
+    g.close()
+
+
 @pytest.mark.parametrize("der, adv", [(2, 1), (3, 1), (1, 2), (1, 3)])
 def test_step_parity_schemes(pkg, orc, der, adv):
     """Five whole dam-break steps with the centred or second-order upwind classico, the

@@ -117,11 +117,15 @@ def test_boundary_waves_gpu(orc, wave_t):
 
 
 @pytest.mark.gpu
-def test_step_parity_waves(orc):
+@pytest.mark.parametrize("wave_t", [1, 2, 5])
+def test_step_parity_waves(orc, wave_t):
     """One step of the wave flume (three stages, each with boundary_waves): velocities within
     1e-6 of the velocity scale, other fields within 1e-6 of their scale (the level set passes
-    through single precision at every stage)."""
-    p, init = cases.wave_channel(wave_t=1, cg_tol=1e-12)
+    through single precision at every stage).  The wave's inflow flux is not matched by the
+    reference's outflow copy, which leaves graddin's all-Neumann system inconsistent and its
+    CG iterates at the mercy of rounding; outflow_fix = 1 balances the flux so that the two
+    solves converge to the same field."""
+    p, init = cases.wave_channel(wave_t=wave_t, cg_tol=1e-12, outflow_fix=1)
     g = pkg.Solver(p)
     o = orc.Oracle(p)
     init(g)
