@@ -3,8 +3,9 @@
 
 Workload (one "step" = one time step of 1_principal.f90:64-108 plus est()): the sloshing
 tank at 256 x 128 x 128 cells (dx = 0.005 m, water/air 1000/1.2, Smagorinsky Cs = 0.1, RK3,
-fixed dt from CFL 0.25), Poisson solves to a relative FP64 residual of 1e-8.  Seeded
-synthetic initial state; the fields (~2.6 GB) exceed the 126 MB L2, so no flush is needed.
+fixed dt from CFL 0.25), every Poisson solve stopped by two tests on every path: relative FP64
+residual <= 1e-8 and max |div u| after the projection <= 1e-8 (div_tol).  Seeded synthetic
+initial state; the fields (~2.6 GB) exceed the 126 MB L2, so no flush is needed.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -13,7 +14,7 @@ max over ranks); `e2e` times the same steps through the C-ABI with the state cop
 to pinned host memory every step.  Multi-GPU runs are independent replicas (the path is one
 domain on one GPU), so `value` sums the replicas' time steps over the slowest replica's time.
 The reference arm (--impl reference) times the CPU restatement of the same path (OpenMP, all
-host cores) on a bounded sample of the same workload.
+host cores): a bounded number of real, whole steps of the same workload (no iteration cap).
 """
 from __future__ import annotations
 
@@ -58,6 +59,8 @@ def parse_args():
     ap.add_argument("--nz", type=int, default=128)
     ap.add_argument("--dx", type=float, default=0.005)
     ap.add_argument("--cg-tol", type=float, default=1e-8)
+    ap.add_argument("--div-tol", type=float, default=1e-8,
+                    help="second stopping test of every Poisson solve: max |div u| after the projection")
     ap.add_argument("--inner-tol", type=float, default=1e-4, help="relative tolerance of each FP32 inner solve")
     ap.add_argument("--mg-omega", type=float, default=0.9, help="damping of the multigrid Jacobi sweeps")
     ap.add_argument("--mg-alpha", type=float, default=1.8, help="scale of the multigrid coarse-grid correction")
@@ -68,9 +71,13 @@ def parse_args():
     ap.add_argument("--mms-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--cpu-cap", type=int, default=20, help="CG iterations per solve in the CPU sample")
-    ap.add_argument("--cpu-serial-cap", type=int, default=5,
-                    help="CG iterations per solve in the one-thread CPU sample (0: skip it)")
+    ap.add_argument("--cpu-steps", type=int, default=3, help="whole steps timed on the host cores (after one warm-up step)")
+    ap.add_argument("--cpu-serial-steps", type=int, default=1,
+                    help="whole steps timed on one thread, as the reference runs (0: skip)")
+    ap.add_argument("--long-steps", type=int, default=500,
+                    help="steps of the long-window block (C3's 500; 0: skip)")
+    ap.add_argument("--long-paths", default="learned,plain",
+                    help="paths timed over the long window (comma list of plain, mixed, learned)")
     return ap.parse_args()
 
 
@@ -197,53 +204,45 @@ def profiled_traffic(kernel: str, ncell: int):
     return vals["dram_bytes_per_launch"] * scale
 
 
-# ------------------------------------------------------------------------------ CPU sample
-def cpu_sample(pkg, p, init, cap: int, full_iters: float | None, openmp: bool = True):
-    """Time one step of the CPU restatement on the host cores (OpenMP build), or on one
-    thread (serial build, like the reference's own single-threaded program).
-
-    Sample: one full step of everything but the Poisson iterations, with each of the three
-    Poisson solves capped at `cap` iterations, plus two more capped solves to separate the
-    per-iteration cost from the per-solve setup.  The step time is scaled to the full
-    iteration count `full_iters` (the iterations a step of this workload performs)."""
+# ------------------------------------------------------------------------------ CPU steps
+def cpu_steps(pkg, p, init, timed: int, openmp: bool = True, warm: int = 1):
+    """Whole time steps of the CPU restatement (oracle/, FP64): the OpenMP build on every host
+    core it may use, or the serial build on one thread (as the reference's own program runs).
+    `warm` untimed steps from the initial state, then `timed` steps, each timed by the wall
+    clock; every Poisson solve runs to the same two stopping tests as the GPU paths."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
 
-    q = p.copy()
-    q.cg_maxit = cap
-    o = oracle.Oracle(q, openmp=openmp)
+    t_init = time.perf_counter()
+    o = oracle.Oracle(p, openmp=openmp)
     init(o)
-    t0 = time.perf_counter()
-    t_cg = 0.0
-    o.level_set()
-    for tt in range(1, o.ntt + 1):
-        o.set_dt(o.a_dt[tt - 1])
-        o.visco(); o.convdiff(); o.tempo(tt, 1); o.contorno(2)
-        t1 = time.perf_counter()
-        o.graddin()
-        t_cg += time.perf_counter() - t1
-        o.posdin(); o.contorno(1)
-    o.est()
-    t_step_capped = time.perf_counter() - t0
-    t_noncg = t_step_capped - t_cg
-    # per-iteration cost from a cap and a 2*cap solve on the same state
-    o.contorno(2)
-    t1 = time.perf_counter(); o.graddin(); ta = time.perf_counter() - t1
-    q2 = q.copy(); q2.cg_maxit = 2 * cap
-    o2 = oracle.Oracle(q2, openmp=openmp)
-    for name in ("u", "v", "w", "prd1", "rho", "ls"):
-        o2.upload(name, o.download(name))
-    o2.set_dt(o.a_dt[0]); o2.contorno(2)
-    t1 = time.perf_counter(); o2.graddin(); tb = time.perf_counter() - t1
-    t_iter = max((tb - ta) / cap, 1e-9)
-    t_setup = max(ta - cap * t_iter, 0.0)
-    iters = full_iters if full_iters is not None else 3 * cap
-    t_step = t_noncg + 3 * t_setup + iters * t_iter
-    cores = oracle.num_threads(openmp)
-    return {
-        "t_step_s": t_step, "t_noncg_s": t_noncg, "t_iter_s": t_iter, "t_setup_s": t_setup,
-        "iters_per_step": iters, "cores": cores, "sample_wall_s": t_step_capped + ta + tb,
-    }
+    t_init = time.perf_counter() - t_init
+    it = 0
+    for _ in range(warm):
+        it += 1
+        o.step(it)
+    times, iters, divs, res = [], [], [], []
+    for _ in range(timed):
+        it += 1
+        t0 = time.perf_counter()
+        st = o.step(it)
+        times.append(time.perf_counter() - t0)
+        iters.append(sum(st["cg_iters"]))
+        divs.append(st["max_div"])
+        res.append(max(st["cg_resid"]))
+    o.close()
+    return {"t_step_s_median": statistics.median(times), "t_step_s": times, "steps_timed": list(range(it - timed + 1, it + 1)),
+            "poisson_iters_per_step": iters, "max_div": max(divs), "cg_resid_max": max(res),
+            "cores": oracle.num_threads(openmp), "init_s": t_init}
+
+
+def cpu_desc(cs, openmp):
+    who = "OpenMP build of the FP64 CPU restatement on every host core" if openmp else \
+        "serial build of the FP64 CPU restatement on one thread (as the reference runs)"
+    return (f"{who}: median of {len(cs['t_step_s'])} whole steps (steps {cs['steps_timed'][0]}-"
+            f"{cs['steps_timed'][-1]} from the seeded state, after {cs['steps_timed'][0] - 1} untimed), "
+            f"Poisson solves to the same two stopping tests, no iteration cap "
+            f"({statistics.mean(cs['poisson_iters_per_step']):.0f} CG iterations per step)")
 
 
 # ------------------------------------------------------------------------------ arms
@@ -257,36 +256,26 @@ def run_reference(args):
         # library loads, below)
         os.environ["OMP_NUM_THREADS"] = str(len(os.sched_getaffinity(0)))
     pkg = load_pkg()
-    p, init = pkg.cases.sloshing(nx=args.nx, ny=args.ny, nz=args.nz, dx=args.dx, cg_tol=args.cg_tol)
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle
-
-    # the iterations one step needs, from one full CPU step (first warm-up step)
-    o = oracle.Oracle(p, openmp=True)
-    init(o)
-    st = o.step(1)
-    full_iters = float(sum(st["cg_iters"]))
-    del o
-    samples = []
-    for w in range(max(args.warmup - 1, 0)):
-        cpu_sample(pkg, p, init, args.cpu_cap, full_iters)
-    for k in range(args.steps):
-        samples.append(cpu_sample(pkg, p, init, args.cpu_cap, full_iters))
-    t = sum(s["t_step_s"] for s in samples)
-    value = args.steps / t
-    cores = samples[0]["cores"]
-    sample_desc = (f"per step: level set + 3 RK stages of visco/convdiff/tempo/contorno/posdin at full size, "
-                   f"Poisson solves capped at {args.cpu_cap} iterations and scaled to the {full_iters:.0f} "
-                   f"iterations a full CPU step took (FP64, OpenMP restatement)")
+    p, init = pkg.cases.sloshing(nx=args.nx, ny=args.ny, nz=args.nz, dx=args.dx, cg_tol=args.cg_tol,
+                                 div_tol=args.div_tol)
+    # a bounded sample: --steps whole steps would take minutes each on the host cores
+    timed = max(1, min(args.steps, args.cpu_steps))
+    t0 = time.perf_counter()
+    cs = cpu_steps(pkg, p, init, timed, openmp=True)
+    wall = time.perf_counter() - t0
+    t = sum(cs["t_step_s"])
+    value = timed / t
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "impl": "reference",
-        "config": workload_config(p, args, "cpu-openmp-fp64"),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample_desc},
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": timed,
+        "steps_requested": args.steps, "warmup": 1, "ms_per_step": 1e3 * t / timed, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cs["cores"], "kind": "port",
+                         "sample": cpu_desc(cs, True)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "gpu_launches": 0,
+        "gpu_launches": 0, "max_div": cs["max_div"], "cg_resid_max": cs["cg_resid_max"],
+        "poisson_iters_per_step": cs["poisson_iters_per_step"], "t_step_s": cs["t_step_s"],
+        "wall_s_incl_init": wall,
+        "config": workload_config(p, args, "cpu-openmp-fp64"),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -294,8 +283,9 @@ def run_reference(args):
 
 def workload_config(p, args, path):
     return {
-        "workload": f"sloshing tank {p.nx}x{p.ny}x{p.nz} dx={p.dx} RK3 Smagorinsky, Poisson rel. residual {p.cg_tol:g}",
-        "nx": p.nx, "ny": p.ny, "nz": p.nz, "dt": p.dt, "cg_tol": p.cg_tol, "path": path,
+        "workload": (f"sloshing tank {p.nx}x{p.ny}x{p.nz} dx={p.dx} RK3 Smagorinsky, Poisson rel. residual "
+                     f"{p.cg_tol:g} and max|div u| {p.div_tol:g}"),
+        "nx": p.nx, "ny": p.ny, "nz": p.nz, "dt": p.dt, "cg_tol": p.cg_tol, "div_tol": p.div_tol, "path": path,
         "l2": "state of ~2.6 GB per replica exceeds the 126 MB L2; no flush",
         "parallelism": f"replicas{args.gpus}",
     }
@@ -501,6 +491,63 @@ def mms_check(pkg, args, dev):
     return out
 
 
+STATE = ("u", "v", "w", "ls", "prd1")
+
+
+def state_of(s):
+    """The fields compared between paths: velocities, level set and the mean-free pressure."""
+    out = {f: s.download(f) for f in STATE if f != "prd1"}
+    pr = s.download("prd1")[1:-1, 1:-1, 1:-1]
+    out["prd1"] = pr - pr.mean()
+    return out
+
+
+def field_errors(a, ref):
+    """Max |a - ref| per field: the velocity components over the velocity scale (the largest
+    |u|, |v|, |w| of the reference state), the level set and the pressure over their own."""
+    import numpy as np
+    vs = max(float(np.abs(ref[f]).max()) for f in ("u", "v", "w"))
+    e = {f: float(np.abs(a[f] - ref[f]).max()) / vs for f in ("u", "v", "w")}
+    for f in ("ls", "prd1"):
+        e[f] = float(np.abs(a[f] - ref[f]).max()) / max(float(np.abs(ref[f]).max()), 1e-300)
+    return e
+
+
+def long_window(args, dist, pkg, p, init, dev, net=None):
+    """A fresh run of `--long-steps` steps from the seeded state, timed as one CUDA-event window:
+    steps/s, Poisson iterations per step in blocks of 50 steps, the worst max|div u| and residual,
+    and the clocks sampled over the window."""
+    import torch
+    s = pkg.Solver(p, device=dev)
+    init(s)
+    if net is not None:
+        s.attach_nn(net)
+    ext = torch.cuda.ExternalStream(s.stream_ptr, device=dev)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    iters, divs, res = [], [], []
+    for it in range(1, args.long_steps + 1):
+        st = s.step(it)
+        iters.append(sum(st["cg_iters"]))
+        divs.append(st["max_div"])
+        res.append(max(st["cg_resid"]))
+    e1.record(ext)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = dist.max(e0.elapsed_time(e1))
+    vol0, vol1 = s.get_scalar("vol_ini"), s.get_scalar("vol_ins")
+    s.close()
+    blk = 50
+    return {"steps": args.long_steps, "value": dist.world * args.long_steps / (ms / 1e3), "ms_per_step": ms / args.long_steps,
+            "poisson_iters_per_step_by_50": [round(statistics.mean(iters[q:q + blk]), 1) for q in range(0, len(iters), blk)],
+            "max_div": max(divs), "cg_resid_max": max(res), "volume_drift": (vol1 - vol0) / vol0,
+            "clocks": {k: clk.get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons", "samples")}}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -509,7 +556,8 @@ def run_ours(args):
     dev = dist.local
     torch.cuda.set_device(dev)
     pkg = load_pkg()
-    p, init = pkg.cases.sloshing(nx=args.nx, ny=args.ny, nz=args.nz, dx=args.dx, cg_tol=args.cg_tol)
+    p, init = pkg.cases.sloshing(nx=args.nx, ny=args.ny, nz=args.nz, dx=args.dx, cg_tol=args.cg_tol,
+                                 div_tol=args.div_tol)
     q = mixed_params(p, args)
     runs = {}
     # plain FP64 path (the reference's Jacobi-scaled CG): the comparison
@@ -528,6 +576,11 @@ def run_ours(args):
             raise SystemExit(f"--path learned: {net_src}")
     head_key = "learned" if "learned" in runs else ("mixed" if "mixed" in runs else "plain")
     head = runs[head_key]
+    # every path ran the same warm-up + timed steps from the same state: per-field error of the
+    # mixed-precision paths against the plain FP64 run
+    states = {k: state_of(r["solver"]) for k, r in runs.items()}
+    errors = {k: field_errors(states[k], states["plain"]) for k in runs if k != "plain" and "plain" in states}
+    del states
     for k, r in runs.items():
         if k != head_key:
             r["solver"].close()
@@ -570,68 +623,84 @@ def run_ours(args):
         e2e = {"value": dist.world * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": h2d, "fields": names, "path": head_key}
     s.close()
+    # ---- the long window (C3's 500 steps) of the headline and the plain path
+    long = {}
+    if args.long_steps > 0:
+        for k in [x.strip() for x in args.long_paths.split(",") if x.strip()]:
+            if k == "plain":
+                long[k] = long_window(args, dist, pkg, p, init, dev)
+            elif k == "mixed":
+                long[k] = long_window(args, dist, pkg, q, init, dev)
+            elif k == "learned" and net is not None:
+                long[k] = long_window(args, dist, pkg, q, init, dev, net=net)
+        if "plain" in long:
+            for k in long:
+                if k != "plain":
+                    long[k]["speedup_vs_plain_fp64"] = long[k]["value"] / long["plain"]["value"]
     if net is not None:
         net.close()
-    # ---- CPU baseline (rank 0, N = 1 only)
+    # ---- CPU baseline (rank 0, N = 1 only): whole steps, no cap
     cpu = None
-    ref_iters = runs["plain"]["iters_per_step"] if "plain" in runs else head["iters_per_step"]
     if dist.world == 1 and not args.no_cpu_baseline:
-        cs = cpu_sample(pkg, p, init, args.cpu_cap, ref_iters)
-        cpu = {"value": 1.0 / cs["t_step_s"], "unit": UNIT, "cores": cs["cores"], "kind": "port",
-               "sample": (f"one step of the OpenMP FP64 restatement at full size with Poisson solves capped at "
-                          f"{args.cpu_cap} iterations, scaled to the {ref_iters:.0f} iterations per step the GPU "
-                          f"measured: non-Poisson {cs['t_noncg_s']:.2f} s + {cs['t_iter_s'] * 1e3:.2f} ms/iteration"),
-               "detail": cs}
-        if args.cpu_serial_cap > 0:
-            ss = cpu_sample(pkg, p, init, args.cpu_serial_cap, ref_iters, openmp=False)
-            cpu["one_thread"] = {
-                "value": 1.0 / ss["t_step_s"], "unit": UNIT, "cores": ss["cores"], "kind": "port",
-                "sample": (f"the same step on one thread (serial build, as the reference runs), Poisson solves "
-                           f"capped at {args.cpu_serial_cap} iterations and scaled to {ref_iters:.0f}: non-Poisson "
-                           f"{ss['t_noncg_s']:.2f} s + {ss['t_iter_s'] * 1e3:.2f} ms/iteration"),
-                "detail": ss}
+        cs = cpu_steps(pkg, p, init, args.cpu_steps, openmp=True)
+        cpu = {"value": 1.0 / cs["t_step_s_median"], "unit": UNIT, "cores": cs["cores"], "kind": "port",
+               "sample": cpu_desc(cs, True), "t_step_s": cs["t_step_s"],
+               "poisson_iters_per_step": cs["poisson_iters_per_step"], "max_div": cs["max_div"]}
+        if args.cpu_serial_steps > 0:
+            ss = cpu_steps(pkg, p, init, args.cpu_serial_steps, openmp=False)
+            cpu["one_thread"] = {"value": 1.0 / ss["t_step_s_median"], "unit": UNIT, "cores": ss["cores"],
+                                 "kind": "port", "sample": cpu_desc(ss, False), "t_step_s": ss["t_step_s"]}
     mms = None
     if dist.world == 1 and args.mms_n > 0:
         mms = mms_check(pkg, args, dev)
     if dist.rank == 0:
         desc = {"plain": "plain FP64: the reference's Jacobi-scaled CG",
-                "mixed": "mixed: FP64 stencils, FP32 multigrid-preconditioned inner CG inside FP64 iterative "
-                         "refinement to the same FP64 relative residual",
+                "mixed": "mixed: FP32 stencils, FP32 multigrid-preconditioned inner CG inside FP64 iterative "
+                         "refinement to the same FP64 stopping tests",
                 "learned": "learned + mixed: the U-Net's guess (energy-optimal FP64 step) starts every pressure "
-                           "solve of the mixed path, which then runs to the same FP64 relative residual"}
+                           "solve of the mixed path, which then runs to the same FP64 stopping tests"}
         cfg = workload_config(q if head_key != "plain" else p, args, desc[head_key])
         cfg["inner_tol"] = args.inner_tol
         cfg["mg_omega"], cfg["mg_alpha"] = args.mg_omega, args.mg_alpha
         if net_src:
             cfg["weights"] = net_src
+        arm_acc = {k: {"max_div": max(st["max_div"] for st in r["stats"]),
+                       "cg_resid_max": max(max(st["cg_resid"]) for st in r["stats"])} for k, r in runs.items()}
+        ok = all(a["max_div"] <= args.div_tol and a["cg_resid_max"] <= args.cg_tol for a in arm_acc.values())
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64+f32+bf16" if head_key == "learned" else "f64+f32", "data": "synthetic",
+            "accuracy_ok": ok,
+            "accuracy": {"bound": {"cg_resid": args.cg_tol, "max_div": args.div_tol}, **arm_acc},
+            "error_vs_plain_fp64": errors,
+            "e2e": e2e, "gpu_launches": head["launches"],
+            "cpu_baseline": cpu,
+            "roofline": roofline,
+            "clocks": clk,
+            "poisson_iters_per_step": head["iters_per_step"],
             "config": cfg,
-            "roofline": roofline, "roofline_classes": roof_head, "roofline_plain_fp64": roof_plain,
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["launches"],
-            "clocks": clk, "poisson_iters_per_step": head["iters_per_step"],
-            "max_div": max(st["max_div"] for st in stats),
-            "cg_resid_max": max(max(st["cg_resid"]) for st in stats), "kernels": head["kernels"],
         }
         for k, r in runs.items():
             if k == head_key:
                 continue
             line[{"plain": "plain_fp64", "mixed": "mixed_no_net", "learned": "learned"}[k]] = {
                 "value": r["value"], "ms_per_step": r["ms"] / args.steps,
-                "poisson_iters_per_step": r["iters_per_step"], "max_div": max(st["max_div"] for st in r["stats"]),
-                "cg_resid_max": max(max(st["cg_resid"]) for st in r["stats"]), "clocks": r["clocks"],
-                "gpu_launches": r["launches"],
-                "kernels": r["kernels"]}
+                "poisson_iters_per_step": r["iters_per_step"], "gpu_launches": r["launches"],
+                "clocks": {kk: r["clocks"].get(kk) for kk in ("sm_mhz", "sm_max_mhz", "reasons")}}
         if "plain" in runs and head_key != "plain":
             line["speedup_vs_plain_fp64"] = value / runs["plain"]["value"]
         if "mixed" in runs and head_key == "learned":
             line["learned_vs_mixed"] = {"speedup": value / runs["mixed"]["value"],
                                         "poisson_iters_saved_per_step":
                                             runs["mixed"]["iters_per_step"] - head["iters_per_step"]}
+        if long:
+            line["long_window"] = long
+        line["roofline_classes"] = roof_head
+        line["roofline_plain_fp64"] = roof_plain
         if mms is not None:
             line["mms"] = mms
+        line["kernels"] = {k: {kk: round(vv, 4) for kk, vv in v.items()} for k, v in head["kernels"].items()}
         line["config"]["path"] = head_key
         print(json.dumps(line), flush=True)
     dist.close()

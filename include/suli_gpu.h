@@ -98,7 +98,12 @@ typedef struct suli_params {
                                        outflow plane u(nx+1,:,:) above the obstacle mask by one uniform
                                        value so that the net boundary flux is zero and graddin's
                                        all-Neumann system (9_grad.f90:96-116) is consistent */
-    int    reserved[1];
+    int    reserved;
+    double div_tol;                 /* 0 = off (the reference); > 0 (extension): the Poisson solve also
+                                       requires max |sqrt(d) r~| <= div_tol, the largest |div u| the
+                                       projection leaves (the unscaled residual), and iterates on
+                                       (FP64 CG: threshold lowered and the loop resumed; precision 1:
+                                       another refinement pass) until both tests hold or the cap */
 } suli_params;
 
 /* ---- field identifiers (module arrays of 0_modules.f90) ------------------------------ */

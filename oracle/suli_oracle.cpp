@@ -98,6 +98,7 @@ struct Oracle {
     /* statistics of the last calls */
     int last_cg_iters = 0;
     double last_cg_resid = 0.0;
+    double last_cg_rmax = 0.0;
     int last_reinit_iters = 0;
     int last_volfix_iters = 0;
 
@@ -1530,11 +1531,15 @@ int Oracle::graddin() {
     p.a = r.a;
     int cont = 0;
     double rr = alfamupr;
-    const double thr = (P.cg_stop == 0) ? P.cg_tol / N : P.cg_tol * P.cg_tol * bb;
+    double thr = (P.cg_stop == 0) ? P.cg_tol / N : P.cg_tol * P.cg_tol * bb;
     auto keep_going = [&]() {
         if (cont >= P.cg_maxit) return false;
         return (P.cg_stop == 0) ? (std::fabs(alfamupr) > thr) : (rr > thr);
     };
+    /* div_tol > 0 (an extension): once the residual test holds, max |sqrt(d) r~| (the largest
+       |div u| posdin leaves) must be within div_tol too; otherwise the threshold is lowered by
+       (div_tol/max)^2 / 2, at least 4x, and the iterations resume. */
+    for (;;) {
     while (keep_going()) {
         cont = cont + 1;
         double amu = 0., adi = 0., bmu = 0.;
@@ -1565,6 +1570,14 @@ int Oracle::graddin() {
         ghosts(e);
         ghosts(p);
         rr = bmu;
+    }
+    if (!(P.div_tol > 0.) || cont >= P.cg_maxit) break;
+    double m = 0.;
+    for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i)
+        m = std::max(m, std::fabs(std::sqrt(d(i, j, k)) * r(i, j, k)));
+    last_cg_rmax = m;
+    if (!(m > P.div_tol)) break;
+    thr = thr * std::min(0.25, 0.5 * (P.div_tol / m) * (P.div_tol / m));
     }
     /* de-normalisation over the whole halo box (:268-274) */
     for (int k = 0; k <= nz + 1; ++k) for (int j = 0; j <= ny + 1; ++j) for (int i = 0; i <= nx + 1; ++i)

@@ -46,7 +46,8 @@ class SuliParams(C.Structure):
         ("mg_kernels", C.c_int),
         ("wave_t", C.c_int),
         ("outflow_fix", C.c_int),
-        ("reserved", C.c_int * 1),
+        ("reserved", C.c_int),
+        ("div_tol", C.c_double),
     ]
 
     def copy(self) -> "SuliParams":

@@ -78,12 +78,13 @@ def dam_break(nx=64, ny=32, nz=48, dx=0.01, cg_tol=1e-10):
     return p, init
 
 
-def sloshing(nx=256, ny=128, nz=128, dx=0.005, cg_tol=1e-8, cfl=0.25, amp=0.02, depth=0.32):
+def sloshing(nx=256, ny=128, nz=128, dx=0.005, cg_tol=1e-8, cfl=0.25, amp=0.02, depth=0.32, div_tol=0.0):
     """Sloshing tank: free surface z = depth + amp cos(pi x/Lx) cos(pi y/Ly).
 
     L = (nx, ny, nz) * dx (1.28 x 0.64 x 0.64 m at the metric size), closed no-slip tank with
     a free-slip lid, Smagorinsky Cs = 0.1, RK3.  The time step follows CFL `cfl` with the
-    linear gravity-wave speed sqrt(g*depth) and stays fixed over the run.
+    linear gravity-wave speed sqrt(g*depth) and stays fixed over the run.  div_tol > 0 adds
+    the Poisson solve's divergence test (max |div u| after the projection within div_tol).
     """
     p = default_params()
     p.nx, p.ny, p.nz = nx, ny, nz
@@ -93,6 +94,7 @@ def sloshing(nx=256, ny=128, nz=128, dx=0.005, cg_tol=1e-8, cfl=0.25, amp=0.02, 
     p.ccz0, p.cczf = 2, 1
     _two_phase(p, cs=0.1)
     p.cg_tol = cg_tol
+    p.div_tol = div_tol
     p.dt = cfl * dx / math.sqrt(9.81 * depth)
     lx, ly = nx * dx, ny * dx
     depth = depth * (nz * dx / 0.64)

@@ -27,6 +27,8 @@ struct CGState {
     int mode;         // suli_params.cg_stop
     int status;       // 0 ok, SULI_WARN_CG_MAXIT, SULI_ERR_NAN
     int pad;
+    double div_tol;   // suli_params.div_tol (0: off)
+    double rmax;      // max |sqrt(d) r~| of the last check: the max |div u| projection leaves
 };
 
 // State of the FP32 inner preconditioned CG of the mixed-precision solve (device resident).
@@ -229,6 +231,7 @@ void launch_contorno(suli_ctx* c, int nlock);
 void launch_cg_setup(suli_ctx* c);
 void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new);
 void launch_cg_cond(suli_ctx* c, cudaGraphConditionalHandle h);
+void launch_cg_divcheck(suli_ctx* c);
 void launch_cg_final(suli_ctx* c, const double* e);
 // ---- mixed-precision solve (k_mixed.cu) ----
 void launch_mx_setup(suli_ctx* c);

@@ -935,6 +935,7 @@ struct CGConst {
     double cx, cy, cz;     // dt/(dx*dx) ...
     double dx, dy, dz;
     double tol;            // cg_tol
+    double div_tol;        // div_tol (0: off)
     double ncell;          // nx*ny*nz
     int mode, maxit;
 };
@@ -1051,6 +1052,8 @@ __global__ void __launch_bounds__(256, 4) k_cg_coef(Geo G, BC bc, CGConst K, con
         st->maxit = K.maxit;
         st->mode = K.mode;
         st->status = 0;
+        st->div_tol = K.div_tol;
+        st->rmax = 0.;
         const bool go = (fabs(trr) > st->thr) && (K.maxit > 0);
         st->done = go ? 0 : 1;
         if (!isfinite(trr)) { st->status = SULI_ERR_NAN; st->done = 1; }
@@ -1209,6 +1212,32 @@ __global__ void __launch_bounds__(kTX * kTY) k_cg_update(Geo G, double* __restri
         if (st->iters >= st->maxit) { go = false; st->status = SULI_WARN_CG_MAXIT; }
         if (!isfinite(trr)) { go = false; st->status = SULI_ERR_NAN; }
         st->done = go ? 0 : 1;
+    }
+}
+
+// Divergence test of a finished CG solve (div_tol > 0): max |sqrt(d) r~| over the cells is the
+// max |div u| that posdin leaves with this pressure (the unscaled residual of the face-flux
+// balance).  Above div_tol, the stopping threshold on r~.r~ is lowered by (div_tol/max)^2 / 2
+// (at least 4x) and the solve resumes; the host relaunches the iteration loop.
+__global__ void __launch_bounds__(256) k_cg_divcheck(Geo G, const double* __restrict__ sd,
+                                                     const double* __restrict__ r, CGState* st, double* partial,
+                                                     unsigned int* counter) {
+    if (!st->done || st->status != 0 || !(st->div_tol > 0.)) return;
+    const Thread3 t = tid3(1, 1, 1);
+    double m = 0.;
+    if (t.i <= G.nx && t.j <= G.ny && t.k <= G.nz) {
+        const long long c = G.idx(t.i, t.j, t.k);
+        m = fabs(sd[c] * r[c]);
+        if (isnan(m)) m = INFINITY;
+    }
+    double ta, tb, tm;
+    if (reduce3_last(0., 0., m, partial, counter, ta, tb, tm) && flat_tid() == 0) {
+        st->rmax = tm;
+        if (tm > st->div_tol && st->iters < st->maxit && isfinite(tm)) {
+            const double f = 0.5 * (st->div_tol / tm) * (st->div_tol / tm);
+            st->thr = st->thr * fmin(0.25, f);
+            st->done = 0;
+        }
     }
 }
 
@@ -1502,6 +1531,7 @@ static CGConst cg_const(const suli_ctx* c) {
     K.cz = c->dt / (c->P.dz * c->P.dz);
     K.dx = c->P.dx; K.dy = c->P.dy; K.dz = c->P.dz;
     K.tol = c->P.cg_tol;
+    K.div_tol = c->P.div_tol;
     K.ncell = (double)(c->P.nx * c->P.ny * c->P.nz);
     K.mode = c->P.cg_stop;
     K.maxit = c->P.cg_maxit;
@@ -1543,6 +1573,11 @@ void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new) {
                c->red_partial, c->red_counter);
 }
 void launch_cg_cond(suli_ctx* c, cudaGraphConditionalHandle h) { pdl_launch(k_cg_cond, 1, 1, c->stream, h, c->cg); }
+void launch_cg_divcheck(suli_ctx* c) {
+    const Geo& G = c->g;
+    ProfScope ps(c, SULI_K_CG_FINAL, 1);
+    k_cg_divcheck<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->cg_sd, c->cg_r, c->cg, c->red_partial, c->red_counter);
+}
 void launch_cg_final(suli_ctx* c, const double* e) {
     const Geo& G = c->g;
     ProfScope ps(c, SULI_K_CG_FINAL, 1);

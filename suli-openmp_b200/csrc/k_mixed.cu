@@ -484,6 +484,24 @@ __global__ void __launch_bounds__(256) k_pcg_updc(Geo G, float* __restrict__ x, 
 // FP64 refinement: e <- e - sqrt(d) dp, r~ = A~ e - b~, r_u = sqrt(d) r~ (FP32); sqrt(d) is the
 // set-up's stored value (sd)
 // ------------------------------------------------------------------------------------
+// Block partials of the refinement residual: r~.r~, r_u.r_u and max |r_u| (r_u = sqrt(d) r~ is the
+// divergence the projection would leave).  The last block sets the stopping test: r~.r~ within
+// the threshold and, with div_tol > 0, max |r_u| within div_tol.
+__device__ __forceinline__ void mx_outer_finish(double rr, double ru2, double um, int apply, CGState* cg,
+                                                PCGState* pst, double* partial, unsigned int* counter) {
+    if (isnan(um)) um = INFINITY;
+    double t1, t2, tm;
+    if (reduce3_last(rr, ru2, um, partial, counter, t1, t2, tm) && flat_tid() == 0) {
+        cg->rr = t1;
+        cg->rmax = tm;
+        if (apply) cg->iters = cg->iters + 1;
+        const bool div_ok = !(cg->div_tol > 0.) || tm <= cg->div_tol;
+        cg->done = (t1 > cg->thr || !div_ok) ? 0 : 1;
+        if (!isfinite(t1)) { cg->status = SULI_ERR_NAN; cg->done = 1; }
+        pst->rr0 = t2;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_mx_outer(Geo G, BC bc, const double* __restrict__ e_in,
                                                   const float* __restrict__ dp, const double* __restrict__ sd,
                                                   const double* __restrict__ ax, const double* __restrict__ ay,
@@ -493,7 +511,7 @@ __global__ void __launch_bounds__(256) k_mx_outer(Geo G, BC bc, const double* __
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z + 1;
-    double rr = 0., ru2 = 0.;
+    double rr = 0., ru2 = 0., um = 0.;
     if (i <= G.nx && j <= G.ny && k <= G.nz) {
         const int c = (int)G.idx(i, j, k);
         const Nb o = neighbours(G, bc, i, j, k);
@@ -506,15 +524,9 @@ __global__ void __launch_bounds__(256) k_mx_outer(Geo G, BC bc, const double* __
         ru[c] = (float)u;
         rr = rv * rv;
         ru2 = u * u;
+        um = fabs(u);
     }
-    double t1, t2;
-    if (reduce2_last(rr, ru2, partial, counter, t1, t2) && flat_tid() == 0) {
-        cg->rr = t1;
-        if (apply) cg->iters = cg->iters + 1;
-        cg->done = (t1 > cg->thr) ? 0 : 1;
-        if (!isfinite(t1)) { cg->status = SULI_ERR_NAN; cg->done = 1; }
-        pst->rr0 = t2;
-    }
+    mx_outer_finish(rr, ru2, um, apply, cg, pst, partial, counter);
 }
 
 // k_mx_outer with two x cells a thread (16-byte row loads; needs nx even): per cell the same
@@ -528,7 +540,7 @@ __global__ void __launch_bounds__(256) k_mx_outer2(Geo G, BC bc, const double* _
     const int i0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z + 1;
-    double rr = 0., ru2 = 0.;
+    double rr = 0., ru2 = 0., um = 0.;
     if (i0 <= G.nx && j <= G.ny && k <= G.nz) {
         const int c = (int)G.idx(i0, j, k), px = G.px, pxy = (int)G.pxy;
         const Nb o0 = neighbours(G, bc, i0, j, k), o1 = neighbours(G, bc, i0 + 1, j, k);
@@ -556,15 +568,9 @@ __global__ void __launch_bounds__(256) k_mx_outer2(Geo G, BC bc, const double* _
         *reinterpret_cast<float2*>(ru + c) = make_float2((float)u0, (float)u1);
         rr = r0 * r0 + r1 * r1;
         ru2 = u0 * u0 + u1 * u1;
+        um = fmax(fabs(u0), fabs(u1));
     }
-    double t1, t2;
-    if (reduce2_last(rr, ru2, partial, counter, t1, t2) && flat_tid() == 0) {
-        cg->rr = t1;
-        if (apply) cg->iters = cg->iters + 1;
-        cg->done = (t1 > cg->thr) ? 0 : 1;
-        if (!isfinite(t1)) { cg->status = SULI_ERR_NAN; cg->done = 1; }
-        pst->rr0 = t2;
-    }
+    mx_outer_finish(rr, ru2, um, apply, cg, pst, partial, counter);
 }
 
 __global__ void k_pcg_init(PCGState* st, double inner_tol, int maxit) {

@@ -98,4 +98,40 @@ static __device__ bool reduce2_last(double a, double b, double* partial, unsigne
     return true;
 }
 
+// Three block partials per block: a and b summed, m maxed; the last block to arrive folds all
+// partials in block order and returns true (totals valid in thread 0 of that block).
+static __device__ bool reduce3_last(double a, double b, double m, double* partial, unsigned int* counter, double& ta,
+                                    double& tb, double& tm) {
+    __shared__ bool last;
+    const int tid = flat_tid();
+    const int nt = blockDim.x * blockDim.y * blockDim.z;
+    const int bid = flat_bid();
+    const int nb = gridDim.x * gridDim.y * gridDim.z;
+    a = block_sum(a);
+    b = block_sum(b);
+    m = block_max(m);
+    if (tid == 0) {
+        partial[3 * bid] = a;
+        partial[3 * bid + 1] = b;
+        partial[3 * bid + 2] = m;
+        __threadfence();
+        const unsigned int t = atomicAdd(counter, 1u);
+        last = (t == (unsigned int)(nb - 1));
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double sa = 0.0, sb = 0.0, sm = 0.0;
+    for (int q = tid; q < nb; q += nt) {
+        sa += __ldcg(&partial[3 * q]);
+        sb += __ldcg(&partial[3 * q + 1]);
+        sm = fmax(sm, __ldcg(&partial[3 * q + 2]));
+    }
+    sa = block_sum(sa);
+    sb = block_sum(sb);
+    sm = block_max(sm);
+    if (tid == 0) { ta = sa; tb = sb; tm = sm; *counter = 0u; }
+    return true;
+}
+
 }  // namespace suli

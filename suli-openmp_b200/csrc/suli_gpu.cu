@@ -116,6 +116,7 @@ int validate(const suli_params* p, std::string& why) {
     if (p->wave_t != 0 && p->wave_t != 1 && p->wave_t != 2 && p->wave_t != 5) {
         why = "wave_t must be 0 (none), 1 (Stokes I), 2 (Stokes II) or 5 (Stokes V)"; return SULI_ERR_ARG;
     }
+    if (!(p->div_tol >= 0)) { why = "div_tol must be >= 0 (0: no divergence test)"; return SULI_ERR_ARG; }
     if (p->outflow_fix != 0 && p->outflow_fix != 1) { why = "outflow_fix must be 0 or 1"; return SULI_ERR_ARG; }
     if (p->outflow_fix == 1 && p->ccxf != 4) { why = "outflow_fix = 1 corrects the outflow plane: it needs ccxf = 4"; return SULI_ERR_ARG; }
     if (p->t_hs != 0 && p->t_hs != 1) { why = "t_hs must be 0 (linear) or 1 (geometric) (14_level_set.f90:696-703)"; return SULI_ERR_ARG; }
@@ -238,7 +239,7 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
         if ((e = cudaMemsetAsync(c->f[f], 0, n * sizeof(double), c->stream)) != cudaSuccess) return bail(e, "memset");
     }
     const long long nb = (long long)((p->nx + 1 + 31) / 32) * ((p->ny + 1 + 7) / 8) * (p->nz + 1) + 64;
-    if ((e = cudaMalloc(&c->red_partial, (size_t)nb * 2 * sizeof(double))) != cudaSuccess) return bail(e, "partial");
+    if ((e = cudaMalloc(&c->red_partial, (size_t)nb * 3 * sizeof(double))) != cudaSuccess) return bail(e, "partial");
     if ((e = cudaMalloc(&c->red_counter, 64 * sizeof(unsigned int))) != cudaSuccess) return bail(e, "counter");
     if ((e = cudaMemsetAsync(c->red_counter, 0, 64 * sizeof(unsigned int), c->stream)) != cudaSuccess) return bail(e, "memset");
     if ((e = cudaMalloc(&c->red_out, 16 * sizeof(double))) != cudaSuccess) return bail(e, "red_out");
@@ -802,6 +803,28 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
         CUDA_TRY(c, cudaGraphLaunch(c->cg_loop, c->stream));
     }
     CHECK_LAUNCH(c);
+    // div_tol > 0: resume the solve while the divergence the projection would leave is too large
+    for (int pass = 0; c->P.div_tol > 0. && pass < 64; ++pass) {
+        launch_cg_divcheck(c);
+        CHECK_LAUNCH(c);
+        int rr = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
+        if (rr != SULI_OK) return rr;
+        const CGState& s = c->cg_host[0];
+        if (s.done) break;
+        // after n iterations the last direction is in cg_pa for odd n, cg_pb for even n; the loop
+        // body starts from cg_pa
+        if (s.iters == 0) {
+            launch_cg_iter(c, c->cg_r, c->cg_pa);
+        } else if (s.iters % 2 == 0) {
+            CUDA_TRY(c, cudaMemcpyAsync(c->cg_pa, c->cg_pb, c->g.n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                        c->stream));
+        }
+        {
+            ProfScope ps(c, SULI_K_CG_SPMV, 0);
+            CUDA_TRY(c, cudaGraphLaunch(c->cg_loop, c->stream));
+        }
+        CHECK_LAUNCH(c);
+    }
     launch_cg_final(c, c->cg_e);
     if (c->rec_in) launch_nn_target(c, c->cg_e, c->rec_target);
     CHECK_LAUNCH(c);

@@ -70,14 +70,29 @@ def test_plain_roofline_from_tracer(bench, pkg):
 
 
 @pytest.mark.parametrize("openmp", [False, True])
-def test_cpu_sample_scaling(bench, pkg, openmp):
-    """The CPU baseline's step estimate: the capped step's non-Poisson time plus three solve
-    set-ups plus the measured iteration count times the per-iteration cost; the serial build
+def test_cpu_steps_are_whole_timed_steps(bench, pkg, openmp):
+    """The CPU baseline times whole steps: one untimed step, then the timed ones, every Poisson
+    solve to the same stopping tests as the GPU (both met), no iteration cap; the serial build
     runs on one thread."""
-    p, init = pkg.cases.sloshing(nx=16, ny=8, nz=8, dx=0.04, cg_tol=1e-8)
-    s = bench.cpu_sample(pkg, p, init, 3, 40.0, openmp=openmp)
-    assert s["t_noncg_s"] > 0 and s["t_iter_s"] > 0 and s["iters_per_step"] == 40.0
-    want = s["t_noncg_s"] + 3 * s["t_setup_s"] + 40.0 * s["t_iter_s"]
-    assert abs(s["t_step_s"] - want) <= 1e-12 * want
+    p, init = pkg.cases.sloshing(nx=16, ny=8, nz=8, dx=0.04, cg_tol=1e-8, div_tol=1e-8)
+    s = bench.cpu_steps(pkg, p, init, 2, openmp=openmp)
+    assert len(s["t_step_s"]) == 2 and all(t > 0 for t in s["t_step_s"])
+    assert s["steps_timed"] == [2, 3]
+    assert s["max_div"] <= 1e-8 and s["cg_resid_max"] <= 1e-8
+    assert all(n > 0 for n in s["poisson_iters_per_step"])
+    assert s["t_step_s_median"] == sorted(s["t_step_s"])[0] + (sorted(s["t_step_s"])[1] - sorted(s["t_step_s"])[0]) / 2
     if not openmp:
         assert s["cores"] == 1
+    assert "no iteration cap" in bench.cpu_desc(s, openmp)
+
+
+def test_field_errors(bench):
+    """Velocity errors over the velocity scale, level set and pressure over their own scale."""
+    import numpy as np
+    ref = {"u": np.array([2.0, -1.0]), "v": np.array([0.5, 0.0]), "w": np.array([0.1, 0.0]),
+           "ls": np.array([4.0, -4.0]), "prd1": np.array([10.0, -10.0])}
+    a = {k: v.copy() for k, v in ref.items()}
+    a["v"][1] += 1e-3
+    a["ls"][0] += 4e-3
+    e = bench.field_errors(a, ref)
+    assert e["u"] == 0.0 and abs(e["v"] - 5e-4) < 1e-15 and abs(e["ls"] - 1e-3) < 1e-15 and e["prd1"] == 0.0

@@ -125,6 +125,29 @@ def test_mixed_stencils_track_fp64(pkg, orc, der, adv, m_turb):
         assert rel_err(g.download(f), o.download(f)) <= 1e-5, f
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_divergence_stopping_test_gpu(pkg, orc, precision):
+    """div_tol = 1e-8 on the sloshing tank: the FP64 CG (precision 0, threshold lowered and the
+    device loop resumed) and the mixed solve (precision 1, more refinement passes) leave
+    max |div u| <= 1e-8 after every step, with the relative residual <= 1e-8; the FP64 path
+    stops where the oracle's does (iteration counts within 3 + 2 %)."""
+    p, init = pkg.cases.sloshing(nx=32, ny=16, nz=16, dx=0.04, cg_tol=1e-8, div_tol=1e-8)
+    q = p.copy()
+    if precision == 1:
+        q.precision, q.refine_maxit, q.inner_tol = 1, 30, 1e-4
+    g = pkg.Solver(q)
+    o = orc.Oracle(p)
+    init(g)
+    init(o)
+    for it in (1, 2, 3):
+        sg, so = g.step(it), o.step(it)
+        assert sg["status"] == 0 and so["status"] == 0
+        assert sg["max_div"] <= 1e-8 and max(sg["cg_resid"]) <= 1e-8, sg
+        if precision == 0:
+            assert all(abs(a - b) <= max(3, 0.02 * b) for a, b in zip(sg["cg_iters"], so["cg_iters"])), (sg, so)
+    g.close()
+
+
 def test_mixed_rejects_unsupported(pkg):
     p = small_params(nx=15, ny=13, nz=11)   # cannot halve to <= 1024 cells
     p.precision, p.cg_stop = 1, 1

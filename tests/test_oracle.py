@@ -11,7 +11,7 @@ import math
 import numpy as np
 import pytest
 
-from helpers import load_state, seeded_state, small_params
+from helpers import load_state, pkg, seeded_state, small_params
 
 
 # ---------------------------------------------------------------------- WENO pencil
@@ -633,3 +633,21 @@ def test_geometric_heaviside(orc):
     # the mix is geometric: at H = 1/2 rho is sqrt(rho1 rho2) + ... - 1, not the mean
     mid = np.abs(h - 0.5).argmin()
     assert abs(o.download("rho").ravel(order="F")[mid] - (p.rho_f1 + p.rho_f2) / 2) > 100
+
+
+def test_divergence_stopping_test(orc):
+    """div_tol: with the relative residual alone (1e-8) the sloshing tank keeps max |div u|
+    well above 1e-8 after each projection; with div_tol = 1e-8 the solve iterates on until the
+    largest unscaled residual (the divergence the projection leaves) is within it, and the
+    step's own max |div u| (est, 4_plot.f90:500-525) confirms it."""
+    out = {}
+    for dt in (0.0, 1e-8):
+        p, init = pkg.cases.sloshing(nx=32, ny=16, nz=16, dx=0.04, cg_tol=1e-8, div_tol=dt)
+        o = orc.Oracle(p)
+        init(o)
+        st = [o.step(it) for it in (1, 2)]
+        out[dt] = st
+        assert all(s["status"] == 0 and max(s["cg_resid"]) <= 1e-8 for s in st)
+    assert max(s["max_div"] for s in out[0.0]) > 1e-8
+    assert max(s["max_div"] for s in out[1e-8]) <= 1e-8
+    assert sum(map(sum, (s["cg_iters"] for s in out[1e-8]))) > sum(map(sum, (s["cg_iters"] for s in out[0.0])))
