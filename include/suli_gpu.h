@@ -98,7 +98,11 @@ typedef struct suli_params {
                                        outflow plane u(nx+1,:,:) above the obstacle mask by one uniform
                                        value so that the net boundary flux is zero and graddin's
                                        all-Neumann system (9_grad.f90:96-116) is consistent */
-    int    reserved;
+    int    periodic_faces;          /* 0 = the reference: graddin and posdin take the face density of
+                                       interp?_cf, whose end faces copy their neighbour (8_derivadas.f90:318-323);
+                                       1 (extension) = on a periodic axis both end faces, one face of the
+                                       periodic box, take the average across the wrap, which keeps the
+                                       scaled Poisson operator symmetric when the density varies there */
     double div_tol;                 /* 0 = off (the reference); > 0 (extension): the Poisson solve also
                                        requires max |sqrt(d) r~| <= div_tol, the largest |div u| the
                                        projection leaves (the unscaled residual), and iterates on

@@ -89,6 +89,7 @@ struct Oracle {
     void contorno_obstacle();
     void level_set_obstacle();
     void outflow_fix();
+    void wrap_faces(Arr& rx, Arr& ry, Arr& rz) const;
     /* wave inflow (module wave_c, 0_modules.f90:164-174) */
     double p_w = 0, n_w = 0, c_w = 0, l_w = 0, a_w = 0, f_w = 0, h0_f = 0, l0_w = 0;
     double avel[6] = {0}, aeta[6] = {0};   /* avel1..5, aeta1..5 at [1..5] */
@@ -1158,6 +1159,24 @@ void Oracle::contorno_obstacle() {
         for (int k = 0; k <= KV(i, ny1 + 1); ++k) v(i, ny1 + 1, k) = 0.;
 }
 
+/* Option periodic_faces = 1 (an extension; the reference has no counterpart): on a periodic axis
+ * the two end faces of interp?_cf, which are one face of the periodic box, both take the average
+ * across the wrap, (rho(1) + rho(n)) * 0.5, in place of the copies of their neighbour faces
+ * (8_derivadas.f90:318-323).  graddin's scaled operator is then symmetric where the density
+ * varies across the periodic boundary, and posdin moves both copies of that face alike. */
+void Oracle::wrap_faces(Arr& rx, Arr& ry, Arr& rz) const {
+    if (P.periodic_faces != 1) return;
+    if (P.ccx0 == 0)
+        for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j)
+            rx(1, j, k) = rx(nx1, j, k) = (rho(1, j, k) + rho(nx, j, k)) * 0.5;
+    if (P.ccy0 == 0)
+        for (int k = 1; k <= nz; ++k) for (int i = 1; i <= nx; ++i)
+            ry(i, 1, k) = ry(i, ny1, k) = (rho(i, 1, k) + rho(i, ny, k)) * 0.5;
+    if (P.ccz0 == 0)
+        for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i)
+            rz(i, j, 1) = rz(i, j, nz1) = (rho(i, j, 1) + rho(i, j, nz)) * 0.5;
+}
+
 /* Option outflow_fix = 1 (an extension; the reference has no counterpart): after
  * contorno(2) has copied the outflow plane (ccxf = 4, 3_contorno.f90:193-197, 362-409), shift
  * u(nx+1,j,k) by one uniform delta over the outflow faces above the obstacle mask so that the
@@ -1478,6 +1497,7 @@ int Oracle::graddin() {
     interpx_cf(rho, nx, ny, nz, rhox);
     interpy_cf(rho, nx, ny, nz, rhoy);
     interpz_cf(rho, nx, ny, nz, rhoz);
+    wrap_faces(rhox, rhoy, rhoz);
     si.init(1, nx1, 1, ny, 1, nz); sj.init(1, nx, 1, ny1, 1, nz); sk.init(1, nx, 1, ny, 1, nz1);
     const double cx = dt / (dx * dx), cy = dt / (dy * dy), cz = dt / (dz * dz);
     for (auto& x : si.a) x = cx;
@@ -1594,6 +1614,7 @@ void Oracle::posdin() {
     interpx_cf(rho, nx, ny, nz, rhox);
     interpy_cf(rho, nx, ny, nz, rhoy);
     interpz_cf(rho, nx, ny, nz, rhoz);
+    wrap_faces(rhox, rhoy, rhoz);
     for (int k = 1; k <= nz; ++k) {
         for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx1; ++i)
             u(i, j, k) = u(i, j, k) - aux1 * (prd1(i, j, k) - prd1(i - 1, j, k)) / rhox(i, j, k);

@@ -46,7 +46,7 @@ class SuliParams(C.Structure):
         ("mg_kernels", C.c_int),
         ("wave_t", C.c_int),
         ("outflow_fix", C.c_int),
-        ("reserved", C.c_int),
+        ("periodic_faces", C.c_int),
         ("div_tol", C.c_double),
     ]
 
@@ -56,7 +56,7 @@ class SuliParams(C.Structure):
         return out
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class SuliStepStats(C.Structure):

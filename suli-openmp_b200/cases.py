@@ -278,7 +278,7 @@ def bump_channel(nx=32, ny=16, nz=24, dx=0.02, cg_tol=1e-10, u_init=0.1, outflow
     return p, init, masks
 
 
-def les_channel(nx=512, ny=256, nz=256, cg_tol=1e-8, seed=0, x0=3.0, outflow_fix=1):
+def les_channel(nx=512, ny=256, nz=256, cg_tol=1e-8, seed=0, x0=3.0, outflow_fix=1, periodic_faces=1):
     """The LES channel over a bottom bump: 6 x 3 x 3 m (dx = dy = dz = 6/nx at the default
     size, 0.01171875), water 2 m deep, the obst_t = 3 Gaussian bump with height 0.3 m, no flat
     base (d = 0), sigma 0.5 m, centred at (x0, Ly/2); inflow u = 1 + 0.05 U(-1, 1) (seeded,
@@ -291,7 +291,11 @@ def les_channel(nx=512, ny=256, nz=256, cg_tol=1e-8, seed=0, x0=3.0, outflow_fix
     outflow copy carries, the problem is inconsistent and its CG diverges within the first
     steps (in this library and in the CPU restatement of the tests alike), as it does for the
     wave flume; a uniform flow through the same faces stays exactly steady.  The case therefore
-    turns on outflow_fix (the outflow plane shifted to balance the inflow) unless told not to."""
+    turns on outflow_fix (the outflow plane shifted to balance the inflow) unless told not to.
+    Once the surface moves, the density also varies across the periodic y boundary, where the
+    reference's clamped end faces make the scaled Poisson operator non-symmetric and the CG
+    breaks down after a few steps; periodic_faces (the wrap average at both end faces) is on
+    for the same reason."""
     p = default_params()
     p.nx, p.ny, p.nz = nx, ny, nz
     p.dx, p.dy, p.dz = 6.0 / nx, 3.0 / ny, 3.0 / nz
@@ -302,6 +306,7 @@ def les_channel(nx=512, ny=256, nz=256, cg_tol=1e-8, seed=0, x0=3.0, outflow_fix
     p.cg_tol = cg_tol
     p.obst_t = 3
     p.outflow_fix = outflow_fix
+    p.periodic_faces = periodic_faces
     p.dt = 0.3 * min(p.dx, p.dy, p.dz) / (1.05 + math.sqrt(9.81 * 2.0))
     ly = ny * p.dy
 

@@ -49,6 +49,7 @@ inline Geo make_geo(int nx, int ny, int nz) {
 struct BC {
     int x0, xf, y0, yf, z0, zf;   // ccx0..cczf
     int perx, pery, perz;         // periodic flags as the reference tests them
+    int wrapf;                    // suli_params.periodic_faces: end faces of a periodic axis averaged across the wrap
 };
 
 // Neighbour index maps of the Poisson operator's ghost copies (9_grad.f90:99-116):

@@ -939,17 +939,22 @@ struct CGConst {
     double ncell;          // nx*ny*nz
     int mode, maxit;
 };
-__device__ __forceinline__ double face_s_x(const Geo& G, const double* rho, double cx, int f, int j, int k) {
+// face density of graddin and posdin: the centre average with the reference's clamped end faces,
+// or (periodic_faces = 1 on a periodic axis) the average across the wrap at both end faces
+__device__ __forceinline__ double rho_face_x(const Geo& G, const BC& bc, const double* rho, int f, int j, int k) {
+    if (bc.wrapf && bc.perx && (f == 1 || f == G.nx + 1)) return (FIDX(rho, 1, j, k) + FIDX(rho, G.nx, j, k)) * 0.5;
     const int fc = clampi(f, 2, G.nx);
-    return cx / ((FIDX(rho, fc, j, k) + FIDX(rho, fc - 1, j, k)) * 0.5);
+    return (FIDX(rho, fc, j, k) + FIDX(rho, fc - 1, j, k)) * 0.5;
 }
-__device__ __forceinline__ double face_s_y(const Geo& G, const double* rho, double cy, int i, int f, int k) {
+__device__ __forceinline__ double rho_face_y(const Geo& G, const BC& bc, const double* rho, int i, int f, int k) {
+    if (bc.wrapf && bc.pery && (f == 1 || f == G.ny + 1)) return (FIDX(rho, i, 1, k) + FIDX(rho, i, G.ny, k)) * 0.5;
     const int fc = clampi(f, 2, G.ny);
-    return cy / ((FIDX(rho, i, fc, k) + FIDX(rho, i, fc - 1, k)) * 0.5);
+    return (FIDX(rho, i, fc, k) + FIDX(rho, i, fc - 1, k)) * 0.5;
 }
-__device__ __forceinline__ double face_s_z(const Geo& G, const double* rho, double cz, int i, int j, int f) {
+__device__ __forceinline__ double rho_face_z(const Geo& G, const BC& bc, const double* rho, int i, int j, int f) {
+    if (bc.wrapf && bc.perz && (f == 1 || f == G.nz + 1)) return (FIDX(rho, i, j, 1) + FIDX(rho, i, j, G.nz)) * 0.5;
     const int fc = clampi(f, 2, G.nz);
-    return cz / ((FIDX(rho, i, j, fc) + FIDX(rho, i, j, fc - 1)) * 0.5);
+    return (FIDX(rho, i, j, fc) + FIDX(rho, i, j, fc - 1)) * 0.5;
 }
 
 // Set-up of the scaled system in three passes, so that each face conductance is divided once:
@@ -959,29 +964,32 @@ __device__ __forceinline__ double face_s_z(const Geo& G, const double* rho, doub
 
 // minus-face conductances of every cell, the reference's c/((rho_a + rho_b)/2) with the clamped
 // end faces (:46-87): sx(i) = face between i-1 and i (at i = 1 the face of i = 2)
-__global__ void __launch_bounds__(256) k_cg_faces(Geo G, CGConst K, const double* __restrict__ rho, double* sx,
+__global__ void __launch_bounds__(256) k_cg_faces(Geo G, BC bc, CGConst K, const double* __restrict__ rho, double* sx,
                                                   double* sy, double* sz) {
     const Thread3 t = tid3(1, 1, 1);
     const int i = t.i, j = t.j, k = t.k;
     if (i > G.nx || j > G.ny || k > G.nz) return;
     const long long c = G.idx(i, j, k);
-    sx[c] = face_s_x(G, rho, K.cx, i, j, k);
-    sy[c] = face_s_y(G, rho, K.cy, i, j, k);
-    sz[c] = face_s_z(G, rho, K.cz, i, j, k);
+    sx[c] = K.cx / rho_face_x(G, bc, rho, i, j, k);
+    sy[c] = K.cy / rho_face_y(G, bc, rho, i, j, k);
+    sz[c] = K.cz / rho_face_z(G, bc, rho, i, j, k);
 }
 
 // the plus face of a cell: the next cell's minus face, or at the last cell the same clamped face
+// (with periodic_faces on a periodic axis: the first cell's minus face, the same face of the box)
 struct PlusFaces {
     double xp, yp, zp;
 };
-__device__ __forceinline__ PlusFaces plus_faces(const Geo& G, int i, int j, int k, long long c, const double* sx,
-                                                const double* sy, const double* sz) {
-    return PlusFaces{(i < G.nx) ? sx[c + 1] : sx[c], (j < G.ny) ? sy[c + G.px] : sy[c],
-                     (k < G.nz) ? sz[c + G.pxy] : sz[c]};
+__device__ __forceinline__ PlusFaces plus_faces(const Geo& G, const BC& bc, int i, int j, int k, long long c,
+                                                const double* sx, const double* sy, const double* sz) {
+    const bool wx = bc.wrapf && bc.perx, wy = bc.wrapf && bc.pery, wz = bc.wrapf && bc.perz;
+    return PlusFaces{(i < G.nx) ? sx[c + 1] : sx[c - (wx ? G.nx - 1 : 0)],
+                     (j < G.ny) ? sy[c + G.px] : sy[c - (wy ? (long long)(G.ny - 1) * G.px : 0)],
+                     (k < G.nz) ? sz[c + G.pxy] : sz[c - (wz ? (long long)(G.nz - 1) * G.pxy : 0)]};
 }
 
 // diagonal d, scaled unknown e = prd1*sqrt(d), scaled right-hand side b = q/sqrt(d) (:46-87, :118-124)
-__global__ void __launch_bounds__(256) k_cg_diag(Geo G, CGConst K, const double* __restrict__ sx,
+__global__ void __launch_bounds__(256) k_cg_diag(Geo G, BC bc, CGConst K, const double* __restrict__ sx,
                                                  const double* __restrict__ sy, const double* __restrict__ sz,
                                                  const double* __restrict__ u, const double* __restrict__ v,
                                                  const double* __restrict__ w, const double* __restrict__ prd1,
@@ -990,7 +998,7 @@ __global__ void __launch_bounds__(256) k_cg_diag(Geo G, CGConst K, const double*
     const int i = t.i, j = t.j, k = t.k;
     if (i > G.nx || j > G.ny || k > G.nz) return;
     const long long c = G.idx(i, j, k);
-    const PlusFaces P = plus_faces(G, i, j, k, c, sx, sy, sz);
+    const PlusFaces P = plus_faces(G, bc, i, j, k, c, sx, sy, sz);
     const double dv = P.xp + sx[c] + P.yp + sy[c] + P.zp + sz[c];
     const double q = (FIDX(u, i, j, k) - FIDX(u, i + 1, j, k)) / K.dx + (FIDX(v, i, j, k) - FIDX(v, i, j + 1, k)) / K.dy +
                      (FIDX(w, i, j, k) - FIDX(w, i, j, k + 1)) / K.dz;
@@ -1019,8 +1027,8 @@ __global__ void __launch_bounds__(256, 4) k_cg_coef(Geo G, BC bc, CGConst K, con
         const int px = G.px, pxy = (int)G.pxy;
         const Nb o = neighbours(G, bc, i, j, k);   // ghost-mapped neighbours (periodic wrap / Neumann self)
         const double ic = isd[c];
-        const double sxp = (i < nx) ? sx[c + 1] : sx[c], syp = (j < ny) ? sy[c + px] : sy[c],
-                     szp = (k < nz) ? sz[c + pxy] : sz[c];
+        const PlusFaces P = plus_faces(G, bc, i, j, k, c, sx, sy, sz);
+        const double sxp = P.xp, syp = P.yp, szp = P.zp;
         const double app = sxp * ic * isd[c + o.xp];
         const double anp = sx[c] * ic * isd[c + o.xm];
         const double bpp = syp * ic * isd[c + o.yp];
@@ -1268,25 +1276,22 @@ __global__ void k_cg_final(Geo G, BC bc, const double* __restrict__ sdv, const d
 // ------------------------------------------------------------------------------------
 // posdin (10_pos.f90:1-96) and est (4_plot.f90:500-525)
 // ------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_posdin(Geo G, double aux1, double aux2, double aux3,
+__global__ void __launch_bounds__(256) k_posdin(Geo G, BC bc, double aux1, double aux2, double aux3,
                                                 const double* __restrict__ rho, const double* __restrict__ prd1,
                                                 double* u, double* v, double* w) {
     const Thread3 t = tid3(1, 1, 1);
     const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
     if (i > nx + 1 || j > ny + 1 || k > nz + 1) return;
     if (j <= ny && k <= nz) {
-        const int ic = clampi(i, 2, nx);
-        const double rhox = (FIDX(rho, ic, j, k) + FIDX(rho, ic - 1, j, k)) * 0.5;
+        const double rhox = rho_face_x(G, bc, rho, i, j, k);
         FIDX(u, i, j, k) = FIDX(u, i, j, k) - aux1 * (FIDX(prd1, i, j, k) - FIDX(prd1, i - 1, j, k)) / rhox;
     }
     if (i <= nx && k <= nz) {
-        const int jc = clampi(j, 2, ny);
-        const double rhoy = (FIDX(rho, i, jc, k) + FIDX(rho, i, jc - 1, k)) * 0.5;
+        const double rhoy = rho_face_y(G, bc, rho, i, j, k);
         FIDX(v, i, j, k) = FIDX(v, i, j, k) - aux2 * (FIDX(prd1, i, j, k) - FIDX(prd1, i, j - 1, k)) / rhoy;
     }
     if (i <= nx && j <= ny) {
-        const int kc = clampi(k, 2, nz);
-        const double rhoz = (FIDX(rho, i, j, kc) + FIDX(rho, i, j, kc - 1)) * 0.5;
+        const double rhoz = rho_face_z(G, bc, rho, i, j, k);
         FIDX(w, i, j, k) = FIDX(w, i, j, k) - aux3 * (FIDX(prd1, i, j, k) - FIDX(prd1, i, j, k - 1)) / rhoz;
     }
 }
@@ -1543,8 +1548,8 @@ void launch_cg_setup(suli_ctx* c) {
     ProfScope ps(c, SULI_K_CG_SETUP, 3);
     // face scratch: the CG direction and product vectors, written again before the iterations read them
     double *sx = c->cg_pa, *sy = c->cg_pb, *sz = c->cg_q;
-    k_cg_faces<<<cells_grid(G), kBlk, 0, c->stream>>>(G, K, c->f[SULI_F_RHO], sx, sy, sz);
-    k_cg_diag<<<cells_grid(G), kBlk, 0, c->stream>>>(G, K, sx, sy, sz, c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W],
+    k_cg_faces<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->bc, K, c->f[SULI_F_RHO], sx, sy, sz);
+    k_cg_diag<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->bc, K, sx, sy, sz, c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W],
                                                       c->f[SULI_F_PRD1], c->cg_d, c->cg_e, c->cg_b, c->cg_sd, c->cg_isd);
     k_cg_coef<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->bc, K, sx, sy, sz, c->cg_sd, c->cg_isd, c->cg_e, c->cg_b,
                                                       c->f[SULI_F_PRD1], c->cg_ax, c->cg_ay, c->cg_az, c->cg_r, c->cg,
@@ -1588,7 +1593,7 @@ void launch_posdin(suli_ctx* c) {
     const Geo& G = c->g;
     const double aux1 = c->dt / c->P.dx, aux2 = c->dt / c->P.dy, aux3 = c->dt / c->P.dz;
     ProfScope ps(c, SULI_K_POSDIN, 1);
-    k_posdin<<<faces_grid(G), kBlk, 0, c->stream>>>(G, aux1, aux2, aux3, c->f[SULI_F_RHO], c->f[SULI_F_PRD1],
+    k_posdin<<<faces_grid(G), kBlk, 0, c->stream>>>(G, c->bc, aux1, aux2, aux3, c->f[SULI_F_RHO], c->f[SULI_F_PRD1],
                                                      c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W]);
     cudaMemcpyAsync(c->f[SULI_F_PRD], c->f[SULI_F_PRD1], G.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
 }

@@ -116,6 +116,7 @@ int validate(const suli_params* p, std::string& why) {
     if (p->wave_t != 0 && p->wave_t != 1 && p->wave_t != 2 && p->wave_t != 5) {
         why = "wave_t must be 0 (none), 1 (Stokes I), 2 (Stokes II) or 5 (Stokes V)"; return SULI_ERR_ARG;
     }
+    if (p->periodic_faces != 0 && p->periodic_faces != 1) { why = "periodic_faces must be 0 or 1"; return SULI_ERR_ARG; }
     if (!(p->div_tol >= 0)) { why = "div_tol must be >= 0 (0: no divergence test)"; return SULI_ERR_ARG; }
     if (p->outflow_fix != 0 && p->outflow_fix != 1) { why = "outflow_fix must be 0 or 1"; return SULI_ERR_ARG; }
     if (p->outflow_fix == 1 && p->ccxf != 4) { why = "outflow_fix = 1 corrects the outflow plane: it needs ccxf = 4"; return SULI_ERR_ARG; }
@@ -209,6 +210,7 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
     c->g = make_geo(p->nx, p->ny, p->nz);
     c->bc.x0 = p->ccx0; c->bc.xf = p->ccxf; c->bc.y0 = p->ccy0; c->bc.yf = p->ccyf; c->bc.z0 = p->ccz0; c->bc.zf = p->cczf;
     c->bc.perx = (p->ccx0 == 0); c->bc.pery = (p->ccy0 == 0); c->bc.perz = (p->ccz0 == 0);
+    c->bc.wrapf = p->periodic_faces;
     auto bail = [&](cudaError_t e, const char* what) {
         std::fprintf(stderr, "suli_create: %s: %s\n", what, cudaGetErrorString(e));
         suli_destroy(c);

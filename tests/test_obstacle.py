@@ -355,6 +355,28 @@ def test_restart_and_campos_carry_the_masks(orc, tmp_path):
         assert (kaux[i - 1, j - 1, :] == (np.arange(1, p.nz + 1) < kw[i, j])).all()
 
 
+def test_les_channel_steps(orc):
+    """The LES channel at 64 x 32 x 32 runs 12 steps on the oracle with both consistency options
+    (every solve converged, the level-set volume within 1e-4); with the reference's end faces
+    across the periodic y boundary its CG breaks down within those steps."""
+    for pf in (1, 0):
+        p, init, masks = cases.les_channel(nx=64, ny=32, nz=32, periodic_faces=pf)
+        p.cg_maxit = 3000
+        o = orc.Oracle(p, openmp=True)
+        init(o)
+        v0 = o.get_scalar("vol_ini")
+        ok = True
+        for it in range(1, 13):
+            st = o.step(it)
+            ok = ok and st["status"] == 0 and max(st["cg_resid"]) <= 1e-8
+            if not ok:
+                break
+        if pf == 1:
+            assert ok and abs(o.get_scalar("vol_ins") - v0) / v0 < 1e-4
+        else:
+            assert not ok
+
+
 def test_les_channel_case():
     """Config C5 built at a small size: the 6 x 3 x 3 m box, the 0.3 m bump's masks, the seeded
     inflow 1 +- 0.05."""

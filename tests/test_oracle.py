@@ -651,3 +651,54 @@ def test_divergence_stopping_test(orc):
     assert max(s["max_div"] for s in out[0.0]) > 1e-8
     assert max(s["max_div"] for s in out[1e-8]) <= 1e-8
     assert sum(map(sum, (s["cg_iters"] for s in out[1e-8]))) > sum(map(sum, (s["cg_iters"] for s in out[0.0])))
+
+
+def test_periodic_faces_make_the_operator_symmetric(orc):
+    """Density varying across the periodic x and y boundaries: with the reference's clamped end
+    faces graddin's operator is not symmetric and its CG does not reach 1e-12 within 2000
+    iterations; with periodic_faces = 1 both end faces of a periodic axis take the average
+    across the wrap, the CG converges and posdin, using the same faces, leaves the divergence
+    at the solve's level."""
+    out = {}
+    for pf in (0, 1):
+        p = small_params(nx=14, ny=12, nz=10, bc=(0, 0, 0, 0, 2, 1))
+        p.cg_stop, p.cg_tol, p.cg_maxit = 1, 1e-12, 2000
+        p.periodic_faces = pf
+        o = orc.Oracle(p)
+        load_state(o, seeded_state(p, 8))
+        o.heaviside()
+        o.contorno(1)
+        o.set_dt(1e-3)
+        o.contorno(2)
+        n, r = o.graddin()
+        o.posdin()
+        o.contorno(1)
+        out[pf] = (n, r, o.est())
+    assert out[0][0] == 2000 and out[0][1] > 1e-12
+    assert out[1][0] < 2000 and out[1][1] <= 1e-12
+    assert out[1][2] < 1e-7
+    # the faces themselves: the two end faces of x equal the wrap average, the interior faces
+    # are unchanged (one solve each with a single iteration, read back through posdin)
+    q = small_params(nx=14, ny=12, nz=10, bc=(0, 0, 0, 0, 2, 1))
+    st = seeded_state(q, 8)
+    prd = np.zeros(pkg.field_shape(q, "prd1"))
+    prd[1, :, :] = 1.0                       # a pressure step across the face i = 1 only
+    outs = []
+    for pf in (0, 1):
+        q.periodic_faces = pf
+        o = orc.Oracle(q)
+        load_state(o, st)
+        o.heaviside()
+        o.upload("prd1", prd)
+        o.set_dt(1e-3)
+        u0 = o.download("u")
+        o.posdin()
+        outs.append((u0 - o.download("u"), o.download("rho")))
+    (d0, rho), (d1, _) = outs
+    aux = 1e-3 / q.dx
+    want1 = aux * 1.0 / ((rho[0] + rho[-1]) * 0.5)          # face i = 1: p(1) - p(0) = 1
+    want0 = aux * 1.0 / ((rho[1] + rho[0]) * 0.5)
+    assert np.allclose(d1[1, 1:-1, 1:-1], want1, rtol=1e-9, atol=0)
+    assert np.allclose(d0[1, 1:-1, 1:-1], want0, rtol=1e-9, atol=0)
+    assert not np.allclose(want0, want1, rtol=1e-3, atol=0)
+    assert np.array_equal(d0[3:-2], d1[3:-2])
