@@ -78,6 +78,9 @@ def parse_args():
                     help="steps of the long-window block (C3's 500; 0: skip)")
     ap.add_argument("--long-paths", default="learned,plain",
                     help="paths timed over the long window (comma list of plain, mixed, learned)")
+    ap.add_argument("--c5-steps", type=int, default=4,
+                    help="timed steps of the LES channel over a bump at 512x256x256 (0: skip)")
+    ap.add_argument("--c5-n", default="512,256,256", help="grid of the LES channel block")
     return ap.parse_args()
 
 
@@ -243,6 +246,80 @@ def cpu_desc(cs, openmp):
             f"{cs['steps_timed'][-1]} from the seeded state, after {cs['steps_timed'][0] - 1} untimed), "
             f"Poisson solves to the same two stopping tests, no iteration cap "
             f"({statistics.mean(cs['poisson_iters_per_step']):.0f} CG iterations per step)")
+
+
+# ------------------------------------------------------------------------------ C5
+# Algorithmic N-sized FP64 passes (8 bytes a cell) per launch of each stencil kernel class:
+# reads and writes of whole fields, halos not counted twice.
+CLASS_PASSES = {
+    "ls_advect": 6,    # ls, stage start, u, v, w in; ls out
+    "reinit": 4,       # mean of S(phi0) (2), stage (5) and band error (2) launches
+    "lsprops": 11,     # ls in; mod_ls, 3 normals, hs, hsx..z, rho, ls_nu out
+    "curv": 7,         # 3 normals in; ddlsdx..z, kurv out
+    "visco": 5,        # nut: u, v, w, rho in, nut out; faces: nut, ls_nu in, xnut..znut out
+    "convdiff": 20,    # u, v, w, rho, hsx..z, kurv, nut, xnut..znut in, Fu..Fw out; prd0 = prd1 copy
+    "tempo": 15,       # per component: velocity, F in; velocity and two stage stores out
+    "posdin": 8,       # u, v, w, prd1, rho in; u, v, w out
+    "est": 3,          # u, v, w in
+}
+
+
+def class_bandwidth(p, kernels):
+    """GB/s of the stencil kernel classes from the tracer's device time and launches per step."""
+    n8 = 8.0 * p.nx * p.ny * p.nz
+    out = {}
+    for k, passes in CLASS_PASSES.items():
+        v = kernels.get(k)
+        if not v or v["ms_per_step"] <= 0:
+            continue
+        b = passes * n8 * v["launches_per_step"]
+        out[k] = {"ms_per_step": round(v["ms_per_step"], 4), "launches_per_step": v["launches_per_step"],
+                  "gbs": round(b / (v["ms_per_step"] / 1e3) / 1e9, 1)}
+    return out
+
+
+def c5_block(args, dist, pkg, dev):
+    """The LES channel over a Gaussian bump (6 x 3 x 3 m, water 2 m deep, inflow 1 m/s + 5 %
+    seeded noise, outflow, periodic y, Cs = 0.12, CFL 0.3): the plain FP64 path and the
+    learned + mixed path, each timed over --c5-steps steps after 2 warm-up steps from the same
+    state; time-steps/s, GB/s per stencil kernel class, level-set volume drift, the divergence
+    and the learned path's error per field against the plain run."""
+    import torch
+    nx, ny, nz = (int(v) for v in args.c5_n.split(","))
+    p, init, _ = pkg.cases.les_channel(nx=nx, ny=ny, nz=nz, cg_tol=args.cg_tol)
+    q = mixed_params(p, args)
+    q.div_tol = 0.0
+    out = {"grid": f"{nx}x{ny}x{nz}", "dx": p.dx, "dt": p.dt, "steps": args.c5_steps, "warmup": 2,
+           "options": "outflow_fix = 1, periodic_faces = 1 (the reference's outflow copy and periodic end faces "
+                      "make this Poisson system inconsistent and non-symmetric)",
+           "max_div_note": "max|div u| includes the cells beside the bump, where contorno zeroes the velocities "
+                           "after the projection (3_contorno.f90:266-294)"}
+    sub = argparse.Namespace(**vars(args))
+    sub.steps, sub.warmup = args.c5_steps, 2
+    net = None
+    states = {}
+    for key, prm in (("plain_fp64", p), ("learned", q)):
+        if key == "learned":
+            net, src = load_net(pkg, q, args, dev)
+            if net is None:
+                out[key] = {"skipped": src}
+                continue
+        r = time_path(sub, dist, pkg, prm, init, dev, net=net)
+        s = r["solver"]
+        v0, v1 = s.get_scalar("vol_ini"), s.get_scalar("vol_ins")
+        states[key] = state_of(s)
+        s.close()
+        out[key] = {"value": r["value"], "ms_per_step": r["ms"] / sub.steps, "poisson_iters_per_step": r["iters_per_step"],
+                    "volume_drift": (v1 - v0) / v0, "max_div": max(st["max_div"] for st in r["stats"]),
+                    "cg_resid_max": max(max(st["cg_resid"]) for st in r["stats"]),
+                    "kernel_gbs": class_bandwidth(prm, r["kernels"]),
+                    "clocks": {k: r["clocks"].get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
+    if net is not None:
+        net.close()
+    if "plain_fp64" in states and "learned" in states:
+        out["learned"]["error_vs_plain_fp64"] = field_errors(states["learned"], states["plain_fp64"])
+        out["learned"]["speedup_vs_plain_fp64"] = out["learned"]["value"] / out["plain_fp64"]["value"]
+    return out
 
 
 # ------------------------------------------------------------------------------ arms
@@ -653,6 +730,7 @@ def run_ours(args):
     mms = None
     if dist.world == 1 and args.mms_n > 0:
         mms = mms_check(pkg, args, dev)
+    c5 = c5_block(args, dist, pkg, dev) if args.c5_steps > 0 else None
     if dist.rank == 0:
         desc = {"plain": "plain FP64: the reference's Jacobi-scaled CG",
                 "mixed": "mixed: FP32 stencils, FP32 multigrid-preconditioned inner CG inside FP64 iterative "
@@ -700,6 +778,11 @@ def run_ours(args):
         line["roofline_plain_fp64"] = roof_plain
         if mms is not None:
             line["mms"] = mms
+        if c5 is not None:
+            line["c5_les_channel"] = c5
+        line["kernel_gbs"] = class_bandwidth(p, head["kernels"])
+        if "plain" in runs:
+            line["kernel_gbs_plain_fp64"] = class_bandwidth(p, runs["plain"]["kernels"])
         line["kernels"] = {k: {kk: round(vv, 4) for kk, vv in v.items()} for k, v in head["kernels"].items()}
         line["config"]["path"] = head_key
         print(json.dumps(line), flush=True)

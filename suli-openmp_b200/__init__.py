@@ -12,10 +12,10 @@ the synthetic cases (cases).  Load it by path, e.g.
 from ._abi import (FIELD, FIELD_NAMES, SCALAR, SuliParams, SuliStepStats, default_params,
                    field_extent, field_shape, load_library, LIB_PATH)
 from .solver import Solver, SuliError
-from . import cases, fileio, learned, snapshots
+from . import cases, fileio, learned, mms_weng, snapshots
 
 __all__ = [
     "FIELD", "FIELD_NAMES", "SCALAR", "SuliParams", "SuliStepStats", "default_params",
     "field_extent", "field_shape", "load_library", "LIB_PATH", "Solver", "SuliError", "cases", "fileio",
-    "learned", "snapshots",
+    "learned", "mms_weng", "snapshots",
 ]

@@ -150,8 +150,10 @@ struct suli_ctx {
     double* nn_e0 = nullptr;                     // e0 of a recorded solve (box layout)
     suli::NNScale* nn_scale = nullptr;
     float *rec_in = nullptr, *rec_target = nullptr;
-    // cached CUDA graphs of CG iteration batches (parity 0: p_old = pa)
-    cudaGraphExec_t cg_graph = nullptr;
+    // false (environment SULI_EAGER_LOOPS=1, for per-kernel profiling): the CG and inner PCG
+    // iterations are launched one by one from the host, two at a time with a check of the
+    // device state after each pair, in place of the device-side graph loop; same kernels, same
+    // order, same results
     bool use_graphs = true;
     // tracing: CUDA-event pairs around each kernel class (suli_profile_*)
     struct Prof {

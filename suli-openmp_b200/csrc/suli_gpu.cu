@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -211,6 +212,7 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
     c->bc.x0 = p->ccx0; c->bc.xf = p->ccxf; c->bc.y0 = p->ccy0; c->bc.yf = p->ccyf; c->bc.z0 = p->ccz0; c->bc.zf = p->cczf;
     c->bc.perx = (p->ccx0 == 0); c->bc.pery = (p->ccy0 == 0); c->bc.perz = (p->ccz0 == 0);
     c->bc.wrapf = p->periodic_faces;
+    if (const char* ev = std::getenv("SULI_EAGER_LOOPS")) c->use_graphs = (std::strcmp(ev, "1") != 0);
     auto bail = [&](cudaError_t e, const char* what) {
         std::fprintf(stderr, "suli_create: %s: %s\n", what, cudaGetErrorString(e));
         suli_destroy(c);
@@ -293,7 +295,6 @@ int suli_destroy(suli_ctx* c) {
     if (!c) return SULI_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    if (c->cg_graph) cudaGraphExecDestroy(c->cg_graph);
     if (c->pcg_loop) cudaGraphExecDestroy(c->pcg_loop);
     if (c->cg_loop) cudaGraphExecDestroy(c->cg_loop);
     for (auto& e : c->prof.ev) cudaEventDestroy(e);
@@ -757,16 +758,26 @@ int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
             launch_vcycle(c);
         }
         launch_pcg_iter(c, c->mg[0].y, c->pc_pa);   // p_old = z with beta = 0
-        {
+        if (c->use_graphs) {
             ProfScope ps(c, SULI_K_MG, 0);   // kernel launches are counted below, once known
             CUDA_TRY(c, cudaGraphLaunch(c->pcg_loop, c->stream));
+        } else {
+            for (int pair = 0; pair < c->inner_maxit; ++pair) {
+                launch_pcg_iter(c, c->pc_pa, c->pc_pb);
+                launch_pcg_iter(c, c->pc_pb, c->pc_pa);
+                CHECK_LAUNCH(c);
+                if (int rr = sync_read(c, c->pcg, c->pcg_host, sizeof(PCGState))) return rr;
+                if (c->pcg_host[0].done) break;
+            }
         }
         r = sync_read(c, c->pcg, c->pcg_host, sizeof(PCGState));
         if (r != SULI_OK) return r;
         if (c->pcg_host[0].status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the inner solve");
         inner_total += c->pcg_host[0].iters;
-        const long long bodies = std::max(1, (c->pcg_host[0].iters - 1 + 1) / 2);
-        c->prof.launches[SULI_K_MG] += bodies * (2LL * c->pcg_graph_kernels + 1);
+        if (c->use_graphs) {   // eager launches were counted as they went
+            const long long bodies = std::max(1, (c->pcg_host[0].iters - 1 + 1) / 2);
+            c->prof.launches[SULI_K_MG] += bodies * (2LL * c->pcg_graph_kernels + 1);
+        }
         launch_mx_residual(c, ecur, enext, true);
         std::swap(ecur, enext);
         CHECK_LAUNCH(c);
@@ -800,10 +811,21 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
     CHECK_LAUNCH(c);
     // iteration 1 uses p_old = r with beta = 0 (erroppr = erropr, :172); then the device loop
     launch_cg_iter(c, c->cg_r, c->cg_pa);
-    {
-        ProfScope ps(c, SULI_K_CG_SPMV, 0);   // kernel launches are counted below, once known
-        CUDA_TRY(c, cudaGraphLaunch(c->cg_loop, c->stream));
-    }
+    auto run_loop = [&]() -> int {
+        if (c->use_graphs) {
+            ProfScope ps(c, SULI_K_CG_SPMV, 0);   // kernel launches are counted below, once known
+            CUDA_TRY(c, cudaGraphLaunch(c->cg_loop, c->stream));
+            return SULI_OK;
+        }
+        for (;;) {
+            launch_cg_iter(c, c->cg_pa, c->cg_pb);
+            launch_cg_iter(c, c->cg_pb, c->cg_pa);
+            CHECK_LAUNCH(c);
+            if (int rr = sync_read(c, c->cg, c->cg_host, sizeof(CGState))) return rr;
+            if (c->cg_host[0].done) return SULI_OK;
+        }
+    };
+    if (int rl = run_loop()) return rl;
     CHECK_LAUNCH(c);
     // div_tol > 0: resume the solve while the divergence the projection would leave is too large
     for (int pass = 0; c->P.div_tol > 0. && pass < 64; ++pass) {
@@ -821,10 +843,7 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
             CUDA_TRY(c, cudaMemcpyAsync(c->cg_pa, c->cg_pb, c->g.n * sizeof(double), cudaMemcpyDeviceToDevice,
                                         c->stream));
         }
-        {
-            ProfScope ps(c, SULI_K_CG_SPMV, 0);
-            CUDA_TRY(c, cudaGraphLaunch(c->cg_loop, c->stream));
-        }
+        if (int rl = run_loop()) return rl;
         CHECK_LAUNCH(c);
     }
     launch_cg_final(c, c->cg_e);
@@ -834,7 +853,7 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
     if (r != SULI_OK) return r;
     const CGState& s = c->cg_host[0];
     c->prof.cg_iters += s.iters;
-    {   // the loop ran ceil((iters - 1) / 2) two-iteration bodies (at least one)
+    if (c->use_graphs) {   // the loop ran ceil((iters - 1) / 2) two-iteration bodies (at least one)
         const long long bodies = std::max(1, s.iters / 2);
         c->prof.launches[SULI_K_CG_SPMV] += 2 * bodies;
         c->prof.launches[SULI_K_CG_UPDATE] += 2 * bodies;

@@ -148,6 +148,27 @@ def test_divergence_stopping_test_gpu(pkg, orc, precision):
     g.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_eager_loops_match_graph_loops(pkg, precision, monkeypatch):
+    """SULI_EAGER_LOOPS=1 (a profiling aid: iterations launched from the host instead of the
+    device-side graph loop) runs the same kernels in the same order: bit-identical pressure,
+    velocities and iteration counts over two steps."""
+    p, init = pkg.cases.sloshing(nx=32, ny=16, nz=16, dx=0.04, cg_tol=1e-8, div_tol=1e-8)
+    if precision == 1:
+        p.precision, p.refine_maxit, p.inner_tol = 1, 30, 1e-4
+    out = []
+    for eager in ("0", "1"):
+        monkeypatch.setenv("SULI_EAGER_LOOPS", eager)
+        s = pkg.Solver(p)
+        init(s)
+        its = [s.step(it)["cg_iters"] for it in (1, 2)]
+        out.append((its, {f: s.download(f) for f in ("u", "v", "w", "prd1")}))
+        s.close()
+    assert out[0][0] == out[1][0]
+    for f in ("u", "v", "w", "prd1"):
+        assert np.array_equal(out[0][1][f], out[1][1][f]), f
+
+
 def test_mixed_rejects_unsupported(pkg):
     p = small_params(nx=15, ny=13, nz=11)   # cannot halve to <= 1024 cells
     p.precision, p.cg_stop = 1, 1
