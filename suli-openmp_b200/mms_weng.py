@@ -16,8 +16,8 @@ Host side only, as in the reference, where it is driver code around the hot path
                      and per RK stage visco, convdiff, tempo and contorno(2) only (graddin and
                      posdin are skipped when mms_t > 0, 1_principal.f90:89).
 
-`model` is a suli_b200.Solver or the CPU oracle: both expose the reference's subroutines, so the
-harness drives either one with the same sequence.
+`model` is a suli_b200.Solver, or any object with the same subroutine surface (the tests pass the
+CPU restatement used as their checker), driven by one sequence.
 
 The case: the reference's fluids (14_level_set.f90:25-31) and schemes, the domain
 [0, 2 pi]^2 x [0, lz] (mms_t = 1) or [-pi, pi]^2 x [0, lz] (mms_t = 2, the fields' own offsets),
