@@ -90,8 +90,11 @@ typedef struct suli_params {
     double mg_omega;                /* precision 1: damping of the multigrid Jacobi sweeps (0 = 0.9) */
     double mg_alpha;                /* precision 1: scale of the coarse-grid correction (0 = 1.8)     */
     int    mg_kernels;              /* precision 1: 0 = vectorised multigrid/PCG kernels (4 cells a
-                                       thread, float4 loads; default), 1 = one cell a thread (same
-                                       arithmetic, kept as the reference the tests compare with) */
+                                       thread, float4 loads) with the three coarsest levels in one
+                                       16-CTA cluster launch where their shapes allow (default);
+                                       1 = one cell a thread (same arithmetic, kept as the reference
+                                       the tests compare with); 2 = vectorised, every level its own
+                                       kernels */
     int    wave_t;                  /* wave inflow at x = 0: 0 none, 1 Stokes I, 2 Stokes II, 5 Stokes V (0_modules.f90:35) */
     int    outflow_fix;             /* 0 = the reference's outflow copy (3_contorno.f90:193-197, 362-409);
                                        1 (extension, needs ccxf = 4) = contorno(2) then shifts the

@@ -134,6 +134,7 @@ struct suli_ctx {
     suli::PCGState* pcg_host = nullptr;
     float* f32_arena = nullptr;
     int coarse_sweeps = 40;
+    bool cluster_ok = false;   // the device runs k_mg_cluster (16-CTA cluster with its shared memory)
     int inner_maxit = 200;
     int inner_batch = 4;
     int last_outer_iters = 0;
@@ -234,6 +235,7 @@ void launch_cg_setup(suli_ctx* c);
 void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new);
 void launch_cg_cond(suli_ctx* c, cudaGraphConditionalHandle h);
 void launch_cg_divcheck(suli_ctx* c);
+int cluster_ready(suli_ctx* c);
 void launch_cg_final(suli_ctx* c, const double* e);
 // ---- mixed-precision solve (k_mixed.cu) ----
 void launch_mx_setup(suli_ctx* c);

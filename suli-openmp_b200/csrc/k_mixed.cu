@@ -14,6 +14,8 @@
 // (not flexible) PCG applies.
 #include <cuda_runtime.h>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include "ctx.cuh"
 #include "pdl.cuh"
 #include "reduce.cuh"
@@ -595,6 +597,7 @@ __global__ void k_zero_f(float* a, long long n) {
 
 }  // namespace suli
 #include "k_mg_vec.cuh"
+#include "k_mg_cluster.cuh"
 namespace suli {
 
 // ------------------------------------------------------------------------------------
@@ -646,8 +649,8 @@ void launch_pcg_init(suli_ctx* c, int maxit) {
 
 static inline OpRho4 from_rho4(const MGLevel& L) { return OpRho4{L.rho, L.idg, L.c2}; }
 static inline OpStored4 stored4(const MGLevel& L) { return OpStored4{L.sx, L.sy, L.sz, L.idg}; }
-// the 4-cells-a-thread kernels on a level (mg_kernels = 0 and x divisible by 4)
-static inline bool vec_level(const suli_ctx* c, const Geo& g) { return c->P.mg_kernels == 0 && g.nx % kVX == 0; }
+// the 4-cells-a-thread kernels on a level (mg_kernels 0 or 2 and x divisible by 4)
+static inline bool vec_level(const suli_ctx* c, const Geo& g) { return c->P.mg_kernels != 1 && g.nx % kVX == 0; }
 
 // pre-smoothing and restriction of level l (level 0 forms its faces from the density)
 static void vc_down(suli_ctx* c, int l, const float* f, float om) {
@@ -709,12 +712,89 @@ static void vc_up(suli_ctx* c, int l, const float* f, float om, float alpha) {
     }
 }
 
+// The three coarsest levels run as one cluster launch (k_mg_cluster) when their shapes fit it,
+// the vectorised kernels are selected (mg_kernels = 0) and the device runs a 16-CTA cluster with
+// the kernel's shared memory (checked once, cluster_ready).
+static bool use_cluster(const suli_ctx* c) {
+    const int L = (int)c->mg.size();
+    return c->P.mg_kernels == 0 && c->cluster_ok && L >= 4 && vec_level(c, c->mg[L - 4].g) &&
+           cl_fits(c->mg[L - 3].g, c->mg[L - 2].g, c->mg[L - 1].g);
+}
+
+int cluster_ready(suli_ctx* c) {
+    c->cluster_ok = false;
+    if (const char* ev = std::getenv("SULI_NO_CLUSTER"))   // keep the per-level kernels
+        if (std::strcmp(ev, "1") == 0) return SULI_OK;
+    const int L = (int)c->mg.size();
+    if (L < 4 || !cl_fits(c->mg[L - 3].g, c->mg[L - 2].g, c->mg[L - 1].g)) return SULI_OK;
+    const size_t smem = cl_smem_bytes(c->mg[L - 3].g, c->mg[L - 2].g, c->mg[L - 1].g);
+    if (cudaFuncSetAttribute(k_mg_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return SULI_OK;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kClCTAs);
+    cfg.blockDim = dim3(kClThreads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClCTAs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_mg_cluster, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return SULI_OK;
+    }
+    c->cluster_ok = (n > 0);
+    return SULI_OK;
+}
+
+static void launch_cluster(suli_ctx* c, float om, float alpha) {
+    const int L = (int)c->mg.size();
+    const MGLevel &M = c->mg[L - 3], &C = c->mg[L - 2], &B = c->mg[L - 1];
+    ClArgs a;
+    a.M = ClLevel{M.g, M.sx, M.sy, M.sz, M.idg};
+    a.C = ClLevel{C.g, C.sx, C.sy, C.sz, C.idg};
+    a.B = ClLevel{B.g, B.sx, B.sy, B.sz, B.idg};
+    a.bc = c->bc;
+    a.fM = M.f;
+    a.yM = M.y;
+    a.omega = om;
+    a.alpha = alpha;
+    a.sweeps = c->coarse_sweeps;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kClCTAs);
+    cfg.blockDim = dim3(kClThreads);
+    cfg.dynamicSmemBytes = cl_smem_bytes(M.g, C.g, B.g);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClCTAs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 2;
+    cudaLaunchKernelEx(&cfg, k_mg_cluster, a, (const PCGState*)c->pcg);
+}
+
 // z = M r: one V-cycle; the last level-0 sweep also forms r.z and beta
 void launch_vcycle(suli_ctx* c) {
     const float om = (float)c->P.mg_omega;
     const float alpha = (float)c->P.mg_alpha;
     const int L = (int)c->mg.size();
     const BC bc = c->bc;
+    if (use_cluster(c)) {   // levels 0 .. L-4 as kernels per level, the last three in the cluster
+        for (int l = 0; l < L - 3; ++l) vc_down(c, l, l == 0 ? c->pc_r : c->mg[l].f, om);
+        launch_cluster(c, om, alpha);
+        for (int l = L - 4; l >= 0; --l) vc_up(c, l, l == 0 ? c->pc_r : c->mg[l].f, om, alpha);
+        return;
+    }
     for (int l = 0; l < L - 1; ++l) vc_down(c, l, l == 0 ? c->pc_r : c->mg[l].f, om);
     MGLevel& B = c->mg[L - 1];
     if (L == 1) {   // a single level: coarsest sweeps, then one more sweep that forms r.z
@@ -762,6 +842,7 @@ void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new) {
 
 int vcycle_kernels(const suli_ctx* c) {
     const int L = (int)c->mg.size();
+    if (use_cluster(c)) return 4 * (L - 3) + 1;
     return (L == 1) ? 2 : 4 * (L - 1) + 1;
 }
 

@@ -136,7 +136,7 @@ int validate(const suli_params* p, std::string& why) {
         if (!(p->inner_tol > 0 && p->inner_tol < 1)) { why = "inner_tol must lie in (0, 1)"; return SULI_ERR_ARG; }
         if (!(p->mg_omega >= 0 && p->mg_omega < 1)) { why = "mg_omega must lie in [0, 1)"; return SULI_ERR_ARG; }
         if (!(p->mg_alpha >= 0 && p->mg_alpha <= 2)) { why = "mg_alpha must lie in [0, 2]"; return SULI_ERR_ARG; }
-        if (p->mg_kernels != 0 && p->mg_kernels != 1) { why = "mg_kernels must be 0 or 1"; return SULI_ERR_ARG; }
+        if (p->mg_kernels < 0 || p->mg_kernels > 2) { why = "mg_kernels must be 0, 1 or 2"; return SULI_ERR_ARG; }
         int nx = p->nx, ny = p->ny, nz = p->nz;
         while ((long long)nx * ny * nz > 1024 && nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0 && nx >= 4 && ny >= 4 && nz >= 4) {
             nx /= 2; ny /= 2; nz /= 2;
@@ -281,6 +281,7 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
         if ((e = cudaMalloc(&c->pcg, sizeof(PCGState))) != cudaSuccess) return bail(e, "pcg state");
         if ((e = cudaMemsetAsync(c->pcg, 0, sizeof(PCGState), c->stream)) != cudaSuccess) return bail(e, "memset");
         if ((e = cudaMallocHost(&c->pcg_host, 2 * sizeof(PCGState))) != cudaSuccess) return bail(e, "pinned");
+        cluster_ready(c);
     }
     if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bail(e, "sync");
     c->dt = p->dt;

@@ -73,6 +73,47 @@ def test_mixed_steps_track_fp64(pkg, orc):
 
 
 @pytest.mark.parametrize("case", ["dam_break", "periodic"])
+def test_cluster_levels_match_per_level_kernels(pkg, case):
+    """The three coarsest levels in one 16-CTA cluster launch (mg_kernels = 0) against the same
+    levels as kernels per level (mg_kernels = 2): the same stages and per-cell arithmetic (only
+    the restriction to the coarsest grid adds its children in two halves), so the inner solves
+    follow the same course.  Walls (dam break 128x64x64, cluster levels 64x32x32 .. 16x8x8) and a
+    box periodic in every direction (64^3, so the z wrap crosses from the last CTA to the first),
+    two steps each: iteration counts within 2 per step, velocities within 1e-9 of their scale, and
+    the tracer shows the cluster path's launch count (7 kernels an inner iteration, not 15)."""
+    res = {}
+    for mk in (0, 2):
+        if case == "dam_break":
+            p, init = pkg.cases.dam_break(nx=128, ny=64, nz=64, dx=0.005, cg_tol=1e-10)
+            p.precision, p.inner_tol, p.refine_maxit = 1, 1e-4, 30
+            p.mg_kernels = mk
+            s = pkg.Solver(p)
+            init(s)
+            s.profile_enable(True)
+            steps = [s.step(it) for it in (1, 2)]
+        else:
+            m = pkg.cases.TaylorGreenMMS(64, precision=1)
+            m.p.mg_kernels = mk
+            s = pkg.Solver(m.p)
+            m.init(s)
+            s.profile_enable(True)
+            steps = [m.step(s, it) for it in (1, 2)]
+        prof = s.profile_read()
+        s.profile_enable(False)
+        assert all(st["status"] == 0 for st in steps)
+        iters = [sum(st["cg_iters"]) if isinstance(st["cg_iters"], list) else st["cg_iters"] for st in steps]
+        res[mk] = (iters, {f: s.download(f) for f in ("u", "v", "w")}, prof)
+        s.close()
+    (it0, v0, p0), (it2, v2, p2) = res[0], res[2]
+    assert all(abs(a - b) <= 2 for a, b in zip(it0, it2)), (it0, it2)
+    vs = max(float(np.abs(b).max()) for b in v2.values())
+    for f in v0:
+        assert float(np.abs(v0[f] - v2[f]).max()) <= 1e-9 * vs, f
+    per_it = lambda pr: pr["mg"]["launches"] / max(pr["cg_iterations"], 1)
+    assert per_it(p0) < 0.6 * per_it(p2), (per_it(p0), per_it(p2))
+
+
+@pytest.mark.parametrize("case", ["dam_break", "periodic"])
 def test_vector_kernels_match_one_cell_kernels(pkg, case):
     """The 4-cells-a-thread multigrid/PCG kernels (mg_kernels = 0) against the one-cell kernels
     (mg_kernels = 1): per cell the same arithmetic, only the FP64 dot products sum in another
