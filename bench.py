@@ -81,6 +81,8 @@ def parse_args():
     ap.add_argument("--c5-steps", type=int, default=4,
                     help="timed steps of the LES channel over a bump at 512x256x256 (0: skip)")
     ap.add_argument("--c5-n", default="512,256,256", help="grid of the LES channel block")
+    ap.add_argument("--c4-snapshots", type=int, default=3,
+                    help="held-out random tanks (two solves each) of the per-solve comparison at the bench grid (0: skip)")
     return ap.parse_args()
 
 
@@ -319,6 +321,61 @@ def c5_block(args, dist, pkg, dev):
     if "plain_fp64" in states and "learned" in states:
         out["learned"]["error_vs_plain_fp64"] = field_errors(states["learned"], states["plain_fp64"])
         out["learned"]["speedup_vs_plain_fp64"] = out["learned"]["value"] / out["plain_fp64"]["value"]
+    return out
+
+
+# ------------------------------------------------------------------------------ C4
+def c4_block(args, pkg, dev):
+    """Iterations and device time per pressure solve at the bench grid, to the same FP64
+    relative residual, on held-out random tanks (snapshots.SnapshotGenerator with seeds the
+    network was not trained on; each tank is solved from zero pressure and then again from that
+    solution with a correlated velocity field): the plain FP64 Jacobi-scaled CG of the reference,
+    the mixed FP32 multigrid-preconditioned solve, and the same with the learned initial guess."""
+    import torch
+    out = {"grid": f"{args.nx}x{args.ny}x{args.nz}", "cg_tol": args.cg_tol, "snapshots": args.c4_snapshots,
+           "seeds": [9001 + q for q in range(args.c4_snapshots)]}
+    net = None
+    for key, prec, learned in (("plain_jacobi_pcg_fp64", 0, False), ("mixed_multigrid_pcg", 1, False),
+                               ("mixed_multigrid_pcg_learned_guess", 1, True)):
+        q = pkg.snapshots.tank_params(n=args.nx, ny=args.ny, nz=args.nz, dx=args.dx, cg_tol=args.cg_tol, precision=prec)
+        if prec == 1:
+            q.refine_maxit, q.inner_tol = 30, args.inner_tol
+            q.mg_omega, q.mg_alpha = args.mg_omega, args.mg_alpha
+        s = pkg.Solver(q, device=dev)
+        if learned:
+            net, src = load_net(pkg, q, args, dev)
+            if net is None:
+                out[key] = {"skipped": src}
+                s.close()
+                continue
+            s.attach_nn(net)
+        ext = torch.cuda.ExternalStream(s.stream_ptr, device=dev)
+        its, ms, res = [], [], []
+        for seed in out["seeds"]:
+            gen = pkg.snapshots.SnapshotGenerator(s, seed)
+
+            def solve(k):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.synchronize()
+                e0.record(ext)
+                n, r = s.graddin()
+                e1.record(ext)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+                return n, r
+            for n, r in gen.solve_pair(gen.draw(), solve):
+                its.append(n)
+                res.append(r)
+        s.close()
+        out[key] = {"iters_per_solve": statistics.mean(its), "ms_per_solve": statistics.mean(ms),
+                    "iters": its, "resid_max": max(res),
+                    "iterations": "FP64 CG iterations" if prec == 0 else "inner FP32 PCG iterations"}
+    if net is not None:
+        net.close()
+    base = out.get("plain_jacobi_pcg_fp64", {}).get("ms_per_solve")
+    for k in ("mixed_multigrid_pcg", "mixed_multigrid_pcg_learned_guess"):
+        if base and "ms_per_solve" in out.get(k, {}):
+            out[k]["speedup_vs_plain_jacobi_pcg"] = base / out[k]["ms_per_solve"]
     return out
 
 
@@ -731,6 +788,7 @@ def run_ours(args):
     if dist.world == 1 and args.mms_n > 0:
         mms = mms_check(pkg, args, dev)
     c5 = c5_block(args, dist, pkg, dev) if args.c5_steps > 0 else None
+    c4 = c4_block(args, pkg, dev) if (args.c4_snapshots > 0 and dist.world == 1) else None
     if dist.rank == 0:
         desc = {"plain": "plain FP64: the reference's Jacobi-scaled CG",
                 "mixed": "mixed: FP32 stencils, FP32 multigrid-preconditioned inner CG inside FP64 iterative "
@@ -780,6 +838,8 @@ def run_ours(args):
             line["mms"] = mms
         if c5 is not None:
             line["c5_les_channel"] = c5
+        if c4 is not None:
+            line["c4_per_solve"] = c4
         line["kernel_gbs"] = class_bandwidth(p, head["kernels"])
         if "plain" in runs:
             line["kernel_gbs_plain_fp64"] = class_bandwidth(p, runs["plain"]["kernels"])

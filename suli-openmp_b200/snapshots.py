@@ -21,10 +21,14 @@ from .cases import _two_phase
 from ._abi import default_params
 
 
-def tank_params(n: int = 128, dx: float = 0.005, cg_tol: float = 1e-8, precision: int = 1):
-    """Closed tank, no-slip walls and a free-slip lid, as the sloshing case."""
+def tank_params(n: int = 128, dx: float = 0.005, cg_tol: float = 1e-8, precision: int = 1, ny: int | None = None,
+                nz: int | None = None):
+    """Closed tank, no-slip walls and a free-slip lid, as the sloshing case (n^3 cells, or
+    n x ny x nz)."""
     p = default_params()
-    p.nx = p.ny = p.nz = n
+    p.nx = n
+    p.ny = ny if ny else n
+    p.nz = nz if nz else n
     p.dx = p.dy = p.dz = dx
     p.ccx0 = p.ccxf = 2
     p.ccy0 = p.ccyf = 2
