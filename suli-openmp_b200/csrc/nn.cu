@@ -130,9 +130,10 @@ __global__ void k_head_fwd(long long V, const __nv_bfloat16* __restrict__ x, con
     for (int c = 0; c < 16; ++c) s += w[c] * __bfloat162float(x[v * 16 + c]);
     out[v] = s;
 }
-// head backward: dx[v][c] = w[c] dout[v]; dw[c] += sum_v x[v][c] dout[v]; db += sum dout
+// head backward: dx[v][c] = w[c] dout[v]; the block's sums of x[v][c] dout[v] and of dout into
+// part[block][0..16] (k_sum_parts adds them to dw, db)
 __global__ void k_head_bwd(long long V, const __nv_bfloat16* __restrict__ x, const float* __restrict__ w,
-                           const float* __restrict__ dout, __nv_bfloat16* __restrict__ dx, float* dw) {
+                           const float* __restrict__ dout, __nv_bfloat16* __restrict__ dx, float* part) {
     __shared__ float sh[17][8];
     const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     float g[17];
@@ -157,8 +158,18 @@ __global__ void k_head_bwd(long long V, const __nv_bfloat16* __restrict__ x, con
     if (threadIdx.x < 17) {
         float s = 0.f;
         for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s += sh[threadIdx.x][q];
-        atomicAdd(&dw[threadIdx.x], s);
+        part[(long long)blockIdx.x * 17 + threadIdx.x] = s;   // summed in block order by k_sum_parts
     }
+}
+
+// out[q] += sum over the nparts rows of part[row][q], rows in order (a fixed summation order,
+// so a gradient is the same from run to run)
+__global__ void k_sum_parts(long long nparts, long long width, const float* __restrict__ part, float* out) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= width) return;
+    float s = 0.f;
+    for (long long r = 0; r < nparts; ++r) s += part[r * width + q];
+    out[q] += s;
 }
 
 // W'[tap'][ci][co] = W[26 - tap'][co][ci]: weights of the input-gradient convolution
@@ -173,11 +184,14 @@ __global__ void k_flip_weights(int cin, int cout, const __nv_bfloat16* __restric
 }
 
 // weight gradient of one layer: dW[tap][co][ci] += sum_v X[v + off(tap)][ci] dZ[v][co];
-// a CTA owns one tap and a chunk of voxels; threads hold a (CO16 x CI16) register block.
+// a CTA owns one tap and a chunk of voxels; threads hold a (CO16 x CI16) register block.  Each
+// CTA writes its chunk's sums to its own row of part (row = chunk, 27 COUT CIN weights then COUT
+// biases); k_sum_parts adds the rows in chunk order, so there are no float atomics and the
+// gradient is reproducible.
 constexpr int kWgChunk = 4096, kWgSub = 32;
 template <int CO16, int CI16>
-__global__ void __launch_bounds__(256) k_wgrad(Vol vol, ConvIn in, const __nv_bfloat16* __restrict__ dz, float* dw,
-                                               float* db) {
+__global__ void __launch_bounds__(256) k_wgrad(Vol vol, ConvIn in, const __nv_bfloat16* __restrict__ dz,
+                                               float* part) {
     constexpr int COUT = CO16 * 16, CIN = CI16 * 16;
     __shared__ float sx[kWgSub][CIN + 1];
     __shared__ float sz[kWgSub][COUT + 1];
@@ -239,12 +253,12 @@ __global__ void __launch_bounds__(256) k_wgrad(Vol vol, ConvIn in, const __nv_bf
         }
         __syncthreads();
     }
+    float* row = part + (long long)blockIdx.x * (27LL * COUT * CIN + COUT);
 #pragma unroll
     for (int a = 0; a < CO16; ++a) {
 #pragma unroll
-        for (int b = 0; b < CI16; ++b)
-            atomicAdd(&dw[((long long)tap * COUT + tc + 16 * a) * CIN + ti + 16 * b], acc[a][b]);
-        if (ti == 0 && tap == 13) atomicAdd(&db[tc + 16 * a], bacc[a]);
+        for (int b = 0; b < CI16; ++b) row[((long long)tap * COUT + tc + 16 * a) * CIN + ti + 16 * b] = acc[a][b];
+        if (ti == 0 && tap == 13) row[27LL * COUT * CIN + tc + 16 * a] = bacc[a];
     }
 }
 
@@ -329,6 +343,9 @@ struct suli_nn {
     double* host_sums = nullptr;
     int* err_flag = nullptr;         // set by a tensor-core convolution whose wait timed out
     int kernel = 0;                  // convolution kernel: 0 tcgen05 pipeline, 1 mma.sync, 2 tcgen05 one tile per CTA
+    float* part = nullptr;           // per-CTA partial sums of the parameter gradient (training)
+    long long part_floats = 0;
+    bool grad_error = false;         // the partial-sum buffer could not be allocated
     std::string err;
 };
 
@@ -509,11 +526,30 @@ void conv(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, 
     }
 }
 
+// per-CTA rows of partial sums (k_wgrad, k_head_bwd), grown on demand (training only)
+float* part_buffer(suli_nn* N, long long floats) {
+    if (floats > N->part_floats) {
+        cudaFree(N->part);
+        N->part = nullptr;
+        N->part_floats = 0;
+        if (cudaMalloc(&N->part, floats * sizeof(float)) != cudaSuccess) return nullptr;
+        N->part_floats = floats;
+    }
+    return N->part;
+}
+
 template <int CO16, int CI16>
 void wgrad_launch(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* dz, float* dw, float* db) {
     const long long V = (long long)vol.nx * vol.ny * vol.nz;
-    const dim3 grid((unsigned)((V + kWgChunk - 1) / kWgChunk), 27);
-    k_wgrad<CO16, CI16><<<grid, 256, 0, N->stream>>>(vol, in, dz, dw, db);
+    const long long chunks = (V + kWgChunk - 1) / kWgChunk;
+    const long long width = 27LL * (CO16 * 16) * (CI16 * 16) + CO16 * 16;   // dw then db, contiguous
+    float* part = part_buffer(N, chunks * width);
+    if (!part) { N->grad_error = true; return; }
+    const dim3 grid((unsigned)chunks, 27);
+    k_wgrad<CO16, CI16><<<grid, 256, 0, N->stream>>>(vol, in, dz, part);
+    // the layer's bias follows its weights in the parameter vector (db == dw + 27 COUT CIN)
+    if (db != dw + 27LL * (CO16 * 16) * (CI16 * 16)) { N->grad_error = true; return; }
+    k_sum_parts<<<nb(width), 256, 0, N->stream>>>(chunks, width, part, dw);
 }
 void wgrad(suli_nn* N, const Vol& vol, const ConvIn& in, int cout, const __nv_bfloat16* dz, float* dw, float* db) {
     const int cin = in.ca + in.cb;
@@ -598,8 +634,13 @@ void backward(suli_nn* N) {
     // gradients w.r.t. each layer's output, accumulated where a tensor feeds two consumers
     for (int l = 0; l < kConv; ++l)
         k_zero_bf<<<nb(N->V[kLayer[l].level] * kLayer[l].cout), 256, 0, N->stream>>>(N->V[kLayer[l].level] * kLayer[l].cout, N->gact[l]);
-    k_head_bwd<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->a[13], N->w + N->off[kConv], N->dout, N->gact[13],
-                                                  N->g + N->off[kConv]);
+    {
+        float* part = part_buffer(N, (long long)nb(N->V[0]) * 17);
+        if (!part) { N->grad_error = true; return; }
+        k_head_bwd<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->a[13], N->w + N->off[kConv], N->dout,
+                                                      N->gact[13], part);
+        k_sum_parts<<<1, 32, 0, N->stream>>>((long long)nb(N->V[0]), 17, part, N->g + N->off[kConv]);
+    }
     for (int l = kConv - 1; l >= 0; --l) {
         const LayerSpec& L = kLayer[l];
         const Vol& vol = N->vol[L.level];
@@ -766,6 +807,7 @@ int suli_nn_destroy(suli_nn* N) {
     for (int l = 0; l < kConv; ++l) { cudaFree(N->a[l]); cudaFree(N->gact[l]); }
     for (int l = 0; l < kLevels - 1; ++l) cudaFree(N->pool[l]);
     cudaFree(N->gcat); cudaFree(N->gtmp); cudaFree(N->out); cudaFree(N->dout); cudaFree(N->sums);
+    cudaFree(N->part);
     cudaFree(N->err_flag);
     if (N->host_sums) cudaFreeHost(N->host_sums);
     if (N->stream) cudaStreamDestroy(N->stream);
@@ -814,7 +856,9 @@ int suli_nn_loss_grad(suli_nn* N, const float* d_in3, const float* d_target, dou
     k_loss_sums<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->out, d_target, N->sums);
     k_loss_grad<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->out, d_target, N->dout);
     cudaMemsetAsync(N->g, 0, N->nparam * 4, N->stream);
+    N->grad_error = false;
     backward(N);
+    if (N->grad_error) return SULI_ERR_NOMEM;
     cudaMemcpyAsync(N->host_sums, N->sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, N->stream);
     if (host_grad) cudaMemcpyAsync(host_grad, N->g, N->nparam * 4, cudaMemcpyDeviceToHost, N->stream);
     if (int r = nn_sync(N)) return r;
