@@ -140,7 +140,9 @@ def test_errors_fall_under_refinement(orc):
 @pytest.mark.parametrize("mt", [1, 2])
 def test_error_norms_gpu(orc, mt):
     """Ten steps of each case on the GPU and on the oracle: every error norm of mms() within
-    1e-9 relative (or 1e-15 absolute), the velocities within 1e-10 of their scale."""
+    1e-9 of the largest one (w is 0 in the exact field for a = 0, so its error is rounding noise
+    of order 1e-11 on both sides), the velocities within 1e-10 of the velocity scale and the
+    level set of its own."""
     mg = W.WengMMS(mt, nx=32, ny=32, nz=24, dt=2e-3)
     mo = W.WengMMS(mt, nx=32, ny=32, nz=24, dt=2e-3)
     g = pkg.Solver(mg.p)
@@ -149,9 +151,13 @@ def test_error_norms_gpu(orc, mt):
     mo.init(o)
     for it in range(1, 11):
         eg, eo = mg.step(g, it), mo.step(o, it)
+        scale = max(eo["u"], eo["v"], eo["w"], 1e-300)
         for k in ("u", "v", "w", "p"):
-            assert abs(eg[k] - eo[k]) <= max(1e-9 * abs(eo[k]), 1e-15), (it, k, eg[k], eo[k])
+            assert abs(eg[k] - eo[k]) <= 1e-9 * scale, (it, k, eg[k], eo[k])
     assert mg.erro_t == pytest.approx(mo.erro_t, rel=1e-9)
-    for f in ("u", "v", "w", "ls"):
-        assert rel_err(g.download(f), o.download(f)) <= 1e-10, f
+    vel = {f: (g.download(f), o.download(f)) for f in ("u", "v", "w")}
+    vs = max(float(np.abs(b).max()) for _, b in vel.values())
+    for f, (a, b) in vel.items():
+        assert float(np.abs(a - b).max()) <= 1e-10 * vs, f
+    assert rel_err(g.download("ls"), o.download("ls")) <= 1e-10
     g.close()
