@@ -61,7 +61,7 @@ def parse_args():
     ap.add_argument("--cg-tol", type=float, default=1e-8)
     ap.add_argument("--div-tol", type=float, default=1e-8,
                     help="second stopping test of every Poisson solve: max |div u| after the projection")
-    ap.add_argument("--inner-tol", type=float, default=1e-4, help="relative tolerance of each FP32 inner solve")
+    ap.add_argument("--inner-tol", type=float, default=1e-3, help="relative tolerance of each FP32 inner solve")
     ap.add_argument("--mg-omega", type=float, default=0.9, help="damping of the multigrid Jacobi sweeps")
     ap.add_argument("--mg-alpha", type=float, default=1.8, help="scale of the multigrid coarse-grid correction")
     ap.add_argument("--path", choices=["all", "plain", "mixed", "learned"], default="all",

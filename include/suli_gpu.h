@@ -146,6 +146,8 @@ enum suli_scalar {
     SULI_S_T,           /* disc t */
     SULI_S_NTT,         /* number of RK stages (2_iniciais.f90:85-104) */
     SULI_S_A_DT1, SULI_S_A_DT2, SULI_S_A_DT3,
+    SULI_S_FALLBACKS,   /* read only, no counterpart in the reference: precision-1 solves that the
+                           plain FP64 CG finished because the FP32 refinement stopped converging */
     SULI_S_COUNT
 };
 

@@ -1712,6 +1712,7 @@ int orc_set_scalar(void* h, int id, double val) {
     }
 }
 int orc_get_scalar(void* h, int id, double* val) {
+    if (id == SULI_S_FALLBACKS) { *val = 0.; return 0; }   /* the restatement solves in FP64 only */
     Oracle* o = static_cast<Oracle*>(h);
     switch (id) {
     case SULI_S_DT: *val = o->dt; return 0;

@@ -94,7 +94,7 @@ FIELD_NAMES = [
 FIELD = {n: i for i, n in enumerate(FIELD_NAMES)}
 FIELD_COUNT = len(FIELD_NAMES)
 
-SCALAR_NAMES = ["dt", "vol_ini", "vol_ins", "dt1", "t", "ntt", "a_dt1", "a_dt2", "a_dt3"]
+SCALAR_NAMES = ["dt", "vol_ini", "vol_ins", "dt1", "t", "ntt", "a_dt1", "a_dt2", "a_dt3", "fallbacks"]
 SCALAR = {n: i for i, n in enumerate(SCALAR_NAMES)}
 
 

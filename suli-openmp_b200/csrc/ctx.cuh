@@ -138,6 +138,7 @@ struct suli_ctx {
     int inner_maxit = 200;
     int inner_batch = 4;
     int last_outer_iters = 0;
+    long long fallbacks = 0;   // mixed solves finished by the plain FP64 CG (the refinement stalled)
     // one CUDA graph per ping-pong parity holding a whole inner PCG iteration
     // the inner PCG loop as one graph: a WHILE node repeats two iterations (ping-pong) and a
     // kernel that clears the condition once the inner solve is done

@@ -399,6 +399,7 @@ int suli_set_scalar(suli_ctx* c, int id, double v) {
     case SULI_S_A_DT1: c->a_dt[0] = v; return SULI_OK;
     case SULI_S_A_DT2: c->a_dt[1] = v; return SULI_OK;
     case SULI_S_A_DT3: c->a_dt[2] = v; return SULI_OK;
+    case SULI_S_FALLBACKS: return fail(c, SULI_ERR_ARG, "fallbacks is read only");
     default: return fail(c, SULI_ERR_ARG, "set_scalar: bad id");
     }
 }
@@ -415,6 +416,7 @@ int suli_get_scalar(suli_ctx* c, int id, double* v) {
     case SULI_S_A_DT1: *v = c->a_dt[0]; return SULI_OK;
     case SULI_S_A_DT2: *v = c->a_dt[1]; return SULI_OK;
     case SULI_S_A_DT3: *v = c->a_dt[2]; return SULI_OK;
+    case SULI_S_FALLBACKS: *v = (double)c->fallbacks; return SULI_OK;
     default: return fail(c, SULI_ERR_ARG, "get_scalar: bad id");
     }
 }
@@ -735,80 +737,13 @@ void nn_begin(suli_ctx* c) {
     launch_nn_step(c, c->nn_out, c->cg_e);
 }
 
-int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
-    if (int rg = ensure_pcg_loop(c)) return rg;
-    launch_cg_setup(c);   // FP64 diagonal, coefficients, b~, first residual and threshold
-    launch_mx_setup(c);   // FP32 faces of every multigrid level
-    nn_begin(c);
-    double* ecur = c->cg_e;
-    double* enext = c->cg_e2;
-    launch_mx_residual(c, ecur, enext, false);
-    std::swap(ecur, enext);
-    CHECK_LAUNCH(c);
-    long long inner_total = 0;
-    int outer = 0, status = SULI_OK;
-    while (true) {
-        int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
-        if (r != SULI_OK) return r;
-        if (c->cg_host[0].status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the Poisson solve");
-        if (c->cg_host[0].done) break;
-        if (outer >= c->P.refine_maxit) { status = SULI_WARN_CG_MAXIT; break; }
-        launch_pcg_init(c, c->inner_maxit);
-        {
-            ProfScope ps(c, SULI_K_MG, vcycle_kernels(c));
-            launch_vcycle(c);
-        }
-        launch_pcg_iter(c, c->mg[0].y, c->pc_pa);   // p_old = z with beta = 0
-        if (c->use_graphs) {
-            ProfScope ps(c, SULI_K_MG, 0);   // kernel launches are counted below, once known
-            CUDA_TRY(c, cudaGraphLaunch(c->pcg_loop, c->stream));
-        } else {
-            for (int pair = 0; pair < c->inner_maxit; ++pair) {
-                launch_pcg_iter(c, c->pc_pa, c->pc_pb);
-                launch_pcg_iter(c, c->pc_pb, c->pc_pa);
-                CHECK_LAUNCH(c);
-                if (int rr = sync_read(c, c->pcg, c->pcg_host, sizeof(PCGState))) return rr;
-                if (c->pcg_host[0].done) break;
-            }
-        }
-        r = sync_read(c, c->pcg, c->pcg_host, sizeof(PCGState));
-        if (r != SULI_OK) return r;
-        if (c->pcg_host[0].status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the inner solve");
-        inner_total += c->pcg_host[0].iters;
-        if (c->use_graphs) {   // eager launches were counted as they went
-            const long long bodies = std::max(1, (c->pcg_host[0].iters - 1 + 1) / 2);
-            c->prof.launches[SULI_K_MG] += bodies * (2LL * c->pcg_graph_kernels + 1);
-        }
-        launch_mx_residual(c, ecur, enext, true);
-        std::swap(ecur, enext);
-        CHECK_LAUNCH(c);
-        ++outer;
-    }
-    c->last_outer_iters = outer;
-    if (c->nn && c->nn_mode == 1 && !c->rec_in && suli::nn::take_error(c->nn))
-        return fail(c, SULI_ERR_CUDA, "graddin: the network's tensor-core convolution timed out");
-    launch_cg_final(c, ecur);
-    if (c->rec_in) launch_nn_target(c, ecur, c->rec_target);
-    CHECK_LAUNCH(c);
-    int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
-    if (r != SULI_OK) return r;
-    const CGState& s = c->cg_host[0];
-    c->prof.cg_iters += inner_total;
-    if (iters) *iters = (int)inner_total;
-    if (resid) *resid = (s.bb > 0.) ? std::sqrt(s.rr / s.bb) : 0.;
-    return status;
-}
-}  // namespace
-
-extern "C" {
-
-int suli_graddin(suli_ctx* c, int* iters, double* resid) {
-    if (!c) return SULI_ERR_ARG;
-    cudaSetDevice(c->device);
-    if (c->P.precision == 1) return graddin_mixed(c, iters, resid);
+// The plain FP64 Jacobi-scaled CG (9_grad.f90:118-264) from prd1: set-up, the device-side loop,
+// the divergence test's resumptions, de-normalisation.  `record` takes a training pair
+// (suli_graddin_record).
+int graddin_fp64(suli_ctx* c, int* iters, double* resid, bool record) {
     if (int rg = ensure_cg_loop(c)) return rg;
     launch_cg_setup(c);
-    nn_begin(c);   // recording only: the learned guess needs the refinement loop
+    if (record) nn_begin(c);   // recording only: the learned guess needs the refinement loop
     CHECK_LAUNCH(c);
     // iteration 1 uses p_old = r with beta = 0 (erroppr = erropr, :172); then the device loop
     launch_cg_iter(c, c->cg_r, c->cg_pa);
@@ -848,7 +783,7 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
         CHECK_LAUNCH(c);
     }
     launch_cg_final(c, c->cg_e);
-    if (c->rec_in) launch_nn_target(c, c->cg_e, c->rec_target);
+    if (record && c->rec_in) launch_nn_target(c, c->cg_e, c->rec_target);
     CHECK_LAUNCH(c);
     int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
     if (r != SULI_OK) return r;
@@ -863,6 +798,107 @@ int suli_graddin(suli_ctx* c, int* iters, double* resid) {
     if (resid) *resid = (s.bb > 0.) ? std::sqrt(s.rr / s.bb) : 0.;
     if (s.status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the Poisson solve");
     return s.status;
+}
+
+int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
+    if (int rg = ensure_pcg_loop(c)) return rg;
+    launch_cg_setup(c);   // FP64 diagonal, coefficients, b~, first residual and threshold
+    launch_mx_setup(c);   // FP32 faces of every multigrid level
+    nn_begin(c);
+    double* ecur = c->cg_e;
+    double* enext = c->cg_e2;
+    launch_mx_residual(c, ecur, enext, false);
+    std::swap(ecur, enext);
+    CHECK_LAUNCH(c);
+    long long inner_total = 0;
+    int outer = 0, status = SULI_OK;
+    bool fallback = false;
+    double rr_prev = -1.;
+    bool inner_capped = false;
+    while (true) {
+        int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
+        if (r != SULI_OK) return r;
+        if (c->cg_host[0].status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the Poisson solve");
+        if (c->cg_host[0].done) break;
+        // a pass that did not halve the FP64 residual, or an inner solve that hit its cap: the
+        // FP32 inner solve no longer helps; the plain FP64 CG finishes from the better iterate
+        const double rr_now = c->cg_host[0].rr;
+        if (rr_prev >= 0. && (rr_now > 0.5 * rr_prev || inner_capped)) {
+            if (rr_now > rr_prev) std::swap(ecur, enext);   // the pass made it worse: keep the one before
+            fallback = true;
+            break;
+        }
+        rr_prev = rr_now;
+        if (outer >= c->P.refine_maxit) { status = SULI_WARN_CG_MAXIT; break; }
+        launch_pcg_init(c, c->inner_maxit);
+        {
+            ProfScope ps(c, SULI_K_MG, vcycle_kernels(c));
+            launch_vcycle(c);
+        }
+        launch_pcg_iter(c, c->mg[0].y, c->pc_pa);   // p_old = z with beta = 0
+        if (c->use_graphs) {
+            ProfScope ps(c, SULI_K_MG, 0);   // kernel launches are counted below, once known
+            CUDA_TRY(c, cudaGraphLaunch(c->pcg_loop, c->stream));
+        } else {
+            for (int pair = 0; pair < c->inner_maxit; ++pair) {
+                launch_pcg_iter(c, c->pc_pa, c->pc_pb);
+                launch_pcg_iter(c, c->pc_pb, c->pc_pa);
+                CHECK_LAUNCH(c);
+                if (int rr = sync_read(c, c->pcg, c->pcg_host, sizeof(PCGState))) return rr;
+                if (c->pcg_host[0].done) break;
+            }
+        }
+        r = sync_read(c, c->pcg, c->pcg_host, sizeof(PCGState));
+        if (r != SULI_OK) return r;
+        if (c->pcg_host[0].status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the inner solve");
+        inner_total += c->pcg_host[0].iters;
+        inner_capped = (c->pcg_host[0].iters >= c->inner_maxit);
+        if (c->use_graphs) {   // eager launches were counted as they went
+            const long long bodies = std::max(1, (c->pcg_host[0].iters - 1 + 1) / 2);
+            c->prof.launches[SULI_K_MG] += bodies * (2LL * c->pcg_graph_kernels + 1);
+        }
+        launch_mx_residual(c, ecur, enext, true);
+        std::swap(ecur, enext);
+        CHECK_LAUNCH(c);
+        ++outer;
+    }
+    c->last_outer_iters = outer;
+    if (c->nn && c->nn_mode == 1 && !c->rec_in && suli::nn::take_error(c->nn))
+        return fail(c, SULI_ERR_CUDA, "graddin: the network's tensor-core convolution timed out");
+    if (fallback) {   // prd1 from the iterate, then the FP64 CG to the same stopping tests
+        launch_cg_final(c, ecur);
+        int n64 = 0;
+        double res64 = 0.;
+        const int rf = graddin_fp64(c, &n64, &res64, false);
+        ++c->fallbacks;
+        if (rf < 0) return rf;
+        if (c->rec_in) launch_nn_target(c, c->cg_e, c->rec_target);
+        CHECK_LAUNCH(c);
+        c->prof.cg_iters += inner_total;
+        if (iters) *iters = (int)(inner_total + n64);
+        if (resid) *resid = res64;
+        return rf;
+    }
+    launch_cg_final(c, ecur);
+    if (c->rec_in) launch_nn_target(c, ecur, c->rec_target);
+    CHECK_LAUNCH(c);
+    int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
+    if (r != SULI_OK) return r;
+    const CGState& s = c->cg_host[0];
+    c->prof.cg_iters += inner_total;
+    if (iters) *iters = (int)inner_total;
+    if (resid) *resid = (s.bb > 0.) ? std::sqrt(s.rr / s.bb) : 0.;
+    return status;
+}
+}  // namespace
+
+extern "C" {
+
+int suli_graddin(suli_ctx* c, int* iters, double* resid) {
+    if (!c) return SULI_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->P.precision == 1) return graddin_mixed(c, iters, resid);
+    return graddin_fp64(c, iters, resid, true);
 }
 
 int suli_attach_nn(suli_ctx* c, suli_nn* net, int mode) {

@@ -189,6 +189,22 @@ def test_divergence_stopping_test_gpu(pkg, orc, precision):
     g.close()
 
 
+def test_stalled_refinement_falls_back_to_fp64_cg(pkg):
+    """The sloshing tank at 256x128x128 with inner solves to 1e-4 and the divergence test: later
+    refinement passes stop converging (the FP32 inner solve hits its cap on the small, rough
+    residuals), and the plain FP64 CG finishes those solves from the better iterate.  Every step
+    still meets both stopping tests, and the fallback count says it happened."""
+    p, init = pkg.cases.sloshing(cg_tol=1e-8, div_tol=1e-8)
+    p.precision, p.refine_maxit, p.inner_tol = 1, 30, 1e-4
+    s = pkg.Solver(p)
+    init(s)
+    for it in (1, 2, 3):
+        st = s.step(it)
+        assert st["status"] == 0 and max(st["cg_resid"]) <= 1e-8 and st["max_div"] <= 1e-8, st
+    assert s.get_scalar("fallbacks") >= 1
+    s.close()
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 def test_eager_loops_match_graph_loops(pkg, precision, monkeypatch):
     """SULI_EAGER_LOOPS=1 (a profiling aid: iterations launched from the host instead of the
