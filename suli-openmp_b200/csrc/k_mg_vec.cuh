@@ -105,12 +105,12 @@ __device__ __forceinline__ void apply4(const Faces (&F)[kVX], const float (&xc)[
 }
 
 // two damped Jacobi sweeps from zero (k_mg_pre): x1 = w f/dg, y = x1 + w (f - A x1)/dg
-template <class Op4>
-__global__ void __launch_bounds__(256, 3) k_mgv_pre(Geo G, BC bc, const float* __restrict__ f, Op4 A,
+template <int KZ, class Op4>
+__global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_mgv_pre(Geo G, BC bc, const float* __restrict__ f, Op4 A,
                                                  float* __restrict__ y, float omega, const PCGState* st) {
     pdl_wait();
     if (st->done) return;
-    const VQ q = vquad(G, bc, kKZ);
+    const VQ q = vquad(G, bc, KZ);
     if (!q.in) return;
     const int pxy = (int)G.pxy;
     auto x1 = [&](int cc, float (&o)[kVX]) {
@@ -119,11 +119,11 @@ __global__ void __launch_bounds__(256, 3) k_mgv_pre(Geo G, BC bc, const float* _
         for (int e = 0; e < kVX; ++e) o[e] = omega * fv.v[e] * dv.v[e];
     };
     auto x1s = [&](int cc) { return omega * f[cc] * A.idg[cc]; };
-    float col[kKZ + 2][kVX];
+    float col[KZ + 2][kVX];
 #pragma unroll
-    for (int m = 0; m < kKZ + 2; ++m) x1(q.c0 + pxy * map_any(q.k0 - 1 + m, G.nz, bc.perz), col[m]);
+    for (int m = 0; m < KZ + 2; ++m) x1(q.c0 + pxy * map_any(q.k0 - 1 + m, G.nz, bc.perz), col[m]);
 #pragma unroll
-    for (int m = 0; m < kKZ; ++m) {
+    for (int m = 0; m < KZ; ++m) {
         const int k = q.k0 + m;
         if (k > G.nz) break;
         const int c = q.c0 + pxy * k;
@@ -141,26 +141,26 @@ __global__ void __launch_bounds__(256, 3) k_mgv_pre(Geo G, BC bc, const float* _
 }
 
 // x_out = x_in + w (f - A x_in)/dg; with do_dot also f.x_out -> rz, beta (k_mg_jacc)
-template <class Op4>
-__global__ void __launch_bounds__(256, 3) k_mgv_jacc(Geo G, BC bc, const float* __restrict__ xin,
+template <int KZ, class Op4>
+__global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_mgv_jacc(Geo G, BC bc, const float* __restrict__ xin,
                                                   const float* __restrict__ f, Op4 A, float* __restrict__ xout,
                                                   float omega, PCGState* st, int do_dot, double* partial,
                                                   unsigned int* counter) {
     pdl_wait();
     if (st->done) return;
-    const VQ q = vquad(G, bc, kKZ);
+    const VQ q = vquad(G, bc, KZ);
     double dot = 0.;
     if (q.in) {
         const int pxy = (int)G.pxy;
-        float col[kKZ + 2][kVX];
+        float col[KZ + 2][kVX];
 #pragma unroll
-        for (int m = 0; m < kKZ + 2; ++m) {
+        for (int m = 0; m < KZ + 2; ++m) {
             const V4 t = ld4(xin, q.c0 + pxy * map_any(q.k0 - 1 + m, G.nz, bc.perz));
 #pragma unroll
             for (int e = 0; e < kVX; ++e) col[m][e] = t.v[e];
         }
 #pragma unroll
-        for (int m = 0; m < kKZ; ++m) {
+        for (int m = 0; m < KZ; ++m) {
             const int k = q.k0 + m;
             if (k > G.nz) break;
             const int c = q.c0 + pxy * k;
@@ -190,14 +190,14 @@ __global__ void __launch_bounds__(256, 3) k_mgv_jacc(Geo G, BC bc, const float* 
 }
 
 // x_out = x' + w (f - A x')/dg with x' = y + a P xc (k_mg_post)
-template <class Op4>
-__global__ void __launch_bounds__(256, 3) k_mgv_post(Geo Gf, Geo Gc, BC bc, const float* __restrict__ y,
+template <int KZ, class Op4>
+__global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_mgv_post(Geo Gf, Geo Gc, BC bc, const float* __restrict__ y,
                                                   const float* __restrict__ xc, const float* __restrict__ f, Op4 A,
                                                   float* __restrict__ xout, float omega, float alpha,
                                                   const PCGState* st) {
     pdl_wait();
     if (st->done) return;
-    const VQ q = vquad(Gf, bc, kKZ);
+    const VQ q = vquad(Gf, bc, KZ);
     if (!q.in) return;
     const int pxy = (int)Gf.pxy;
     // x' of the quad in row jj (fine j index, already ghost-mapped) and plane kk (mapped), at
@@ -215,14 +215,14 @@ __global__ void __launch_bounds__(256, 3) k_mgv_post(Geo Gf, Geo Gc, BC bc, cons
     };
     const int ixm = map_any(q.i0 - 1, Gf.nx, bc.perx), ixp = map_any(q.i0 + kVX, Gf.nx, bc.perx);
     const int jym = map_any(q.j - 1, Gf.ny, bc.pery), jyp = map_any(q.j + 1, Gf.ny, bc.pery);
-    float col[kKZ + 2][kVX];
+    float col[KZ + 2][kVX];
 #pragma unroll
-    for (int m = 0; m < kKZ + 2; ++m) {
+    for (int m = 0; m < KZ + 2; ++m) {
         const int k = map_any(q.k0 - 1 + m, Gf.nz, bc.perz);
         xq(q.c0 + pxy * k, q.j, k, col[m]);
     }
 #pragma unroll
-    for (int m = 0; m < kKZ; ++m) {
+    for (int m = 0; m < KZ; ++m) {
         const int k = q.k0 + m;
         if (k > Gf.nz) break;
         const int c = q.c0 + pxy * k;
@@ -279,15 +279,15 @@ __global__ void __launch_bounds__(256, 3) k_mgv_restrict(Geo Gf, Geo Gc, BC bc, 
 static inline dim3 vgrid_restrict(const Geo& gc) { return dim3((gc.nx / 2 + 31) / 32, (gc.ny + 7) / 8, gc.nz); }
 
 // p = z + beta p_old (also at the neighbours), q = A p, p.q -> alpha (k_pcg_spmvc)
-template <class Op4>
-__global__ void __launch_bounds__(256, 3) k_pcgv_spmvc(Geo G, BC bc, const float* __restrict__ z,
+template <int KZ, class Op4>
+__global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_pcgv_spmvc(Geo G, BC bc, const float* __restrict__ z,
                                                     const float* __restrict__ p_old, float* __restrict__ p_new,
                                                     float* __restrict__ qv, Op4 A, PCGState* st, double* partial,
                                                     unsigned int* counter) {
     pdl_wait();
     if (st->done) return;
     const float beta = (float)st->beta;
-    const VQ q = vquad(G, bc, kKZ);
+    const VQ q = vquad(G, bc, KZ);
     double dot = 0.;
     if (q.in) {
         const int pxy = (int)G.pxy;
@@ -297,11 +297,11 @@ __global__ void __launch_bounds__(256, 3) k_pcgv_spmvc(Geo G, BC bc, const float
             for (int e = 0; e < kVX; ++e) o[e] = a.v[e] + beta * b.v[e];
         };
         auto pns = [&](int cc) { return z[cc] + beta * p_old[cc]; };
-        float col[kKZ + 2][kVX];
+        float col[KZ + 2][kVX];
 #pragma unroll
-        for (int m = 0; m < kKZ + 2; ++m) pn(q.c0 + pxy * map_any(q.k0 - 1 + m, G.nz, bc.perz), col[m]);
+        for (int m = 0; m < KZ + 2; ++m) pn(q.c0 + pxy * map_any(q.k0 - 1 + m, G.nz, bc.perz), col[m]);
 #pragma unroll
-        for (int m = 0; m < kKZ; ++m) {
+        for (int m = 0; m < KZ; ++m) {
             const int k = q.k0 + m;
             if (k > G.nz) break;
             const int c = q.c0 + pxy * k;

@@ -648,6 +648,12 @@ void launch_pcg_init(suli_ctx* c, int maxit) {
 }
 
 static inline OpRho4 from_rho4(const MGLevel& L) { return OpRho4{L.rho, L.idg, L.c2}; }
+// launch a column kernel of the vectorised family with the context's column depth (2 or 4)
+#define VLAUNCH(kern, Op, G, ...)                                                                          \
+    do {                                                                                                   \
+        if (c->mg_kz == 2) pdl_launch(kern<2, Op>, vgrid((G), 2), kB2, c->stream, __VA_ARGS__);            \
+        else pdl_launch(kern<4, Op>, vgrid((G), 4), kB2, c->stream, __VA_ARGS__);                         \
+    } while (0)
 static inline OpStored4 stored4(const MGLevel& L) { return OpStored4{L.sx, L.sy, L.sz, L.idg}; }
 // the 4-cells-a-thread kernels on a level (mg_kernels 0 or 2 and x divisible by 4)
 static inline bool vec_level(const suli_ctx* c, const Geo& g) { return c->P.mg_kernels != 1 && g.nx % kVX == 0; }
@@ -659,11 +665,11 @@ static void vc_down(suli_ctx* c, int l, const float* f, float om) {
     const BC bc = c->bc;
     if (vec_level(c, M.g)) {
         if (l == 0) {
-            pdl_launch(k_mgv_pre<OpRho4>, vgrid(M.g, kKZ), kB2, c->stream, M.g, bc, f, from_rho4(M), M.y, om, c->pcg);
+            VLAUNCH(k_mgv_pre, OpRho4, M.g, M.g, bc, f, from_rho4(M), M.y, om, c->pcg);
             pdl_launch(k_mgv_restrict<OpRho4>, vgrid_restrict(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, from_rho4(M),
                        C.f, c->pcg);
         } else {
-            pdl_launch(k_mgv_pre<OpStored4>, vgrid(M.g, kKZ), kB2, c->stream, M.g, bc, f, stored4(M), M.y, om, c->pcg);
+            VLAUNCH(k_mgv_pre, OpStored4, M.g, M.g, bc, f, stored4(M), M.y, om, c->pcg);
             pdl_launch(k_mgv_restrict<OpStored4>, vgrid_restrict(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, stored4(M),
                        C.f, c->pcg);
         }
@@ -685,17 +691,14 @@ static void vc_up(suli_ctx* c, int l, const float* f, float om, float alpha) {
     const BC bc = c->bc;
     const int dot = (l == 0) ? 1 : 0;
     if (vec_level(c, M.g)) {
-        const dim3 g = vgrid(M.g, kKZ);
         if (l == 0) {
-            pdl_launch(k_mgv_post<OpRho4>, g, kB2, c->stream, M.g, C.g, bc, M.y, C.y, f, from_rho4(M), M.x, om, alpha,
-                       c->pcg);
-            pdl_launch(k_mgv_jacc<OpRho4>, g, kB2, c->stream, M.g, bc, M.x, f, from_rho4(M), M.y, om, c->pcg, dot,
-                       c->red_partial, c->red_counter);
+            VLAUNCH(k_mgv_post, OpRho4, M.g, M.g, C.g, bc, M.y, C.y, f, from_rho4(M), M.x, om, alpha, c->pcg);
+            VLAUNCH(k_mgv_jacc, OpRho4, M.g, M.g, bc, M.x, f, from_rho4(M), M.y, om, c->pcg, dot, c->red_partial,
+                    c->red_counter);
         } else {
-            pdl_launch(k_mgv_post<OpStored4>, g, kB2, c->stream, M.g, C.g, bc, M.y, C.y, f, stored4(M), M.x, om, alpha,
-                       c->pcg);
-            pdl_launch(k_mgv_jacc<OpStored4>, g, kB2, c->stream, M.g, bc, M.x, f, stored4(M), M.y, om, c->pcg, dot,
-                       c->red_partial, c->red_counter);
+            VLAUNCH(k_mgv_post, OpStored4, M.g, M.g, C.g, bc, M.y, C.y, f, stored4(M), M.x, om, alpha, c->pcg);
+            VLAUNCH(k_mgv_jacc, OpStored4, M.g, M.g, bc, M.x, f, stored4(M), M.y, om, c->pcg, dot, c->red_partial,
+                    c->red_counter);
         }
         return;
     }
@@ -723,6 +726,9 @@ static bool use_cluster(const suli_ctx* c) {
 
 int cluster_ready(suli_ctx* c) {
     c->cluster_ok = false;
+    c->mg_kz = 4;
+    if (const char* ev = std::getenv("SULI_MG_KZ"))   // column depth of the vectorised kernels
+        if (std::strcmp(ev, "2") == 0) c->mg_kz = 2;
     if (const char* ev = std::getenv("SULI_NO_CLUSTER"))   // keep the per-level kernels
         if (std::strcmp(ev, "1") == 0) return SULI_OK;
     const int L = (int)c->mg.size();
@@ -815,8 +821,8 @@ void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new) {
         ProfScope ps(c, SULI_K_CG_SPMV, 1);
         if (c->mg.size() > 1) {
             if (vec)
-                pdl_launch(k_pcgv_spmvc<OpRho4>, vgrid(G, kKZ), kB2, c->stream, G, c->bc, M0.y, p_old, p_new, c->pc_q,
-                           from_rho4(M0), c->pcg, c->red_partial, c->red_counter);
+                VLAUNCH(k_pcgv_spmvc, OpRho4, G, G, c->bc, M0.y, p_old, p_new, c->pc_q, from_rho4(M0), c->pcg,
+                        c->red_partial, c->red_counter);
             else
                 pdl_launch(k_pcg_spmvc<OpRho>, colgrid(G), kB2, c->stream, G, c->bc, M0.y, p_old, p_new, c->pc_q,
                            from_rho(M0), c->pcg, c->red_partial, c->red_counter);

@@ -113,6 +113,28 @@ def test_cluster_levels_match_per_level_kernels(pkg, case):
     assert per_it(p0) < 0.6 * per_it(p2), (per_it(p0), per_it(p2))
 
 
+def test_column_depths_agree(pkg, monkeypatch):
+    """The vectorised kernels with 2 cells along z a thread (SULI_MG_KZ=2) against 4 (default):
+    the same per-cell arithmetic, the FP64 dot products grouped differently; dam break
+    128x64x64, two steps: iteration counts within 2, velocities within 1e-9 of their scale."""
+    res = {}
+    for kz in ("4", "2"):
+        monkeypatch.setenv("SULI_MG_KZ", kz)
+        p, init = pkg.cases.dam_break(nx=128, ny=64, nz=64, dx=0.005, cg_tol=1e-10)
+        p.precision, p.inner_tol, p.refine_maxit = 1, 1e-4, 30
+        s = pkg.Solver(p)
+        init(s)
+        steps = [s.step(it) for it in (1, 2)]
+        assert all(st["status"] == 0 for st in steps)
+        res[kz] = ([sum(st["cg_iters"]) for st in steps], {f: s.download(f) for f in ("u", "v", "w")})
+        s.close()
+    (i4, v4), (i2, v2) = res["4"], res["2"]
+    assert all(abs(a - b) <= 2 for a, b in zip(i4, i2)), (i4, i2)
+    vs = max(float(np.abs(b).max()) for b in v4.values())
+    for f in v4:
+        assert float(np.abs(v4[f] - v2[f]).max()) <= 1e-9 * vs, f
+
+
 @pytest.mark.parametrize("case", ["dam_break", "periodic"])
 def test_vector_kernels_match_one_cell_kernels(pkg, case):
     """The 4-cells-a-thread multigrid/PCG kernels (mg_kernels = 0) against the one-cell kernels
