@@ -639,14 +639,27 @@ struct BCArgs {
     int nlock;
     int obst;   // obstacle columns replace the wall-friction capture of the walls
 };
-// pressure ghosts: composition of the x, y, z copies (:37-54) = value at the mapped index
+// pressure ghosts: composition of the x, y, z copies (:37-54) = value at the mapped index.  One
+// thread per ghost cell of the halo surface: the two x layers (all j, k), the two y layers
+// (interior i, all k), the two z layers (interior i, j); reads touch only interior cells.
 __global__ void k_prd_ghosts(Geo G, BC bc, double* prd1) {
-    const Thread3 t = tid3(0, 0, 0);
-    const int i = t.i, j = t.j, k = t.k;
-    if (i > G.nx + 1 || j > G.ny + 1 || k > G.nz + 1) return;
-    const bool gh = (i < 1 || i > G.nx || j < 1 || j > G.ny || k < 1 || k > G.nz);
-    if (!gh) return;
-    const int mi = map_any(i, G.nx, bc.perx), mj = map_any(j, G.ny, bc.pery), mk = map_any(k, G.nz, bc.perz);
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const long long nxf = 2LL * (ny + 2) * (nz + 2), nyf = 2LL * nx * (nz + 2), nzf = 2LL * nx * ny;
+    int i, j, k;
+    if (q < nxf) {
+        const long long r = q >> 1;
+        i = (q & 1) ? nx + 1 : 0; j = (int)(r % (ny + 2)); k = (int)(r / (ny + 2));
+    } else if (q < nxf + nyf) {
+        const long long r = (q - nxf) >> 1;
+        j = ((q - nxf) & 1) ? ny + 1 : 0; i = 1 + (int)(r % nx); k = (int)(r / nx);
+    } else if (q < nxf + nyf + nzf) {
+        const long long r = (q - nxf - nyf) >> 1;
+        k = ((q - nxf - nyf) & 1) ? nz + 1 : 0; i = 1 + (int)(r % nx); j = 1 + (int)(r / nx);
+    } else {
+        return;
+    }
+    const int mi = map_any(i, nx, bc.perx), mj = map_any(j, ny, bc.pery), mk = map_any(k, nz, bc.perz);
     FIDX(prd1, i, j, k) = FIDX(prd1, mi, mj, mk);
 }
 
@@ -1524,7 +1537,10 @@ void launch_contorno(suli_ctx* c, int nlock) {
     const bool capy = !obst && (c->bc.y0 == 2 || c->bc.yf == 2);
     ProfScope ps(c, SULI_K_CONTORNO, (nlock == 2 ? 7 + (c->P.outflow_fix == 1 && c->bc.xf == 4 ? 1 : 0) : 4) +
                                          (capy || obst ? 1 : 0));
-    k_prd_ghosts<<<grid3(G.nx + 2, G.ny + 2, G.nz + 2, kBlk), kBlk, 0, c->stream>>>(G, c->bc, A.prd1);
+    {
+        const long long ng = 2LL * (G.ny + 2) * (G.nz + 2) + 2LL * G.nx * (G.nz + 2) + 2LL * G.nx * G.ny;
+        k_prd_ghosts<<<(unsigned)((ng + 255) / 256), 256, 0, c->stream>>>(G, c->bc, A.prd1);
+    }
     k_bc_y<<<grid3(G.nx + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
     k_bc_x<<<grid3(G.ny + 3, G.nz + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
     k_bc_z<<<grid3(G.nx + 3, G.ny + 3, 1, b2), b2, 0, c->stream>>>(G, c->bc, A);
