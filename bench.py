@@ -425,7 +425,7 @@ def workload_config(p, args, path):
     }
 
 
-def time_path(args, dist, pkg, p, init, dev, it0=0, net=None):
+def time_path(args, dist, pkg, p, init, dev, it0=0, net=None, nn_mode=1):
     """Warm up, then time K steps of one solver path with CUDA events on its own stream
     (with `net` attached as the pressure solve's initial guess, if given)."""
     import torch
@@ -433,7 +433,7 @@ def time_path(args, dist, pkg, p, init, dev, it0=0, net=None):
     s = pkg.Solver(p, device=dev)
     init(s)
     if net is not None:
-        s.attach_nn(net)
+        s.attach_nn(net, nn_mode)
     ext = torch.cuda.ExternalStream(s.stream_ptr, device=dev)
     it = it0
     for _ in range(args.warmup):
@@ -708,6 +708,10 @@ def run_ours(args):
             runs["learned"] = time_path(args, dist, pkg, q, init, dev, net=net)
         elif args.path == "learned":
             raise SystemExit(f"--path learned: {net_src}")
+    # the network also as the preconditioner of the outer refinement iteration (measured beside)
+    if net is not None and args.path == "all":
+        q2 = q.copy()
+        runs["learned_precond"] = time_path(args, dist, pkg, q2, init, dev, net=net, nn_mode=2)
     head_key = "learned" if "learned" in runs else ("mixed" if "mixed" in runs else "plain")
     head = runs[head_key]
     # every path ran the same warm-up + timed steps from the same state: per-field error of the
@@ -820,7 +824,8 @@ def run_ours(args):
         for k, r in runs.items():
             if k == head_key:
                 continue
-            line[{"plain": "plain_fp64", "mixed": "mixed_no_net", "learned": "learned"}[k]] = {
+            line[{"plain": "plain_fp64", "mixed": "mixed_no_net", "learned": "learned",
+                  "learned_precond": "learned_preconditioner"}[k]] = {
                 "value": r["value"], "ms_per_step": r["ms"] / args.steps,
                 "poisson_iters_per_step": r["iters_per_step"], "gpu_launches": r["launches"],
                 "clocks": {kk: r["clocks"].get(kk) for kk in ("sm_mhz", "sm_max_mhz", "reasons")}}
@@ -830,6 +835,10 @@ def run_ours(args):
             line["learned_vs_mixed"] = {"speedup": value / runs["mixed"]["value"],
                                         "poisson_iters_saved_per_step":
                                             runs["mixed"]["iters_per_step"] - head["iters_per_step"]}
+        if "mixed" in runs and "learned_precond" in runs:
+            line["learned_preconditioner_vs_mixed"] = {
+                "speedup": runs["learned_precond"]["value"] / runs["mixed"]["value"],
+                "poisson_iters_saved_per_step": runs["mixed"]["iters_per_step"] - runs["learned_precond"]["iters_per_step"]}
         if long:
             line["long_window"] = long
         line["roofline_classes"] = roof_head

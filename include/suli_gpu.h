@@ -258,8 +258,13 @@ int suli_nn_set_kernel(suli_nn* n, int kernel);
    graddin's set-up the network maps (r~0/s, H, (e0 - mean)/s_e) to a correction y of the
    scaled pressure, and e0 <- e0 + alpha s y with alpha = -(r~0 . y)/(y . A~ y), the
    energy-norm optimal step in FP64, so the guess never raises the A~-norm error of e0.  The
-   solve then runs to the same FP64 stopping test as without the network.  A network serves
-   one context at a time (it keeps its activations). */
+   solve then runs to the same FP64 stopping test as without the network.  Mode 2 (precision 1)
+   also applies the network as the preconditioner of the outer FP64 iteration: after every
+   refinement pass that has not met the stopping tests, the network maps the current residual
+   and iterate to a correction, applied with the same energy-optimal step (a nonlinear
+   preconditioner; the multigrid-preconditioned inner CG, and the plain FP64 CG as its fallback,
+   still decide when the solve is done).  A network serves one context at a time (it keeps its
+   activations). */
 int suli_attach_nn(suli_ctx* c, suli_nn* net, int mode);
 /* graddin() that also records a training pair of the network: d_in3 [V][3] receives the
    network's input features of the solve's starting state and d_target [V] the scaled

@@ -249,6 +249,7 @@ void launch_vcycle(suli_ctx* c);
 // ---- learned initial guess (k_learned.cu) ----
 void launch_nn_features(suli_ctx* c, float* in3);
 void launch_nn_features16(suli_ctx* c, void* in16);
+void launch_nn_features16_at(suli_ctx* c, void* in16, const double* r, const double* e);
 void launch_nn_step(suli_ctx* c, const float* out, double* e);
 void launch_nn_target(suli_ctx* c, const double* e_star, float* target);
 void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new);

@@ -177,10 +177,13 @@ void launch_nn_features(suli_ctx* c, float* in3) {
     k_nn_features<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_r, c->cg_e, c->f[SULI_F_HS], c->nn_scale, in3);
 }
 
-void launch_nn_features16(suli_ctx* c, void* in16) {
+void launch_nn_features16(suli_ctx* c, void* in16) { launch_nn_features16_at(c, in16, c->cg_r, c->cg_e); }
+
+// the features of the FP64 scaled residual r and iterate e (the refinement's current ones)
+void launch_nn_features16_at(suli_ctx* c, void* in16, const double* r, const double* e) {
     const Geo& G = c->g;
-    k_nn_stats<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_e, c->cg, c->nn_scale, c->red_partial, c->red_counter);
-    k_nn_features16<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_r, c->cg_e, c->f[SULI_F_HS], c->nn_scale,
+    k_nn_stats<<<grid_cells(G), kBL, 0, c->stream>>>(G, e, c->cg, c->nn_scale, c->red_partial, c->red_counter);
+    k_nn_features16<<<grid_cells(G), kBL, 0, c->stream>>>(G, r, e, c->f[SULI_F_HS], c->nn_scale,
                                                            static_cast<__nv_bfloat16*>(in16));
 }
 

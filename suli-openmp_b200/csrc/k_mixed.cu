@@ -509,7 +509,8 @@ __global__ void __launch_bounds__(256) k_mx_outer(Geo G, BC bc, const double* __
                                                   const double* __restrict__ ax, const double* __restrict__ ay,
                                                   const double* __restrict__ az, const double* __restrict__ b,
                                                   double* __restrict__ e_out, float* __restrict__ ru, int apply,
-                                                  CGState* cg, PCGState* pst, double* partial, unsigned int* counter) {
+                                                  CGState* cg, PCGState* pst, double* partial, unsigned int* counter,
+                                                  double* __restrict__ r_out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z + 1;
@@ -522,6 +523,7 @@ __global__ void __launch_bounds__(256) k_mx_outer(Geo G, BC bc, const double* __
         const double rv = ec - ax[c + 1] * en(c + o.xp) - ax[c] * en(c + o.xm) - ay[c + G.px] * en(c + o.yp) -
                           ay[c] * en(c + o.ym) - az[c + (int)G.pxy] * en(c + o.zp) - az[c] * en(c + o.zm) - b[c];
         e_out[c] = ec;
+        if (r_out) r_out[c] = rv;
         const double u = sd[c] * rv;
         ru[c] = (float)u;
         rr = rv * rv;
@@ -538,7 +540,8 @@ __global__ void __launch_bounds__(256) k_mx_outer2(Geo G, BC bc, const double* _
                                                    const double* __restrict__ ax, const double* __restrict__ ay,
                                                    const double* __restrict__ az, const double* __restrict__ b,
                                                    double* __restrict__ e_out, float* __restrict__ ru, int apply,
-                                                   CGState* cg, PCGState* pst, double* partial, unsigned int* counter) {
+                                                   CGState* cg, PCGState* pst, double* partial, unsigned int* counter,
+                                                   double* __restrict__ r_out) {
     const int i0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z + 1;
@@ -566,6 +569,7 @@ __global__ void __launch_bounds__(256) k_mx_outer2(Geo G, BC bc, const double* _
         const double r1 = ec.y - ax2 * exp_ - axc.y * ec.x - ayp.y * eyp.y - ayc.y * eym.y - azp.y * ezp.y -
                           azc.y * ezm.y - bc2.y;
         *reinterpret_cast<double2*>(e_out + c) = ec;
+        if (r_out) *reinterpret_cast<double2*>(r_out + c) = make_double2(r0, r1);
         const double u0 = sdc.x * r0, u1 = sdc.y * r1;
         *reinterpret_cast<float2*>(ru + c) = make_float2((float)u0, (float)u1);
         rr = r0 * r0 + r1 * r1;
@@ -623,19 +627,22 @@ void launch_mx_setup(suli_ctx* c) {
     }
 }
 
-// r_u from the FP64 first residual (no correction applied); also initialises the inner solve
+// r_u from the FP64 first residual (no correction applied); also initialises the inner solve.
+// With the network as the outer iteration's preconditioner (nn_mode 2) the FP64 scaled residual
+// is kept as well, in cg_r, for the network's features and step length.
 void launch_mx_residual(suli_ctx* c, const double* e_in, double* e_out, bool apply) {
+    double* r_out = (c->nn && c->nn_mode == 2 && !c->rec_in) ? c->cg_r : nullptr;
     ProfScope ps(c, SULI_K_REFINE, 1);
     const Geo& G = c->g;
     if (G.nx % 2 == 0) {
         const dim3 g2((G.nx / 2 + 31) / 32, (G.ny + 7) / 8, G.nz);
         k_mx_outer2<<<g2, kB2, 0, c->stream>>>(G, c->bc, e_in, c->pc_x, c->cg_sd, c->cg_ax, c->cg_ay, c->cg_az,
                                                c->cg_b, e_out, c->pc_r, apply ? 1 : 0, c->cg, c->pcg,
-                                               c->red_partial, c->red_counter);
+                                               c->red_partial, c->red_counter, r_out);
     } else {
         k_mx_outer<<<cells3(G), kB2, 0, c->stream>>>(G, c->bc, e_in, c->pc_x, c->cg_sd, c->cg_ax, c->cg_ay, c->cg_az,
                                                      c->cg_b, e_out, c->pc_r, apply ? 1 : 0, c->cg, c->pcg,
-                                                     c->red_partial, c->red_counter);
+                                                     c->red_partial, c->red_counter, r_out);
     }
 }
 

@@ -715,7 +715,7 @@ int ensure_nn_buffers(suli_ctx* c, bool net) {
 // After graddin's set-up: record the features and e0, or apply the learned initial guess.
 void nn_begin(suli_ctx* c) {
     const bool rec = c->rec_in != nullptr;
-    const bool learn = !rec && c->nn && c->nn_mode == 1;
+    const bool learn = !rec && c->nn && c->nn_mode >= 1;
     if (!rec && !learn) return;
     if (rec) {
         {
@@ -861,9 +861,32 @@ int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
         std::swap(ecur, enext);
         CHECK_LAUNCH(c);
         ++outer;
+        if (c->nn && c->nn_mode == 2 && !c->rec_in) {
+            // the network as the outer iteration's preconditioner: its correction of the current
+            // residual, with the energy-optimal FP64 step, before the next pass (or the test)
+            r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
+            if (r != SULI_OK) return r;
+            if (!c->cg_host[0].done) {
+                {
+                    ProfScope ps(c, SULI_K_CG_SETUP, 2);
+                    launch_nn_features16_at(c, suli::nn::input16(c->nn), c->cg_r, ecur);
+                }
+                {
+                    ProfScope ps(c, SULI_K_NN, 0);
+                    c->prof.launches[SULI_K_NN] += suli::nn::forward_packed_on(c->nn, c->stream, c->nn_out);
+                }
+                {
+                    ProfScope ps(c, SULI_K_CG_SETUP, 2);
+                    launch_nn_step(c, c->nn_out, ecur);
+                }
+                launch_mx_residual(c, ecur, enext, false);
+                std::swap(ecur, enext);
+                CHECK_LAUNCH(c);
+            }
+        }
     }
     c->last_outer_iters = outer;
-    if (c->nn && c->nn_mode == 1 && !c->rec_in && suli::nn::take_error(c->nn))
+    if (c->nn && c->nn_mode >= 1 && !c->rec_in && suli::nn::take_error(c->nn))
         return fail(c, SULI_ERR_CUDA, "graddin: the network's tensor-core convolution timed out");
     if (fallback) {   // prd1 from the iterate, then the FP64 CG to the same stopping tests
         launch_cg_final(c, ecur);
@@ -909,7 +932,7 @@ int suli_attach_nn(suli_ctx* c, suli_nn* net, int mode) {
         c->nn_mode = 0;
         return SULI_OK;
     }
-    if (mode != 1 || !net) return fail(c, SULI_ERR_ARG, "attach_nn: mode must be 0 or 1 with a network");
+    if ((mode != 1 && mode != 2) || !net) return fail(c, SULI_ERR_ARG, "attach_nn: mode must be 0, 1 or 2 with a network");
     if (c->P.precision != 1) return fail(c, SULI_ERR_UNSUPPORTED, "attach_nn: the learned guess needs precision 1");
     int nx, ny, nz, dev;
     suli::nn::dims(net, &nx, &ny, &nz, &dev);

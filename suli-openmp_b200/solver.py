@@ -206,7 +206,8 @@ class Solver:
 
     def attach_nn(self, net, mode: int = 1) -> None:
         """Use `net` (a `learned.Net` of the same grid) as the pressure solve's initial guess
-        (mode 1, precision 1), or detach it (mode 0 / net None)."""
+        (mode 1, precision 1), also as the preconditioner of the outer refinement iteration
+        (mode 2), or detach it (mode 0 / net None)."""
         if net is None or mode == 0:
             self._check(self.lib.suli_attach_nn(self._h, None, 0), "attach_nn")
             self._net = None

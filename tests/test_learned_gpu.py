@@ -92,9 +92,9 @@ def test_density_feature_is_the_heaviside_for_both_mixes(pkg, torch):
         s.close()
 
 
-def _solve(s, torch, ls, vel, net=None):
+def _solve(s, torch, ls, vel, net=None, mode=1):
     _load(s, torch, ls, vel)
-    s.attach_nn(net)
+    s.attach_nn(net, mode)
     iters, res = s.graddin()
     prd = s.download("prd1")
     s.attach_nn(None)
@@ -124,6 +124,28 @@ def test_untrained_network_converges_to_same_pressure(pkg, torch):
     assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(a)
     # the energy-optimal step cannot make the start worse; allow the count to wobble
     assert it1 <= it0 + 3, (it0, it1)
+    s.close()
+    net.close()
+
+
+@pytest.mark.parametrize("trained", [False, True])
+def test_network_as_outer_preconditioner(pkg, torch, trained):
+    """Mode 2 (the network also corrects the iterate before every further refinement pass):
+    the solve reaches the same FP64 tolerance and the same pressure (up to the constant of the
+    all-Neumann problem) as without the network, with an untrained and with the shipped network;
+    the energy-optimal step keeps any pass from making the iterate worse."""
+    s, gen, ls, vel = _problem(pkg, torch, 13)
+    it0, r0, p0 = _solve(s, torch, ls, vel)
+    if trained:
+        net = pkg.learned.Net.load(N, N, N)
+    else:
+        net = pkg.learned.Net(N, N, N, params=pkg.learned.init_params(2, head_scale=1.0))
+    it2, r2, p2 = _solve(s, torch, ls, vel, net, mode=2)
+    assert r0 <= TOL and r2 <= TOL
+    a = p0[1:-1, 1:-1, 1:-1] - p0[1:-1, 1:-1, 1:-1].mean()
+    b = p2[1:-1, 1:-1, 1:-1] - p2[1:-1, 1:-1, 1:-1].mean()
+    assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(a)
+    assert it2 <= it0 + 3, (it0, it2)
     s.close()
     net.close()
 
