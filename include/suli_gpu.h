@@ -89,12 +89,12 @@ typedef struct suli_params {
     double inner_tol;               /* relative tolerance of each FP32 inner solve             */
     double mg_omega;                /* precision 1: damping of the multigrid Jacobi sweeps (0 = 0.9) */
     double mg_alpha;                /* precision 1: scale of the coarse-grid correction (0 = 1.8)     */
-    int    mg_kernels;              /* precision 1: 0 = vectorised multigrid/PCG kernels (4 cells a
-                                       thread, float4 loads) with the three coarsest levels in one
-                                       16-CTA cluster launch where their shapes allow (default);
+    int    mg_kernels;              /* precision 1: 0 = vectorised multigrid/PCG kernels (4 x cells a
+                                       thread, float4 loads), every level its own kernels (default);
                                        1 = one cell a thread (same arithmetic, kept as the reference
-                                       the tests compare with); 2 = vectorised, every level its own
-                                       kernels */
+                                       the tests compare with); 2 = vectorised, with the three
+                                       coarsest levels in one 16-CTA cluster launch where their
+                                       shapes allow (measured slower at 256x128x128) */
     int    wave_t;                  /* wave inflow at x = 0: 0 none, 1 Stokes I, 2 Stokes II, 5 Stokes V (0_modules.f90:35) */
     int    outflow_fix;             /* 0 = the reference's outflow copy (3_contorno.f90:193-197, 362-409);
                                        1 (extension, needs ccxf = 4) = contorno(2) then shifts the

@@ -135,7 +135,7 @@ struct suli_ctx {
     float* f32_arena = nullptr;
     int coarse_sweeps = 40;
     bool cluster_ok = false;
-    int mg_kz = 4;             // cells along z a thread of the vectorised multigrid kernels owns (2 or 4)   // the device runs k_mg_cluster (16-CTA cluster with its shared memory)
+    int mg_kz = 2;             // cells along z a thread of the vectorised multigrid kernels owns (2 or 4)   // the device runs k_mg_cluster (16-CTA cluster with its shared memory)
     int inner_maxit = 200;
     int inner_batch = 4;
     int last_outer_iters = 0;

@@ -722,20 +722,22 @@ static void vc_up(suli_ctx* c, int l, const float* f, float om, float alpha) {
     }
 }
 
-// The three coarsest levels run as one cluster launch (k_mg_cluster) when their shapes fit it,
-// the vectorised kernels are selected (mg_kernels = 0) and the device runs a 16-CTA cluster with
-// the kernel's shared memory (checked once, cluster_ready).
+// The three coarsest levels run as one cluster launch (k_mg_cluster) when selected
+// (mg_kernels = 2), their shapes fit it and the device runs a 16-CTA cluster with the kernel's
+// shared memory (checked once, cluster_ready).  Measured at 256x128x128 it is slower than the
+// per-level kernels it replaces (54 us a launch against about 40 us for the nine kernels), so
+// it is not the default.
 static bool use_cluster(const suli_ctx* c) {
     const int L = (int)c->mg.size();
-    return c->P.mg_kernels == 0 && c->cluster_ok && L >= 4 && vec_level(c, c->mg[L - 4].g) &&
+    return c->P.mg_kernels == 2 && c->cluster_ok && L >= 4 && vec_level(c, c->mg[L - 4].g) &&
            cl_fits(c->mg[L - 3].g, c->mg[L - 2].g, c->mg[L - 1].g);
 }
 
 int cluster_ready(suli_ctx* c) {
     c->cluster_ok = false;
-    c->mg_kz = 4;
+    c->mg_kz = 2;
     if (const char* ev = std::getenv("SULI_MG_KZ"))   // column depth of the vectorised kernels
-        if (std::strcmp(ev, "2") == 0) c->mg_kz = 2;
+        if (std::strcmp(ev, "4") == 0) c->mg_kz = 4;
     if (const char* ev = std::getenv("SULI_NO_CLUSTER"))   // keep the per-level kernels
         if (std::strcmp(ev, "1") == 0) return SULI_OK;
     const int L = (int)c->mg.size();

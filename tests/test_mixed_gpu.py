@@ -74,8 +74,8 @@ def test_mixed_steps_track_fp64(pkg, orc):
 
 @pytest.mark.parametrize("case", ["dam_break", "periodic"])
 def test_cluster_levels_match_per_level_kernels(pkg, case):
-    """The three coarsest levels in one 16-CTA cluster launch (mg_kernels = 0) against the same
-    levels as kernels per level (mg_kernels = 2): the same stages and per-cell arithmetic (only
+    """The three coarsest levels in one 16-CTA cluster launch (mg_kernels = 2) against the same
+    levels as kernels per level (mg_kernels = 0): the same stages and per-cell arithmetic (only
     the restriction to the coarsest grid adds its children in two halves), so the inner solves
     follow the same course.  Walls (dam break 128x64x64, cluster levels 64x32x32 .. 16x8x8) and a
     box periodic in every direction (64^3, so the z wrap crosses from the last CTA to the first),
@@ -106,15 +106,15 @@ def test_cluster_levels_match_per_level_kernels(pkg, case):
         s.close()
     (it0, v0, p0), (it2, v2, p2) = res[0], res[2]
     assert all(abs(a - b) <= 2 for a, b in zip(it0, it2)), (it0, it2)
-    vs = max(float(np.abs(b).max()) for b in v2.values())
+    vs = max(float(np.abs(b).max()) for b in v0.values())
     for f in v0:
         assert float(np.abs(v0[f] - v2[f]).max()) <= 1e-9 * vs, f
     per_it = lambda pr: pr["mg"]["launches"] / max(pr["cg_iterations"], 1)
-    assert per_it(p0) < 0.6 * per_it(p2), (per_it(p0), per_it(p2))
+    assert per_it(p2) < 0.6 * per_it(p0), (per_it(p2), per_it(p0))
 
 
 def test_column_depths_agree(pkg, monkeypatch):
-    """The vectorised kernels with 2 cells along z a thread (SULI_MG_KZ=2) against 4 (default):
+    """The vectorised kernels with 4 cells along z a thread (SULI_MG_KZ=4) against 2 (default):
     the same per-cell arithmetic, the FP64 dot products grouped differently; dam break
     128x64x64, two steps: iteration counts within 2, velocities within 1e-9 of their scale."""
     res = {}
