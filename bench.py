@@ -64,6 +64,8 @@ def parse_args():
     ap.add_argument("--inner-tol", type=float, default=1e-3, help="relative tolerance of each FP32 inner solve")
     ap.add_argument("--mg-omega", type=float, default=0.9, help="damping of the multigrid Jacobi sweeps")
     ap.add_argument("--mg-alpha", type=float, default=1.8, help="scale of the multigrid coarse-grid correction")
+    ap.add_argument("--mg-omega2", type=float, default=0.0,
+                    help="weight of the second pre-smoothing (first post-smoothing) sweep; 0: --mg-omega")
     ap.add_argument("--path", choices=["all", "plain", "mixed", "learned"], default="all",
                     help="time every solver path (headline = learned + mixed precision) or one of them")
     ap.add_argument("--weights", default=None, help="network weights (.npy); default: the shipped ones")
@@ -584,6 +586,7 @@ def mixed_params(p, args):
     q.precision, q.cg_stop, q.cg_tol = 1, 1, args.cg_tol
     q.inner_tol, q.refine_maxit = args.inner_tol, 30
     q.mg_omega, q.mg_alpha = args.mg_omega, args.mg_alpha
+    q.mg_omega2 = args.mg_omega2
     return q
 
 
@@ -802,6 +805,7 @@ def run_ours(args):
         cfg = workload_config(q if head_key != "plain" else p, args, desc[head_key])
         cfg["inner_tol"] = args.inner_tol
         cfg["mg_omega"], cfg["mg_alpha"] = args.mg_omega, args.mg_alpha
+        cfg["mg_omega2"] = args.mg_omega2 or args.mg_omega
         if net_src:
             cfg["weights"] = net_src
         arm_acc = {k: {"max_div": max(st["max_div"] for st in r["stats"]),

@@ -106,6 +106,9 @@ typedef struct suli_params {
                                        1 (extension) = on a periodic axis both end faces, one face of the
                                        periodic box, take the average across the wrap, which keeps the
                                        scaled Poisson operator symmetric when the density varies there */
+    double mg_omega2;               /* precision 1: weight of the second pre-smoothing sweep and of the
+                                       first post-smoothing one (0 = mg_omega); two different weights
+                                       make the smoother a degree-2 polynomial (Chebyshev-like) */
     double div_tol;                 /* 0 = off (the reference); > 0 (extension): the Poisson solve also
                                        requires max |sqrt(d) r~| <= div_tol, the largest |div u| the
                                        projection leaves (the unscaled residual), and iterates on

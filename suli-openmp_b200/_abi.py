@@ -47,6 +47,7 @@ class SuliParams(C.Structure):
         ("wave_t", C.c_int),
         ("outflow_fix", C.c_int),
         ("periodic_faces", C.c_int),
+        ("mg_omega2", C.c_double),
         ("div_tol", C.c_double),
     ]
 

@@ -43,6 +43,7 @@ struct ClArgs {
     const float* fM;   // level M's right-hand side (the restriction from the level above)
     float* yM;         // level M's result (read by the prolongation into the level above)
     float omega, alpha;
+    float omega2;      // weight of the second pre-smoothing sweep, of the first post-smoothing one
     int sweeps;        // Jacobi sweeps of the coarsest solve
 };
 
@@ -117,7 +118,7 @@ __global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(ClArgs A, const PC
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank(), tid = threadIdx.x;
     const BC bc = A.bc;
-    const float om = A.omega, al = A.alpha;
+    const float om = A.omega, om2 = A.omega2, al = A.alpha;
     extern __shared__ __align__(16) float smem[];
     float* p = smem;
     ClSlab M, C;
@@ -150,7 +151,7 @@ __global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(ClArgs A, const PC
         const int i = q % M.nx + 1, j = (q / M.nx) % M.ny + 1, kl = q / (M.nx * M.ny);
         const float xc = om * M.f[q] * M.d[q];
         const float ax = cl_apply(M, bc, nzM, i, j, kl, xc, x1M);
-        M.y[q] = xc + om * (M.f[q] - ax) * M.d[q];
+        M.y[q] = xc + om2 * (M.f[q] - ax) * M.d[q];
     }
     cl.sync();
     // ---- restriction M -> C: f_C = (1/8) sum of the 8 children of (f - A y)
@@ -180,7 +181,7 @@ __global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(ClArgs A, const PC
         const int i = q % C.nx + 1, j = (q / C.nx) % C.ny + 1, kl = q / (C.nx * C.ny);
         const float xc = om * C.f[q] * C.d[q];
         const float ax = cl_apply(C, bc, nzC, i, j, kl, xc, x1C);
-        C.y[q] = xc + om * (C.f[q] - ax) * C.d[q];
+        C.y[q] = xc + om2 * (C.f[q] - ax) * C.d[q];
     }
     cl.sync();
     // ---- restriction C -> B: CTA r holds C plane r + 1, the children dz = r % 2 of B plane r/2 + 1;
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(ClArgs A, const PC
         const int i = q % C.nx + 1, j = (q / C.nx) % C.ny + 1, kl = q / (C.nx * C.ny);
         const float xv = xpC(i, j, C.k0 + kl);
         const float ax = cl_apply(C, bc, nzC, i, j, kl, xv, xpC);
-        C.x[q] = xv + om * (C.f[q] - ax) * C.d[q];
+        C.x[q] = xv + om2 * (C.f[q] - ax) * C.d[q];
     }
     cl.sync();
     auto xC = [&](int i, int j, int k) { return cl_at(cl, C, [](const ClSlab& s) { return (const float*)s.x; }, i, j, k); };
@@ -271,7 +272,7 @@ __global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(ClArgs A, const PC
         const int i = q % M.nx + 1, j = (q / M.nx) % M.ny + 1, kl = q / (M.nx * M.ny);
         const float xv = xpM(i, j, M.k0 + kl);
         const float ax = cl_apply(M, bc, nzM, i, j, kl, xv, xpM);
-        M.x[q] = xv + om * (M.f[q] - ax) * M.d[q];
+        M.x[q] = xv + om2 * (M.f[q] - ax) * M.d[q];
     }
     cl.sync();
     auto xM = [&](int i, int j, int k) { return cl_at(cl, M, [](const ClSlab& s) { return (const float*)s.x; }, i, j, k); };

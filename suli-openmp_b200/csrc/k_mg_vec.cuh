@@ -104,10 +104,11 @@ __device__ __forceinline__ void apply4(const Faces (&F)[kVX], const float (&xc)[
     }
 }
 
-// two damped Jacobi sweeps from zero (k_mg_pre): x1 = w f/dg, y = x1 + w (f - A x1)/dg
+// two damped Jacobi sweeps from zero (k_mg_pre): x1 = w f/dg, y = x1 + w2 (f - A x1)/dg
 template <int KZ, class Op4>
 __global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_mgv_pre(Geo G, BC bc, const float* __restrict__ f, Op4 A,
-                                                 float* __restrict__ y, float omega, const PCGState* st) {
+                                                 float* __restrict__ y, float omega, float omega2,
+                                                 const PCGState* st) {
     pdl_wait();
     if (st->done) return;
     const VQ q = vquad(G, bc, KZ);
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_mgv_pre(Geo G, BC bc, 
         apply4(F, col[m + 1], x1s(c + q.fxm), x1s(c + kVX - 1 + q.fxp), ym, yp, col[m], col[m + 2], ax);
         const V4 fc = ld4(f, c), dc = A.inv_diag(c);
 #pragma unroll
-        for (int e = 0; e < kVX; ++e) out[e] = col[m + 1][e] + omega * (fc.v[e] - ax[e]) * dc.v[e];
+        for (int e = 0; e < kVX; ++e) out[e] = col[m + 1][e] + omega2 * (fc.v[e] - ax[e]) * dc.v[e];
         st4(y, c, out);
     }
 }

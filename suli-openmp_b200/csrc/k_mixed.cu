@@ -208,7 +208,8 @@ __device__ __forceinline__ float apply_faces(const Faces& F, float xc, float xm,
 // two damped Jacobi sweeps from zero in one pass: x1 = w f/dg, y = x1 + w (f - A x1)/dg
 template <class Op>
 __global__ void __launch_bounds__(256) k_mg_pre(Geo G, BC bc, const float* __restrict__ f, Op A,
-                                                float* __restrict__ y, float omega, const PCGState* st) {
+                                                float* __restrict__ y, float omega, float omega2,
+                                                const PCGState* st) {
     pdl_wait();
     if (st->done) return;
     const Col q = column(G, bc);
@@ -226,7 +227,7 @@ __global__ void __launch_bounds__(256) k_mg_pre(Geo G, BC bc, const float* __res
         const Faces F = A.at(G, q, cs, m, c);
         const float ax = apply_faces(F, xc, x1(c + q.o.xm), x1(c + q.o.xp), x1(c + q.o.ym), x1(c + q.o.yp), col[m],
                                      col[m + 2]);
-        y[c] = xc + omega * (f[c] - ax) * A.inv_diag(c);
+        y[c] = xc + omega2 * (f[c] - ax) * A.inv_diag(c);
     }
 }
 
@@ -665,57 +666,59 @@ static inline OpStored4 stored4(const MGLevel& L) { return OpStored4{L.sx, L.sy,
 // the 4-cells-a-thread kernels on a level (mg_kernels 0 or 2 and x divisible by 4)
 static inline bool vec_level(const suli_ctx* c, const Geo& g) { return c->P.mg_kernels != 1 && g.nx % kVX == 0; }
 
-// pre-smoothing and restriction of level l (level 0 forms its faces from the density)
-static void vc_down(suli_ctx* c, int l, const float* f, float om) {
+// pre-smoothing (weights om, then om2) and restriction of level l (level 0 forms its faces from
+// the density)
+static void vc_down(suli_ctx* c, int l, const float* f, float om, float om2) {
     MGLevel& M = c->mg[l];
     MGLevel& C = c->mg[l + 1];
     const BC bc = c->bc;
     if (vec_level(c, M.g)) {
         if (l == 0) {
-            VLAUNCH(k_mgv_pre, OpRho4, M.g, M.g, bc, f, from_rho4(M), M.y, om, c->pcg);
+            VLAUNCH(k_mgv_pre, OpRho4, M.g, M.g, bc, f, from_rho4(M), M.y, om, om2, c->pcg);
             pdl_launch(k_mgv_restrict<OpRho4>, vgrid_restrict(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, from_rho4(M),
                        C.f, c->pcg);
         } else {
-            VLAUNCH(k_mgv_pre, OpStored4, M.g, M.g, bc, f, stored4(M), M.y, om, c->pcg);
+            VLAUNCH(k_mgv_pre, OpStored4, M.g, M.g, bc, f, stored4(M), M.y, om, om2, c->pcg);
             pdl_launch(k_mgv_restrict<OpStored4>, vgrid_restrict(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, stored4(M),
                        C.f, c->pcg);
         }
         return;
     }
     if (l == 0) {
-        pdl_launch(k_mg_pre<OpRho>, colgrid(M.g), kB2, c->stream, M.g, bc, f, from_rho(M), M.y, om, c->pcg);
+        pdl_launch(k_mg_pre<OpRho>, colgrid(M.g), kB2, c->stream, M.g, bc, f, from_rho(M), M.y, om, om2, c->pcg);
         pdl_launch(k_mg_restrict<OpRho>, cells3(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, from_rho(M), C.f, c->pcg);
     } else {
-        pdl_launch(k_mg_pre<OpStored>, colgrid(M.g), kB2, c->stream, M.g, bc, f, stored(M), M.y, om, c->pcg);
+        pdl_launch(k_mg_pre<OpStored>, colgrid(M.g), kB2, c->stream, M.g, bc, f, stored(M), M.y, om, om2, c->pcg);
         pdl_launch(k_mg_restrict<OpStored>, cells3(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, stored(M), C.f, c->pcg);
     }
 }
 
-// prolongation + post-smoothing of level l, then the last sweep (level 0: with r.z and beta)
-static void vc_up(suli_ctx* c, int l, const float* f, float om, float alpha) {
+// prolongation + post-smoothing of level l (weight om2), then the last sweep (om; level 0: with
+// r.z and beta): the pre-smoothing's sweeps in reverse order, so the V-cycle stays symmetric
+static void vc_up(suli_ctx* c, int l, const float* f, float om, float om2, float alpha) {
     MGLevel& M = c->mg[l];
     MGLevel& C = c->mg[l + 1];
     const BC bc = c->bc;
     const int dot = (l == 0) ? 1 : 0;
     if (vec_level(c, M.g)) {
         if (l == 0) {
-            VLAUNCH(k_mgv_post, OpRho4, M.g, M.g, C.g, bc, M.y, C.y, f, from_rho4(M), M.x, om, alpha, c->pcg);
+            VLAUNCH(k_mgv_post, OpRho4, M.g, M.g, C.g, bc, M.y, C.y, f, from_rho4(M), M.x, om2, alpha, c->pcg);
             VLAUNCH(k_mgv_jacc, OpRho4, M.g, M.g, bc, M.x, f, from_rho4(M), M.y, om, c->pcg, dot, c->red_partial,
                     c->red_counter);
         } else {
-            VLAUNCH(k_mgv_post, OpStored4, M.g, M.g, C.g, bc, M.y, C.y, f, stored4(M), M.x, om, alpha, c->pcg);
+            VLAUNCH(k_mgv_post, OpStored4, M.g, M.g, C.g, bc, M.y, C.y, f, stored4(M), M.x, om2, alpha, c->pcg);
             VLAUNCH(k_mgv_jacc, OpStored4, M.g, M.g, bc, M.x, f, stored4(M), M.y, om, c->pcg, dot, c->red_partial,
                     c->red_counter);
         }
         return;
     }
     if (l == 0) {
-        pdl_launch(k_mg_post<OpRho>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, C.y, f, from_rho(M), M.x, om,
+        pdl_launch(k_mg_post<OpRho>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, C.y, f, from_rho(M), M.x, om2,
                    alpha, c->pcg);
         pdl_launch(k_mg_jacc<OpRho>, colgrid(M.g), kB2, c->stream, M.g, bc, M.x, f, from_rho(M), M.y, om, c->pcg, dot,
                    c->red_partial, c->red_counter);
     } else {
-        pdl_launch(k_mg_post<OpStored>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, C.y, f, stored(M), M.x, om,
+        pdl_launch(k_mg_post<OpStored>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, C.y, f, stored(M), M.x, om2,
                    alpha, c->pcg);
         pdl_launch(k_mg_jacc<OpStored>, colgrid(M.g), kB2, c->stream, M.g, bc, M.x, f, stored(M), M.y, om, c->pcg, dot,
                    c->red_partial, c->red_counter);
@@ -779,6 +782,7 @@ static void launch_cluster(suli_ctx* c, float om, float alpha) {
     a.fM = M.f;
     a.yM = M.y;
     a.omega = om;
+    a.omega2 = (float)c->P.mg_omega2;
     a.alpha = alpha;
     a.sweeps = c->coarse_sweeps;
     cudaLaunchConfig_t cfg = {};
@@ -801,16 +805,17 @@ static void launch_cluster(suli_ctx* c, float om, float alpha) {
 // z = M r: one V-cycle; the last level-0 sweep also forms r.z and beta
 void launch_vcycle(suli_ctx* c) {
     const float om = (float)c->P.mg_omega;
+    const float om2 = (float)c->P.mg_omega2;
     const float alpha = (float)c->P.mg_alpha;
     const int L = (int)c->mg.size();
     const BC bc = c->bc;
     if (use_cluster(c)) {   // levels 0 .. L-4 as kernels per level, the last three in the cluster
-        for (int l = 0; l < L - 3; ++l) vc_down(c, l, l == 0 ? c->pc_r : c->mg[l].f, om);
+        for (int l = 0; l < L - 3; ++l) vc_down(c, l, l == 0 ? c->pc_r : c->mg[l].f, om, om2);
         launch_cluster(c, om, alpha);
-        for (int l = L - 4; l >= 0; --l) vc_up(c, l, l == 0 ? c->pc_r : c->mg[l].f, om, alpha);
+        for (int l = L - 4; l >= 0; --l) vc_up(c, l, l == 0 ? c->pc_r : c->mg[l].f, om, om2, alpha);
         return;
     }
-    for (int l = 0; l < L - 1; ++l) vc_down(c, l, l == 0 ? c->pc_r : c->mg[l].f, om);
+    for (int l = 0; l < L - 1; ++l) vc_down(c, l, l == 0 ? c->pc_r : c->mg[l].f, om, om2);
     MGLevel& B = c->mg[L - 1];
     if (L == 1) {   // a single level: coarsest sweeps, then one more sweep that forms r.z
         pdl_launch(k_mg_coarsest, 1, 1024, c->stream, B.g, bc, c->pc_r, stored(B), B.x, c->coarse_sweeps, om, c->pcg);
@@ -819,7 +824,7 @@ void launch_vcycle(suli_ctx* c) {
         return;
     }
     pdl_launch(k_mg_coarsest, 1, 1024, c->stream, B.g, bc, B.f, stored(B), B.y, c->coarse_sweeps, om, c->pcg);
-    for (int l = L - 2; l >= 0; --l) vc_up(c, l, l == 0 ? c->pc_r : c->mg[l].f, om, alpha);
+    for (int l = L - 2; l >= 0; --l) vc_up(c, l, l == 0 ? c->pc_r : c->mg[l].f, om, om2, alpha);
 }
 
 void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new) {

@@ -136,6 +136,7 @@ int validate(const suli_params* p, std::string& why) {
         if (!(p->inner_tol > 0 && p->inner_tol < 1)) { why = "inner_tol must lie in (0, 1)"; return SULI_ERR_ARG; }
         if (!(p->mg_omega >= 0 && p->mg_omega < 1)) { why = "mg_omega must lie in [0, 1)"; return SULI_ERR_ARG; }
         if (!(p->mg_alpha >= 0 && p->mg_alpha <= 2)) { why = "mg_alpha must lie in [0, 2]"; return SULI_ERR_ARG; }
+        if (!(p->mg_omega2 >= 0 && p->mg_omega2 < 2)) { why = "mg_omega2 must lie in [0, 2)"; return SULI_ERR_ARG; }
         if (p->mg_kernels < 0 || p->mg_kernels > 2) { why = "mg_kernels must be 0, 1 or 2"; return SULI_ERR_ARG; }
         int nx = p->nx, ny = p->ny, nz = p->nz;
         while ((long long)nx * ny * nz > 1024 && nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0 && nx >= 4 && ny >= 4 && nz >= 4) {
@@ -207,6 +208,7 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
     c->P = *p;
     if (c->P.mg_omega == 0.) c->P.mg_omega = 0.9;   // zero-initialised structs get the defaults
     if (c->P.mg_alpha == 0.) c->P.mg_alpha = 1.8;
+    if (c->P.mg_omega2 == 0.) c->P.mg_omega2 = c->P.mg_omega;   // one weight for both sweeps
     c->device = device;
     c->g = make_geo(p->nx, p->ny, p->nz);
     c->bc.x0 = p->ccx0; c->bc.xf = p->ccxf; c->bc.y0 = p->ccy0; c->bc.yf = p->ccyf; c->bc.z0 = p->ccz0; c->bc.zf = p->cczf;
