@@ -64,6 +64,8 @@ def parse_args():
     ap.add_argument("--inner-tol", type=float, default=1e-3, help="relative tolerance of each FP32 inner solve")
     ap.add_argument("--mg-omega", type=float, default=0.9, help="damping of the multigrid Jacobi sweeps")
     ap.add_argument("--mg-alpha", type=float, default=1.8, help="scale of the multigrid coarse-grid correction")
+    ap.add_argument("--mg-kernels", type=int, default=0,
+                    help="multigrid kernels: 0 vectorised per level, 1 one cell a thread, 2 with the cluster coarse levels")
     ap.add_argument("--mg-omega2", type=float, default=0.0,
                     help="weight of the second pre-smoothing (first post-smoothing) sweep; 0: --mg-omega")
     ap.add_argument("--path", choices=["all", "plain", "mixed", "learned"], default="all",
@@ -587,6 +589,7 @@ def mixed_params(p, args):
     q.inner_tol, q.refine_maxit = args.inner_tol, 30
     q.mg_omega, q.mg_alpha = args.mg_omega, args.mg_alpha
     q.mg_omega2 = args.mg_omega2
+    q.mg_kernels = args.mg_kernels
     return q
 
 
@@ -806,6 +809,7 @@ def run_ours(args):
         cfg["inner_tol"] = args.inner_tol
         cfg["mg_omega"], cfg["mg_alpha"] = args.mg_omega, args.mg_alpha
         cfg["mg_omega2"] = args.mg_omega2 or args.mg_omega
+        cfg["mg_kernels"] = args.mg_kernels
         if net_src:
             cfg["weights"] = net_src
         arm_acc = {k: {"max_div": max(st["max_div"] for st in r["stats"]),

@@ -67,26 +67,36 @@ __device__ __forceinline__ float* carve(float*& p, int n) {
     return r;
 }
 
+// A thread's share of a slab array: up to kClLoads elements, all loads issued before the first
+// store so that their L2 latencies overlap (a loop with one load and one store per trip would
+// wait out each latency in turn).
+constexpr int kClLoads = 8;
+template <class Idx>
+__device__ __forceinline__ void cl_copy(const float* __restrict__ src, float* dst, int n, int tid, Idx gidx) {
+    float v[kClLoads];
+#pragma unroll
+    for (int t = 0; t < kClLoads; ++t) {
+        const int q = tid + t * kClThreads;
+        v[t] = (q < n) ? src[gidx(q)] : 0.f;
+    }
+#pragma unroll
+    for (int t = 0; t < kClLoads; ++t) {
+        const int q = tid + t * kClThreads;
+        if (q < n) dst[q] = v[t];
+    }
+}
+
 __device__ inline void cl_load_slab(const ClLevel& L, ClSlab& S, const float* fglob, int tid) {
     const Geo& G = L.g;
-    for (int q = tid; q < S.nx * S.ny * S.pl; q += kClThreads) {
-        const int i = q % S.nx + 1, j = (q / S.nx) % S.ny + 1, kl = q / (S.nx * S.ny);
-        const long long c = G.idx(i, j, S.k0 + kl);
-        S.d[q] = L.idg[c];
-        if (fglob) S.f[q] = fglob[c];
-    }
-    for (int q = tid; q < (S.nx + 1) * S.ny * S.pl; q += kClThreads) {
-        const int i = q % (S.nx + 1) + 1, j = (q / (S.nx + 1)) % S.ny + 1, kl = q / ((S.nx + 1) * S.ny);
-        S.sx[q] = L.sx[G.idx(i, j, S.k0 + kl)];
-    }
-    for (int q = tid; q < S.nx * (S.ny + 1) * S.pl; q += kClThreads) {
-        const int i = q % S.nx + 1, j = (q / S.nx) % (S.ny + 1) + 1, kl = q / (S.nx * (S.ny + 1));
-        S.sy[q] = L.sy[G.idx(i, j, S.k0 + kl)];
-    }
-    for (int q = tid; q < S.nx * S.ny * (S.pl + 1); q += kClThreads) {
-        const int i = q % S.nx + 1, j = (q / S.nx) % S.ny + 1, kl = q / (S.nx * S.ny);
-        S.sz[q] = L.sz[G.idx(i, j, S.k0 + kl)];
-    }
+    const int nx = S.nx, ny = S.ny, k0 = S.k0;
+    auto cell = [&](int q) { return G.idx(q % nx + 1, (q / nx) % ny + 1, k0 + q / (nx * ny)); };
+    cl_copy(L.idg, S.d, nx * ny * S.pl, tid, cell);
+    if (fglob) cl_copy(fglob, S.f, nx * ny * S.pl, tid, cell);
+    cl_copy(L.sx, S.sx, (nx + 1) * ny * S.pl, tid,
+            [&](int q) { return G.idx(q % (nx + 1) + 1, (q / (nx + 1)) % ny + 1, k0 + q / ((nx + 1) * ny)); });
+    cl_copy(L.sy, S.sy, nx * (ny + 1) * S.pl, tid,
+            [&](int q) { return G.idx(q % nx + 1, (q / nx) % (ny + 1) + 1, k0 + q / (nx * (ny + 1))); });
+    cl_copy(L.sz, S.sz, nx * ny * (S.pl + 1), tid, cell);
 }
 
 // value of a slab array at global cell (i, j, k) (already ghost-mapped): this CTA's shared
@@ -288,7 +298,9 @@ __global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(ClArgs A, const PC
 // whether the three coarsest levels fit the cluster kernel's layout
 inline bool cl_fits(const Geo& M, const Geo& C, const Geo& B) {
     return M.nz == 2 * kClCTAs && C.nz == kClCTAs && B.nz * 2 == C.nz && C.nx * 2 == M.nx && C.ny * 2 == M.ny &&
-           B.nx * 2 == C.nx && B.ny * 2 == C.ny && 2LL * M.nx * M.ny <= kClMaxM && (long long)B.nx * B.ny * B.nz <= kClMaxB;
+           B.nx * 2 == C.nx && B.ny * 2 == C.ny && 2LL * M.nx * M.ny <= kClMaxM && (long long)B.nx * B.ny * B.nz <= kClMaxB &&
+           3LL * M.nx * M.ny <= (long long)kClLoads * kClThreads &&                    // z faces of a slab
+           2LL * (M.nx + 1) * (M.ny + 1) <= (long long)kClLoads * kClThreads;
 }
 // shared memory of the cluster kernel
 inline size_t cl_smem_bytes(const Geo& M, const Geo& C, const Geo& B) {
