@@ -557,7 +557,8 @@ def headline_rooflines(pkg, p, head, peaks):
         out["inner_pcg_iteration"] = {
             "kernel": "one FP32 inner PCG iteration (CUDA graph: SpMV, update, multigrid V-cycle)",
             "bound": "hbm", "achieved": b / t / 1e9, "peak": peak_hbm, "unit": "GB/s", "frac": b / t / 1e9 / peak_hbm,
-            "algorithmic_bytes": b, "us": t * 1e6, "traffic": None}
+            "algorithmic_bytes": b, "us": t * 1e6,
+            "traffic": profiled_traffic("inner_pcg_iteration_256x128x128", p.nx * p.ny * p.nz)}
     if k.get("nn", {}).get("launches_per_step", 0) > 0:
         # one forward per Poisson solve; every solve ends with one k_cg_final
         fwd = k.get("cg_final", {}).get("launches_per_step", 0)
