@@ -62,11 +62,11 @@ def parse_args():
     ap.add_argument("--div-tol", type=float, default=1e-8,
                     help="second stopping test of every Poisson solve: max |div u| after the projection")
     ap.add_argument("--inner-tol", type=float, default=1e-3, help="relative tolerance of each FP32 inner solve")
-    ap.add_argument("--mg-omega", type=float, default=0.9, help="damping of the multigrid Jacobi sweeps")
+    ap.add_argument("--mg-omega", type=float, default=0.56, help="damping of the multigrid Jacobi sweeps")
     ap.add_argument("--mg-alpha", type=float, default=1.8, help="scale of the multigrid coarse-grid correction")
     ap.add_argument("--mg-kernels", type=int, default=0,
                     help="multigrid kernels: 0 vectorised per level, 1 one cell a thread, 2 with the cluster coarse levels")
-    ap.add_argument("--mg-omega2", type=float, default=0.0,
+    ap.add_argument("--mg-omega2", type=float, default=1.39,
                     help="weight of the second pre-smoothing (first post-smoothing) sweep; 0: --mg-omega")
     ap.add_argument("--path", choices=["all", "plain", "mixed", "learned"], default="all",
                     help="time every solver path (headline = learned + mixed precision) or one of them")
@@ -345,6 +345,7 @@ def c4_block(args, pkg, dev):
         if prec == 1:
             q.refine_maxit, q.inner_tol = 30, args.inner_tol
             q.mg_omega, q.mg_alpha = args.mg_omega, args.mg_alpha
+            q.mg_omega2 = args.mg_omega2
         s = pkg.Solver(q, device=dev)
         if learned:
             net, src = load_net(pkg, q, args, dev)

@@ -127,6 +127,7 @@ struct suli_ctx {
     // mixed-precision solve (precision = 1)
     std::vector<suli::MGLevel> mg;
     float *pc_x = nullptr, *pc_r = nullptr, *pc_pa = nullptr, *pc_pb = nullptr, *pc_q = nullptr;
+    float* pc_r2 = nullptr;   // the inner residual is updated from one buffer into the other
     double* cg_e2 = nullptr;
     double* cg_sd = nullptr;    // sqrt(d), stored once per solve (ghost values, the refinement's scaling)
     double* cg_isd = nullptr;   // 1/sqrt(d) (the coefficient scaling)
@@ -135,6 +136,7 @@ struct suli_ctx {
     float* f32_arena = nullptr;
     int coarse_sweeps = 40;
     bool cluster_ok = false;
+    bool fuse_update = false;   // the inner PCG update runs inside the level-0 pre-smoothing kernel
     int mg_kz = 2;             // cells along z a thread of the vectorised multigrid kernels owns (2 or 4)   // the device runs k_mg_cluster (16-CTA cluster with its shared memory)
     int inner_maxit = 200;
     int inner_batch = 4;
@@ -245,14 +247,15 @@ void launch_mx_residual(suli_ctx* c, const double* e_in, double* e_out, bool app
 void launch_pcg_init(suli_ctx* c, int maxit);
 // the loop condition of the inner-solve graph: non-zero while the inner solve is not done
 void launch_pcg_cond(suli_ctx* c, cudaGraphConditionalHandle h);
-void launch_vcycle(suli_ctx* c);
+void launch_vcycle(suli_ctx* c, const float* f0, bool pre_done = false);
 // ---- learned initial guess (k_learned.cu) ----
 void launch_nn_features(suli_ctx* c, float* in3);
 void launch_nn_features16(suli_ctx* c, void* in16);
 void launch_nn_features16_at(suli_ctx* c, void* in16, const double* r, const double* e);
 void launch_nn_step(suli_ctx* c, const float* out, double* e);
 void launch_nn_target(suli_ctx* c, const double* e_star, float* target);
-void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new);
+void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new, const float* r_old, float* r_new);
+int pcg_iter_kernels(const suli_ctx* c);
 int vcycle_kernels(const suli_ctx* c);
 void launch_posdin(suli_ctx* c);
 void launch_est(suli_ctx* c);

@@ -261,29 +261,43 @@ __global__ void k_volfix(Geo G, double* ls, const double* __restrict__ mod_ls, d
 struct ViscConst {
     double dx, dy, dz, cdel, csmag;   // cdel = (dx*dy*dz)**(2/3) computed on the host
 };
-template <typename R>
+// A thread owns KZ cells of a column (i, j, k0 .. k0 + KZ - 1); the loads of the unrolled loop
+// share their addresses between neighbouring cells (a plane's values serve the cell below and
+// the one above), so a cell costs about 21 distinct loads instead of 36 and all are issued
+// together.  KZ > 1 is used only when nz is a multiple of KZ.
+template <typename R, int KZ>
 __global__ void __launch_bounds__(256) k_nut(Geo G, ViscConst V, const double* __restrict__ u,
                                              const double* __restrict__ v, const double* __restrict__ w,
-                                             const double* __restrict__ rho, double* nut) {
-    const Thread3 t = tid3(1, 1, 1);
-    if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
-    const int i = t.i, j = t.j, k = t.k;
+                                             const double* __restrict__ rho, double* __restrict__ nut) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k0 = blockIdx.z * KZ + 1;
+    if (i > G.nx || j > G.ny || k0 > G.nz) return;
+    const int px = G.px, pxy = (int)G.pxy;
+    int cp[KZ + 3];   // index of (i, j, k0 - 1 + q)
+#pragma unroll
+    for (int q = 0; q < KZ + 3; ++q) cp[q] = G.idx32(i, j, k0 - 1) + q * pxy;
     const R itdx = R(1. / (2. * V.dx)), itdy = R(1. / (2. * V.dy)), itdz = R(1. / (2. * V.dz));
-    // derivax/y/z of the staggered fields, then interp?_fc to the cell centre
-    const R dudx = ((RLD(u, i + 1, j, k) - RLD(u, i - 1, j, k)) * itdx + (RLD(u, i + 2, j, k) - RLD(u, i, j, k)) * itdx) * R(0.5);
-    const R dudy = ((RLD(u, i, j + 1, k) - RLD(u, i, j - 1, k)) * itdy + (RLD(u, i + 1, j + 1, k) - RLD(u, i + 1, j - 1, k)) * itdy) * R(0.5);
-    const R dudz = ((RLD(u, i, j, k + 1) - RLD(u, i, j, k - 1)) * itdz + (RLD(u, i + 1, j, k + 1) - RLD(u, i + 1, j, k - 1)) * itdz) * R(0.5);
-    const R dvdx = ((RLD(v, i + 1, j, k) - RLD(v, i - 1, j, k)) * itdx + (RLD(v, i + 1, j + 1, k) - RLD(v, i - 1, j + 1, k)) * itdx) * R(0.5);
-    const R dvdy = ((RLD(v, i, j + 1, k) - RLD(v, i, j - 1, k)) * itdy + (RLD(v, i, j + 2, k) - RLD(v, i, j, k)) * itdy) * R(0.5);
-    const R dvdz = ((RLD(v, i, j, k + 1) - RLD(v, i, j, k - 1)) * itdz + (RLD(v, i, j + 1, k + 1) - RLD(v, i, j + 1, k - 1)) * itdz) * R(0.5);
-    const R dwdx = ((RLD(w, i + 1, j, k) - RLD(w, i - 1, j, k)) * itdx + (RLD(w, i + 1, j, k + 1) - RLD(w, i - 1, j, k + 1)) * itdx) * R(0.5);
-    const R dwdy = ((RLD(w, i, j + 1, k) - RLD(w, i, j - 1, k)) * itdy + (RLD(w, i, j + 1, k + 1) - RLD(w, i, j - 1, k + 1)) * itdy) * R(0.5);
-    const R dwdz = ((RLD(w, i, j, k + 1) - RLD(w, i, j, k - 1)) * itdz + (RLD(w, i, j, k + 2) - RLD(w, i, j, k)) * itdz) * R(0.5);
-    const R p1 = dudx + R(0.5) * (dudy + dvdx + dudz + dwdx);
-    const R p2 = dvdy + R(0.5) * (dvdx + dudy + dvdz + dwdy);
-    const R p3 = dwdz + R(0.5) * (dwdy + dvdz + dudz + dwdx);
-    const long long c = G.idx(i, j, k);
-    nut[c] = (double)(R(V.cdel * V.csmag * V.csmag) * sqrt(R(2.) * (p1 + p2 + p3) * (p1 + p2 + p3)) * R(rho[c]));
+#pragma unroll
+    for (int m = 0; m < KZ; ++m) {
+// a field value at (i + di, j + dj, k + dk) of cell k = k0 + m
+#define AT(a, di, dj, dk) R((a)[cp[m + 1 + (dk)] + (di) + (dj) * px])
+        // derivax/y/z of the staggered fields, then interp?_fc to the cell centre
+        const R dudx = ((AT(u, 1, 0, 0) - AT(u, -1, 0, 0)) * itdx + (AT(u, 2, 0, 0) - AT(u, 0, 0, 0)) * itdx) * R(0.5);
+        const R dudy = ((AT(u, 0, 1, 0) - AT(u, 0, -1, 0)) * itdy + (AT(u, 1, 1, 0) - AT(u, 1, -1, 0)) * itdy) * R(0.5);
+        const R dudz = ((AT(u, 0, 0, 1) - AT(u, 0, 0, -1)) * itdz + (AT(u, 1, 0, 1) - AT(u, 1, 0, -1)) * itdz) * R(0.5);
+        const R dvdx = ((AT(v, 1, 0, 0) - AT(v, -1, 0, 0)) * itdx + (AT(v, 1, 1, 0) - AT(v, -1, 1, 0)) * itdx) * R(0.5);
+        const R dvdy = ((AT(v, 0, 1, 0) - AT(v, 0, -1, 0)) * itdy + (AT(v, 0, 2, 0) - AT(v, 0, 0, 0)) * itdy) * R(0.5);
+        const R dvdz = ((AT(v, 0, 0, 1) - AT(v, 0, 0, -1)) * itdz + (AT(v, 0, 1, 1) - AT(v, 0, 1, -1)) * itdz) * R(0.5);
+        const R dwdx = ((AT(w, 1, 0, 0) - AT(w, -1, 0, 0)) * itdx + (AT(w, 1, 0, 1) - AT(w, -1, 0, 1)) * itdx) * R(0.5);
+        const R dwdy = ((AT(w, 0, 1, 0) - AT(w, 0, -1, 0)) * itdy + (AT(w, 0, 1, 1) - AT(w, 0, -1, 1)) * itdy) * R(0.5);
+        const R dwdz = ((AT(w, 0, 0, 1) - AT(w, 0, 0, -1)) * itdz + (AT(w, 0, 0, 2) - AT(w, 0, 0, 0)) * itdz) * R(0.5);
+#undef AT
+        const R p1 = dudx + R(0.5) * (dudy + dvdx + dudz + dwdx);
+        const R p2 = dvdy + R(0.5) * (dvdx + dudy + dvdz + dwdy);
+        const R p3 = dwdz + R(0.5) * (dwdy + dvdz + dudz + dwdx);
+        const int c = cp[m + 1];
+        nut[c] = (double)(R(V.cdel * V.csmag * V.csmag) * sqrt(R(2.) * (p1 + p2 + p3) * (p1 + p2 + p3)) * R(rho[c]));
+    }
 }
 
 // xnut/ynut/znut = face(ls_nu) + face(nut) with the end-face copy of interp?_cf
@@ -1295,7 +1309,8 @@ __global__ void k_cg_final(Geo G, BC bc, const double* __restrict__ sdv, const d
 constexpr int kPosZ = 8;
 __global__ void __launch_bounds__(256) k_posdin(Geo G, BC bc, double aux1, double aux2, double aux3,
                                                 const double* __restrict__ rho, const double* __restrict__ prd1,
-                                                double* u, double* v, double* w) {
+                                                double* __restrict__ u, double* __restrict__ v,
+                                                double* __restrict__ w) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k0 = blockIdx.z * kPosZ + 1;
     const int nx = G.nx, ny = G.ny, nz = G.nz;
@@ -1317,9 +1332,10 @@ __global__ void __launch_bounds__(256) k_posdin(Geo G, BC bc, double aux1, doubl
     }
 }
 
-// A thread walks a column of kEstZ cells (the w face above a cell is the face below the next
-// one), so a block reduces 16x more cells than one plane and there are 16x fewer partials.
-constexpr int kEstZ = 16;
+// A thread walks a column of kEstZ cells.  The loop is unrolled and loads from clamped plane
+// indices, so its loads are issued together; planes past nz are left out of the maximum.  The w
+// face above a cell is the face below the next one.
+constexpr int kEstZ = 4;
 __global__ void __launch_bounds__(256) k_est(Geo G, double dx, double dy, double dz, const double* __restrict__ u,
                                              const double* __restrict__ v, const double* __restrict__ w,
                                              double* partial, unsigned int* counter, double* out) {
@@ -1327,11 +1343,15 @@ __global__ void __launch_bounds__(256) k_est(Geo G, double dx, double dy, double
     const int k0 = blockIdx.z * kEstZ + 1;
     double m = 0.;
     if (i <= G.nx && j <= G.ny) {
-        const int k1 = min(k0 + kEstZ - 1, G.nz);
-        for (int k = k0; k <= k1; ++k) {
+        double wz[kEstZ + 1];
+#pragma unroll
+        for (int q = 0; q <= kEstZ; ++q) wz[q] = FIDX(w, i, j, min(k0 + q, G.nz + 1));
+#pragma unroll
+        for (int q = 0; q < kEstZ; ++q) {
+            const int k = min(k0 + q, G.nz);
             const double dv = (FIDX(u, i + 1, j, k) - FIDX(u, i, j, k)) / dx + (FIDX(v, i, j + 1, k) - FIDX(v, i, j, k)) / dy +
-                              (FIDX(w, i, j, k + 1) - FIDX(w, i, j, k)) / dz;
-            m = isnan(dv) ? INFINITY : fmax(m, fabs(dv));
+                              (wz[q + 1] - wz[q]) / dz;
+            if (k0 + q <= G.nz) m = isnan(dv) ? INFINITY : fmax(m, fabs(dv));
         }
     }
     double ta, tb;
@@ -1418,6 +1438,7 @@ void launch_volfix(suli_ctx* c, double dt1fac) {
     ProfScope ps(c, SULI_K_VOLFIX, 1);
     k_volfix<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->f[SULI_F_LS], c->f[SULI_F_MOD_LS], dt1fac, c->vol_ini);
 }
+constexpr int kNutZ = 4;   // cells of a column per thread in k_nut
 void launch_visco(suli_ctx* c) {
     const Geo& G = c->g;
     ProfScope ps(c, SULI_K_VISCO, c->P.m_turb == 1 ? 2 : 1);
@@ -1442,12 +1463,17 @@ void launch_visco(suli_ctx* c) {
         ViscConst V;
         V.dx = c->P.dx; V.dy = c->P.dy; V.dz = c->P.dz; V.csmag = c->P.csmag;
         V.cdel = pow(c->P.dx * c->P.dy * c->P.dz, 2. / 3.);
-        if (c->P.precision == 1)   // FP32 arithmetic over the FP64 state
-            k_nut<float><<<cells_grid(G), kBlk, 0, c->stream>>>(G, V, c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W],
-                                                               c->f[SULI_F_RHO], c->f[SULI_F_NUT]);
-        else
-            k_nut<double><<<cells_grid(G), kBlk, 0, c->stream>>>(G, V, c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W],
-                                                                c->f[SULI_F_RHO], c->f[SULI_F_NUT]);
+        const bool col = G.nz % kNutZ == 0;
+        const dim3 gn = grid3(G.nx, G.ny, col ? G.nz / kNutZ : G.nz, kBlk);
+        const double *u = c->f[SULI_F_U], *v = c->f[SULI_F_V], *w = c->f[SULI_F_W], *rho = c->f[SULI_F_RHO];
+        double* nut = c->f[SULI_F_NUT];
+        if (c->P.precision == 1) {   // FP32 arithmetic over the FP64 state
+            if (col) k_nut<float, kNutZ><<<gn, kBlk, 0, c->stream>>>(G, V, u, v, w, rho, nut);
+            else k_nut<float, 1><<<gn, kBlk, 0, c->stream>>>(G, V, u, v, w, rho, nut);
+        } else {
+            if (col) k_nut<double, kNutZ><<<gn, kBlk, 0, c->stream>>>(G, V, u, v, w, rho, nut);
+            else k_nut<double, 1><<<gn, kBlk, 0, c->stream>>>(G, V, u, v, w, rho, nut);
+        }
     }
     k_facenu<<<faces_grid(G), kBlk, 0, c->stream>>>(G, c->P.m_turb, c->f[SULI_F_LS_NU], c->f[SULI_F_NUT],
                                                      c->f[SULI_F_XNUT], c->f[SULI_F_YNUT], c->f[SULI_F_ZNUT]);

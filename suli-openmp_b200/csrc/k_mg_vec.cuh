@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_mgv_pre(Geo G, BC bc, 
 #pragma unroll
     for (int m = 0; m < KZ; ++m) {
         const int k = q.k0 + m;
-        if (k > G.nz) break;
+        if (KZ > 2 && k > G.nz) break;   // KZ = 2 runs only where nz is even
         const int c = q.c0 + pxy * k;
         Faces F[kVX];
         A.faces(G, q.i0, q.j, k, c, F);
@@ -138,6 +138,83 @@ __global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_mgv_pre(Geo G, BC bc, 
 #pragma unroll
         for (int e = 0; e < kVX; ++e) out[e] = col[m + 1][e] + omega2 * (fc.v[e] - ax[e]) * dc.v[e];
         st4(y, c, out);
+    }
+}
+
+// The inner PCG's update fused into the V-cycle's first level-0 kernel (k_pcgv_updc followed
+// by k_mgv_pre): with alpha from the SpMV's p.q, x += alpha p and r_out = r - alpha q at the
+// thread's cells, r.r and the inner stop test; the two pre-smoothing sweeps read the updated
+// residual at the neighbours too, formed there again from r and q (the same expression, so the
+// same value), which saves the update's own pass over x, p, r and q.  r is read from one buffer
+// and written to another, so no thread reads a neighbour's already-updated residual.  When the
+// stop test ends the loop, the V-cycle's other kernels return at once.
+template <int KZ, class Op4>
+__global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_mgv_preu(Geo G, BC bc, float* __restrict__ x,
+                                                  const float* __restrict__ p, const float* __restrict__ r,
+                                                  const float* __restrict__ qv, float* __restrict__ r_out, Op4 A,
+                                                  float* __restrict__ y, float omega, float omega2, PCGState* st,
+                                                  double* partial, unsigned int* counter) {
+    pdl_wait();
+    if (st->done) return;
+    const float alpha = (float)st->alpha;
+    const VQ q = vquad(G, bc, KZ);
+    double rr = 0.;
+    if (q.in) {
+        const int pxy = (int)G.pxy;
+        auto fr = [&](int cc, float (&o)[kVX]) {
+            const V4 a = ld4(r, cc), b = ld4(qv, cc);
+#pragma unroll
+            for (int e = 0; e < kVX; ++e) o[e] = a.v[e] - alpha * b.v[e];
+        };
+        auto x1 = [&](int cc, float (&o)[kVX]) {
+            float fv[kVX];
+            fr(cc, fv);
+            const V4 dv = A.inv_diag(cc);
+#pragma unroll
+            for (int e = 0; e < kVX; ++e) o[e] = omega * fv[e] * dv.v[e];
+        };
+        auto x1s = [&](int cc) {
+            const float fv = r[cc] - alpha * qv[cc];
+            return omega * fv * A.idg[cc];
+        };
+        float col[KZ + 2][kVX];
+#pragma unroll
+        for (int m = 0; m < KZ + 2; ++m) x1(q.c0 + pxy * map_any(q.k0 - 1 + m, G.nz, bc.perz), col[m]);
+#pragma unroll
+        for (int m = 0; m < KZ; ++m) {
+            const int k = q.k0 + m;
+            if (KZ > 2 && k > G.nz) break;   // KZ = 2 runs only where nz is even
+            const int c = q.c0 + pxy * k;
+            Faces F[kVX];
+            A.faces(G, q.i0, q.j, k, c, F);
+            float ym[kVX], yp[kVX], ax[kVX], out[kVX], fc[kVX];
+            x1(c + q.fym, ym);
+            x1(c + q.fyp, yp);
+            apply4(F, col[m + 1], x1s(c + q.fxm), x1s(c + kVX - 1 + q.fxp), ym, yp, col[m], col[m + 2], ax);
+            fr(c, fc);
+            const V4 dc = A.inv_diag(c);
+#pragma unroll
+            for (int e = 0; e < kVX; ++e) {
+                out[e] = col[m + 1][e] + omega2 * (fc[e] - ax[e]) * dc.v[e];
+                rr += (double)fc[e] * (double)fc[e];
+            }
+            st4(y, c, out);
+            st4(r_out, c, fc);
+            const V4 xv = ld4(x, c), pv = ld4(p, c);
+            float xo[kVX];
+#pragma unroll
+            for (int e = 0; e < kVX; ++e) xo[e] = xv.v[e] + alpha * pv.v[e];
+            st4(x, c, xo);
+        }
+    }
+    double t, u;
+    if (reduce2_last(rr, 0.0, partial, counter, t, u) && flat_tid() == 0) {
+        st->rr = t;
+        st->iters = st->iters + 1;
+        bool go = t > st->tol2;
+        if (st->iters >= st->maxit) go = false;
+        if (!isfinite(t)) { go = false; st->status = SULI_ERR_NAN; }
+        st->done = go ? 0 : 1;
     }
 }
 
@@ -163,7 +240,7 @@ __global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_mgv_jacc(Geo G, BC bc,
 #pragma unroll
         for (int m = 0; m < KZ; ++m) {
             const int k = q.k0 + m;
-            if (k > G.nz) break;
+            if (KZ > 2 && k > G.nz) break;   // KZ = 2 runs only where nz is even
             const int c = q.c0 + pxy * k;
             Faces F[kVX];
             A.faces(G, q.i0, q.j, k, c, F);
@@ -225,7 +302,7 @@ __global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_mgv_post(Geo Gf, Geo G
 #pragma unroll
     for (int m = 0; m < KZ; ++m) {
         const int k = q.k0 + m;
-        if (k > Gf.nz) break;
+        if (KZ > 2 && k > Gf.nz) break;   // KZ = 2 runs only where nz is even
         const int c = q.c0 + pxy * k;
         Faces F[kVX];
         A.faces(Gf, q.i0, q.j, k, c, F);
@@ -304,7 +381,7 @@ __global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_pcgv_spmvc(Geo G, BC b
 #pragma unroll
         for (int m = 0; m < KZ; ++m) {
             const int k = q.k0 + m;
-            if (k > G.nz) break;
+            if (KZ > 2 && k > G.nz) break;   // KZ = 2 runs only where nz is even
             const int c = q.c0 + pxy * k;
             Faces F[kVX];
             A.faces(G, q.i0, q.j, k, c, F);
@@ -327,9 +404,10 @@ __global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_pcgv_spmvc(Geo G, BC b
 }
 
 // x += alpha p, r -= alpha q, r.r and the inner stop test (k_pcg_updc)
-__global__ void __launch_bounds__(256) k_pcgv_updc(Geo G, float* __restrict__ x, float* __restrict__ r,
-                                                   const float* __restrict__ p, const float* __restrict__ qv,
-                                                   PCGState* st, double* partial, unsigned int* counter) {
+__global__ void __launch_bounds__(256) k_pcgv_updc(Geo G, float* __restrict__ x, const float* __restrict__ r,
+                                                   float* __restrict__ r_out, const float* __restrict__ p,
+                                                   const float* __restrict__ qv, PCGState* st, double* partial,
+                                                   unsigned int* counter) {
     pdl_wait();
     if (st->done) return;
     const float alpha = (float)st->alpha;
@@ -353,7 +431,7 @@ __global__ void __launch_bounds__(256) k_pcgv_updc(Geo G, float* __restrict__ x,
                 rr += (double)ro[e] * (double)ro[e];
             }
             st4(x, c, xo);
-            st4(r, c, ro);
+            st4(r_out, c, ro);
         }
     }
     double t, u;

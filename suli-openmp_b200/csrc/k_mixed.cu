@@ -451,9 +451,10 @@ __global__ void __launch_bounds__(256) k_pcg_spmvc(Geo G, BC bc, const float* __
 }
 
 constexpr int kKZU = 8;
-__global__ void __launch_bounds__(256) k_pcg_updc(Geo G, float* __restrict__ x, float* __restrict__ r,
-                                                  const float* __restrict__ p, const float* __restrict__ q,
-                                                  PCGState* st, double* partial, unsigned int* counter) {
+__global__ void __launch_bounds__(256) k_pcg_updc(Geo G, float* __restrict__ x, const float* __restrict__ r,
+                                                  float* __restrict__ r_out, const float* __restrict__ p,
+                                                  const float* __restrict__ q, PCGState* st, double* partial,
+                                                  unsigned int* counter) {
     pdl_wait();
     if (st->done) return;
     const float alpha = (float)st->alpha;
@@ -468,7 +469,7 @@ __global__ void __launch_bounds__(256) k_pcg_updc(Geo G, float* __restrict__ x, 
             const int c = c0 + pxy * k;
             x[c] = x[c] + alpha * p[c];
             const float rv = r[c] - alpha * q[c];
-            r[c] = rv;
+            r_out[c] = rv;
             rr += (double)rv * (double)rv;
         }
     }
@@ -657,9 +658,10 @@ void launch_pcg_init(suli_ctx* c, int maxit) {
 
 static inline OpRho4 from_rho4(const MGLevel& L) { return OpRho4{L.rho, L.idg, L.c2}; }
 // launch a column kernel of the vectorised family with the context's column depth (2 or 4)
+// (the depth-2 kernels assume an even nz, true of every level that is coarsened further)
 #define VLAUNCH(kern, Op, G, ...)                                                                          \
     do {                                                                                                   \
-        if (c->mg_kz == 2) pdl_launch(kern<2, Op>, vgrid((G), 2), kB2, c->stream, __VA_ARGS__);            \
+        if (c->mg_kz == 2 && (G).nz % 2 == 0) pdl_launch(kern<2, Op>, vgrid((G), 2), kB2, c->stream, __VA_ARGS__); \
         else pdl_launch(kern<4, Op>, vgrid((G), 4), kB2, c->stream, __VA_ARGS__);                         \
     } while (0)
 static inline OpStored4 stored4(const MGLevel& L) { return OpStored4{L.sx, L.sy, L.sz, L.idg}; }
@@ -668,13 +670,13 @@ static inline bool vec_level(const suli_ctx* c, const Geo& g) { return c->P.mg_k
 
 // pre-smoothing (weights om, then om2) and restriction of level l (level 0 forms its faces from
 // the density)
-static void vc_down(suli_ctx* c, int l, const float* f, float om, float om2) {
+static void vc_down(suli_ctx* c, int l, const float* f, float om, float om2, bool pre_done = false) {
     MGLevel& M = c->mg[l];
     MGLevel& C = c->mg[l + 1];
     const BC bc = c->bc;
     if (vec_level(c, M.g)) {
         if (l == 0) {
-            VLAUNCH(k_mgv_pre, OpRho4, M.g, M.g, bc, f, from_rho4(M), M.y, om, om2, c->pcg);
+            if (!pre_done) VLAUNCH(k_mgv_pre, OpRho4, M.g, M.g, bc, f, from_rho4(M), M.y, om, om2, c->pcg);
             pdl_launch(k_mgv_restrict<OpRho4>, vgrid_restrict(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, from_rho4(M),
                        C.f, c->pcg);
         } else {
@@ -741,6 +743,9 @@ int cluster_ready(suli_ctx* c) {
     c->mg_kz = 2;
     if (const char* ev = std::getenv("SULI_MG_KZ"))   // column depth of the vectorised kernels
         if (std::strcmp(ev, "4") == 0) c->mg_kz = 4;
+    c->fuse_update = false;
+    if (const char* ev = std::getenv("SULI_FUSED_UPDATE"))   // the PCG update inside the pre-smoothing
+        if (std::strcmp(ev, "1") == 0) c->fuse_update = true;
     if (const char* ev = std::getenv("SULI_NO_CLUSTER"))   // keep the per-level kernels
         if (std::strcmp(ev, "1") == 0) return SULI_OK;
     const int L = (int)c->mg.size();
@@ -802,32 +807,41 @@ static void launch_cluster(suli_ctx* c, float om, float alpha) {
     cudaLaunchKernelEx(&cfg, k_mg_cluster, a, (const PCGState*)c->pcg);
 }
 
-// z = M r: one V-cycle; the last level-0 sweep also forms r.z and beta
-void launch_vcycle(suli_ctx* c) {
+// z = M r for the level-0 right-hand side f0: one V-cycle; the last level-0 sweep also forms r.z
+// and beta.  pre_done: the level-0 pre-smoothing already ran (fused with the PCG update).
+void launch_vcycle(suli_ctx* c, const float* f0, bool pre_done) {
     const float om = (float)c->P.mg_omega;
     const float om2 = (float)c->P.mg_omega2;
     const float alpha = (float)c->P.mg_alpha;
     const int L = (int)c->mg.size();
     const BC bc = c->bc;
     if (use_cluster(c)) {   // levels 0 .. L-4 as kernels per level, the last three in the cluster
-        for (int l = 0; l < L - 3; ++l) vc_down(c, l, l == 0 ? c->pc_r : c->mg[l].f, om, om2);
+        for (int l = 0; l < L - 3; ++l) vc_down(c, l, l == 0 ? f0 : c->mg[l].f, om, om2, pre_done);
         launch_cluster(c, om, alpha);
-        for (int l = L - 4; l >= 0; --l) vc_up(c, l, l == 0 ? c->pc_r : c->mg[l].f, om, om2, alpha);
+        for (int l = L - 4; l >= 0; --l) vc_up(c, l, l == 0 ? f0 : c->mg[l].f, om, om2, alpha);
         return;
     }
-    for (int l = 0; l < L - 1; ++l) vc_down(c, l, l == 0 ? c->pc_r : c->mg[l].f, om, om2);
+    for (int l = 0; l < L - 1; ++l) vc_down(c, l, l == 0 ? f0 : c->mg[l].f, om, om2, pre_done);
     MGLevel& B = c->mg[L - 1];
     if (L == 1) {   // a single level: coarsest sweeps, then one more sweep that forms r.z
-        pdl_launch(k_mg_coarsest, 1, 1024, c->stream, B.g, bc, c->pc_r, stored(B), B.x, c->coarse_sweeps, om, c->pcg);
-        pdl_launch(k_mg_jac, cells3(B.g), kB2, c->stream, B.g, bc, B.x, c->pc_r, stored(B), B.y, om, c->pcg, 1,
+        pdl_launch(k_mg_coarsest, 1, 1024, c->stream, B.g, bc, f0, stored(B), B.x, c->coarse_sweeps, om, c->pcg);
+        pdl_launch(k_mg_jac, cells3(B.g), kB2, c->stream, B.g, bc, B.x, f0, stored(B), B.y, om, c->pcg, 1,
                    c->red_partial, c->red_counter);
         return;
     }
     pdl_launch(k_mg_coarsest, 1, 1024, c->stream, B.g, bc, B.f, stored(B), B.y, c->coarse_sweeps, om, c->pcg);
-    for (int l = L - 2; l >= 0; --l) vc_up(c, l, l == 0 ? c->pc_r : c->mg[l].f, om, om2, alpha);
+    for (int l = L - 2; l >= 0; --l) vc_up(c, l, l == 0 ? f0 : c->mg[l].f, om, om2, alpha);
 }
 
-void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new) {
+// the update fuses into the level-0 pre-smoothing (SULI_FUSED_UPDATE=1) where the level uses
+// the vectorised kernels and there is a level below it.  Measured at 256x128x128 the fused
+// kernel is slower than the two it replaces (195 against 184 us an inner iteration: it reads r
+// and q at the neighbours), so it is not the default.
+static bool fused_update(const suli_ctx* c) { return c->fuse_update && c->mg.size() > 1 && vec_level(c, c->g); }
+
+// one inner PCG iteration: p = z + beta p_old, q = A p (p.q -> alpha); x += alpha p,
+// r_new = r_old - alpha q (r.r -> stop test); z = M r_new (r.z -> beta)
+void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new, const float* r_old, float* r_new) {
     const Geo& G = c->g;
     MGLevel& M0 = c->mg[0];
     const bool vec = vec_level(c, G);
@@ -845,20 +859,29 @@ void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new) {
                        stored(M0), c->pcg, c->red_partial, c->red_counter);
         }
     }
+    if (fused_update(c)) {
+        ProfScope ps(c, SULI_K_MG, vcycle_kernels(c));
+        VLAUNCH(k_mgv_preu, OpRho4, G, G, c->bc, c->pc_x, p_new, r_old, c->pc_q, r_new, from_rho4(M0), M0.y,
+                (float)c->P.mg_omega, (float)c->P.mg_omega2, c->pcg, c->red_partial, c->red_counter);
+        launch_vcycle(c, r_new, true);
+        return;
+    }
     {
         ProfScope ps(c, SULI_K_CG_UPDATE, 1);
         if (vec) {
-            pdl_launch(k_pcgv_updc, vgrid_upd(G), kB2, c->stream, G, c->pc_x, c->pc_r, p_new, c->pc_q, c->pcg,
+            pdl_launch(k_pcgv_updc, vgrid_upd(G), kB2, c->stream, G, c->pc_x, r_old, r_new, p_new, c->pc_q, c->pcg,
                        c->red_partial, c->red_counter);
         } else {
             const dim3 gu((G.nx + 31) / 32, (G.ny + 7) / 8, (G.nz + kKZU - 1) / kKZU);
-            pdl_launch(k_pcg_updc, gu, kB2, c->stream, G, c->pc_x, c->pc_r, p_new, c->pc_q, c->pcg, c->red_partial,
-                       c->red_counter);
+            pdl_launch(k_pcg_updc, gu, kB2, c->stream, G, c->pc_x, r_old, r_new, p_new, c->pc_q, c->pcg,
+                       c->red_partial, c->red_counter);
         }
     }
     ProfScope ps(c, SULI_K_MG, vcycle_kernels(c));
-    launch_vcycle(c);
+    launch_vcycle(c, r_new);
 }
+
+int pcg_iter_kernels(const suli_ctx* c) { return fused_update(c) ? 1 + vcycle_kernels(c) : 2 + vcycle_kernels(c); }
 
 int vcycle_kernels(const suli_ctx* c) {
     const int L = (int)c->mg.size();

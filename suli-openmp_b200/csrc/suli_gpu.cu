@@ -262,14 +262,14 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
             nx /= 2; ny /= 2; nz /= 2;
             gs.push_back(make_geo(nx, ny, nz));
         }
-        size_t tot = 6 * (size_t)gs[0].n + 64;
+        size_t tot = 7 * (size_t)gs[0].n + 64;
         for (auto& g : gs) tot += 7 * (size_t)g.n;
         if ((e = cudaMalloc(&c->f32_arena, tot * sizeof(float))) != cudaSuccess) return bail(e, "f32 arena");
         if ((e = cudaMemsetAsync(c->f32_arena, 0, tot * sizeof(float), c->stream)) != cudaSuccess) return bail(e, "memset");
         float* q = c->f32_arena;
         auto take = [&](size_t n) { float* r = q; q += n; return r; };
         c->pc_x = take(gs[0].n); c->pc_r = take(gs[0].n); c->pc_pa = take(gs[0].n); c->pc_pb = take(gs[0].n);
-        c->pc_q = take(gs[0].n);
+        c->pc_q = take(gs[0].n); c->pc_r2 = take(gs[0].n);
         for (auto& g : gs) {
             MGLevel L;
             L.g = g;
@@ -683,12 +683,12 @@ int ensure_pcg_loop(suli_ctx* c) {
     if (int r = make_loop_graph(
             c, &c->pcg_loop,
             [&] {
-                launch_pcg_iter(c, c->pc_pa, c->pc_pb);
-                launch_pcg_iter(c, c->pc_pb, c->pc_pa);
+                launch_pcg_iter(c, c->pc_pa, c->pc_pb, c->pc_r2, c->pc_r);
+                launch_pcg_iter(c, c->pc_pb, c->pc_pa, c->pc_r, c->pc_r2);
             },
             [&](cudaGraphConditionalHandle h) { launch_pcg_cond(c, h); }, "inner-solve graph"))
         return r;
-    c->pcg_graph_kernels = 2 + vcycle_kernels(c);
+    c->pcg_graph_kernels = pcg_iter_kernels(c);
     return SULI_OK;
 }
 
@@ -835,16 +835,16 @@ int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
         launch_pcg_init(c, c->inner_maxit);
         {
             ProfScope ps(c, SULI_K_MG, vcycle_kernels(c));
-            launch_vcycle(c);
+            launch_vcycle(c, c->pc_r);
         }
-        launch_pcg_iter(c, c->mg[0].y, c->pc_pa);   // p_old = z with beta = 0
+        launch_pcg_iter(c, c->mg[0].y, c->pc_pa, c->pc_r, c->pc_r2);   // p_old = z with beta = 0
         if (c->use_graphs) {
             ProfScope ps(c, SULI_K_MG, 0);   // kernel launches are counted below, once known
             CUDA_TRY(c, cudaGraphLaunch(c->pcg_loop, c->stream));
         } else {
             for (int pair = 0; pair < c->inner_maxit; ++pair) {
-                launch_pcg_iter(c, c->pc_pa, c->pc_pb);
-                launch_pcg_iter(c, c->pc_pb, c->pc_pa);
+                launch_pcg_iter(c, c->pc_pa, c->pc_pb, c->pc_r2, c->pc_r);
+                launch_pcg_iter(c, c->pc_pb, c->pc_pa, c->pc_r, c->pc_r2);
                 CHECK_LAUNCH(c);
                 if (int rr = sync_read(c, c->pcg, c->pcg_host, sizeof(PCGState))) return rr;
                 if (c->pcg_host[0].done) break;

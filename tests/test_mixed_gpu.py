@@ -135,6 +135,29 @@ def test_column_depths_agree(pkg, monkeypatch):
         assert float(np.abs(v4[f] - v2[f]).max()) <= 1e-9 * vs, f
 
 
+def test_fused_update_matches_separate_update(pkg, monkeypatch):
+    """The inner PCG update inside the level-0 pre-smoothing kernel (SULI_FUSED_UPDATE=1)
+    against the separate update kernel (default): the same residual values, r.r summed in
+    another grouping; dam break 128x64x64, two steps: iteration counts within 2, velocities
+    within 1e-9 of their scale."""
+    res = {}
+    for fu in ("1", "0"):
+        monkeypatch.setenv("SULI_FUSED_UPDATE", fu)
+        p, init = pkg.cases.dam_break(nx=128, ny=64, nz=64, dx=0.005, cg_tol=1e-10)
+        p.precision, p.inner_tol, p.refine_maxit = 1, 1e-4, 30
+        s = pkg.Solver(p)
+        init(s)
+        steps = [s.step(it) for it in (1, 2)]
+        assert all(st["status"] == 0 for st in steps)
+        res[fu] = ([sum(st["cg_iters"]) for st in steps], {f: s.download(f) for f in ("u", "v", "w")})
+        s.close()
+    (i1, v1), (i0, v0) = res["1"], res["0"]
+    assert all(abs(a - b) <= 2 for a, b in zip(i1, i0)), (i1, i0)
+    vs = max(float(np.abs(b).max()) for b in v0.values())
+    for f in v0:
+        assert float(np.abs(v1[f] - v0[f]).max()) <= 1e-9 * vs, f
+
+
 @pytest.mark.parametrize("case", ["dam_break", "periodic"])
 def test_vector_kernels_match_one_cell_kernels(pkg, case):
     """The 4-cells-a-thread multigrid/PCG kernels (mg_kernels = 0) against the one-cell kernels
