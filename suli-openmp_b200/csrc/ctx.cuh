@@ -1,6 +1,7 @@
 // ctx.cuh — the solver context: device field arena, scalars, scratch, and the kernel
 // launchers shared by the host API (suli_gpu.cu) and the kernel translation units.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <string>
 #include <vector>
@@ -135,9 +136,16 @@ struct suli_ctx {
     suli::PCGState* pcg_host = nullptr;
     float* f32_arena = nullptr;
     int coarse_sweeps = 40;
-    bool cluster_ok = false;
+    bool cluster_ok = false;    // the device runs k_mg_cluster (16-CTA cluster with its shared memory)
     bool fuse_update = false;   // the inner PCG update runs inside the level-0 pre-smoothing kernel
-    int mg_kz = 2;             // cells along z a thread of the vectorised multigrid kernels owns (2 or 4)   // the device runs k_mg_cluster (16-CTA cluster with its shared memory)
+    int mg_kz = 2;              // cells along z a thread of the vectorised multigrid kernels owns (2 or 4)
+    // level-0 kernels that stream z-planes through shared memory with TMA (k_mg_stream.cuh):
+    // one tensor map per level-0 array they read, the planes a CTA computes, and whether they run
+    bool stream_ok = false;
+    int stream_chunk = 16;
+    int n_smap = 0;
+    CUtensorMap smap[12];
+    const float* smap_ptr[12] = {nullptr};
     int inner_maxit = 200;
     int inner_batch = 4;
     int last_outer_iters = 0;
@@ -240,6 +248,7 @@ void launch_cg_iter(suli_ctx* c, const double* p_old, double* p_new);
 void launch_cg_cond(suli_ctx* c, cudaGraphConditionalHandle h);
 void launch_cg_divcheck(suli_ctx* c);
 int cluster_ready(suli_ctx* c);
+int stream_ready(suli_ctx* c);
 void launch_cg_final(suli_ctx* c, const double* e);
 // ---- mixed-precision solve (k_mixed.cu) ----
 void launch_mx_setup(suli_ctx* c);

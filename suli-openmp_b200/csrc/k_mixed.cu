@@ -12,7 +12,10 @@
 // Jacobi sweeps before and after, a one-block Jacobi solve on the coarsest grid.  Pre- and
 // post-smoothing mirror each other, so the V-cycle is a symmetric positive operator and plain
 // (not flexible) PCG applies.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -604,6 +607,7 @@ __global__ void k_zero_f(float* a, long long n) {
 }  // namespace suli
 #include "k_mg_vec.cuh"
 #include "k_mg_cluster.cuh"
+#include "k_mg_stream.cuh"
 namespace suli {
 
 // ------------------------------------------------------------------------------------
@@ -668,6 +672,120 @@ static inline OpStored4 stored4(const MGLevel& L) { return OpStored4{L.sx, L.sy,
 // the 4-cells-a-thread kernels on a level (mg_kernels 0 or 2 and x divisible by 4)
 static inline bool vec_level(const suli_ctx* c, const Geo& g) { return c->P.mg_kernels != 1 && g.nx % kVX == 0; }
 
+// ---- level-0 kernels streaming z-planes through shared memory (k_mg_stream.cuh)
+static PFN_cuTensorMapEncodeTiled_v12000 plane_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+// a level-0 FP32 array as a 3-D tensor {px, py, nz + 3} (x = kBase + i - 1 within row j of
+// plane k), box {kSBoxX, kSBoxY, 1}, zero fill outside
+static bool add_plane_map(suli_ctx* c, const float* a) {
+    auto enc = plane_map_encoder();
+    const Geo& g = c->mg[0].g;
+    if (!enc || !a || (reinterpret_cast<uintptr_t>(a) & 15) || c->n_smap >= 12) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)(g.nz + 3)};
+    cuuint64_t strides[2] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.pxy * 4};
+    cuuint32_t box[3] = {(cuuint32_t)kSBoxX, (cuuint32_t)kSBoxY, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    if (enc(&c->smap[c->n_smap], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(a), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    c->smap_ptr[c->n_smap++] = a;
+    return true;
+}
+static const CUtensorMap& plane_map(const suli_ctx* c, const float* a) {
+    for (int q = 0; q < c->n_smap; ++q)
+        if (c->smap_ptr[q] == a) return c->smap[q];
+    return c->smap[0];   // not reached: every array the streaming kernels read has a map
+}
+
+// Decide once per context whether level 0 runs the streaming kernels: vectorised kernels on a
+// multigrid hierarchy (mg_kernels 0), nx a multiple of 16, no periodic x or y axis, a tensor map
+// for every level-0 array they read, and two CTAs' shared memory an SM.  SULI_NO_STREAM=1
+// keeps the vectorised level-0 kernels; SULI_STREAM_CHUNK sets the planes a CTA computes.
+int stream_ready(suli_ctx* c) {
+    c->stream_ok = false;
+    c->n_smap = 0;
+    if (const char* ev = std::getenv("SULI_NO_STREAM"))
+        if (std::strcmp(ev, "1") == 0) return SULI_OK;
+    if (c->mg.size() < 2 || c->P.mg_kernels != 0) return SULI_OK;
+    const Geo& g = c->mg[0].g;
+    if (g.nx % 16 != 0 || g.px < g.nx + 16 || c->bc.perx || c->bc.pery) return SULI_OK;
+    const MGLevel& M0 = c->mg[0];
+    const float* arrays[] = {c->pc_r, c->pc_r2, M0.x, M0.y, c->pc_pa, c->pc_pb, M0.idg, M0.rho};
+    for (const float* a : arrays)
+        if (!add_plane_map(c, a)) { c->n_smap = 0; return SULI_OK; }
+    const int s3 = (int)stream_smem_bytes(3), s4 = (int)stream_smem_bytes(4);
+    if (cudaFuncSetAttribute(k_mgs_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, s3) != cudaSuccess ||
+        cudaFuncSetAttribute(k_pcgs_spmvc, cudaFuncAttributeMaxDynamicSharedMemorySize, s3) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mgs_jacc, cudaFuncAttributeMaxDynamicSharedMemorySize, s4) != cudaSuccess) {
+        cudaGetLastError();
+        return SULI_OK;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mgs_jacc, kSTX * kSTY, s4) != cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        return SULI_OK;
+    }
+    // planes a CTA computes: as many chunks as fill the SMs' CTA slots once
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+    const int tiles = ((g.nx + kSTileX - 1) / kSTileX) * ((g.ny + kSTY - 1) / kSTY);
+    const int chunks = std::max(1, std::min(g.nz, (per_sm * nsm) / std::max(tiles, 1)));
+    c->stream_chunk = (g.nz + chunks - 1) / chunks;
+    if (const char* ev = std::getenv("SULI_STREAM_CHUNK")) {   // planes a CTA computes, for tests
+        const int v = std::atoi(ev);
+        if (v >= 1 && v <= g.nz) c->stream_chunk = v;
+    }
+    c->stream_ok = true;
+    return SULI_OK;
+}
+
+template <typename... KArgs, typename... Args>
+static void stream_launch(suli_ctx* c, void (*kernel)(KArgs...), size_t smem, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = sgrid(c->mg[0].g, c->stream_chunk);
+    cfg.blockDim = dim3(kSTX, kSTY, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+static void launch_stream_pre(suli_ctx* c, const float* f, float om, float om2) {
+    const MGLevel& M = c->mg[0];
+    stream_launch(c, k_mgs_pre, stream_smem_bytes(3), M.g, c->bc, plane_map(c, f), plane_map(c, M.idg),
+                  plane_map(c, M.rho), (const float*)M.c2, M.y, om, om2, c->stream_chunk, c->pcg);
+}
+static void launch_stream_jacc(suli_ctx* c, const float* f, float om) {
+    const MGLevel& M = c->mg[0];
+    stream_launch(c, k_mgs_jacc, stream_smem_bytes(4), M.g, c->bc, plane_map(c, M.x), plane_map(c, f),
+                  plane_map(c, M.idg), plane_map(c, M.rho), (const float*)M.c2, M.y, om, c->stream_chunk, c->pcg,
+                  c->red_partial, c->red_counter);
+}
+static void launch_stream_spmvc(suli_ctx* c, const float* p_old, float* p_new) {
+    const MGLevel& M = c->mg[0];
+    stream_launch(c, k_pcgs_spmvc, stream_smem_bytes(3), M.g, c->bc, plane_map(c, M.y), plane_map(c, p_old),
+                  plane_map(c, M.rho), (const float*)M.c2, p_new, c->pc_q, c->stream_chunk, c->pcg, c->red_partial,
+                  c->red_counter);
+}
+
 // pre-smoothing (weights om, then om2) and restriction of level l (level 0 forms its faces from
 // the density)
 static void vc_down(suli_ctx* c, int l, const float* f, float om, float om2, bool pre_done = false) {
@@ -676,7 +794,10 @@ static void vc_down(suli_ctx* c, int l, const float* f, float om, float om2, boo
     const BC bc = c->bc;
     if (vec_level(c, M.g)) {
         if (l == 0) {
-            if (!pre_done) VLAUNCH(k_mgv_pre, OpRho4, M.g, M.g, bc, f, from_rho4(M), M.y, om, om2, c->pcg);
+            if (!pre_done) {
+                if (c->stream_ok) launch_stream_pre(c, f, om, om2);
+                else VLAUNCH(k_mgv_pre, OpRho4, M.g, M.g, bc, f, from_rho4(M), M.y, om, om2, c->pcg);
+            }
             pdl_launch(k_mgv_restrict<OpRho4>, vgrid_restrict(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, from_rho4(M),
                        C.f, c->pcg);
         } else {
@@ -705,8 +826,9 @@ static void vc_up(suli_ctx* c, int l, const float* f, float om, float om2, float
     if (vec_level(c, M.g)) {
         if (l == 0) {
             VLAUNCH(k_mgv_post, OpRho4, M.g, M.g, C.g, bc, M.y, C.y, f, from_rho4(M), M.x, om2, alpha, c->pcg);
-            VLAUNCH(k_mgv_jacc, OpRho4, M.g, M.g, bc, M.x, f, from_rho4(M), M.y, om, c->pcg, dot, c->red_partial,
-                    c->red_counter);
+            if (c->stream_ok) launch_stream_jacc(c, f, om);
+            else VLAUNCH(k_mgv_jacc, OpRho4, M.g, M.g, bc, M.x, f, from_rho4(M), M.y, om, c->pcg, dot, c->red_partial,
+                         c->red_counter);
         } else {
             VLAUNCH(k_mgv_post, OpStored4, M.g, M.g, C.g, bc, M.y, C.y, f, stored4(M), M.x, om2, alpha, c->pcg);
             VLAUNCH(k_mgv_jacc, OpStored4, M.g, M.g, bc, M.x, f, stored4(M), M.y, om, c->pcg, dot, c->red_partial,
@@ -848,7 +970,9 @@ void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new, const float*
     {
         ProfScope ps(c, SULI_K_CG_SPMV, 1);
         if (c->mg.size() > 1) {
-            if (vec)
+            if (c->stream_ok)
+                launch_stream_spmvc(c, p_old, p_new);
+            else if (vec)
                 VLAUNCH(k_pcgv_spmvc, OpRho4, G, G, c->bc, M0.y, p_old, p_new, c->pc_q, from_rho4(M0), c->pcg,
                         c->red_partial, c->red_counter);
             else

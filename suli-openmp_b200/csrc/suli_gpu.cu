@@ -284,6 +284,7 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
         if ((e = cudaMemsetAsync(c->pcg, 0, sizeof(PCGState), c->stream)) != cudaSuccess) return bail(e, "memset");
         if ((e = cudaMallocHost(&c->pcg_host, 2 * sizeof(PCGState))) != cudaSuccess) return bail(e, "pinned");
         cluster_ready(c);
+        stream_ready(c);
     }
     if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bail(e, "sync");
     c->dt = p->dt;

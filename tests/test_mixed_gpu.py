@@ -135,6 +135,35 @@ def test_column_depths_agree(pkg, monkeypatch):
         assert float(np.abs(v4[f] - v2[f]).max()) <= 1e-9 * vs, f
 
 
+@pytest.mark.parametrize("shape,chunk", [((128, 64, 64), None), ((64, 36, 24), None), ((128, 64, 64), "7")])
+def test_streaming_kernels_match_vectorised(pkg, monkeypatch, shape, chunk):
+    """The level-0 kernels that stream z-planes through shared memory with TMA (default where
+    they apply) against the vectorised level-0 kernels (SULI_NO_STREAM=1): per cell the same
+    arithmetic, the FP64 dot products grouped differently.  Dam break at 128x64x64 (2 planes a
+    CTA), at 64x36x24 (rows not a multiple of the 8-row tile, 1 plane a CTA) and at 128x64x64
+    with 7 planes a CTA (SULI_STREAM_CHUNK: the slot ring wraps, the last CTA of a column has 1
+    plane); two steps: iteration counts within 2, velocities within 1e-9 of their scale."""
+    res = {}
+    if chunk:
+        monkeypatch.setenv("SULI_STREAM_CHUNK", chunk)
+    for ns in ("1", "0"):
+        monkeypatch.setenv("SULI_NO_STREAM", ns)
+        nx, ny, nz = shape
+        p, init = pkg.cases.dam_break(nx=nx, ny=ny, nz=nz, dx=0.005, cg_tol=1e-10)
+        p.precision, p.inner_tol, p.refine_maxit = 1, 1e-4, 30
+        s = pkg.Solver(p)
+        init(s)
+        steps = [s.step(it) for it in (1, 2)]
+        assert all(st["status"] == 0 for st in steps)
+        res[ns] = ([sum(st["cg_iters"]) for st in steps], {f: s.download(f) for f in ("u", "v", "w")})
+        s.close()
+    (i1, v1), (i0, v0) = res["1"], res["0"]
+    assert all(abs(a - b) <= 2 for a, b in zip(i1, i0)), (i1, i0)
+    vs = max(float(np.abs(b).max()) for b in v1.values())
+    for f in v1:
+        assert float(np.abs(v1[f] - v0[f]).max()) <= 1e-9 * vs, f
+
+
 def test_fused_update_matches_separate_update(pkg, monkeypatch):
     """The inner PCG update inside the level-0 pre-smoothing kernel (SULI_FUSED_UPDATE=1)
     against the separate update kernel (default): the same residual values, r.r summed in
