@@ -142,9 +142,12 @@ struct suli_ctx {
     // level-0 kernels that stream z-planes through shared memory with TMA (k_mg_stream.cuh):
     // one tensor map per level-0 array they read, the planes a CTA computes, and whether they run
     bool stream_ok = false;
+    bool stream_post_ok = false;   // also the post-smoothing (nx a multiple of 32)
     int stream_chunk = 16;
     int n_smap = 0;
-    CUtensorMap smap[12];
+    CUtensorMap smap_c;            // level 1's correction, the post-smoothing's prolongation source
+    CUtensorMap smap[12];          // boxes with the halo
+    CUtensorMap smap_own[12];      // the same arrays, boxes of the tile's own cells
     const float* smap_ptr[12] = {nullptr};
     int inner_maxit = 200;
     int inner_batch = 4;

@@ -35,8 +35,23 @@ constexpr int kSBoxY = kSTY + 2;                               // one row on eac
 constexpr int kSBoxBytes = kSBoxX * kSBoxY * 4;                // 5440
 constexpr int kSSlotBytes = (kSBoxBytes + 127) / 128 * 128;    // TMA destinations 128-byte aligned
 constexpr int kSR = 5;                                         // ring: planes k-1, k, k+1 + 2 ahead
+// the coarse level's box (the prolongation source of the post-smoothing): the parents of the
+// tile's cells and of their neighbours, 72 floats x 6 rows from coarse cell 64 bx - 3, row 4 by
+constexpr int kSCBoxX = 72, kSCBoxY = 6;
+constexpr int kSCBoxBytes = kSCBoxX * kSCBoxY * 4;              // 1728
+constexpr int kSCSlotBytes = (kSCBoxBytes + 127) / 128 * 128;
 
-static inline size_t stream_smem_bytes(int nf) { return (size_t)kSR * nf * kSSlotBytes + kSR * sizeof(uint64_t); }
+// a field read only at the thread's own cells: the tile without halo, 128 floats x 8 rows
+constexpr int kSOBoxX = kSTileX, kSOBoxY = kSTY;
+constexpr int kSOBoxBytes = kSOBoxX * kSOBoxY * 4;              // 4096
+constexpr int kSOSlotBytes = kSOBoxBytes;
+
+static inline size_t stream_stage_bytes(int nf, int no, int nc) {
+    return (size_t)nf * kSSlotBytes + (size_t)no * kSOSlotBytes + (size_t)nc * kSCSlotBytes;
+}
+static inline size_t stream_smem_bytes(int nf, int no = 0, int nc = 0) {
+    return kSR * stream_stage_bytes(nf, no, nc) + kSR * sizeof(uint64_t) + 2 * kSTX * kSTY * sizeof(float);
+}
 
 __device__ __forceinline__ uint32_t s_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ bool s_try_wait(uint32_t bar, uint32_t parity) {
@@ -69,6 +84,13 @@ __device__ __forceinline__ V4 sq(const float* s, int ly, int lx) {
     return V4{{t.x, t.y, t.z, t.w}};
 }
 __device__ __forceinline__ float ss(const float* s, int ly, int lx) { return s[ly * kSBoxX + lx]; }
+// the thread's quad in a slot of a field read at its own cells only
+__device__ __forceinline__ V4 sqo(const float* s) {
+    const float4 t = *reinterpret_cast<const float4*>(s + threadIdx.y * kSOBoxX + kVX * threadIdx.x);
+    return V4{{t.x, t.y, t.z, t.w}};
+}
+// one value of a coarse slot (row pitch kSCBoxX)
+__device__ __forceinline__ float ssc(const float* s, int ly, int lx) { return s[ly * kSCBoxX + lx]; }
 
 // A thread's quad in the tile and the tile positions of its neighbours: the unknowns' Neumann
 // map (a neighbour outside the box is the cell itself) and the faces' clamped end rule (the
@@ -117,44 +139,64 @@ __device__ __forceinline__ void s_faces(const STile& t, int k, int nz, const flo
     }
 }
 
-// The plane engine.  Body::plane(k, sm, s0, sp) computes plane k from the slots (one pointer a
-// field) of the planes k-1, k, k+1.  Returns false if a wait ran out.
-template <int NF>
+// The plane engine.  NF fine fields with the halo, NO fine fields at the tile's own cells (box
+// kSOBox) and NC coarse fields (the parent planes, box kSCBox) are loaded for every plane of the
+// sequence.  body.begin() runs before the first wait, body.plane(k,
+// sm, s0, sp) computes plane k from the slots (one pointer a field, fine then coarse) of the
+// planes k-1, k, k+1, and body.finish() runs after a barrier that follows the last
+// plane.  A scratch of 2 floats a thread (body.xbuf) follows the barriers.  Returns false if a
+// wait ran out.
+template <int NF, int NO, int NC>
 struct SSlots {
-    const float* f[NF];
+    const float* f[NF + NO + NC];   // fine fields with halo, own-cell fields, coarse fields
 };
-template <int NF, class Body>
-__device__ __forceinline__ bool s_march(const Geo& G, const BC& bc, const CUtensorMap* const (&maps)[NF], int chunk,
-                                        Body& body, PCGState* st) {
+template <int NF, int NO, int NC, class Body>
+__device__ __forceinline__ bool s_march(const Geo& G, const BC& bc, const CUtensorMap* const (&maps)[NF + NO + NC],
+                                        int chunk, Body& body, PCGState* st) {
     extern __shared__ __align__(128) unsigned char s_smem[];
+    constexpr size_t kStage = (size_t)NF * kSSlotBytes + (size_t)NO * kSOSlotBytes + (size_t)NC * kSCSlotBytes;
     const int tid = threadIdx.x + kSTX * threadIdx.y;
     const int k0 = 1 + chunk * blockIdx.z;
     const int nplanes = min(chunk, G.nz - k0 + 1);
     const int nseq = nplanes + 2;   // planes k0 - 1 .. k0 + nplanes
-    uint64_t* bars = reinterpret_cast<uint64_t*>(s_smem + (size_t)kSR * NF * kSSlotBytes);
-    const int x0 = kBase - 1 + kSTileX * blockIdx.x - 3;   // x of cell 128 bx - 3 (4 before the tile): a multiple of 4
-    const int y0 = kSTY * blockIdx.y;                       // row j_first - 1
+    uint64_t* bars = reinterpret_cast<uint64_t*>(s_smem + kSR * kStage);
+    body.xbuf = reinterpret_cast<float*>(bars + kSR);
+    const int x0 = kBase - 1 + kSTileX * blockIdx.x - 3;        // x of cell 128 bx - 3: a multiple of 4
+    const int y0 = kSTY * blockIdx.y;                            // row j_first - 1
+    const int x0c = kBase - 1 + (kSTileX / 2) * blockIdx.x - 3;  // coarse cell 64 bx - 3
+    const int y0c = (kSTY / 2) * blockIdx.y;                     // coarse row 4 by
     if (tid == 0) {
         for (int s = 0; s < kSR; ++s)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_addr(&bars[s])), "r"(1) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    auto slot = [&](int q, int f) {
-        return reinterpret_cast<const float*>(s_smem + ((size_t)(q % kSR) * NF + f) * kSSlotBytes);
+    auto off = [](int f) -> size_t {   // byte offset of field f in a stage
+        return f < NF ? (size_t)f * kSSlotBytes
+                      : (f < NF + NO ? (size_t)NF * kSSlotBytes + (size_t)(f - NF) * kSOSlotBytes
+                                     : (size_t)NF * kSSlotBytes + (size_t)NO * kSOSlotBytes + (size_t)(f - NF - NO) * kSCSlotBytes);
+    };
+    auto slot = [&](int q, int f) -> const float* {
+        return reinterpret_cast<const float*>(s_smem + (size_t)(q % kSR) * kStage + off(f));
     };
     auto issue = [&](int q) {
         const int s = q % kSR;
         const uint32_t bar = s_addr(&bars[s]);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(NF * kSBoxBytes)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"(NF * kSBoxBytes + NO * kSOBoxBytes + NC * kSCBoxBytes)
                      : "memory");
         const int z = map_any(k0 - 1 + q, G.nz, bc.perz);
+        unsigned char* b = s_smem + (size_t)s * kStage;
 #pragma unroll
-        for (int f = 0; f < NF; ++f)
-            s_tma3(s_addr(s_smem + ((size_t)s * NF + f) * kSSlotBytes), maps[f], x0, y0, z, bar);
+        for (int f = 0; f < NF; ++f) s_tma3(s_addr(b + off(f)), maps[f], x0, y0, z, bar);
+#pragma unroll
+        for (int f = NF; f < NF + NO; ++f) s_tma3(s_addr(b + off(f)), maps[f], x0 + 4, y0 + 1, z, bar);
+#pragma unroll
+        for (int f = NF + NO; f < NF + NO + NC; ++f) s_tma3(s_addr(b + off(f)), maps[f], x0c, y0c, (z + 1) >> 1, bar);
     };
     if (tid == 0)
         for (int q = 0; q < min(kSR, nseq); ++q) issue(q);
+    body.begin(k0, nplanes);
     for (int m = 0; m < nplanes; ++m) {
         bool ok = true;
         if (m == 0) ok = s_wait(s_addr(&bars[0]), 0) && s_wait(s_addr(&bars[1]), 0);
@@ -172,33 +214,49 @@ __device__ __forceinline__ bool s_march(const Geo& G, const BC& bc, const CUtens
         }
         // every thread is done with plane k0 + m - 2 (sequence m - 1): refill its slot
         if (tid == 0 && m >= 1 && m - 1 + kSR < nseq) issue(m - 1 + kSR);
-        SSlots<NF> sm, s0, sp;
+        SSlots<NF, NO, NC> sm, s0, sp;
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
+        for (int f = 0; f < NF + NO + NC; ++f) {
             sm.f[f] = slot(m, f);
             s0.f[f] = slot(m + 1, f);
             sp.f[f] = slot(m + 2, f);
         }
         body.plane(k0 + m, sm, s0, sp);
     }
+    __syncthreads();
+    body.finish();
     return true;
 }
 
-// ---- two damped Jacobi sweeps from zero (k_mgv_pre on level 0): fields f, 1/diag, density
-struct SPreBody {
+// Body members every body has: the thread's tile position and the march's scratch
+struct SBase {
     STile t;
     int nz, pxy;
-    float omega, omega2, cx2, cy2, cz2;
+    float cx2, cy2, cz2;
+    float* xbuf;
+    __device__ __forceinline__ void init(const Geo& G, const float* c2) {
+        t = s_tile(G);
+        nz = G.nz;
+        pxy = (int)G.pxy;
+        cx2 = c2[0]; cy2 = c2[1]; cz2 = c2[2];
+    }
+    __device__ __forceinline__ void begin(int, int) {}
+    __device__ __forceinline__ void finish() {}
+};
+
+// ---- two damped Jacobi sweeps from zero (k_mgv_pre on level 0): slots f, 1/diag, density
+struct SPreBody : SBase {
+    float omega, omega2;
     float* y;
-    __device__ __forceinline__ void x1(const SSlots<3>& s, int ly, int lx, float (&o)[kVX]) const {
+    __device__ __forceinline__ void x1(const SSlots<3, 0, 0>& s, int ly, int lx, float (&o)[kVX]) const {
         const V4 fv = sq(s.f[0], ly, lx), dv = sq(s.f[1], ly, lx);
 #pragma unroll
         for (int e = 0; e < kVX; ++e) o[e] = omega * fv.v[e] * dv.v[e];
     }
-    __device__ __forceinline__ float x1s(const SSlots<3>& s, int ly, int lx) const {
+    __device__ __forceinline__ float x1s(const SSlots<3, 0, 0>& s, int ly, int lx) const {
         return omega * ss(s.f[0], ly, lx) * ss(s.f[1], ly, lx);
     }
-    __device__ __forceinline__ void plane(int k, const SSlots<3>& sm, const SSlots<3>& s0, const SSlots<3>& sp) {
+    __device__ __forceinline__ void plane(int k, const SSlots<3, 0, 0>& sm, const SSlots<3, 0, 0>& s0, const SSlots<3, 0, 0>& sp) {
         if (!t.in) return;
         float zm[kVX], xc[kVX], zp[kVX], ym[kVX], yp[kVX], ax[kVX], out[kVX];
         x1(sm, t.ly, t.qx, zm);
@@ -223,34 +281,30 @@ __global__ void __launch_bounds__(kSTX * kSTY, 2) k_mgs_pre(Geo G, BC bc, const 
     pdl_wait();
     if (st->done) return;
     SPreBody b;
-    b.t = s_tile(G);
-    b.nz = G.nz;
-    b.pxy = (int)G.pxy;
+    b.init(G, c2);
     b.omega = omega;
     b.omega2 = omega2;
-    b.cx2 = c2[0]; b.cy2 = c2[1]; b.cz2 = c2[2];
     b.y = y;
     const CUtensorMap* const maps[3] = {&mf, &md, &mr};
-    s_march<3>(G, bc, maps, chunk, b, st);
+    s_march<3, 0, 0>(G, bc, maps, chunk, b, st);
 }
 
 // ---- x_out = x_in + w (f - A x_in)/dg, f.x_out -> rz, beta (k_mgv_jacc on level 0, with the
-// dot product): fields x_in, f, 1/diag, density
-struct SJaccBody {
-    STile t;
-    int nz, pxy;
-    float omega, cx2, cy2, cz2;
+// dot product): slots x_in, density with the halo; f, 1/diag at the tile's own cells
+struct SJaccBody : SBase {
+    float omega;
     float* xout;
     double dot;
-    __device__ __forceinline__ void plane(int k, const SSlots<4>& sm, const SSlots<4>& s0, const SSlots<4>& sp) {
+    __device__ __forceinline__ void plane(int k, const SSlots<2, 2, 0>& sm, const SSlots<2, 2, 0>& s0,
+                                          const SSlots<2, 2, 0>& sp) {
         if (!t.in) return;
         const V4 zm = sq(sm.f[0], t.ly, t.qx), xc = sq(s0.f[0], t.ly, t.qx), zp = sq(sp.f[0], t.ly, t.qx);
         Faces F[kVX];
-        s_faces(t, k, nz, sm.f[3], s0.f[3], sp.f[3], cx2, cy2, cz2, F);
+        s_faces(t, k, nz, sm.f[1], s0.f[1], sp.f[1], cx2, cy2, cz2, F);
         const V4 y1 = sq(s0.f[0], t.uym, t.qx), y2 = sq(s0.f[0], t.uyp, t.qx);
         float ax[kVX], out[kVX];
         apply4(F, xc.v, ss(s0.f[0], t.ly, t.uxm), ss(s0.f[0], t.ly, t.uxp), y1.v, y2.v, zm.v, zp.v, ax);
-        const V4 fc = sq(s0.f[1], t.ly, t.qx), dc = sq(s0.f[2], t.ly, t.qx);
+        const V4 fc = sqo(s0.f[2]), dc = sqo(s0.f[3]);
 #pragma unroll
         for (int e = 0; e < kVX; ++e) {
             out[e] = xc.v[e] + omega * (fc.v[e] - ax[e]) * dc.v[e];
@@ -260,23 +314,20 @@ struct SJaccBody {
     }
 };
 __global__ void __launch_bounds__(kSTX * kSTY, 2) k_mgs_jacc(Geo G, BC bc, const __grid_constant__ CUtensorMap mx,
+                                                          const __grid_constant__ CUtensorMap mr,
                                                           const __grid_constant__ CUtensorMap mf,
-                                                          const __grid_constant__ CUtensorMap md,
-                                                          const __grid_constant__ CUtensorMap mr, const float* c2,
+                                                          const __grid_constant__ CUtensorMap md, const float* c2,
                                                           float* xout, float omega, int chunk, PCGState* st,
                                                           double* partial, unsigned int* counter) {
     pdl_wait();
     if (st->done) return;
     SJaccBody b;
-    b.t = s_tile(G);
-    b.nz = G.nz;
-    b.pxy = (int)G.pxy;
+    b.init(G, c2);
     b.omega = omega;
-    b.cx2 = c2[0]; b.cy2 = c2[1]; b.cz2 = c2[2];
     b.xout = xout;
     b.dot = 0.;
-    const CUtensorMap* const maps[4] = {&mx, &mf, &md, &mr};
-    s_march<4>(G, bc, maps, chunk, b, st);   // every CTA joins the reduction, even one that gave up
+    const CUtensorMap* const maps[4] = {&mx, &mr, &mf, &md};
+    s_march<2, 2, 0>(G, bc, maps, chunk, b, st);   // every CTA joins the reduction, even one that gave up
     double t, u;
     if (reduce2_last(b.dot, 0.0, partial, counter, t, u) && flat_tid() == 0) {
         const double rz_old = st->rz;
@@ -287,22 +338,20 @@ __global__ void __launch_bounds__(kSTX * kSTY, 2) k_mgs_jacc(Geo G, BC bc, const
 }
 
 // ---- p = z + beta p_old (also at the neighbours), q = A p, p.q -> alpha (k_pcgv_spmvc on level
-// 0): fields z, p_old, density
-struct SSpmvBody {
-    STile t;
-    int nz, pxy;
-    float beta, cx2, cy2, cz2;
+// 0): slots z, p_old, density
+struct SSpmvBody : SBase {
+    float beta;
     float *p_new, *qv;
     double dot;
-    __device__ __forceinline__ void pn(const SSlots<3>& s, int ly, int lx, float (&o)[kVX]) const {
+    __device__ __forceinline__ void pn(const SSlots<3, 0, 0>& s, int ly, int lx, float (&o)[kVX]) const {
         const V4 a = sq(s.f[0], ly, lx), b = sq(s.f[1], ly, lx);
 #pragma unroll
         for (int e = 0; e < kVX; ++e) o[e] = a.v[e] + beta * b.v[e];
     }
-    __device__ __forceinline__ float pns(const SSlots<3>& s, int ly, int lx) const {
+    __device__ __forceinline__ float pns(const SSlots<3, 0, 0>& s, int ly, int lx) const {
         return ss(s.f[0], ly, lx) + beta * ss(s.f[1], ly, lx);
     }
-    __device__ __forceinline__ void plane(int k, const SSlots<3>& sm, const SSlots<3>& s0, const SSlots<3>& sp) {
+    __device__ __forceinline__ void plane(int k, const SSlots<3, 0, 0>& sm, const SSlots<3, 0, 0>& s0, const SSlots<3, 0, 0>& sp) {
         if (!t.in) return;
         float zm[kVX], xc[kVX], zp[kVX], ym[kVX], yp[kVX], ax[kVX];
         pn(sm, t.ly, t.qx, zm);
@@ -328,16 +377,13 @@ __global__ void __launch_bounds__(kSTX * kSTY, 2) k_pcgs_spmvc(Geo G, BC bc, con
     pdl_wait();
     if (st->done) return;
     SSpmvBody b;
-    b.t = s_tile(G);
-    b.nz = G.nz;
-    b.pxy = (int)G.pxy;
+    b.init(G, c2);
     b.beta = (float)st->beta;
-    b.cx2 = c2[0]; b.cy2 = c2[1]; b.cz2 = c2[2];
     b.p_new = p_new;
     b.qv = qv;
     b.dot = 0.;
     const CUtensorMap* const maps[3] = {&mz, &mp, &mr};
-    s_march<3>(G, bc, maps, chunk, b, st);   // every CTA joins the reduction, even one that gave up
+    s_march<3, 0, 0>(G, bc, maps, chunk, b, st);   // every CTA joins the reduction, even one that gave up
     double t, u;
     if (reduce2_last(b.dot, 0.0, partial, counter, t, u) && flat_tid() == 0) {
         st->pq = t;
@@ -346,6 +392,131 @@ __global__ void __launch_bounds__(kSTX * kSTY, 2) k_pcgs_spmvc(Geo G, BC bc, con
     }
 }
 
+// ---- restriction f_c = (1/8) sum over the 8 children of (f - A x) (k_mgv_restrict on level
+// 0): slots x, density with the halo; f at the tile's own cells.  A thread sums its quad's
+// residuals over the two planes of a coarse plane (cells 0, 1 -> s0; 2, 3 -> s1, children in
+// the order plane, cell); the thread of the odd row adds its row's sums to the even row's
+// through the scratch.  The chunk is even and starts on an odd plane, so coarse planes never
+// straddle two CTAs.
+struct SRestrictBody : SBase {
+    Geo Gc;
+    float* fc;
+    float s0, s1;
+    int kpair;   // first fine plane of the pending coarse plane (0: none)
+    __device__ __forceinline__ void begin(int, int) {
+        s0 = 0.f;
+        s1 = 0.f;
+        kpair = 0;
+    }
+    // the pending coarse plane: rows of odd threads in the scratch, the even threads store
+    __device__ __forceinline__ void flush() {
+        if (kpair == 0) return;
+        const int tid = threadIdx.x + kSTX * threadIdx.y;
+        if (t.in && (threadIdx.y & 1) == 0) {
+            const float a0 = s0 + xbuf[2 * (tid + kSTX)], a1 = s1 + xbuf[2 * (tid + kSTX) + 1];
+            const int I0 = (t.i0 + 1) >> 1, J = (t.j + 1) >> 1, K = (kpair + 1) >> 1;
+            fc[Gc.idx(I0, J, K)] = 0.125f * a0;
+            if (I0 + 1 <= Gc.nx) fc[Gc.idx(I0 + 1, J, K)] = 0.125f * a1;
+        }
+        kpair = 0;
+    }
+    __device__ __forceinline__ void plane(int k, const SSlots<2, 1, 0>& sm, const SSlots<2, 1, 0>& s0s,
+                                          const SSlots<2, 1, 0>& sp) {
+        if ((k & 1) == 1) {   // first plane of a coarse plane: store the previous one (after the barrier)
+            flush();
+            s0 = 0.f;
+            s1 = 0.f;
+        }
+        if (!t.in) return;
+        const V4 zm = sq(sm.f[0], t.ly, t.qx), xc = sq(s0s.f[0], t.ly, t.qx), zp = sq(sp.f[0], t.ly, t.qx);
+        Faces F[kVX];
+        s_faces(t, k, nz, sm.f[1], s0s.f[1], sp.f[1], cx2, cy2, cz2, F);
+        const V4 y1 = sq(s0s.f[0], t.uym, t.qx), y2 = sq(s0s.f[0], t.uyp, t.qx);
+        float ax[kVX];
+        apply4(F, xc.v, ss(s0s.f[0], t.ly, t.uxm), ss(s0s.f[0], t.ly, t.uxp), y1.v, y2.v, zm.v, zp.v, ax);
+        const V4 fv = sqo(s0s.f[2]);
+        s0 += fv.v[0] - ax[0];
+        s0 += fv.v[1] - ax[1];
+        s1 += fv.v[2] - ax[2];
+        s1 += fv.v[3] - ax[3];
+        if ((k & 1) == 0) {   // second plane: the odd row publishes its sums
+            kpair = k - 1;
+            if (threadIdx.y & 1) {
+                const int tid = threadIdx.x + kSTX * threadIdx.y;
+                xbuf[2 * tid] = s0;
+                xbuf[2 * tid + 1] = s1;
+            }
+        }
+    }
+    __device__ __forceinline__ void finish() { flush(); }
+};
+__global__ void __launch_bounds__(kSTX * kSTY, 2) k_mgs_restrict(Geo G, Geo Gc, BC bc,
+                                                              const __grid_constant__ CUtensorMap mx,
+                                                              const __grid_constant__ CUtensorMap mr,
+                                                              const __grid_constant__ CUtensorMap mf, const float* c2,
+                                                              float* fc, int chunk, PCGState* st) {
+    pdl_wait();
+    if (st->done) return;
+    SRestrictBody b;
+    b.init(G, c2);
+    b.Gc = Gc;
+    b.fc = fc;
+    const CUtensorMap* const maps[3] = {&mx, &mr, &mf};
+    s_march<2, 1, 0>(G, bc, maps, chunk, b, st);
+}
+
+// ---- x_out = x' + w (f - A x')/dg with x' = y + a P xc (k_mgv_post on level 0): slots y,
+// density with the halo, f and 1/diag at the tile's own cells, the coarse correction xc (parent
+// planes).  A fine cell at tile column lx, row ly has its parent at coarse tile
+// column lx/2 + 2, row (ly + 1)/2.
+struct SPostBody : SBase {
+    float omega, alpha;
+    float* xout;
+    // x' of the quad at tile row ly from the y slot and the coarse slot of its plane
+    __device__ __forceinline__ void xq(const float* ys, const float* cs, int ly, float (&o)[kVX]) const {
+        const V4 yv = sq(ys, ly, t.qx);
+        const int cx = (t.qx >> 1) + 2, cy = (ly + 1) >> 1;
+        const float p0 = alpha * ssc(cs, cy, cx), p1 = alpha * ssc(cs, cy, cx + 1);
+        o[0] = yv.v[0] + p0; o[1] = yv.v[1] + p0; o[2] = yv.v[2] + p1; o[3] = yv.v[3] + p1;
+    }
+    __device__ __forceinline__ float xs(const float* ys, const float* cs, int ly, int lx) const {
+        return ss(ys, ly, lx) + alpha * ssc(cs, (ly + 1) >> 1, (lx >> 1) + 2);
+    }
+    __device__ __forceinline__ void plane(int k, const SSlots<2, 2, 1>& sm, const SSlots<2, 2, 1>& s0,
+                                          const SSlots<2, 2, 1>& sp) {
+        if (!t.in) return;
+        float zm[kVX], xc[kVX], zp[kVX], ym[kVX], yp[kVX], ax[kVX], out[kVX];
+        xq(sm.f[0], sm.f[4], t.ly, zm);
+        xq(s0.f[0], s0.f[4], t.ly, xc);
+        xq(sp.f[0], sp.f[4], t.ly, zp);
+        Faces F[kVX];
+        s_faces(t, k, nz, sm.f[1], s0.f[1], sp.f[1], cx2, cy2, cz2, F);
+        xq(s0.f[0], s0.f[4], t.uym, ym);
+        xq(s0.f[0], s0.f[4], t.uyp, yp);
+        apply4(F, xc, xs(s0.f[0], s0.f[4], t.ly, t.uxm), xs(s0.f[0], s0.f[4], t.ly, t.uxp), ym, yp, zm, zp, ax);
+        const V4 fc = sqo(s0.f[2]), dc = sqo(s0.f[3]);
+#pragma unroll
+        for (int e = 0; e < kVX; ++e) out[e] = xc[e] + omega * (fc.v[e] - ax[e]) * dc.v[e];
+        st4(xout, t.c0 + pxy * k, out);
+    }
+};
+__global__ void __launch_bounds__(kSTX * kSTY, 2) k_mgs_post(Geo G, BC bc, const __grid_constant__ CUtensorMap my,
+                                                          const __grid_constant__ CUtensorMap mr,
+                                                          const __grid_constant__ CUtensorMap mf,
+                                                          const __grid_constant__ CUtensorMap md,
+                                                          const __grid_constant__ CUtensorMap mc, const float* c2,
+                                                          float* xout, float omega, float alpha, int chunk,
+                                                          PCGState* st) {
+    pdl_wait();
+    if (st->done) return;
+    SPostBody b;
+    b.init(G, c2);
+    b.omega = omega;
+    b.alpha = alpha;
+    b.xout = xout;
+    const CUtensorMap* const maps[5] = {&my, &mr, &mf, &md, &mc};
+    s_march<2, 2, 1>(G, bc, maps, chunk, b, st);
+}
 static inline dim3 sgrid(const Geo& g, int chunk) {
     return dim3((g.nx + kSTileX - 1) / kSTileX, (g.ny + kSTY - 1) / kSTY, (g.nz + chunk - 1) / chunk);
 }

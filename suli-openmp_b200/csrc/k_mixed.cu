@@ -689,26 +689,49 @@ static PFN_cuTensorMapEncodeTiled_v12000 plane_map_encoder() {
     return fn;
 }
 // a level-0 FP32 array as a 3-D tensor {px, py, nz + 3} (x = kBase + i - 1 within row j of
-// plane k), box {kSBoxX, kSBoxY, 1}, zero fill outside
-static bool add_plane_map(suli_ctx* c, const float* a) {
+// plane k), zero fill outside; box {kSBoxX, kSBoxY, 1} (with the halo) or, own = true,
+// {kSOBoxX, kSOBoxY, 1} (the tile's own cells)
+static bool encode_plane_map(CUtensorMap* m, const Geo& g, const float* a, bool own) {
     auto enc = plane_map_encoder();
-    const Geo& g = c->mg[0].g;
-    if (!enc || !a || (reinterpret_cast<uintptr_t>(a) & 15) || c->n_smap >= 12) return false;
+    if (!enc || !a || (reinterpret_cast<uintptr_t>(a) & 15)) return false;
     cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)(g.nz + 3)};
     cuuint64_t strides[2] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.pxy * 4};
-    cuuint32_t box[3] = {(cuuint32_t)kSBoxX, (cuuint32_t)kSBoxY, 1};
+    cuuint32_t box[3] = {(cuuint32_t)(own ? kSOBoxX : kSBoxX), (cuuint32_t)(own ? kSOBoxY : kSBoxY), 1};
     cuuint32_t es[3] = {1, 1, 1};
-    if (enc(&c->smap[c->n_smap], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(a), dims, strides, box, es,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(a), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+static bool add_plane_map(suli_ctx* c, const float* a) {
+    if (c->n_smap >= 12) return false;
+    const Geo& g = c->mg[0].g;
+    if (!encode_plane_map(&c->smap[c->n_smap], g, a, false) || !encode_plane_map(&c->smap_own[c->n_smap], g, a, true))
         return false;
     c->smap_ptr[c->n_smap++] = a;
     return true;
+}
+// the coarse level-1 correction as the post-smoothing's prolongation source: box {kSCBoxX, kSCBoxY, 1}
+static bool set_coarse_map(suli_ctx* c, const float* a) {
+    auto enc = plane_map_encoder();
+    const Geo& g = c->mg[1].g;
+    if (!enc || !a || (reinterpret_cast<uintptr_t>(a) & 15)) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)(g.nz + 3)};
+    cuuint64_t strides[2] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.pxy * 4};
+    cuuint32_t box[3] = {(cuuint32_t)kSCBoxX, (cuuint32_t)kSCBoxY, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    return enc(&c->smap_c, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(a), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 static const CUtensorMap& plane_map(const suli_ctx* c, const float* a) {
     for (int q = 0; q < c->n_smap; ++q)
         if (c->smap_ptr[q] == a) return c->smap[q];
     return c->smap[0];   // not reached: every array the streaming kernels read has a map
+}
+static const CUtensorMap& own_map(const suli_ctx* c, const float* a) {
+    for (int q = 0; q < c->n_smap; ++q)
+        if (c->smap_ptr[q] == a) return c->smap_own[q];
+    return c->smap_own[0];
 }
 
 // Decide once per context whether level 0 runs the streaming kernels: vectorised kernels on a
@@ -717,6 +740,7 @@ static const CUtensorMap& plane_map(const suli_ctx* c, const float* a) {
 // keeps the vectorised level-0 kernels; SULI_STREAM_CHUNK sets the planes a CTA computes.
 int stream_ready(suli_ctx* c) {
     c->stream_ok = false;
+    c->stream_post_ok = false;
     c->n_smap = 0;
     if (const char* ev = std::getenv("SULI_NO_STREAM"))
         if (std::strcmp(ev, "1") == 0) return SULI_OK;
@@ -727,19 +751,27 @@ int stream_ready(suli_ctx* c) {
     const float* arrays[] = {c->pc_r, c->pc_r2, M0.x, M0.y, c->pc_pa, c->pc_pb, M0.idg, M0.rho};
     for (const float* a : arrays)
         if (!add_plane_map(c, a)) { c->n_smap = 0; return SULI_OK; }
-    const int s3 = (int)stream_smem_bytes(3), s4 = (int)stream_smem_bytes(4);
-    if (cudaFuncSetAttribute(k_mgs_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, s3) != cudaSuccess ||
-        cudaFuncSetAttribute(k_pcgs_spmvc, cudaFuncAttributeMaxDynamicSharedMemorySize, s3) != cudaSuccess ||
-        cudaFuncSetAttribute(k_mgs_jacc, cudaFuncAttributeMaxDynamicSharedMemorySize, s4) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k_mgs_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stream_smem_bytes(3)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_pcgs_spmvc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stream_smem_bytes(3)) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_mgs_jacc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stream_smem_bytes(2, 2)) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_mgs_restrict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stream_smem_bytes(2, 1)) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_mgs_post, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stream_smem_bytes(2, 2, 1)) !=
+            cudaSuccess) {
         cudaGetLastError();
         return SULI_OK;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mgs_jacc, kSTX * kSTY, s4) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mgs_post, kSTX * kSTY, stream_smem_bytes(2, 2, 1)) !=
+            cudaSuccess ||
         per_sm < 1) {
         cudaGetLastError();
         return SULI_OK;
     }
+    // the post-smoothing also needs the level-1 correction's rows to hold its tile's parents
+    c->stream_post_ok = (g.nx % 32 == 0) && c->mg[1].g.px >= c->mg[1].g.nx + 16 && set_coarse_map(c, c->mg[1].y);
     // planes a CTA computes: as many chunks as fill the SMs' CTA slots once
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
@@ -775,9 +807,33 @@ static void launch_stream_pre(suli_ctx* c, const float* f, float om, float om2) 
 }
 static void launch_stream_jacc(suli_ctx* c, const float* f, float om) {
     const MGLevel& M = c->mg[0];
-    stream_launch(c, k_mgs_jacc, stream_smem_bytes(4), M.g, c->bc, plane_map(c, M.x), plane_map(c, f),
-                  plane_map(c, M.idg), plane_map(c, M.rho), (const float*)M.c2, M.y, om, c->stream_chunk, c->pcg,
+    stream_launch(c, k_mgs_jacc, stream_smem_bytes(2, 2), M.g, c->bc, plane_map(c, M.x), plane_map(c, M.rho),
+                  own_map(c, f), own_map(c, M.idg), (const float*)M.c2, M.y, om, c->stream_chunk, c->pcg,
                   c->red_partial, c->red_counter);
+}
+// the restriction's chunk is even (a coarse plane's two fine planes in one CTA)
+static void launch_stream_restrict(suli_ctx* c, const float* f) {
+    const MGLevel& M = c->mg[0];
+    const MGLevel& C = c->mg[1];
+    const int ch = (c->stream_chunk + 1) & ~1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = sgrid(M.g, ch);
+    cfg.blockDim = dim3(kSTX, kSTY, 1);
+    cfg.dynamicSmemBytes = stream_smem_bytes(2, 1);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_mgs_restrict, M.g, C.g, c->bc, plane_map(c, M.y), plane_map(c, M.rho), own_map(c, f),
+                       (const float*)M.c2, C.f, ch, c->pcg);
+}
+static void launch_stream_post(suli_ctx* c, const float* f, float om2, float alpha) {
+    const MGLevel& M = c->mg[0];
+    stream_launch(c, k_mgs_post, stream_smem_bytes(2, 2, 1), M.g, c->bc, plane_map(c, M.y), plane_map(c, M.rho),
+                  own_map(c, f), own_map(c, M.idg), c->smap_c, (const float*)M.c2, M.x, om2, alpha, c->stream_chunk,
+                  c->pcg);
 }
 static void launch_stream_spmvc(suli_ctx* c, const float* p_old, float* p_new) {
     const MGLevel& M = c->mg[0];
@@ -798,8 +854,11 @@ static void vc_down(suli_ctx* c, int l, const float* f, float om, float om2, boo
                 if (c->stream_ok) launch_stream_pre(c, f, om, om2);
                 else VLAUNCH(k_mgv_pre, OpRho4, M.g, M.g, bc, f, from_rho4(M), M.y, om, om2, c->pcg);
             }
-            pdl_launch(k_mgv_restrict<OpRho4>, vgrid_restrict(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, from_rho4(M),
-                       C.f, c->pcg);
+            if (c->stream_ok)
+                launch_stream_restrict(c, f);
+            else
+                pdl_launch(k_mgv_restrict<OpRho4>, vgrid_restrict(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f,
+                           from_rho4(M), C.f, c->pcg);
         } else {
             VLAUNCH(k_mgv_pre, OpStored4, M.g, M.g, bc, f, stored4(M), M.y, om, om2, c->pcg);
             pdl_launch(k_mgv_restrict<OpStored4>, vgrid_restrict(C.g), kB2, c->stream, M.g, C.g, bc, M.y, f, stored4(M),
@@ -825,7 +884,10 @@ static void vc_up(suli_ctx* c, int l, const float* f, float om, float om2, float
     const int dot = (l == 0) ? 1 : 0;
     if (vec_level(c, M.g)) {
         if (l == 0) {
-            VLAUNCH(k_mgv_post, OpRho4, M.g, M.g, C.g, bc, M.y, C.y, f, from_rho4(M), M.x, om2, alpha, c->pcg);
+            if (c->stream_ok && c->stream_post_ok)
+                launch_stream_post(c, f, om2, alpha);
+            else
+                VLAUNCH(k_mgv_post, OpRho4, M.g, M.g, C.g, bc, M.y, C.y, f, from_rho4(M), M.x, om2, alpha, c->pcg);
             if (c->stream_ok) launch_stream_jacc(c, f, om);
             else VLAUNCH(k_mgv_jacc, OpRho4, M.g, M.g, bc, M.x, f, from_rho4(M), M.y, om, c->pcg, dot, c->red_partial,
                          c->red_counter);
