@@ -138,6 +138,7 @@ struct suli_ctx {
     int coarse_sweeps = 40;
     bool cluster_ok = false;    // the device runs k_mg_cluster (16-CTA cluster with its shared memory)
     bool fuse_update = false;   // the inner PCG update runs inside the level-0 pre-smoothing kernel
+    bool tail_ok = false;       // the device runs k_mg_tail (one CTA, the last two levels)
     int mg_kz = 2;              // cells along z a thread of the vectorised multigrid kernels owns (2 or 4)
     // level-0 kernels that stream z-planes through shared memory with TMA (k_mg_stream.cuh):
     // one tensor map per level-0 array they read, the planes a CTA computes, and whether they run
@@ -252,6 +253,7 @@ void launch_cg_cond(suli_ctx* c, cudaGraphConditionalHandle h);
 void launch_cg_divcheck(suli_ctx* c);
 int cluster_ready(suli_ctx* c);
 int stream_ready(suli_ctx* c);
+int tail_ready(suli_ctx* c);
 void launch_cg_final(suli_ctx* c, const double* e);
 // ---- mixed-precision solve (k_mixed.cu) ----
 void launch_mx_setup(suli_ctx* c);

@@ -608,6 +608,7 @@ __global__ void k_zero_f(float* a, long long n) {
 #include "k_mg_vec.cuh"
 #include "k_mg_cluster.cuh"
 #include "k_mg_stream.cuh"
+#include "k_mg_tail.cuh"
 namespace suli {
 
 // ------------------------------------------------------------------------------------
@@ -927,6 +928,10 @@ int cluster_ready(suli_ctx* c) {
     c->mg_kz = 2;
     if (const char* ev = std::getenv("SULI_MG_KZ"))   // column depth of the vectorised kernels
         if (std::strcmp(ev, "4") == 0) c->mg_kz = 4;
+    if (const char* ev = std::getenv("SULI_COARSE_SWEEPS")) {   // Jacobi sweeps of the coarsest solve
+        const int v = std::atoi(ev);
+        if (v >= 2 && v <= 400) c->coarse_sweeps = v;
+    }
     c->fuse_update = false;
     if (const char* ev = std::getenv("SULI_FUSED_UPDATE"))   // the PCG update inside the pre-smoothing
         if (std::strcmp(ev, "1") == 0) c->fuse_update = true;
@@ -991,6 +996,57 @@ static void launch_cluster(suli_ctx* c, float om, float alpha) {
     cudaLaunchKernelEx(&cfg, k_mg_cluster, a, (const PCGState*)c->pcg);
 }
 
+// The last level above the coarsest and the coarsest solve as one CTA (k_mg_tail), selected by
+// SULI_TAIL=1, when the vectorised per-level kernels are selected (mg_kernels 0), there are at
+// least three levels, the two fit it, and the device grants its shared memory (checked once,
+// tail_ready).  Measured at 256x128x128 it is slower than the five launches it replaces (192
+// against 168 us an inner iteration: one SM works through 8192 cells a phase), so it is not
+// the default.
+static bool use_tail(const suli_ctx* c) {
+    const int L = (int)c->mg.size();
+    if (!c->tail_ok || c->P.mg_kernels != 0 || L < 3) return false;
+    const Geo &M = c->mg[L - 2].g, &B = c->mg[L - 1].g;
+    return (long long)M.nx * M.ny * M.nz <= kTailM && (long long)B.nx * B.ny * B.nz <= 1024;
+}
+int tail_ready(suli_ctx* c) {
+    c->tail_ok = false;
+    const char* ev = std::getenv("SULI_TAIL");
+    if (!ev || std::strcmp(ev, "1") != 0) return SULI_OK;
+    if (cudaFuncSetAttribute(k_mg_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tail_smem_bytes()) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return SULI_OK;
+    }
+    c->tail_ok = true;
+    return SULI_OK;
+}
+static void launch_tail(suli_ctx* c, float om, float om2, float alpha) {
+    const int L = (int)c->mg.size();
+    const MGLevel &M = c->mg[L - 2], &B = c->mg[L - 1];
+    TailArgs a;
+    a.gm = M.g;
+    a.gb = B.g;
+    a.am = stored(M);
+    a.ab = stored(B);
+    a.fm = M.f;
+    a.ym = M.y;
+    a.omega = om;
+    a.omega2 = om2;
+    a.alpha = alpha;
+    a.sweeps = c->coarse_sweeps;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(kTailThreads);
+    cfg.dynamicSmemBytes = tail_smem_bytes();
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_mg_tail, a, c->bc, (const PCGState*)c->pcg);
+}
+
 // z = M r for the level-0 right-hand side f0: one V-cycle; the last level-0 sweep also forms r.z
 // and beta.  pre_done: the level-0 pre-smoothing already ran (fused with the PCG update).
 void launch_vcycle(suli_ctx* c, const float* f0, bool pre_done) {
@@ -1003,6 +1059,12 @@ void launch_vcycle(suli_ctx* c, const float* f0, bool pre_done) {
         for (int l = 0; l < L - 3; ++l) vc_down(c, l, l == 0 ? f0 : c->mg[l].f, om, om2, pre_done);
         launch_cluster(c, om, alpha);
         for (int l = L - 4; l >= 0; --l) vc_up(c, l, l == 0 ? f0 : c->mg[l].f, om, om2, alpha);
+        return;
+    }
+    if (use_tail(c)) {   // levels 0 .. L-3 as kernels per level, the last two in one CTA
+        for (int l = 0; l < L - 2; ++l) vc_down(c, l, l == 0 ? f0 : c->mg[l].f, om, om2, pre_done);
+        launch_tail(c, om, om2, alpha);
+        for (int l = L - 3; l >= 0; --l) vc_up(c, l, l == 0 ? f0 : c->mg[l].f, om, om2, alpha);
         return;
     }
     for (int l = 0; l < L - 1; ++l) vc_down(c, l, l == 0 ? f0 : c->mg[l].f, om, om2, pre_done);
@@ -1072,6 +1134,7 @@ int pcg_iter_kernels(const suli_ctx* c) { return fused_update(c) ? 1 + vcycle_ke
 int vcycle_kernels(const suli_ctx* c) {
     const int L = (int)c->mg.size();
     if (use_cluster(c)) return 4 * (L - 3) + 1;
+    if (use_tail(c)) return 4 * (L - 2) + 1;
     return (L == 1) ? 2 : 4 * (L - 1) + 1;
 }
 

@@ -285,6 +285,7 @@ int suli_create(const suli_params* p, int device, suli_ctx** out) {
         if ((e = cudaMallocHost(&c->pcg_host, 2 * sizeof(PCGState))) != cudaSuccess) return bail(e, "pinned");
         cluster_ready(c);
         stream_ready(c);
+        tail_ready(c);
     }
     if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bail(e, "sync");
     c->dt = p->dt;

@@ -164,6 +164,38 @@ def test_streaming_kernels_match_vectorised(pkg, monkeypatch, shape, chunk):
         assert float(np.abs(v1[f] - v0[f]).max()) <= 1e-9 * vs, f
 
 
+@pytest.mark.parametrize("case", ["dam_break", "periodic"])
+def test_tail_kernel_matches_per_level_kernels(pkg, monkeypatch, case):
+    """The last level above the coarsest and the coarsest solve in one CTA (k_mg_tail,
+    SULI_TAIL=1) against their per-level kernels (default): the same per-cell
+    arithmetic.  Walls (dam break 128x64x64: 32x16x16 and 16x8x8 in the CTA) and a box periodic
+    in every direction (64^3: 16^3 and 8^3, wrapped neighbours); two steps: iteration counts
+    within 2, velocities within 1e-9 of their scale."""
+    res = {}
+    for nt in ("0", "1"):
+        monkeypatch.setenv("SULI_TAIL", nt)
+        if case == "dam_break":
+            p, init = pkg.cases.dam_break(nx=128, ny=64, nz=64, dx=0.005, cg_tol=1e-10)
+            p.precision, p.inner_tol, p.refine_maxit = 1, 1e-4, 30
+            s = pkg.Solver(p)
+            init(s)
+            steps = [s.step(it) for it in (1, 2)]
+        else:
+            m = pkg.cases.TaylorGreenMMS(64, precision=1)
+            s = pkg.Solver(m.p)
+            m.init(s)
+            steps = [m.step(s, it) for it in (1, 2)]
+        assert all(st["status"] == 0 for st in steps)
+        iters = [sum(st["cg_iters"]) if isinstance(st["cg_iters"], list) else st["cg_iters"] for st in steps]
+        res[nt] = (iters, {f: s.download(f) for f in ("u", "v", "w")})
+        s.close()
+    (i1, v1), (i0, v0) = res["1"], res["0"]
+    assert all(abs(a - b) <= 2 for a, b in zip(i1, i0)), (i1, i0)
+    vs = max(float(np.abs(b).max()) for b in v1.values())
+    for f in v1:
+        assert float(np.abs(v1[f] - v0[f]).max()) <= 1e-9 * vs, f
+
+
 def test_fused_update_matches_separate_update(pkg, monkeypatch):
     """The inner PCG update inside the level-0 pre-smoothing kernel (SULI_FUSED_UPDATE=1)
     against the separate update kernel (default): the same residual values, r.r summed in
