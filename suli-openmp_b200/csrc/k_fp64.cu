@@ -53,21 +53,30 @@ struct Weno3 {
     R dpx, dnx, dpy, dny, dpz, dnz;
 };
 // der_weno at one cell (14_level_set.f90:343-384) of a cell field f, in compute type R.
+// rx, ry, rz: 1/dx, 1/dy, 1/dz in R
 template <typename R>
 __device__ __forceinline__ Weno3<R> der_weno_at(const Geo& G, const double* __restrict__ f, int i, int j, int k,
-                                                int ihx, int ihy, int ihz, double dx, double dy, double dz) {
+                                                int ihx, int ihy, int ihz, R rx, R ry, R rz) {
     Weno3<R> W;
     R P[7];
     pencil7<R>([&](int q) { return R(FIDX(f, q, j, k)); }, i, G.nx, ihx, P);
-    weno_pair<R>(P, R(dx), W.dpx, W.dnx);
+    weno_pair<R>(P, rx, W.dpx, W.dnx);
     pencil7<R>([&](int q) { return R(FIDX(f, i, q, k)); }, j, G.ny, ihy, P);
-    weno_pair<R>(P, R(dy), W.dpy, W.dny);
+    weno_pair<R>(P, ry, W.dpy, W.dny);
     pencil7<R>([&](int q) { return R(FIDX(f, i, j, q)); }, k, G.nz, ihz, P);
-    weno_pair<R>(P, R(dz), W.dpz, W.dnz);
+    weno_pair<R>(P, rz, W.dpz, W.dnz);
     return W;
 }
 template <typename R>
 __device__ __forceinline__ R larger(R a, R b) { return (fabs(a) > fabs(b)) ? a : b; }
+// a / b in the compute type: IEEE in FP64; in the mixed path's FP32 arithmetic the hardware
+// reciprocal (__fdividef, 2 ulp), since an IEEE FP32 division costs as much as the rest of a
+// stencil term (every divisor here is a density, a norm or a sum of squares, far below 2^126)
+template <typename R>
+__device__ __forceinline__ R rdiv(R a, R b) {
+    if constexpr (sizeof(R) == 8) return a / b;
+    else return __fdividef(a, b);
+}
 
 struct LsConst {
     int ihx, ihy, ihz, ihn;
@@ -77,6 +86,13 @@ struct LsConst {
     double rho1, rho2, mi1, mi2;
     int t_hs;           // 0 linear mix of rho and mu in H, 1 geometric (14_level_set.f90:696-703)
     double mu1s, mu2s;  // mi_f1 * 10000, mi_f2 * 10000
+    double rx, ry, rz;  // 1/dx, 1/dy, 1/dz (the WENO divided differences)
+    float frx, fry, frz;   // the same reciprocals formed in FP32 (1.f / float(dx)), for R = float
+    template <typename R>
+    __device__ __forceinline__ R rcp(int d) const {
+        if constexpr (sizeof(R) == 8) return R(d == 0 ? rx : (d == 1 ? ry : rz));
+        else return R(d == 0 ? frx : (d == 1 ? fry : frz));
+    }
 };
 
 // ------------------------------------------------------------------------------------
@@ -93,13 +109,13 @@ __global__ void __launch_bounds__(256) k_lsprops(Geo G, LsConst L, const double*
     double vol = 0.0;
     if (in) {
         const long long c = G.idx(t.i, t.j, t.k);
-        const Weno3<R> W = der_weno_at<R>(G, ls, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
+        const Weno3<R> W = der_weno_at<R>(G, ls, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.rcp<R>(0), L.rcp<R>(1), L.rcp<R>(2));
         const R ar = larger(W.dpx, W.dnx), br = larger(W.dpy, W.dny), cr = larger(W.dpz, W.dnz);
         if (do_mod) {
             const R m = sqrt(ar * ar + br * br + cr * cr);
             mod_ls[c] = (double)m;
             if (m == R(0)) { nrmx[c] = 0.; nrmy[c] = 0.; nrmz[c] = 0.; }
-            else { const R im = R(1) / m; nrmx[c] = (double)(ar * im); nrmy[c] = (double)(br * im); nrmz[c] = (double)(cr * im); }
+            else { const R im = rdiv<R>(R(1), m); nrmx[c] = (double)(ar * im); nrmy[c] = (double)(br * im); nrmz[c] = (double)(cr * im); }
         }
         const double a = (double)ar, b = (double)br, cc = (double)cr;   // the Heaviside stays FP64
         if (do_hs) {
@@ -142,13 +158,13 @@ __global__ void __launch_bounds__(256) k_curv(Geo G, LsConst L, const double* __
     if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
     R P[7], dp, dn;
     pencil7<R>([&](int q) { return R(FIDX(nx_, q, t.j, t.k)); }, t.i, G.nx, L.ihn, P);
-    weno_pair<R>(P, R(L.dx), dp, dn);
+    weno_pair<R>(P, L.rcp<R>(0), dp, dn);
     const R ax = (fabs(dn) > fabs(dp)) ? dn : dp;
     pencil7<R>([&](int q) { return R(FIDX(ny_, t.i, q, t.k)); }, t.j, G.ny, L.ihn, P);
-    weno_pair<R>(P, R(L.dy), dp, dn);
+    weno_pair<R>(P, L.rcp<R>(1), dp, dn);
     const R ay = (fabs(dn) > fabs(dp)) ? dn : dp;
     pencil7<R>([&](int q) { return R(FIDX(nz_, t.i, t.j, q)); }, t.k, G.nz, L.ihn, P);
-    weno_pair<R>(P, R(L.dz), dp, dn);
+    weno_pair<R>(P, L.rcp<R>(2), dp, dn);
     const R az = (fabs(dn) > fabs(dp)) ? dn : dp;
     const long long c = G.idx(t.i, t.j, t.k);
     ddx[c] = (double)ax; ddy[c] = (double)ay; ddz[c] = (double)az;
@@ -164,7 +180,7 @@ __global__ void __launch_bounds__(256) k_ls_advect(Geo G, LsConst L, const doubl
     const Thread3 t = tid3(1, 1, 1);
     if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
     const int i = t.i, j = t.j, k = t.k;
-    const Weno3<R> W = der_weno_at<R>(G, cur, i, j, k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
+    const Weno3<R> W = der_weno_at<R>(G, cur, i, j, k, L.ihx, L.ihy, L.ihz, L.rcp<R>(0), L.rcp<R>(1), L.rcp<R>(2));
     const R ua = (RLD(u, i, j, k) + RLD(u, i + 1, j, k)) * R(0.5);
     const R va = (RLD(v, i, j, k) + RLD(v, i, j + 1, k)) * R(0.5);
     const R wa = (RLD(w, i, j, k) + RLD(w, i, j, k + 1)) * R(0.5);
@@ -200,12 +216,12 @@ __global__ void __launch_bounds__(256) k_reinit_funcs(Geo G, LsConst L, const do
                                                       double* funcs) {
     const Thread3 t = tid3(1, 1, 1);
     if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
-    const Weno3<R> W = der_weno_at<R>(G, ls, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
+    const Weno3<R> W = der_weno_at<R>(G, ls, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.rcp<R>(0), L.rcp<R>(1), L.rcp<R>(2));
     const long long c = G.idx(t.i, t.j, t.k);
     const R l = R(ls[c]);
     const R m = reinit_mod(l, W);
     const R dx1 = R(L.dx1);
-    funcs[c] = (double)(l / sqrt(l * l + m * m * dx1 * dx1));
+    funcs[c] = (double)rdiv<R>(l, sqrt(l * l + m * m * dx1 * dx1));
 }
 
 template <typename R>
@@ -215,7 +231,7 @@ __global__ void __launch_bounds__(256) k_reinit_stage(Geo G, LsConst L, const do
                                                       double gd) {
     const Thread3 t = tid3(1, 1, 1);
     if (t.i > G.nx || t.j > G.ny || t.k > G.nz) return;
-    const Weno3<R> W = der_weno_at<R>(G, cur, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.dx, L.dy, L.dz);
+    const Weno3<R> W = der_weno_at<R>(G, cur, t.i, t.j, t.k, L.ihx, L.ihy, L.ihz, L.rcp<R>(0), L.rcp<R>(1), L.rcp<R>(2));
     const long long c = G.idx(t.i, t.j, t.k);
     const double l = cur[c];
     const R m = reinit_mod(R(l), W);
@@ -480,8 +496,8 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
             uint_ = classico_hi<R, DER>(u, c0, s, m, n, vel, ih);
         }
         const R rhox = (AT(F.rho, (ic) - i, 0, 0) + AT(F.rho, (ic - 1) - i, 0, 0)) * R(0.5);
-        const R tx1 = AT(F.hsx, (ic) - i, 0, 0) * AT(F.kurv, (ic) - i, 0, 0) / AT(F.rho, (ic) - i, 0, 0);
-        const R tx0 = AT(F.hsx, (ic - 1) - i, 0, 0) * AT(F.kurv, (ic - 1) - i, 0, 0) / AT(F.rho, (ic - 1) - i, 0, 0);
+        const R tx1 = rdiv<R>(AT(F.hsx, (ic) - i, 0, 0) * AT(F.kurv, (ic) - i, 0, 0), AT(F.rho, (ic) - i, 0, 0));
+        const R tx0 = rdiv<R>(AT(F.hsx, (ic - 1) - i, 0, 0) * AT(F.kurv, (ic - 1) - i, 0, 0), AT(F.rho, (ic - 1) - i, 0, 0));
         const R dhsdx = (tx1 + tx0) * R(0.5);
         const R ama_i = AT(F.nut, (clampi(i, 1, nx)) - i, 0, 0) * idx;
         const R ama_m = AT(F.nut, (clampi(i - 1, 1, nx)) - i, 0, 0) * idx;
@@ -496,7 +512,7 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
                           bma_m * ((uc - AT(u, 0, -1, 0)) * idy + (AT(v, 0, 0, 0) - AT(v, -1, 0, 0)) * idx) +
                           dma_p * ((AT(u, 0, 0, 1) - uc) * idz + (AT(w, 0, 0, 1) - AT(w, -1, 0, 1)) * idx) -
                           dma_m * ((uc - AT(u, 0, 0, -1)) * idz + (AT(w, 0, 0, 0) - AT(w, -1, 0, 0)) * idx);
-        R r = -uint_ + Gv / rhox + R(C.gx) - R(C.sigma) * dhsdx;
+        R r = -uint_ + rdiv<R>(Gv, rhox) + R(C.gx) - R(C.sigma) * dhsdx;
         if (C.tf) r = r + AT(F.tfu, 0, 0, 0);
         if (on_cap(C, j, k, ny)) { const R b = AT(F.ub, 0, 0, 0); r = r - R(C.cz) * sqrt(b * b) * uc; }
         F.Fu[c0] = (double)r;
@@ -527,8 +543,8 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
             vint = classico_hi<R, DER>(v, c0, s, m, n, vel, ih);
         }
         const R rhoy = (AT(F.rho, 0, (jc) - j, 0) + AT(F.rho, 0, (jc - 1) - j, 0)) * R(0.5);
-        const R ty1 = AT(F.hsy, 0, (jc) - j, 0) * AT(F.kurv, 0, (jc) - j, 0) / AT(F.rho, 0, (jc) - j, 0);
-        const R ty0 = AT(F.hsy, 0, (jc - 1) - j, 0) * AT(F.kurv, 0, (jc - 1) - j, 0) / AT(F.rho, 0, (jc - 1) - j, 0);
+        const R ty1 = rdiv<R>(AT(F.hsy, 0, (jc) - j, 0) * AT(F.kurv, 0, (jc) - j, 0), AT(F.rho, 0, (jc) - j, 0));
+        const R ty0 = rdiv<R>(AT(F.hsy, 0, (jc - 1) - j, 0) * AT(F.kurv, 0, (jc - 1) - j, 0), AT(F.rho, 0, (jc - 1) - j, 0));
         const R dhsdy = (ty1 + ty0) * R(0.5);
         const int ip = clampi(i + 1, 2, nx), im = clampi(i, 2, nx);
         const R amb_p = ((AT(F.ynut, (ip) - i, 0, 0) + AT(F.ynut, (ip - 1) - i, 0, 0)) * R(0.5)) * idx;
@@ -543,7 +559,7 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
                           (bmb_j * R(2.) * (AT(v, 0, 1, 0) - vc) - bmb_m * R(2.) * (vc - AT(v, 0, -1, 0))) * idy +
                           dmb_p * ((AT(v, 0, 0, 1) - vc) * idz + (AT(w, 0, 0, 1) - AT(w, 0, -1, 1)) * idy) -
                           dmb_m * ((vc - AT(v, 0, 0, -1)) * idz + (AT(w, 0, 0, 0) - AT(w, 0, -1, 0)) * idy);
-        R r = -vint + Gv / rhoy - R(C.sigma) * dhsdy;
+        R r = -vint + rdiv<R>(Gv, rhoy) - R(C.sigma) * dhsdy;
         if (C.tf) r = r + AT(F.tfv, 0, 0, 0);
         if (on_cap(C, j, k, ny)) { const R b = AT(F.vb, 0, 0, 0); r = r - R(C.cz) * sqrt(b * b) * vc; }
         F.Fv[c0] = (double)r;
@@ -574,8 +590,8 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
             wint = classico_hi<R, DER>(w, c0, s, m, n, vel, ih);
         }
         const R rhoz = (AT(F.rho, 0, 0, (kc) - k) + AT(F.rho, 0, 0, (kc - 1) - k)) * R(0.5);
-        const R tz1 = AT(F.hsz, 0, 0, (kc) - k) * AT(F.kurv, 0, 0, (kc) - k) / AT(F.rho, 0, 0, (kc) - k);
-        const R tz0 = AT(F.hsz, 0, 0, (kc - 1) - k) * AT(F.kurv, 0, 0, (kc - 1) - k) / AT(F.rho, 0, 0, (kc - 1) - k);
+        const R tz1 = rdiv<R>(AT(F.hsz, 0, 0, (kc) - k) * AT(F.kurv, 0, 0, (kc) - k), AT(F.rho, 0, 0, (kc) - k));
+        const R tz0 = rdiv<R>(AT(F.hsz, 0, 0, (kc - 1) - k) * AT(F.kurv, 0, 0, (kc - 1) - k), AT(F.rho, 0, 0, (kc - 1) - k));
         const R dhsdz = (tz1 + tz0) * R(0.5);
         const int ip = clampi(i + 1, 2, nx), im = clampi(i, 2, nx);
         const R amd_p = ((AT(F.znut, (ip) - i, 0, 0) + AT(F.znut, (ip - 1) - i, 0, 0)) * R(0.5)) * idx;
@@ -590,7 +606,7 @@ __global__ void __launch_bounds__(256) k_convdiff(Geo G, CDConst C, CDFields F) 
                           bmd_p * ((AT(w, 0, 1, 0) - wc) * idy + (AT(v, 0, 1, 0) - AT(v, 0, 1, -1)) * idz) -
                           bmd_m * ((wc - AT(w, 0, -1, 0)) * idy + (AT(v, 0, 0, 0) - AT(v, 0, 0, -1)) * idz) +
                           (dmd_k * R(2.) * (AT(w, 0, 0, 1) - wc) - dmd_m * R(2.) * (wc - AT(w, 0, 0, -1))) * idz;
-        R r = -wint + Gv / rhoz - R(C.gz) - R(C.sigma) * dhsdz;
+        R r = -wint + rdiv<R>(Gv, rhoz) - R(C.gz) - R(C.sigma) * dhsdz;
         if (C.tf) r = r + AT(F.tfw, 0, 0, 0);
         if (on_cap(C, j, k, ny)) { const R b = AT(F.wb, 0, 0, 0); r = r - R(C.cz) * sqrt(b * b) * wc; }
         F.Fw[c0] = (double)r;
@@ -1039,6 +1055,7 @@ __global__ void __launch_bounds__(256) k_cg_diag(Geo G, BC bc, CGConst K, const 
 
 // scaled face coefficients s/sqrt(d_c d_nb) = s * (1/sqrt(d_c)) * (1/sqrt(d_nb)) and the first
 // residual (:126-151); reduction of r.r and b.b
+constexpr int kCoefZ = 4;
 __global__ void __launch_bounds__(256, 4) k_cg_coef(Geo G, BC bc, CGConst K, const double* __restrict__ sx,
                                                     const double* __restrict__ sy, const double* __restrict__ sz,
                                                     const double* __restrict__ sd, const double* __restrict__ isd,
@@ -1046,9 +1063,14 @@ __global__ void __launch_bounds__(256, 4) k_cg_coef(Geo G, BC bc, CGConst K, con
                                                     const double* __restrict__ prd1, double* ax, double* ay,
                                                     double* az, double* r, CGState* st, double* partial,
                                                     unsigned int* counter) {
-    const Thread3 t = tid3(1, 1, 1);
-    const int i = t.i, j = t.j, k = t.k, nx = G.nx, ny = G.ny, nz = G.nz;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
     double rr = 0.0, bbv = 0.0;
+    // a thread owns kCoefZ cells of a column: 4x fewer blocks than one cell a thread, whose
+    // partials the grid reduction (one counter) would otherwise take in turn
+#pragma unroll
+    for (int m = 0; m < kCoefZ; ++m) {
+    const int k = blockIdx.z * kCoefZ + 1 + m;
     if (i <= nx && j <= ny && k <= nz) {
         const int c = (int)G.idx(i, j, k);
         const int px = G.px, pxy = (int)G.pxy;
@@ -1073,8 +1095,9 @@ __global__ void __launch_bounds__(256, 4) k_cg_coef(Geo G, BC bc, CGConst K, con
                           bpp * ee(j == ny, c + px, o.yp) - bnp * ee(j == 1, c - px, o.ym) -
                           cpp * ee(k == nz, c + pxy, o.zp) - cnp * ee(k == 1, c - pxy, o.zm) - bv;
         r[c] = rv;
-        rr = rv * rv;
-        bbv = bv * bv;
+        rr += rv * rv;
+        bbv += bv * bv;
+    }
     }
     double trr, tbb;
     if (reduce2_last(rr, bbv, partial, counter, trr, tbb) && flat_tid() == 0) {
@@ -1332,26 +1355,31 @@ __global__ void __launch_bounds__(256) k_posdin(Geo G, BC bc, double aux1, doubl
     }
 }
 
-// A thread walks a column of kEstZ cells.  The loop is unrolled and loads from clamped plane
-// indices, so its loads are issued together; planes past nz are left out of the maximum.  The w
-// face above a cell is the face below the next one.
-constexpr int kEstZ = 4;
+// A thread walks kEstChunks chunks of kEstZ cells of a column.  Each chunk's loop is unrolled and
+// loads from clamped plane indices, so its loads are issued together; planes past nz are left
+// out of the maximum.  The w face above a cell is the face below the next one.  The chunks keep
+// the grid at about a thousand blocks: the grid reduction's single counter takes the blocks'
+// partials in turn, which at one cell a thread (or four) was the kernel's tail.
+constexpr int kEstZ = 4, kEstChunks = 4;
 __global__ void __launch_bounds__(256) k_est(Geo G, double dx, double dy, double dz, const double* __restrict__ u,
                                              const double* __restrict__ v, const double* __restrict__ w,
                                              double* partial, unsigned int* counter, double* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k0 = blockIdx.z * kEstZ + 1;
     double m = 0.;
     if (i <= G.nx && j <= G.ny) {
-        double wz[kEstZ + 1];
+        for (int ch = 0; ch < kEstChunks; ++ch) {
+            const int k0 = (blockIdx.z * kEstChunks + ch) * kEstZ + 1;
+            if (k0 > G.nz) break;
+            double wz[kEstZ + 1];
 #pragma unroll
-        for (int q = 0; q <= kEstZ; ++q) wz[q] = FIDX(w, i, j, min(k0 + q, G.nz + 1));
+            for (int q = 0; q <= kEstZ; ++q) wz[q] = FIDX(w, i, j, min(k0 + q, G.nz + 1));
 #pragma unroll
-        for (int q = 0; q < kEstZ; ++q) {
-            const int k = min(k0 + q, G.nz);
-            const double dv = (FIDX(u, i + 1, j, k) - FIDX(u, i, j, k)) / dx + (FIDX(v, i, j + 1, k) - FIDX(v, i, j, k)) / dy +
-                              (wz[q + 1] - wz[q]) / dz;
-            if (k0 + q <= G.nz) m = isnan(dv) ? INFINITY : fmax(m, fabs(dv));
+            for (int q = 0; q < kEstZ; ++q) {
+                const int k = min(k0 + q, G.nz);
+                const double dv = (FIDX(u, i + 1, j, k) - FIDX(u, i, j, k)) / dx + (FIDX(v, i, j + 1, k) - FIDX(v, i, j, k)) / dy +
+                                  (wz[q + 1] - wz[q]) / dz;
+                if (k0 + q <= G.nz) m = isnan(dv) ? INFINITY : fmax(m, fabs(dv));
+            }
         }
     }
     double ta, tb;
@@ -1373,6 +1401,8 @@ static LsConst ls_const(const suli_ctx* c) {
     L.ihz = (c->P.ccz0 == 0) ? 0 : 1;
     L.ihn = L.ihz;   // der_weno leaves ihs at its z value (14_level_set.f90:377, 717)
     L.dx = c->P.dx; L.dy = c->P.dy; L.dz = c->P.dz;
+    L.rx = 1. / L.dx; L.ry = 1. / L.dy; L.rz = 1. / L.dz;
+    L.frx = 1.f / (float)L.dx; L.fry = 1.f / (float)L.dy; L.frz = 1.f / (float)L.dz;
     L.dx1 = fmax(L.dx, fmax(L.dy, L.dz));
     L.ad = c->P.alpha1 * L.dx1;
     L.pi = acos(-1.0);
@@ -1606,7 +1636,7 @@ void launch_cg_setup(suli_ctx* c) {
     k_cg_faces<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->bc, K, c->f[SULI_F_RHO], sx, sy, sz);
     k_cg_diag<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->bc, K, sx, sy, sz, c->f[SULI_F_U], c->f[SULI_F_V], c->f[SULI_F_W],
                                                       c->f[SULI_F_PRD1], c->cg_d, c->cg_e, c->cg_b, c->cg_sd, c->cg_isd);
-    k_cg_coef<<<cells_grid(G), kBlk, 0, c->stream>>>(G, c->bc, K, sx, sy, sz, c->cg_sd, c->cg_isd, c->cg_e, c->cg_b,
+    k_cg_coef<<<grid3(G.nx, G.ny, (G.nz + kCoefZ - 1) / kCoefZ, kBlk), kBlk, 0, c->stream>>>(G, c->bc, K, sx, sy, sz, c->cg_sd, c->cg_isd, c->cg_e, c->cg_b,
                                                       c->f[SULI_F_PRD1], c->cg_ax, c->cg_ay, c->cg_az, c->cg_r, c->cg,
                                                       c->red_partial, c->red_counter);
 }
@@ -1655,7 +1685,7 @@ void launch_posdin(suli_ctx* c) {
 void launch_est(suli_ctx* c) {
     const Geo& G = c->g;
     ProfScope ps(c, SULI_K_EST, 1);
-    k_est<<<grid3(G.nx, G.ny, (G.nz + kEstZ - 1) / kEstZ, kBlk), kBlk, 0, c->stream>>>(G, c->P.dx, c->P.dy, c->P.dz, c->f[SULI_F_U], c->f[SULI_F_V],
+    k_est<<<grid3(G.nx, G.ny, (G.nz + kEstZ * kEstChunks - 1) / (kEstZ * kEstChunks), kBlk), kBlk, 0, c->stream>>>(G, c->P.dx, c->P.dy, c->P.dz, c->f[SULI_F_U], c->f[SULI_F_V],
                                                   c->f[SULI_F_W], c->red_partial, c->red_counter, c->red_out);
 }
 void launch_fill(suli_ctx* c, double* a, double v) {

@@ -22,7 +22,11 @@
 // last x neighbour) and the device grants the shared memory.
 //
 // Every wait on a slot is bounded: a wait that runs out makes the CTA wait (bounded again) for
-// the loads it issued, sets the inner solve's status to SULI_ERR_CUDA and done, and return.
+// the loads it issued, sets the inner solve's status to SULI_ERR_CUDA and done, and return; the
+// host then fails the solve with SULI_ERR_CUDA (a CTA that started after the flag was set skips
+// the grid reduction, so the context should be destroyed after that error).  The kernels read
+// the level's face constants (c2) before their grid-dependency wait: the multigrid set-up wrote
+// them before the inner solve began, never the kernel launched just before.
 #pragma once
 #include <cuda.h>
 
@@ -122,21 +126,42 @@ __device__ __forceinline__ STile s_tile(const Geo& G) {
     return t;
 }
 
-// the quad's faces in plane k from the density slots of planes k-1, k, k+1 (OpRho4::faces)
+// The quad's faces in plane k from the density slots of planes k-1, k, k+1 (OpRho4::faces).  A
+// face shared by two cells is formed once: the three x faces inside the quad (rho_a + rho_b is
+// the same sum in either order), and the z face below the plane, which is the face above the
+// previous plane of the same march (carried in zc while zk records that plane).
+struct SZCarry {
+    float f[kVX];
+    int k = -1;
+};
 __device__ __forceinline__ void s_faces(const STile& t, int k, int nz, const float* rm, const float* r0,
-                                        const float* rp, float cx2, float cy2, float cz2, Faces (&F)[kVX]) {
+                                        const float* rp, float cx2, float cy2, float cz2, Faces (&F)[kVX],
+                                        SZCarry& zc) {
     const V4 rc = sq(r0, t.ly, t.qx);
     const V4 rym = sq(r0, t.fym, t.qx), ryp = sq(r0, t.fyp, t.qx);
-    const V4 rzm = sq((k > 1) ? rm : rp, t.ly, t.qx), rzp = sq((k < nz) ? rp : rm, t.ly, t.qx);
     const float rxm0 = ss(r0, t.ly, t.fxm), rxp3 = ss(r0, t.ly, t.fxp);
+    float fx[kVX + 1];
+    fx[0] = face_div(cx2, rc.v[0] + rxm0);
+#pragma unroll
+    for (int e = 1; e < kVX; ++e) fx[e] = face_div(cx2, rc.v[e - 1] + rc.v[e]);
+    fx[kVX] = face_div(cx2, rc.v[kVX - 1] + rxp3);
+    float fzm[kVX];
+    if (k > 1 && zc.k == k - 1) {
+#pragma unroll
+        for (int e = 0; e < kVX; ++e) fzm[e] = zc.f[e];
+    } else {
+        const V4 rzm = sq((k > 1) ? rm : rp, t.ly, t.qx);
+#pragma unroll
+        for (int e = 0; e < kVX; ++e) fzm[e] = face_div(cz2, rc.v[e] + rzm.v[e]);
+    }
+    const V4 rzp = sq((k < nz) ? rp : rm, t.ly, t.qx);
 #pragma unroll
     for (int e = 0; e < kVX; ++e) {
         const float r = rc.v[e];
-        const float rxm = (e == 0) ? rxm0 : rc.v[e - 1];
-        const float rxp = (e == kVX - 1) ? rxp3 : rc.v[e + 1];
-        F[e] = Faces{face_div(cx2, r + rxm), face_div(cx2, r + rxp), face_div(cy2, r + rym.v[e]),
-                     face_div(cy2, r + ryp.v[e]), face_div(cz2, r + rzm.v[e]), face_div(cz2, r + rzp.v[e])};
+        zc.f[e] = face_div(cz2, r + rzp.v[e]);
+        F[e] = Faces{fx[e], fx[e + 1], face_div(cy2, r + rym.v[e]), face_div(cy2, r + ryp.v[e]), fzm[e], zc.f[e]};
     }
+    zc.k = k;
 }
 
 // The plane engine.  NF fine fields with the halo, NO fine fields at the tile's own cells (box
@@ -144,15 +169,18 @@ __device__ __forceinline__ void s_faces(const STile& t, int k, int nz, const flo
 // sequence.  body.begin() runs before the first wait, body.plane(k,
 // sm, s0, sp) computes plane k from the slots (one pointer a field, fine then coarse) of the
 // planes k-1, k, k+1, and body.finish() runs after a barrier that follows the last
-// plane.  A scratch of 2 floats a thread (body.xbuf) follows the barriers.  Returns false if a
-// wait ran out.
+// plane.  A scratch of 2 floats a thread (body.xbuf) follows the barriers.  The slot barriers
+// are set up before the wait for the preceding kernel (griddepcontrol.wait), and the first
+// planes' loads are issued before the solve's done flag is read, so neither waits on the
+// other; a CTA that finds the solve done waits for those loads and leaves.  Returns -1 when the
+// solve was done, 1 if a wait ran out, 0 otherwise.
 template <int NF, int NO, int NC>
 struct SSlots {
     const float* f[NF + NO + NC];   // fine fields with halo, own-cell fields, coarse fields
 };
 template <int NF, int NO, int NC, class Body>
-__device__ __forceinline__ bool s_march(const Geo& G, const BC& bc, const CUtensorMap* const (&maps)[NF + NO + NC],
-                                        int chunk, Body& body, PCGState* st) {
+__device__ __forceinline__ int s_march(const Geo& G, const BC& bc, const CUtensorMap* const (&maps)[NF + NO + NC],
+                                       int chunk, Body& body, PCGState* st) {
     extern __shared__ __align__(128) unsigned char s_smem[];
     constexpr size_t kStage = (size_t)NF * kSSlotBytes + (size_t)NO * kSOSlotBytes + (size_t)NC * kSCSlotBytes;
     const int tid = threadIdx.x + kSTX * threadIdx.y;
@@ -171,13 +199,14 @@ __device__ __forceinline__ bool s_march(const Geo& G, const BC& bc, const CUtens
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    pdl_wait();
     auto off = [](int f) -> size_t {   // byte offset of field f in a stage
         return f < NF ? (size_t)f * kSSlotBytes
                       : (f < NF + NO ? (size_t)NF * kSSlotBytes + (size_t)(f - NF) * kSOSlotBytes
                                      : (size_t)NF * kSSlotBytes + (size_t)NO * kSOSlotBytes + (size_t)(f - NF - NO) * kSCSlotBytes);
     };
-    auto slot = [&](int q, int f) -> const float* {
-        return reinterpret_cast<const float*>(s_smem + (size_t)(q % kSR) * kStage + off(f));
+    auto slot_at = [&](int sidx, int f) -> const float* {
+        return reinterpret_cast<const float*>(s_smem + (size_t)sidx * kStage + off(f));
     };
     auto issue = [&](int q) {
         const int s = q % kSR;
@@ -196,11 +225,18 @@ __device__ __forceinline__ bool s_march(const Geo& G, const BC& bc, const CUtens
     };
     if (tid == 0)
         for (int q = 0; q < min(kSR, nseq); ++q) issue(q);
+    if (st->done) {   // the same for every CTA: wait (bounded) for the issued loads, then leave
+        if (tid == 0)
+            for (int q = 0; q < min(kSR, nseq); ++q) s_wait(s_addr(&bars[q]), 0);
+        __syncthreads();
+        return -1;
+    }
     body.begin(k0, nplanes);
+    int sl0 = 0, sl1 = 1, sl2 = 2;   // ring slots of sequence m, m + 1, m + 2
     for (int m = 0; m < nplanes; ++m) {
         bool ok = true;
         if (m == 0) ok = s_wait(s_addr(&bars[0]), 0) && s_wait(s_addr(&bars[1]), 0);
-        ok = ok && s_wait(s_addr(&bars[(m + 2) % kSR]), ((m + 2) / kSR) & 1);
+        ok = ok && s_wait(s_addr(&bars[sl2]), ((m + 2) / kSR) & 1);
         if (__syncthreads_or(!ok)) {
             // wait (bounded) for the loads issued and not yet consumed, then give up
             if (tid == 0) {
@@ -210,22 +246,25 @@ __device__ __forceinline__ bool s_march(const Geo& G, const BC& bc, const CUtens
                 st->done = 1;
             }
             __syncthreads();
-            return false;
+            return 1;
         }
         // every thread is done with plane k0 + m - 2 (sequence m - 1): refill its slot
         if (tid == 0 && m >= 1 && m - 1 + kSR < nseq) issue(m - 1 + kSR);
         SSlots<NF, NO, NC> sm, s0, sp;
 #pragma unroll
         for (int f = 0; f < NF + NO + NC; ++f) {
-            sm.f[f] = slot(m, f);
-            s0.f[f] = slot(m + 1, f);
-            sp.f[f] = slot(m + 2, f);
+            sm.f[f] = slot_at(sl0, f);
+            s0.f[f] = slot_at(sl1, f);
+            sp.f[f] = slot_at(sl2, f);
         }
         body.plane(k0 + m, sm, s0, sp);
+        sl0 = sl1;   // the ring's slots of sequence m + 1, m + 2, m + 3 for the next plane
+        sl1 = sl2;
+        sl2 = (sl2 + 1 == kSR) ? 0 : sl2 + 1;
     }
     __syncthreads();
     body.finish();
-    return true;
+    return 0;
 }
 
 // Body members every body has: the thread's tile position and the march's scratch
@@ -234,6 +273,7 @@ struct SBase {
     int nz, pxy;
     float cx2, cy2, cz2;
     float* xbuf;
+    SZCarry zc;
     __device__ __forceinline__ void init(const Geo& G, const float* c2) {
         t = s_tile(G);
         nz = G.nz;
@@ -263,7 +303,7 @@ struct SPreBody : SBase {
         x1(s0, t.ly, t.qx, xc);
         x1(sp, t.ly, t.qx, zp);
         Faces F[kVX];
-        s_faces(t, k, nz, sm.f[2], s0.f[2], sp.f[2], cx2, cy2, cz2, F);
+        s_faces(t, k, nz, sm.f[2], s0.f[2], sp.f[2], cx2, cy2, cz2, F, zc);
         x1(s0, t.uym, t.qx, ym);
         x1(s0, t.uyp, t.qx, yp);
         apply4(F, xc, x1s(s0, t.ly, t.uxm), x1s(s0, t.ly, t.uxp), ym, yp, zm, zp, ax);
@@ -278,8 +318,6 @@ __global__ void __launch_bounds__(kSTX * kSTY, 2) k_mgs_pre(Geo G, BC bc, const 
                                                          const __grid_constant__ CUtensorMap mr, const float* c2,
                                                          float* y, float omega, float omega2, int chunk,
                                                          PCGState* st) {
-    pdl_wait();
-    if (st->done) return;
     SPreBody b;
     b.init(G, c2);
     b.omega = omega;
@@ -300,7 +338,7 @@ struct SJaccBody : SBase {
         if (!t.in) return;
         const V4 zm = sq(sm.f[0], t.ly, t.qx), xc = sq(s0.f[0], t.ly, t.qx), zp = sq(sp.f[0], t.ly, t.qx);
         Faces F[kVX];
-        s_faces(t, k, nz, sm.f[1], s0.f[1], sp.f[1], cx2, cy2, cz2, F);
+        s_faces(t, k, nz, sm.f[1], s0.f[1], sp.f[1], cx2, cy2, cz2, F, zc);
         const V4 y1 = sq(s0.f[0], t.uym, t.qx), y2 = sq(s0.f[0], t.uyp, t.qx);
         float ax[kVX], out[kVX];
         apply4(F, xc.v, ss(s0.f[0], t.ly, t.uxm), ss(s0.f[0], t.ly, t.uxp), y1.v, y2.v, zm.v, zp.v, ax);
@@ -319,15 +357,14 @@ __global__ void __launch_bounds__(kSTX * kSTY, 2) k_mgs_jacc(Geo G, BC bc, const
                                                           const __grid_constant__ CUtensorMap md, const float* c2,
                                                           float* xout, float omega, int chunk, PCGState* st,
                                                           double* partial, unsigned int* counter) {
-    pdl_wait();
-    if (st->done) return;
     SJaccBody b;
     b.init(G, c2);
     b.omega = omega;
     b.xout = xout;
     b.dot = 0.;
     const CUtensorMap* const maps[4] = {&mx, &mr, &mf, &md};
-    s_march<2, 2, 0>(G, bc, maps, chunk, b, st);   // every CTA joins the reduction, even one that gave up
+    // every CTA joins the reduction, even one that gave up; none when the solve is done
+    if (s_march<2, 2, 0>(G, bc, maps, chunk, b, st) < 0) return;
     double t, u;
     if (reduce2_last(b.dot, 0.0, partial, counter, t, u) && flat_tid() == 0) {
         const double rz_old = st->rz;
@@ -341,8 +378,11 @@ __global__ void __launch_bounds__(kSTX * kSTY, 2) k_mgs_jacc(Geo G, BC bc, const
 // 0): slots z, p_old, density
 struct SSpmvBody : SBase {
     float beta;
+    const PCGState* pst;
     float *p_new, *qv;
     double dot;
+    // beta comes from the preceding kernel: read after the march's griddepcontrol.wait
+    __device__ __forceinline__ void begin(int, int) { beta = (float)pst->beta; }
     __device__ __forceinline__ void pn(const SSlots<3, 0, 0>& s, int ly, int lx, float (&o)[kVX]) const {
         const V4 a = sq(s.f[0], ly, lx), b = sq(s.f[1], ly, lx);
 #pragma unroll
@@ -358,7 +398,7 @@ struct SSpmvBody : SBase {
         pn(s0, t.ly, t.qx, xc);
         pn(sp, t.ly, t.qx, zp);
         Faces F[kVX];
-        s_faces(t, k, nz, sm.f[2], s0.f[2], sp.f[2], cx2, cy2, cz2, F);
+        s_faces(t, k, nz, sm.f[2], s0.f[2], sp.f[2], cx2, cy2, cz2, F, zc);
         pn(s0, t.uym, t.qx, ym);
         pn(s0, t.uyp, t.qx, yp);
         apply4(F, xc, pns(s0, t.ly, t.uxm), pns(s0, t.ly, t.uxp), ym, yp, zm, zp, ax);
@@ -374,16 +414,15 @@ __global__ void __launch_bounds__(kSTX * kSTY, 2) k_pcgs_spmvc(Geo G, BC bc, con
                                                             const __grid_constant__ CUtensorMap mr, const float* c2,
                                                             float* p_new, float* qv, int chunk, PCGState* st,
                                                             double* partial, unsigned int* counter) {
-    pdl_wait();
-    if (st->done) return;
     SSpmvBody b;
     b.init(G, c2);
-    b.beta = (float)st->beta;
+    b.pst = st;
     b.p_new = p_new;
     b.qv = qv;
     b.dot = 0.;
     const CUtensorMap* const maps[3] = {&mz, &mp, &mr};
-    s_march<3, 0, 0>(G, bc, maps, chunk, b, st);   // every CTA joins the reduction, even one that gave up
+    // every CTA joins the reduction, even one that gave up; none when the solve is done
+    if (s_march<3, 0, 0>(G, bc, maps, chunk, b, st) < 0) return;
     double t, u;
     if (reduce2_last(b.dot, 0.0, partial, counter, t, u) && flat_tid() == 0) {
         st->pq = t;
@@ -430,7 +469,7 @@ struct SRestrictBody : SBase {
         if (!t.in) return;
         const V4 zm = sq(sm.f[0], t.ly, t.qx), xc = sq(s0s.f[0], t.ly, t.qx), zp = sq(sp.f[0], t.ly, t.qx);
         Faces F[kVX];
-        s_faces(t, k, nz, sm.f[1], s0s.f[1], sp.f[1], cx2, cy2, cz2, F);
+        s_faces(t, k, nz, sm.f[1], s0s.f[1], sp.f[1], cx2, cy2, cz2, F, zc);
         const V4 y1 = sq(s0s.f[0], t.uym, t.qx), y2 = sq(s0s.f[0], t.uyp, t.qx);
         float ax[kVX];
         apply4(F, xc.v, ss(s0s.f[0], t.ly, t.uxm), ss(s0s.f[0], t.ly, t.uxp), y1.v, y2.v, zm.v, zp.v, ax);
@@ -455,8 +494,6 @@ __global__ void __launch_bounds__(kSTX * kSTY, 2) k_mgs_restrict(Geo G, Geo Gc, 
                                                               const __grid_constant__ CUtensorMap mr,
                                                               const __grid_constant__ CUtensorMap mf, const float* c2,
                                                               float* fc, int chunk, PCGState* st) {
-    pdl_wait();
-    if (st->done) return;
     SRestrictBody b;
     b.init(G, c2);
     b.Gc = Gc;
@@ -490,7 +527,7 @@ struct SPostBody : SBase {
         xq(s0.f[0], s0.f[4], t.ly, xc);
         xq(sp.f[0], sp.f[4], t.ly, zp);
         Faces F[kVX];
-        s_faces(t, k, nz, sm.f[1], s0.f[1], sp.f[1], cx2, cy2, cz2, F);
+        s_faces(t, k, nz, sm.f[1], s0.f[1], sp.f[1], cx2, cy2, cz2, F, zc);
         xq(s0.f[0], s0.f[4], t.uym, ym);
         xq(s0.f[0], s0.f[4], t.uyp, yp);
         apply4(F, xc, xs(s0.f[0], s0.f[4], t.ly, t.uxm), xs(s0.f[0], s0.f[4], t.ly, t.uxp), ym, yp, zm, zp, ax);
@@ -507,8 +544,6 @@ __global__ void __launch_bounds__(kSTX * kSTY, 2) k_mgs_post(Geo G, BC bc, const
                                                           const __grid_constant__ CUtensorMap mc, const float* c2,
                                                           float* xout, float omega, float alpha, int chunk,
                                                           PCGState* st) {
-    pdl_wait();
-    if (st->done) return;
     SPostBody b;
     b.init(G, c2);
     b.omega = omega;

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -262,8 +263,10 @@ __global__ void __launch_bounds__(256) k_wgrad(Vol vol, ConvIn in, const __nv_bf
     }
 }
 
-// squared error L = mean(e^2), e = pred - target; dout = 2 e / V
-__global__ void k_loss_sums(long long V, const float* __restrict__ pred, const float* __restrict__ tgt, double* sums) {
+// squared error L = mean(e^2), e = pred - target; dout = 2 e / V.  The sums are block partials
+// (fixed warp-shuffle tree) folded in block order by k_loss_fold, so the loss is reproducible.
+__global__ void k_loss_sums(long long V, const float* __restrict__ pred, const float* __restrict__ tgt,
+                            double* __restrict__ part) {
     __shared__ double sh[2][8];
     const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double e = 0., e2 = 0.;
@@ -281,9 +284,26 @@ __global__ void k_loss_sums(long long V, const float* __restrict__ pred, const f
     if (threadIdx.x == 0) {
         double a = 0., b = 0.;
         for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { a += sh[0][q]; b += sh[1][q]; }
-        atomicAdd(&sums[0], a);
-        atomicAdd(&sums[1], b);
+        part[2 * blockIdx.x] = a;
+        part[2 * blockIdx.x + 1] = b;
     }
+}
+// one block: thread t folds partials t, t + 256, ... in order, then a fixed tree
+__global__ void __launch_bounds__(256) k_loss_fold(int nparts, const double* __restrict__ part, double* sums) {
+    __shared__ double sh[2][256];
+    double a = 0., b = 0.;
+    for (int q = threadIdx.x; q < nparts; q += 256) { a += part[2 * q]; b += part[2 * q + 1]; }
+    sh[0][threadIdx.x] = a;
+    sh[1][threadIdx.x] = b;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + h];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { sums[0] = sh[0][0]; sums[1] = sh[1][0]; }
 }
 __global__ void k_loss_grad(long long V, const float* __restrict__ pred, const float* __restrict__ tgt,
                             float* __restrict__ dout) {
@@ -340,6 +360,7 @@ struct suli_nn {
     __nv_bfloat16 *gact[kConv] = {nullptr}, *gpool[kLevels - 1] = {nullptr}, *gcat = nullptr, *gtmp = nullptr;
     float *out = nullptr, *dout = nullptr;
     double* sums = nullptr;
+    double* loss_part = nullptr;     // block partials of the loss sums
     double* host_sums = nullptr;
     int* err_flag = nullptr;         // set by a tensor-core convolution whose wait timed out
     int kernel = 0;                  // convolution kernel: 0 tcgen05 pipeline, 1 mma.sync, 2 tcgen05 one tile per CTA
@@ -526,6 +547,135 @@ void conv(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* W, 
     }
 }
 
+// The weight gradient on the tensor cores (mma.sync m16n8k16, BF16 x BF16 -> FP32).  Per tap it
+// is the GEMM dW_tap (COUT x CIN) += dZ^T (COUT x V) X_tap (V x CIN) over the CTA's chunk of
+// voxels: dZ and the shifted input of kWgTcSub voxels are staged as BF16 rows (voxel-major, rows
+// padded by 8 elements so that ldmatrix reads are free of bank conflicts), A fragments (COUT rows,
+// voxels along K) and B fragments (voxels along K, CIN columns) come from ldmatrix.trans of those
+// rows.  The warps split the 16 x 8 output tiles and, where a layer has fewer tiles than warps,
+// the voxels; the voxel-split partials are added in warp order through shared memory.  Each CTA
+// writes its row of part exactly as k_wgrad does, so the sum over rows is as reproducible.
+constexpr int kWgTcSub = 64;
+__device__ __forceinline__ void ldmatrix_x4_trans(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2,
+                                                  uint32_t& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+__device__ __forceinline__ void ldmatrix_x2_trans(uint32_t addr, uint32_t& r0, uint32_t& r1) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n" : "=r"(r0), "=r"(r1) : "r"(addr));
+}
+template <int CO16, int CI16>
+__global__ void __launch_bounds__(256) k_wgrad_tc(Vol vol, ConvIn in, const __nv_bfloat16* __restrict__ dz,
+                                                  float* part) {
+    constexpr int COUT = CO16 * 16, CIN = CI16 * 16;
+    constexpr int TN = CIN / 8, TILES = CO16 * TN;
+    constexpr int KW = (TILES < 8 && 8 % TILES == 0) ? 8 / TILES : 1;   // warps sharing a tile's voxels
+    constexpr int TW = 8 / KW;                                           // warps splitting the tiles
+    constexpr int TPW = (TILES + TW - 1) / TW;                           // tiles a warp owns
+    constexpr int RZ = COUT + 8, RX = CIN + 8;
+    __shared__ __align__(16) __nv_bfloat16 sz[kWgTcSub][RZ];
+    __shared__ __align__(16) __nv_bfloat16 sx[kWgTcSub][RX];
+    __shared__ float red[KW > 1 ? (KW - 1) * TW * TPW * 128 : 1];
+    const int tap = blockIdx.y;
+    const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dzz = tap / 9 - 1;
+    const long long V = (long long)vol.nx * vol.ny * vol.nz;
+    const long long v0 = (long long)blockIdx.x * kWgChunk;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tw = warp % TW, kw = warp / TW;
+    float acc[TPW][4];
+#pragma unroll
+    for (int i = 0; i < TPW; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
+    float bacc = 0.f;   // the bias gradient of channel tid (tap 13)
+    const int hxn = (vol.nx + 1) / 2, hyn = (vol.ny + 1) / 2;
+    const uint32_t szu = smem_u32(&sz[0][0]), sxu = smem_u32(&sx[0][0]);
+    for (long long vs = v0; vs < v0 + kWgChunk && vs < V; vs += kWgTcSub) {
+        // stage dZ and the shifted input of kWgTcSub voxels (16-byte vectors, zero outside)
+        for (int q = tid; q < kWgTcSub * (COUT / 8); q += 256) {
+            const int m = q / (COUT / 8), c = (q % (COUT / 8)) * 8;
+            const long long v = vs + m;
+            uint4 val = make_uint4(0u, 0u, 0u, 0u);
+            if (v < V) val = *reinterpret_cast<const uint4*>(dz + v * COUT + c);
+            *reinterpret_cast<uint4*>(&sz[m][c]) = val;
+        }
+        for (int q = tid; q < kWgTcSub * (CIN / 8); q += 256) {
+            const int m = q / (CIN / 8), c = (q % (CIN / 8)) * 8;
+            const long long v = vs + m;
+            uint4 val = make_uint4(0u, 0u, 0u, 0u);
+            if (v < V) {
+                const int x = (int)(v % vol.nx) + dx, y = (int)((v / vol.nx) % vol.ny) + dy,
+                          z = (int)(v / ((long long)vol.nx * vol.ny)) + dzz;
+                if (x >= 0 && x < vol.nx && y >= 0 && y < vol.ny && z >= 0 && z < vol.nz) {
+                    if (c < in.ca) {
+                        const long long vi = in.a_half ? ((long long)(x >> 1) + hxn * ((long long)(y >> 1) + (long long)hyn * (z >> 1)))
+                                                       : ((long long)x + vol.nx * ((long long)y + (long long)vol.ny * z));
+                        val = *reinterpret_cast<const uint4*>(in.a + vi * in.ca + c);
+                    } else {
+                        const long long vi = (long long)x + vol.nx * ((long long)y + (long long)vol.ny * z);
+                        val = *reinterpret_cast<const uint4*>(in.b + vi * in.cb + (c - in.ca));
+                    }
+                }
+            }
+            *reinterpret_cast<uint4*>(&sx[m][c]) = val;
+        }
+        __syncthreads();
+        if (tap == 13 && tid < COUT)
+            for (int m = 0; m < kWgTcSub; ++m) bacc += __bfloat162float(sz[m][tid]);
+        // this warp's K steps (16 voxels each) of the staged block
+        for (int ks = kw; ks < kWgTcSub / 16; ks += KW) {
+            const int vb = ks * 16;
+            // A: lane -> matrix mi = lane / 8 (co + 8 (mi & 1), voxels + 8 (mi >> 1)), row lane % 8
+            const int ar = vb + (lane & 7) + 8 * (lane >> 4), ac = 8 * ((lane >> 3) & 1);
+            // B: lanes 0-15 give the rows of the two 8-voxel halves (x2)
+            const int br = vb + (lane & 15);
+#pragma unroll
+            for (int i = 0; i < TPW; ++i) {
+                const int t = tw + TW * i;
+                if (t < TILES) {
+                    const int co0 = 16 * (t / TN), ci0 = 8 * (t % TN);
+                    uint32_t a0, a1, a2, a3, b0, b1;
+                    ldmatrix_x4_trans(szu + (uint32_t)((ar * RZ + co0 + ac) * 2), a0, a1, a2, a3);
+                    ldmatrix_x2_trans(sxu + (uint32_t)((br * RX + ci0) * 2), b0, b1);
+                    mma_bf16(acc[i], a0, a1, a2, a3, b0, b1);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // voxel-split warps: add the partials in warp order (kw = 1 .. KW - 1 into kw = 0)
+    if (KW > 1) {
+        if (kw > 0)
+#pragma unroll
+            for (int i = 0; i < TPW; ++i)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) red[(((kw - 1) * TW + tw) * TPW + i) * 128 + e * 32 + lane] = acc[i][e];
+        __syncthreads();
+        if (kw == 0)
+            for (int w = 1; w < KW; ++w)
+#pragma unroll
+                for (int i = 0; i < TPW; ++i)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) acc[i][e] += red[(((w - 1) * TW + tw) * TPW + i) * 128 + e * 32 + lane];
+    }
+    float* row = part + (long long)blockIdx.x * (27LL * COUT * CIN + COUT);
+    if (kw == 0) {
+#pragma unroll
+        for (int i = 0; i < TPW; ++i) {
+            const int t = tw + TW * i;
+            if (t >= TILES) continue;
+            const int co0 = 16 * (t / TN), ci0 = 8 * (t % TN);
+            // accumulator: rows lane / 4 (+ 8), columns 2 (lane % 4) + {0, 1}
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const int co = co0 + (lane >> 2) + 8 * half, ci = ci0 + 2 * (lane & 3);
+                row[((long long)tap * COUT + co) * CIN + ci] = acc[i][2 * half];
+                row[((long long)tap * COUT + co) * CIN + ci + 1] = acc[i][2 * half + 1];
+            }
+        }
+    }
+    if (tap == 13 && tid < COUT) row[27LL * COUT * CIN + tid] = bacc;
+}
+
 // per-CTA rows of partial sums (k_wgrad, k_head_bwd), grown on demand (training only)
 float* part_buffer(suli_nn* N, long long floats) {
     if (floats > N->part_floats) {
@@ -538,6 +688,11 @@ float* part_buffer(suli_nn* N, long long floats) {
     return N->part;
 }
 
+// SULI_WGRAD_CUDA_CORES=1 keeps the CUDA-core weight gradient (k_wgrad), for comparison
+static bool wgrad_cuda_cores() {
+    const char* ev = std::getenv("SULI_WGRAD_CUDA_CORES");
+    return ev && std::strcmp(ev, "1") == 0;
+}
 template <int CO16, int CI16>
 void wgrad_launch(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloat16* dz, float* dw, float* db) {
     const long long V = (long long)vol.nx * vol.ny * vol.nz;
@@ -546,7 +701,10 @@ void wgrad_launch(suli_nn* N, const Vol& vol, const ConvIn& in, const __nv_bfloa
     float* part = part_buffer(N, chunks * width);
     if (!part) { N->grad_error = true; return; }
     const dim3 grid((unsigned)chunks, 27);
-    k_wgrad<CO16, CI16><<<grid, 256, 0, N->stream>>>(vol, in, dz, part);
+    if (wgrad_cuda_cores())
+        k_wgrad<CO16, CI16><<<grid, 256, 0, N->stream>>>(vol, in, dz, part);
+    else
+        k_wgrad_tc<CO16, CI16><<<grid, 256, 0, N->stream>>>(vol, in, dz, part);
     // the layer's bias follows its weights in the parameter vector (db == dw + 27 COUT CIN)
     if (db != dw + 27LL * (CO16 * 16) * (CI16 * 16)) { N->grad_error = true; return; }
     k_sum_parts<<<nb(width), 256, 0, N->stream>>>(chunks, width, part, dw);
@@ -779,6 +937,7 @@ int suli_nn_create(int nx, int ny, int nz, int device, suli_nn** out) {
     A(alloc(&N->out, N->V[0]));
     A(alloc(&N->dout, N->V[0]));
     A(alloc(&N->sums, 4));
+    A(alloc(&N->loss_part, 2 * (long long)nb(N->V[0])));
     A(alloc(&N->err_flag, 1));
     A(cudaMallocHost(&N->host_sums, 4 * sizeof(double)));
     if (ok) {
@@ -806,7 +965,7 @@ int suli_nn_destroy(suli_nn* N) {
     cudaFree(N->in0);
     for (int l = 0; l < kConv; ++l) { cudaFree(N->a[l]); cudaFree(N->gact[l]); }
     for (int l = 0; l < kLevels - 1; ++l) cudaFree(N->pool[l]);
-    cudaFree(N->gcat); cudaFree(N->gtmp); cudaFree(N->out); cudaFree(N->dout); cudaFree(N->sums);
+    cudaFree(N->gcat); cudaFree(N->gtmp); cudaFree(N->out); cudaFree(N->dout); cudaFree(N->sums); cudaFree(N->loss_part);
     cudaFree(N->part);
     cudaFree(N->err_flag);
     if (N->host_sums) cudaFreeHost(N->host_sums);
@@ -852,8 +1011,8 @@ int suli_nn_loss_grad(suli_nn* N, const float* d_in3, const float* d_target, dou
     cudaSetDevice(N->device);
     k_pack_input<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], d_in3, N->in0);
     forward(N, N->out, true);
-    cudaMemsetAsync(N->sums, 0, 4 * sizeof(double), N->stream);
-    k_loss_sums<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->out, d_target, N->sums);
+    k_loss_sums<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->out, d_target, N->loss_part);
+    k_loss_fold<<<1, 256, 0, N->stream>>>((int)nb(N->V[0]), N->loss_part, N->sums);
     k_loss_grad<<<nb(N->V[0]), 256, 0, N->stream>>>(N->V[0], N->out, d_target, N->dout);
     cudaMemsetAsync(N->g, 0, N->nparam * 4, N->stream);
     N->grad_error = false;

@@ -222,19 +222,32 @@ __global__ void __launch_bounds__(TP_THREADS, 1)
                         tp_tma3(wdst, &map_w, c0, 0, 0, full(s));
                         tp_tma3(wdst + wplane, &map_w, c0 + 8, 0, 0, full(s));
                     }
-                    for (int q = tid; q < G::HXR * G::HYR * (NZ + 2) * 2; q += 128) {
-                        const int kc = q & 1, h = q >> 1;
-                        const int hx = h % G::HXR, hy = (h / G::HXR) % G::HYR, hz = h / (G::HXR * G::HYR);
+                    // a thread copies the rows h = (tid >> 1) + 64 m of 8-channel plane kc = tid & 1;
+                    // its (hx, hy, hz) advance by the constant step of 64 rows (no division per row)
+                    constexpr int NH = G::HXR * G::HYR * (NZ + 2);
+                    constexpr int DX = 64 % G::HXR, DY = (64 / G::HXR) % G::HYR, DZ = 64 / (G::HXR * G::HYR);
+                    const int kc = tid & 1, h0 = tid >> 1;
+                    int hx = h0 % G::HXR, hy = (h0 / G::HXR) % G::HYR, hz = h0 / (G::HXR * G::HYR);
+                    const __nv_bfloat16* abase = in.a + c0 + kc * 8;
+                    const uint32_t dbase = dst + (uint32_t)(kc * cfg.kc_bytes);
+                    for (int h = h0; h < NH; h += 64) {
                         const int gx = x0 + hx - 1, gy = y0 + hy - 1, gz = z0 + hz - 1;
                         const void* src = in.a;
                         int bytes = 0;
                         if (gx >= 0 && gx < vol.nx && gy >= 0 && gy < vol.ny && gz >= 0 && gz < vol.nz) {
                             const long long vi =
                                 (long long)(gx >> 1) + hxn * ((long long)(gy >> 1) + (long long)hyn * (gz >> 1));
-                            src = in.a + vi * in.ca + c0 + kc * 8;
+                            src = abase + vi * in.ca;
                             bytes = 16;
                         }
-                        cp_async16(dst + (uint32_t)(kc * cfg.kc_bytes + (hz * G::HYR + hy) * RUN + hx * 16), src, bytes);
+                        cp_async16(dbase + (uint32_t)((hz * G::HYR + hy) * RUN + hx * 16), src, bytes);
+                        hx += DX;
+                        const int cy = (hx >= G::HXR) ? 1 : 0;
+                        hx -= cy * G::HXR;
+                        hy += DY + cy;
+                        const int cz = (hy >= G::HYR) ? 1 : 0;
+                        hy -= cz * G::HYR;
+                        hz += DZ + cz;
                     }
                     tp_cp_async_arrive(full(s));
                 } else if (tid == 0) {

@@ -819,9 +819,27 @@ int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
     bool fallback = false;
     double rr_prev = -1.;
     bool inner_capped = false;
+    // The inner solve's state is copied to the host right after its loop and read at the next
+    // synchronisation, so the refinement residual is launched without waiting for the host.
+    bool pcg_pending = false;
+    auto take_inner = [&]() -> int {
+        pcg_pending = false;
+        if (c->pcg_host[0].status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the inner solve");
+        if (c->pcg_host[0].status == SULI_ERR_CUDA)
+            return fail(c, SULI_ERR_CUDA, "graddin: a streaming multigrid kernel's wait for its loads ran out");
+        inner_total += c->pcg_host[0].iters;
+        inner_capped = (c->pcg_host[0].iters >= c->inner_maxit);
+        if (c->use_graphs) {   // eager launches were counted as they went
+            const long long bodies = std::max(1, (c->pcg_host[0].iters - 1 + 1) / 2);
+            c->prof.launches[SULI_K_MG] += bodies * (2LL * c->pcg_graph_kernels + 1);
+        }
+        return SULI_OK;
+    };
     while (true) {
         int r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
         if (r != SULI_OK) return r;
+        if (pcg_pending)
+            if (int ri = take_inner()) return ri;
         if (c->cg_host[0].status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the Poisson solve");
         if (c->cg_host[0].done) break;
         // a pass that did not halve the FP64 residual, or an inner solve that hit its cap: the
@@ -852,15 +870,8 @@ int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
                 if (c->pcg_host[0].done) break;
             }
         }
-        r = sync_read(c, c->pcg, c->pcg_host, sizeof(PCGState));
-        if (r != SULI_OK) return r;
-        if (c->pcg_host[0].status == SULI_ERR_NAN) return fail(c, SULI_ERR_NAN, "graddin: NaN/Inf in the inner solve");
-        inner_total += c->pcg_host[0].iters;
-        inner_capped = (c->pcg_host[0].iters >= c->inner_maxit);
-        if (c->use_graphs) {   // eager launches were counted as they went
-            const long long bodies = std::max(1, (c->pcg_host[0].iters - 1 + 1) / 2);
-            c->prof.launches[SULI_K_MG] += bodies * (2LL * c->pcg_graph_kernels + 1);
-        }
+        CUDA_TRY(c, cudaMemcpyAsync(c->pcg_host, c->pcg, sizeof(PCGState), cudaMemcpyDeviceToHost, c->stream));
+        pcg_pending = true;
         launch_mx_residual(c, ecur, enext, true);
         std::swap(ecur, enext);
         CHECK_LAUNCH(c);
@@ -870,6 +881,8 @@ int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
             // residual, with the energy-optimal FP64 step, before the next pass (or the test)
             r = sync_read(c, c->cg, c->cg_host, sizeof(CGState));
             if (r != SULI_OK) return r;
+            if (pcg_pending)
+                if (int ri = take_inner()) return ri;
             if (!c->cg_host[0].done) {
                 {
                     ProfScope ps(c, SULI_K_CG_SETUP, 2);

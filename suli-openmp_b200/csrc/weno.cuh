@@ -6,8 +6,8 @@
 // rules (ihs, :530-570): 0 periodic with phi(0) = phi(n-1) (the reference's offset),
 // 1 one-sided extrapolation (1/5 rows at the low end, 1/11 rows at the high end),
 // 2 the 1/11 "zero derivative" rows at both ends.  The arithmetic is the reference's with its
-// divisions rearranged: one reciprocal of h per pencil, and the nonlinear weights
-// w_k/q_k^2 / sum_m w_m/q_m^2 formed over a common denominator (one division per side).
+// divisions rearranged: the reciprocal of h formed once on the host, and in FP64 the nonlinear
+// weights w_k/q_k^2 / sum_m w_m/q_m^2 formed over a common denominator (one division per side).
 #pragma once
 
 namespace suli {
@@ -55,7 +55,10 @@ __device__ __forceinline__ void pencil7(F at, int i, int n, int ihs, T P[7]) {
 
 // omega_k = (w_k/q_k^2) / sum_m (w_m/q_m^2), q_k = eps + is_k.  FP64: over the common
 // denominator q_1^2 q_2^2 q_3^2 (q >= eps = 1e-8, so the products stay far inside the FP64
-// range); other types: the three quotients and one reciprocal of their sum.
+// range); FP32 (the mixed path's arithmetic, where that product can underflow): the three
+// quotients and one reciprocal of their sum, each with the hardware reciprocal (__fdividef, 2
+// ulp; q^2 stays far below the 2^126 where it would flush), since IEEE FP32 divisions were a
+// third of the WENO kernels' instructions.
 template <typename T>
 __device__ __forceinline__ void nonlinear_weights(T is1, T is2, T is3, T eps, T w1, T w2, T w3, T& o1, T& o2,
                                                   T& o3) {
@@ -65,19 +68,19 @@ __device__ __forceinline__ void nonlinear_weights(T is1, T is2, T is3, T eps, T 
         const T inv = T(1) / (n1 + n2 + n3);
         o1 = n1 * inv; o2 = n2 * inv; o3 = n3 * inv;
     } else {
-        const T al1 = w1 / a, al2 = w2 / b, al3 = w3 / c;
-        const T inv = T(1) / (al1 + al2 + al3);
+        const T al1 = __fdividef(w1, a), al2 = __fdividef(w2, b), al3 = __fdividef(w3, c);
+        const T inv = __fdividef(T(1), al1 + al2 + al3);
         o1 = al1 * inv; o2 = al2 * inv; o3 = al3 * inv;
     }
 }
 
-// One-sided derivatives from the seven values P[0..6] = phi(i-3..i+3):
-// dp = phi_x^+ (dphidxp, right-biased), dn = phi_x^- (dphidxn, left-biased).
+// One-sided derivatives from the seven values P[0..6] = phi(i-3..i+3) and ih = 1/h (formed
+// once on the host, in the compute type): dp = phi_x^+ (dphidxp, right-biased), dn = phi_x^-
+// (dphidxn, left-biased).
 template <typename T>
-__device__ __forceinline__ void weno_pair(const T P[7], T h, T& dp, T& dn) {
+__device__ __forceinline__ void weno_pair(const T P[7], T ih, T& dp, T& dn) {
     // D[m] = (phi(i-2+m) - phi(i-3+m))/h; up(i-4..i) = D1..D5, un(i..i+4) = D0..D4
     T D[6];
-    const T ih = T(1) / h;
 #pragma unroll
     for (int m = 0; m < 6; ++m) D[m] = (P[m + 1] - P[m]) * ih;
     const T aux1 = T(13. / 12.), aux2 = T(1. / 4.), aux3 = T(1. / 6.), aux6 = T(0.00000001);

@@ -242,6 +242,31 @@ def test_loss_and_gradient_match_oracle(pkg, torch, kernel):
     net.close()
 
 
+@pytest.mark.parametrize("n", [16, 32])
+def test_tensor_core_weight_gradient_matches_cuda_cores(pkg, torch, monkeypatch, n):
+    """The weight gradients on the tensor cores (k_wgrad_tc, mma.sync BF16 -> FP32, default)
+    against the CUDA-core kernel (SULI_WGRAD_CUDA_CORES=1): the same BF16 products summed in FP32
+    in another order, so every parameter block agrees to 1e-3 of its norm; at 32^3 the CTAs'
+    voxel chunks and the row sums are exercised (8 chunks of 4096 voxels).  Both reproducible."""
+    theta32, _, x3, _, tgt = _setup(torch, n, 5)
+    d_in = torch.from_numpy(x3).to("cuda:0")
+    d_t = torch.from_numpy(tgt.ravel()).to("cuda:0")
+    grads = {}
+    for cc in ("1", "0"):
+        monkeypatch.setenv("SULI_WGRAD_CUDA_CORES", cc)
+        net = pkg.learned.Net(n, n, n, params=theta32)
+        loss, g = net.loss_grad(d_in, d_t)
+        _, g2 = net.loss_grad(d_in, d_t)
+        assert np.array_equal(g, g2)
+        grads[cc] = (loss, g.astype(np.float64))
+        net.close()
+    (l1, g1), (l0, g0) = grads["1"], grads["0"]
+    assert l1 == l0
+    for name, sl in _layer_slices():
+        a, b = g0[sl], g1[sl]
+        assert np.linalg.norm(a - b) <= 1e-3 * max(np.linalg.norm(b), 1e-30), name
+
+
 def test_adam_lowers_loss_and_params_roundtrip(pkg, torch):
     n = 16
     theta32, _, x3, _, tgt = _setup(torch, n, 11)
