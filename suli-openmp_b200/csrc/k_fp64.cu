@@ -977,6 +977,7 @@ __global__ void __launch_bounds__(kFixThreads) k_outflow_fix(Geo G, BCArgs A, co
 struct CGConst {
     double cx, cy, cz;     // dt/(dx*dx) ...
     double dx, dy, dz;
+    double rdx, rdy, rdz;  // 1/dx, 1/dy, 1/dz
     double tol;            // cg_tol
     double div_tol;        // div_tol (0: off)
     double ncell;          // nx*ny*nz
@@ -1043,14 +1044,15 @@ __global__ void __launch_bounds__(256) k_cg_diag(Geo G, BC bc, CGConst K, const 
     const long long c = G.idx(i, j, k);
     const PlusFaces P = plus_faces(G, bc, i, j, k, c, sx, sy, sz);
     const double dv = P.xp + sx[c] + P.yp + sy[c] + P.zp + sz[c];
-    const double q = (FIDX(u, i, j, k) - FIDX(u, i + 1, j, k)) / K.dx + (FIDX(v, i, j, k) - FIDX(v, i, j + 1, k)) / K.dy +
-                     (FIDX(w, i, j, k) - FIDX(w, i, j, k + 1)) / K.dz;
+    const double q = (FIDX(u, i, j, k) - FIDX(u, i + 1, j, k)) * K.rdx + (FIDX(v, i, j, k) - FIDX(v, i, j + 1, k)) * K.rdy +
+                     (FIDX(w, i, j, k) - FIDX(w, i, j, k + 1)) * K.rdz;
     const double sd = sqrt(dv);
+    const double isd = 1.0 / sd;
     d[c] = dv;
     e[c] = prd1[c] * sd;
-    b[c] = q / sd;
+    b[c] = q * isd;
     sdo[c] = sd;
-    isdo[c] = 1.0 / sd;
+    isdo[c] = isd;
 }
 
 // scaled face coefficients s/sqrt(d_c d_nb) = s * (1/sqrt(d_c)) * (1/sqrt(d_nb)) and the first
@@ -1357,11 +1359,11 @@ __global__ void __launch_bounds__(256) k_posdin(Geo G, BC bc, double aux1, doubl
 
 // A thread walks kEstChunks chunks of kEstZ cells of a column.  Each chunk's loop is unrolled and
 // loads from clamped plane indices, so its loads are issued together; planes past nz are left
-// out of the maximum.  The w face above a cell is the face below the next one.  The chunks keep
-// the grid at about a thousand blocks: the grid reduction's single counter takes the blocks'
-// partials in turn, which at one cell a thread (or four) was the kernel's tail.
+// out of the maximum.  The w face above a cell is the face below the next one.  The differences
+// are multiplied by the cell sizes' reciprocals, formed on the host (as in every FP64 kernel
+// here, a division by a constant is one reciprocal and multiplications).
 constexpr int kEstZ = 4, kEstChunks = 4;
-__global__ void __launch_bounds__(256) k_est(Geo G, double dx, double dy, double dz, const double* __restrict__ u,
+__global__ void __launch_bounds__(256) k_est(Geo G, double rdx, double rdy, double rdz, const double* __restrict__ u,
                                              const double* __restrict__ v, const double* __restrict__ w,
                                              double* partial, unsigned int* counter, double* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -1376,8 +1378,8 @@ __global__ void __launch_bounds__(256) k_est(Geo G, double dx, double dy, double
 #pragma unroll
             for (int q = 0; q < kEstZ; ++q) {
                 const int k = min(k0 + q, G.nz);
-                const double dv = (FIDX(u, i + 1, j, k) - FIDX(u, i, j, k)) / dx + (FIDX(v, i, j + 1, k) - FIDX(v, i, j, k)) / dy +
-                                  (wz[q + 1] - wz[q]) / dz;
+                const double dv = (FIDX(u, i + 1, j, k) - FIDX(u, i, j, k)) * rdx + (FIDX(v, i, j + 1, k) - FIDX(v, i, j, k)) * rdy +
+                                  (wz[q + 1] - wz[q]) * rdz;
                 if (k0 + q <= G.nz) m = isnan(dv) ? INFINITY : fmax(m, fabs(dv));
             }
         }
@@ -1620,6 +1622,7 @@ static CGConst cg_const(const suli_ctx* c) {
     K.cy = c->dt / (c->P.dy * c->P.dy);
     K.cz = c->dt / (c->P.dz * c->P.dz);
     K.dx = c->P.dx; K.dy = c->P.dy; K.dz = c->P.dz;
+    K.rdx = 1. / K.dx; K.rdy = 1. / K.dy; K.rdz = 1. / K.dz;
     K.tol = c->P.cg_tol;
     K.div_tol = c->P.div_tol;
     K.ncell = (double)(c->P.nx * c->P.ny * c->P.nz);
@@ -1685,8 +1688,9 @@ void launch_posdin(suli_ctx* c) {
 void launch_est(suli_ctx* c) {
     const Geo& G = c->g;
     ProfScope ps(c, SULI_K_EST, 1);
-    k_est<<<grid3(G.nx, G.ny, (G.nz + kEstZ * kEstChunks - 1) / (kEstZ * kEstChunks), kBlk), kBlk, 0, c->stream>>>(G, c->P.dx, c->P.dy, c->P.dz, c->f[SULI_F_U], c->f[SULI_F_V],
-                                                  c->f[SULI_F_W], c->red_partial, c->red_counter, c->red_out);
+    k_est<<<grid3(G.nx, G.ny, (G.nz + kEstZ * kEstChunks - 1) / (kEstZ * kEstChunks), kBlk), kBlk, 0, c->stream>>>(G, 1. / c->P.dx, 1. / c->P.dy, 1. / c->P.dz, c->f[SULI_F_U],
+                                                  c->f[SULI_F_V], c->f[SULI_F_W], c->red_partial, c->red_counter,
+                                                  c->red_out);
 }
 void launch_fill(suli_ctx* c, double* a, double v) {
     const long long n = (long long)c->g.n;

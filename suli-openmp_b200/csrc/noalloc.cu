@@ -40,7 +40,7 @@ __device__ double warp_max(double v) {
 // u(0:nx+2,0:ny+1,0:nz+1), v(0:nx+1,0:ny+2,0:nz+1), w(0:nx+1,0:ny+1,0:nz+2).
 __global__ void __launch_bounds__(kTX * kTY) k_est_static(const double* __restrict__ u, const double* __restrict__ v,
                                                           const double* __restrict__ w, int nx, int ny, int nz,
-                                                          double dx, double dy, double dz, double* scratch,
+                                                          double rdx, double rdy, double rdz, double* scratch,
                                                           double* out) {
     __shared__ double sh[kTX * kTY / 32];
     __shared__ bool last;
@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(kTX * kTY) k_est_static(const double* __restri
             const long long cu = i + su * j + pu * k;
             const long long cv = i + sv * j + pv * k;
             const long long cw = i + sw * j + pw * k;
-            const double dv = (u[cu + 1] - u[cu]) / dx + (v[cv + sv] - v[cv]) / dy + (w[cw + pw] - w[cw]) / dz;
+            const double dv = (u[cu + 1] - u[cu]) * rdx + (v[cv + sv] - v[cv]) * rdy + (w[cw + pw] - w[cw]) * rdz;
             m = isnan(dv) ? INFINITY : fmax(m, fabs(dv));
         }
     }
@@ -113,7 +113,8 @@ extern "C" int suli_est_static(const double* u, const double* v, const double* w
     double* scratch = static_cast<double*>(g_scratch_addr[dev]);
     // the counter must start at zero even if an earlier call was interrupted
     if (cudaMemsetAsync(scratch, 0, sizeof(unsigned int), s) != cudaSuccess) return SULI_ERR_CUDA;
-    k_est_static<<<dim3((unsigned)gx, (unsigned)gy, (unsigned)gz), dim3(kTX, kTY), 0, s>>>(u, v, w, nx, ny, nz, dx, dy,
-                                                                                           dz, scratch, max_div);
+    // the cell sizes' reciprocals, as k_est multiplies by them
+    k_est_static<<<dim3((unsigned)gx, (unsigned)gy, (unsigned)gz), dim3(kTX, kTY), 0, s>>>(
+        u, v, w, nx, ny, nz, 1. / dx, 1. / dy, 1. / dz, scratch, max_div);
     return (cudaGetLastError() == cudaSuccess) ? SULI_OK : SULI_ERR_CUDA;
 }
