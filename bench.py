@@ -567,7 +567,8 @@ def headline_rooflines(pkg, p, head, peaks):
         fl = unet_flops(pkg, p)
         pk = measured_tensor_peak()
         out["unet_forward"] = {
-            "kernel": "U-Net forward (k_pack_input + 14 x k_conv3_tp: TMA + tcgen05 pipeline, pooling and head in the epilogues)",
+            "kernel": "U-Net forward with its input features and guess (k_nn_stats, k_nn_features16, 14 x k_conv3_tp: "
+                      "TMA + tcgen05 pipeline with pooling and head in the epilogues, k_nn_dots, k_nn_apply)",
             "bound": "tensor", "achieved": fl / t / 1e12, "peak": pk, "unit": "TFLOP/s", "frac": fl / t / 1e12 / pk,
             "peak_source": "measured bf16_tflops_sustained (MEASURED_PEAKS.json)",
             "algorithmic_flops": fl, "ms": t * 1e3,
