@@ -135,7 +135,8 @@ struct suli_ctx {
     suli::PCGState* pcg = nullptr;
     suli::PCGState* pcg_host = nullptr;
     float* f32_arena = nullptr;
-    int coarse_sweeps = 40;
+    int coarse_sweeps = 20;     // steps of the coarsest solve
+    float coarse_lo = 0.02f;    // > 0: the coarsest solve is a Chebyshev polynomial over [coarse_lo, 2]
     bool cluster_ok = false;    // the device runs k_mg_cluster (16-CTA cluster with its shared memory)
     bool fuse_update = false;   // the inner PCG update runs inside the level-0 pre-smoothing kernel
     bool tail_ok = false;       // the device runs k_mg_tail (one CTA, the last two levels)

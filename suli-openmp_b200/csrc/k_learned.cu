@@ -25,17 +25,32 @@ __device__ __forceinline__ long long cell_v(const Geo& G, int i, int j, int k) {
     return (long long)(i - 1) + (long long)G.nx * ((j - 1) + (long long)G.ny * (k - 1));
 }
 
+// The reductions over the cells give a thread kColChunks chunks of kColZ cells of one column:
+// each chunk's loads come from clamped plane indices and are issued together, and the grid has
+// 16x fewer blocks than one cell a thread (whose launch, block reduction and counter update were
+// most of those kernels' time).  Planes past nz are left out of the sums.
+constexpr int kColZ = 4, kColChunks = 4;
+
 // s = sqrt(rr/n) from graddin's set-up reduction; mean and rms deviation of e0
 __global__ void __launch_bounds__(256) k_nn_stats(Geo G, const double* __restrict__ e, const CGState* cg,
                                                   NNScale* sc, double* partial, unsigned int* counter) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k = blockIdx.z + 1;
     double s1 = 0., s2 = 0.;
-    if (i <= G.nx && j <= G.ny && k <= G.nz) {
-        const double v = e[G.idx(i, j, k)];
-        s1 = v;
-        s2 = v * v;
+    if (i <= G.nx && j <= G.ny) {
+        for (int ch = 0; ch < kColChunks; ++ch) {
+            const int k0 = (blockIdx.z * kColChunks + ch) * kColZ + 1;
+            if (k0 > G.nz) break;
+            double v[kColZ];
+#pragma unroll
+            for (int q = 0; q < kColZ; ++q) v[q] = e[G.idx(i, j, min(k0 + q, G.nz))];
+#pragma unroll
+            for (int q = 0; q < kColZ; ++q)
+                if (k0 + q <= G.nz) {
+                    s1 += v[q];
+                    s2 += v[q] * v[q];
+                }
+        }
     }
     double t1, t2;
     if (reduce2_last(s1, s2, partial, counter, t1, t2) && flat_tid() == 0) {
@@ -98,26 +113,53 @@ __global__ void __launch_bounds__(256) k_nn_features16(Geo G, const double* __re
 }
 
 // r.y and y.A~y with A~ the set-up's scaled operator (ghost rules as the refinement residual);
-// y is the network output, read in place at the ghost-mapped neighbours
+// y is the network output, read in place at the ghost-mapped neighbours.  A thread walks a
+// column (kColChunks chunks of kColZ cells): the x and y neighbours are mapped once, and y
+// below and at a cell are the values at and above the cell before it.
 __global__ void __launch_bounds__(256) k_nn_dots(Geo G, BC bc, const float* __restrict__ out,
                                                  const double* __restrict__ r, const double* __restrict__ ax,
                                                  const double* __restrict__ ay, const double* __restrict__ az,
                                                  NNScale* sc, double* partial, unsigned int* counter) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k = blockIdx.z + 1;
+    const int kb = blockIdx.z * kColChunks * kColZ + 1;
     double ry = 0., yay = 0.;
-    if (i <= G.nx && j <= G.ny && k <= G.nz) {
-        const int c = (int)G.idx(i, j, k);
-        auto y = [&](int ii, int jj, int kk) {
-            return (double)out[cell_v(G, map_any(ii, G.nx, bc.perx), map_any(jj, G.ny, bc.pery),
-                                      map_any(kk, G.nz, bc.perz))];
-        };
-        const double yc = y(i, j, k);
-        const double ayv = yc - ax[c + 1] * y(i + 1, j, k) - ax[c] * y(i - 1, j, k) - ay[c + G.px] * y(i, j + 1, k) -
-                           ay[c] * y(i, j - 1, k) - az[c + (int)G.pxy] * y(i, j, k + 1) - az[c] * y(i, j, k - 1);
-        ry = r[c] * yc;
-        yay = yc * ayv;
+    if (i <= G.nx && j <= G.ny && kb <= G.nz) {
+        const long long nxy = (long long)G.nx * G.ny;
+        const long long v0 = cell_v(G, i, j, 1);
+        const int dxm = map_any(i - 1, G.nx, bc.perx) - i, dxp = map_any(i + 1, G.nx, bc.perx) - i;
+        const int dym = (map_any(j - 1, G.ny, bc.pery) - j) * G.nx, dyp = (map_any(j + 1, G.ny, bc.pery) - j) * G.nx;
+        auto yz = [&](int kk) { return out[v0 + nxy * (map_any(kk, G.nz, bc.perz) - 1)]; };
+        const int px = G.px, pxy = (int)G.pxy;
+        float ym = yz(kb - 1), yc = yz(kb);
+        for (int ch = 0; ch < kColChunks; ++ch) {
+            const int k0 = kb + ch * kColZ;
+            if (k0 > G.nz) break;
+            float yxm[kColZ], yxp[kColZ], yym[kColZ], yyp[kColZ], yzp[kColZ];
+            double rc[kColZ], axc[kColZ], axp[kColZ], ayc[kColZ], ayp[kColZ], azc[kColZ], azp[kColZ];
+#pragma unroll
+            for (int q = 0; q < kColZ; ++q) {
+                const int k = min(k0 + q, G.nz);
+                const long long v = v0 + nxy * (k - 1);
+                const int c = G.idx32(i, j, k);
+                yxm[q] = out[v + dxm]; yxp[q] = out[v + dxp]; yym[q] = out[v + dym]; yyp[q] = out[v + dyp];
+                yzp[q] = yz(k + 1);
+                rc[q] = r[c]; axc[q] = ax[c]; axp[q] = ax[c + 1]; ayc[q] = ay[c]; ayp[q] = ay[c + px];
+                azc[q] = az[c]; azp[q] = az[c + pxy];
+            }
+#pragma unroll
+            for (int q = 0; q < kColZ; ++q) {
+                if (k0 + q > G.nz) break;
+                const double ycd = yc;
+                const double ayv = ycd - axp[q] * (double)yxp[q] - axc[q] * (double)yxm[q] -
+                                   ayp[q] * (double)yyp[q] - ayc[q] * (double)yym[q] -
+                                   azp[q] * (double)yzp[q] - azc[q] * (double)ym;
+                ry += rc[q] * ycd;
+                yay += ycd * ayv;
+                ym = yc;
+                yc = yzp[q];
+            }
+        }
     }
     double t1, t2;
     if (reduce2_last(ry, yay, partial, counter, t1, t2) && flat_tid() == 0) {
@@ -169,11 +211,15 @@ __global__ void __launch_bounds__(256) k_nn_target(Geo G, const double* __restri
 
 const dim3 kBL(32, 8, 1);
 inline dim3 grid_cells(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
+// the column reductions (k_nn_stats, k_nn_dots)
+inline dim3 grid_cols(const Geo& g) {
+    return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kColChunks * kColZ - 1) / (kColChunks * kColZ));
+}
 }  // namespace
 
 void launch_nn_features(suli_ctx* c, float* in3) {
     const Geo& G = c->g;
-    k_nn_stats<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_e, c->cg, c->nn_scale, c->red_partial, c->red_counter);
+    k_nn_stats<<<grid_cols(G), kBL, 0, c->stream>>>(G, c->cg_e, c->cg, c->nn_scale, c->red_partial, c->red_counter);
     k_nn_features<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->cg_r, c->cg_e, c->f[SULI_F_HS], c->nn_scale, in3);
 }
 
@@ -182,14 +228,14 @@ void launch_nn_features16(suli_ctx* c, void* in16) { launch_nn_features16_at(c, 
 // the features of the FP64 scaled residual r and iterate e (the refinement's current ones)
 void launch_nn_features16_at(suli_ctx* c, void* in16, const double* r, const double* e) {
     const Geo& G = c->g;
-    k_nn_stats<<<grid_cells(G), kBL, 0, c->stream>>>(G, e, c->cg, c->nn_scale, c->red_partial, c->red_counter);
+    k_nn_stats<<<grid_cols(G), kBL, 0, c->stream>>>(G, e, c->cg, c->nn_scale, c->red_partial, c->red_counter);
     k_nn_features16<<<grid_cells(G), kBL, 0, c->stream>>>(G, r, e, c->f[SULI_F_HS], c->nn_scale,
                                                            static_cast<__nv_bfloat16*>(in16));
 }
 
 void launch_nn_step(suli_ctx* c, const float* out, double* e) {
     const Geo& G = c->g;
-    k_nn_dots<<<grid_cells(G), kBL, 0, c->stream>>>(G, c->bc, out, c->cg_r, c->cg_ax, c->cg_ay, c->cg_az, c->nn_scale,
+    k_nn_dots<<<grid_cols(G), kBL, 0, c->stream>>>(G, c->bc, out, c->cg_r, c->cg_ax, c->cg_ay, c->cg_az, c->nn_scale,
                                                       c->red_partial, c->red_counter);
     k_nn_apply<<<grid_cells(G), kBL, 0, c->stream>>>(G, out, c->nn_scale, e);
 }

@@ -45,6 +45,7 @@ struct ClArgs {
     float omega, alpha;
     float omega2;      // weight of the second pre-smoothing sweep, of the first post-smoothing one
     int sweeps;        // Jacobi sweeps of the coarsest solve
+    float lo;          // > 0: the coarsest solve is k_mg_coarsest's Chebyshev polynomial
 };
 
 // one level's slab in shared memory: pl planes of nx x ny cells, faces of those cells (x faces
@@ -214,7 +215,8 @@ __global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(ClArgs A, const PC
         }
     }
     cl.sync();
-    // ---- coarsest level B in CTA 0: damped Jacobi sweeps from x1 = w f/dg (k_mg_coarsest)
+    // ---- coarsest level B in CTA 0: damped Jacobi sweeps from x1 = w f/dg, or the Chebyshev
+    //      polynomial (k_mg_coarsest)
     if (rank == 0) {
         float fv = 0.f, idgv = 1.f, s6[6] = {0, 0, 0, 0, 0, 0};
         int nb[6] = {0, 0, 0, 0, 0, 0};
@@ -232,18 +234,31 @@ __global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(ClArgs A, const PC
             auto lin = [&](int a, int b, int d) { return (a - 1) + GB.nx * ((b - 1) + GB.ny * (d - 1)); };
             nb[0] = lin(im, j, k); nb[1] = lin(ip, j, k); nb[2] = lin(i, jm, k);
             nb[3] = lin(i, jp, k); nb[4] = lin(i, j, km); nb[5] = lin(i, j, kp);
-            xb0[t] = om * fv * idgv;
+        }
+        const bool cheb = A.lo > 0.f;
+        CoarseCheb P(cheb ? A.lo : 0.5f);
+        float dv = 0.f;
+        if (t < nB) {
+            dv = cheb ? P.g0() * fv * idgv : 0.f;
+            xb0[t] = cheb ? dv : om * fv * idgv;
         }
         __syncthreads();
         float* cur = xb0;
         float* nxt = xb1;
         for (int sw = 1; sw < A.sweeps; ++sw) {
+            float h = 0.f, g = 0.f;
+            if (cheb) P.next(h, g);
             if (t < nB) {
                 const float xc = cur[t];
                 float ax = 0.f;
 #pragma unroll
                 for (int m = 0; m < 6; ++m) ax += s6[m] * (xc - cur[nb[m]]);
-                nxt[t] = xc + om * (fv - ax) * idgv;
+                if (cheb) {
+                    dv = h * dv + g * (fv - ax) * idgv;
+                    nxt[t] = xc + dv;
+                } else {
+                    nxt[t] = xc + om * (fv - ax) * idgv;
+                }
             }
             __syncthreads();
             float* tmp = cur; cur = nxt; nxt = tmp;

@@ -27,6 +27,7 @@ struct TailArgs {
     float* ym;                  // M's result (the level above's coarse correction)
     float omega, omega2, alpha;
     int sweeps;
+    float lo;                   // > 0: the coarsest solve is k_mg_coarsest's Chebyshev polynomial
 };
 
 // neighbour cell numbers (0-based, x fastest) of cell (i, j, k) under the unknowns' map
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailArgs a, BC bc, con
         fb[p] = 0.125f * s;
     }
     __syncthreads();
-    // coarsest: Jacobi sweeps from x = w f/dg (k_mg_coarsest)
+    // coarsest: Jacobi sweeps from x = w f/dg or the Chebyshev polynomial (k_mg_coarsest)
     int cb = 0, nbb[6] = {0, 0, 0, 0, 0, 0};
     float fv = 0.f, idv = 1.f;
     Faces FB{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -108,11 +109,19 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailArgs a, BC bc, con
         idv = a.ab.inv_diag(cb);
         FB = a.ab.cell(B, i, j, k, cb);
         tail_nb(B, bc, i, j, k, nbb);
-        xb[0][t] = a.omega * fv * idv;
+    }
+    const bool cheb = a.lo > 0.f;
+    CoarseCheb P(cheb ? a.lo : 0.5f);
+    float dv = 0.f;
+    if (t < nbc) {
+        dv = cheb ? P.g0() * fv * idv : 0.f;
+        xb[0][t] = cheb ? dv : a.omega * fv * idv;
     }
     __syncthreads();
     int cur = 0;
     for (int sw = 1; sw < a.sweeps; ++sw) {
+        float h = 0.f, g = 0.f;
+        if (cheb) P.next(h, g);
         if (t < nbc) {
             const float xc = xb[cur][t];
             float ax = 0.f;
@@ -122,7 +131,12 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailArgs a, BC bc, con
             ax += FB.yp * (xc - xb[cur][nbb[3]]);
             ax += FB.zm * (xc - xb[cur][nbb[4]]);
             ax += FB.zp * (xc - xb[cur][nbb[5]]);
-            xb[cur ^ 1][t] = xc + a.omega * (fv - ax) * idv;
+            if (cheb) {
+                dv = h * dv + g * (fv - ax) * idv;
+                xb[cur ^ 1][t] = xc + dv;
+            } else {
+                xb[cur ^ 1][t] = xc + a.omega * (fv - ax) * idv;
+            }
         }
         __syncthreads();
         cur ^= 1;

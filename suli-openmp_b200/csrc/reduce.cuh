@@ -121,11 +121,25 @@ static __device__ bool reduce3_last(double a, double b, double m, double* partia
     __syncthreads();
     if (!last) return false;
     __threadfence();
+    // partials tid, tid + nt, ... in that order, eight triples loaded ahead of the folds
+    constexpr int U = 8;
     double sa = 0.0, sb = 0.0, sm = 0.0;
-    for (int q = tid; q < nb; q += nt) {
-        sa += __ldcg(&partial[3 * q]);
-        sb += __ldcg(&partial[3 * q + 1]);
-        sm = fmax(sm, __ldcg(&partial[3 * q + 2]));
+    for (int q0 = tid; q0 < nb; q0 += U * nt) {
+        double pa[U], pb[U], pm[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int q = q0 + u * nt;
+            pa[u] = (q < nb) ? __ldcg(&partial[3 * q]) : 0.0;
+            pb[u] = (q < nb) ? __ldcg(&partial[3 * q + 1]) : 0.0;
+            pm[u] = (q < nb) ? __ldcg(&partial[3 * q + 2]) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (q0 + u * nt >= nb) break;
+            sa += pa[u];
+            sb += pb[u];
+            sm = fmax(sm, pm[u]);
+        }
     }
     sa = block_sum(sa);
     sb = block_sum(sb);

@@ -196,6 +196,30 @@ def test_tail_kernel_matches_per_level_kernels(pkg, monkeypatch, case):
         assert float(np.abs(v1[f] - v0[f]).max()) <= 1e-9 * vs, f
 
 
+def test_chebyshev_coarsest_solve(pkg, monkeypatch):
+    """The coarsest solve as the Chebyshev polynomial over [lo, 2] of the Jacobi-scaled operator
+    (SULI_COARSE_CHEB=lo) against the damped Jacobi sweeps (SULI_COARSE_CHEB=0): another fixed
+    symmetric positive preconditioner, so PCG still converges to the same FP64 tolerance; dam
+    break 128x64x64 (levels down to 16x8x8), two steps: no more iterations than the Jacobi
+    sweeps, velocities within 1e-7 of their scale (both solves stop at relative residual 1e-10)."""
+    res = {}
+    for lo in ("0", "0.02"):
+        monkeypatch.setenv("SULI_COARSE_CHEB", lo)
+        p, init = pkg.cases.dam_break(nx=128, ny=64, nz=64, dx=0.005, cg_tol=1e-10)
+        p.precision, p.inner_tol, p.refine_maxit = 1, 1e-4, 30
+        s = pkg.Solver(p)
+        init(s)
+        steps = [s.step(it) for it in (1, 2)]
+        assert all(st["status"] == 0 for st in steps)
+        res[lo] = (sum(sum(st["cg_iters"]) for st in steps), {f: s.download(f) for f in ("u", "v", "w")})
+        s.close()
+    (ic, vc), (ij, vj) = res["0.02"], res["0"]
+    assert ic <= ij, (ic, ij)
+    vs = max(float(np.abs(b).max()) for b in vj.values())
+    for f in vj:
+        assert float(np.abs(vc[f] - vj[f]).max()) <= 1e-7 * vs, f
+
+
 def test_fused_update_matches_separate_update(pkg, monkeypatch):
     """The inner PCG update inside the level-0 pre-smoothing kernel (SULI_FUSED_UPDATE=1)
     against the separate update kernel (default): the same residual values, r.r summed in
