@@ -139,6 +139,7 @@ struct suli_ctx {
     float coarse_lo = 0.02f;    // > 0: the coarsest solve is a Chebyshev polynomial over [coarse_lo, 2]
     bool cluster_ok = false;    // the device runs k_mg_cluster (16-CTA cluster with its shared memory)
     bool fuse_update = false;   // the inner PCG update runs inside the level-0 pre-smoothing kernel
+    bool mg_fused = false;      // the coarse levels run one kernel a V-cycle leg (k_mg_fused.cuh)
     bool tail_ok = false;       // the device runs k_mg_tail (one CTA, the last two levels)
     int mg_kz = 2;              // cells along z a thread of the vectorised multigrid kernels owns (2 or 4)
     // level-0 kernels that stream z-planes through shared memory with TMA (k_mg_stream.cuh):

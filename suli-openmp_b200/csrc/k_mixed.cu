@@ -681,6 +681,7 @@ __global__ void k_zero_f(float* a, long long n) {
 
 }  // namespace suli
 #include "k_mg_vec.cuh"
+#include "k_mg_fused.cuh"
 #include "k_mg_cluster.cuh"
 #include "k_mg_stream.cuh"
 #include "k_mg_tail.cuh"
@@ -747,6 +748,11 @@ static inline OpRho4 from_rho4(const MGLevel& L) { return OpRho4{L.rho, L.idg, L
 static inline OpStored4 stored4(const MGLevel& L) { return OpStored4{L.sx, L.sy, L.sz, L.idg}; }
 // the 4-cells-a-thread kernels on a level (mg_kernels 0 or 2 and x divisible by 4)
 static inline bool vec_level(const suli_ctx* c, const Geo& g) { return c->P.mg_kernels != 1 && g.nx % kVX == 0; }
+// the coarse levels 1 .. L-2 run each leg of the V-cycle as one kernel (k_mg_fused.cuh)
+static inline bool fused_level(const suli_ctx* c, int l) { return c->mg_fused && l >= 1 && l <= (int)c->mg.size() - 2; }
+// where level l leaves its V-cycle result (the coarse correction the level above prolongs):
+// the fused up leg writes x, every other path y
+static inline const float* mg_corr(const suli_ctx* c, int l) { return fused_level(c, l) ? c->mg[l].x : c->mg[l].y; }
 
 // ---- level-0 kernels streaming z-planes through shared memory (k_mg_stream.cuh)
 static PFN_cuTensorMapEncodeTiled_v12000 plane_map_encoder() {
@@ -847,7 +853,7 @@ int stream_ready(suli_ctx* c) {
         return SULI_OK;
     }
     // the post-smoothing also needs the level-1 correction's rows to hold its tile's parents
-    c->stream_post_ok = (g.nx % 32 == 0) && c->mg[1].g.px >= c->mg[1].g.nx + 16 && set_coarse_map(c, c->mg[1].y);
+    c->stream_post_ok = (g.nx % 32 == 0) && c->mg[1].g.px >= c->mg[1].g.nx + 16 && set_coarse_map(c, mg_corr(c, 1));
     // planes a CTA computes: as many chunks as fill the SMs' CTA slots once
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
@@ -924,6 +930,11 @@ static void vc_down(suli_ctx* c, int l, const float* f, float om, float om2, boo
     MGLevel& M = c->mg[l];
     MGLevel& C = c->mg[l + 1];
     const BC bc = c->bc;
+    if (fused_level(c, l)) {
+        pdl_launch(k_mgf_down, fgrid(M.g), dim3(kFTX, kFTY, 1), c->stream, M.g, C.g, bc, f, stored(M), M.y, C.f, om,
+                   om2, c->pcg);
+        return;
+    }
     if (vec_level(c, M.g)) {
         if (l == 0) {
             if (!pre_done) {
@@ -958,29 +969,35 @@ static void vc_up(suli_ctx* c, int l, const float* f, float om, float om2, float
     MGLevel& C = c->mg[l + 1];
     const BC bc = c->bc;
     const int dot = (l == 0) ? 1 : 0;
+    const float* xc = mg_corr(c, l + 1);
+    if (fused_level(c, l)) {
+        pdl_launch(k_mgf_up, fgrid(M.g), dim3(kFTX, kFTY, 1), c->stream, M.g, C.g, bc, (const float*)M.y, xc, f,
+                   stored(M), M.x, om, om2, alpha, c->pcg);
+        return;
+    }
     if (vec_level(c, M.g)) {
         if (l == 0) {
             if (c->stream_ok && c->stream_post_ok)
                 launch_stream_post(c, f, om2, alpha);
             else
-                VLAUNCH(k_mgv_post, OpRho4, M.g, M.g, C.g, bc, M.y, C.y, f, from_rho4(M), M.x, om2, alpha, c->pcg);
+                VLAUNCH(k_mgv_post, OpRho4, M.g, M.g, C.g, bc, M.y, xc, f, from_rho4(M), M.x, om2, alpha, c->pcg);
             if (c->stream_ok) launch_stream_jacc(c, f, om);
             else VLAUNCH(k_mgv_jacc, OpRho4, M.g, M.g, bc, M.x, f, from_rho4(M), M.y, om, c->pcg, dot, c->red_partial,
                          c->red_counter);
         } else {
-            VLAUNCH(k_mgv_post, OpStored4, M.g, M.g, C.g, bc, M.y, C.y, f, stored4(M), M.x, om2, alpha, c->pcg);
+            VLAUNCH(k_mgv_post, OpStored4, M.g, M.g, C.g, bc, M.y, xc, f, stored4(M), M.x, om2, alpha, c->pcg);
             VLAUNCH(k_mgv_jacc, OpStored4, M.g, M.g, bc, M.x, f, stored4(M), M.y, om, c->pcg, dot, c->red_partial,
                     c->red_counter);
         }
         return;
     }
     if (l == 0) {
-        pdl_launch(k_mg_post<OpRho>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, C.y, f, from_rho(M), M.x, om2,
+        pdl_launch(k_mg_post<OpRho>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, xc, f, from_rho(M), M.x, om2,
                    alpha, c->pcg);
         pdl_launch(k_mg_jacc<OpRho>, colgrid(M.g), kB2, c->stream, M.g, bc, M.x, f, from_rho(M), M.y, om, c->pcg, dot,
                    c->red_partial, c->red_counter);
     } else {
-        pdl_launch(k_mg_post<OpStored>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, C.y, f, stored(M), M.x, om2,
+        pdl_launch(k_mg_post<OpStored>, colgrid(M.g), kB2, c->stream, M.g, C.g, bc, M.y, xc, f, stored(M), M.x, om2,
                    alpha, c->pcg);
         pdl_launch(k_mg_jacc<OpStored>, colgrid(M.g), kB2, c->stream, M.g, bc, M.x, f, stored(M), M.y, om, c->pcg, dot,
                    c->red_partial, c->red_counter);
@@ -1018,6 +1035,15 @@ int cluster_ready(suli_ctx* c) {
         const int v = std::atoi(ev);
         if (v >= 2 && v <= 400) c->coarse_sweeps = v;
     }
+    // one kernel a leg on the coarse levels (k_mg_fused.cuh, SULI_MG_FUSED=1) with the vectorised
+    // per-level kernels (mg_kernels 0) and no one-CTA tail.  Measured at 256x128x128 it is slower
+    // than the four kernels a level it replaces (228 against 172 us an inner iteration: the cells
+    // around a tile triple the first stage's work), so it is not the default.
+    c->mg_fused = false;
+    if (const char* ev = std::getenv("SULI_MG_FUSED"))
+        if (std::strcmp(ev, "1") == 0) c->mg_fused = (c->P.mg_kernels == 0);
+    if (const char* ev = std::getenv("SULI_TAIL"))
+        if (std::strcmp(ev, "1") == 0) c->mg_fused = false;
     c->fuse_update = false;
     if (const char* ev = std::getenv("SULI_FUSED_UPDATE"))   // the PCG update inside the pre-smoothing
         if (std::strcmp(ev, "1") == 0) c->fuse_update = true;
@@ -1225,7 +1251,10 @@ int vcycle_kernels(const suli_ctx* c) {
     const int L = (int)c->mg.size();
     if (use_cluster(c)) return 4 * (L - 3) + 1;
     if (use_tail(c)) return 4 * (L - 2) + 1;
-    return (L == 1) ? 2 : 4 * (L - 1) + 1;
+    if (L == 1) return 2;
+    int n = 1;
+    for (int l = 0; l < L - 1; ++l) n += fused_level(c, l) ? 2 : 4;
+    return n;
 }
 
 }  // namespace suli

@@ -73,14 +73,16 @@ def test_mixed_steps_track_fp64(pkg, orc):
 
 
 @pytest.mark.parametrize("case", ["dam_break", "periodic"])
-def test_cluster_levels_match_per_level_kernels(pkg, case):
+def test_cluster_levels_match_per_level_kernels(pkg, monkeypatch, case):
     """The three coarsest levels in one 16-CTA cluster launch (mg_kernels = 2) against the same
     levels as kernels per level (mg_kernels = 0): the same stages and per-cell arithmetic (only
     the restriction to the coarsest grid adds its children in two halves), so the inner solves
     follow the same course.  Walls (dam break 128x64x64, cluster levels 64x32x32 .. 16x8x8) and a
     box periodic in every direction (64^3, so the z wrap crosses from the last CTA to the first),
     two steps each: iteration counts within 2 per step, velocities within 1e-9 of their scale, and
-    the tracer shows the cluster path's launch count (7 kernels an inner iteration, not 15)."""
+    the tracer shows the cluster path's launch count (7 kernels an inner iteration, not 15).
+    The per-level side keeps four kernels a coarse level (SULI_MG_FUSED=0)."""
+    monkeypatch.setenv("SULI_MG_FUSED", "0")
     res = {}
     for mk in (0, 2):
         if case == "dam_break":
@@ -193,6 +195,38 @@ def test_tail_kernel_matches_per_level_kernels(pkg, monkeypatch, case):
     assert all(abs(a - b) <= 2 for a, b in zip(i1, i0)), (i1, i0)
     vs = max(float(np.abs(b).max()) for b in v1.values())
     for f in v1:
+        assert float(np.abs(v1[f] - v0[f]).max()) <= 1e-9 * vs, f
+
+
+@pytest.mark.parametrize("case", ["dam_break", "periodic"])
+def test_fused_coarse_legs_match_per_level_kernels(pkg, monkeypatch, case):
+    """Each leg of the V-cycle on the coarse levels as one kernel (k_mgf_down, k_mgf_up;
+    SULI_MG_FUSED=1) against the four per-level kernels (default): the same per-cell
+    expressions, the cells around a tile recomputed under the operator's ghost map.  Walls
+    (dam break 128x64x64) and a box periodic in every direction (64^3, wrapped neighbours around
+    the tiles); two steps: iteration counts within 2, velocities within 1e-9 of their scale."""
+    res = {}
+    for fu in ("0", "1"):
+        monkeypatch.setenv("SULI_MG_FUSED", fu)
+        if case == "dam_break":
+            p, init = pkg.cases.dam_break(nx=128, ny=64, nz=64, dx=0.005, cg_tol=1e-10)
+            p.precision, p.inner_tol, p.refine_maxit = 1, 1e-4, 30
+            s = pkg.Solver(p)
+            init(s)
+            steps = [s.step(it) for it in (1, 2)]
+        else:
+            m = pkg.cases.TaylorGreenMMS(64, precision=1)
+            s = pkg.Solver(m.p)
+            m.init(s)
+            steps = [m.step(s, it) for it in (1, 2)]
+        assert all(st["status"] == 0 for st in steps)
+        iters = [sum(st["cg_iters"]) if isinstance(st["cg_iters"], list) else st["cg_iters"] for st in steps]
+        res[fu] = (iters, {f: s.download(f) for f in ("u", "v", "w")})
+        s.close()
+    (i1, v1), (i0, v0) = res["1"], res["0"]
+    assert all(abs(a - b) <= 2 for a, b in zip(i1, i0)), (i1, i0)
+    vs = max(float(np.abs(b).max()) for b in v0.values())
+    for f in v0:
         assert float(np.abs(v1[f] - v0[f]).max()) <= 1e-9 * vs, f
 
 
