@@ -813,6 +813,10 @@ def run_ours(args):
         cfg["mg_omega"], cfg["mg_alpha"] = args.mg_omega, args.mg_alpha
         cfg["mg_omega2"] = args.mg_omega2 or args.mg_omega
         cfg["mg_kernels"] = args.mg_kernels
+        lo = os.environ.get("SULI_COARSE_CHEB", "0.02")
+        steps = os.environ.get("SULI_COARSE_SWEEPS", "20" if float(lo) > 0 else "40")
+        cfg["coarse_solve"] = (f"Chebyshev over [{lo}, 2] of D^-1 A, {steps} steps" if float(lo) > 0
+                               else f"damped Jacobi, {steps} sweeps")
         if net_src:
             cfg["weights"] = net_src
         arm_acc = {k: {"max_div": max(st["max_div"] for st in r["stats"]),

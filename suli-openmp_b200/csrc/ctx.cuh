@@ -11,6 +11,14 @@
 
 namespace suli {
 
+// the coarsest multigrid solve's Chebyshev coefficients (formed on the host, k_mixed.cu)
+constexpr int kCoarseMaxCheb = 64;   // most Chebyshev steps
+struct CoarsePoly {
+    float lo;                        // > 0: the Chebyshev polynomial over [lo, 2], else damped Jacobi sweeps
+    float g0;
+    float h[kCoarseMaxCheb], g[kCoarseMaxCheb];   // step m = 1 .. steps - 1 at index m - 1
+};
+
 // Device-resident state of the Poisson solve (graddin, 9_grad.f90:10-278).  Written by the
 // last block of each reduction kernel; read by the next kernel and, at poll points, by the
 // host through a pinned mirror.
@@ -137,6 +145,7 @@ struct suli_ctx {
     float* f32_arena = nullptr;
     int coarse_sweeps = 20;     // steps of the coarsest solve
     float coarse_lo = 0.02f;    // > 0: the coarsest solve is a Chebyshev polynomial over [coarse_lo, 2]
+    suli::CoarsePoly coarse_poly = {};
     bool cluster_ok = false;    // the device runs k_mg_cluster (16-CTA cluster with its shared memory)
     bool fuse_update = false;   // the inner PCG update runs inside the level-0 pre-smoothing kernel
     bool mg_fused = false;      // the coarse levels run one kernel a V-cycle leg (k_mg_fused.cuh)

@@ -45,7 +45,7 @@ struct ClArgs {
     float omega, alpha;
     float omega2;      // weight of the second pre-smoothing sweep, of the first post-smoothing one
     int sweeps;        // Jacobi sweeps of the coarsest solve
-    float lo;          // > 0: the coarsest solve is k_mg_coarsest's Chebyshev polynomial
+    CoarsePoly cp;     // the coarsest solve's polynomial (k_mg_coarsest)
 };
 
 // one level's slab in shared memory: pl planes of nx x ny cells, faces of those cells (x faces
@@ -123,7 +123,7 @@ __device__ __forceinline__ float cl_apply(const ClSlab& S, const BC& bc, int nz,
                        val(i, j, kp));
 }
 
-__global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(ClArgs A, const PCGState* st) {
+__global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(const __grid_constant__ ClArgs A, const PCGState* st) {
     pdl_wait();
     if (st->done) return;   // the same value in every CTA of the cluster
     cg::cluster_group cl = cg::this_cluster();
@@ -235,19 +235,17 @@ __global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(ClArgs A, const PC
             nb[0] = lin(im, j, k); nb[1] = lin(ip, j, k); nb[2] = lin(i, jm, k);
             nb[3] = lin(i, jp, k); nb[4] = lin(i, j, km); nb[5] = lin(i, j, kp);
         }
-        const bool cheb = A.lo > 0.f;
-        CoarseCheb P(cheb ? A.lo : 0.5f);
+        const bool cheb = A.cp.lo > 0.f;
         float dv = 0.f;
         if (t < nB) {
-            dv = cheb ? P.g0() * fv * idgv : 0.f;
+            dv = cheb ? A.cp.g0 * fv * idgv : 0.f;
             xb0[t] = cheb ? dv : om * fv * idgv;
         }
         __syncthreads();
         float* cur = xb0;
         float* nxt = xb1;
         for (int sw = 1; sw < A.sweeps; ++sw) {
-            float h = 0.f, g = 0.f;
-            if (cheb) P.next(h, g);
+            const float h = cheb ? A.cp.h[sw - 1] : 0.f, g = cheb ? A.cp.g[sw - 1] : 0.f;
             if (t < nB) {
                 const float xc = cur[t];
                 float ax = 0.f;

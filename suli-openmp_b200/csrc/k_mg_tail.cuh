@@ -27,7 +27,7 @@ struct TailArgs {
     float* ym;                  // M's result (the level above's coarse correction)
     float omega, omega2, alpha;
     int sweeps;
-    float lo;                   // > 0: the coarsest solve is k_mg_coarsest's Chebyshev polynomial
+    CoarsePoly cp;              // the coarsest solve's polynomial (k_mg_coarsest)
 };
 
 // neighbour cell numbers (0-based, x fastest) of cell (i, j, k) under the unknowns' map
@@ -49,7 +49,7 @@ __device__ __forceinline__ float tail_ax(const Faces& F, const float* x, int q, 
     return apply_faces(F, x[q], x[nb[0]], x[nb[1]], x[nb[2]], x[nb[3]], x[nb[4]], x[nb[5]]);
 }
 
-__global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailArgs a, BC bc, const PCGState* st) {
+__global__ void __launch_bounds__(kTailThreads) k_mg_tail(const __grid_constant__ TailArgs a, BC bc, const PCGState* st) {
     pdl_wait();
     if (st->done) return;
     extern __shared__ __align__(16) float t_smem[];
@@ -110,18 +110,16 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailArgs a, BC bc, con
         FB = a.ab.cell(B, i, j, k, cb);
         tail_nb(B, bc, i, j, k, nbb);
     }
-    const bool cheb = a.lo > 0.f;
-    CoarseCheb P(cheb ? a.lo : 0.5f);
+    const bool cheb = a.cp.lo > 0.f;
     float dv = 0.f;
     if (t < nbc) {
-        dv = cheb ? P.g0() * fv * idv : 0.f;
+        dv = cheb ? a.cp.g0 * fv * idv : 0.f;
         xb[0][t] = cheb ? dv : a.omega * fv * idv;
     }
     __syncthreads();
     int cur = 0;
     for (int sw = 1; sw < a.sweeps; ++sw) {
-        float h = 0.f, g = 0.f;
-        if (cheb) P.next(h, g);
+        const float h = cheb ? a.cp.h[sw - 1] : 0.f, g = cheb ? a.cp.g[sw - 1] : 0.f;
         if (t < nbc) {
             const float xc = xb[cur][t];
             float ax = 0.f;

@@ -380,30 +380,31 @@ __global__ void __launch_bounds__(256) k_mg_restrict(Geo Gf, Geo Gc, BC bc, cons
 // rho_m = 1/(2 sigma - rho_{m-1}), h_m = rho_m rho_{m-1}, g_m = 2 rho_m/delta).  The result is
 // q(D^-1 A) D^-1 f with q > 0 on (0, 2], a fixed symmetric positive operator as the damped Jacobi
 // sweeps are, but it reduces every mode of [lo, 2] by the Chebyshev factor, where Jacobi leaves
-// the smooth modes of the coarsest grid almost untouched.  Every thread forms the same
-// coefficients.  lo = 0 keeps the damped Jacobi sweeps.
-struct CoarseCheb {
-    float sigma, delta, rho;
-    __device__ explicit CoarseCheb(float lo) {
-        const float theta = 1.f + 0.5f * lo;
-        delta = 1.f - 0.5f * lo;
-        sigma = theta / delta;
-        rho = delta / theta;
-    }
-    __device__ float g0() const { return rho / delta; }   // 1/theta
-    __device__ void next(float& h, float& g) {
-        const float r = 1.f / (2.f * sigma - rho);
-        h = r * rho;
-        g = 2.f * r / delta;
+// the smooth modes of the coarsest grid almost untouched.  The coefficients depend only on lo and
+// the step count, so the host forms them once (in FP64, rounded to FP32) and the kernels read
+// them from their parameters; lo = 0 keeps the damped Jacobi sweeps.
+// (CoarsePoly is declared with the solver context)
+static CoarsePoly coarse_poly(float lo, int steps) {
+    CoarsePoly P = {};
+    P.lo = lo;
+    if (!(lo > 0.f)) return P;
+    const double theta = 1. + 0.5 * lo, delta = 1. - 0.5 * lo, sigma = theta / delta;
+    double rho = 1. / sigma;
+    P.g0 = (float)(1. / theta);
+    for (int m = 1; m < steps && m <= kCoarseMaxCheb; ++m) {
+        const double r = 1. / (2. * sigma - rho);
+        P.h[m - 1] = (float)(r * rho);
+        P.g[m - 1] = (float)(2. * r / delta);
         rho = r;
     }
-};
+    return P;
+}
 
 // coarsest grid (<= 1024 cells): damped Jacobi sweeps or the Chebyshev polynomial (lo > 0) in
 // shared memory, one block
 __global__ void __launch_bounds__(1024) k_mg_coarsest(Geo G, BC bc, const float* __restrict__ f, OpStored A,
-                                                      float* y, int sweeps, float omega, float lo,
-                                                      const PCGState* st) {
+                                                      float* y, int sweeps, float omega,
+                                                      const __grid_constant__ CoarsePoly cp, const PCGState* st) {
     pdl_wait();
     if (st->done) return;
     __shared__ float xs[2][1024];
@@ -425,17 +426,15 @@ __global__ void __launch_bounds__(1024) k_mg_coarsest(Geo G, BC bc, const float*
         nb[0] = lin(im, j, k); nb[1] = lin(ip, j, k); nb[2] = lin(i, jm, k); nb[3] = lin(i, jp, k); nb[4] = lin(i, j, km); nb[5] = lin(i, j, kp);
     }
     int cur = 0;
-    if (lo > 0.f) {
-        CoarseCheb P(lo);
+    if (cp.lo > 0.f) {
         float d = 0.f;
         if (t < n) {
-            d = P.g0() * fv * idgv;
+            d = cp.g0 * fv * idgv;
             xs[0][t] = d;
         }
         __syncthreads();
         for (int sw = 1; sw < sweeps; ++sw) {
-            float h, g;
-            P.next(h, g);
+            const float h = cp.h[sw - 1], g = cp.g[sw - 1];
             if (t < n) {
                 const float xc = xs[cur][t];
                 float ax = 0.f;
@@ -1035,6 +1034,8 @@ int cluster_ready(suli_ctx* c) {
         const int v = std::atoi(ev);
         if (v >= 2 && v <= 400) c->coarse_sweeps = v;
     }
+    if (c->coarse_lo > 0.f) c->coarse_sweeps = std::min(c->coarse_sweeps, kCoarseMaxCheb + 1);
+    c->coarse_poly = coarse_poly(c->coarse_lo, c->coarse_sweeps);
     // one kernel a leg on the coarse levels (k_mg_fused.cuh, SULI_MG_FUSED=1) with the vectorised
     // per-level kernels (mg_kernels 0) and no one-CTA tail.  Measured at 256x128x128 it is slower
     // than the four kernels a level it replaces (228 against 172 us an inner iteration: the cells
@@ -1091,7 +1092,7 @@ static void launch_cluster(suli_ctx* c, float om, float alpha) {
     a.omega2 = (float)c->P.mg_omega2;
     a.alpha = alpha;
     a.sweeps = c->coarse_sweeps;
-    a.lo = c->coarse_lo;
+    a.cp = c->coarse_poly;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(kClCTAs);
     cfg.blockDim = dim3(kClThreads);
@@ -1147,7 +1148,7 @@ static void launch_tail(suli_ctx* c, float om, float om2, float alpha) {
     a.omega2 = om2;
     a.alpha = alpha;
     a.sweeps = c->coarse_sweeps;
-    a.lo = c->coarse_lo;
+    a.cp = c->coarse_poly;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(1);
     cfg.blockDim = dim3(kTailThreads);
@@ -1185,13 +1186,13 @@ void launch_vcycle(suli_ctx* c, const float* f0, bool pre_done) {
     MGLevel& B = c->mg[L - 1];
     if (L == 1) {   // a single level: coarsest sweeps, then one more sweep that forms r.z
         pdl_launch(k_mg_coarsest, 1, 1024, c->stream, B.g, bc, f0, stored(B), B.x, c->coarse_sweeps, om,
-                   c->coarse_lo, c->pcg);
+                   c->coarse_poly, c->pcg);
         pdl_launch(k_mg_jac, cells3(B.g), kB2, c->stream, B.g, bc, B.x, f0, stored(B), B.y, om, c->pcg, 1,
                    c->red_partial, c->red_counter);
         return;
     }
-    pdl_launch(k_mg_coarsest, 1, 1024, c->stream, B.g, bc, B.f, stored(B), B.y, c->coarse_sweeps, om, c->coarse_lo,
-               c->pcg);
+    pdl_launch(k_mg_coarsest, 1, 1024, c->stream, B.g, bc, B.f, stored(B), B.y, c->coarse_sweeps, om,
+               c->coarse_poly, c->pcg);
     for (int l = L - 2; l >= 0; --l) vc_up(c, l, l == 0 ? f0 : c->mg[l].f, om, om2, alpha);
 }
 
