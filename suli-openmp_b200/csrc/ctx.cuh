@@ -279,7 +279,8 @@ void launch_nn_features16(suli_ctx* c, void* in16);
 void launch_nn_features16_at(suli_ctx* c, void* in16, const double* r, const double* e);
 void launch_nn_step(suli_ctx* c, const float* out, double* e);
 void launch_nn_target(suli_ctx* c, const double* e_star, float* target);
-void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new, const float* r_old, float* r_new);
+void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new, const float* r_old, float* r_new,
+                     bool x_zero = false);
 int pcg_iter_kernels(const suli_ctx* c);
 int vcycle_kernels(const suli_ctx* c);
 void launch_posdin(suli_ctx* c);

@@ -403,11 +403,12 @@ __global__ void __launch_bounds__(256, KZ == 2 ? 4 : 3) k_pcgv_spmvc(Geo G, BC b
     }
 }
 
-// x += alpha p, r -= alpha q, r.r and the inner stop test (k_pcg_updc)
+// x += alpha p (x_zero: x = alpha p, the pass's first update), r -= alpha q, r.r and the inner stop
+// test (k_pcg_updc)
 __global__ void __launch_bounds__(256) k_pcgv_updc(Geo G, float* __restrict__ x, const float* __restrict__ r,
                                                    float* __restrict__ r_out, const float* __restrict__ p,
                                                    const float* __restrict__ qv, PCGState* st, double* partial,
-                                                   unsigned int* counter) {
+                                                   unsigned int* counter, int x_zero) {
     pdl_wait();
     if (st->done) return;
     const float alpha = (float)st->alpha;
@@ -422,7 +423,7 @@ __global__ void __launch_bounds__(256) k_pcgv_updc(Geo G, float* __restrict__ x,
             const int k = k0 + m;
             if (k > G.nz) break;
             const int c = c0 + pxy * k;
-            const V4 xv = ld4(x, c), pv = ld4(p, c), rv = ld4(r, c), qq = ld4(qv, c);
+            const V4 xv = x_zero ? V4{{0.f, 0.f, 0.f, 0.f}} : ld4(x, c), pv = ld4(p, c), rv = ld4(r, c), qq = ld4(qv, c);
             float xo[kVX], ro[kVX];
 #pragma unroll
             for (int e = 0; e < kVX; ++e) {

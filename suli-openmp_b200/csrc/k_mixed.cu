@@ -510,7 +510,7 @@ constexpr int kKZU = 8;
 __global__ void __launch_bounds__(256) k_pcg_updc(Geo G, float* __restrict__ x, const float* __restrict__ r,
                                                   float* __restrict__ r_out, const float* __restrict__ p,
                                                   const float* __restrict__ q, PCGState* st, double* partial,
-                                                  unsigned int* counter) {
+                                                  unsigned int* counter, int x_zero) {
     pdl_wait();
     if (st->done) return;
     const float alpha = (float)st->alpha;
@@ -523,7 +523,7 @@ __global__ void __launch_bounds__(256) k_pcg_updc(Geo G, float* __restrict__ x, 
         const int k1 = min(k0 + kKZU - 1, G.nz);
         for (int k = k0; k <= k1; ++k) {
             const int c = c0 + pxy * k;
-            x[c] = x[c] + alpha * p[c];
+            x[c] = (x_zero ? 0.f : x[c]) + alpha * p[c];
             const float rv = r[c] - alpha * q[c];
             r_out[c] = rv;
             rr += (double)rv * (double)rv;
@@ -594,7 +594,9 @@ __global__ void __launch_bounds__(256) k_mx_outer(Geo G, BC bc, const double* __
 // k_mx_outer with two x cells a thread (16-byte row loads; needs nx even) and kOuterZ planes of
 // their column (loads from clamped planes, so that the planes' loads are issued together; stores
 // and sums only inside the grid): per cell the same expressions, only the two reductions group
-// their terms differently.  A quarter of the blocks of one plane a thread.
+// their terms differently.  A quarter of the blocks of one plane a thread; measured at
+// 256x128x128 one, two (at 64 registers) and four planes a thread run alike (latency-bound, about
+// 80 us a launch).
 constexpr int kOuterZ = 4;
 __global__ void __launch_bounds__(256) k_mx_outer2(Geo G, BC bc, const double* __restrict__ e_in,
                                                    const float* __restrict__ dp, const double* __restrict__ sd,
@@ -730,8 +732,12 @@ void launch_mx_residual(suli_ctx* c, const double* e_in, double* e_out, bool app
 
 void launch_pcg_cond(suli_ctx* c, cudaGraphConditionalHandle h) { pdl_launch(k_pcg_cond, 1, 1, c->stream, h, c->pcg); }
 
+// The pass's first PCG update writes x = alpha p (launch_pcg_iter with x_zero), so x needs no
+// zero fill, except where the update runs inside the pre-smoothing kernel (SULI_FUSED_UPDATE=1).
+static bool fused_update(const suli_ctx* c);
 void launch_pcg_init(suli_ctx* c, int maxit) {
     k_pcg_init<<<1, 1, 0, c->stream>>>(c->pcg, c->P.inner_tol, maxit);
+    if (!fused_update(c)) return;
     const long long n = (long long)c->g.n;
     k_zero_f<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->pc_x, n);
 }
@@ -1204,7 +1210,7 @@ static bool fused_update(const suli_ctx* c) { return c->fuse_update && c->mg.siz
 
 // one inner PCG iteration: p = z + beta p_old, q = A p (p.q -> alpha); x += alpha p,
 // r_new = r_old - alpha q (r.r -> stop test); z = M r_new (r.z -> beta)
-void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new, const float* r_old, float* r_new) {
+void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new, const float* r_old, float* r_new, bool x_zero) {
     const Geo& G = c->g;
     MGLevel& M0 = c->mg[0];
     const bool vec = vec_level(c, G);
@@ -1235,11 +1241,11 @@ void launch_pcg_iter(suli_ctx* c, const float* p_old, float* p_new, const float*
         ProfScope ps(c, SULI_K_CG_UPDATE, 1);
         if (vec) {
             pdl_launch(k_pcgv_updc, vgrid_upd(G), kB2, c->stream, G, c->pc_x, r_old, r_new, p_new, c->pc_q, c->pcg,
-                       c->red_partial, c->red_counter);
+                       c->red_partial, c->red_counter, x_zero ? 1 : 0);
         } else {
             const dim3 gu((G.nx + 31) / 32, (G.ny + 7) / 8, (G.nz + kKZU - 1) / kKZU);
             pdl_launch(k_pcg_updc, gu, kB2, c->stream, G, c->pc_x, r_old, r_new, p_new, c->pc_q, c->pcg,
-                       c->red_partial, c->red_counter);
+                       c->red_partial, c->red_counter, x_zero ? 1 : 0);
         }
     }
     ProfScope ps(c, SULI_K_MG, vcycle_kernels(c));

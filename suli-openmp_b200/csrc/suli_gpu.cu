@@ -857,7 +857,7 @@ int graddin_mixed(suli_ctx* c, int* iters, double* resid) {
             ProfScope ps(c, SULI_K_MG, vcycle_kernels(c));
             launch_vcycle(c, c->pc_r);
         }
-        launch_pcg_iter(c, c->mg[0].y, c->pc_pa, c->pc_r, c->pc_r2);   // p_old = z with beta = 0
+        launch_pcg_iter(c, c->mg[0].y, c->pc_pa, c->pc_r, c->pc_r2, true);   // p_old = z with beta = 0, x = 0
         if (c->use_graphs) {
             ProfScope ps(c, SULI_K_MG, 0);   // kernel launches are counted below, once known
             CUDA_TRY(c, cudaGraphLaunch(c->pcg_loop, c->stream));
