@@ -265,7 +265,7 @@ CLASS_PASSES = {
     "visco": 5,        # nut: u, v, w, rho in, nut out; faces: nut, ls_nu in, xnut..znut out
     "convdiff": 20,    # u, v, w, rho, hsx..z, kurv, nut, xnut..znut in, Fu..Fw out; prd0 = prd1 copy
     "tempo": 15,       # per component: velocity, F in; velocity and two stage stores out
-    "posdin": 8,       # u, v, w, prd1, rho in; u, v, w out
+    "posdin": 10,      # u, v, w, prd1, rho in; u, v, w out; the prd = prd1 copy timed with it
     "est": 3,          # u, v, w in
 }
 
