@@ -12,7 +12,7 @@
 //
 // The stages and the per-cell arithmetic are those of the per-level kernels (k_mgv_pre,
 // k_mgv_restrict, k_mg_coarsest, k_mgv_post, k_mgv_jacc on stored faces): two damped Jacobi
-// sweeps from zero, restriction of (f - A y)/8, the coarsest Jacobi sweeps, prolongation
+// sweeps from zero, restriction of (f - A y)/8, the coarsest solve (k_mg_coarsest), prolongation
 // y + alpha P x_c, then two sweeps.  Only the restriction to B sums its 8 children in two
 // halves (one per CTA holding them) before adding.  The level M's right-hand side comes from,
 // and its result returns to, global memory (mg[b].f, mg[b].y): the finer levels' kernels are
@@ -44,7 +44,7 @@ struct ClArgs {
     float* yM;         // level M's result (read by the prolongation into the level above)
     float omega, alpha;
     float omega2;      // weight of the second pre-smoothing sweep, of the first post-smoothing one
-    int sweeps;        // Jacobi sweeps of the coarsest solve
+    int sweeps;        // steps of the coarsest solve
     CoarsePoly cp;     // the coarsest solve's polynomial (k_mg_coarsest)
 };
 

@@ -2,7 +2,7 @@
 // solve's V-cycle in one CTA (included by k_mixed.cu after the vectorised kernels).
 //
 // At 256x128x128 these are 32x16x16 (8192 cells) and 16x8x8 (1024 cells): five launches of the
-// per-level path (pre-smoothing, restriction, coarsest sweeps, prolongation + post-smoothing,
+// per-level path (pre-smoothing, restriction, coarsest solve, prolongation + post-smoothing,
 // last sweep) with microseconds of work each, bound by launch and memory latency.  Here one CTA
 // of 1024 threads runs them as phases separated by CTA barriers, with the level's smoothing
 // iterates and the coarsest grid in shared memory; the level's faces, inverse diagonal and

@@ -9,9 +9,10 @@
 //
 // Preconditioner: a geometric multigrid V-cycle in FP32 — piecewise-constant prolongation,
 // restriction P^T/8 and Galerkin coarse faces (sum of the four fine faces)/8, two damped
-// Jacobi sweeps before and after, a one-block Jacobi solve on the coarsest grid.  Pre- and
-// post-smoothing mirror each other, so the V-cycle is a symmetric positive operator and plain
-// (not flexible) PCG applies.
+// Jacobi sweeps before and after, a one-block Chebyshev polynomial (or damped Jacobi sweeps) on
+// the coarsest grid.  Pre- and post-smoothing mirror each other and the coarsest solve is a
+// fixed symmetric positive operator, so the V-cycle is one too and plain (not flexible) PCG
+// applies.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
