@@ -10,8 +10,9 @@ initial state; the fields (~2.6 GB) exceed the 126 MB L2, so no flush is needed.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints ONE JSON line (rank 0).  `value` is device-timed (CUDA events on the library's stream,
-max over ranks); `e2e` times the same steps through the C-ABI with the state copied from and
-to pinned host memory every step.  Multi-GPU runs are independent replicas (the path is one
+max over ranks); `e2e` times the same steps through the C-ABI (suli_step_host) with the state
+copied from and to pinned host memory every step, the copies overlapping the step where its
+order allows.  Multi-GPU runs are independent replicas (the path is one
 domain on one GPU), so `value` sums the replicas' time steps over the slowest replica's time.
 The reference arm (--impl reference) times the CPU restatement of the same path (OpenMP, all
 host cores): a bounded number of real, whole steps of the same workload (no iteration cap).
@@ -758,17 +759,14 @@ def run_ours(args):
         s.synchronize()
         dist.barrier()
         t0 = time.perf_counter()
+        state = {nm: pinned[nm][1] for nm in names}
         for _ in range(args.steps):
             it += 1
-            for nm in names:
-                s.upload(nm, pinned[nm][1])
-            s.step(it)
-            for nm in names:
-                s.download(nm, out=pinned[nm][1])
+            s.step_host(it, state, state)   # in from and back to the same pinned arrays
         s.synchronize()
         t_e2e = dist.max(time.perf_counter() - t0)
         e2e = {"value": dist.world * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": h2d, "fields": names, "path": head_key}
+               "d2h_bytes_per_step": h2d, "fields": names, "path": head_key, "api": "suli_step_host"}
     s.close()
     # ---- the long window (C3's 500 steps) of the headline and the plain path
     long = {}

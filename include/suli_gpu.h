@@ -223,6 +223,24 @@ typedef struct suli_step_stats {
 /* One time step it (1_principal.f90:64-108 without MMS/plot/restart), plus est(). */
 int suli_step(suli_ctx* c, int it, suli_step_stats* st);
 
+/* One time step whose state crosses from and back to host memory, for a time loop that keeps
+   the module arrays on the host as the reference's loop does (1_principal.f90:64-108, every
+   subroutine acting on the host arrays of 0_modules.f90).  The same as suli_upload of each
+   in_fields[q] from in_host[q], suli_step, then suli_download of each out_fields[q] into
+   out_host[q], with the same results, but the copies run on two copy streams and overlap the
+   step where its order allows: prd1, which the step first reads in the first RK stage's
+   convdiff (its prd0 = prd1 copy), is copied in while the level-set stage runs, and ls, which
+   nothing after the level-set stage writes (without wave inflow), is copied out while the RK
+   stages run.  Host buffers should be pinned for the overlap (pageable memory works, with the
+   copies serialised).  At most SULI_STEP_HOST_MAX_FIELDS fields each way, no field twice in
+   one list; planes and tf_u/v/w are copied synchronously before or after the step.  The call
+   returns once every copy has landed.  The first call allocates one staging box per copied
+   field and two streams; later calls allocate nothing.
+   No counterpart in the reference (an addition for a host-side driver of this library). */
+#define SULI_STEP_HOST_MAX_FIELDS 8
+int suli_step_host(suli_ctx* c, int it, int n_in, const int* in_fields, const double* const* in_host, int n_out,
+                   const int* out_fields, double* const* out_host, suli_step_stats* st);
+
 /* ---- learned initial guess / preconditioner of the pressure solve ------------------------
    No counterpart in the reference (an addition of this build for the variable-density
    Poisson solve of 9_grad.f90).  A 3-D U-Net (4 levels, 16/32/64/96 channels, 3x3x3

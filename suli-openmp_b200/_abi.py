@@ -225,6 +225,8 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
         "suli_set_obstacle": (C.c_int, [vp, P(C.c_int), P(C.c_int), P(C.c_int)]),
         "suli_boundary_waves": (C.c_int, [vp]),
         "suli_step": (C.c_int, [vp, C.c_int, P(SuliStepStats)]),
+        "suli_step_host": (C.c_int, [vp, C.c_int, C.c_int, P(C.c_int), P(vp), C.c_int, P(C.c_int), P(vp),
+                                     P(SuliStepStats)]),
         "suli_stream": (C.c_int, [vp, P(vp)]),
         "suli_profile_enable": (C.c_int, [vp, C.c_int]),
         "suli_profile_read": (C.c_int, [vp, P(C.c_double), P(C.c_longlong), P(C.c_longlong)]),
@@ -261,13 +263,14 @@ HEADER_SYMBOLS = [
     "suli_set_scalar", "suli_get_scalar", "suli_iniciais", "suli_level_set_ini",
     "suli_level_set", "suli_heaviside", "suli_mod_ls1", "suli_visco", "suli_convdiff",
     "suli_tempo", "suli_contorno", "suli_graddin", "suli_posdin", "suli_est",
-    "suli_set_dt", "suli_set_obstacle", "suli_boundary_waves", "suli_step", "suli_stream", "suli_profile_enable", "suli_profile_read",
+    "suli_set_dt", "suli_set_obstacle", "suli_boundary_waves", "suli_step", "suli_step_host", "suli_stream", "suli_profile_enable", "suli_profile_read",
     "suli_est_static",
     "suli_nn_num_params", "suli_nn_create", "suli_nn_destroy", "suli_nn_last_error",
     "suli_nn_set_params", "suli_nn_get_params", "suli_nn_forward", "suli_nn_loss_grad",
     "suli_nn_train_step", "suli_nn_conv3d", "suli_nn_conv3d_ex", "suli_nn_set_kernel", "suli_attach_nn", "suli_graddin_record",
 ]
 EST_STATIC_MAX_BLOCKS = 8192   # SULI_EST_STATIC_MAX_BLOCKS
+STEP_HOST_MAX_FIELDS = 8       # SULI_STEP_HOST_MAX_FIELDS
 
 # enum suli_kernel: kernel classes of the tracing counters
 KERNEL_NAMES = [

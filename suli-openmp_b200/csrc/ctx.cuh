@@ -183,6 +183,11 @@ struct suli_ctx {
     // device state after each pair, in place of the device-side graph loop; same kernels, same
     // order, same results
     bool use_graphs = true;
+    // suli_step_host (allocated on its first call): one copy stream per direction, and per
+    // copied field a staging box (Fortran layout) and the event that orders its copy
+    cudaStream_t io_in = nullptr, io_out = nullptr;
+    double* io_stage[2 * SULI_STEP_HOST_MAX_FIELDS] = {nullptr};
+    cudaEvent_t io_ev[2 * SULI_STEP_HOST_MAX_FIELDS] = {nullptr};
     // tracing: CUDA-event pairs around each kernel class (suli_profile_*)
     struct Prof {
         bool on = false;

@@ -316,6 +316,12 @@ int suli_destroy(suli_ctx* c) {
     cudaFree(c->nn_out);
     cudaFree(c->nn_e0);
     cudaFree(c->nn_scale);
+    for (int q = 0; q < 2 * SULI_STEP_HOST_MAX_FIELDS; ++q) {
+        cudaFree(c->io_stage[q]);
+        if (c->io_ev[q]) cudaEventDestroy(c->io_ev[q]);
+    }
+    if (c->io_in) cudaStreamDestroy(c->io_in);
+    if (c->io_out) cudaStreamDestroy(c->io_out);
     if (c->pcg_host) cudaFreeHost(c->pcg_host);
     if (c->cg_host) cudaFreeHost(c->cg_host);
     if (c->host_scalars) cudaFreeHost(c->host_scalars);
@@ -1030,16 +1036,60 @@ int suli_profile_read(suli_ctx* c, double ms[SULI_K_COUNT], long long launches[S
 }
 
 // one time step (1_principal.f90:64-108, without MMS/plot/restart), then est()
-int suli_step(suli_ctx* c, int it, suli_step_stats* st) {
-    if (!c) return SULI_ERR_ARG;
+// Copies of suli_step_host that overlap the step: the inputs not yet scattered into their
+// fields (prd1), the outputs already gathered and on their way out (ls).
+struct StepIO {
+    int n_in, n_out;
+    const int* fin;
+    const int* fout;
+    double* const* hout;
+    bool late_in[SULI_STEP_HOST_MAX_FIELDS];    // copied in; scattered before the first convdiff
+    bool early_out[SULI_STEP_HOST_MAX_FIELDS];  // gathered after the level-set stage
+};
+
+static int io_scatter(suli_ctx* c, int slot, int field) {
+    int lo[3], hi[3];
+    extent(&c->P, field, lo, hi);
+    const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
+    const size_t n = (size_t)n0 * n1 * n2;
+    CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->io_ev[slot], 0));
+    k_scatter<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->g, c->io_stage[slot], c->f[field], lo[0], lo[1],
+                                                                   lo[2], n0, n1, n2);
+    CHECK_LAUNCH(c);
+    return SULI_OK;
+}
+
+static int io_send(suli_ctx* c, int slot, int field, double* host) {
+    int lo[3], hi[3];
+    extent(&c->P, field, lo, hi);
+    const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
+    const size_t n = (size_t)n0 * n1 * n2;
+    k_gather<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->g, c->f[field], c->io_stage[slot], lo[0], lo[1],
+                                                                  lo[2], n0, n1, n2);
+    CHECK_LAUNCH(c);
+    CUDA_TRY(c, cudaEventRecord(c->io_ev[slot], c->stream));
+    CUDA_TRY(c, cudaStreamWaitEvent(c->io_out, c->io_ev[slot], 0));
+    CUDA_TRY(c, cudaMemcpyAsync(host, c->io_stage[slot], n * sizeof(double), cudaMemcpyDefault, c->io_out));
+    return SULI_OK;
+}
+
+// The time step (1_principal.f90:64-108); `io` (suli_step_host) places the overlapped copies.
+static int step_body(suli_ctx* c, int it, suli_step_stats* st, const StepIO* io) {
     int status = SULI_OK;
     c->t = it * c->dt;
     int r = suli_level_set(c, nullptr);
     if (r < 0) return r;
     if (c->P.obst_t != 0 && (r = suli_contorno(c, 3)) < 0) return r;   // 1_principal.f90:75
+    if (io)   // ls is final here unless the wave inflow rounds it in every stage
+        for (int q = 0; q < io->n_out; ++q)
+            if (io->early_out[q] && (r = io_send(c, SULI_STEP_HOST_MAX_FIELDS + q, io->fout[q], io->hout[q])) < 0)
+                return r;
     for (int tt = 1; tt <= c->ntt; ++tt) {
         c->dt = c->a_dt[tt - 1];
         if ((r = suli_visco(c)) < 0) return r;
+        if (io && tt == 1)   // convdiff's prd0 = prd1 copy is the step's first read of prd1
+            for (int q = 0; q < io->n_in; ++q)
+                if (io->late_in[q] && (r = io_scatter(c, q, io->fin[q])) < 0) return r;
         if ((r = suli_convdiff(c)) < 0) return r;
         if ((r = suli_tempo(c, tt, it)) < 0) return r;
         if (c->P.wave_t > 0 && (r = suli_boundary_waves(c)) < 0) return r;   // 1_principal.f90:84
@@ -1061,6 +1111,97 @@ int suli_step(suli_ctx* c, int it, suli_step_stats* st) {
         st->max_div = md;
         st->status = status;
     }
+    return status;
+}
+
+int suli_step(suli_ctx* c, int it, suli_step_stats* st) {
+    if (!c) return SULI_ERR_ARG;
+    return step_body(c, it, st, nullptr);
+}
+
+static int io_ready(suli_ctx* c, int slot) {
+    if (!c->io_in) CUDA_TRY(c, cudaStreamCreateWithFlags(&c->io_in, cudaStreamNonBlocking));
+    if (!c->io_out) CUDA_TRY(c, cudaStreamCreateWithFlags(&c->io_out, cudaStreamNonBlocking));
+    if (!c->io_stage[slot]) CUDA_TRY(c, cudaMalloc(&c->io_stage[slot], c->g.n * sizeof(double)));
+    if (!c->io_ev[slot]) CUDA_TRY(c, cudaEventCreateWithFlags(&c->io_ev[slot], cudaEventDisableTiming));
+    return SULI_OK;
+}
+
+// a box field the overlapped copies handle (planes and the forcing arrays go through
+// suli_upload / suli_download, which treat them specially)
+static bool io_box_field(int f) {
+    return f >= 0 && f < SULI_F_COUNT && !is_plane(f) && f != SULI_F_TF_U && f != SULI_F_TF_V && f != SULI_F_TF_W;
+}
+
+int suli_step_host(suli_ctx* c, int it, int n_in, const int* in_fields, const double* const* in_host, int n_out,
+                   const int* out_fields, double* const* out_host, suli_step_stats* st) {
+    if (!c) return SULI_ERR_ARG;
+    if (n_in < 0 || n_in > SULI_STEP_HOST_MAX_FIELDS || n_out < 0 || n_out > SULI_STEP_HOST_MAX_FIELDS ||
+        (n_in > 0 && (!in_fields || !in_host)) || (n_out > 0 && (!out_fields || !out_host)))
+        return fail(c, SULI_ERR_ARG, "step_host: bad field lists");
+    for (int a = 0; a < n_in; ++a) {
+        if (in_fields[a] < 0 || in_fields[a] >= SULI_F_COUNT || !in_host[a])
+            return fail(c, SULI_ERR_ARG, "step_host: bad input field");
+        for (int b = 0; b < a; ++b)
+            if (in_fields[b] == in_fields[a]) return fail(c, SULI_ERR_ARG, "step_host: input field listed twice");
+    }
+    for (int a = 0; a < n_out; ++a) {
+        if (out_fields[a] < 0 || out_fields[a] >= SULI_F_COUNT || !out_host[a])
+            return fail(c, SULI_ERR_ARG, "step_host: bad output field");
+        for (int b = 0; b < a; ++b)
+            if (out_fields[b] == out_fields[a]) return fail(c, SULI_ERR_ARG, "step_host: output field listed twice");
+    }
+    cudaSetDevice(c->device);
+    StepIO io{};
+    io.n_in = n_in; io.n_out = n_out; io.fin = in_fields; io.fout = out_fields; io.hout = out_host;
+    for (int q = 0; q < n_in; ++q)
+        if (io_box_field(in_fields[q]))
+            if (int r = io_ready(c, q)) return r;
+    for (int q = 0; q < n_out; ++q)
+        if (io_box_field(out_fields[q]))
+            if (int r = io_ready(c, SULI_STEP_HOST_MAX_FIELDS + q)) return r;
+    // inputs: the special ones synchronously, the box fields on the copy stream, each scattered
+    // as soon as it lands (prd1 only before the first convdiff)
+    for (int q = 0; q < n_in; ++q)
+        if (!io_box_field(in_fields[q]))
+            if (int r = suli_upload(c, in_fields[q], in_host[q])) return r;
+    int r = SULI_OK;
+    for (int q = 0; q < n_in && r == SULI_OK; ++q) {
+        const int f = in_fields[q];
+        if (!io_box_field(f)) continue;
+        int lo[3], hi[3];
+        extent(&c->P, f, lo, hi);
+        const size_t n = (size_t)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+        cudaError_t e = cudaMemcpyAsync(c->io_stage[q], in_host[q], n * sizeof(double), cudaMemcpyDefault, c->io_in);
+        if (e == cudaSuccess) e = cudaEventRecord(c->io_ev[q], c->io_in);
+        if (e != cudaSuccess) {
+            r = fail(c, SULI_ERR_CUDA, std::string("step_host: copy in: ") + cudaGetErrorString(e));
+            break;
+        }
+        io.late_in[q] = (f == SULI_F_PRD1);
+        if (!io.late_in[q]) r = io_scatter(c, q, f);
+    }
+    for (int q = 0; q < n_out; ++q) io.early_out[q] = (out_fields[q] == SULI_F_LS && c->P.wave_t == 0);
+    if (r == SULI_OK) r = step_body(c, it, st, &io);
+    int status = r;
+    // outputs: each box field gathered into its staging box and copied out while the next one
+    // is gathered
+    if (status >= 0)
+        for (int q = 0; q < n_out; ++q) {
+            if (!io_box_field(out_fields[q]) || io.early_out[q]) continue;
+            if (int rs = io_send(c, SULI_STEP_HOST_MAX_FIELDS + q, out_fields[q], out_host[q])) { status = rs; break; }
+        }
+    // nothing may still read the caller's inputs or write its outputs once the call returns
+    cudaError_t e1 = cudaStreamSynchronize(c->io_in);
+    cudaError_t e2 = cudaStreamSynchronize(c->io_out);
+    cudaError_t e3 = cudaStreamSynchronize(c->stream);
+    if (status >= 0 && (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess))
+        return fail(c, SULI_ERR_CUDA, std::string("step_host: ") +
+                                          cudaGetErrorString(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3)));
+    if (status < 0) return status;
+    for (int q = 0; q < n_out; ++q)
+        if (!io_box_field(out_fields[q]))
+            if (int rd = suli_download(c, out_fields[q], out_host[q])) return rd;
     return status;
 }
 

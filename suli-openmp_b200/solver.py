@@ -226,9 +226,8 @@ class Solver:
     def set_dt(self, dt: float) -> None:
         self._check(self.lib.suli_set_dt(self._h, float(dt)), "set_dt")
 
-    def step(self, it: int) -> dict:
-        st = SuliStepStats()
-        self._check(self.lib.suli_step(self._h, int(it), C.byref(st)), "step")
+    @staticmethod
+    def _stats(st) -> dict:
         return {
             "cg_iters": list(st.cg_iters),
             "cg_resid": list(st.cg_resid),
@@ -236,3 +235,32 @@ class Solver:
             "max_div": st.max_div,
             "status": st.status,
         }
+
+    def step(self, it: int) -> dict:
+        st = SuliStepStats()
+        self._check(self.lib.suli_step(self._h, int(it), C.byref(st)), "step")
+        return self._stats(st)
+
+    def step_host(self, it: int, inputs: dict, outputs: dict) -> dict:
+        """One time step with the state in host arrays (suli_step_host): every array of
+        `inputs` is copied in before the fields it feeds are read, every array of `outputs`
+        receives its field after the step; the copies overlap the step where its order allows.
+        Arrays are float64, Fortran-ordered, of the field's shape (pinned memory, e.g. a
+        numpy view of a pinned torch tensor, lets the copies overlap)."""
+        def lists(d, what):
+            if len(d) > _abi.STEP_HOST_MAX_FIELDS:
+                raise ValueError(f"step_host: at most {_abi.STEP_HOST_MAX_FIELDS} {what} fields")
+            ids, ptrs = [], []
+            for name, a in d.items():
+                if a.shape != self.shape(name) or a.dtype != np.float64 or not a.flags.f_contiguous:
+                    raise ValueError(f"step_host {name}: need float64, Fortran-ordered, {self.shape(name)}")
+                ids.append(FIELD[name])
+                ptrs.append(a.ctypes.data)
+            n = len(ids)
+            return n, (C.c_int * max(n, 1))(*ids), (C.c_void_p * max(n, 1))(*ptrs)
+        n_in, f_in, p_in = lists(inputs, "input")
+        n_out, f_out, p_out = lists(outputs, "output")
+        st = SuliStepStats()
+        self._check(self.lib.suli_step_host(self._h, int(it), n_in, f_in, p_in, n_out, f_out, p_out, C.byref(st)),
+                    "step_host")
+        return self._stats(st)
