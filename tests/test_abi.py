@@ -75,6 +75,15 @@ def test_create_without_gpu_fails_loudly(pkg):
     assert not h.value
 
 
+def test_step_host_without_context_is_refused(pkg):
+    """suli_step_host checks its context before touching a device or a host pointer."""
+    lib = pkg.load_library()
+    ids = (C.c_int * 1)(pkg._abi.FIELD["u"])
+    ptrs = (C.c_void_p * 1)(None)
+    assert lib.suli_step_host(None, 1, 1, ids, ptrs, 1, ids, ptrs, None) == pkg._abi.ERR_ARG
+    assert pkg._abi.STEP_HOST_MAX_FIELDS == 8
+
+
 def test_invalid_parameters_rejected(pkg):
     lib = pkg.load_library()
     h = C.c_void_p()
