@@ -185,7 +185,7 @@ _LIB = None
 
 
 def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
-    """Load libsuli_gpu.so (built in-tree by csrc/build.py).  Fails loudly if absent."""
+    """Load libsuli_gpu.so (built in-tree by csrc/Makefile).  Fails loudly if absent."""
     global _LIB
     if _LIB is not None and path is None:
         return _LIB
@@ -193,7 +193,7 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
     if not lib_path.exists():
         raise RuntimeError(
             f"libsuli_gpu.so not found at {lib_path}; build it with "
-            "`python suli-openmp_b200/csrc/build.py` (there is no CPU fallback)")
+            "`make -C suli-openmp_b200/csrc` (there is no CPU fallback)")
     lib = C.CDLL(str(lib_path))
     P = C.POINTER
     vp = C.c_void_p
