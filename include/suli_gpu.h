@@ -233,8 +233,10 @@ int suli_step(suli_ctx* c, int it, suli_step_stats* st);
    nothing after the level-set stage writes (without wave inflow), is copied out while the RK
    stages run.  Host buffers should be pinned for the overlap (pageable memory works, with the
    copies serialised).  At most SULI_STEP_HOST_MAX_FIELDS fields each way, no field twice in
-   one list; planes and tf_u/v/w are copied synchronously before or after the step.  The call
-   returns once every copy has landed.  The first call allocates one staging box per copied
+   one list; planes and tf_u/v/w are copied synchronously before or after the step.  A field's
+   output may use the same host array as its input; an output array must not overlap the
+   input array of another field.  The call returns once every copy has landed; after an error
+   the fields may hold a partly updated state.  The first call allocates one staging box per copied
    field and two streams; later calls allocate nothing.
    No counterpart in the reference (an addition for a host-side driver of this library). */
 #define SULI_STEP_HOST_MAX_FIELDS 8
