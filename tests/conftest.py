@@ -32,15 +32,19 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); calls libsuli_gpu.so")
 
 
-# Run order: the per-step hot path first, then the reference's optional features (bottom
-# obstacles, wave inflow, restart and field files), and the no-allocation entry point last, so
-# that a run stopping at its first failure (-x) has covered everything before the failing part.
+# Run order: the C++ driver's GPU test first (it starts its own processes on the GPU, so it
+# runs before this process holds a CUDA context, whatever the GPU's compute mode), then the
+# per-step hot path, then the reference's optional features (bottom obstacles, wave inflow,
+# restart and field files), and the no-allocation entry point last, so that a run stopping at
+# its first failure (-x) has covered everything before the failing part.
 OPTIONAL_FEATURE_FILES = ("test_obstacle.py", "test_waves.py", "test_fileio.py")
 
 
 def pytest_collection_modifyitems(session, config, items):
     def rank(item):
         name = pathlib.Path(str(item.fspath)).name
+        if name == "test_driver_gpu.py":
+            return -1
         if name == "test_zz_no_alloc.py":
             return 2
         return 1 if name in OPTIONAL_FEATURE_FILES else 0
