@@ -121,3 +121,25 @@ def test_no_oracle_in_product(pkg):
         assert "oracle" not in text.lower(), path
     lib = pkg.load_library()
     assert not hasattr(lib, "orc_create")
+
+
+def test_step_host_binding_checks_arrays_before_the_call(pkg):
+    """Solver.step_host refuses arrays of the wrong shape, order or type, and more fields than
+    the library takes, before it calls the library (no context or GPU needed to reach them)."""
+    import numpy as np
+    s = object.__new__(pkg.Solver)   # the checks need only the parameters
+    s.params = pkg.default_params()
+    s.params.nx, s.params.ny, s.params.nz = 6, 5, 4
+    s.lib, s._h = None, None
+    good = np.zeros(s.shape("u"), order="F")
+    with pytest.raises(ValueError):
+        s.step_host(1, {"u": np.zeros((3, 3, 3), order="F")}, {})
+    with pytest.raises(ValueError):
+        s.step_host(1, {}, {"u": np.ascontiguousarray(good)})     # C order
+    with pytest.raises(ValueError):
+        s.step_host(1, {"u": good.astype(np.float32)}, {})
+    names = ["u", "v", "w", "prd1", "prd0", "prd", "rho", "ls", "hs"]
+    many = {n: np.zeros(s.shape(n), order="F") for n in names}
+    assert len(many) > pkg._abi.STEP_HOST_MAX_FIELDS
+    with pytest.raises(ValueError):
+        s.step_host(1, many, {})
