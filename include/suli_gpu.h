@@ -237,7 +237,8 @@ int suli_step(suli_ctx* c, int it, suli_step_stats* st);
    output may use the same host array as its input; an output array must not overlap the
    input array of another field.  The call returns once every copy has landed; after an error
    the fields may hold a partly updated state.  The first call allocates one staging box per copied
-   field and two streams; later calls allocate nothing.
+   field and two streams; a later call allocates only for list positions that no earlier call
+   used.
    No counterpart in the reference (an addition for a host-side driver of this library). */
 #define SULI_STEP_HOST_MAX_FIELDS 8
 int suli_step_host(suli_ctx* c, int it, int n_in, const int* in_fields, const double* const* in_host, int n_out,
