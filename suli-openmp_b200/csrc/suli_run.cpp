@@ -15,9 +15,11 @@
 //
 // Usage: suli_run [key=value ...]
 //   case=dam_break|sloshing  nx= ny= nz= dx=  steps=  print=  mode=loop|step|host
-//   precision=0|1  cg_tol=  div_tol=  device=  dump=<prefix>
+//   precision=0|1  cg_tol=  div_tol=  device=  dump=<prefix>  preset=<file>
 // `dump` writes u, v, w, prd1 and ls after the last step as raw float64 in the module arrays'
-// Fortran order and extents (<prefix>_u.bin, ...).
+// Fortran order and extents (<prefix>_u.bin, ...).  `preset` writes the case's time step and
+// level-set preset (one float64, then ls over the cells in Fortran order) and stops before
+// the library is asked for a device.
 //
 // Exit status: 0 on success, 1 on a usage error, 2 when the library returns an error (its
 // message is printed; without a GPU that is SULI_ERR_NODEVICE from suli_create).
@@ -33,7 +35,7 @@
 namespace {
 
 struct Config {
-    std::string kase = "dam_break", mode = "loop", dump;
+    std::string kase = "dam_break", mode = "loop", dump, preset;
     int nx = 64, ny = 32, nz = 48, steps = 10, print = 1, precision = 0, device = 0;
     double dx = 0.01, cg_tol = 1e-10, div_tol = 0.0;
 };
@@ -62,6 +64,7 @@ bool parse(int argc, char** argv, Config& c) {
         if (k == "case") c.kase = v;
         else if (k == "mode") c.mode = v;
         else if (k == "dump") c.dump = v;
+        else if (k == "preset") c.preset = v;
         else if (k == "nx") c.nx = std::atoi(v.c_str());
         else if (k == "ny") c.ny = std::atoi(v.c_str());
         else if (k == "nz") c.nz = std::atoi(v.c_str());
@@ -221,11 +224,24 @@ int main(int argc, char** argv) {
     if (!parse(argc, argv, cfg)) {
         std::fprintf(stderr,
                      "usage: suli_run [case=dam_break|sloshing] [nx= ny= nz= dx=] [steps=] [print=] "
-                     "[mode=loop|step|host] [precision=0|1] [cg_tol=] [div_tol=] [device=] [dump=prefix]\n");
+                     "[mode=loop|step|host] [precision=0|1] [cg_tol=] [div_tol=] [device=] [dump=prefix] "
+                     "[preset=file]\n");
         return 1;
     }
     double depth = 0.0;
     const suli_params p = case_params(cfg, depth);
+    if (!cfg.preset.empty()) {
+        const std::vector<double> ls = ls_preset(cfg);
+        FILE* f = std::fopen(cfg.preset.c_str(), "wb");
+        const bool ok = f && std::fwrite(&p.dt, sizeof(double), 1, f) == 1 &&
+                        std::fwrite(ls.data(), sizeof(double), ls.size(), f) == ls.size();
+        if (f) std::fclose(f);
+        if (!ok) {
+            std::fprintf(stderr, "suli_run: cannot write %s\n", cfg.preset.c_str());
+            return 1;
+        }
+        return 0;
+    }
     Run R;
     if (!R.ok(suli_create(&p, cfg.device, &R.ctx), "suli_create")) return 2;
     // set-up (1_principal.f90:46-62): iniciais, the preset, level_set_ini, contorno(1), contorno(3)
